@@ -1,0 +1,339 @@
+"""Benchmark: raycastFirst on the 2M-triangle noisy torus knot, 2^24 incoherent + 4096^2 camera rays.
+
+One step = one raycastFirst pass of the engine over both ray sets (33,554,432 rays), inputs
+already resident in HBM.  `e2e` is the same work through the public API with host (pinned)
+buffers: host->device copy of the rays, the kernel, device->host copy of the hits.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Under torchrun each rank runs its own copy of the workload (queries shard with the BVH
+replicated: weak scaling, no collective on the data path); `value` is all ranks' rays divided
+by the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s raycastFirst (2M tri)"
+UNIT = "Mrays/s"
+WORKLOAD = ("raycastFirst, TorusKnot(10,3,2000,500) 2,000,000 tri + N(0,0.02) normal noise (seed 1), "
+            "SAH leaf 10; 2^24 incoherent rays (sphere shell r=40, uniform dirs, seed 1) + 4096x4096 "
+            "pinhole camera (distance 35, 45 deg FOV), float32")
+BYTES_RAY_IN, BYTES_HIT_OUT, BYTES_NODE, BYTES_TRI = 24, 32, 32, 36
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--tubular", type=int, default=2000)
+    ap.add_argument("--radial", type=int, default=500)
+    ap.add_argument("--rays-log2", type=int, default=24)
+    ap.add_argument("--camera", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 25, help="rays (both sets together) timed on the CPU baseline")
+    ap.add_argument("--ref-sample", type=int, default=1 << 21, help="rays per set per step in --impl reference")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "engine" else "gloo"
+        if backend == "nccl":
+            import torch
+
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def scene(pkg, args, rank):
+    geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
+    inc = pkg.rays_incoherent(1 << args.rays_log2, seed=1 + 1000 * rank)
+    cam = pkg.rays_camera(args.camera, args.camera)
+    return geo, bvh, inc, cam
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]), reasons=f[4],
+                                 hw=f[5], hwt=f[6], swt=f[7], pcap=f[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max(r["power"] for r in rows)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name> (None if absent)."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def cpu_reference(pkg, bvh, geo, sets, sample, threads):
+    """The oracle (C++ float64 restatement of the reference) on a bounded sample of each ray set.
+    Returns rays/s over the sample plus the reference traversal's mean node reads and triangle
+    tests per ray (the algorithmic-bytes counters)."""
+    import oracle.oracle as orc
+
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+    stats = []
+    total_rays, total_s = 0, 0.0
+    chunk = 1 << 21
+    for rays in sets:
+        idx = np.linspace(0, rays.shape[0] - 1, min(sample, rays.shape[0])).astype(np.int64)
+        sn = st = 0
+        for c0 in range(0, idx.size, chunk):
+            sub = np.ascontiguousarray(rays[idx[c0:c0 + chunk]])
+            t0 = time.perf_counter()
+            _, nn, nt = ref.raycast_first(sub, 0, 0.0, math.inf, threads=threads, counters=True)
+            total_s += time.perf_counter() - t0
+            sn += int(nn.sum())
+            st += int(nt.sum())
+        total_rays += idx.size
+        stats.append((sn / idx.size, st / idx.size))
+    return total_rays / total_s, stats, total_rays
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference path's CPU implementation (the oracle port; the JS
+    reference cannot run without Node and three.js) on all host threads, bounded per step."""
+    if rank != 0:
+        return
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    geo, bvh, inc, cam = scene(pkg, args, 0)
+    threads = os.cpu_count() or 1
+    import oracle.oracle as orc
+
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+    per = max(1, args.ref_sample)
+    sub = np.concatenate([inc[np.linspace(0, inc.shape[0] - 1, per).astype(np.int64)],
+                          cam[np.linspace(0, cam.shape[0] - 1, per).astype(np.int64)]])
+    for _ in range(args.warmup):
+        ref.raycast_first(sub[: min(4096, sub.shape[0])], threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.raycast_first(sub, threads=threads)
+        times.append(time.perf_counter() - t0)
+    rate = sub.shape[0] / statistics.mean(times) / 1e6
+    sample = f"{sub.shape[0]} rays per step ({per} incoherent + {per} camera, evenly strided)"
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "implementation": "oracle C++ float64 restatement (port)"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, ws, rank, local):
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo, bvh, inc, cam = scene(pkg, args, rank)
+    info = bvh.mesh_info()
+    sets = [("incoherent", inc), ("camera", cam)]
+    d_rays = [torch.from_numpy(r).to(dev) for _, r in sets]
+    d_out = [torch.empty((r.shape[0], 8), dtype=torch.float32, device=dev) for _, r in sets]
+    n_step = sum(r.shape[0] for _, r in sets)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(ev=None):
+        for k in range(len(sets)):
+            if ev is not None:
+                ev[k][0].record(stream)
+            bvh.raycast_first_batch(d_rays[k], out=d_out[k], stream=stream.cuda_stream)
+            if ev is not None:
+                ev[k][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    bvh.synchronize(stream.cuda_stream)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    kev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in sets]
+           for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        for s in range(args.steps):
+            step(kev[s])
+        t_end.record(stream)
+        torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    bvh.synchronize(stream.cuda_stream)
+    ms = t_start.elapsed_time(t_end)
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    per_set_ms = [statistics.mean(kev[s][k][0].elapsed_time(kev[s][k][1]) for s in range(args.steps))
+                  for k in range(len(sets))]
+    value = ws * n_step * args.steps / (ms / 1e3) / 1e6
+
+    # e2e through the public API with pinned host buffers (copies inside the timed region)
+    pinned_in = [torch.from_numpy(r).pin_memory() for _, r in sets]
+    pinned_out = [torch.empty((r.shape[0] * 32,), dtype=torch.uint8).pin_memory() for _, r in sets]
+    host_in = [p.numpy() for p in pinned_in]
+    host_out = [p.numpy().view(pkg.HIT_DTYPE) for p in pinned_out]
+    for k in range(len(sets)):
+        bvh.raycast_first_batch(host_in[k], out=host_out[k])
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for k in range(len(sets)):
+            bvh.raycast_first_batch(host_in[k], out=host_out[k])
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": ws * n_step / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": n_step * BYTES_RAY_IN,
+           "d2h_bytes_per_step": n_step * BYTES_HIT_OUT}
+
+    cpu = None
+    roof = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, stats, nsample = cpu_reference(pkg, bvh, geo, [r for _, r in sets], args.cpu_sample // 2, threads)
+        cpu = {"value": rate / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{nsample} rays ({args.cpu_sample // 2} evenly strided from each set), float64 oracle"}
+        bytes_per_launch = []
+        for (name, rays), (mn, mt) in zip(sets, stats):
+            bytes_per_launch.append(rays.shape[0] * (BYTES_RAY_IN + BYTES_HIT_OUT + BYTES_NODE * mn + BYTES_TRI * mt))
+        peak, how = measured_peak()
+        achieved = sum(bytes_per_launch) / (sum(per_set_ms) / 1e3) / 1e9
+        traffic = profile_traffic("raycast_first_k2.md")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": how,
+                "algorithmic_bytes_per_launch": [float(b) for b in bytes_per_launch],
+                "reference_node_reads_per_ray": [s[0] for s in stats],
+                "reference_triangle_tests_per_ray": [s[1] for s in stats],
+                "kernel": "raycast_first_kernel"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "triangles": geo.triangle_count, "rays_per_step": n_step,
+                           "node_records": info["node_records"], "max_depth": info["max_depth"],
+                           "l2": "inputs larger than L2 (805 MB of rays + 1.07 GB of hits per step)",
+                           "parallelism": f"replicas x{ws}"},
+                "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
+                "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": args.steps * len(sets)}
+        print(json.dumps(line), flush=True)
+    bvh.dispose()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_engine(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/*
+ * libbvhcuda — a B200 (sm_100a) query engine for three-mesh-bvh's data-parallel hot path.
+ *
+ * The engine consumes the packed node buffers that `MeshBVH.serialize()` emits (32-byte nodes,
+ * version 1) together with the geometry's position attribute and index, and answers batches of
+ * `raycastFirst`, `raycast` (all hits) and `closestPointToPoint` queries on the GPU.  Results are
+ * in the BVH's local frame, as with the reference's `MeshBVH` methods.
+ *
+ * Reference interfaces (three-mesh-bvh 0.9.14, paths relative to the project root):
+ *   src/core/MeshBVH.js, src/core/BVH.js, src/core/cast/*.js, src/index.d.ts,
+ *   src/utils/ExtensionUtilities.js.
+ *
+ * Conventions
+ *   - Every entry point returns a bvhc_status; BVHC_OK is 0.  Nothing traps or aborts.
+ *   - Buffers are caller-owned.  `mem` says whether the query buffers are host memory
+ *     (BVHC_MEM_HOST: the call copies in, runs and copies out before returning) or device memory
+ *     on the mesh's device (BVHC_MEM_DEVICE: the call only enqueues work on `stream`; call
+ *     bvhc_mesh_synchronize to wait and collect device-side errors).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *   - One bvhc_mesh may be queried from one host thread at a time.
+ *   - All GPU arithmetic is float32 (no FP64 on the device); decisions whose float32 error
+ *     bound does not settle them are re-evaluated in double-float (float-float) arithmetic.
+ */
+#ifndef BVHCUDA_H
+#define BVHCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bvhc_status {
+  BVHC_OK = 0,
+  BVHC_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, bad enum */
+  BVHC_ERR_INVALID_BVH = 2,      /* node buffer fails validation (offsets, counts, depth) */
+  BVHC_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+  BVHC_ERR_OUT_OF_MEMORY = 4,
+  BVHC_ERR_DEVICE = 5,           /* a kernel set the device error word (e.g. stack overflow) */
+  BVHC_ERR_UNSUPPORTED = 6,      /* valid input outside what this build supports */
+  BVHC_ERR_BUILD = 7             /* the CPU builder rejected the input */
+} bvhc_status;
+
+/* three.js side constants (FrontSide, BackSide, DoubleSide). */
+enum { BVHC_FRONT_SIDE = 0, BVHC_BACK_SIDE = 1, BVHC_DOUBLE_SIDE = 2 };
+/* Split strategies (src/core/Constants.js:9,18,28). */
+enum { BVHC_CENTER = 0, BVHC_AVERAGE = 1, BVHC_SAH = 2 };
+/* Memory kind of query buffers. */
+enum { BVHC_MEM_HOST = 0, BVHC_MEM_DEVICE = 1 };
+
+#define BVHC_NO_HIT 0xFFFFFFFFu
+
+/* One ray/triangle intersection in the BVH's local frame (32 bytes).  face_index is the
+ * reference's `faceIndex` (the triangle index after the build's in-place index reorder, or the
+ * indirect-buffer entry); BVHC_NO_HIT when there is no hit.  barycoord is (wA, wB, wC) as
+ * three.js `Triangle.getBarycoord` returns it.  Replaces the `Intersection` objects built by
+ * src/utils/ThreeRayIntersectUtilities.js:49-145 (face/normal/uv are derived on the host from
+ * face_index). */
+typedef struct bvhc_hit {
+  uint32_t face_index;
+  float distance;
+  float point[3];
+  float barycoord[3];
+} bvhc_hit;
+
+/* closestPointToPoint result (20 bytes); face_index == BVHC_NO_HIT for the reference's `null`.
+ * Replaces the HitPointInfo of src/core/cast/closestPointToPoint.js:67-76. */
+typedef struct bvhc_closest {
+  uint32_t face_index;
+  float distance;
+  float point[3];
+} bvhc_closest;
+
+typedef struct bvhc_mesh_info {
+  uint64_t node_records;     /* 64-byte child-pair records on the device */
+  uint64_t triangle_records; /* 48-byte leaf-ordered triangle records on the device */
+  uint64_t device_bytes;     /* device memory held by the mesh */
+  int32_t max_depth;         /* deepest leaf over all roots */
+  int32_t root_count;
+} bvhc_mesh_info;
+
+typedef struct bvhc_serialized bvhc_serialized; /* a MeshBVH.serialize() result owned by the library */
+typedef struct bvhc_mesh bvhc_mesh;             /* a device-resident BVH + triangle set */
+
+/* Human-readable text for a status code. */
+const char* bvhc_status_string(bvhc_status status);
+
+/* ---------------------------------------------------------------------------------------------
+ * Build: `new MeshBVH(geometry, options)` followed by `MeshBVH.serialize(bvh)`
+ * (src/core/GeometryBVH.js:93-163, src/core/build/buildTree.js:123-152,
+ * src/core/MeshBVH.js:112-145).  CPU, run once per mesh; not part of the query path.
+ *   positions        n_verts vertices, `stride_floats` floats apart (xyz first)
+ *   index            optional geometry index (elem 2 or 4 bytes); NULL for non-indexed geometry,
+ *                    in which case a non-indirect build creates one (geometryUtils.js:15-47)
+ *   groups           n_groups (start, count) pairs in index units; count < 0 means Infinity
+ *   range_start/count  draw range in index units; count < 0 means Infinity
+ *   strategy         BVHC_CENTER / BVHC_AVERAGE / BVHC_SAH
+ * The serialized index is the geometry index reordered in place by the build, exactly as the
+ * reference reorders `geometry.index`. */
+bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                       int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                       int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                       int target_leaf_size, int indirect, bvhc_serialized** out);
+int bvhc_serialized_root_count(const bvhc_serialized* s);
+bvhc_status bvhc_serialized_root(const bvhc_serialized* s, int i, const void** data, uint64_t* bytes);
+/* elem_bytes is 0 when there is no index / no indirect buffer. */
+bvhc_status bvhc_serialized_index(const bvhc_serialized* s, const void** data, int* elem_bytes, uint64_t* count);
+bvhc_status bvhc_serialized_indirect(const bvhc_serialized* s, const void** data, int* elem_bytes,
+                                     uint64_t* count);
+void bvhc_serialized_free(bvhc_serialized* s);
+
+/* ---------------------------------------------------------------------------------------------
+ * Upload: `MeshBVH.deserialize(data, geometry)` (src/core/MeshBVH.js:160-232) onto `device`.
+ * Validates every root buffer (node alignment, child links, leaf ranges, depth) and re-lays the
+ * tree as 64-byte child-pair records and the leaf triangles as 48-byte records in leaf order.
+ * `version` 0 buffers (absolute right-child offsets) are converted as the reference does
+ * (MeshBVH.js:206-230). */
+bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, const uint64_t* root_bytes,
+                             int n_roots, const void* index, int index_elem_bytes, uint64_t index_count,
+                             const void* indirect, int indirect_elem_bytes, uint64_t indirect_count,
+                             const float* positions, uint64_t n_verts, int stride_floats, bvhc_mesh** out);
+void bvhc_mesh_destroy(bvhc_mesh* mesh);
+bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
+/* Waits for the mesh's work on `stream` and reports (and clears) the device error word. */
+bvhc_status bvhc_mesh_synchronize(bvhc_mesh* mesh, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Queries.  rays: n x 6 float32 (origin xyz, direction xyz); points: n x 3 float32.
+ */
+
+/* MeshBVH#raycastFirst(ray, side, near, far) for every ray (src/core/MeshBVH.js:558-577,
+ * src/core/cast/raycastFirst.template.js:9-103).  out: n bvhc_hit. */
+bvhc_status bvhc_raycast_first(bvhc_mesh* mesh, const float* rays, uint64_t n, int side, float near_dist,
+                               float far_dist, bvhc_hit* out, int mem, void* stream);
+
+/* MeshBVH#raycast(ray, side, near, far) for every ray (src/core/MeshBVH.js:532-545,
+ * src/core/cast/raycast.template.js:7-53).  Stores at most `cap` hits per ray, in the
+ * reference's DFS order, at hits[i * cap ..]; counts[i] receives the uncapped hit count. */
+bvhc_status bvhc_raycast(bvhc_mesh* mesh, const float* rays, uint64_t n, int side, float near_dist, float far_dist,
+                         uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem, void* stream);
+
+/* MeshBVH#closestPointToPoint(point, target, minThreshold, maxThreshold) for every point
+ * (src/core/MeshBVH.js:874-884, src/core/cast/closestPointToPoint.js:6-78). */
+bvhc_status bvhc_closest_point_to_point(bvhc_mesh* mesh, const float* points, uint64_t n, float min_threshold,
+                                        float max_threshold, bvhc_closest* out, int mem, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BVHCUDA_H */

@@ -1,0 +1,960 @@
+// Oracle: a float64 CPU restatement of three-mesh-bvh 0.9.14's BVH build and query path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA engine is compared against.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load liboracle.so.
+// The product (libbvhcuda) never links, loads or calls it.
+//
+// JavaScript numbers are IEEE-754 doubles and Float32Array stores round to nearest float32, so
+// plain C++ doubles with `(float)` casts at the reference's Float32Array stores reproduce the
+// reference arithmetic operation for operation.  The file must be compiled without FMA
+// contraction or fast-math (-ffp-contract=off), which the Makefile beside it does.
+//
+// The reference's triangle arithmetic lives in three.js r185 (`Ray.intersectTriangle`,
+// `Triangle.getBarycoord`, `Triangle.getNormal`, `Triangle.closestPointToPoint`), which is not
+// vendored.  Those functions are restated here from the published methods they implement:
+//   * ray/triangle: D. Eberly, Geometric Tools, "Intersection of a Ray and a Triangle"
+//     (sign-of-determinant form, DdN / DdQxE2 / DdE1xQ / QdN, non-strict barycentric tests);
+//   * barycentric coordinates: C. Ericson, Real-Time Collision Detection, section 3.4
+//     (dot-product solve; a zero Gram determinant yields (0, 0, 0));
+//   * closest point on triangle: C. Ericson, Real-Time Collision Detection, section 5.1.5.
+//
+// Parity pins for this oracle (the reference holds no numeric golden vectors for this path):
+//   * Utils.geometryUtils.test.js:6-90   degenerate triangle known answer;
+//   * ShapeCasts.test.js:700-754         sphere distance known answers;
+//   * ShapeCasts.test.js:872-1027        hit counts and group/side first hit;
+//   * RandomRaycasts.test.js:179-208     BVH traversal == brute force over every triangle.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr int CENTER = 0, AVERAGE = 1, SAH = 2;             // Constants.js:9,18,28
+constexpr double PRIMITIVE_INTERSECT_COST = 1.25;           // Constants.js:56
+constexpr double TRAVERSAL_COST = 1.0;                      // Constants.js:57
+constexpr int BYTES_PER_NODE = 32;                          // Constants.js:61
+constexpr int UINT32_PER_NODE = 8;                          // Constants.js:62
+constexpr uint16_t IS_LEAFNODE_FLAG = 0xFFFF;               // Constants.js:63
+const double FLOAT32_EPSILON = std::ldexp(1.0, -24);        // Constants.js:71
+constexpr int BIN_COUNT = 32;                               // splitUtils.js:4
+constexpr int FRONT_SIDE = 0, BACK_SIDE = 1, DOUBLE_SIDE = 2;  // three.js side constants
+const double INF = std::numeric_limits<double>::infinity();
+
+struct V3 { double x, y, z; };
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline double dist_sq(V3 a, V3 b) {
+  double dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  return dx * dx + dy * dy + dz * dz;
+}
+
+struct Range { int64_t offset, count; };
+
+// ---------------------------------------------------------------------------------------------
+// Geometry + BVH state (GeometryBVH.js / MeshBVH.js)
+// ---------------------------------------------------------------------------------------------
+struct Bvh {
+  std::vector<float> pos;            // copy of the position attribute
+  int stride = 3;                    // floats per vertex in `pos`
+  int64_t n_verts = 0;
+  bool has_index = false;
+  int index_elem_bytes = 0;          // 2 or 4 when an index exists
+  std::vector<uint32_t> index;       // geometry index (reordered in place by a non-indirect build)
+  bool indirect = false;
+  int indirect_elem_bytes = 0;
+  std::vector<uint32_t> indirect_buf;
+  std::vector<std::vector<uint8_t>> roots;
+
+  int64_t vertex_count() const { return has_index ? (int64_t)index.size() : n_verts; }  // geometryUtils.js:3-7
+  V3 vertex(int64_t v) const {
+    const float* p = &pos[(size_t)v * stride];
+    return {(double)p[0], (double)p[1], (double)p[2]};
+  }
+  // intersectTri: index resolution (ThreeRayIntersectUtilities.js:156-168)
+  void tri_vertices(int64_t tri, int64_t abc[3]) const {
+    for (int k = 0; k < 3; ++k) abc[k] = has_index ? (int64_t)index[(size_t)tri * 3 + k] : tri * 3 + k;
+  }
+  int64_t resolve(int64_t i) const { return indirect ? (int64_t)indirect_buf[(size_t)i] : i; }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Root ranges (geometryUtils.js:60-159)
+// ---------------------------------------------------------------------------------------------
+struct GroupIn { int64_t start; double count; };  // count may be +Infinity
+
+std::vector<Range> get_root_primitive_ranges(int64_t vertex_count, int64_t draw_start, double draw_count,
+                                             const std::vector<GroupIn>& groups, int stride) {
+  // getFullPrimitiveRange (geometryUtils.js:62-75)
+  double primitive_count = (double)vertex_count / stride;
+  double start = (double)draw_start / stride;
+  double end = ((double)draw_start + draw_count) / stride;
+  double offset = std::max(0.0, start);
+  double count = std::min(primitive_count, end) - offset;
+  Range draw{(int64_t)std::floor(offset), (int64_t)std::floor(count)};
+  if (groups.empty()) return {draw};
+
+  struct Ev { double pos; bool is_start; };
+  std::vector<Ev> events;
+  double draw_start_p = (double)draw.offset, draw_end_p = (double)(draw.offset + draw.count);
+  for (const auto& g : groups) {
+    double goff = (double)g.start / stride;
+    double gcount = std::isfinite(g.count / stride) ? g.count / stride : (primitive_count - goff);
+    double gend = goff + gcount;
+    if (goff < draw_end_p && gend > draw_start_p) {
+      events.push_back({std::max(draw_start_p, goff), true});
+      events.push_back({std::min(draw_end_p, gend), false});
+    }
+  }
+  // geometryUtils.js:130-142 orders by position; the order among equal positions never changes the
+  // emitted ranges because a range is only pushed when the position advances.
+  std::stable_sort(events.begin(), events.end(), [](const Ev& a, const Ev& b) { return a.pos < b.pos; });
+  std::vector<Range> ranges;
+  int active = 0;
+  double last = 0;
+  bool have_last = false;
+  for (const auto& e : events) {
+    if (active != 0 && (!have_last || e.pos != last)) ranges.push_back({(int64_t)last, (int64_t)(e.pos - last)});
+    active += e.is_start ? 1 : -1;
+    last = e.pos;
+    have_last = true;
+  }
+  return ranges;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Build (MeshBVH.js:337-436, buildTree.js, splitUtils.js, sortUtils.js, buildUtils.js,
+// computeBoundsUtils.js, ArrayBoxUtilities.js)
+// ---------------------------------------------------------------------------------------------
+struct Node {
+  float bounds[6];
+  bool leaf = false;
+  int64_t offset = 0, count = 0;
+  int split_axis = 0;
+  Node* left = nullptr;
+  Node* right = nullptr;
+  ~Node() { delete left; delete right; }
+};
+
+struct Builder {
+  Bvh& bvh;
+  int strategy, max_depth, target_leaf;
+  std::vector<float> pb;   // primitiveBounds Float32Array: [cx, hx, cy, hy, cz, hz] per primitive
+  int64_t pb_offset = 0;   // primitiveBounds.offset
+  float centroid_cache[6];
+
+  // splitUtils.js:5-17 module-level bin state
+  struct Bin { int64_t count; float bounds[6], right_cache[6], left_cache[6]; double candidate; };
+  Bin bins[BIN_COUNT];
+  float left_bounds[6];
+
+  Builder(Bvh& b, int s, int md, int tl) : bvh(b), strategy(s), max_depth(md), target_leaf(tl) {}
+
+  float& P(int64_t prim, int k) { return pb[(size_t)(prim - pb_offset) * 6 + k]; }
+
+  // MeshBVH.computePrimitiveBounds (MeshBVH.js:365-436)
+  void compute_primitive_bounds(int64_t offset, int64_t count) {
+    for (int64_t i = offset; i < offset + count; ++i) {
+      int64_t tri = bvh.resolve(i);
+      int64_t abc[3];
+      bvh.tri_vertices(tri, abc);
+      for (int el = 0; el < 3; ++el) {
+        double a = bvh.pos[(size_t)abc[0] * bvh.stride + el];
+        double b = bvh.pos[(size_t)abc[1] * bvh.stride + el];
+        double c = bvh.pos[(size_t)abc[2] * bvh.stride + el];
+        double mn = a; if (b < mn) mn = b; if (c < mn) mn = c;
+        double mx = a; if (b > mx) mx = b; if (c > mx) mx = c;
+        double half = (mx - mn) / 2;
+        P(i, el * 2 + 0) = (float)(mn + half);
+        P(i, el * 2 + 1) = (float)(half + (std::fabs(mn) + half) * FLOAT32_EPSILON);
+      }
+    }
+  }
+
+  // getBounds (computeBoundsUtils.js:4-68)
+  void get_bounds(int64_t offset, int64_t count, float* target, float* centroid) {
+    double mn[3] = {INF, INF, INF}, mx[3] = {-INF, -INF, -INF};
+    double cmn[3] = {INF, INF, INF}, cmx[3] = {-INF, -INF, -INF};
+    for (int64_t i = offset; i < offset + count; ++i) {
+      for (int d = 0; d < 3; ++d) {
+        double c = P(i, 2 * d), h = P(i, 2 * d + 1);
+        double l = c - h, r = c + h;
+        if (l < mn[d]) mn[d] = l;
+        if (r > mx[d]) mx[d] = r;
+        if (c < cmn[d]) cmn[d] = c;
+        if (c > cmx[d]) cmx[d] = c;
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      target[d] = (float)mn[d]; target[d + 3] = (float)mx[d];
+      centroid[d] = (float)cmn[d]; centroid[d + 3] = (float)cmx[d];
+    }
+  }
+
+  // ArrayBoxUtilities.js:22-41
+  static int longest_edge(const float* b) {
+    int idx = -1;
+    double best = -INF;
+    for (int i = 0; i < 3; ++i) {
+      double dist = (double)b[i + 3] - (double)b[i];
+      if (dist > best) { best = dist; idx = i; }
+    }
+    return idx;
+  }
+  // ArrayBoxUtilities.js:101-108
+  static double surface_area(const float* b) {
+    double d0 = (double)b[3] - b[0], d1 = (double)b[4] - b[1], d2 = (double)b[5] - b[2];
+    return 2 * (d0 * d1 + d1 * d2 + d2 * d0);
+  }
+  // ArrayBoxUtilities.js:82-99 (expandByPrimitiveBounds)
+  void expand(int64_t prim, float* b) {
+    for (int d = 0; d < 3; ++d) {
+      double c = P(prim, 2 * d), h = P(prim, 2 * d + 1);
+      double tmin = c - h, tmax = c + h;
+      if (tmin < b[d]) b[d] = (float)tmin;
+      if (tmax > b[d + 3]) b[d + 3] = (float)tmax;
+    }
+  }
+  static void make_empty(float* b) {
+    for (int d = 0; d < 3; ++d) { b[d] = (float)INF; b[d + 3] = (float)-INF; }
+  }
+  static void union_bounds(const float* a, const float* b, float* t) {  // ArrayBoxUtilities.js:58-79
+    for (int d = 0; d < 3; ++d) {
+      t[d] = a[d] < b[d] ? a[d] : b[d];
+      t[d + 3] = a[d + 3] > b[d + 3] ? a[d + 3] : b[d + 3];
+    }
+  }
+
+  // getOptimalSplit (splitUtils.js:21-294)
+  void optimal_split(const float* node_bounds, const float* centroid, int64_t offset, int64_t count,
+                     int& axis, double& pos) {
+    axis = -1;
+    pos = 0;
+    if (strategy == CENTER) {
+      axis = longest_edge(centroid);
+      if (axis != -1) pos = ((double)centroid[axis] + (double)centroid[axis + 3]) / 2;
+    } else if (strategy == AVERAGE) {
+      axis = longest_edge(node_bounds);
+      if (axis != -1) {
+        double avg = 0;
+        for (int64_t i = offset; i < offset + count; ++i) avg += P(i, axis * 2);
+        pos = avg / (double)count;
+      }
+    } else if (strategy == SAH) {
+      double root_area = surface_area(node_bounds);
+      double best_cost = PRIMITIVE_INTERSECT_COST * (double)count;
+      for (int a = 0; a < 3; ++a) {
+        double axis_left = centroid[a], axis_right = centroid[a + 3];
+        double axis_length = axis_right - axis_left;
+        double bin_width = axis_length / BIN_COUNT;
+        if (count < BIN_COUNT / 4) {
+          // splitUtils.js:63-174: every primitive center is a candidate
+          std::vector<Bin*> tb;
+          int64_t b = 0;
+          for (int64_t i = offset; i < offset + count; ++i, ++b) {
+            Bin* bin = &bins[b];
+            bin->candidate = P(i, 2 * a);
+            bin->count = 0;
+            make_empty(bin->right_cache);
+            make_empty(bin->left_cache);
+            make_empty(bin->bounds);
+            expand(i, bin->bounds);
+            tb.push_back(bin);
+          }
+          std::stable_sort(tb.begin(), tb.end(), [](const Bin* x, const Bin* y) { return x->candidate < y->candidate; });
+          int64_t split_count = count;
+          for (int64_t bi = 0; bi < split_count; ++bi) {
+            while (bi + 1 < split_count && tb[bi + 1]->candidate == tb[bi]->candidate) {
+              tb.erase(tb.begin() + bi + 1);
+              --split_count;
+            }
+          }
+          for (int64_t i = offset; i < offset + count; ++i) {
+            double center = P(i, 2 * a);
+            for (int64_t bi = 0; bi < split_count; ++bi) {
+              Bin* bin = tb[bi];
+              if (center >= bin->candidate) {
+                expand(i, bin->right_cache);
+              } else {
+                expand(i, bin->left_cache);
+                bin->count++;
+              }
+            }
+          }
+          for (int64_t bi = 0; bi < split_count; ++bi) {
+            Bin* bin = tb[bi];
+            int64_t lc = bin->count, rc = count - bin->count;
+            double lp = 0, rp = 0;
+            if (lc != 0) lp = surface_area(bin->left_cache) / root_area;
+            if (rc != 0) rp = surface_area(bin->right_cache) / root_area;
+            double cost = TRAVERSAL_COST + PRIMITIVE_INTERSECT_COST * (lp * (double)lc + rp * (double)rc);
+            if (cost < best_cost) { axis = a; best_cost = cost; pos = bin->candidate; }
+          }
+        } else {
+          // splitUtils.js:176-281: 32 uniform bins over the centroid extent
+          for (int i = 0; i < BIN_COUNT; ++i) {
+            bins[i].count = 0;
+            bins[i].candidate = axis_left + bin_width + (double)i * bin_width;
+            make_empty(bins[i].bounds);
+          }
+          for (int64_t i = offset; i < offset + count; ++i) {
+            double tri_center = P(i, 2 * a);
+            double rel = tri_center - axis_left;
+            double q = rel / bin_width;
+            int bin_index = std::isnan(q) ? 0 : (int)std::trunc(q);  // `~~` of a value in [0, 32]
+            if (bin_index >= BIN_COUNT) bin_index = BIN_COUNT - 1;
+            bins[bin_index].count++;
+            expand(i, bins[bin_index].bounds);
+          }
+          std::memcpy(bins[BIN_COUNT - 1].right_cache, bins[BIN_COUNT - 1].bounds, sizeof(float) * 6);
+          for (int i = BIN_COUNT - 2; i >= 0; --i) union_bounds(bins[i].bounds, bins[i + 1].right_cache, bins[i].right_cache);
+          int64_t left_count = 0;
+          for (int i = 0; i < BIN_COUNT - 1; ++i) {
+            int64_t bc = bins[i].count;
+            if (bc != 0) {
+              if (left_count == 0) std::memcpy(left_bounds, bins[i].bounds, sizeof(float) * 6);
+              else union_bounds(bins[i].bounds, left_bounds, left_bounds);
+            }
+            left_count += bc;
+            double lp = 0, rp = 0;
+            if (left_count != 0) lp = surface_area(left_bounds) / root_area;
+            int64_t right_count = count - left_count;
+            if (right_count != 0) rp = surface_area(bins[i + 1].right_cache) / root_area;
+            double cost = TRAVERSAL_COST + PRIMITIVE_INTERSECT_COST * (lp * (double)left_count + rp * (double)right_count);
+            if (cost < best_cost) { axis = a; best_cost = cost; pos = bins[i].candidate; }
+          }
+        }
+      }
+    }
+  }
+
+  // partition (sortUtils.js:4-62): Hoare partition of the partition buffer and the bounds
+  int64_t partition(int64_t offset, int64_t count, int axis, double pos) {
+    int64_t left = offset, right = offset + count - 1;
+    uint32_t* buf = bvh.indirect ? bvh.indirect_buf.data() : bvh.index.data();
+    int stride = bvh.indirect ? 1 : 3;
+    while (true) {
+      while (left <= right && (double)P(left, axis * 2) < pos) ++left;
+      while (left <= right && (double)P(right, axis * 2) >= pos) --right;
+      if (left < right) {
+        for (int i = 0; i < stride; ++i) std::swap(buf[left * stride + i], buf[right * stride + i]);
+        for (int i = 0; i < 6; ++i) std::swap(P(left, i), P(right, i));
+        ++left;
+        --right;
+      } else {
+        return left;
+      }
+    }
+  }
+
+  // splitNode (buildTree.js:46-119)
+  void split_node(Node* node, int64_t offset, int64_t count, int depth) {
+    if (count <= target_leaf || depth >= max_depth) {
+      node->leaf = true; node->offset = offset; node->count = count;
+      return;
+    }
+    int axis;
+    double pos;
+    optimal_split(node->bounds, centroid_cache, offset, count, axis, pos);
+    int64_t split_offset = axis == -1 ? -1 : partition(offset, count, axis, pos);
+    if (axis == -1 || split_offset == offset || split_offset == offset + count) {
+      node->leaf = true; node->offset = offset; node->count = count;
+      return;
+    }
+    node->split_axis = axis;
+    node->left = new Node();
+    int64_t lcount = split_offset - offset;
+    get_bounds(offset, lcount, node->left->bounds, centroid_cache);
+    split_node(node->left, offset, lcount, depth + 1);
+    node->right = new Node();
+    int64_t rcount = count - lcount;
+    get_bounds(split_offset, rcount, node->right->bounds, centroid_cache);
+    split_node(node->right, split_offset, rcount, depth + 1);
+  }
+
+  static int64_t count_nodes(const Node* n) { return n->leaf ? 1 : 1 + count_nodes(n->left) + count_nodes(n->right); }
+
+  // _populateBuffer (buildUtils.js:35-92)
+  static int64_t populate(uint8_t* buf, int64_t byte_offset, const Node* n) {
+    float* f32 = reinterpret_cast<float*>(buf + byte_offset);
+    for (int i = 0; i < 6; ++i) f32[i] = n->bounds[i];
+    uint32_t* u32 = reinterpret_cast<uint32_t*>(buf + byte_offset);
+    uint16_t* u16 = reinterpret_cast<uint16_t*>(buf + byte_offset);
+    if (n->leaf) {
+      u32[6] = (uint32_t)n->offset;
+      u16[14] = (uint16_t)n->count;
+      u16[15] = IS_LEAFNODE_FLAG;
+      return byte_offset + BYTES_PER_NODE;
+    }
+    int64_t right_byte = populate(buf, byte_offset + BYTES_PER_NODE, n->left);
+    int64_t rel = right_byte / BYTES_PER_NODE - byte_offset / BYTES_PER_NODE;
+    if (rel > (int64_t)4294967296LL) throw std::runtime_error("MeshBVH: Cannot store relative child node offset greater than 32 bits.");
+    u32[6] = (uint32_t)rel;
+    u32[7] = (uint32_t)n->split_axis;
+    return populate(buf, right_byte, n->right);
+  }
+
+  // buildPackedTree (buildTree.js:123-152)
+  void build(const std::vector<Range>& root_ranges) {
+    Range first = root_ranges.front(), last = root_ranges.back();
+    Range full{first.offset, last.offset + last.count - first.offset};
+    pb.assign((size_t)full.count * 6, 0.0f);
+    pb_offset = full.offset;
+    compute_primitive_bounds(full.offset, full.count);
+    bvh.roots.clear();
+    for (const Range& r : root_ranges) {
+      Node root;
+      get_bounds(r.offset, r.count, root.bounds, centroid_cache);
+      split_node(&root, r.offset, r.count, 0);
+      int64_t n = count_nodes(&root);
+      std::vector<uint8_t> buf((size_t)n * BYTES_PER_NODE, 0);
+      populate(buf.data(), 0, &root);
+      bvh.roots.push_back(std::move(buf));
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Node buffer accessors (nodeBufferUtils.js:3-47)
+// ---------------------------------------------------------------------------------------------
+struct NodeView {
+  const uint8_t* buf;
+  bool is_leaf(int64_t n32) const { return reinterpret_cast<const uint16_t*>(buf)[n32 * 2 + 15] == IS_LEAFNODE_FLAG; }
+  uint32_t offset(int64_t n32) const { return reinterpret_cast<const uint32_t*>(buf)[n32 + 6]; }
+  uint16_t count(int64_t n32) const { return reinterpret_cast<const uint16_t*>(buf)[n32 * 2 + 14]; }
+  int64_t left(int64_t n32) const { return n32 + UINT32_PER_NODE; }
+  int64_t right(int64_t n32) const { return n32 + (int64_t)reinterpret_cast<const uint32_t*>(buf)[n32 + 6] * UINT32_PER_NODE; }
+  uint32_t split_axis(int64_t n32) const { return reinterpret_cast<const uint32_t*>(buf)[n32 + 7]; }
+  double f(int64_t i) const { return (double)reinterpret_cast<const float*>(buf)[i]; }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Leaf arithmetic (three.js r185 functions restated from their published methods)
+// ---------------------------------------------------------------------------------------------
+struct Ray { V3 o, d; };
+
+// Eberly ray/triangle, as called by checkIntersection (ThreeRayIntersectUtilities.js:21-47)
+bool ray_intersect_triangle(const Ray& ray, V3 a, V3 b, V3 c, bool backface_culling, V3& point) {
+  V3 edge1 = sub(b, a), edge2 = sub(c, a);
+  V3 normal = cross(edge1, edge2);
+  double DdN = dot(ray.d, normal);
+  double sign;
+  if (DdN > 0) {
+    if (backface_culling) return false;
+    sign = 1;
+  } else if (DdN < 0) {
+    sign = -1;
+    DdN = -DdN;
+  } else {
+    return false;
+  }
+  V3 diff = sub(ray.o, a);
+  double DdQxE2 = sign * dot(ray.d, cross(diff, edge2));
+  if (DdQxE2 < 0) return false;
+  double DdE1xQ = sign * dot(ray.d, cross(edge1, diff));
+  if (DdE1xQ < 0) return false;
+  if (DdQxE2 + DdE1xQ > DdN) return false;
+  double QdN = -sign * dot(diff, normal);
+  if (QdN < 0) return false;
+  double t = QdN / DdN;
+  point = add(ray.o, scale(ray.d, t));
+  return true;
+}
+
+// Ericson RTCD 3.4 barycentric coordinates, returned as (weight a, weight b, weight c)
+V3 barycoord(V3 p, V3 a, V3 b, V3 c) {
+  V3 v0 = sub(b, a), v1 = sub(c, a), v2 = sub(p, a);
+  double d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1);
+  double d20 = dot(v2, v0), d21 = dot(v2, v1);
+  double denom = d00 * d11 - d01 * d01;
+  if (denom == 0) return {0, 0, 0};
+  double wb = (d11 * d20 - d01 * d21) / denom;
+  double wc = (d00 * d21 - d01 * d20) / denom;
+  return {1 - wb - wc, wb, wc};
+}
+
+// Face normal: (c - b) x (a - b), normalised; zero for a zero-area triangle
+V3 face_normal(V3 a, V3 b, V3 c) {
+  V3 n = cross(sub(c, b), sub(a, b));
+  double l2 = dot(n, n);
+  if (l2 > 0) return scale(n, 1 / std::sqrt(l2));
+  return {0, 0, 0};
+}
+
+// Ericson RTCD 5.1.5 closest point on triangle
+V3 closest_point_on_triangle(V3 p, V3 a, V3 b, V3 c) {
+  V3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+  double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0 && d2 <= 0) return a;
+  V3 bp = sub(p, b);
+  double d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0 && d4 <= d3) return b;
+  double vc = d1 * d4 - d3 * d2;
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+    double v = d1 / (d1 - d3);
+    return add(a, scale(ab, v));
+  }
+  V3 cp = sub(p, c);
+  double d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0 && d5 <= d6) return c;
+  double vb = d5 * d2 - d1 * d6;
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+    double w = d2 / (d2 - d6);
+    return add(a, scale(ac, w));
+  }
+  double va = d3 * d6 - d5 * d4;
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+    double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    return add(b, scale(sub(c, b), w));
+  }
+  double denom = 1 / (va + vb + vc);
+  double v = vb * denom, w = vc * denom;
+  return add(add(a, scale(ab, v)), scale(ac, w));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// C ABI (ctypes)
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+struct orc_hit {
+  int64_t face_index;     // -1 = miss
+  double distance;
+  double point[3];
+  double barycoord[3];
+  double normal[3];
+  int64_t face[3];        // face.a, face.b, face.c
+};
+
+struct orc_cp {
+  int64_t face_index;     // -1 = null result
+  double distance;
+  double point[3];
+};
+
+struct orc_bvh;
+
+}  // extern "C"
+
+struct orc_bvh { Bvh b; };
+
+namespace {
+
+// checkBufferGeometryIntersection + intersectTri (ThreeRayIntersectUtilities.js:49-230)
+bool intersect_tri(const Bvh& g, int side, const Ray& ray, int64_t tri, double near, double far, orc_hit* out) {
+  int64_t abc[3];
+  g.tri_vertices(tri, abc);
+  V3 a = g.vertex(abc[0]), b = g.vertex(abc[1]), c = g.vertex(abc[2]);
+  V3 point;
+  bool hit = side == BACK_SIDE ? ray_intersect_triangle(ray, c, b, a, true, point)
+                               : ray_intersect_triangle(ray, a, b, c, side != DOUBLE_SIDE, point);
+  if (!hit) return false;
+  double distance = std::sqrt(dist_sq(ray.o, point));
+  if (distance < near || distance > far) return false;
+  out->face_index = tri;
+  out->distance = distance;
+  out->point[0] = point.x; out->point[1] = point.y; out->point[2] = point.z;
+  V3 bc = barycoord(point, a, b, c);
+  out->barycoord[0] = bc.x; out->barycoord[1] = bc.y; out->barycoord[2] = bc.z;
+  V3 n = face_normal(a, b, c);
+  out->normal[0] = n.x; out->normal[1] = n.y; out->normal[2] = n.z;
+  out->face[0] = abc[0]; out->face[1] = abc[1]; out->face[2] = abc[2];
+  return true;
+}
+
+// intersectsNodeBounds (intersectUtils.js:2-78)
+bool intersects_node_bounds(const NodeView& nv, int64_t n32, const Ray& ray, double near, double far) {
+  double tmin, tmax, tymin, tymax, tzmin, tzmax;
+  double invx = 1 / ray.d.x, invy = 1 / ray.d.y, invz = 1 / ray.d.z;
+  double ox = ray.o.x, oy = ray.o.y, oz = ray.o.z;
+  double minx = nv.f(n32), maxx = nv.f(n32 + 3);
+  double miny = nv.f(n32 + 1), maxy = nv.f(n32 + 4);
+  double minz = nv.f(n32 + 2), maxz = nv.f(n32 + 5);
+  if (invx >= 0) { tmin = (minx - ox) * invx; tmax = (maxx - ox) * invx; }
+  else { tmin = (maxx - ox) * invx; tmax = (minx - ox) * invx; }
+  if (invy >= 0) { tymin = (miny - oy) * invy; tymax = (maxy - oy) * invy; }
+  else { tymin = (maxy - oy) * invy; tymax = (miny - oy) * invy; }
+  if ((tmin > tymax) || (tymin > tmax)) return false;
+  if (tymin > tmin || std::isnan(tmin)) tmin = tymin;
+  if (tymax < tmax || std::isnan(tmax)) tmax = tymax;
+  if (invz >= 0) { tzmin = (minz - oz) * invz; tzmax = (maxz - oz) * invz; }
+  else { tzmin = (maxz - oz) * invz; tzmax = (minz - oz) * invz; }
+  if ((tmin > tzmax) || (tzmin > tmax)) return false;
+  if (tzmin > tmin || tmin != tmin) tmin = tzmin;
+  if (tzmax < tmax || tmax != tmax) tmax = tzmax;
+  return tmin <= far && tmax >= near;
+}
+
+struct Counters { int64_t nodes = 0, tris = 0; };
+
+// _raycastFirst (raycastFirst.template.js:19-103) with intersectClosestTri (iterationUtils.template.js:24-53)
+bool raycast_first_rec(const Bvh& g, const NodeView& nv, int64_t n32, int side, const Ray& ray, double near,
+                       double far, orc_hit* res, Counters& ctr) {
+  if (nv.is_leaf(n32)) {
+    int64_t offset = nv.offset(n32), count = nv.count(n32);
+    double dist = INF;
+    bool found = false;
+    for (int64_t i = offset; i < offset + count; ++i) {
+      orc_hit h;
+      ctr.tris++;
+      if (intersect_tri(g, side, ray, g.resolve(i), near, far, &h) && h.distance < dist) {
+        *res = h;
+        dist = h.distance;
+        found = true;
+      }
+    }
+    return found;
+  }
+  int axis = (int)nv.split_axis(n32);
+  double ray_dir = axis == 0 ? ray.d.x : axis == 1 ? ray.d.y : ray.d.z;
+  bool left_to_right = ray_dir >= 0;
+  int64_t c1, c2;
+  if (left_to_right) { c1 = nv.left(n32); c2 = nv.right(n32); }
+  else { c1 = nv.right(n32); c2 = nv.left(n32); }
+  orc_hit r1, r2;
+  ctr.nodes++;
+  bool has1 = intersects_node_bounds(nv, c1, ray, near, far) && raycast_first_rec(g, nv, c1, side, ray, near, far, &r1, ctr);
+  ctr.nodes++;  // c2's bounds are read either by the early-out test or by intersectsNodeBounds
+  if (has1) {
+    double point = r1.point[axis];
+    bool outside = left_to_right ? point <= nv.f(c2 + axis) : point >= nv.f(c2 + axis + 3);
+    if (outside) { *res = r1; return true; }
+  }
+  bool has2 = intersects_node_bounds(nv, c2, ray, near, far) && raycast_first_rec(g, nv, c2, side, ray, near, far, &r2, ctr);
+  if (has1 && has2) { *res = r1.distance <= r2.distance ? r1 : r2; return true; }
+  if (has1) { *res = r1; return true; }
+  if (has2) { *res = r2; return true; }
+  return false;
+}
+
+// MeshBVH.raycastFirst roots loop (MeshBVH.js:558-577)
+void raycast_first(const Bvh& g, int side, const Ray& ray, double near, double far, orc_hit* out, Counters& ctr) {
+  out->face_index = -1;
+  bool have = false;
+  for (const auto& root : g.roots) {
+    NodeView nv{root.data()};
+    orc_hit h;
+    ctr.nodes++;  // the root record
+    if (raycast_first_rec(g, nv, 0, side, ray, near, far, &h, ctr)) {
+      if (!have || h.distance < out->distance) { *out = h; have = true; }
+    }
+  }
+}
+
+// _raycast (raycast.template.js:15-53) with intersectTris (iterationUtils.template.js:4-22)
+void raycast_all_rec(const Bvh& g, const NodeView& nv, int64_t n32, int side, const Ray& ray, double near, double far,
+                     std::vector<orc_hit>& hits, Counters& ctr) {
+  if (nv.is_leaf(n32)) {
+    int64_t offset = nv.offset(n32), count = nv.count(n32);
+    for (int64_t i = offset; i < offset + count; ++i) {
+      orc_hit h;
+      ctr.tris++;
+      if (intersect_tri(g, side, ray, g.resolve(i), near, far, &h)) hits.push_back(h);
+    }
+    return;
+  }
+  int64_t l = nv.left(n32);
+  ctr.nodes++;
+  if (intersects_node_bounds(nv, l, ray, near, far)) raycast_all_rec(g, nv, l, side, ray, near, far, hits, ctr);
+  int64_t r = nv.right(n32);
+  ctr.nodes++;
+  if (intersects_node_bounds(nv, r, ray, near, far)) raycast_all_rec(g, nv, r, side, ray, near, far, hits, ctr);
+}
+
+// closestPointToPoint (cast/closestPointToPoint.js:6-78) through shapecast (BVH.js:342-413,
+// shapecast.js:41-214) and iterateOverTriangles (iterationUtils.template.js:55-93)
+struct CPState {
+  V3 p;
+  double min_sq, max_sq;
+  double closest_sq = INF;
+  int64_t closest_tri = -1;
+  V3 closest_point{0, 0, 0};
+};
+
+double box_score(const NodeView& nv, int64_t n32, V3 p) {
+  // temp.copy(point).clamp(box.min, box.max); temp.distanceToSquared(point)
+  double mn[3] = {nv.f(n32), nv.f(n32 + 1), nv.f(n32 + 2)};
+  double mx[3] = {nv.f(n32 + 3), nv.f(n32 + 4), nv.f(n32 + 5)};
+  double pv[3] = {p.x, p.y, p.z}, t[3];
+  for (int k = 0; k < 3; ++k) t[k] = std::max(mn[k], std::min(mx[k], pv[k]));
+  V3 tv{t[0], t[1], t[2]};
+  return dist_sq(tv, p);
+}
+
+bool cp_range(const Bvh& g, int64_t offset, int64_t count, CPState& st, Counters& ctr) {
+  for (int64_t i = offset; i < offset + count; ++i) {
+    int64_t tri = g.resolve(i);
+    int64_t abc[3];
+    g.tri_vertices(tri, abc);
+    ctr.tris++;
+    V3 cp = closest_point_on_triangle(st.p, g.vertex(abc[0]), g.vertex(abc[1]), g.vertex(abc[2]));
+    double d2 = dist_sq(st.p, cp);
+    if (d2 < st.closest_sq) { st.closest_point = cp; st.closest_sq = d2; st.closest_tri = tri; }
+    if (d2 < st.min_sq) return true;
+  }
+  return false;
+}
+
+bool cp_traverse(const Bvh& g, const NodeView& nv, int64_t n32, CPState& st, Counters& ctr) {
+  if (nv.is_leaf(n32)) return cp_range(g, nv.offset(n32), nv.count(n32), st, ctr);
+  int64_t c1 = nv.left(n32), c2 = nv.right(n32);
+  ctr.nodes += 2;
+  double s1 = box_score(nv, c1, st.p), s2 = box_score(nv, c2, st.p);
+  if (s2 < s1) { std::swap(c1, c2); std::swap(s1, s2); }
+  if (s1 < st.closest_sq && s1 < st.max_sq) {
+    if (cp_traverse(g, nv, c1, st, ctr)) return true;
+  }
+  if (s2 < st.closest_sq && s2 < st.max_sq) {
+    if (cp_traverse(g, nv, c2, st, ctr)) return true;
+  }
+  return false;
+}
+
+void closest_point(const Bvh& g, V3 p, double min_t, double max_t, orc_cp* out, Counters& ctr) {
+  CPState st;
+  st.p = p;
+  st.min_sq = min_t * min_t;
+  st.max_sq = max_t * max_t;
+  for (const auto& root : g.roots) {
+    NodeView nv{root.data()};
+    ctr.nodes++;
+    if (cp_traverse(g, nv, 0, st, ctr)) break;
+  }
+  if (st.closest_sq == INF) {
+    out->face_index = -1;
+    out->distance = INF;
+    out->point[0] = out->point[1] = out->point[2] = 0;
+    return;
+  }
+  out->face_index = st.closest_tri;
+  out->distance = std::sqrt(st.closest_sq);
+  out->point[0] = st.closest_point.x; out->point[1] = st.closest_point.y; out->point[2] = st.closest_point.z;
+}
+
+template <class F>
+void parallel_for(int64_t n, int threads, F f) {
+  if (threads <= 1 || n < 64) { f(0, n); return; }
+  std::vector<std::thread> pool;
+  int64_t chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    int64_t s = t * chunk, e = std::min(n, s + chunk);
+    if (s >= e) break;
+    pool.emplace_back([=] { f(s, e); });
+  }
+  for (auto& th : pool) th.join();
+}
+
+Ray load_ray(const float* r) { return {{r[0], r[1], r[2]}, {r[3], r[4], r[5]}}; }
+
+}  // namespace
+
+extern "C" {
+
+// Build a MeshBVH (GeometryBVH constructor + init, GeometryBVH.js:93-163).  `index` may be null for a
+// non-indexed geometry; `groups` holds (start, count) pairs in index units, count < 0 meaning
+// Infinity; draw_count < 0 means Infinity.  Returns null on error.
+orc_bvh* orc_build(const float* pos, int64_t n_verts, int stride, const uint32_t* index, int64_t index_count,
+                   int index_elem_bytes, const int64_t* groups, int n_groups, int64_t draw_start,
+                   int64_t draw_count, int strategy, int max_depth, int target_leaf, int indirect) {
+  try {
+    auto* h = new orc_bvh();
+    Bvh& g = h->b;
+    g.pos.assign(pos, pos + (size_t)n_verts * stride);
+    g.stride = stride;
+    g.n_verts = n_verts;
+    if (index) {
+      g.has_index = true;
+      g.index.assign(index, index + index_count);
+      g.index_elem_bytes = index_elem_bytes;
+    }
+    std::vector<GroupIn> gr;
+    for (int i = 0; i < n_groups; ++i) gr.push_back({groups[2 * i], groups[2 * i + 1] < 0 ? INF : (double)groups[2 * i + 1]});
+    double dcount = draw_count < 0 ? INF : (double)draw_count;
+    std::vector<Range> ranges;
+    if (indirect) {
+      // generateIndirectBuffer (GeometryBVH.js:9-37)
+      ranges = get_root_primitive_ranges(g.vertex_count(), draw_start, dcount, gr, 3);
+      g.indirect = true;
+      const Range& last = ranges.back();
+      g.indirect_elem_bytes = (last.offset + last.count > 65536) ? 4 : 2;
+      for (const Range& r : ranges)
+        for (int64_t i = 0; i < r.count; ++i) g.indirect_buf.push_back((uint32_t)(r.offset + i));
+      ranges = {{0, (int64_t)g.indirect_buf.size()}};
+    } else {
+      if (!g.has_index) {
+        // ensureIndex (geometryUtils.js:15-47)
+        g.has_index = true;
+        g.index_elem_bytes = n_verts > 65535 ? 4 : 2;
+        g.index.resize((size_t)n_verts);
+        for (int64_t i = 0; i < n_verts; ++i) g.index[(size_t)i] = (uint32_t)i;
+      }
+      ranges = get_root_primitive_ranges(g.vertex_count(), draw_start, dcount, gr, 3);
+    }
+    Builder b(g, strategy, max_depth, target_leaf);
+    b.build(ranges);
+    return h;
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+// MeshBVH.deserialize (MeshBVH.js:160-232) for version-1 data: adopt the buffers as given.
+orc_bvh* orc_from_serialized(const void* const* roots, const int64_t* root_bytes, int n_roots, const uint32_t* index,
+                             int64_t index_count, const uint32_t* indirect_buf, int64_t n_indirect, const float* pos,
+                             int64_t n_verts, int stride) {
+  auto* h = new orc_bvh();
+  Bvh& g = h->b;
+  g.pos.assign(pos, pos + (size_t)n_verts * stride);
+  g.stride = stride;
+  g.n_verts = n_verts;
+  if (index) { g.has_index = true; g.index.assign(index, index + index_count); g.index_elem_bytes = 4; }
+  if (indirect_buf) { g.indirect = true; g.indirect_buf.assign(indirect_buf, indirect_buf + n_indirect); g.indirect_elem_bytes = 4; }
+  for (int i = 0; i < n_roots; ++i) {
+    const uint8_t* p = static_cast<const uint8_t*>(roots[i]);
+    g.roots.emplace_back(p, p + root_bytes[i]);
+  }
+  return h;
+}
+
+void orc_free(orc_bvh* h) { delete h; }
+int orc_num_roots(const orc_bvh* h) { return (int)h->b.roots.size(); }
+int64_t orc_root_bytes(const orc_bvh* h, int i) { return (int64_t)h->b.roots[i].size(); }
+void orc_copy_root(const orc_bvh* h, int i, void* dst) { std::memcpy(dst, h->b.roots[i].data(), h->b.roots[i].size()); }
+int orc_index_elem_bytes(const orc_bvh* h) { return h->b.has_index ? h->b.index_elem_bytes : 0; }
+int64_t orc_index_count(const orc_bvh* h) { return (int64_t)h->b.index.size(); }
+void orc_copy_index(const orc_bvh* h, uint32_t* dst) { std::memcpy(dst, h->b.index.data(), h->b.index.size() * 4); }
+int orc_indirect_elem_bytes(const orc_bvh* h) { return h->b.indirect ? h->b.indirect_elem_bytes : 0; }
+int64_t orc_indirect_count(const orc_bvh* h) { return (int64_t)h->b.indirect_buf.size(); }
+void orc_copy_indirect(const orc_bvh* h, uint32_t* dst) { std::memcpy(dst, h->b.indirect_buf.data(), h->b.indirect_buf.size() * 4); }
+
+// MeshBVH.raycastFirst over a batch of float32 rays (n x [ox oy oz dx dy dz]).  node_reads and
+// tri_tests (nullable) receive, per ray, the node records and triangles the reference touches.
+void orc_raycast_first(const orc_bvh* h, const float* rays, int64_t n, int side, double near, double far,
+                       orc_hit* out, int64_t* node_reads, int64_t* tri_tests, int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      Counters c;
+      raycast_first(h->b, side, load_ray(rays + 6 * i), near, far, &out[i], c);
+      if (node_reads) node_reads[i] = c.nodes;
+      if (tri_tests) tri_tests[i] = c.tris;
+    }
+  });
+}
+
+// MeshBVH.raycast (all hits, DFS order) with at most `cap` hits stored per ray; counts[i] is the
+// uncapped number of hits.
+void orc_raycast_all(const orc_bvh* h, const float* rays, int64_t n, int side, double near, double far, int cap,
+                     int32_t* counts, orc_hit* hits, int64_t* node_reads, int64_t* tri_tests, int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    std::vector<orc_hit> tmp;
+    for (int64_t i = s; i < e; ++i) {
+      tmp.clear();
+      Counters c;
+      Ray ray = load_ray(rays + 6 * i);
+      for (const auto& root : h->b.roots) {
+        NodeView nv{root.data()};
+        c.nodes++;
+        raycast_all_rec(h->b, nv, 0, side, ray, near, far, tmp, c);
+      }
+      counts[i] = (int32_t)tmp.size();
+      for (int k = 0; k < (int)tmp.size() && k < cap; ++k) hits[i * cap + k] = tmp[k];
+      if (node_reads) node_reads[i] = c.nodes;
+      if (tri_tests) tri_tests[i] = c.tris;
+    }
+  });
+}
+
+// MeshBVH.closestPointToPoint over a batch of float32 points (n x 3).
+void orc_closest_point(const orc_bvh* h, const float* pts, int64_t n, double min_t, double max_t, orc_cp* out,
+                       int64_t* node_reads, int64_t* tri_tests, int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      Counters c;
+      V3 p{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+      closest_point(h->b, p, min_t, max_t, &out[i], c);
+      if (node_reads) node_reads[i] = c.nodes;
+      if (tri_tests) tri_tests[i] = c.tris;
+    }
+  });
+}
+
+// Brute force over every triangle the BVH covers (the roots' ranges, in order): all hits, the way
+// three.js's un-accelerated Mesh.raycast visits them.
+void orc_brute_raycast_all(const orc_bvh* h, const float* rays, int64_t n, int side, double near, double far, int cap,
+                           int32_t* counts, orc_hit* hits, int threads) {
+  std::vector<Range> ranges;
+  for (const auto& root : h->b.roots) {
+    // collect the leaf ranges of each root in buffer order
+    NodeView nv{root.data()};
+    int64_t nodes = (int64_t)root.size() / BYTES_PER_NODE;
+    for (int64_t k = 0; k < nodes; ++k)
+      if (nv.is_leaf(k * UINT32_PER_NODE)) ranges.push_back({nv.offset(k * UINT32_PER_NODE), nv.count(k * UINT32_PER_NODE)});
+  }
+  std::sort(ranges.begin(), ranges.end(), [](const Range& a, const Range& b) { return a.offset < b.offset; });
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      Ray ray = load_ray(rays + 6 * i);
+      int32_t cnt = 0;
+      for (const Range& r : ranges)
+        for (int64_t t = r.offset; t < r.offset + r.count; ++t) {
+          orc_hit hh;
+          if (intersect_tri(h->b, side, ray, h->b.resolve(t), near, far, &hh)) {
+            if (cnt < cap) hits[i * cap + cnt] = hh;
+            ++cnt;
+          }
+        }
+      counts[i] = cnt;
+    }
+  });
+}
+
+// Single triangle test (three.js Ray.intersectTriangle semantics), for unit tests.
+int orc_ray_triangle(const double* o, const double* d, const double* a, const double* b, const double* c, int side,
+                     double near, double far, orc_hit* out) {
+  Bvh g;
+  g.stride = 3;
+  g.n_verts = 3;
+  g.pos = {(float)a[0], (float)a[1], (float)a[2], (float)b[0], (float)b[1], (float)b[2], (float)c[0], (float)c[1], (float)c[2]};
+  Ray ray{{o[0], o[1], o[2]}, {d[0], d[1], d[2]}};
+  out->face_index = -1;
+  return intersect_tri(g, side, ray, 0, near, far, out) ? 1 : 0;
+}
+
+// Single closest-point-on-triangle evaluation (Ericson 5.1.5), for unit tests.
+void orc_closest_point_triangle(const double* p, const double* a, const double* b, const double* c, double* out) {
+  V3 r = closest_point_on_triangle({p[0], p[1], p[2]}, {a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]});
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+// Statistics in the style of getBVHExtremes (debug/Debug.js:36-134): node count, leaf count,
+// max depth, total leaf triangles.
+void orc_stats(const orc_bvh* h, int64_t* out4) {
+  int64_t nodes = 0, leaves = 0, maxd = 0, tris = 0;
+  for (const auto& root : h->b.roots) {
+    NodeView nv{root.data()};
+    std::vector<std::pair<int64_t, int64_t>> st{{0, 0}};
+    while (!st.empty()) {
+      auto [n, d] = st.back();
+      st.pop_back();
+      ++nodes;
+      maxd = std::max(maxd, d);
+      if (nv.is_leaf(n)) { ++leaves; tris += nv.count(n); }
+      else { st.push_back({nv.left(n), d + 1}); st.push_back({nv.right(n), d + 1}); }
+    }
+  }
+  out4[0] = nodes; out4[1] = leaves; out4[2] = maxd; out4[3] = tris;
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+"""ctypes wrapper of liboracle.so — TEST INFRASTRUCTURE ONLY.
+
+The oracle is a float64 CPU restatement of three-mesh-bvh's build and query path (oracle.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+HIT_DTYPE = np.dtype([("face_index", "<i8"), ("distance", "<f8"), ("point", "<f8", 3), ("barycoord", "<f8", 3),
+                      ("normal", "<f8", 3), ("face", "<i8", 3)])
+CP_DTYPE = np.dtype([("face_index", "<i8"), ("distance", "<f8"), ("point", "<f8", 3)])
+
+_lib = None
+
+
+def build() -> Path:
+    src = HERE / "oracle.cpp"
+    if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(str(LIB_PATH))
+        P, I64, I = C.c_void_p, C.c_int64, C.c_int
+        D = C.c_double
+        L.orc_build.restype = P
+        L.orc_build.argtypes = [P, I64, I, P, I64, I, P, I, I64, I64, I, I, I, I]
+        L.orc_from_serialized.restype = P
+        L.orc_from_serialized.argtypes = [P, P, I, P, I64, P, I64, P, I64, I]
+        L.orc_free.argtypes = [P]
+        L.orc_num_roots.argtypes = [P]
+        L.orc_root_bytes.restype = I64
+        L.orc_root_bytes.argtypes = [P, I]
+        L.orc_copy_root.argtypes = [P, I, P]
+        L.orc_index_elem_bytes.argtypes = [P]
+        L.orc_index_count.restype = I64
+        L.orc_index_count.argtypes = [P]
+        L.orc_copy_index.argtypes = [P, P]
+        L.orc_indirect_elem_bytes.argtypes = [P]
+        L.orc_indirect_count.restype = I64
+        L.orc_indirect_count.argtypes = [P]
+        L.orc_copy_indirect.argtypes = [P, P]
+        L.orc_raycast_first.argtypes = [P, P, I64, I, D, D, P, P, P, I]
+        L.orc_raycast_all.argtypes = [P, P, I64, I, D, D, I, P, P, P, P, I]
+        L.orc_closest_point.argtypes = [P, P, I64, D, D, P, P, P, I]
+        L.orc_brute_raycast_all.argtypes = [P, P, I64, I, D, D, I, P, P, I]
+        L.orc_ray_triangle.restype = I
+        L.orc_ray_triangle.argtypes = [P, P, P, P, P, I, D, D, P]
+        L.orc_closest_point_triangle.argtypes = [P, P, P, P, P]
+        L.orc_stats.argtypes = [P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data if a is not None else None
+
+
+def _threads():
+    import os
+    return os.cpu_count() or 1
+
+
+class OracleBVH:
+    """A reference-semantics BVH: built by the restated builder, or adopted from serialized data."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_free(self.h)
+            self.h = None
+
+    @classmethod
+    def build(cls, position, index=None, groups=(), draw_range=(0, math.inf), strategy=2, max_depth=40,
+              target_leaf=10, indirect=False):
+        pos = np.ascontiguousarray(position, dtype=np.float32).reshape(-1, 3)
+        idx = None if index is None else np.ascontiguousarray(index).astype(np.uint32)
+        elem = 0 if index is None else np.asarray(index).dtype.itemsize
+        g = np.array([[s, -1 if (isinstance(c, float) and math.isinf(c)) else c] for s, c, *_ in groups],
+                     dtype=np.int64).reshape(-1)
+        dc = -1 if math.isinf(draw_range[1]) else int(draw_range[1])
+        h = lib().orc_build(_p(pos), pos.shape[0], 3, _p(idx), 0 if idx is None else idx.size, elem,
+                            _p(g) if g.size else None, len(groups), int(draw_range[0]), dc, strategy, max_depth,
+                            target_leaf, 1 if indirect else 0)
+        if not h:
+            raise RuntimeError("oracle build failed")
+        return cls(h)
+
+    @classmethod
+    def from_serialized(cls, roots, index, indirect, position):
+        pos = np.ascontiguousarray(position, dtype=np.float32).reshape(-1, 3)
+        bufs = [np.frombuffer(bytes(r), dtype=np.uint8) for r in roots]
+        ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+        sizes = (C.c_int64 * len(bufs))(*[b.size for b in bufs])
+        idx = None if index is None else np.ascontiguousarray(index).astype(np.uint32)
+        ind = None if indirect is None else np.ascontiguousarray(indirect).astype(np.uint32)
+        h = lib().orc_from_serialized(ptrs, sizes, len(bufs), _p(idx), 0 if idx is None else idx.size, _p(ind),
+                                      0 if ind is None else ind.size, _p(pos), pos.shape[0], 3)
+        obj = cls(h)
+        obj._keep = (bufs, idx, ind, pos)
+        return obj
+
+    def roots(self):
+        L = lib()
+        out = []
+        for i in range(L.orc_num_roots(self.h)):
+            b = np.empty(L.orc_root_bytes(self.h, i), dtype=np.uint8)
+            L.orc_copy_root(self.h, i, _p(b))
+            out.append(b.tobytes())
+        return out
+
+    def index(self):
+        L = lib()
+        eb = L.orc_index_elem_bytes(self.h)
+        if eb == 0:
+            return None
+        a = np.empty(L.orc_index_count(self.h), dtype=np.uint32)
+        L.orc_copy_index(self.h, _p(a))
+        return a.astype(np.uint16 if eb == 2 else np.uint32)
+
+    def indirect(self):
+        L = lib()
+        eb = L.orc_indirect_elem_bytes(self.h)
+        if eb == 0:
+            return None
+        a = np.empty(L.orc_indirect_count(self.h), dtype=np.uint32)
+        L.orc_copy_indirect(self.h, _p(a))
+        return a.astype(np.uint16 if eb == 2 else np.uint32)
+
+    def stats(self):
+        s = np.zeros(4, dtype=np.int64)
+        lib().orc_stats(self.h, _p(s))
+        return dict(nodes=int(s[0]), leaves=int(s[1]), max_depth=int(s[2]), leaf_triangles=int(s[3]))
+
+    def raycast_first(self, rays, side=0, near=0.0, far=math.inf, threads=None, counters=False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        out = np.empty(n, dtype=HIT_DTYPE)
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_raycast_first(self.h, _p(rays), n, side, near, far, _p(out), _p(nn), _p(nt), threads or _threads())
+        return (out, nn, nt) if counters else out
+
+    def raycast_all(self, rays, side=0, near=0.0, far=math.inf, cap=64, threads=None, counters=False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        counts = np.empty(n, dtype=np.int32)
+        hits = np.empty((n, cap), dtype=HIT_DTYPE)
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_raycast_all(self.h, _p(rays), n, side, near, far, cap, _p(counts), _p(hits), _p(nn), _p(nt),
+                              threads or _threads())
+        return (counts, hits, nn, nt) if counters else (counts, hits)
+
+    def brute_raycast_all(self, rays, side=0, near=0.0, far=math.inf, cap=64, threads=None):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        counts = np.empty(n, dtype=np.int32)
+        hits = np.empty((n, cap), dtype=HIT_DTYPE)
+        lib().orc_brute_raycast_all(self.h, _p(rays), n, side, near, far, cap, _p(counts), _p(hits),
+                                    threads or _threads())
+        return counts, hits
+
+    def closest_point(self, points, min_t=0.0, max_t=math.inf, threads=None, counters=False):
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        n = pts.shape[0]
+        out = np.empty(n, dtype=CP_DTYPE)
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_closest_point(self.h, _p(pts), n, min_t, max_t, _p(out), _p(nn), _p(nt), threads or _threads())
+        return (out, nn, nt) if counters else out
+
+
+def ray_triangle(o, d, a, b, c, side=0, near=0.0, far=math.inf):
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (o, d, a, b, c)]
+    out = np.zeros(1, dtype=HIT_DTYPE)
+    hit = lib().orc_ray_triangle(*[_p(x) for x in arrs], side, near, far, _p(out))
+    return out[0] if hit else None
+
+
+def closest_point_triangle(p, a, b, c):
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (p, a, b, c)]
+    out = np.zeros(3)
+    lib().orc_closest_point_triangle(*[_p(x) for x in arrs], _p(out))
+    return out

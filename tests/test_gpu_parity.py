@@ -1,0 +1,174 @@
+"""GPU parity: libbvhcuda's kernels, called through the C ABI, against the oracle on the same
+serialized BVHs and the same float32 inputs (tolerances in tests/parity.py)."""
+import math
+
+import numpy as np
+import pytest
+
+from parity import check_all, check_closest, check_first, tie_exempt
+
+pytestmark = pytest.mark.gpu
+
+ZERO = dict(hitmiss=0, face=0, distance=0, point=0, barycoord=0)
+
+
+def _assert_first_ok(rep):
+    bad = {k: rep[k] for k in ZERO if rep[k]}
+    assert not bad, rep
+
+
+def _oracle_for(orc, bvh, geo):
+    return orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+
+
+@pytest.fixture(scope="module")
+def knot80k(pkg, orc, cuda):
+    geo = pkg.torus_knot(10, 3, 400, 100)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
+    return geo, bvh, _oracle_for(orc, bvh, geo)
+
+
+@pytest.mark.parametrize("side", [0, 1, 2])
+def test_raycast_first_knot80k(pkg, knot80k, side):
+    geo, bvh, ref = knot80k
+    rays = pkg.rays_sphere_to_box(200_000 if side == 0 else 50_000, seed=0)
+    got = bvh.raycast_first_batch(rays, side)
+    exp = ref.raycast_first(rays, side)
+    ac, ah = ref.raycast_all(rays, side, cap=64)
+    rep = check_first(got, exp, tie_exempt(ac, ah))
+    _assert_first_ok(rep)
+    assert rep["hits"] > rays.shape[0] // 10
+
+
+def test_raycast_all_knot80k(pkg, knot80k):
+    geo, bvh, ref = knot80k
+    rays = pkg.rays_sphere_to_box(50_000, seed=5)
+    for side in (0, 2):
+        counts, hits = bvh.raycast_batch(rays, side, cap=64)
+        ec, eh = ref.raycast_all(rays, side, cap=64)
+        rep = check_all(counts, hits, ec, eh)
+        assert rep["count"] == 0 and rep["set"] == 0 and rep["distance"] == 0, rep
+
+
+def test_closest_point_knot80k(pkg, orc, knot80k):
+    geo, bvh, ref = knot80k
+    pts = pkg.grid_points(geo.position.min(0), geo.position.max(0), 40)
+    got = bvh.closest_point_batch(pts, 0.0, 5.0)
+    exp = ref.closest_point(pts, 0.0, 5.0)
+
+    def tri_distance(i, face):
+        t = geo.triangle(face)
+        q = orc.closest_point_triangle(pts[i].astype(np.float64), *t)
+        return float(np.linalg.norm(q - pts[i].astype(np.float64)))
+
+    rep = check_closest(got, exp, tri_distance)
+    assert rep["null"] == 0 and rep["distance"] == 0 and rep["face"] == 0, rep
+
+
+def test_closest_point_min_threshold_and_unbounded(pkg, knot80k):
+    geo, bvh, ref = knot80k
+    pts = pkg.grid_points(geo.position.min(0), geo.position.max(0), 16)
+    for lo, hi in ((0.0, math.inf), (0.5, 3.0)):
+        got = bvh.closest_point_batch(pts, lo, hi)
+        exp = ref.closest_point(pts, lo, hi)
+        rep = check_closest(got, exp)
+        assert rep["null"] == 0, rep
+        if lo == 0.0:
+            assert rep["distance"] == 0, rep
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2])
+@pytest.mark.parametrize("indirect", [False, True])
+@pytest.mark.parametrize("grouped", [False, True])
+def test_random_torus_matrix(pkg, orc, cuda, strategy, indirect, grouped):
+    """RandomRaycasts.test.js:32-38 matrix, with near/far in {0, 6} x {inf, 7}."""
+    geo = pkg.torus(1, 1, 40, 10)
+    if grouped:
+        size = geo.index.size // 10
+        for g in range(10):
+            geo.add_group(g * size, size, 0)
+    bvh = pkg.MeshBVH(geo, {"strategy": strategy, "indirect": indirect})
+    ref = _oracle_for(orc, bvh, geo)
+    rng = np.random.default_rng(100 + strategy * 4 + indirect * 2 + grouped)
+    o = rng.uniform(-5, 5, size=(2000, 3))
+    d = rng.uniform(-1, 1, size=(2000, 3)) - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d], 1).astype(np.float32)
+    for near, far in ((0.0, math.inf), (6.0, math.inf), (0.0, 7.0), (6.0, 7.0)):
+        got = bvh.raycast_first_batch(rays, 0, near, far)
+        exp = ref.raycast_first(rays, 0, near, far)
+        ac, ah = ref.raycast_all(rays, 0, near, far)
+        _assert_first_ok(check_first(got, exp, tie_exempt(ac, ah)))
+        counts, hits = bvh.raycast_batch(rays, 0, near, far)
+        rep = check_all(counts, hits, ac, ah)
+        assert rep["count"] == 0 and rep["set"] == 0, rep
+    bvh.dispose()
+
+
+def test_degenerate_triangle_gpu(pkg, cuda):
+    pos = np.array([[2, 0, 0], [0, 0, 0], [1, 1e-15, 0]], dtype=np.float32)
+    geo = pkg.Geometry(pos, None)
+    bvh = pkg.MeshBVH(geo)
+    hit = bvh.raycastFirst(((0, 0, 1), (0, 0, -1)), pkg.DoubleSide)
+    assert hit is not None
+    assert hit.faceIndex == 0 and hit.distance == 1.0
+    assert list(hit.point) == [0.0, 0.0, 0.0]
+    assert list(hit.barycoord) == [0.0, 0.0, 0.0]
+    assert (hit.face.a, hit.face.b, hit.face.c) == (0, 1, 2)
+    assert list(hit.face.normal) == [0.0, 0.0, -1.0]
+    assert bvh.raycastFirst(((0, 0, 1), (0, 0, -1)), pkg.FrontSide) is None
+
+
+def test_sphere_distance_gpu(pkg, cuda):
+    geo = pkg.sphere(1, 200, 200)
+    bvh = pkg.MeshBVH(geo, {"verbose": False})
+    t = bvh.closestPointToPoint((0, 0, 0))
+    assert 1 - 0.001 <= t.distance <= 1
+    assert bvh.closestPointToPoint((0, 1, 0)).distance == 0
+    rng = np.random.default_rng(11)
+    for _ in range(100):
+        v = rng.uniform(-0.5, 0.5, 3)
+        length = rng.uniform(0, 3)
+        v = v / np.linalg.norm(v) * length
+        t = bvh.closestPointToPoint(v)
+        assert abs(t.distance - abs(1 - length)) <= 0.001 + 1e-6
+
+
+def test_horn_torus_hits_gpu(pkg, cuda):
+    geo = pkg.torus(5, 5, 40, 10)
+    bvh = pkg.MeshBVH(geo)
+    hits = bvh.raycast(((0, 0, -10), (0, 0, 1)))
+    assert len(hits) == 10
+    first = bvh.raycastFirst(((0, 0, -10), (0, 0, 1)))
+    assert first is not None and first.distance == min(h.distance for h in hits)
+
+
+def test_noisy_knot_incoherent_and_camera(pkg, orc, cuda):
+    geo = pkg.torus_knot(10, 3, 500, 125, noise_sigma=0.02, noise_seed=1)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = _oracle_for(orc, bvh, geo)
+    for rays in (pkg.rays_incoherent(200_000, seed=1), pkg.rays_camera(320, 320)):
+        got = bvh.raycast_first_batch(rays)
+        exp = ref.raycast_first(rays)
+        ac, ah = ref.raycast_all(rays, cap=64)
+        _assert_first_ok(check_first(got, exp, tie_exempt(ac, ah)))
+        counts, hits = bvh.raycast_batch(rays[:50_000], cap=64)
+        rep = check_all(counts, hits, ac[:50_000], ah[:50_000])
+        assert rep["count"] == 0 and rep["set"] == 0, rep
+
+
+def test_device_buffers_match_host(pkg, knot80k, cuda):
+    import torch
+
+    geo, bvh, ref = knot80k
+    rays = pkg.rays_sphere_to_box(100_000, seed=3)
+    host = bvh.raycast_first_batch(rays)
+    dev = bvh.raycast_first_batch(torch.from_numpy(rays).to(cuda))
+    bvh.synchronize()
+    got = dev.cpu().numpy().view(np.uint8).reshape(-1).view(host.dtype)
+    assert np.array_equal(got.view(np.uint8), host.view(np.uint8))
+    pts = pkg.grid_points(geo.position.min(0), geo.position.max(0), 20)
+    h2 = bvh.closest_point_batch(pts, 0.0, 5.0)
+    d2 = bvh.closest_point_batch(torch.from_numpy(pts).to(cuda), 0.0, 5.0)
+    bvh.synchronize()
+    assert np.array_equal(d2.cpu().numpy().view(np.uint8).reshape(-1), h2.view(np.uint8))

@@ -1,0 +1,79 @@
+"""ctypes binding of libbvhcuda's C ABI (include/bvhcuda.h).
+
+Loading fails loudly: there is no Python or CPU fallback for any query.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libbvhcuda.so"
+
+BVHC_OK = 0
+FRONT_SIDE, BACK_SIDE, DOUBLE_SIDE = 0, 1, 2
+CENTER, AVERAGE, SAH = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+NO_HIT = 0xFFFFFFFF
+
+
+class BvhcHit(C.Structure):
+    _fields_ = [("face_index", C.c_uint32), ("distance", C.c_float), ("point", C.c_float * 3),
+                ("barycoord", C.c_float * 3)]
+
+
+class BvhcClosest(C.Structure):
+    _fields_ = [("face_index", C.c_uint32), ("distance", C.c_float), ("point", C.c_float * 3)]
+
+
+class BvhcMeshInfo(C.Structure):
+    _fields_ = [("node_records", C.c_uint64), ("triangle_records", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("max_depth", C.c_int32), ("root_count", C.c_int32)]
+
+
+# (name, restype, argtypes) for every entry point declared in include/bvhcuda.h
+_P, _U64, _I64, _I, _F = C.c_void_p, C.c_uint64, C.c_int64, C.c_int, C.c_float
+SIGNATURES = [
+    ("bvhc_status_string", C.c_char_p, [_I]),
+    ("bvhc_build", _I, [_P, _U64, _I, _P, _I, _U64, _P, _I, _I64, _I64, _I, _I, _I, _I, C.POINTER(_P)]),
+    ("bvhc_serialized_root_count", _I, [_P]),
+    ("bvhc_serialized_root", _I, [_P, _I, C.POINTER(_P), C.POINTER(_U64)]),
+    ("bvhc_serialized_index", _I, [_P, C.POINTER(_P), C.POINTER(_I), C.POINTER(_U64)]),
+    ("bvhc_serialized_indirect", _I, [_P, C.POINTER(_P), C.POINTER(_I), C.POINTER(_U64)]),
+    ("bvhc_serialized_free", None, [_P]),
+    ("bvhc_mesh_create", _I, [_I, _I, _P, _P, _I, _P, _I, _U64, _P, _I, _U64, _P, _U64, _I, C.POINTER(_P)]),
+    ("bvhc_mesh_destroy", None, [_P]),
+    ("bvhc_mesh_get_info", _I, [_P, C.POINTER(BvhcMeshInfo)]),
+    ("bvhc_mesh_synchronize", _I, [_P, _P]),
+    ("bvhc_raycast_first", _I, [_P, _P, _U64, _I, _F, _F, _P, _I, _P]),
+    ("bvhc_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
+    ("bvhc_closest_point_to_point", _I, [_P, _P, _U64, _F, _F, _P, _I, _P]),
+]
+
+_lib = None
+
+
+class BVHCError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib().bvhc_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{where}: {msg} (status {status})")
+        self.status = status
+
+
+def lib() -> C.CDLL:
+    """Load libbvhcuda.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"libbvhcuda.so not found at {LIB_PATH}; build it with __graft_entry__.build()")
+        dll = C.CDLL(str(LIB_PATH))
+        for name, res, args in SIGNATURES:
+            fn = getattr(dll, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = dll
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != BVHC_OK:
+        raise BVHCError(status, where)

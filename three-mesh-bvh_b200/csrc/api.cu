@@ -1,0 +1,439 @@
+// C ABI of libbvhcuda: build (CPU), upload (re-layout + validation) and GPU queries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <vector>
+
+#include "bvhc_internal.h"
+#include "kernels.cuh"
+#include "layout.h"
+
+using namespace bvhc;
+
+struct bvhc_mesh {
+  int device = 0;
+  PairNode* d_nodes = nullptr;
+  TriRecord* d_tris = nullptr;
+  uint32_t* d_roots = nullptr;
+  unsigned int* d_err = nullptr;
+  uint64_t n_nodes = 0, n_tris = 0;
+  int n_roots = 0;
+  int max_depth = 0;
+  // staging buffers for BVHC_MEM_HOST calls (grow-only)
+  void* d_in = nullptr;
+  size_t in_cap = 0;
+  void* d_out = nullptr;
+  size_t out_cap = 0;
+  void* d_out2 = nullptr;
+  size_t out2_cap = 0;
+
+  MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
+};
+
+namespace {
+
+struct Status {
+  bvhc_status code;
+};
+
+bvhc_status from_cuda(cudaError_t e) {
+  if (e == cudaSuccess) return BVHC_OK;
+  if (e == cudaErrorMemoryAllocation) return BVHC_ERR_OUT_OF_MEMORY;
+  return BVHC_ERR_CUDA;
+}
+
+#define BVHC_CUDA_TRY(expr)                       \
+  do {                                            \
+    cudaError_t _e = (expr);                      \
+    if (_e != cudaSuccess) return from_cuda(_e);  \
+  } while (0)
+
+bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+uint32_t read_index(const void* p, int elem, uint64_t i) {
+  return elem == 2 ? (uint32_t) static_cast<const uint16_t*>(p)[i] : static_cast<const uint32_t*>(p)[i];
+}
+
+// Re-lays one serialized root (buildUtils.js:31-92 layout) into child-pair records and leaf-ordered
+// triangle records.  Throws Status on invalid input.
+struct Converter {
+  const uint8_t* buf = nullptr;
+  uint64_t n_nodes = 0;
+  int version = 1;
+  const void* index;
+  int index_elem;
+  uint64_t index_count;
+  const void* indirect;
+  int indirect_elem;
+  uint64_t indirect_count;
+  const float* pos;
+  uint64_t n_verts;
+  int stride;
+  uint64_t n_prims;      // valid leaf range end
+  uint64_t tri_count;    // triangles addressable through the index / positions
+  std::vector<PairNode>& pairs;
+  std::vector<TriRecord>& tris;
+  uint64_t visits = 0;
+  int max_depth = 0;
+
+  Converter(std::vector<PairNode>& p, std::vector<TriRecord>& t) : pairs(p), tris(t) {}
+
+  uint32_t u32(uint64_t node, int w) const {
+    uint32_t v;
+    std::memcpy(&v, buf + node * 32 + w * 4, 4);
+    return v;
+  }
+  uint16_t u16(uint64_t node, int h) const {
+    uint16_t v;
+    std::memcpy(&v, buf + node * 32 + h * 2, 2);
+    return v;
+  }
+  void box(uint64_t node, float* out) const { std::memcpy(out, buf + node * 32, 24); }
+  bool is_leaf(uint64_t node) const { return u16(node, 15) == 0xFFFF; }
+
+  uint64_t right_of(uint64_t node) const {
+    uint64_t v = u32(node, 6);
+    if (version == 0) {
+      // version 0 stored the absolute uint32 offset of the right child (MeshBVH.js:206-230)
+      if (v % 8 != 0) throw Status{BVHC_ERR_INVALID_BVH};
+      return v / 8;
+    }
+    return node + v;
+  }
+
+  uint32_t emit_leaf(uint64_t node) {
+    uint64_t off = u32(node, 6), cnt = u16(node, 14);
+    if (off + cnt > n_prims) throw Status{BVHC_ERR_INVALID_BVH};
+    if (cnt == 0) return kEmptyLeaf;
+    if (tris.size() + cnt >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
+    uint32_t first = (uint32_t)tris.size();
+    for (uint64_t i = off; i < off + cnt; ++i) {
+      uint64_t t = indirect ? read_index(indirect, indirect_elem, i) : i;
+      if (t >= tri_count) throw Status{BVHC_ERR_INVALID_BVH};
+      TriRecord r{};
+      for (int k = 0; k < 3; ++k) {
+        uint64_t v = index ? read_index(index, index_elem, 3 * t + k) : 3 * t + k;
+        if (v >= n_verts) throw Status{BVHC_ERR_INVALID_BVH};
+        const float* p = pos + v * (uint64_t)stride;
+        r.v[3 * k + 0] = p[0];
+        r.v[3 * k + 1] = p[1];
+        r.v[3 * k + 2] = p[2];
+      }
+      r.face = (uint32_t)t;
+      r.flags = (i + 1 == off + cnt) ? kTriLast : 0u;
+      tris.push_back(r);
+    }
+    return kLeafBit | first;
+  }
+
+  uint32_t convert(uint64_t node, int depth) {
+    if (++visits > 2 * n_nodes + 2) throw Status{BVHC_ERR_INVALID_BVH};  // shared subtrees
+    if (depth >= kMaxStack - 1) throw Status{BVHC_ERR_UNSUPPORTED};
+    max_depth = std::max(max_depth, depth);
+    if (is_leaf(node)) return emit_leaf(node);
+    uint64_t left = node + 1, right = right_of(node);
+    uint32_t axis = u32(node, 7);
+    if (left >= n_nodes || right >= n_nodes || right <= left || axis > 2) throw Status{BVHC_ERR_INVALID_BVH};
+    if (pairs.size() >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
+    uint32_t idx = (uint32_t)pairs.size();
+    pairs.push_back(PairNode{});
+    uint32_t ll = convert(left, depth + 1);
+    uint32_t lr = convert(right, depth + 1);
+    PairNode& p = pairs[idx];
+    box(left, &p.f[0]);
+    box(right, &p.f[6]);
+    p.link[0] = ll;
+    p.link[1] = lr;
+    p.axis = axis;
+    p.pad = 0;
+    return idx;
+  }
+};
+
+template <class T>
+cudaError_t upload(T** dst, const std::vector<T>& src) {
+  size_t bytes = std::max<size_t>(src.size() * sizeof(T), 16);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), bytes);
+  if (e != cudaSuccess) return e;
+  if (!src.empty()) e = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+cudaError_t ensure(void** buf, size_t* cap, size_t bytes) {
+  if (*cap >= bytes) return cudaSuccess;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(buf, bytes);
+  if (e == cudaSuccess) *cap = bytes;
+  return e;
+}
+
+bvhc_status read_and_clear_error(bvhc_mesh* m, cudaStream_t s) {
+  unsigned int h = 0;
+  BVHC_CUDA_TRY(cudaMemcpyAsync(&h, m->d_err, sizeof h, cudaMemcpyDeviceToHost, s));
+  BVHC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h != 0) {
+    BVHC_CUDA_TRY(cudaMemsetAsync(m->d_err, 0, sizeof h, s));
+    BVHC_CUDA_TRY(cudaStreamSynchronize(s));
+    return BVHC_ERR_DEVICE;
+  }
+  return BVHC_OK;
+}
+
+void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_t>& dst) {
+  dst.resize(src.size() * (size_t)elem);
+  if (elem == 4) {
+    std::memcpy(dst.data(), src.data(), dst.size());
+  } else {
+    for (size_t i = 0; i < src.size(); ++i) {
+      uint16_t v = (uint16_t)src[i];
+      std::memcpy(dst.data() + 2 * i, &v, 2);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bvhc_status_string(bvhc_status s) {
+  switch (s) {
+    case BVHC_OK: return "ok";
+    case BVHC_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BVHC_ERR_INVALID_BVH: return "invalid BVH buffer";
+    case BVHC_ERR_CUDA: return "CUDA runtime error";
+    case BVHC_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case BVHC_ERR_DEVICE: return "device-side error (traversal stack overflow)";
+    case BVHC_ERR_UNSUPPORTED: return "unsupported input (tree deeper than the traversal stack, or too large)";
+    case BVHC_ERR_BUILD: return "BVH build failed";
+  }
+  return "unknown status";
+}
+
+bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                       int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                       int64_t range_start, int64_t range_count, int strategy, int max_depth, int target_leaf_size,
+                       int indirect, bvhc_serialized** out) {
+  if (!out || !positions || stride_floats < 3 || n_verts == 0) return BVHC_ERR_INVALID_ARGUMENT;
+  if (index && index_elem_bytes != 2 && index_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
+  if (strategy < BVHC_CENTER || strategy > BVHC_SAH || max_depth < 0 || target_leaf_size < 0) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n_groups > 0 && !groups) return BVHC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  try {
+    auto* s = new bvhc_serialized();
+    if (index) {
+      s->has_index = true;
+      s->index_elem_bytes = index_elem_bytes;
+      s->index.resize(index_count);
+      for (uint64_t i = 0; i < index_count; ++i) {
+        s->index[i] = read_index(index, index_elem_bytes, i);
+        if (s->index[i] >= n_verts) { delete s; return BVHC_ERR_INVALID_ARGUMENT; }
+      }
+    }
+    try {
+      build_serialized(*s, positions, n_verts, stride_floats, groups, n_groups, range_start, range_count, strategy,
+                       max_depth, target_leaf_size, indirect != 0);
+    } catch (const std::bad_alloc&) {
+      delete s;
+      return BVHC_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+      delete s;
+      return BVHC_ERR_BUILD;
+    }
+    if (s->has_index) export_width(s->index, s->index_elem_bytes, s->index_bytes);
+    if (s->indirect) export_width(s->indirect_buf, s->indirect_elem_bytes, s->indirect_bytes);
+    *out = s;
+    return BVHC_OK;
+  } catch (const std::bad_alloc&) {
+    return BVHC_ERR_OUT_OF_MEMORY;
+  }
+}
+
+int bvhc_serialized_root_count(const bvhc_serialized* s) { return s ? (int)s->roots.size() : 0; }
+
+bvhc_status bvhc_serialized_root(const bvhc_serialized* s, int i, const void** data, uint64_t* bytes) {
+  if (!s || !data || !bytes || i < 0 || i >= (int)s->roots.size()) return BVHC_ERR_INVALID_ARGUMENT;
+  *data = s->roots[i].data();
+  *bytes = s->roots[i].size();
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_serialized_index(const bvhc_serialized* s, const void** data, int* elem_bytes, uint64_t* count) {
+  if (!s || !data || !elem_bytes || !count) return BVHC_ERR_INVALID_ARGUMENT;
+  *data = s->has_index ? s->index_bytes.data() : nullptr;
+  *elem_bytes = s->has_index ? s->index_elem_bytes : 0;
+  *count = s->has_index ? s->index.size() : 0;
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_serialized_indirect(const bvhc_serialized* s, const void** data, int* elem_bytes, uint64_t* count) {
+  if (!s || !data || !elem_bytes || !count) return BVHC_ERR_INVALID_ARGUMENT;
+  *data = s->indirect ? s->indirect_bytes.data() : nullptr;
+  *elem_bytes = s->indirect ? s->indirect_elem_bytes : 0;
+  *count = s->indirect ? s->indirect_buf.size() : 0;
+  return BVHC_OK;
+}
+
+void bvhc_serialized_free(bvhc_serialized* s) { delete s; }
+
+bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, const uint64_t* root_bytes,
+                             int n_roots, const void* index, int index_elem_bytes, uint64_t index_count,
+                             const void* indirect, int indirect_elem_bytes, uint64_t indirect_count,
+                             const float* positions, uint64_t n_verts, int stride_floats, bvhc_mesh** out) {
+  if (!out || !roots || !root_bytes || n_roots <= 0 || !positions || stride_floats < 3 || n_verts == 0)
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (version != 0 && version != 1) return BVHC_ERR_INVALID_ARGUMENT;
+  if (index && index_elem_bytes != 2 && index_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
+  if (indirect && indirect_elem_bytes != 2 && indirect_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  std::vector<PairNode> pairs;
+  std::vector<TriRecord> tris;
+  std::vector<uint32_t> root_links;
+  int max_depth = 0;
+  try {
+    for (int r = 0; r < n_roots; ++r) {
+      if (!roots[r] || root_bytes[r] == 0 || root_bytes[r] % 32 != 0) return BVHC_ERR_INVALID_BVH;
+      Converter c(pairs, tris);
+      c.buf = static_cast<const uint8_t*>(roots[r]);
+      c.n_nodes = root_bytes[r] / 32;
+      c.version = version;
+      c.index = index;
+      c.index_elem = index_elem_bytes;
+      c.index_count = index_count;
+      c.indirect = indirect;
+      c.indirect_elem = indirect_elem_bytes;
+      c.indirect_count = indirect_count;
+      c.pos = positions;
+      c.n_verts = n_verts;
+      c.stride = stride_floats;
+      c.tri_count = index ? index_count / 3 : n_verts / 3;
+      c.n_prims = indirect ? indirect_count : c.tri_count;
+      root_links.push_back(c.convert(0, 0));
+      max_depth = std::max(max_depth, c.max_depth);
+    }
+  } catch (const Status& s) {
+    return s.code;
+  } catch (const std::bad_alloc&) {
+    return BVHC_ERR_OUT_OF_MEMORY;
+  }
+  auto* m = new bvhc_mesh();
+  m->device = device;
+  m->n_nodes = pairs.size();
+  m->n_tris = tris.size();
+  m->n_roots = n_roots;
+  m->max_depth = max_depth;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = upload(&m->d_nodes, pairs);
+  if (e == cudaSuccess) e = upload(&m->d_tris, tris);
+  if (e == cudaSuccess) e = upload(&m->d_roots, root_links);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_err), sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(m->d_err, 0, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    bvhc_mesh_destroy(m);
+    return from_cuda(e);
+  }
+  *out = m;
+  return BVHC_OK;
+}
+
+void bvhc_mesh_destroy(bvhc_mesh* m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  cudaFree(m->d_nodes);
+  cudaFree(m->d_tris);
+  cudaFree(m->d_roots);
+  cudaFree(m->d_err);
+  cudaFree(m->d_in);
+  cudaFree(m->d_out);
+  cudaFree(m->d_out2);
+  delete m;
+}
+
+bvhc_status bvhc_mesh_get_info(const bvhc_mesh* m, bvhc_mesh_info* info) {
+  if (!m || !info) return BVHC_ERR_INVALID_ARGUMENT;
+  info->node_records = m->n_nodes;
+  info->triangle_records = m->n_tris;
+  info->device_bytes = m->n_nodes * sizeof(PairNode) + m->n_tris * sizeof(TriRecord) + m->n_roots * 4 + 4;
+  info->max_depth = m->max_depth;
+  info->root_count = m->n_roots;
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_mesh_synchronize(bvhc_mesh* m, void* stream) {
+  if (!m) return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  return read_and_clear_error(m, static_cast<cudaStream_t>(stream));
+}
+
+bvhc_status bvhc_raycast_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                               bvhc_hit* out, int mem, void* stream) {
+  if (!m || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!rays || !out) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_raycast_first(m->view(), rays, n, side, near_d, far_d, out, s));
+  }
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_hit)));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_raycast_first(m->view(), static_cast<const float*>(m->d_in), n, side, near_d, far_d,
+                                     static_cast<bvhc_hit*>(m->d_out), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
+bvhc_status bvhc_raycast(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                         uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem, void* stream) {
+  if (!m || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!rays || !counts || (cap > 0 && !hits)) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_raycast_all(m->view(), rays, n, side, near_d, far_d, cap, counts, hits, s));
+  }
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
+  BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, near_d, far_d, cap,
+                                   static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
+  if (cap > 0)
+    BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
+bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint64_t n, float min_threshold,
+                                        float max_threshold, bvhc_closest* out, int mem, void* stream) {
+  if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!points || !out) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(points, 4) || !aligned(out, 4)) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s));
+  }
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold, max_threshold,
+                                     static_cast<bvhc_closest*>(m->d_out), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
+}  // extern "C"

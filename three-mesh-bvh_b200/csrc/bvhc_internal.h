@@ -1,0 +1,39 @@
+// Internal declarations shared by the host-side translation units of libbvhcuda.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "bvhcuda.h"
+
+struct bvhc_serialized {
+  // MeshBVH.serialize() result (src/core/MeshBVH.js:112-145): version 1 roots, index, indirect.
+  std::vector<std::vector<uint8_t>> roots;
+  bool has_index = false;
+  int index_elem_bytes = 0;
+  std::vector<uint32_t> index;       // widened to u32; narrowed to index_elem_bytes on export
+  bool indirect = false;
+  int indirect_elem_bytes = 0;
+  std::vector<uint32_t> indirect_buf;
+  // export copies at the serialized element width
+  std::vector<uint8_t> index_bytes, indirect_bytes;
+};
+
+namespace bvhc {
+
+using Serialized = bvhc_serialized;
+
+enum { kCenter = 0, kAverage = 1, kSah = 2 };
+
+struct Range {
+  int64_t offset, count;
+};
+
+std::vector<Range> root_ranges(int64_t vertex_count, int64_t draw_start, int64_t draw_count, const int64_t* groups,
+                               int n_groups);
+
+void build_serialized(Serialized& s, const float* pos, uint64_t n_verts, int stride, const int64_t* groups,
+                      int n_groups, int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                      int leaf, bool indirect);
+
+}  // namespace bvhc

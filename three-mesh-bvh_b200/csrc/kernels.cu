@@ -1,0 +1,490 @@
+// Traversal kernels: raycastFirst, raycast (all hits) and closestPointToPoint.
+//
+// One ray or query per thread.  Each visit of an internal node reads one 64-byte child-pair
+// record (both child boxes and links) with four 16-byte read-only loads; each leaf is a
+// contiguous run of 48-byte triangle records.  The traversal stack lives in thread-local
+// memory (L1-resident), bounded by kMaxStack; the mesh upload rejects deeper trees, and an
+// overflow would set the device error word instead of faulting.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "robust.cuh"
+
+namespace bvhc {
+namespace dev {
+
+constexpr int kBlock = 128;
+constexpr float kInf = __builtin_huge_valf();
+constexpr float kSlabMargin = 9.5367431640625e-07f;  // 2^-20, relative slack on slab distances
+constexpr float kTiny = 1e-30f;                      // stand-in for a zero direction component
+
+__device__ __forceinline__ float4 ld4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+struct RayF {
+  float3 o, d, inv;
+  float d_l1;
+};
+
+__device__ __forceinline__ RayF make_ray(const float* __restrict__ rays, uint64_t i) {
+  const float2* p = reinterpret_cast<const float2*>(rays + 6 * i);
+  float2 r0 = __ldg(p), r1 = __ldg(p + 1), r2 = __ldg(p + 2);
+  RayF r;
+  r.o = make_float3(r0.x, r0.y, r1.x);
+  r.d = make_float3(r1.y, r2.x, r2.y);
+  // A zero component is replaced by +-1e-30 so that (bound - origin) * inv is never 0 * inf:
+  // the slab then becomes (-huge, +huge) or empty, which is what the reference's NaN guards in
+  // intersectsNodeBounds (intersectUtils.js:52-54,70-72) amount to.
+  float dx = fabsf(r.d.x) < kTiny ? copysignf(kTiny, r.d.x) : r.d.x;
+  float dy = fabsf(r.d.y) < kTiny ? copysignf(kTiny, r.d.y) : r.d.y;
+  float dz = fabsf(r.d.z) < kTiny ? copysignf(kTiny, r.d.z) : r.d.z;
+  r.inv = make_float3(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
+  r.d_l1 = fabsf(r.d.x) + fabsf(r.d.y) + fabsf(r.d.z);
+  return r;
+}
+
+// Conservative slab test (intersectUtils.js:2-78).  Accepts whenever the reference's float64
+// test could accept: the entry/exit distances carry at most ~3 roundings, and are widened by
+// 2^-20 relative before the comparisons.  `entry` returns the widened entry distance.
+__device__ __forceinline__ bool box_hit(float x0, float y0, float z0, float x1, float y1, float z1, const RayF& r,
+                                        float near_d, float far_d, float& entry) {
+  float tx0 = (x0 - r.o.x) * r.inv.x, tx1 = (x1 - r.o.x) * r.inv.x;
+  float ty0 = (y0 - r.o.y) * r.inv.y, ty1 = (y1 - r.o.y) * r.inv.y;
+  float tz0 = (z0 - r.o.z) * r.inv.z, tz1 = (z1 - r.o.z) * r.inv.z;
+  float en = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+  float ex = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+  en *= en > 0.0f ? 1.0f - kSlabMargin : 1.0f + kSlabMargin;
+  ex *= ex > 0.0f ? 1.0f + kSlabMargin : 1.0f - kSlabMargin;
+  entry = en;
+  return en <= ex && en <= far_d && ex >= near_d;
+}
+
+struct Tri {
+  float3 a, b, c;
+  uint32_t face, flags;
+};
+
+__device__ __forceinline__ Tri load_tri(const TriRecord* __restrict__ tris, uint32_t k) {
+  const TriRecord* t = tris + k;
+  float4 p0 = ld4(&t->v[0]), p1 = ld4(&t->v[4]), p2 = ld4(&t->v[8]);
+  Tri r;
+  r.a = make_float3(p0.x, p0.y, p0.z);
+  r.b = make_float3(p0.w, p1.x, p1.y);
+  r.c = make_float3(p1.z, p1.w, p2.x);
+  r.face = __float_as_uint(p2.y);
+  r.flags = __float_as_uint(p2.z);
+  return r;
+}
+
+struct Pair {
+  float l[6], r[6];
+  uint32_t ll, lr, axis;
+};
+
+__device__ __forceinline__ Pair load_pair(const PairNode* __restrict__ nodes, uint32_t k) {
+  const PairNode* n = nodes + k;
+  float4 q0 = ld4(&n->f[0]), q1 = ld4(&n->f[4]), q2 = ld4(&n->f[8]), q3 = ld4(&n->link[0]);
+  Pair p;
+  p.l[0] = q0.x; p.l[1] = q0.y; p.l[2] = q0.z; p.l[3] = q0.w; p.l[4] = q1.x; p.l[5] = q1.y;
+  p.r[0] = q1.z; p.r[1] = q1.w; p.r[2] = q2.x; p.r[3] = q2.y; p.r[4] = q2.z; p.r[5] = q2.w;
+  p.ll = __float_as_uint(q3.x);
+  p.lr = __float_as_uint(q3.y);
+  p.axis = __float_as_uint(q3.z);
+  return p;
+}
+
+// |d| in float-float.
+__device__ __forceinline__ ff dir_length(float3 d) {
+  ff s = ff_add(ff_add(two_prod(d.x, d.x), two_prod(d.y, d.y)), two_prod(d.z, d.z));
+  return ff_sqrt(s);
+}
+
+// Full intersection record for a triangle known to be hit, in float-float, rounded once.
+// barycoord follows Triangle.getBarycoord: (0, 0, 0) when the triangle's Gram determinant
+// |e1 x e2|^2 vanishes at float64 resolution (the reference's `denom === 0` case).
+__device__ void make_hit(const Tri& t, const RayF& r, ff tt, ff dist, bvhc_hit& h) {
+  TriFF e = tri_eval_ff(t.a, t.b, t.c, r.o, r.d);
+  ff3 px = {ff_add(ff_from(r.o.x), ff_mul_f(tt, r.d.x)), ff_add(ff_from(r.o.y), ff_mul_f(tt, r.d.y)),
+            ff_add(ff_from(r.o.z), ff_mul_f(tt, r.d.z))};
+  h.face_index = t.face;
+  h.distance = ff_to_f(dist);
+  h.point[0] = ff_to_f(px.x);
+  h.point[1] = ff_to_f(px.y);
+  h.point[2] = ff_to_f(px.z);
+  ff3 e1 = ff3_diff(t.b, t.a), e2 = ff3_diff(t.c, t.a);
+  ff3 n = ff3_cross(e1, e2);
+  ff g = ff3_dot(n, n);
+  ff l12 = ff_mul(ff3_dot(e1, e1), ff3_dot(e2, e2));
+  if (g.hi <= 8.8817841970012523e-16f * l12.hi) {  // 2^-50
+    h.barycoord[0] = h.barycoord[1] = h.barycoord[2] = 0.0f;
+  } else {
+    h.barycoord[0] = ff_to_f(ff_div(e.W, e.N));
+    h.barycoord[1] = ff_to_f(ff_div(e.U, e.N));
+    h.barycoord[2] = ff_to_f(ff_div(e.V, e.N));
+  }
+}
+
+__device__ __forceinline__ void store_hit(bvhc_hit* p, const bvhc_hit& h) {
+  float4* q = reinterpret_cast<float4*>(p);
+  q[0] = make_float4(__uint_as_float(h.face_index), h.distance, h.point[0], h.point[1]);
+  q[1] = make_float4(h.point[2], h.barycoord[0], h.barycoord[1], h.barycoord[2]);
+}
+
+__device__ __forceinline__ void store_miss(bvhc_hit* p) {
+  float4* q = reinterpret_cast<float4*>(p);
+  q[0] = make_float4(__uint_as_float(BVHC_NO_HIT), kInf, 0.0f, 0.0f);
+  q[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// raycastFirst (raycastFirst.template.js:19-103, roots loop MeshBVH.js:558-577).
+// Children are visited near-first by the sign of the ray direction on the split axis, as the
+// reference does; a child whose (widened) entry distance is beyond the best hit so far is
+// skipped, which can only drop triangles that are farther than that hit.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
+                                                               int side, float near_d, float far_d,
+                                                               bvhc_hit* __restrict__ out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RayF r = make_ray(rays, i);
+  ff dlen = dir_length(r.d);
+  ff best_t = {kInf, 0.0f};
+  uint32_t best_rec = 0xFFFFFFFFu;
+  uint32_t stack_link[kMaxStack];
+  float stack_t[kMaxStack];
+  for (int root = 0; root < m.n_roots; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) {
+          uint32_t k = link & ~kLeafBit;
+          for (;;) {
+            Tri t = load_tri(m.tris, k);
+            if (tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, side)) {
+              ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+              ff dist = ff_mul(tt, dlen);
+              bool in_range = !ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist);
+              if (in_range && ff_lt(tt, best_t)) {
+                best_t = tt;
+                best_rec = k;
+              }
+            }
+            if (t.flags & kTriLast) break;
+            ++k;
+          }
+        }
+      } else {
+        Pair p = load_pair(m.nodes, link);
+        float lim = fminf(far_d, best_t.hi * (1.0f + kSlabMargin));
+        float e0, e1;
+        bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, lim, e0);
+        bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, lim, e1);
+        float dir_axis = p.axis == 0 ? r.d.x : (p.axis == 1 ? r.d.y : r.d.z);
+        bool ltr = dir_axis >= 0.0f;
+        uint32_t c1 = ltr ? p.ll : p.lr, c2 = ltr ? p.lr : p.ll;
+        bool h1st = ltr ? h0 : h1, h2nd = ltr ? h1 : h0;
+        float t2nd = ltr ? e1 : e0;
+        if (h1st) {
+          if (h2nd) {
+            if (sp >= kMaxStack) {
+              atomicOr(m.err, kErrStackOverflow);
+              store_miss(out + i);
+              return;
+            }
+            stack_link[sp] = c2;
+            stack_t[sp] = t2nd;
+            ++sp;
+          }
+          link = c1;
+          continue;
+        }
+        if (h2nd) {
+          link = c2;
+          continue;
+        }
+      }
+      // pop, skipping entries that start beyond the best hit found since they were pushed
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+        if (stack_t[sp] <= best_t.hi * (1.0f + kSlabMargin)) {
+          link = stack_link[sp];
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+  }
+  if (best_rec == 0xFFFFFFFFu) {
+    store_miss(out + i);
+    return;
+  }
+  Tri t = load_tri(m.tris, best_rec);
+  bvhc_hit h;
+  make_hit(t, r, best_t, ff_mul(best_t, dlen), h);
+  store_hit(out + i, h);
+}
+
+// ---------------------------------------------------------------------------------------------
+// raycast, all hits (raycast.template.js:15-53): left child then right child, every hit kept
+// in DFS order.  The first `cap` hits are stored; counts[i] is the uncapped total.
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
+                                                             int side, float near_d, float far_d, uint32_t cap,
+                                                             uint32_t* __restrict__ counts,
+                                                             bvhc_hit* __restrict__ hits) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RayF r = make_ray(rays, i);
+  ff dlen = dir_length(r.d);
+  uint32_t cnt = 0;
+  uint32_t stack_link[kMaxStack];
+  bvhc_hit* out = hits + i * (uint64_t)cap;
+  for (int root = 0; root < m.n_roots; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) {
+          uint32_t k = link & ~kLeafBit;
+          for (;;) {
+            Tri t = load_tri(m.tris, k);
+            if (tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, side)) {
+              ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+              ff dist = ff_mul(tt, dlen);
+              if (!ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist)) {
+                if (cnt < cap) {
+                  bvhc_hit h;
+                  make_hit(t, r, tt, dist, h);
+                  store_hit(out + cnt, h);
+                }
+                ++cnt;
+              }
+            }
+            if (t.flags & kTriLast) break;
+            ++k;
+          }
+        }
+      } else {
+        Pair p = load_pair(m.nodes, link);
+        float e0, e1;
+        bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e0);
+        bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e1);
+        if (h0) {
+          if (h1) {
+            if (sp >= kMaxStack) {
+              atomicOr(m.err, kErrStackOverflow);
+              counts[i] = cnt;
+              return;
+            }
+            stack_link[sp++] = p.lr;
+          }
+          link = p.ll;
+          continue;
+        }
+        if (h1) {
+          link = p.lr;
+          continue;
+        }
+      }
+      if (sp == 0) break;
+      link = stack_link[--sp];
+    }
+  }
+  counts[i] = cnt;
+}
+
+// ---------------------------------------------------------------------------------------------
+// closestPointToPoint (closestPointToPoint.js:6-78 through shapecast.js:41-214).
+// At an internal node both child scores (squared distance from the point to the box) are
+// computed; the lower-scoring child is visited first (left on ties), and a child is entered
+// only if its score is below maxThreshold^2 (decided exactly) and not certainly above the best
+// squared distance found so far.  No per-triangle maxThreshold test is made, as in the
+// reference.  Candidate distances are compared in float32 with an error bound and re-compared
+// in float-float when the bound does not separate them.
+// ---------------------------------------------------------------------------------------------
+constexpr float kU = 5.9604644775390625e-08f;  // 2^-24
+
+__device__ __forceinline__ float box_score(const float* b, float3 p) {
+  float dx = fmaxf(b[0], fminf(b[3], p.x)) - p.x;
+  float dy = fmaxf(b[1], fminf(b[4], p.y)) - p.y;
+  float dz = fmaxf(b[2], fminf(b[5], p.z)) - p.z;
+  return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __noinline__ ff box_score_ff(const float* b, float3 p) {
+  ff dx = two_diff(fmaxf(b[0], fminf(b[3], p.x)), p.x);
+  ff dy = two_diff(fmaxf(b[1], fminf(b[4], p.y)), p.y);
+  ff dz = two_diff(fmaxf(b[2], fminf(b[5], p.z)), p.z);
+  return ff_add(ff_add(ff_mul(dx, dx), ff_mul(dy, dy)), ff_mul(dz, dz));
+}
+
+// score < maxThreshold^2, decided exactly (the box score carries at most 5 roundings, all terms
+// positive, so 2^-20 relative slack separates every case the float32 value can settle).
+__device__ __forceinline__ bool under_max(float s, const float* b, float3 p, ff max2) {
+  if (s * (1.0f + kSlabMargin) < max2.hi * (1.0f - kSlabMargin)) return true;
+  if (s * (1.0f - kSlabMargin) > max2.hi * (1.0f + kSlabMargin)) return false;
+  return ff_lt(box_score_ff(b, p), max2);
+}
+
+__global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const float* __restrict__ pts, uint64_t n,
+                                                               float min_t, float max_t,
+                                                               bvhc_closest* __restrict__ out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float3 p = make_float3(__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2));
+  ff max2 = two_prod(max_t, max_t);
+  ff min2 = two_prod(min_t, min_t);
+  float best_d2 = kInf, best_err = 0.0f;
+  uint32_t best_rec = 0xFFFFFFFFu;
+  float3 best_q = make_float3(0.f, 0.f, 0.f);
+  bool best_vertex = false;  // best_q is an input vertex, bit-exact
+  bool best_ff_ok = false;
+  ff best_ff = {kInf, 0.0f};
+  bool stop = false;
+  uint32_t stack_link[kMaxStack];
+  float stack_s[kMaxStack];
+  for (int root = 0; root < m.n_roots && !stop; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) {
+          uint32_t k = link & ~kLeafBit;
+          for (;;) {
+            Tri t = load_tri(m.tris, k);
+            float3 q;
+            float sc;
+            float d2 = closest_sq_f(p, t.a, t.b, t.c, q, sc);
+            // |error| of each closest-point coordinate <= e (local-frame evaluation)
+            float e = 32.0f * kU * sc;
+            float err = 3.5f * e * sqrtf(d2) + 3.0f * e * e;
+            bool is_vertex = (q.x == t.a.x && q.y == t.a.y && q.z == t.a.z) ||
+                             (q.x == t.b.x && q.y == t.b.y && q.z == t.b.z) ||
+                             (q.x == t.c.x && q.y == t.c.y && q.z == t.c.z);
+            bool take;
+            bool have_ff = false;
+            ff cand_ff;
+            if (best_rec == 0xFFFFFFFFu) {
+              take = d2 < kInf;  // the first finite candidate (distSq < Infinity)
+            } else if (d2 + err < best_d2 - best_err) {
+              take = true;
+            } else if (d2 - err > best_d2 + best_err) {
+              take = false;
+            } else if (is_vertex && best_vertex && q.x == best_q.x && q.y == best_q.y && q.z == best_q.z) {
+              take = false;  // the same vertex: an exact tie, the first one found stays
+            } else {
+              if (!best_ff_ok) {
+                Tri bt = load_tri(m.tris, best_rec);
+                best_ff = closest_ff(p, bt.a, bt.b, bt.c).d2;
+                best_ff_ok = true;
+              }
+              cand_ff = closest_ff(p, t.a, t.b, t.c).d2;
+              have_ff = true;
+              take = ff_lt(cand_ff, best_ff);
+            }
+            if (take) {
+              best_d2 = d2;
+              best_err = err;
+              best_rec = k;
+              best_q = q;
+              best_vertex = is_vertex;
+              best_ff_ok = have_ff;
+              best_ff = cand_ff;
+            }
+            // early out below minThreshold (closestPointToPoint.js:55-57)
+            if (min2.hi > 0.0f) {
+              bool below;
+              if (d2 + err < min2.hi * (1.0f - kSlabMargin)) below = true;
+              else if (d2 - err > min2.hi * (1.0f + kSlabMargin)) below = false;
+              else below = ff_lt(have_ff ? cand_ff : closest_ff(p, t.a, t.b, t.c).d2, min2);
+              if (below) { stop = true; break; }
+            }
+            if (t.flags & kTriLast) break;
+            ++k;
+          }
+          if (stop) break;
+        }
+      } else {
+        Pair pr = load_pair(m.nodes, link);
+        float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
+        bool swap = s1 < s0;
+        const float* b1 = swap ? pr.r : pr.l;
+        const float* b2 = swap ? pr.l : pr.r;
+        float sc1 = swap ? s1 : s0, sc2 = swap ? s0 : s1;
+        uint32_t c1 = swap ? pr.lr : pr.ll, c2 = swap ? pr.ll : pr.lr;
+        float best_hi = best_d2 + best_err;
+        if (under_max(sc2, b2, p, max2)) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            stop = true;
+            break;
+          }
+          stack_link[sp] = c2;
+          stack_s[sp] = sc2;
+          ++sp;
+        }
+        if (sc1 * (1.0f - kSlabMargin) <= best_hi && under_max(sc1, b1, p, max2)) {
+          link = c1;
+          continue;
+        }
+      }
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+        if (stack_s[sp] * (1.0f - kSlabMargin) <= best_d2 + best_err) {
+          link = stack_link[sp];
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+  }
+  bvhc_closest* o = out + i;
+  if (best_rec == 0xFFFFFFFFu) {
+    o->face_index = BVHC_NO_HIT;
+    o->distance = kInf;
+    o->point[0] = o->point[1] = o->point[2] = 0.0f;
+    return;
+  }
+  Tri t = load_tri(m.tris, best_rec);
+  CPFF c = closest_ff(p, t.a, t.b, t.c);
+  o->face_index = t.face;
+  o->distance = ff_to_f(ff_sqrt(c.d2));
+  o->point[0] = ff_to_f(c.q.x);
+  o->point[1] = ff_to_f(c.q.y);
+  o->point[2] = ff_to_f(c.q.z);
+}
+
+}  // namespace dev
+
+static unsigned int grid_for(uint64_t n) { return (unsigned int)((n + dev::kBlock - 1) / dev::kBlock); }
+
+cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                                 bvhc_hit* out, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, near_d, far_d, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                               uint32_t cap, uint32_t* counts, bvhc_hit* hits, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, near_d, far_d, cap, counts, hits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
+                                 bvhc_closest* out, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
+  return cudaGetLastError();
+}
+
+}  // namespace bvhc

@@ -1,0 +1,308 @@
+"""`MeshBVH` — the reference's query interface, answered by the GPU engine.
+
+Mirrors src/core/MeshBVH.js (three-mesh-bvh 0.9.14): the constructor builds a BVH over a
+`Geometry` (reordering its index in place, as the reference does), `serialize` / `deserialize`
+move the packed roots in and out, and `raycastFirst`, `raycast` and `closestPointToPoint` keep
+the reference's argument meaning, defaults and null / empty results.  Every query runs on the
+GPU through libbvhcuda; the batched forms (`raycast_first_batch`, ...) are the engine's
+purpose and take whole arrays of rays or points, as numpy arrays (host) or torch CUDA tensors
+(device-resident, enqueued on the current stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .geometry import Geometry
+
+FrontSide, BackSide, DoubleSide = N.FRONT_SIDE, N.BACK_SIDE, N.DOUBLE_SIDE
+CENTER, AVERAGE, SAH = N.CENTER, N.AVERAGE, N.SAH
+DEFAULT_OPTIONS = dict(strategy=CENTER, maxDepth=40, targetLeafSize=10, indirect=False, range=None,
+                       setBoundingBox=True, verbose=True)   # Constants.js:74-85
+
+HIT_DTYPE = np.dtype([("face_index", "<u4"), ("distance", "<f4"), ("point", "<f4", 3), ("barycoord", "<f4", 3)])
+CLOSEST_DTYPE = np.dtype([("face_index", "<u4"), ("distance", "<f4"), ("point", "<f4", 3)])
+assert HIT_DTYPE.itemsize == 32 and CLOSEST_DTYPE.itemsize == 20
+
+
+@dataclass
+class Face:
+    a: int
+    b: int
+    c: int
+    normal: np.ndarray
+    materialIndex: int = 0
+
+
+@dataclass
+class Intersection:
+    distance: float
+    point: np.ndarray
+    face: Face
+    faceIndex: int
+    barycoord: np.ndarray
+
+
+@dataclass
+class HitPointInfo:
+    point: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    distance: float = 0.0
+    faceIndex: int = -1
+
+
+def _side_of(material_or_side) -> int:
+    """getSide (ThreeRayIntersectUtilities.js:147-151): a material's `side`, or the side itself."""
+    side = getattr(material_or_side, "side", material_or_side)
+    if side not in (FrontSide, BackSide, DoubleSide):
+        raise ValueError(f"unsupported side {material_or_side!r}")
+    return int(side)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class MeshBVH:
+    """GPU-backed MeshBVH (src/core/MeshBVH.js:80-886)."""
+
+    def __init__(self, geometry: Geometry, options: dict | None = None, *, device: int = 0, _skip_build=False):
+        opts = dict(DEFAULT_OPTIONS)
+        opts.update(options or {})
+        if "maxLeafSize" in opts:       # BVH.js:76-84 deprecated alias
+            opts["targetLeafSize"] = opts.pop("maxLeafSize")
+        if "maxLeafTris" in opts:       # MeshBVH.js:262-270 deprecated alias
+            opts["targetLeafSize"] = opts.pop("maxLeafTris")
+        self.geometry = geometry
+        self.device = device
+        self._roots: list[bytes] = []
+        self._indirectBuffer: np.ndarray | None = None
+        self._mesh = None
+        if not _skip_build:
+            self._build(opts)
+
+    # -- build -----------------------------------------------------------------------------
+    def _build(self, opts):
+        lib = N.lib()
+        g = self.geometry
+        pos = np.ascontiguousarray(g.position, dtype=np.float32)
+        idx = g.index
+        rng = opts.get("range")
+        start, count = (rng if rng is not None else g.draw_range)
+        count = -1 if count is None or (isinstance(count, float) and math.isinf(count)) else int(count)
+        groups = np.array([[s, -1 if (isinstance(c, float) and math.isinf(c)) else int(c)] for s, c, *_ in g.groups],
+                          dtype=np.int64).reshape(-1)
+        out = C.c_void_p()
+        st = lib.bvhc_build(_ptr(pos), pos.shape[0], 3, _ptr(idx) if idx is not None else None,
+                            idx.dtype.itemsize if idx is not None else 0, idx.size if idx is not None else 0,
+                            _ptr(groups) if groups.size else None, len(g.groups), int(start), count,
+                            int(opts["strategy"]), int(opts["maxDepth"]), int(opts["targetLeafSize"]),
+                            1 if opts.get("indirect") else 0, C.byref(out))
+        N.check(st, "bvhc_build")
+        try:
+            self._adopt_serialized(out)
+        finally:
+            lib.bvhc_serialized_free(out)
+
+    def _adopt_serialized(self, s):
+        lib = N.lib()
+        roots = []
+        for i in range(lib.bvhc_serialized_root_count(s)):
+            p, n = C.c_void_p(), C.c_uint64()
+            N.check(lib.bvhc_serialized_root(s, i, C.byref(p), C.byref(n)), "bvhc_serialized_root")
+            roots.append(C.string_at(p, n.value))
+        self._roots = roots
+        p, eb, n = C.c_void_p(), C.c_int(), C.c_uint64()
+        N.check(lib.bvhc_serialized_index(s, C.byref(p), C.byref(eb), C.byref(n)), "bvhc_serialized_index")
+        if eb.value:
+            dt = np.uint16 if eb.value == 2 else np.uint32
+            self.geometry.index = np.frombuffer(C.string_at(p, n.value * eb.value), dtype=dt).copy()
+        N.check(lib.bvhc_serialized_indirect(s, C.byref(p), C.byref(eb), C.byref(n)), "bvhc_serialized_indirect")
+        if eb.value:
+            dt = np.uint16 if eb.value == 2 else np.uint32
+            self._indirectBuffer = np.frombuffer(C.string_at(p, n.value * eb.value), dtype=dt).copy()
+
+    @property
+    def indirect(self) -> bool:
+        return self._indirectBuffer is not None
+
+    def resolveTriangleIndex(self, i: int) -> int:
+        return int(self._indirectBuffer[i]) if self.indirect else int(i)
+
+    # -- serialize / deserialize (MeshBVH.js:112-232) --------------------------------------
+    @staticmethod
+    def serialize(bvh: "MeshBVH", options: dict | None = None) -> dict:
+        clone = (options or {}).get("cloneBuffers", True)
+        idx = bvh.geometry.index
+        return {
+            "version": 1,
+            "roots": [bytes(r) for r in bvh._roots] if clone else bvh._roots,
+            "index": (idx.copy() if clone else idx) if idx is not None else None,
+            "indirectBuffer": (bvh._indirectBuffer.copy() if clone else bvh._indirectBuffer)
+            if bvh._indirectBuffer is not None else None,
+        }
+
+    @staticmethod
+    def deserialize(data: dict, geometry: Geometry, options: dict | None = None, *, device: int = 0) -> "MeshBVH":
+        opts = {"setIndex": True, **(options or {})}
+        bvh = MeshBVH(geometry, device=device, _skip_build=True)
+        bvh._version = int(data.get("version", 0) or 0)
+        bvh._roots = [bytes(r) for r in data["roots"]]
+        ind = data.get("indirectBuffer")
+        bvh._indirectBuffer = None if ind is None else np.asarray(ind)
+        if opts["setIndex"] and data.get("index") is not None:
+            if geometry.index is None:
+                geometry.index = np.asarray(data["index"])
+            elif geometry.index is not data["index"]:
+                geometry.index[:] = data["index"]
+        return bvh
+
+    # -- device mesh -----------------------------------------------------------------------
+    def _device_mesh(self):
+        if self._mesh is None:
+            lib = N.lib()
+            g = self.geometry
+            pos = np.ascontiguousarray(g.position, dtype=np.float32)
+            idx = g.index
+            ind = self._indirectBuffer
+            bufs = [np.frombuffer(r, dtype=np.uint8) for r in self._roots]
+            ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+            sizes = (C.c_uint64 * len(bufs))(*[b.size for b in bufs])
+            out = C.c_void_p()
+            st = lib.bvhc_mesh_create(self.device, getattr(self, "_version", 1), ptrs, sizes, len(bufs),
+                                      _ptr(idx) if idx is not None else None,
+                                      idx.dtype.itemsize if idx is not None else 0,
+                                      idx.size if idx is not None else 0,
+                                      _ptr(ind) if ind is not None else None,
+                                      ind.dtype.itemsize if ind is not None else 0,
+                                      ind.size if ind is not None else 0, _ptr(pos), pos.shape[0], 3, C.byref(out))
+            N.check(st, "bvhc_mesh_create")
+            self._mesh = out
+        return self._mesh
+
+    def mesh_info(self) -> dict:
+        info = N.BvhcMeshInfo()
+        N.check(N.lib().bvhc_mesh_get_info(self._device_mesh(), C.byref(info)), "bvhc_mesh_get_info")
+        return {k: getattr(info, k) for k, _ in N.BvhcMeshInfo._fields_}
+
+    def dispose(self):
+        if self._mesh is not None:
+            N.lib().bvhc_mesh_destroy(self._mesh)
+            self._mesh = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+    # -- batched queries -------------------------------------------------------------------
+    @staticmethod
+    def _is_torch(x):
+        return type(x).__module__.startswith("torch")
+
+    def raycast_first_batch(self, rays, side=FrontSide, near=0.0, far=math.inf, out=None, stream=None):
+        """raycastFirst for every row of `rays` (n x 6 float32).  numpy in -> numpy HIT_DTYPE out;
+        torch CUDA tensor in -> (n, 8) float32 tensor whose rows are bvhc_hit records."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(rays):
+            import torch
+            n = rays.shape[0]
+            if out is None:
+                out = torch.empty((n, 8), dtype=torch.float32, device=rays.device)
+            s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+            N.check(lib.bvhc_raycast_first(mesh, rays.data_ptr(), n, _side_of(side), float(near), float(far),
+                                           out.data_ptr(), N.MEM_DEVICE, s), "bvhc_raycast_first")
+            return out
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        res = np.empty(rays.shape[0], dtype=HIT_DTYPE) if out is None else out
+        N.check(lib.bvhc_raycast_first(mesh, _ptr(rays), rays.shape[0], _side_of(side), float(near), float(far),
+                                       _ptr(res), N.MEM_HOST, None), "bvhc_raycast_first")
+        return res
+
+    def raycast_batch(self, rays, side=FrontSide, near=0.0, far=math.inf, cap=64, stream=None):
+        """All hits for every ray: (counts[n] uncapped, hits[n, cap]) in the reference's DFS order."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(rays):
+            import torch
+            n = rays.shape[0]
+            counts = torch.empty(n, dtype=torch.int32, device=rays.device)
+            hits = torch.empty((n, cap, 8), dtype=torch.float32, device=rays.device)
+            s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+            N.check(lib.bvhc_raycast(mesh, rays.data_ptr(), n, _side_of(side), float(near), float(far), cap,
+                                     counts.data_ptr(), hits.data_ptr(), N.MEM_DEVICE, s), "bvhc_raycast")
+            return counts, hits
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        counts = np.empty(n, dtype=np.uint32)
+        hits = np.empty((n, cap), dtype=HIT_DTYPE)
+        N.check(lib.bvhc_raycast(mesh, _ptr(rays), n, _side_of(side), float(near), float(far), cap, _ptr(counts),
+                                 _ptr(hits), N.MEM_HOST, None), "bvhc_raycast")
+        return counts, hits
+
+    def closest_point_batch(self, points, min_threshold=0.0, max_threshold=math.inf, stream=None):
+        """closestPointToPoint for every row of `points` (n x 3 float32)."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(points):
+            import torch
+            n = points.shape[0]
+            out = torch.empty((n, 5), dtype=torch.float32, device=points.device)
+            s = stream if stream is not None else torch.cuda.current_stream(points.device).cuda_stream
+            N.check(lib.bvhc_closest_point_to_point(mesh, points.data_ptr(), n, float(min_threshold),
+                                                    float(max_threshold), out.data_ptr(), N.MEM_DEVICE, s),
+                    "bvhc_closest_point_to_point")
+            return out
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        res = np.empty(pts.shape[0], dtype=CLOSEST_DTYPE)
+        N.check(lib.bvhc_closest_point_to_point(mesh, _ptr(pts), pts.shape[0], float(min_threshold),
+                                                float(max_threshold), _ptr(res), N.MEM_HOST, None),
+                "bvhc_closest_point_to_point")
+        return res
+
+    def synchronize(self, stream=None):
+        N.check(N.lib().bvhc_mesh_synchronize(self._device_mesh(), stream), "bvhc_mesh_synchronize")
+
+    # -- reference-shaped single queries (MeshBVH.js:532-577, 874-884) ---------------------
+    def _intersection(self, rec) -> Intersection:
+        f = int(rec["face_index"])
+        tri = self.geometry.triangle(f)
+        base = 3 * f
+        if self.geometry.index is not None:
+            a, b, c = (int(v) for v in self.geometry.index[base:base + 3])
+        else:
+            a, b, c = base, base + 1, base + 2
+        n = np.cross(tri[2] - tri[1], tri[0] - tri[1])       # Triangle.getNormal
+        ln = float(np.dot(n, n))
+        n = n / math.sqrt(ln) if ln > 0 else np.zeros(3)
+        return Intersection(distance=float(rec["distance"]), point=np.array(rec["point"], dtype=np.float64),
+                            face=Face(a, b, c, n, 0), faceIndex=f,
+                            barycoord=np.array(rec["barycoord"], dtype=np.float64))
+
+    @staticmethod
+    def _ray_row(ray) -> np.ndarray:
+        o, d = ray
+        return np.array([[*o, *d]], dtype=np.float32)
+
+    def raycastFirst(self, ray, materialOrSide=FrontSide, near=0.0, far=math.inf):
+        """`ray` is (origin, direction).  Returns an Intersection or None."""
+        rec = self.raycast_first_batch(self._ray_row(ray), materialOrSide, near, far)[0]
+        return None if int(rec["face_index"]) == N.NO_HIT else self._intersection(rec)
+
+    def raycast(self, ray, materialOrSide=FrontSide, near=0.0, far=math.inf, cap=1024):
+        """All hits of one ray, unsorted (DFS order), as a list of Intersection."""
+        counts, hits = self.raycast_batch(self._ray_row(ray), materialOrSide, near, far, cap=cap)
+        return [self._intersection(hits[0, k]) for k in range(min(int(counts[0]), cap))]
+
+    def closestPointToPoint(self, point, target: HitPointInfo | None = None, minThreshold=0.0,
+                            maxThreshold=math.inf):
+        rec = self.closest_point_batch(np.array([point], dtype=np.float32), minThreshold, maxThreshold)[0]
+        if int(rec["face_index"]) == N.NO_HIT:
+            return None
+        target = target if target is not None else HitPointInfo()
+        target.point = np.array(rec["point"], dtype=np.float64)
+        target.distance = float(rec["distance"])
+        target.faceIndex = int(rec["face_index"])
+        return target
