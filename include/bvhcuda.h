@@ -140,6 +140,24 @@ bvhc_status bvhc_raycast_first(bvhc_mesh* mesh, const float* rays, uint64_t n, i
 bvhc_status bvhc_raycast(bvhc_mesh* mesh, const float* rays, uint64_t n, int side, float near_dist, float far_dist,
                          uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem, void* stream);
 
+/* Labels every triangle with the materialIndex of the geometry group that holds it, for the
+ * material-array raycasts below.  groups: n_groups (start, count, materialIndex) triplets in index
+ * units, count < 0 meaning Infinity (BufferGeometry.groups).  A triangle in no group is never hit
+ * by a material-array raycast (the reference tests it against no material); a triangle in two or
+ * more groups is rejected with BVHC_ERR_UNSUPPORTED. */
+bvhc_status bvhc_mesh_set_groups(bvhc_mesh* mesh, const int64_t* groups, int n_groups);
+
+/* raycastFirst / raycast with an array of materials as `materialOrSide`
+ * (src/utils/ThreeRayIntersectUtilities.js:170-205): material_sides[m] (host memory, at most 64
+ * entries) is the side of material m; each triangle is tested with its group material's side, and
+ * with FrontSide when its material index is past the array. */
+bvhc_status bvhc_raycast_first_materials(bvhc_mesh* mesh, const float* rays, uint64_t n, const int8_t* material_sides,
+                                         int n_materials, float near_dist, float far_dist, bvhc_hit* out, int mem,
+                                         void* stream);
+bvhc_status bvhc_raycast_materials(bvhc_mesh* mesh, const float* rays, uint64_t n, const int8_t* material_sides,
+                                   int n_materials, float near_dist, float far_dist, uint32_t cap, uint32_t* counts,
+                                   bvhc_hit* hits, int mem, void* stream);
+
 /* MeshBVH#closestPointToPoint(point, target, minThreshold, maxThreshold) for every point
  * (src/core/MeshBVH.js:874-884, src/core/cast/closestPointToPoint.js:6-78). */
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* mesh, const float* points, uint64_t n, float min_threshold,

@@ -75,6 +75,10 @@ struct Bvh {
   int indirect_elem_bytes = 0;
   std::vector<uint32_t> indirect_buf;
   std::vector<std::vector<uint8_t>> roots;
+  // material-array queries: geometry groups (start, count, materialIndex) in index units and one
+  // side per material; empty `sides` means a single side for every triangle
+  std::vector<int64_t> groups;
+  std::vector<int> sides;
 
   int64_t vertex_count() const { return has_index ? (int64_t)index.size() : n_verts; }  // geometryUtils.js:3-7
   V3 vertex(int64_t v) const {
@@ -536,6 +540,7 @@ struct orc_hit {
   double barycoord[3];
   double normal[3];
   int64_t face[3];        // face.a, face.b, face.c
+  int64_t material_index; // face.materialIndex
 };
 
 struct orc_cp {
@@ -571,7 +576,34 @@ bool intersect_tri(const Bvh& g, int side, const Ray& ray, int64_t tri, double n
   V3 n = face_normal(a, b, c);
   out->normal[0] = n.x; out->normal[1] = n.y; out->normal[2] = n.z;
   out->face[0] = abc[0]; out->face[1] = abc[1]; out->face[2] = abc[2];
+  out->material_index = 0;
   return true;
+}
+
+// intersectTri with an array of materials (ThreeRayIntersectUtilities.js:170-205): one test per
+// group that contains the triangle, with that group's material side (a missing material reads as
+// `undefined`, which tests like FrontSide); all-hits mode keeps every group's hit, first-hit mode
+// the first.  Without materials this is the single-side test.
+template <class Sink>
+bool intersect_tri_groups(const Bvh& g, int side, const Ray& ray, int64_t tri, double near, double far, Sink sink) {
+  if (g.sides.empty()) {
+    orc_hit h;
+    if (!intersect_tri(g, side, ray, tri, near, far, &h)) return false;
+    return sink(h);
+  }
+  int64_t first = tri * 3;
+  for (size_t k = 0; k + 2 < g.groups.size(); k += 3) {
+    int64_t start = g.groups[k], count = g.groups[k + 1], mat = g.groups[k + 2];
+    if (first >= start && (count < 0 || first < start + count)) {
+      int s = (mat >= 0 && mat < (int64_t)g.sides.size()) ? g.sides[(size_t)mat] : FRONT_SIDE;
+      orc_hit h;
+      if (intersect_tri(g, s, ray, tri, near, far, &h)) {
+        h.material_index = mat;
+        if (sink(h)) return true;
+      }
+    }
+  }
+  return false;
 }
 
 // intersectsNodeBounds (intersectUtils.js:2-78)
@@ -609,7 +641,11 @@ bool raycast_first_rec(const Bvh& g, const NodeView& nv, int64_t n32, int side, 
     for (int64_t i = offset; i < offset + count; ++i) {
       orc_hit h;
       ctr.tris++;
-      if (intersect_tri(g, side, ray, g.resolve(i), near, far, &h) && h.distance < dist) {
+      bool hit = intersect_tri_groups(g, side, ray, g.resolve(i), near, far, [&](const orc_hit& x) {
+        h = x;
+        return true;  // intersectTri returns the first group's hit
+      });
+      if (hit && h.distance < dist) {
         *res = h;
         dist = h.distance;
         found = true;
@@ -659,9 +695,11 @@ void raycast_all_rec(const Bvh& g, const NodeView& nv, int64_t n32, int side, co
   if (nv.is_leaf(n32)) {
     int64_t offset = nv.offset(n32), count = nv.count(n32);
     for (int64_t i = offset; i < offset + count; ++i) {
-      orc_hit h;
       ctr.tris++;
-      if (intersect_tri(g, side, ray, g.resolve(i), near, far, &h)) hits.push_back(h);
+      intersect_tri_groups(g, side, ray, g.resolve(i), near, far, [&](const orc_hit& x) {
+        hits.push_back(x);
+        return false;  // all-hits mode keeps every group's hit
+      });
     }
     return;
   }
@@ -829,6 +867,13 @@ orc_bvh* orc_from_serialized(const void* const* roots, const int64_t* root_bytes
 }
 
 void orc_free(orc_bvh* h) { delete h; }
+
+// Material-array mode for raycast queries: `groups` holds (start, count, materialIndex) triplets in
+// index units (count < 0 = Infinity) and `sides` one side per material; n_sides = 0 turns it off.
+void orc_set_materials(orc_bvh* h, const int64_t* groups, int n_groups, const int* sides, int n_sides) {
+  h->b.groups.assign(groups, groups + 3 * n_groups);
+  h->b.sides.assign(sides, sides + n_sides);
+}
 int orc_num_roots(const orc_bvh* h) { return (int)h->b.roots.size(); }
 int64_t orc_root_bytes(const orc_bvh* h, int i) { return (int64_t)h->b.roots[i].size(); }
 void orc_copy_root(const orc_bvh* h, int i, void* dst) { std::memcpy(dst, h->b.roots[i].data(), h->b.roots[i].size()); }
@@ -909,11 +954,11 @@ void orc_brute_raycast_all(const orc_bvh* h, const float* rays, int64_t n, int s
       int32_t cnt = 0;
       for (const Range& r : ranges)
         for (int64_t t = r.offset; t < r.offset + r.count; ++t) {
-          orc_hit hh;
-          if (intersect_tri(h->b, side, ray, h->b.resolve(t), near, far, &hh)) {
+          intersect_tri_groups(h->b, side, ray, h->b.resolve(t), near, far, [&](const orc_hit& hh) {
             if (cnt < cap) hits[i * cap + cnt] = hh;
             ++cnt;
-          }
+            return false;
+          });
         }
       counts[i] = cnt;
     }

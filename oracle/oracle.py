@@ -16,7 +16,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
 
 HIT_DTYPE = np.dtype([("face_index", "<i8"), ("distance", "<f8"), ("point", "<f8", 3), ("barycoord", "<f8", 3),
-                      ("normal", "<f8", 3), ("face", "<i8", 3)])
+                      ("normal", "<f8", 3), ("face", "<i8", 3), ("material_index", "<i8")])
 CP_DTYPE = np.dtype([("face_index", "<i8"), ("distance", "<f8"), ("point", "<f8", 3)])
 
 _lib = None
@@ -61,6 +61,7 @@ def lib():
         L.orc_ray_triangle.argtypes = [P, P, P, P, P, I, D, D, P]
         L.orc_closest_point_triangle.argtypes = [P, P, P, P, P]
         L.orc_stats.argtypes = [P, P]
+        L.orc_set_materials.argtypes = [P, P, I, P, I]
         _lib = L
     return _lib
 
@@ -114,6 +115,14 @@ class OracleBVH:
         obj = cls(h)
         obj._keep = (bufs, idx, ind, pos)
         return obj
+
+    def set_materials(self, groups, sides):
+        """Material-array raycasts: groups [(start, count, materialIndex)], one side per material."""
+        g = np.array([[s, -1 if (isinstance(c, float) and math.isinf(c)) else c, m] for s, c, m in groups],
+                     dtype=np.int64).reshape(-1)
+        sd = np.asarray(sides, dtype=np.int32)
+        self._mat = (g, sd)
+        lib().orc_set_materials(self.h, _p(g) if g.size else None, len(groups), _p(sd) if sd.size else None, sd.size)
 
     def roots(self):
         L = lib()

@@ -172,3 +172,40 @@ def test_device_buffers_match_host(pkg, knot80k, cuda):
     d2 = bvh.closest_point_batch(torch.from_numpy(pts).to(cuda), 0.0, 5.0)
     bvh.synchronize()
     assert np.array_equal(d2.cpu().numpy().view(np.uint8).reshape(-1), h2.view(np.uint8))
+
+
+def test_box_group_sides_gpu(pkg, cuda):
+    """ShapeCasts.test.js:931-979 on the GPU: material-array raycast and raycastFirst."""
+    geo = pkg.box()
+    bvh = pkg.MeshBVH(geo)
+    ray = ((0, 0.25, -10), (0, 0, 1))
+    hits = bvh.raycast(ray, [1, 0, 1, 0, 1, 0])
+    assert len(hits) == 2
+    first = bvh.raycastFirst(ray, [0, 0, 0, 0, 1, 1])
+    assert first is not None and first.point[2] == 0.5 and first.face.materialIndex == 4
+    gap = pkg.box()
+    gap.groups = []
+    gap.add_group(0, 6, 0)
+    gap.add_group(12, 24, 1)
+    bvh2 = pkg.MeshBVH(gap)
+    assert bvh2.raycast(((-2, 0, 0), (1, 0, 0))) == []
+
+
+def test_material_array_random_parity(pkg, orc, cuda):
+    geo = pkg.torus_knot(10, 3, 120, 24)
+    n = geo.index.size
+    step = (n // 3 // 7) * 3
+    for g in range(7):
+        geo.add_group(g * step, step if g < 6 else math.inf, g % 4)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = _oracle_for(orc, bvh, geo)
+    sides = [0, 1, 2]                  # material 3 is past the array: FrontSide
+    ref.set_materials(geo.groups, sides)
+    rays = pkg.rays_sphere_to_box(20_000, seed=9)
+    got = bvh.raycast_first_batch(rays, sides)
+    exp = ref.raycast_first(rays)
+    ac, ah = ref.raycast_all(rays, cap=64)
+    _assert_first_ok(check_first(got, exp, tie_exempt(ac, ah)))
+    counts, hits = bvh.raycast_batch(rays, sides, cap=64)
+    rep = check_all(counts, hits, ac, ah)
+    assert rep["count"] == 0 and rep["set"] == 0, rep

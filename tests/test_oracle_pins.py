@@ -125,3 +125,28 @@ def test_closest_point_equals_brute_force(pkg, orc):
     for i in range(0, pts.shape[0], 37):
         best = min(np.sum((orc.closest_point_triangle(pts[i], *t) - pts[i]) ** 2) for t in tri)
         assert res["distance"][i] == pytest.approx(math.sqrt(best), rel=1e-12, abs=1e-12)
+
+
+def test_box_group_sides_known_answer(pkg, orc):
+    """ShapeCasts.test.js:931-979: a unit box, one group per face, per-group material sides."""
+    geo = pkg.box()
+    o = orc.OracleBVH.build(geo.position, geo.index, strategy=0)
+    o.set_materials(geo.groups, [1, 0, 1, 0, 1, 0])        # Back, Front, Back, Front, Back, Front
+    ray = np.array([[0, 0.25, -10, 0, 0, 1]], dtype=np.float32)
+    counts, hits = o.raycast_all(ray)
+    assert counts[0] == 2
+    o.set_materials(geo.groups, [0, 0, 0, 0, 1, 1])        # Front x4, Back, Back
+    first = o.raycast_first(ray)[0]
+    assert first["point"][2] == 0.5
+    assert first["material_index"] == 4
+
+
+def test_box_group_gap_is_never_hit(pkg, orc):
+    """ShapeCasts.test.js:981-1003: triangles in no group are not in the BVH."""
+    geo = pkg.box()
+    geo.groups = []
+    geo.add_group(0, 6, 0)
+    geo.add_group(12, 24, 1)
+    o = orc.OracleBVH.build(geo.position, geo.index, groups=geo.groups, strategy=0)
+    counts, _ = o.raycast_all(np.array([[-2, 0, 0, 1, 0, 0]], dtype=np.float32))
+    assert counts[0] == 0

@@ -47,6 +47,9 @@ SIGNATURES = [
     ("bvhc_raycast_first", _I, [_P, _P, _U64, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
     ("bvhc_closest_point_to_point", _I, [_P, _P, _U64, _F, _F, _P, _I, _P]),
+    ("bvhc_mesh_set_groups", _I, [_P, _P, _I]),
+    ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
+    ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
 ]
 
 _lib = None

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <exception>
@@ -24,6 +25,7 @@ struct bvhc_mesh {
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
   int max_depth = 0;
+  std::vector<uint32_t> rec_face;   // faceIndex of every triangle record (material labelling)
   // staging buffers for BVHC_MEM_HOST calls (grow-only)
   void* d_in = nullptr;
   size_t in_cap = 0;
@@ -126,6 +128,7 @@ struct Converter {
       }
       r.face = (uint32_t)t;
       r.flags = (i + 1 == off + cnt) ? kTriLast : 0u;
+      r.material = kNoMaterial;
       tris.push_back(r);
     }
     return kLeafBit | first;
@@ -172,6 +175,25 @@ cudaError_t ensure(void** buf, size_t* cap, size_t bytes) {
   cudaError_t e = cudaMalloc(buf, bytes);
   if (e == cudaSuccess) *cap = bytes;
   return e;
+}
+
+SideTable single_side() {
+  SideTable t{};
+  t.n = 0;
+  t.per_material = 0;
+  return t;
+}
+
+bool material_table(const int8_t* sides, int n, SideTable& t) {
+  if (n < 0 || n > kMaxMaterials || (n > 0 && !sides)) return false;
+  t = SideTable{};
+  for (int i = 0; i < n; ++i) {
+    if (sides[i] < BVHC_FRONT_SIDE || sides[i] > BVHC_DOUBLE_SIDE) return false;
+    t.side[i] = sides[i];
+  }
+  t.n = n;
+  t.per_material = 1;
+  return true;
 }
 
 bvhc_status read_and_clear_error(bvhc_mesh* m, cudaStream_t s) {
@@ -328,6 +350,8 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
   m->n_tris = tris.size();
   m->n_roots = n_roots;
   m->max_depth = max_depth;
+  m->rec_face.resize(tris.size());
+  for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = upload(&m->d_nodes, pairs);
   if (e == cudaSuccess) e = upload(&m->d_tris, tris);
@@ -371,8 +395,8 @@ bvhc_status bvhc_mesh_synchronize(bvhc_mesh* m, void* stream) {
   return read_and_clear_error(m, static_cast<cudaStream_t>(stream));
 }
 
-bvhc_status bvhc_raycast_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                               bvhc_hit* out, int mem, void* stream) {
+static bvhc_status raycast_first_impl(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
+                                      float near_d, float far_d, bvhc_hit* out, int mem, void* stream) {
   if (!m || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
     return BVHC_ERR_INVALID_ARGUMENT;
   if (n == 0) return BVHC_OK;
@@ -381,19 +405,20 @@ bvhc_status bvhc_raycast_first(bvhc_mesh* m, const float* rays, uint64_t n, int 
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_raycast_first(m->view(), rays, n, side, near_d, far_d, out, s));
+    return from_cuda(launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, s));
   }
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_hit)));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
-  BVHC_CUDA_TRY(launch_raycast_first(m->view(), static_cast<const float*>(m->d_in), n, side, near_d, far_d,
+  BVHC_CUDA_TRY(launch_raycast_first(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d,
                                      static_cast<bvhc_hit*>(m->d_out), s));
   BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
 }
 
-bvhc_status bvhc_raycast(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                         uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem, void* stream) {
+static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
+                                    float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem,
+                                    void* stream) {
   if (!m || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
     return BVHC_ERR_INVALID_ARGUMENT;
   if (n == 0) return BVHC_OK;
@@ -402,18 +427,65 @@ bvhc_status bvhc_raycast(bvhc_mesh* m, const float* rays, uint64_t n, int side, 
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_raycast_all(m->view(), rays, n, side, near_d, far_d, cap, counts, hits, s));
+    return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s));
   }
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
-  BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, near_d, far_d, cap,
+  BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
                                    static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
+}
+
+bvhc_status bvhc_raycast_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                               bvhc_hit* out, int mem, void* stream) {
+  return raycast_first_impl(m, rays, n, side, single_side(), near_d, far_d, out, mem, stream);
+}
+
+bvhc_status bvhc_raycast(bvhc_mesh* m, const float* rays, uint64_t n, int side, float near_d, float far_d,
+                         uint32_t cap, uint32_t* counts, bvhc_hit* hits, int mem, void* stream) {
+  return raycast_all_impl(m, rays, n, side, single_side(), near_d, far_d, cap, counts, hits, mem, stream);
+}
+
+bvhc_status bvhc_raycast_first_materials(bvhc_mesh* m, const float* rays, uint64_t n, const int8_t* material_sides,
+                                         int n_materials, float near_d, float far_d, bvhc_hit* out, int mem,
+                                         void* stream) {
+  SideTable tab;
+  if (!material_table(material_sides, n_materials, tab)) return BVHC_ERR_INVALID_ARGUMENT;
+  return raycast_first_impl(m, rays, n, BVHC_FRONT_SIDE, tab, near_d, far_d, out, mem, stream);
+}
+
+bvhc_status bvhc_raycast_materials(bvhc_mesh* m, const float* rays, uint64_t n, const int8_t* material_sides,
+                                   int n_materials, float near_d, float far_d, uint32_t cap, uint32_t* counts,
+                                   bvhc_hit* hits, int mem, void* stream) {
+  SideTable tab;
+  if (!material_table(material_sides, n_materials, tab)) return BVHC_ERR_INVALID_ARGUMENT;
+  return raycast_all_impl(m, rays, n, BVHC_FRONT_SIDE, tab, near_d, far_d, cap, counts, hits, mem, stream);
+}
+
+bvhc_status bvhc_mesh_set_groups(bvhc_mesh* m, const int64_t* groups, int n_groups) {
+  if (!m || n_groups < 0 || (n_groups > 0 && !groups)) return BVHC_ERR_INVALID_ARGUMENT;
+  std::vector<uint32_t> mat(m->rec_face.size(), kNoMaterial);
+  for (size_t k = 0; k < m->rec_face.size(); ++k) {
+    int64_t first = 3 * (int64_t)m->rec_face[k];
+    for (int g = 0; g < n_groups; ++g) {
+      int64_t start = groups[3 * g], count = groups[3 * g + 1], mi = groups[3 * g + 2];
+      if (mi < 0 || mi >= (int64_t)kNoMaterial) return BVHC_ERR_INVALID_ARGUMENT;
+      if (first >= start && (count < 0 || first < start + count)) {
+        if (mat[k] != kNoMaterial) return BVHC_ERR_UNSUPPORTED;  // triangle in two groups
+        mat[k] = (uint32_t)mi;
+      }
+    }
+  }
+  if (mat.empty()) return BVHC_OK;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  BVHC_CUDA_TRY(cudaMemcpy2D(reinterpret_cast<char*>(m->d_tris) + offsetof(TriRecord, material), sizeof(TriRecord),
+                             mat.data(), sizeof(uint32_t), sizeof(uint32_t), mat.size(), cudaMemcpyHostToDevice));
+  return BVHC_OK;
 }
 
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint64_t n, float min_threshold,

@@ -63,7 +63,7 @@ __device__ __forceinline__ bool box_hit(float x0, float y0, float z0, float x1, 
 
 struct Tri {
   float3 a, b, c;
-  uint32_t face, flags;
+  uint32_t face, flags, material;
 };
 
 __device__ __forceinline__ Tri load_tri(const TriRecord* __restrict__ tris, uint32_t k) {
@@ -75,7 +75,18 @@ __device__ __forceinline__ Tri load_tri(const TriRecord* __restrict__ tris, uint
   r.c = make_float3(p1.z, p1.w, p2.x);
   r.face = __float_as_uint(p2.y);
   r.flags = __float_as_uint(p2.z);
+  r.material = __float_as_uint(p2.w);
   return r;
+}
+
+// The side a triangle is tested with: the call's side, or with an array of materials the side of
+// the triangle's group material (ThreeRayIntersectUtilities.js:170-205; a material index past the
+// array reads as `undefined` and tests like FrontSide).  -1: the triangle is in no group and is
+// not tested.
+__device__ __forceinline__ int tri_side(const Tri& t, int side, const SideTable& tab) {
+  if (!tab.per_material) return side;
+  if (t.material == kNoMaterial) return -1;
+  return t.material < (uint32_t)tab.n ? (int)tab.side[t.material] : kSideFront;
 }
 
 struct Pair {
@@ -145,8 +156,8 @@ __device__ __forceinline__ void store_miss(bvhc_hit* p) {
 // skipped, which can only drop triangles that are farther than that hit.
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
-                                                               int side, float near_d, float far_d,
-                                                               bvhc_hit* __restrict__ out) {
+                                                               int side, const SideTable sides, float near_d,
+                                                               float far_d, bvhc_hit* __restrict__ out) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   RayF r = make_ray(rays, i);
@@ -164,7 +175,8 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
           uint32_t k = link & ~kLeafBit;
           for (;;) {
             Tri t = load_tri(m.tris, k);
-            if (tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, side)) {
+            int ts = tri_side(t, side, sides);
+            if (ts >= 0 && tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts)) {
               ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
               ff dist = ff_mul(tt, dlen);
               bool in_range = !ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist);
@@ -235,8 +247,8 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
 // in DFS order.  The first `cap` hits are stored; counts[i] is the uncapped total.
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
-                                                             int side, float near_d, float far_d, uint32_t cap,
-                                                             uint32_t* __restrict__ counts,
+                                                             int side, const SideTable sides, float near_d,
+                                                             float far_d, uint32_t cap, uint32_t* __restrict__ counts,
                                                              bvhc_hit* __restrict__ hits) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -254,7 +266,8 @@ __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const fl
           uint32_t k = link & ~kLeafBit;
           for (;;) {
             Tri t = load_tri(m.tris, k);
-            if (tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, side)) {
+            int ts = tri_side(t, side, sides);
+            if (ts >= 0 && tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts)) {
               ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
               ff dist = ff_mul(tt, dlen);
               if (!ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist)) {
@@ -466,17 +479,19 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 
 static unsigned int grid_for(uint64_t n) { return (unsigned int)((n + dev::kBlock - 1) / dev::kBlock); }
 
-cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                                 bvhc_hit* out, cudaStream_t stream) {
+cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                                 float near_d, float far_d, bvhc_hit* out, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  dev::raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, near_d, far_d, out);
+  dev::raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
   return cudaGetLastError();
 }
 
-cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                               uint32_t cap, uint32_t* counts, bvhc_hit* hits, cudaStream_t stream) {
+cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                               float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
+                               cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, near_d, far_d, cap, counts, hits);
+  dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts,
+                                                                    hits);
   return cudaGetLastError();
 }
 

@@ -23,10 +23,11 @@ struct MeshDev {
   unsigned int* err;
 };
 
-cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                                 bvhc_hit* out, cudaStream_t stream);
-cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, float near_d, float far_d,
-                               uint32_t cap, uint32_t* counts, bvhc_hit* hits, cudaStream_t stream);
+cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                                 float near_d, float far_d, bvhc_hit* out, cudaStream_t stream);
+cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                               float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
+                               cudaStream_t stream);
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 

@@ -33,14 +33,24 @@ struct alignas(16) PairNode {
 static_assert(sizeof(PairNode) == 64, "PairNode must be 64 bytes");
 
 struct alignas(16) TriRecord {
-  // v[0..8] = a.xyz, b.xyz, c.xyz ; face = reference faceIndex ; flags bit 0 = last in leaf
+  // v[0..8] = a.xyz, b.xyz, c.xyz ; face = reference faceIndex ; flags bit 0 = last in leaf ;
+  // material = materialIndex of the geometry group holding the triangle (kNoMaterial: none)
   float v[9];
   uint32_t face;
   uint32_t flags;
-  uint32_t pad;
+  uint32_t material;
 };
 static_assert(sizeof(TriRecord) == 48, "TriRecord must be 48 bytes");
 
 constexpr uint32_t kTriLast = 1u;
+constexpr uint32_t kNoMaterial = 0xFFFFFFFFu;
+constexpr int kMaxMaterials = 64;
+
+// Per-call side selection: a single side for every triangle, or one side per material.
+struct SideTable {
+  int8_t side[kMaxMaterials];
+  int32_t n;        // number of materials
+  int32_t per_material;
+};
 
 }  // namespace bvhc

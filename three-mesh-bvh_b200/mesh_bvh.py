@@ -62,6 +62,14 @@ def _side_of(material_or_side) -> int:
     return int(side)
 
 
+def _material_sides(materials) -> np.ndarray | None:
+    """An array of materials as `materialOrSide` (ThreeRayIntersectUtilities.js:170-205) -> int8
+    side per material; None for a single material or side."""
+    if isinstance(materials, (list, tuple)):
+        return np.array([_side_of(m) for m in materials], dtype=np.int8)
+    return None
+
+
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
@@ -181,6 +189,10 @@ class MeshBVH:
                                       ind.size if ind is not None else 0, _ptr(pos), pos.shape[0], 3, C.byref(out))
             N.check(st, "bvhc_mesh_create")
             self._mesh = out
+            if g.groups:
+                grp = np.array([[st_, -1 if (isinstance(c, float) and math.isinf(c)) else int(c), mi]
+                                for st_, c, mi in g.groups], dtype=np.int64).reshape(-1)
+                N.check(lib.bvhc_mesh_set_groups(out, _ptr(grp), len(g.groups)), "bvhc_mesh_set_groups")
         return self._mesh
 
     def mesh_info(self) -> dict:
@@ -219,6 +231,12 @@ class MeshBVH:
             return out
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
         res = np.empty(rays.shape[0], dtype=HIT_DTYPE) if out is None else out
+        mats = _material_sides(side)
+        if mats is not None:
+            N.check(lib.bvhc_raycast_first_materials(mesh, _ptr(rays), rays.shape[0], _ptr(mats) if mats.size else None,
+                                                     mats.size, float(near), float(far), _ptr(res), N.MEM_HOST, None),
+                    "bvhc_raycast_first_materials")
+            return res
         N.check(lib.bvhc_raycast_first(mesh, _ptr(rays), rays.shape[0], _side_of(side), float(near), float(far),
                                        _ptr(res), N.MEM_HOST, None), "bvhc_raycast_first")
         return res
@@ -239,6 +257,12 @@ class MeshBVH:
         n = rays.shape[0]
         counts = np.empty(n, dtype=np.uint32)
         hits = np.empty((n, cap), dtype=HIT_DTYPE)
+        mats = _material_sides(side)
+        if mats is not None:
+            N.check(lib.bvhc_raycast_materials(mesh, _ptr(rays), n, _ptr(mats) if mats.size else None, mats.size,
+                                               float(near), float(far), cap, _ptr(counts), _ptr(hits), N.MEM_HOST,
+                                               None), "bvhc_raycast_materials")
+            return counts, hits
         N.check(lib.bvhc_raycast(mesh, _ptr(rays), n, _side_of(side), float(near), float(far), cap, _ptr(counts),
                                  _ptr(hits), N.MEM_HOST, None), "bvhc_raycast")
         return counts, hits
@@ -266,7 +290,14 @@ class MeshBVH:
         N.check(N.lib().bvhc_mesh_synchronize(self._device_mesh(), stream), "bvhc_mesh_synchronize")
 
     # -- reference-shaped single queries (MeshBVH.js:532-577, 874-884) ---------------------
-    def _intersection(self, rec) -> Intersection:
+    def _material_index(self, face_index: int) -> int:
+        first = 3 * face_index
+        for start, count, mi in self.geometry.groups:
+            if first >= start and (math.isinf(count) or first < start + count):
+                return int(mi)
+        return 0
+
+    def _intersection(self, rec, materials=False) -> Intersection:
         f = int(rec["face_index"])
         tri = self.geometry.triangle(f)
         base = 3 * f
@@ -278,7 +309,7 @@ class MeshBVH:
         ln = float(np.dot(n, n))
         n = n / math.sqrt(ln) if ln > 0 else np.zeros(3)
         return Intersection(distance=float(rec["distance"]), point=np.array(rec["point"], dtype=np.float64),
-                            face=Face(a, b, c, n, 0), faceIndex=f,
+                            face=Face(a, b, c, n, self._material_index(f) if materials else 0), faceIndex=f,
                             barycoord=np.array(rec["barycoord"], dtype=np.float64))
 
     @staticmethod
@@ -289,12 +320,15 @@ class MeshBVH:
     def raycastFirst(self, ray, materialOrSide=FrontSide, near=0.0, far=math.inf):
         """`ray` is (origin, direction).  Returns an Intersection or None."""
         rec = self.raycast_first_batch(self._ray_row(ray), materialOrSide, near, far)[0]
-        return None if int(rec["face_index"]) == N.NO_HIT else self._intersection(rec)
+        if int(rec["face_index"]) == N.NO_HIT:
+            return None
+        return self._intersection(rec, isinstance(materialOrSide, (list, tuple)))
 
     def raycast(self, ray, materialOrSide=FrontSide, near=0.0, far=math.inf, cap=1024):
         """All hits of one ray, unsorted (DFS order), as a list of Intersection."""
         counts, hits = self.raycast_batch(self._ray_row(ray), materialOrSide, near, far, cap=cap)
-        return [self._intersection(hits[0, k]) for k in range(min(int(counts[0]), cap))]
+        mats = isinstance(materialOrSide, (list, tuple))
+        return [self._intersection(hits[0, k], mats) for k in range(min(int(counts[0]), cap))]
 
     def closestPointToPoint(self, point, target: HitPointInfo | None = None, minThreshold=0.0,
                             maxThreshold=math.inf):
