@@ -18,7 +18,6 @@ import math
 import os
 import re
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -50,6 +49,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=1 << 25, help="rays (both sets together) timed on the CPU baseline")
     ap.add_argument("--ref-sample", type=int, default=1 << 21, help="rays per set per step in --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default traversal variant)")
+    ap.add_argument("--traversal", default=None, help="force a traversal variant 'persistent,order,refill'")
     return ap.parse_args()
 
 
@@ -80,61 +81,66 @@ def scene(pkg, args, rank):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled (read-only NVML queries, every 5 ms) during the
+    timed region; falls back to no record when NVML is unavailable."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+        self.rows = []
+        self.stop = threading.Event()
+        self.nv = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.gpu]) if vis and vis.split(",")[0].isdigit() else self.gpu
+            self.h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._run, daemon=True)
             self.t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+        except Exception:
+            self.nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.rows.append((sm, rs, pw))
+            except Exception:
+                pass
+            time.sleep(0.005)
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
-        rows = []
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                rows.append(dict(sm=float(f[1]), smax=float(f[2]), power=float(f[3]), reasons=f[4],
-                                 hw=f[5], hwt=f[6], swt=f[7], pcap=f[8]))
-            except ValueError:
-                continue
-        if not rows:
+        if not self.rows:
             return None
+        nv = self.nv
         reasons = set()
-        for r in rows:
-            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
-                              ("pcap", "sw_power_cap")):
-                if r[key].lower() == "active":
+        for _, rs, _ in self.rows:
+            for name, const in self.REASONS:
+                if rs & getattr(nv, const, 0):
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
-                "reasons": sorted(reasons), "samples": len(rows),
-                "power_w_max": max(r["power"] for r in rows)}
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.smax,
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "power_w_max": max(r[2] for r in self.rows)}
 
 
 def measured_peak():
@@ -228,9 +234,26 @@ def run_engine(args, ws, rank, local):
     d_out = [torch.empty((r.shape[0], 8), dtype=torch.float32, device=dev) for _, r in sets]
     n_step = sum(r.shape[0] for _, r in sets)
     stream = torch.cuda.current_stream(dev)
+    # traversal variant per ray set: forced, autotuned on a strided 2^21-ray sample of the set, or
+    # the library default
+    tuned = {}
+    configs = [None] * len(sets)
+    if args.traversal:
+        configs = [[int(x) for x in args.traversal.split(",")]] * len(sets)
+    elif not args.no_tune:
+        from three_mesh_bvh_b200 import autotune
+
+        k = 1 << 21
+        for i, (name, _) in enumerate(sets):
+            sample = d_rays[i][torch.linspace(0, d_rays[i].shape[0] - 1, k, device=dev).long()].contiguous()
+            tuned[name] = autotune.tune_raycast_first(bvh, sample, tag=f"knot2M-{name}")
+            configs[i] = tuned[name]["best"]
+            del sample
 
     def step(ev=None):
         for k in range(len(sets)):
+            if configs[k] is not None:
+                bvh.set_traversal(*configs[k])
             if ev is not None:
                 ev[k][0].record(stream)
             bvh.raycast_first_batch(d_rays[k], out=d_out[k], stream=stream.cuda_stream)
@@ -314,6 +337,7 @@ def run_engine(args, ws, rank, local):
                            "parallelism": f"replicas x{ws}"},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
+                "traversal": bvh.get_traversal(), "autotune": tuned,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": args.steps * len(sets)}
         print(json.dumps(line), flush=True)

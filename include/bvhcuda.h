@@ -122,6 +122,23 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
                              const float* positions, uint64_t n_verts, int stride_floats, bvhc_mesh** out);
 void bvhc_mesh_destroy(bvhc_mesh* mesh);
 bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
+/* Traversal variant used by this mesh's raycastFirst calls (no reference counterpart: the
+ * reference has one recursive traversal).  persistent = 1 runs a grid of resident warps that
+ * refill idle lanes from a work counter once `refill` (1..32) lanes are idle; 0 runs one ray per
+ * thread.  order = 0 visits the near child by the sign of the ray direction on the split axis (the
+ * reference's order), 1 by the smaller entry distance.  occupancy selects the persistent
+ * kernel's register budget: 0 the compiler's choice, 1 at least six and 2 at least eight resident
+ * 128-thread blocks per SM.  Results are the same for every variant (up to exact ties); the
+ * autotuner picks the fastest per mesh and workload. */
+typedef struct bvhc_traversal_config {
+  int32_t persistent;
+  int32_t order;
+  int32_t refill;
+  int32_t occupancy;
+} bvhc_traversal_config;
+bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
+bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);
+
 /* Waits for the mesh's work on `stream` and reports (and clears) the device error word. */
 bvhc_status bvhc_mesh_synchronize(bvhc_mesh* mesh, void* stream);
 

@@ -27,6 +27,7 @@ def tie_exempt(all_counts, all_hits):
     return ex
 
 
+@np.errstate(invalid="ignore")
 def check_first(got, exp, exempt=None):
     """Returns a dict of mismatch counts (all zero when the parity bar is met)."""
     n = exp.shape[0]
@@ -68,6 +69,7 @@ def check_all(counts, hits, exp_counts, exp_hits):
     return dict(count=bad_count, set=bad_set, distance=bad_dist, rays=n)
 
 
+@np.errstate(invalid="ignore")
 def check_closest(got, exp, tri_distance=None):
     """tri_distance(i, face) -> float64 distance from query i to triangle `face` (tie check)."""
     gh = got["face_index"] != NO_HIT

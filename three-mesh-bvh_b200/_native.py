@@ -25,6 +25,10 @@ class BvhcClosest(C.Structure):
     _fields_ = [("face_index", C.c_uint32), ("distance", C.c_float), ("point", C.c_float * 3)]
 
 
+class BvhcTraversalConfig(C.Structure):
+    _fields_ = [("persistent", C.c_int32), ("order", C.c_int32), ("refill", C.c_int32), ("occupancy", C.c_int32)]
+
+
 class BvhcMeshInfo(C.Structure):
     _fields_ = [("node_records", C.c_uint64), ("triangle_records", C.c_uint64), ("device_bytes", C.c_uint64),
                 ("max_depth", C.c_int32), ("root_count", C.c_int32)]
@@ -48,6 +52,8 @@ SIGNATURES = [
     ("bvhc_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
     ("bvhc_closest_point_to_point", _I, [_P, _P, _U64, _F, _F, _P, _I, _P]),
     ("bvhc_mesh_set_groups", _I, [_P, _P, _I]),
+    ("bvhc_mesh_set_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
+    ("bvhc_mesh_get_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
 ]

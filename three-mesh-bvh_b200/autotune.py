@@ -1,0 +1,65 @@
+"""Autotuner for the traversal kernels.
+
+For a mesh and a representative ray batch already on the device, each candidate traversal
+variant (persistent warps with lane refill or one ray per thread, child visiting order, refill
+threshold) is timed with CUDA events on the launching stream after a warm-up launch, and the
+fastest is installed on the mesh.  Results are cached per (GPU name, triangle-count bucket,
+workload tag), in memory and optionally in a JSON file, so a serving process tunes once per
+mesh class.  Every variant returns the same hits (up to exact ties), so tuning never changes
+results, only speed.
+"""
+from __future__ import annotations
+
+import json
+import math
+from pathlib import Path
+
+CANDIDATES = [(0, 0, 16, 0), (0, 1, 16, 0)] + [(1, order, refill, occ) for order in (0, 1) for refill in (8, 16, 24, 32)
+                                               for occ in (0, 1, 2)]
+
+_cache: dict = {}
+
+
+def _key(bvh, tag: str) -> str:
+    import torch
+
+    tris = bvh.mesh_info()["triangle_records"]
+    bucket = int(math.log2(max(tris, 1)))
+    return f"{torch.cuda.get_device_name()}|tri2^{bucket}|{tag}"
+
+
+def tune_raycast_first(bvh, rays, side: int = 0, near: float = 0.0, far: float = math.inf, tag: str = "default",
+                       reps: int = 3, cache_file: str | Path | None = None, candidates=CANDIDATES) -> dict:
+    """Time every candidate on `rays` (torch CUDA tensor, n x 6) and install the fastest."""
+    import torch
+
+    key = _key(bvh, tag)
+    if cache_file is not None and not _cache:
+        p = Path(cache_file)
+        if p.exists():
+            _cache.update(json.loads(p.read_text()))
+    if key in _cache:
+        best = _cache[key]["best"]
+        bvh.set_traversal(*best)
+        return _cache[key]
+    stream = torch.cuda.current_stream(rays.device)
+    out = torch.empty((rays.shape[0], 8), dtype=torch.float32, device=rays.device)
+    timings = {}
+    for cand in candidates:
+        bvh.set_traversal(*cand)
+        bvh.raycast_first_batch(rays, side, near, far, out=out, stream=stream.cuda_stream)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(reps):
+            bvh.raycast_first_batch(rays, side, near, far, out=out, stream=stream.cuda_stream)
+        end.record(stream)
+        end.synchronize()
+        timings[str(list(cand))] = start.elapsed_time(end) / reps
+    bvh.synchronize(stream.cuda_stream)
+    best = min(candidates, key=lambda c: timings[str(list(c))])
+    bvh.set_traversal(*best)
+    entry = {"best": list(best), "ms": timings[str(list(best))], "timings_ms": timings, "rays": int(rays.shape[0])}
+    _cache[key] = entry
+    if cache_file is not None:
+        Path(cache_file).write_text(json.dumps(_cache, indent=1))
+    return entry

@@ -16,12 +16,17 @@
 
 using namespace bvhc;
 
+// Rays per chunk of the pipelined host-memory raycastFirst path (24 MB in + 32 MB out per slot).
+constexpr uint64_t kPipeChunk = 1ull << 20;
+
 struct bvhc_mesh {
   int device = 0;
   PairNode* d_nodes = nullptr;
   TriRecord* d_tris = nullptr;
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
+  unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
+  TraversalConfig cfg{1, 1, 16, 0};
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
   int max_depth = 0;
@@ -33,6 +38,11 @@ struct bvhc_mesh {
   size_t out_cap = 0;
   void* d_out2 = nullptr;
   size_t out2_cap = 0;
+  // pipelined host-memory raycastFirst: two streams, staging slots and work counters
+  cudaStream_t pipe[2] = {nullptr, nullptr};
+  void* slot_in[2] = {nullptr, nullptr};
+  void* slot_out[2] = {nullptr, nullptr};
+  unsigned long long* d_work2 = nullptr;
 
   MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
 };
@@ -357,6 +367,7 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
   if (e == cudaSuccess) e = upload(&m->d_tris, tris);
   if (e == cudaSuccess) e = upload(&m->d_roots, root_links);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_err), sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_work), sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(m->d_err, 0, sizeof(unsigned int));
   if (e != cudaSuccess) {
     bvhc_mesh_destroy(m);
@@ -373,9 +384,16 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_tris);
   cudaFree(m->d_roots);
   cudaFree(m->d_err);
+  cudaFree(m->d_work);
   cudaFree(m->d_in);
   cudaFree(m->d_out);
   cudaFree(m->d_out2);
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(m->slot_in[k]);
+    cudaFree(m->slot_out[k]);
+    if (m->pipe[k]) cudaStreamDestroy(m->pipe[k]);
+  }
+  cudaFree(m->d_work2);
   delete m;
 }
 
@@ -395,6 +413,55 @@ bvhc_status bvhc_mesh_synchronize(bvhc_mesh* m, void* stream) {
   return read_and_clear_error(m, static_cast<cudaStream_t>(stream));
 }
 
+static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
+                                  float near_d, float far_d, bvhc_hit* out, unsigned long long* work, cudaStream_t s) {
+  if (m->cfg.persistent)
+    return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
+                                           s);
+  return launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
+}
+
+// Streams, staging slots and the second work counter of the pipelined host-memory path.
+static cudaError_t ensure_pipeline(bvhc_mesh* m) {
+  for (int k = 0; k < 2; ++k) {
+    if (!m->pipe[k]) {
+      cudaError_t e = cudaStreamCreateWithFlags(&m->pipe[k], cudaStreamNonBlocking);
+      if (e != cudaSuccess) return e;
+    }
+    size_t cap_in = 0, cap_out = 0;
+    if (m->slot_in[k] == nullptr) {
+      cudaError_t e = ensure(&m->slot_in[k], &cap_in, kPipeChunk * 24);
+      if (e != cudaSuccess) return e;
+    }
+    if (m->slot_out[k] == nullptr) {
+      cudaError_t e = ensure(&m->slot_out[k], &cap_out, kPipeChunk * sizeof(bvhc_hit));
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (!m->d_work2) return cudaMalloc(reinterpret_cast<void**>(&m->d_work2), sizeof(unsigned long long));
+  return cudaSuccess;
+}
+
+static bool valid_config(const bvhc_traversal_config* cfg) {
+  return cfg && (cfg->persistent == 0 || cfg->persistent == 1) && (cfg->order == 0 || cfg->order == 1) &&
+         cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2;
+}
+
+bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
+  if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy};
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* cfg) {
+  if (!m || !cfg) return BVHC_ERR_INVALID_ARGUMENT;
+  cfg->persistent = m->cfg.persistent;
+  cfg->order = m->cfg.order;
+  cfg->refill = m->cfg.refill;
+  cfg->occupancy = m->cfg.occupancy;
+  return BVHC_OK;
+}
+
 static bvhc_status raycast_first_impl(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
                                       float near_d, float far_d, bvhc_hit* out, int mem, void* stream) {
   if (!m || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
@@ -405,14 +472,38 @@ static bvhc_status raycast_first_impl(bvhc_mesh* m, const float* rays, uint64_t 
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, s));
+    return from_cuda(dispatch_first(m, rays, n, side, tab, near_d, far_d, out, m->d_work, s));
   }
-  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
-  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_hit)));
-  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
-  BVHC_CUDA_TRY(launch_raycast_first(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d,
-                                     static_cast<bvhc_hit*>(m->d_out), s));
-  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+  if (n <= kPipeChunk) {
+    BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
+    BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_hit)));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
+    BVHC_CUDA_TRY(dispatch_first(m, static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d,
+                                 static_cast<bvhc_hit*>(m->d_out), m->d_work, s));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+    return read_and_clear_error(m, s);
+  }
+  // Large host batches: chunks alternate between two streams, each with its own staging slot and
+  // work counter, so the host->device copy of one chunk, the traversal of another and the
+  // device->host copy of a third overlap (copies overlap only for page-locked host memory).
+  BVHC_CUDA_TRY(ensure_pipeline(m));
+  cudaEvent_t ready;
+  BVHC_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  cudaEventRecord(ready, s);
+  for (int k = 0; k < 2; ++k) cudaStreamWaitEvent(m->pipe[k], ready, 0);
+  cudaEventDestroy(ready);
+  unsigned long long* works[2] = {m->d_work, m->d_work2};
+  for (uint64_t j = 0, off = 0; off < n; ++j, off += kPipeChunk) {
+    int k = (int)(j & 1);
+    uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
+    cudaStream_t st = m->pipe[k];
+    BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], rays + 6 * off, cnt * 24, cudaMemcpyHostToDevice, st));
+    BVHC_CUDA_TRY(dispatch_first(m, static_cast<const float*>(m->slot_in[k]), cnt, side, tab, near_d, far_d,
+                                 static_cast<bvhc_hit*>(m->slot_out[k]), works[k], st));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(out + off, m->slot_out[k], cnt * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, st));
+  }
+  BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[0]));
+  BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[1]));
   return read_and_clear_error(m, s);
 }
 

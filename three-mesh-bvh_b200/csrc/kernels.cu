@@ -7,6 +7,7 @@
 // overflow would set the device error word instead of faulting.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -30,7 +31,8 @@ struct RayF {
 
 __device__ __forceinline__ RayF make_ray(const float* __restrict__ rays, uint64_t i) {
   const float2* p = reinterpret_cast<const float2*>(rays + 6 * i);
-  float2 r0 = __ldg(p), r1 = __ldg(p + 1), r2 = __ldg(p + 2);
+  // rays are read once: streaming loads keep them from evicting the BVH from L2
+  float2 r0 = __ldcs(p), r1 = __ldcs(p + 1), r2 = __ldcs(p + 2);
   RayF r;
   r.o = make_float3(r0.x, r0.y, r1.x);
   r.d = make_float3(r1.y, r2.x, r2.y);
@@ -139,31 +141,111 @@ __device__ void make_hit(const Tri& t, const RayF& r, ff tt, ff dist, bvhc_hit& 
 
 __device__ __forceinline__ void store_hit(bvhc_hit* p, const bvhc_hit& h) {
   float4* q = reinterpret_cast<float4*>(p);
-  q[0] = make_float4(__uint_as_float(h.face_index), h.distance, h.point[0], h.point[1]);
-  q[1] = make_float4(h.point[2], h.barycoord[0], h.barycoord[1], h.barycoord[2]);
+  __stcs(q, make_float4(__uint_as_float(h.face_index), h.distance, h.point[0], h.point[1]));
+  __stcs(q + 1, make_float4(h.point[2], h.barycoord[0], h.barycoord[1], h.barycoord[2]));
 }
 
 __device__ __forceinline__ void store_miss(bvhc_hit* p) {
   float4* q = reinterpret_cast<float4*>(p);
-  q[0] = make_float4(__uint_as_float(BVHC_NO_HIT), kInf, 0.0f, 0.0f);
-  q[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  __stcs(q, make_float4(__uint_as_float(BVHC_NO_HIT), kInf, 0.0f, 0.0f));
+  __stcs(q + 1, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
 }
 
 // ---------------------------------------------------------------------------------------------
-// raycastFirst (raycastFirst.template.js:19-103, roots loop MeshBVH.js:558-577).
-// Children are visited near-first by the sign of the ray direction on the split axis, as the
-// reference does; a child whose (widened) entry distance is beyond the best hit so far is
-// skipped, which can only drop triangles that are farther than that hit.
+// raycastFirst leaf step shared by both kernel forms.  Candidate hits are ordered with float32 t
+// values and their error bounds; float-float only settles candidates the bounds cannot separate
+// (the reference keeps the strictly closer one; exact ties keep the candidate found first).
 // ---------------------------------------------------------------------------------------------
+constexpr float kTwoU = 1.1920928955078125e-07f;  // 2u
+
+// near <= dist <= far for dist = t |d|, decided with the float32 bounds, else in float-float.
+__device__ __forceinline__ bool in_range(float t, float t_err, const Tri& tr, const RayF& r, float dlen, float near_d,
+                                         float far_d) {
+  float dist = t * dlen;
+  float derr = t_err * dlen + fabsf(dist) * kTwoU + 1e-30f;
+  if (dist - derr >= near_d && dist + derr <= far_d) return true;
+  if (dist + derr < near_d || dist - derr > far_d) return false;
+  ff dl = ff_mul(tri_t_ff(tri_eval_ff(tr.a, tr.b, tr.c, r.o, r.d)), dir_length(r.d));
+  return !ff_lt(dl, ff_from(near_d)) && !ff_lt(ff_from(far_d), dl);
+}
+
+struct Best {
+  float t, err;
+  uint32_t rec;
+};
+
+__device__ __forceinline__ void leaf_first(const MeshDev& m, uint32_t k, const RayF& r, float dlen, int side,
+                                           const SideTable& sides, float near_d, float far_d, Best& best) {
+  for (;;) {
+    Tri t = load_tri(m.tris, k);
+    int ts = tri_side(t, side, sides);
+    float th, te;
+    if (ts >= 0 && tri_hit_t(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts, th, te) &&
+        in_range(th, te, t, r, dlen, near_d, far_d)) {
+      bool take;
+      if (best.rec == 0xFFFFFFFFu || th + te < best.t - best.err) {
+        take = true;
+      } else if (th - te > best.t + best.err) {
+        take = false;
+      } else {
+        Tri bt = load_tri(m.tris, best.rec);
+        ff tn = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+        ff tb = tri_t_ff(tri_eval_ff(bt.a, bt.b, bt.c, r.o, r.d));
+        take = ff_lt(tn, tb);
+        if (take) {
+          th = tn.hi;
+          te = fabsf(tn.hi) * kTinyRel + 1e-30f;
+        }
+      }
+      if (take) {
+        best.t = th;
+        best.err = te;
+        best.rec = k;
+      }
+    }
+    if (t.flags & kTriLast) break;
+    ++k;
+  }
+}
+
+// The reported record of the best hit: t, distance, point and barycentrics in float-float.
+__device__ __forceinline__ void finish_first(const MeshDev& m, uint32_t rec, const RayF& r, bvhc_hit* o) {
+  if (rec == 0xFFFFFFFFu) {
+    store_miss(o);
+    return;
+  }
+  Tri t = load_tri(m.tris, rec);
+  ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+  bvhc_hit h;
+  make_hit(t, r, tt, ff_mul(tt, dir_length(r.d)), h);
+  store_hit(o, h);
+}
+
+// ---------------------------------------------------------------------------------------------
+// raycastFirst (raycastFirst.template.js:19-103, roots loop MeshBVH.js:558-577), one ray per
+// thread.  ORDER 0 visits the near child by the sign of the ray direction on the split axis, as
+// the reference does; ORDER 1 by the smaller entry distance.  A child whose (widened) entry
+// distance is beyond the best hit so far is skipped, which can only drop triangles that are
+// farther than that hit.
+// ---------------------------------------------------------------------------------------------
+template <int ORDER>
+__device__ __forceinline__ bool left_first(const Pair& p, const RayF& r, float e0, float e1) {
+  if (ORDER == 0) {
+    float dir_axis = p.axis == 0 ? r.d.x : (p.axis == 1 ? r.d.y : r.d.z);
+    return dir_axis >= 0.0f;
+  }
+  return e0 <= e1;
+}
+
+template <int ORDER>
 __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
                                                                int side, const SideTable sides, float near_d,
                                                                float far_d, bvhc_hit* __restrict__ out) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   RayF r = make_ray(rays, i);
-  ff dlen = dir_length(r.d);
-  ff best_t = {kInf, 0.0f};
-  uint32_t best_rec = 0xFFFFFFFFu;
+  float dlen = sqrtf(r.d.x * r.d.x + r.d.y * r.d.y + r.d.z * r.d.z);
+  Best best{kInf, 0.0f, 0xFFFFFFFFu};
   uint32_t stack_link[kMaxStack];
   float stack_t[kMaxStack];
   for (int root = 0; root < m.n_roots; ++root) {
@@ -171,35 +253,16 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
     int sp = 0;
     for (;;) {
       if (link & kLeafBit) {
-        if (link != kEmptyLeaf) {
-          uint32_t k = link & ~kLeafBit;
-          for (;;) {
-            Tri t = load_tri(m.tris, k);
-            int ts = tri_side(t, side, sides);
-            if (ts >= 0 && tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts)) {
-              ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
-              ff dist = ff_mul(tt, dlen);
-              bool in_range = !ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist);
-              if (in_range && ff_lt(tt, best_t)) {
-                best_t = tt;
-                best_rec = k;
-              }
-            }
-            if (t.flags & kTriLast) break;
-            ++k;
-          }
-        }
+        if (link != kEmptyLeaf) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
       } else {
         Pair p = load_pair(m.nodes, link);
-        float lim = fminf(far_d, best_t.hi * (1.0f + kSlabMargin));
+        float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
         float e0, e1;
         bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, lim, e0);
         bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, lim, e1);
-        float dir_axis = p.axis == 0 ? r.d.x : (p.axis == 1 ? r.d.y : r.d.z);
-        bool ltr = dir_axis >= 0.0f;
-        uint32_t c1 = ltr ? p.ll : p.lr, c2 = ltr ? p.lr : p.ll;
-        bool h1st = ltr ? h0 : h1, h2nd = ltr ? h1 : h0;
-        float t2nd = ltr ? e1 : e0;
+        bool lf = left_first<ORDER>(p, r, e0, e1);
+        uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+        bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
         if (h1st) {
           if (h2nd) {
             if (sp >= kMaxStack) {
@@ -208,7 +271,7 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
               return;
             }
             stack_link[sp] = c2;
-            stack_t[sp] = t2nd;
+            stack_t[sp] = lf ? e1 : e0;
             ++sp;
           }
           link = c1;
@@ -221,9 +284,10 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
       }
       // pop, skipping entries that start beyond the best hit found since they were pushed
       bool found = false;
+      float lim = (best.t + best.err) * (1.0f + kSlabMargin);
       while (sp > 0) {
         --sp;
-        if (stack_t[sp] <= best_t.hi * (1.0f + kSlabMargin)) {
+        if (stack_t[sp] <= lim) {
           link = stack_link[sp];
           found = true;
           break;
@@ -232,14 +296,7 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
       if (!found) break;
     }
   }
-  if (best_rec == 0xFFFFFFFFu) {
-    store_miss(out + i);
-    return;
-  }
-  Tri t = load_tri(m.tris, best_rec);
-  bvhc_hit h;
-  make_hit(t, r, best_t, ff_mul(best_t, dlen), h);
-  store_hit(out + i, h);
+  finish_first(m, best.rec, r, out + i);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -475,14 +532,254 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
   o->point[2] = ff_to_f(c.q.z);
 }
 
+// ---------------------------------------------------------------------------------------------
+// raycastFirst, persistent form.  A fixed grid of warps pulls rays from a global work counter in
+// chunks of kChunk rays per warp (one atomicAdd per chunk); a lane whose ray is finished sits idle
+// until `refill` lanes of its warp are idle, and then those lanes take the next rays of the warp's
+// chunk together, so warps stay full while rays of very different cost (early misses, deep
+// traversals) are mixed.  Each outer iteration runs the "while-while" phases: every lane walks
+// child pairs until it reaches a leaf or finishes, then the lanes holding a leaf test it together.
+// A finished hit is written as a pending (record, t) pair; finalize_first_kernel then computes the
+// reported records one ray per thread, so the float-float work runs with full warps.
+// ---------------------------------------------------------------------------------------------
+constexpr unsigned kChunk = 256;
+
+// Mesh of ray `rid` in a batch: the last mesh whose first ray is <= rid (ray_off is CSR).
+__device__ __forceinline__ int mesh_of_ray(const BatchDev& bd, uint64_t rid) {
+  int lo = 0, hi = bd.n_meshes - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(bd.ray_off + mid) <= rid) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// BATCHED: every ray belongs to one of many meshes packed into one node/triangle pool (the
+// meshes of a BatchedMesh, ExtensionUtilities.js:87-161); a lane looks up its ray's mesh when it
+// takes the ray and traverses that mesh's roots.  Otherwise the mesh's roots are m.roots[0..n).
+// MINB: minimum resident blocks per SM requested from the register allocator (1 = no limit).
+template <int ORDER, bool BATCHED, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
+    MeshDev m, const BatchDev bd, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides,
+    float near_d, float far_d, bvhc_hit* __restrict__ out, unsigned long long* __restrict__ work, int refill) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  bool active = false;
+  uint64_t rid = 0;
+  RayF r;
+  float dlen = 0.0f;
+  Best best{kInf, 0.0f, 0xFFFFFFFFu};
+  uint32_t link = 0;
+  int sp = 0, root = 0, root_end = m.n_roots;
+  uint32_t stack_link[kMaxStack];
+  float stack_t[kMaxStack];
+  uint64_t pool = 0, pool_end = 0;  // warp-uniform: this warp's untaken rays [pool, pool_end)
+  bool drained = false;             // warp-uniform: the work counter is exhausted
+
+  // Next link after a leaf or a dead end: pop the nearest stacked child whose entry distance does
+  // not lie beyond the best hit, else move to the next root, else finish the ray.
+  auto pop_next = [&]() {
+    float lim = (best.t + best.err) * (1.0f + kSlabMargin);
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= lim) {
+        link = stack_link[sp];
+        return;
+      }
+    }
+    if (++root < root_end) {
+      link = m.roots[root];
+      return;
+    }
+    if (best.rec == 0xFFFFFFFFu) {
+      store_miss(out + rid);
+    } else {
+      // pending: the record index in face_index, finalize_first_kernel completes it
+      __stcs(reinterpret_cast<float4*>(out + rid), make_float4(__uint_as_float(best.rec), best.t, 0.0f, 0.0f));
+    }
+    active = false;
+  };
+
+  for (;;) {
+    unsigned idle = __ballot_sync(0xFFFFFFFFu, !active);
+    if (idle == 0xFFFFFFFFu || (idle != 0u && __popc(idle) >= refill)) {
+      unsigned need = __popc(idle);
+      uint64_t avail = pool_end - pool;
+      uint64_t nb = 0, ne = 0;
+      if (need > avail && !drained) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(work, (unsigned long long)kChunk);
+        b = __shfl_sync(0xFFFFFFFFu, b, 0);
+        if (b >= n) {
+          drained = true;
+        } else {
+          nb = b;
+          ne = b + kChunk < n ? b + kChunk : n;
+        }
+      }
+      if (!active) {
+        uint64_t rank = __popc(idle & lt_mask);
+        bool got = true;
+        if (rank < avail) rid = pool + rank;
+        else if (rank - avail < ne - nb) rid = nb + (rank - avail);
+        else got = false;
+        if (got) {
+          active = true;
+          r = make_ray(rays, rid);
+          dlen = sqrtf(r.d.x * r.d.x + r.d.y * r.d.y + r.d.z * r.d.z);
+          best = Best{kInf, 0.0f, 0xFFFFFFFFu};
+          if (BATCHED) {
+            int mesh = mesh_of_ray(bd, rid);
+            root = (int)__ldg(bd.mesh_root_off + mesh);
+            root_end = (int)__ldg(bd.mesh_root_off + mesh + 1);
+          } else {
+            root = 0;
+            root_end = m.n_roots;
+          }
+          sp = 0;
+          link = m.roots[root];
+        }
+      }
+      if (need <= avail) {
+        pool += need;
+      } else {
+        uint64_t used = need - avail;
+        pool = nb + used < ne ? nb + used : ne;
+        pool_end = ne;
+      }
+      if (idle == 0xFFFFFFFFu && __ballot_sync(0xFFFFFFFFu, active) == 0u) break;
+    }
+    if (!active) continue;
+    // phase 1: child pairs, until this lane holds a leaf or has finished its ray
+    while (active && !(link & kLeafBit)) {
+      Pair p = load_pair(m.nodes, link);
+      float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
+      float e0, e1;
+      bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, lim, e0);
+      bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, lim, e1);
+      bool lf = left_first<ORDER>(p, r, e0, e1);
+      uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+      bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+      if (h1st && h2nd) {
+        if (sp >= kMaxStack) {
+          atomicOr(m.err, kErrStackOverflow);
+          best.rec = 0xFFFFFFFFu;
+          sp = 0;
+          root = root_end;
+          pop_next();
+        } else {
+          stack_link[sp] = c2;
+          stack_t[sp] = lf ? e1 : e0;
+          ++sp;
+          link = c1;
+        }
+      } else if (h1st) {
+        link = c1;
+      } else if (h2nd) {
+        link = c2;
+      } else {
+        pop_next();
+      }
+    }
+    // phase 2: the leaf
+    if (active) {
+      if (link != kEmptyLeaf) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
+      pop_next();
+    }
+  }
+}
+
+// Completes the pending hits of raycast_first_persistent_kernel, one ray per thread.
+__global__ void __launch_bounds__(kBlock) finalize_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
+                                                                bvhc_hit* __restrict__ out) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t rec = __float_as_uint(__ldcs(reinterpret_cast<const float*>(out + i)));
+  if (rec == BVHC_NO_HIT) return;
+  RayF r = make_ray(rays, i);
+  finish_first(m, rec, r, out + i);
+}
+
 }  // namespace dev
 
 static unsigned int grid_for(uint64_t n) { return (unsigned int)((n + dev::kBlock - 1) / dev::kBlock); }
 
-cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
-                                 float near_d, float far_d, bvhc_hit* out, cudaStream_t stream) {
+// Resident blocks per SM x SM count for a persistent kernel on the current device, cached per
+// (device, kernel variant).
+template <class K>
+static unsigned int persistent_grid(K kernel, int variant) {
+  constexpr int kDevs = 64, kVariants = 12;
+  static unsigned int cache[kDevs][kVariants] = {};
+  int dev_id = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev_id);
+  if (dev_id >= 0 && dev_id < kDevs && cache[dev_id][variant]) return cache[dev_id][variant];
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, dev::kBlock, 0);
+  unsigned int g = (unsigned int)(std::max(1, sms) * std::max(1, per_sm));
+  if (dev_id >= 0 && dev_id < kDevs) cache[dev_id][variant] = g;
+  return g;
+}
+
+struct PersistentArgs {
+  MeshDev m;
+  BatchDev bd;
+  const float* rays;
+  uint64_t n;
+  int side;
+  SideTable sides;
+  float near_d, far_d;
+  bvhc_hit* out;
+  unsigned long long* work;
+  int refill;
+};
+
+template <int ORDER, bool BATCHED, int MINB>
+static void launch_persistent(const PersistentArgs& a, cudaStream_t stream) {
+  auto kernel = dev::raycast_first_persistent_kernel<ORDER, BATCHED, MINB>;
+  int variant = ORDER * 6 + (BATCHED ? 3 : 0) + (MINB == 1 ? 0 : (MINB == 6 ? 1 : 2));
+  unsigned int g = persistent_grid(kernel, variant);
+  g = (unsigned int)std::min<uint64_t>(g, (a.n + dev::kBlock - 1) / dev::kBlock);
+  kernel<<<g, dev::kBlock, 0, stream>>>(a.m, a.bd, a.rays, a.n, a.side, a.sides, a.near_d, a.far_d, a.out, a.work,
+                                        a.refill);
+}
+
+template <int ORDER, bool BATCHED>
+static void launch_persistent_occ(const PersistentArgs& a, int occupancy, cudaStream_t stream) {
+  if (occupancy == 0) launch_persistent<ORDER, BATCHED, 1>(a, stream);
+  else if (occupancy == 1) launch_persistent<ORDER, BATCHED, 6>(a, stream);
+  else launch_persistent<ORDER, BATCHED, 8>(a, stream);
+}
+
+cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
+                                            int side, const SideTable& sides, float near_d, float far_d,
+                                            bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
+                                            cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
-  dev::raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
+  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return e;
+  PersistentArgs a{m, batch ? *batch : BatchDev{nullptr, nullptr, 0}, rays, n, side, sides, near_d, far_d, out,
+                   work, cfg.refill};
+  if (batch) {
+    if (cfg.order == 0) launch_persistent_occ<0, true>(a, cfg.occupancy, stream);
+    else launch_persistent_occ<1, true>(a, cfg.occupancy, stream);
+  } else {
+    if (cfg.order == 0) launch_persistent_occ<0, false>(a, cfg.occupancy, stream);
+    else launch_persistent_occ<1, false>(a, cfg.occupancy, stream);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dev::finalize_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                                 float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if (order == 0)
+    dev::raycast_first_kernel<0><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
+  else
+    dev::raycast_first_kernel<1><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
   return cudaGetLastError();
 }
 

@@ -24,10 +24,32 @@ struct MeshDev {
 };
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
-                                 float near_d, float far_d, bvhc_hit* out, cudaStream_t stream);
+                                 float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream);
+// Traversal variant chosen per call (autotuned): persistent vs one-ray-per-thread grid, child
+// order, and the number of idle lanes that triggers a warp refill.
+struct TraversalConfig {
+  int persistent;  // 1: persistent warps with lane refill; 0: one ray per thread
+  int order;       // 0: split-axis direction sign (reference order); 1: nearest entry first
+  int refill;      // idle lanes (1..32) that trigger a refill in the persistent form
+  int occupancy;   // persistent form register budget: 0 compiler's choice, 1 six blocks/SM, 2 eight
+};
+
+// Many meshes in one node/triangle pool: rays [ray_off[k], ray_off[k+1]) belong to mesh k, whose
+// roots are MeshDev::roots[mesh_root_off[k] .. mesh_root_off[k+1]).
+struct BatchDev {
+  const uint64_t* ray_off;        // n_meshes + 1 entries
+  const uint32_t* mesh_root_off;  // n_meshes + 1 entries
+  int n_meshes;
+};
+
+// `batch` null: one mesh (all of m.roots).  The work counter `work` is reset on `stream` first.
+cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
+                                            int side, const SideTable& sides, float near_d, float far_d,
+                                            bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
+                                            cudaStream_t stream);
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 

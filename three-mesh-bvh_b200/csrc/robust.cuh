@@ -202,6 +202,60 @@ __device__ __forceinline__ bool tri_hit(float3 a, float3 b, float3 c, float3 o, 
 // t = -T / N in float-float, for a triangle already known to be hit.
 __device__ __forceinline__ ff tri_t_ff(const TriFF& r) { return ff_div(ff_neg(r.T), r.N); }
 
+constexpr float kTinyRel = 9.094947017729282e-13f;  // 2^-40: relative error of a float-float t
+
+__device__ __noinline__ bool tri_hit_slow_t(float3 a, float3 b, float3 c, float3 o, float3 d, int side, float& t,
+                                            float& t_err) {
+  TriFF r = tri_eval_ff(a, b, c, o, d);
+  if (!tri_decide_ff(r, side)) return false;
+  ff tt = tri_t_ff(r);
+  t = tt.hi;
+  t_err = fabsf(tt.hi) * kTinyRel + 1e-30f;
+  return true;
+}
+
+// tri_hit, and on a hit the ray parameter t = -T / N with an absolute error bound `t_err`: from
+// the float32 values (relative error <= bT/|T| + bN/|N| + 4u) when the filter settled every sign,
+// otherwise from the float-float evaluation.
+__device__ __forceinline__ bool tri_hit_t(float3 a, float3 b, float3 c, float3 o, float3 d, float d_l1, int side,
+                                          float& t, float& t_err) {
+  const float kB = 1.9073486328125e-06f;  // 2^-19
+  float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
+  float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
+  float nx = e1y * e2z - e1z * e2y;
+  float ny = e1z * e2x - e1x * e2z;
+  float nz = e1x * e2y - e1y * e2x;
+  float N = d.x * nx + d.y * ny + d.z * nz;
+  float m1 = max3abs(e1x, e1y, e1z), m2 = max3abs(e2x, e2y, e2z);
+  float bN = kB * d_l1 * m1 * m2;
+  if (!(fabsf(N) > bN)) return tri_hit_slow_t(a, b, c, o, d, side, t, t_err);
+  if (N > 0.0f ? side == kSideFront : side == kSideBack) return false;
+  float qx = o.x - a.x, qy = o.y - a.y, qz = o.z - a.z;
+  float mq = max3abs(qx, qy, qz);
+  float s = N > 0.0f ? 1.0f : -1.0f;
+  float ux = qy * e2z - qz * e2y, uy = qz * e2x - qx * e2z, uz = qx * e2y - qy * e2x;
+  float U = s * (d.x * ux + d.y * uy + d.z * uz);
+  float bU = kB * d_l1 * mq * m2;
+  if (U < -bU) return false;
+  float vx = e1y * qz - e1z * qy, vy = e1z * qx - e1x * qz, vz = e1x * qy - e1y * qx;
+  float V = s * (d.x * vx + d.y * vy + d.z * vz);
+  float bV = kB * d_l1 * m1 * mq;
+  if (V < -bV) return false;
+  float aN = fabsf(N);
+  float W = aN - U - V;
+  float bW = bN + bU + bV + 2.384185791015625e-07f * (aN + fabsf(U) + fabsf(V));
+  if (W < -bW) return false;
+  float T = -s * (qx * nx + qy * ny + qz * nz);
+  float bT = kB * (fabsf(qx) + fabsf(qy) + fabsf(qz)) * m1 * m2;
+  if (T < -bT) return false;
+  if (U > bU && V > bV && W > bW && T > bT) {
+    t = T / aN;
+    t_err = t * (bT / T + bN / aN + 2.384185791015625e-07f);
+    return true;
+  }
+  return tri_hit_slow_t(a, b, c, o, d, side, t, t_err);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Closest point on a triangle (Ericson, Real-Time Collision Detection, 5.1.5), evaluated in the
 // local frame of vertex a so that rounding scales with the triangle and the query distance

@@ -200,6 +200,16 @@ class MeshBVH:
         N.check(N.lib().bvhc_mesh_get_info(self._device_mesh(), C.byref(info)), "bvhc_mesh_get_info")
         return {k: getattr(info, k) for k, _ in N.BvhcMeshInfo._fields_}
 
+    def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0) -> None:
+        """Select the raycastFirst traversal variant (see bvhc_mesh_set_traversal)."""
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy)
+        N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
+
+    def get_traversal(self) -> dict:
+        cfg = N.BvhcTraversalConfig()
+        N.check(N.lib().bvhc_mesh_get_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_get_traversal")
+        return {k: getattr(cfg, k) for k, _ in N.BvhcTraversalConfig._fields_}
+
     def dispose(self):
         if self._mesh is not None:
             N.lib().bvhc_mesh_destroy(self._mesh)
