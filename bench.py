@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", choices=["first", "batched"], default="first",
+                    help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form")
+    ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
     ap.add_argument("--radial", type=int, default=500)
     ap.add_argument("--rays-log2", type=int, default=24)
@@ -339,9 +342,82 @@ def run_engine(args, ws, rank, local):
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
                 "traversal": bvh.get_traversal(), "autotune": tuned,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps * len(sets)}
+                "gpu_launches": args.steps * sum(2 if (c is None or c[0] == 1) else 1 for c in configs)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
+
+
+def run_batched(args, ws, rank, local):
+    """BatchedMesh form (1024 sub-geometries, log-uniform 200..200,000 triangles and 1,000..1,000,000
+    rays each): one graph-captured persistent launch versus one plain launch per geometry."""
+    import torch
+
+    import __graft_entry__ as ge
+    from three_mesh_bvh_b200.batched import BatchedMeshBVH
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geoms, _, rays, off = pkg.batched_scene(n_geometries=args.batch_meshes, seed=2)
+    batch = BatchedMeshBVH(geoms, {"strategy": pkg.SAH, "maxLeafSize": 10}, threads=os.cpu_count())
+    n = rays.shape[0]
+    d_rays = torch.from_numpy(rays).to(dev)
+    out = torch.empty((n, 8), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / steps
+
+    # autotune the batched launch over the traversal variants
+    from three_mesh_bvh_b200.autotune import CANDIDATES
+
+    timings = {}
+    for cand in CANDIDATES:
+        batch.set_traversal(*cand)
+        timings[str(list(cand))] = timed(lambda: batch.raycast_first(d_rays, off, out=out, stream=s), 1, 1)
+    best = min(CANDIDATES, key=lambda c: timings[str(list(c))])
+    batch.set_traversal(*best)
+    graph = batch.capture(d_rays, off, out)
+    with ClockSampler(local) as clk:
+        ms_graph = timed(lambda: graph.launch(s), args.steps, args.warmup)
+    batch.synchronize(s)
+    ref_out = out.clone()
+    # per-geometry launches: plain one-ray-per-thread kernel (same child order), and persistent
+    batch.set_traversal(0, best[1], 16, 0)
+    ms_plain = timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s), max(1, args.steps // 2), 1)
+    batch.synchronize(s)
+    same_plain = bool(torch.equal(out.view(torch.int32)[:, 0], ref_out.view(torch.int32)[:, 0]))
+    batch.set_traversal(*best)
+    ms_pers = timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s), max(1, args.steps // 2), 1)
+    batch.synchronize(s)
+    if rank == 0:
+        line = {"metric": "Mrays/s batched raycastFirst (1024 meshes)", "value": n / (ms_graph / 1e3) / 1e6,
+                "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"{args.batch_meshes} geometries alternating TorusKnot / Icosahedron, "
+                                       "triangles log-uniform 200..200000, rays log-uniform 1e3..1e6 per geometry "
+                                       "(seed 2), SAH leaf 10; one CUDA-graph persistent launch",
+                           "triangles": int(batch.triangle_base[-1]), "rays_per_step": int(n)},
+                "per_mesh_plain_launches": {"ms": ms_plain, "mrays_s": n / (ms_plain / 1e3) / 1e6,
+                                            "same_face_indices": same_plain},
+                "per_mesh_persistent_launches": {"ms": ms_pers, "mrays_s": n / (ms_pers / 1e3) / 1e6},
+                "speedup_vs_per_mesh_plain": ms_plain / ms_graph, "traversal": list(best),
+                "autotune_ms": timings, "clocks": clk.summary(),
+                "gpu_launches": args.steps * (2 if best[0] == 1 else 1)}
+        print(json.dumps(line), flush=True)
+    graph.destroy()
+    batch.dispose()
 
 
 def main():
@@ -350,6 +426,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.workload == "batched":
+            run_batched(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:

@@ -175,6 +175,61 @@ bvhc_status bvhc_raycast_materials(bvhc_mesh* mesh, const float* rays, uint64_t 
                                    int n_materials, float near_dist, float far_dist, uint32_t cap, uint32_t* counts,
                                    bvhc_hit* hits, int mem, void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched meshes: the bounds trees of a BatchedMesh (computeBatchedBoundsTree,
+ * src/utils/ExtensionUtilities.js:216-268): one MeshBVH per geometry, all over one shared index
+ * and position buffer (each built with `range` = its draw range, so leaf offsets are absolute
+ * triangle indices).  bvhc_batch_create packs them into one device pool; the result is a
+ * bvhc_mesh whose roots are grouped per geometry (roots_per_mesh[k] roots of geometry k, taken in
+ * order from roots / root_bytes).  Replaces the per-instance serial raycast loop of
+ * acceleratedBatchedMeshRaycast (ExtensionUtilities.js:87-161) for rays already in each
+ * geometry's local frame.
+ */
+bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per_mesh, const void* const* roots,
+                              const uint64_t* root_bytes, const void* index, int index_elem_bytes,
+                              uint64_t index_count, const float* positions, uint64_t n_verts, int stride_floats,
+                              bvhc_mesh** out);
+int bvhc_batch_mesh_count(const bvhc_mesh* batch);
+/* raycastFirst for every geometry's rays in ONE persistent launch: rays (device memory) of
+ * geometry k are rows [ray_offsets[k], ray_offsets[k+1]) (host array of n_meshes + 1 entries,
+ * ray_offsets[0] = 0); results land in the same rows of out (device memory). */
+bvhc_status bvhc_batch_raycast_first(bvhc_mesh* batch, const float* rays, const uint64_t* ray_offsets, int side,
+                                     float near_dist, float far_dist, bvhc_hit* out, void* stream);
+/* The same work as one launch per geometry, back to back on `stream` (the comparison baseline). */
+bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* batch, const float* rays, const uint64_t* ray_offsets,
+                                              int side, float near_dist, float far_dist, bvhc_hit* out,
+                                              void* stream);
+/* Captures bvhc_batch_raycast_first on fixed device buffers into a CUDA graph (work-counter reset,
+ * persistent traversal, finalize); bvhc_graph_launch replays it on `stream`. */
+typedef struct bvhc_graph bvhc_graph;
+bvhc_status bvhc_batch_graph_create(bvhc_mesh* batch, const float* rays, const uint64_t* ray_offsets, int side,
+                                    float near_dist, float far_dist, bvhc_hit* out, bvhc_graph** graph);
+bvhc_status bvhc_graph_launch(bvhc_graph* graph, void* stream);
+void bvhc_graph_destroy(bvhc_graph* graph);
+
+/* ---------------------------------------------------------------------------------------------
+ * Gradients (no reference counterpart: the forward values are the reference's raycastFirst and
+ * closestPointToPoint results; the backward differentiates the same formulas).  All buffers are
+ * device memory; work is enqueued on `stream`.
+ */
+/* Uploads the geometry's triangle -> vertex map and positions, which the backward passes use to
+ * replay each query's recorded triangle and to address vertex gradients. */
+bvhc_status bvhc_mesh_enable_gradients(bvhc_mesh* mesh, const void* index, int index_elem_bytes, uint64_t index_count,
+                                       const float* positions, uint64_t n_verts, int stride_floats);
+/* Backward of raycastFirst: rays (n x 6) and the forward's hits; grad_distance (n, nullable) and
+ * grad_barycoord (n x 3, nullable) are dL/d(distance) and dL/d(barycoord).  grad_vertices
+ * (n_verts x 3) is ACCUMULATED into (the caller zeroes it); grad_origins / grad_directions (n x 3)
+ * are written; any output may be NULL.  Misses contribute nothing. */
+bvhc_status bvhc_raycast_first_backward(bvhc_mesh* mesh, const float* rays, const bvhc_hit* hits, uint64_t n,
+                                        const float* grad_distance, const float* grad_barycoord, float* grad_vertices,
+                                        float* grad_origins, float* grad_directions, void* stream);
+/* Backward of closestPointToPoint's distance: points (n x 3), the forward's results,
+ * grad_distance (n).  grad_vertices accumulated, grad_points (n x 3) written; zero for null results
+ * and for points on the surface (distance 0). */
+bvhc_status bvhc_closest_point_backward(bvhc_mesh* mesh, const float* points, const bvhc_closest* results, uint64_t n,
+                                        const float* grad_distance, float* grad_vertices, float* grad_points,
+                                        void* stream);
+
 /* MeshBVH#closestPointToPoint(point, target, minThreshold, maxThreshold) for every point
  * (src/core/MeshBVH.js:874-884, src/core/cast/closestPointToPoint.js:6-78). */
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* mesh, const float* points, uint64_t n, float min_threshold,

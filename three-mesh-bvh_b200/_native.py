@@ -52,6 +52,13 @@ SIGNATURES = [
     ("bvhc_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
     ("bvhc_closest_point_to_point", _I, [_P, _P, _U64, _F, _F, _P, _I, _P]),
     ("bvhc_mesh_set_groups", _I, [_P, _P, _I]),
+    ("bvhc_batch_create", _I, [_I, _I, _P, _P, _P, _P, _I, _U64, _P, _U64, _I, C.POINTER(_P)]),
+    ("bvhc_batch_mesh_count", _I, [_P]),
+    ("bvhc_batch_raycast_first", _I, [_P, _P, _P, _I, _F, _F, _P, _P]),
+    ("bvhc_batch_raycast_first_per_mesh", _I, [_P, _P, _P, _I, _F, _F, _P, _P]),
+    ("bvhc_batch_graph_create", _I, [_P, _P, _P, _I, _F, _F, _P, C.POINTER(_P)]),
+    ("bvhc_graph_launch", _I, [_P, _P]),
+    ("bvhc_graph_destroy", None, [_P]),
     ("bvhc_mesh_set_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_mesh_get_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),

@@ -1,0 +1,155 @@
+"""Batched meshes: the bounds trees of a BatchedMesh served by one persistent GPU launch.
+
+Mirrors `computeBatchedBoundsTree` (src/utils/ExtensionUtilities.js:216-268): one MeshBVH per
+geometry over one shared index/position buffer, each built over its own draw range so that its
+leaf offsets are absolute triangle indices of the shared index.  Each geometry's BVH is built on
+its own (in parallel host threads; the build releases the GIL), then merged into the shared
+buffers: vertex indices move by the geometry's first vertex and leaf offsets by its first
+triangle (`shiftTriangleOffsets`, src/core/BVH.js:146-190).  The tree of every geometry is the one
+a build over the shared geometry with `range` produces, because the build only sees the
+triangles of the range, in the same order.
+
+`raycast_first` replaces the per-instance serial loop of acceleratedBatchedMeshRaycast
+(ExtensionUtilities.js:87-161) for rays already expressed in each geometry's local frame.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+from . import _native as N
+from .geometry import Geometry, index_dtype
+from .mesh_bvh import FrontSide, MeshBVH, _side_of
+
+
+def shift_triangle_offsets(root: bytes, offset: int) -> bytes:
+    """Adds `offset` to every leaf's triangle offset of a serialized root (BVH.js:146-190)."""
+    u32 = np.frombuffer(root, dtype=np.uint32).reshape(-1, 8).copy()
+    leaf = (u32[:, 7] >> 16) == 0xFFFF
+    u32[leaf, 6] += np.uint32(offset)
+    return u32.tobytes()
+
+
+class BatchedMeshBVH:
+    def __init__(self, geometries: list[Geometry], options: dict | None = None, *, device: int = 0,
+                 threads: int | None = None):
+        self.device = device
+        opts = dict(options or {})
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            bvhs = list(ex.map(lambda g: MeshBVH(g, opts, device=device), geometries))
+        self.geometries = geometries
+        vbase = np.cumsum([0] + [g.position.shape[0] for g in geometries])
+        tbase = np.cumsum([0] + [g.triangle_count for g in geometries])
+        self.vertex_base = vbase
+        self.triangle_base = tbase
+        self.position = np.ascontiguousarray(np.concatenate([g.position for g in geometries]), dtype=np.float32)
+        dt = index_dtype(int(vbase[-1]))
+        self.index = np.concatenate([g.index.astype(np.int64) + vbase[k] for k, g in enumerate(geometries)]).astype(dt)
+        self.roots = []
+        self.roots_per_mesh = []
+        for k, b in enumerate(bvhs):
+            rs = [shift_triangle_offsets(r, int(tbase[k])) for r in b._roots]
+            self.roots.extend(rs)
+            self.roots_per_mesh.append(len(rs))
+            b.dispose()
+        self._mesh = None
+        self._graphs = []
+
+    @property
+    def n_meshes(self) -> int:
+        return len(self.roots_per_mesh)
+
+    def _device_mesh(self):
+        if self._mesh is None:
+            lib = N.lib()
+            bufs = [np.frombuffer(r, dtype=np.uint8) for r in self.roots]
+            ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+            sizes = (C.c_uint64 * len(bufs))(*[b.size for b in bufs])
+            rpm = np.asarray(self.roots_per_mesh, dtype=np.int32)
+            out = C.c_void_p()
+            st = lib.bvhc_batch_create(self.device, self.n_meshes, rpm.ctypes.data, ptrs, sizes, self.index.ctypes.data,
+                                       self.index.dtype.itemsize, self.index.size, self.position.ctypes.data,
+                                       self.position.shape[0], 3, C.byref(out))
+            N.check(st, "bvhc_batch_create")
+            self._mesh = out
+        return self._mesh
+
+    def set_traversal(self, persistent=1, order=1, refill=16, occupancy=0):
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy)
+        N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
+
+    @staticmethod
+    def _offsets(ray_offsets) -> np.ndarray:
+        return np.ascontiguousarray(ray_offsets, dtype=np.uint64)
+
+    def raycast_first(self, rays, ray_offsets, side=FrontSide, near=0.0, far=float("inf"), out=None, stream=None):
+        """One persistent launch over every geometry's rays.  rays: torch CUDA tensor (n, 6) whose
+        rows [ray_offsets[k], ray_offsets[k+1]) are geometry k's rays in its local frame; returns an
+        (n, 8) float32 tensor of bvhc_hit records, faceIndex in the shared index."""
+        import torch
+
+        off = self._offsets(ray_offsets)
+        if out is None:
+            out = torch.empty((rays.shape[0], 8), dtype=torch.float32, device=rays.device)
+        s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+        N.check(N.lib().bvhc_batch_raycast_first(self._device_mesh(), rays.data_ptr(), off.ctypes.data,
+                                                 _side_of(side), float(near), float(far), out.data_ptr(), s),
+                "bvhc_batch_raycast_first")
+        return out
+
+    def raycast_first_per_mesh(self, rays, ray_offsets, side=FrontSide, near=0.0, far=float("inf"), out=None,
+                               stream=None):
+        """The same work as one launch per geometry (the comparison baseline)."""
+        import torch
+
+        off = self._offsets(ray_offsets)
+        if out is None:
+            out = torch.empty((rays.shape[0], 8), dtype=torch.float32, device=rays.device)
+        s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+        N.check(N.lib().bvhc_batch_raycast_first_per_mesh(self._device_mesh(), rays.data_ptr(), off.ctypes.data,
+                                                          _side_of(side), float(near), float(far), out.data_ptr(), s),
+                "bvhc_batch_raycast_first_per_mesh")
+        return out
+
+    def capture(self, rays, ray_offsets, out, side=FrontSide, near=0.0, far=float("inf")):
+        """CUDA graph of the batched launch on these fixed buffers; call .launch(stream) to replay."""
+        off = self._offsets(ray_offsets)
+        g = C.c_void_p()
+        N.check(N.lib().bvhc_batch_graph_create(self._device_mesh(), rays.data_ptr(), off.ctypes.data, _side_of(side),
+                                                float(near), float(far), out.data_ptr(), C.byref(g)),
+                "bvhc_batch_graph_create")
+        graph = _Graph(g)
+        self._graphs.append(graph)
+        return graph
+
+    def synchronize(self, stream=None):
+        N.check(N.lib().bvhc_mesh_synchronize(self._device_mesh(), stream), "bvhc_mesh_synchronize")
+
+    def dispose(self):
+        for g in self._graphs:
+            g.destroy()
+        self._graphs = []
+        if self._mesh is not None:
+            N.lib().bvhc_mesh_destroy(self._mesh)
+            self._mesh = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+class _Graph:
+    def __init__(self, handle):
+        self.h = handle
+
+    def launch(self, stream=None):
+        N.check(N.lib().bvhc_graph_launch(self.h, stream), "bvhc_graph_launch")
+
+    def destroy(self):
+        if self.h:
+            N.lib().bvhc_graph_destroy(self.h)
+            self.h = None

@@ -43,6 +43,15 @@ struct bvhc_mesh {
   void* slot_in[2] = {nullptr, nullptr};
   void* slot_out[2] = {nullptr, nullptr};
   unsigned long long* d_work2 = nullptr;
+  // batched meshes (bvhc_batch_create): mesh k owns roots [mesh_root_off[k], mesh_root_off[k+1])
+  int n_meshes = 0;
+  std::vector<uint32_t> mesh_root_off;
+  uint32_t* d_mesh_root_off = nullptr;
+  uint64_t* d_ray_off = nullptr;   // per-call ray offsets (n_meshes + 1)
+  // gradient support (bvhc_mesh_enable_gradients): triangle -> vertex ids and compact positions
+  uint32_t* d_index32 = nullptr;
+  float* d_pos = nullptr;
+  uint64_t grad_tris = 0, grad_verts = 0;
 
   MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
 };
@@ -232,6 +241,40 @@ void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_
 
 }  // namespace
 
+// Uploads converted records and allocates the per-mesh device state.  mesh_root_off is empty for a
+// single mesh, or the n_meshes + 1 root offsets of a batch.
+static bvhc_status finish_mesh(int device, const std::vector<PairNode>& pairs, const std::vector<TriRecord>& tris,
+                               const std::vector<uint32_t>& root_links, int max_depth,
+                               const std::vector<uint32_t>& mesh_root_off, bvhc_mesh** out) {
+  auto* m = new bvhc_mesh();
+  m->device = device;
+  m->n_nodes = pairs.size();
+  m->n_tris = tris.size();
+  m->n_roots = (int)root_links.size();
+  m->max_depth = max_depth;
+  m->rec_face.resize(tris.size());
+  for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
+  m->mesh_root_off = mesh_root_off;
+  m->n_meshes = mesh_root_off.empty() ? 0 : (int)mesh_root_off.size() - 1;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = upload(&m->d_nodes, pairs);
+  if (e == cudaSuccess) e = upload(&m->d_tris, tris);
+  if (e == cudaSuccess) e = upload(&m->d_roots, root_links);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_err), sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_work), sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(m->d_err, 0, sizeof(unsigned int));
+  if (e == cudaSuccess && m->n_meshes > 0) {
+    e = upload(&m->d_mesh_root_off, mesh_root_off);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_ray_off), mesh_root_off.size() * 8);
+  }
+  if (e != cudaSuccess) {
+    bvhc_mesh_destroy(m);
+    return from_cuda(e);
+  }
+  *out = m;
+  return BVHC_OK;
+}
+
 extern "C" {
 
 const char* bvhc_status_string(bvhc_status s) {
@@ -354,27 +397,55 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
   } catch (const std::bad_alloc&) {
     return BVHC_ERR_OUT_OF_MEMORY;
   }
-  auto* m = new bvhc_mesh();
-  m->device = device;
-  m->n_nodes = pairs.size();
-  m->n_tris = tris.size();
-  m->n_roots = n_roots;
-  m->max_depth = max_depth;
-  m->rec_face.resize(tris.size());
-  for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
-  cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = upload(&m->d_nodes, pairs);
-  if (e == cudaSuccess) e = upload(&m->d_tris, tris);
-  if (e == cudaSuccess) e = upload(&m->d_roots, root_links);
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_err), sizeof(unsigned int));
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&m->d_work), sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemset(m->d_err, 0, sizeof(unsigned int));
-  if (e != cudaSuccess) {
-    bvhc_mesh_destroy(m);
-    return from_cuda(e);
+  return finish_mesh(device, pairs, tris, root_links, max_depth, {}, out);
+}
+
+bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per_mesh, const void* const* roots,
+                              const uint64_t* root_bytes, const void* index, int index_elem_bytes,
+                              uint64_t index_count, const float* positions, uint64_t n_verts, int stride_floats,
+                              bvhc_mesh** out) {
+  if (!out || n_meshes <= 0 || !roots_per_mesh || !roots || !root_bytes || !positions || stride_floats < 3 ||
+      n_verts == 0)
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (index && index_elem_bytes != 2 && index_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  std::vector<PairNode> pairs;
+  std::vector<TriRecord> tris;
+  std::vector<uint32_t> root_links;
+  std::vector<uint32_t> mesh_root_off{0};
+  int max_depth = 0;
+  try {
+    int r = 0;
+    for (int k = 0; k < n_meshes; ++k) {
+      if (roots_per_mesh[k] <= 0) return BVHC_ERR_INVALID_ARGUMENT;
+      for (int j = 0; j < roots_per_mesh[k]; ++j, ++r) {
+        if (!roots[r] || root_bytes[r] == 0 || root_bytes[r] % 32 != 0) return BVHC_ERR_INVALID_BVH;
+        Converter c(pairs, tris);
+        c.buf = static_cast<const uint8_t*>(roots[r]);
+        c.n_nodes = root_bytes[r] / 32;
+        c.version = 1;
+        c.index = index;
+        c.index_elem = index_elem_bytes;
+        c.index_count = index_count;
+        c.indirect = nullptr;
+        c.indirect_elem = 0;
+        c.indirect_count = 0;
+        c.pos = positions;
+        c.n_verts = n_verts;
+        c.stride = stride_floats;
+        c.tri_count = index ? index_count / 3 : n_verts / 3;
+        c.n_prims = c.tri_count;
+        root_links.push_back(c.convert(0, 0));
+        max_depth = std::max(max_depth, c.max_depth);
+      }
+      mesh_root_off.push_back((uint32_t)root_links.size());
+    }
+  } catch (const Status& s) {
+    return s.code;
+  } catch (const std::bad_alloc&) {
+    return BVHC_ERR_OUT_OF_MEMORY;
   }
-  *out = m;
-  return BVHC_OK;
+  return finish_mesh(device, pairs, tris, root_links, max_depth, mesh_root_off, out);
 }
 
 void bvhc_mesh_destroy(bvhc_mesh* m) {
@@ -394,6 +465,10 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
     if (m->pipe[k]) cudaStreamDestroy(m->pipe[k]);
   }
   cudaFree(m->d_work2);
+  cudaFree(m->d_mesh_root_off);
+  cudaFree(m->d_ray_off);
+  cudaFree(m->d_index32);
+  cudaFree(m->d_pos);
   delete m;
 }
 
@@ -419,6 +494,15 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
     return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
                                            s);
   return launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
+}
+
+// raycastFirst over one mesh of a batch (view = that mesh's roots), with the batch's variant.
+static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* rays, uint64_t n, int side,
+                                 float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
+  if (m->cfg.persistent)
+    return launch_raycast_first_persistent(v, nullptr, rays, n, side, single_side(), near_d, far_d, out, m->d_work,
+                                           m->cfg, s);
+  return launch_raycast_first(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order, s);
 }
 
 // Streams, staging slots and the second work counter of the pipelined host-memory path.
@@ -597,6 +681,156 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
                                      static_cast<bvhc_closest*>(m->d_out), s));
   BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched meshes
+// ---------------------------------------------------------------------------------------------
+static bool valid_offsets(const bvhc_mesh* m, const uint64_t* ray_offsets) {
+  if (!ray_offsets || ray_offsets[0] != 0) return false;
+  for (int k = 0; k < m->n_meshes; ++k)
+    if (ray_offsets[k + 1] < ray_offsets[k]) return false;
+  return true;
+}
+
+bvhc_status bvhc_batch_raycast_first(bvhc_mesh* m, const float* rays, const uint64_t* ray_offsets, int side,
+                                     float near_d, float far_d, bvhc_hit* out, void* stream) {
+  if (!m || m->n_meshes <= 0 || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || !valid_offsets(m, ray_offsets))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  uint64_t n = ray_offsets[m->n_meshes];
+  if (n == 0) return BVHC_OK;
+  if (!rays || !out || !aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_ray_off, ray_offsets, (m->n_meshes + 1) * 8, cudaMemcpyHostToDevice, s));
+  BatchDev bd{m->d_ray_off, m->d_mesh_root_off, m->n_meshes};
+  return from_cuda(launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d, out,
+                                                   m->d_work, m->cfg, s));
+}
+
+bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* m, const float* rays, const uint64_t* ray_offsets, int side,
+                                              float near_d, float far_d, bvhc_hit* out, void* stream) {
+  if (!m || m->n_meshes <= 0 || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE || !valid_offsets(m, ray_offsets))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (ray_offsets[m->n_meshes] == 0) return BVHC_OK;
+  if (!rays || !out || !aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  for (int k = 0; k < m->n_meshes; ++k) {
+    uint64_t off = ray_offsets[k], cnt = ray_offsets[k + 1] - off;
+    if (cnt == 0) continue;
+    MeshDev v = m->view();
+    v.roots = m->d_roots + m->mesh_root_off[k];
+    v.n_roots = (int)(m->mesh_root_off[k + 1] - m->mesh_root_off[k]);
+    BVHC_CUDA_TRY(dispatch_view(m, v, rays + 6 * off, cnt, side, near_d, far_d, out + off, s));
+  }
+  return BVHC_OK;
+}
+
+struct bvhc_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+bvhc_status bvhc_batch_graph_create(bvhc_mesh* m, const float* rays, const uint64_t* ray_offsets, int side,
+                                    float near_d, float far_d, bvhc_hit* out, bvhc_graph** graph) {
+  if (!m || !graph || m->n_meshes <= 0 || side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE ||
+      !valid_offsets(m, ray_offsets))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  uint64_t n = ray_offsets[m->n_meshes];
+  if (n == 0 || !rays || !out || !aligned(rays, 8) || !aligned(out, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+  *graph = nullptr;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  // the offsets are part of the captured work: copy them once, before capture
+  BVHC_CUDA_TRY(cudaMemcpy(m->d_ray_off, ray_offsets, (m->n_meshes + 1) * 8, cudaMemcpyHostToDevice));
+  cudaStream_t cs;
+  BVHC_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  auto* g = new bvhc_graph();
+  g->device = m->device;
+  BatchDev bd{m->d_ray_off, m->d_mesh_root_off, m->n_meshes};
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t le = launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d,
+                                                     out, m->d_work, m->cfg, cs);
+    e = cudaStreamEndCapture(cs, &g->graph);
+    if (le != cudaSuccess) e = le;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    bvhc_graph_destroy(g);
+    return from_cuda(e);
+  }
+  *graph = g;
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_graph_launch(bvhc_graph* g, void* stream) {
+  if (!g || !g->exec) return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(g->device));
+  return from_cuda(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)));
+}
+
+void bvhc_graph_destroy(bvhc_graph* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+}
+
+int bvhc_batch_mesh_count(const bvhc_mesh* m) { return m ? m->n_meshes : 0; }
+
+// ---------------------------------------------------------------------------------------------
+// Gradients
+// ---------------------------------------------------------------------------------------------
+bvhc_status bvhc_mesh_enable_gradients(bvhc_mesh* m, const void* index, int index_elem_bytes, uint64_t index_count,
+                                       const float* positions, uint64_t n_verts, int stride_floats) {
+  if (!m || !positions || n_verts == 0 || stride_floats < 3) return BVHC_ERR_INVALID_ARGUMENT;
+  if (index && index_elem_bytes != 2 && index_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
+  uint64_t n_tris = index ? index_count / 3 : n_verts / 3;
+  std::vector<uint32_t> idx(n_tris * 3);
+  for (uint64_t i = 0; i < n_tris * 3; ++i) {
+    idx[i] = index ? read_index(index, index_elem_bytes, i) : (uint32_t)i;
+    if (idx[i] >= n_verts) return BVHC_ERR_INVALID_ARGUMENT;
+  }
+  std::vector<float> pos(n_verts * 3);
+  for (uint64_t v = 0; v < n_verts; ++v)
+    for (int k = 0; k < 3; ++k) pos[3 * v + k] = positions[v * (uint64_t)stride_floats + k];
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  cudaFree(m->d_index32);
+  cudaFree(m->d_pos);
+  m->d_index32 = nullptr;
+  m->d_pos = nullptr;
+  BVHC_CUDA_TRY(upload(&m->d_index32, idx));
+  BVHC_CUDA_TRY(upload(&m->d_pos, pos));
+  m->grad_tris = n_tris;
+  m->grad_verts = n_verts;
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_raycast_first_backward(bvhc_mesh* m, const float* rays, const bvhc_hit* hits, uint64_t n,
+                                        const float* grad_distance, const float* grad_barycoord, float* grad_vertices,
+                                        float* grad_origins, float* grad_directions, void* stream) {
+  if (!m || !m->d_index32) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!rays || !hits || (!grad_distance && !grad_barycoord)) return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  return from_cuda(launch_raycast_first_backward(m->d_index32, m->d_pos, rays, hits, n, grad_distance, grad_barycoord,
+                                                 grad_vertices, grad_origins, grad_directions,
+                                                 static_cast<cudaStream_t>(stream)));
+}
+
+bvhc_status bvhc_closest_point_backward(bvhc_mesh* m, const float* points, const bvhc_closest* results, uint64_t n,
+                                        const float* grad_distance, float* grad_vertices, float* grad_points,
+                                        void* stream) {
+  if (!m || !m->d_index32) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!points || !results || !grad_distance) return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  return from_cuda(launch_closest_point_backward(m->d_index32, m->d_pos, points, results, n, grad_distance,
+                                                 grad_vertices, grad_points, static_cast<cudaStream_t>(stream)));
 }
 
 }  // extern "C"

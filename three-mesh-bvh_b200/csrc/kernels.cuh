@@ -53,4 +53,12 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 
+// Adjoint kernels (adjoint.cu).  index: 3 uint32 per triangle; pos: 3 float per vertex.
+cudaError_t launch_raycast_first_backward(const uint32_t* index, const float* pos, const float* rays,
+                                          const bvhc_hit* hits, uint64_t n, const float* g_dist, const float* g_bary,
+                                          float* g_vert, float* g_orig, float* g_dir, cudaStream_t stream);
+cudaError_t launch_closest_point_backward(const uint32_t* index, const float* pos, const float* pts,
+                                          const bvhc_closest* res, uint64_t n, const float* g_dist, float* g_vert,
+                                          float* g_pts, cudaStream_t stream);
+
 }  // namespace bvhc

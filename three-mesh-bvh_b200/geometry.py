@@ -270,3 +270,49 @@ def grid_points(lo, hi, res, pad=0.1) -> np.ndarray:
     axes = [np.linspace(lo2[k], hi2[k], res) for k in range(3)]
     g = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
     return g.astype(np.float32)
+
+
+# ------------------------------------------------------------------------------------------
+# Batched scene: many sub-geometries of very uneven size, each with its own rays
+# ------------------------------------------------------------------------------------------
+
+def batched_scene(n_geometries=1024, tri_range=(200, 200_000), ray_range=(1_000, 1_000_000), seed=2,
+                  make_rays=True):
+    """Sub-geometries alternating torus knots (radius 10, tube 3) and subdivided icosahedra
+    (radius 10), triangle counts log-uniform in `tri_range`, each with a random rigid transform and
+    a log-uniform number of rays in `ray_range` drawn as for the 80,000-triangle knot (origins on
+    the r = 40 sphere, directions at uniform points of [-13, 13]^3) in its local frame.
+    Returns (geometries, transforms (n, 4, 4), rays (sum, 6) float32 or None, ray_offsets)."""
+    rng = np.random.default_rng(seed)
+    lo_t, hi_t = tri_range
+    lo_r, hi_r = ray_range
+    tri_target = np.exp(rng.uniform(math.log(lo_t), math.log(hi_t), n_geometries))
+    ray_counts = np.exp(rng.uniform(math.log(lo_r), math.log(hi_r), n_geometries)).astype(np.int64)
+    geoms = []
+    for k in range(n_geometries):
+        t = float(tri_target[k])
+        if k % 2 == 0:
+            radial = max(3, int(round(math.sqrt(t / 8))))
+            tubular = max(3, int(round(t / (2 * radial))))
+            geoms.append(torus_knot(10, 3, tubular, radial))
+        else:
+            detail = max(0, int(round(math.sqrt(t / 20))) - 1)
+            geoms.append(icosahedron(10.0, detail))
+    transforms = np.zeros((n_geometries, 4, 4))
+    for k in range(n_geometries):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        transforms[k, :3, :3] = rot
+        transforms[k, :3, 3] = rng.uniform(-200, 200, 3)
+        transforms[k, 3, 3] = 1
+    offsets = np.concatenate([[0], np.cumsum(ray_counts)]).astype(np.uint64)
+    rays = None
+    if make_rays:
+        rays = np.empty((int(offsets[-1]), 6), dtype=np.float32)
+        for k in range(n_geometries):
+            rays[int(offsets[k]):int(offsets[k + 1])] = rays_sphere_to_box(int(ray_counts[k]), seed=10_000 + k)
+    return geoms, transforms, rays, offsets
