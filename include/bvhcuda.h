@@ -39,7 +39,8 @@ typedef enum bvhc_status {
   BVHC_ERR_OUT_OF_MEMORY = 4,
   BVHC_ERR_DEVICE = 5,           /* a kernel set the device error word (e.g. stack overflow) */
   BVHC_ERR_UNSUPPORTED = 6,      /* valid input outside what this build supports */
-  BVHC_ERR_BUILD = 7             /* the CPU builder rejected the input */
+  BVHC_ERR_BUILD = 7,            /* the CPU builder rejected the input */
+  BVHC_ERR_SCRATCH_LIMIT = 8     /* request larger than bvhc_raycast_first_noalloc's fixed scratch */
 } bvhc_status;
 
 /* three.js side constants (FrontSide, BackSide, DoubleSide). */
@@ -206,6 +207,20 @@ bvhc_status bvhc_batch_graph_create(bvhc_mesh* batch, const float* rays, const u
                                     float near_dist, float far_dist, bvhc_hit* out, bvhc_graph** graph);
 bvhc_status bvhc_graph_launch(bvhc_graph* graph, void* stream);
 void bvhc_graph_destroy(bvhc_graph* graph);
+
+/* raycastFirst that allocates nothing.  No counterpart in the reference: it exists for callers
+ * that must not call cudaMalloc -- code inside someone else's fixed device-memory budget, a
+ * latency-critical thread where an allocation could stall or fail, or a host that allocates only
+ * at start-up.  Same arguments and results as bvhc_raycast_first (the persistent traversal with the
+ * mesh's order / refill / occupancy).  Its scratch (work counter, and device staging of host
+ * buffers) is a fixed 3.6 MB device array that each GPU loading the library holds until exit:
+ *   - host-memory calls take at most 65,536 rays; more returns BVHC_ERR_SCRATCH_LIMIT;
+ *   - device-memory calls are not size-limited;
+ *   - all calls share the array: calls that overlap on the GPU (other streams or threads) race;
+ *   - the first call on a device looks the array up on that device: make it before any stream
+ *     capture. */
+bvhc_status bvhc_raycast_first_noalloc(bvhc_mesh* mesh, const float* rays, uint64_t n, int side, float near_dist,
+                                       float far_dist, bvhc_hit* out, int mem, void* stream);
 
 /* ---------------------------------------------------------------------------------------------
  * Gradients (no reference counterpart: the forward values are the reference's raycastFirst and

@@ -59,6 +59,10 @@ SIGNATURES = [
     ("bvhc_batch_graph_create", _I, [_P, _P, _P, _I, _F, _F, _P, C.POINTER(_P)]),
     ("bvhc_graph_launch", _I, [_P, _P]),
     ("bvhc_graph_destroy", None, [_P]),
+    ("bvhc_mesh_enable_gradients", _I, [_P, _P, _I, _U64, _P, _U64, _I]),
+    ("bvhc_raycast_first_backward", _I, [_P, _P, _P, _U64, _P, _P, _P, _P, _P, _P]),
+    ("bvhc_closest_point_backward", _I, [_P, _P, _P, _U64, _P, _P, _P, _P]),
+    ("bvhc_raycast_first_noalloc", _I, [_P, _P, _U64, _I, _F, _F, _P, _I, _P]),
     ("bvhc_mesh_set_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_mesh_get_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),

@@ -241,6 +241,14 @@ void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_
 
 }  // namespace
 
+bool bvhc::mesh_launch_info(const bvhc_mesh* m, MeshDev* view, TraversalConfig* cfg, int* device) {
+  if (!m) return false;
+  *view = m->view();
+  *cfg = m->cfg;
+  *device = m->device;
+  return true;
+}
+
 // Uploads converted records and allocates the per-mesh device state.  mesh_root_off is empty for a
 // single mesh, or the n_meshes + 1 root offsets of a batch.
 static bvhc_status finish_mesh(int device, const std::vector<PairNode>& pairs, const std::vector<TriRecord>& tris,
@@ -287,6 +295,8 @@ const char* bvhc_status_string(bvhc_status s) {
     case BVHC_ERR_DEVICE: return "device-side error (traversal stack overflow)";
     case BVHC_ERR_UNSUPPORTED: return "unsupported input (tree deeper than the traversal stack, or too large)";
     case BVHC_ERR_BUILD: return "BVH build failed";
+    case BVHC_ERR_SCRATCH_LIMIT:
+      return "request exceeds the fixed scratch of bvhc_raycast_first_noalloc (at most 65536 host-memory rays)";
   }
   return "unknown status";
 }

@@ -53,6 +53,10 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 
+// What another translation unit needs to launch on a mesh: its device view, traversal variant and
+// device ordinal (defined in api.cu).  Returns false for a null mesh.
+bool mesh_launch_info(const bvhc_mesh* mesh, MeshDev* view, TraversalConfig* cfg, int* device);
+
 // Adjoint kernels (adjoint.cu).  index: 3 uint32 per triangle; pos: 3 float per vertex.
 cudaError_t launch_raycast_first_backward(const uint32_t* index, const float* pos, const float* rays,
                                           const bvhc_hit* hits, uint64_t n, const float* g_dist, const float* g_bary,
