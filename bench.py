@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched"], default="first",
+    ap.add_argument("--workload", choices=["first", "batched", "adjoint"], default="first",
                     help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
@@ -353,9 +353,10 @@ def run_batched(args, ws, rank, local):
     import torch
 
     import __graft_entry__ as ge
-    from three_mesh_bvh_b200.batched import BatchedMeshBVH
 
     pkg = ge.load_package()
+    from three_mesh_bvh_b200.batched import BatchedMeshBVH
+
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     geoms, _, rays, off = pkg.batched_scene(n_geometries=args.batch_meshes, seed=2)
@@ -420,6 +421,82 @@ def run_batched(args, ws, rank, local):
     batch.dispose()
 
 
+def run_adjoint(args, ws, rank, local):
+    """Differentiable depth and SDF on the 2M-triangle knot: forward raycastFirst of a 1024^2 camera
+    and backward of L = sum (t - t*)^2 (t* rendered from the mesh with vertices moved by N(0, 0.01),
+    seed 3); forward closestPointToPoint of a 128^3 grid and backward of sum distance."""
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10})
+    pert = geo.clone()
+    pert.position = pert.position + np.random.default_rng(3).normal(0, 0.01, pert.position.shape).astype(np.float32)
+    bvh_star = pkg.MeshBVH(pert, {"strategy": pkg.SAH, "maxLeafSize": 10})
+    rays = torch.from_numpy(pkg.rays_camera(1024, 1024)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    star = bvh_star.raycast_first_batch(rays, stream=s)
+    t_star = star[:, 1].clone()
+    star_hit = star[:, 0].view(torch.int32) != -1
+    gv = torch.zeros((geo.position.shape[0], 3), dtype=torch.float32, device=dev)
+    pts = torch.from_numpy(pkg.grid_points(geo.position.min(0), geo.position.max(0), 128)).to(dev)
+    ones = torch.ones(pts.shape[0], dtype=torch.float32, device=dev)
+
+    def fwd():
+        return bvh.raycast_first_batch(rays, stream=s)
+
+    def fwd_bwd():
+        hits = bvh.raycast_first_batch(rays, stream=s)
+        hit = (hits[:, 0].view(torch.int32) != -1) & star_hit
+        g = torch.where(hit, 2 * (hits[:, 1] - t_star), torch.zeros_like(t_star))
+        gv.zero_()
+        bvh.raycast_first_backward(rays, hits, g, grad_vertices=gv, stream=s)
+
+    def cp_fwd():
+        return bvh.closest_point_batch(pts, 0.0, 5.0, stream=s)
+
+    def cp_fwd_bwd():
+        res = bvh.closest_point_batch(pts, 0.0, 5.0, stream=s)
+        gv.zero_()
+        bvh.closest_point_backward(pts, res, ones, grad_vertices=gv, stream=s)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / args.steps
+
+    with ClockSampler(local) as clk:
+        ms_f, ms_fb = timed(fwd), timed(fwd_bwd)
+        ms_cf, ms_cfb = timed(cp_fwd), timed(cp_fwd_bwd)
+    bvh.synchronize(s)
+    if rank == 0:
+        line = {"metric": "fwd+bwd / fwd time, raycastFirst depth loss (2M tri, 1024^2 camera)",
+                "value": ms_fb / ms_f, "unit": "ratio", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_fb, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "TorusKnot(10,3,2000,500) + N(0,0.02) noise, SAH leaf 10; 1024^2 camera; "
+                                       "L = sum (t - t*)^2, t* from vertices + N(0,0.01) (seed 3); "
+                                       "128^3 grid closest point, max 5, L = sum distance"},
+                "raycast": {"fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f},
+                "closest_point": {"fwd_ms": ms_cf, "fwd_bwd_ms": ms_cfb, "ratio": ms_cfb / ms_cf},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    bvh.dispose()
+    bvh_star.dispose()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -428,6 +505,8 @@ def main():
             run_reference(args, ws, rank)
         elif args.workload == "batched":
             run_batched(args, ws, rank, local)
+        elif args.workload == "adjoint":
+            run_adjoint(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:

@@ -129,13 +129,16 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * thread.  order = 0 visits the near child by the sign of the ray direction on the split axis (the
  * reference's order), 1 by the smaller entry distance.  occupancy selects the persistent
  * kernel's register budget: 0 the compiler's choice, 1 at least six and 2 at least eight resident
- * 128-thread blocks per SM.  Results are the same for every variant (up to exact ties); the
- * autotuner picks the fastest per mesh and workload. */
+ * 128-thread blocks per SM.  compact = 1 (persistent form) first finishes, in one coalesced pass,
+ * the rays that miss every root's child boxes and traverses only the others.  Results are the
+ * same for every variant (up to exact ties); the autotuner picks the fastest per mesh and
+ * workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;
   int32_t order;
   int32_t refill;
   int32_t occupancy;
+  int32_t compact;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);

@@ -983,6 +983,65 @@ void orc_closest_point_triangle(const double* p, const double* a, const double* 
   out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
 
+// Gradient reference for the engine's adjoint kernels: the ray/triangle quantities of the Eberly
+// formula (N = d.(e1 x e2), U = d.(q x e2), V = d.(e1 x q), T = q.(e1 x e2), t = -T/N,
+// wb = U/N, wc = V/N, wa = 1 - wb - wc, distance = t |d|) evaluated on forward-mode dual numbers
+// carrying the 15 partials with respect to a, b, c, o, d.  Exact float64 derivatives, independent
+// of the engine's hand-written reverse mode.
+struct Dual {
+  double v;
+  double g[15];
+};
+static Dual dconst(double v) { Dual r{v, {}}; return r; }
+static Dual dvar(double v, int i) { Dual r{v, {}}; r.g[i] = 1; return r; }
+static Dual operator+(const Dual& a, const Dual& b) { Dual r{a.v + b.v, {}}; for (int i = 0; i < 15; ++i) r.g[i] = a.g[i] + b.g[i]; return r; }
+static Dual operator-(const Dual& a, const Dual& b) { Dual r{a.v - b.v, {}}; for (int i = 0; i < 15; ++i) r.g[i] = a.g[i] - b.g[i]; return r; }
+static Dual operator*(const Dual& a, const Dual& b) {
+  Dual r{a.v * b.v, {}};
+  for (int i = 0; i < 15; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+  return r;
+}
+static Dual operator/(const Dual& a, const Dual& b) {
+  Dual r{a.v / b.v, {}};
+  for (int i = 0; i < 15; ++i) r.g[i] = (a.g[i] * b.v - a.v * b.g[i]) / (b.v * b.v);
+  return r;
+}
+static Dual dsqrt(const Dual& a) {
+  Dual r{std::sqrt(a.v), {}};
+  for (int i = 0; i < 15; ++i) r.g[i] = a.g[i] / (2 * r.v);
+  return r;
+}
+struct D3 { Dual x, y, z; };
+static D3 dsub(const D3& a, const D3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static Dual ddot(const D3& a, const D3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static D3 dcross(const D3& a, const D3& b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+// out[0..4] = distance, t, wa, wb, wc; grads[5][15] = their partials w.r.t. (a, b, c, o, d).
+void orc_ray_triangle_jacobian(const double* o, const double* d, const double* a, const double* b, const double* c,
+                               double* out5, double* grads) {
+  D3 A{dvar(a[0], 0), dvar(a[1], 1), dvar(a[2], 2)}, B{dvar(b[0], 3), dvar(b[1], 4), dvar(b[2], 5)};
+  D3 Cc{dvar(c[0], 6), dvar(c[1], 7), dvar(c[2], 8)}, O{dvar(o[0], 9), dvar(o[1], 10), dvar(o[2], 11)};
+  D3 Dd{dvar(d[0], 12), dvar(d[1], 13), dvar(d[2], 14)};
+  D3 e1 = dsub(B, A), e2 = dsub(Cc, A), q = dsub(O, A);
+  D3 n = dcross(e1, e2);
+  Dual N = ddot(Dd, n), U = ddot(Dd, dcross(q, e2)), V = ddot(Dd, dcross(e1, q)), T = ddot(q, n);
+  Dual t = dconst(0) - T / N, wb = U / N, wc = V / N;
+  Dual wa = dconst(1) - wb - wc;
+  Dual dist = t * dsqrt(ddot(Dd, Dd));
+  const Dual* vals[5] = {&dist, &t, &wa, &wb, &wc};
+  for (int k = 0; k < 5; ++k) {
+    out5[k] = vals[k]->v;
+    for (int i = 0; i < 15; ++i) grads[15 * k + i] = vals[k]->g[i];
+  }
+}
+
+// Distance from p to triangle (a, b, c) (closest point by Ericson 5.1.5), for finite differences.
+double orc_point_triangle_distance(const double* p, const double* a, const double* b, const double* c) {
+  V3 P{p[0], p[1], p[2]};
+  V3 r = closest_point_on_triangle(P, {a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]});
+  return std::sqrt(dist_sq(P, r));
+}
+
 // Statistics in the style of getBVHExtremes (debug/Debug.js:36-134): node count, leaf count,
 // max depth, total leaf triangles.
 void orc_stats(const orc_bvh* h, int64_t* out4) {

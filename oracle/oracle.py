@@ -62,6 +62,9 @@ def lib():
         L.orc_closest_point_triangle.argtypes = [P, P, P, P, P]
         L.orc_stats.argtypes = [P, P]
         L.orc_set_materials.argtypes = [P, P, I, P, I]
+        L.orc_ray_triangle_jacobian.argtypes = [P, P, P, P, P, P, P]
+        L.orc_point_triangle_distance.restype = D
+        L.orc_point_triangle_distance.argtypes = [P, P, P, P]
         _lib = L
     return _lib
 
@@ -200,6 +203,21 @@ def ray_triangle(o, d, a, b, c, side=0, near=0.0, far=math.inf):
     out = np.zeros(1, dtype=HIT_DTYPE)
     hit = lib().orc_ray_triangle(*[_p(x) for x in arrs], side, near, far, _p(out))
     return out[0] if hit else None
+
+
+def ray_triangle_jacobian(o, d, a, b, c):
+    """(values, jacobian): values = (distance, t, wa, wb, wc) of the ray/triangle formula in float64,
+    jacobian (5, 15) = their partials w.r.t. (a, b, c, o, d), from forward-mode dual numbers."""
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (o, d, a, b, c)]
+    vals = np.zeros(5)
+    jac = np.zeros((5, 15))
+    lib().orc_ray_triangle_jacobian(*[_p(x) for x in arrs], _p(vals), _p(jac))
+    return vals, jac
+
+
+def point_triangle_distance(p, a, b, c):
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (p, a, b, c)]
+    return lib().orc_point_triangle_distance(*[_p(x) for x in arrs])
 
 
 def closest_point_triangle(p, a, b, c):

@@ -32,7 +32,7 @@ def _hits(t):
         np.dtype([("face_index", "<u4"), ("distance", "<f4"), ("point", "<f4", 3), ("barycoord", "<f4", 3)]))
 
 
-@pytest.mark.parametrize("cfg", [(1, 1, 16, 0), (1, 0, 32, 1), (0, 1, 16, 0)])
+@pytest.mark.parametrize("cfg", [(1, 1, 16, 0, 0), (1, 0, 32, 1, 1), (0, 1, 16, 0, 0), (1, 1, 8, 2, 1)])
 def test_batched_matches_oracle_per_geometry(orc, scene, cfg):
     batch, rays, off, d_rays = scene
     batch.set_traversal(*cfg)

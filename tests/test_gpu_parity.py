@@ -211,14 +211,16 @@ def test_material_array_random_parity(pkg, orc, cuda):
     assert rep["count"] == 0 and rep["set"] == 0, rep
 
 
-@pytest.mark.parametrize("persistent,order,refill,occupancy", [(0, 0, 16, 0), (0, 1, 16, 0), (1, 0, 1, 0), (1, 1, 16, 1),
-                                                                (1, 1, 32, 2), (1, 0, 24, 2)])
-def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occupancy):
+@pytest.mark.parametrize("persistent,order,refill,occupancy,compact",
+                         [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0), (1, 0, 1, 0, 0), (1, 1, 16, 1, 0), (1, 1, 32, 2, 0),
+                          (1, 0, 24, 2, 0), (1, 1, 8, 2, 1), (1, 0, 16, 1, 1)])
+def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occupancy, compact):
     geo = pkg.torus_knot(10, 3, 500, 125, noise_sigma=0.02, noise_seed=1)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
     ref = _oracle_for(orc, bvh, geo)
-    bvh.set_traversal(persistent, order, refill, occupancy)
-    assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy)
+    bvh.set_traversal(persistent, order, refill, occupancy, compact)
+    assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
+                                       compact=compact)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -240,11 +242,14 @@ def test_pipelined_host_path_matches_device(pkg, knot80k, cuda):
     geo, bvh, ref = knot80k
     rays = pkg.rays_sphere_to_box(3_000_000 + 1234, seed=12)
     pinned = torch.from_numpy(rays).pin_memory()
-    host = bvh.raycast_first_batch(pinned.numpy())
-    dev = bvh.raycast_first_batch(torch.from_numpy(rays).to(cuda))
-    bvh.synchronize()
-    assert np.array_equal(dev.cpu().numpy().view(np.uint8).reshape(-1), host.view(np.uint8).reshape(-1))
-    sub = slice(0, 20_000)
-    exp = ref.raycast_first(rays[sub])
-    ac, ah = ref.raycast_all(rays[sub], cap=64)
-    _assert_first_ok(check_first(host[sub], exp, tie_exempt(ac, ah)))
+    for compact in (0, 1):      # the compacting variant keeps one queue per pipeline slot
+        bvh.set_traversal(1, 1, 16, 2, compact)
+        host = bvh.raycast_first_batch(pinned.numpy())
+        dev = bvh.raycast_first_batch(torch.from_numpy(rays).to(cuda))
+        bvh.synchronize()
+        assert np.array_equal(dev.cpu().numpy().view(np.uint8).reshape(-1), host.view(np.uint8).reshape(-1))
+        sub = slice(0, 20_000)
+        exp = ref.raycast_first(rays[sub])
+        ac, ah = ref.raycast_all(rays[sub], cap=64)
+        _assert_first_ok(check_first(host[sub], exp, tie_exempt(ac, ah)))
+    bvh.set_traversal(1, 1, 16, 0, 0)

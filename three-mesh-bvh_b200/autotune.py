@@ -14,8 +14,10 @@ import json
 import math
 from pathlib import Path
 
-CANDIDATES = [(0, 0, 16, 0), (0, 1, 16, 0)] + [(1, order, refill, occ) for order in (0, 1) for refill in (8, 16, 24, 32)
-                                               for occ in (0, 1, 2)]
+# (persistent, order, refill, occupancy, compact)
+CANDIDATES = [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0)] + [(1, order, refill, occ, compact) for order in (0, 1)
+                                                     for refill in (8, 16, 24, 32) for occ in (1, 2)
+                                                     for compact in (0, 1)]
 
 _cache: dict = {}
 

@@ -26,7 +26,7 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
-  TraversalConfig cfg{1, 1, 16, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0};
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
   int max_depth = 0;
@@ -43,6 +43,11 @@ struct bvhc_mesh {
   void* slot_in[2] = {nullptr, nullptr};
   void* slot_out[2] = {nullptr, nullptr};
   unsigned long long* d_work2 = nullptr;
+  // compaction queues of the persistent path (grow-only): [0] direct calls, [1], [2] the two
+  // pipeline slots, so that concurrently running chunks never share a queue
+  uint32_t* d_queue[3] = {nullptr, nullptr, nullptr};
+  size_t queue_cap[3] = {0, 0, 0};
+  unsigned int* d_qcount[3] = {nullptr, nullptr, nullptr};
   // batched meshes (bvhc_batch_create): mesh k owns roots [mesh_root_off[k], mesh_root_off[k+1])
   int n_meshes = 0;
   std::vector<uint32_t> mesh_root_off;
@@ -479,6 +484,10 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_ray_off);
   cudaFree(m->d_index32);
   cudaFree(m->d_pos);
+  for (int k = 0; k < 3; ++k) {
+    cudaFree(m->d_queue[k]);
+    cudaFree(m->d_qcount[k]);
+  }
   delete m;
 }
 
@@ -498,20 +507,47 @@ bvhc_status bvhc_mesh_synchronize(bvhc_mesh* m, void* stream) {
   return read_and_clear_error(m, static_cast<cudaStream_t>(stream));
 }
 
+// Compaction queue `slot` with room for n rays when the mesh's variant compacts, else nulls.
+static cudaError_t queue_for(bvhc_mesh* m, int slot, uint64_t n, uint32_t** queue, unsigned int** qcount) {
+  *queue = nullptr;
+  *qcount = nullptr;
+  if (!m->cfg.persistent || !m->cfg.compact || n >= (1ull << 32)) return cudaSuccess;
+  cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  if (!m->d_qcount[slot]) {
+    e = cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int));
+    if (e != cudaSuccess) return e;
+  }
+  *queue = m->d_queue[slot];
+  *qcount = m->d_qcount[slot];
+  return cudaSuccess;
+}
+
 static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
-                                  float near_d, float far_d, bvhc_hit* out, unsigned long long* work, cudaStream_t s) {
-  if (m->cfg.persistent)
+                                  float near_d, float far_d, bvhc_hit* out, unsigned long long* work, cudaStream_t s,
+                                  int qslot = 0) {
+  if (m->cfg.persistent) {
+    uint32_t* q;
+    unsigned int* qc;
+    cudaError_t e = queue_for(m, qslot, n, &q, &qc);
+    if (e != cudaSuccess) return e;
     return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
-                                           s);
+                                           s, q, qc);
+  }
   return launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
 }
 
 // raycastFirst over one mesh of a batch (view = that mesh's roots), with the batch's variant.
 static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* rays, uint64_t n, int side,
                                  float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
-  if (m->cfg.persistent)
+  if (m->cfg.persistent) {
+    uint32_t* q;
+    unsigned int* qc;
+    cudaError_t e = queue_for(m, 0, n, &q, &qc);
+    if (e != cudaSuccess) return e;
     return launch_raycast_first_persistent(v, nullptr, rays, n, side, single_side(), near_d, far_d, out, m->d_work,
-                                           m->cfg, s);
+                                           m->cfg, s, q, qc);
+  }
   return launch_raycast_first(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order, s);
 }
 
@@ -538,12 +574,13 @@ static cudaError_t ensure_pipeline(bvhc_mesh* m) {
 
 static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && (cfg->persistent == 0 || cfg->persistent == 1) && (cfg->order == 0 || cfg->order == 1) &&
-         cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2;
+         cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
+         (cfg->compact == 0 || cfg->compact == 1);
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact};
   return BVHC_OK;
 }
 
@@ -553,6 +590,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->order = m->cfg.order;
   cfg->refill = m->cfg.refill;
   cfg->occupancy = m->cfg.occupancy;
+  cfg->compact = m->cfg.compact;
   return BVHC_OK;
 }
 
@@ -593,7 +631,7 @@ static bvhc_status raycast_first_impl(bvhc_mesh* m, const float* rays, uint64_t 
     cudaStream_t st = m->pipe[k];
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], rays + 6 * off, cnt * 24, cudaMemcpyHostToDevice, st));
     BVHC_CUDA_TRY(dispatch_first(m, static_cast<const float*>(m->slot_in[k]), cnt, side, tab, near_d, far_d,
-                                 static_cast<bvhc_hit*>(m->slot_out[k]), works[k], st));
+                                 static_cast<bvhc_hit*>(m->slot_out[k]), works[k], st, 1 + k));
     BVHC_CUDA_TRY(cudaMemcpyAsync(out + off, m->slot_out[k], cnt * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, st));
   }
   BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[0]));
@@ -714,8 +752,11 @@ bvhc_status bvhc_batch_raycast_first(bvhc_mesh* m, const float* rays, const uint
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_ray_off, ray_offsets, (m->n_meshes + 1) * 8, cudaMemcpyHostToDevice, s));
   BatchDev bd{m->d_ray_off, m->d_mesh_root_off, m->n_meshes};
+  uint32_t* q;
+  unsigned int* qc;
+  BVHC_CUDA_TRY(queue_for(m, 0, n, &q, &qc));
   return from_cuda(launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d, out,
-                                                   m->d_work, m->cfg, s));
+                                                   m->d_work, m->cfg, s, q, qc));
 }
 
 bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* m, const float* rays, const uint64_t* ray_offsets, int side,
@@ -759,10 +800,13 @@ bvhc_status bvhc_batch_graph_create(bvhc_mesh* m, const float* rays, const uint6
   auto* g = new bvhc_graph();
   g->device = m->device;
   BatchDev bd{m->d_ray_off, m->d_mesh_root_off, m->n_meshes};
-  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  uint32_t* q = nullptr;
+  unsigned int* qc = nullptr;
+  cudaError_t e = queue_for(m, 0, n, &q, &qc);  // allocated before capture: captured work cannot allocate
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     cudaError_t le = launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d,
-                                                     out, m->d_work, m->cfg, cs);
+                                                     out, m->d_work, m->cfg, cs, q, qc);
     e = cudaStreamEndCapture(cs, &g->graph);
     if (le != cudaSuccess) e = le;
   }

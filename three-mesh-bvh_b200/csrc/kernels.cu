@@ -562,9 +562,12 @@ __device__ __forceinline__ int mesh_of_ray(const BatchDev& bd, uint64_t rid) {
 template <int ORDER, bool BATCHED, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
     MeshDev m, const BatchDev bd, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides,
-    float near_d, float far_d, bvhc_hit* __restrict__ out, unsigned long long* __restrict__ work, int refill) {
+    float near_d, float far_d, bvhc_hit* __restrict__ out, unsigned long long* __restrict__ work, int refill,
+    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
+  // with a queue (written by classify_kernel) the work items are its entries, else all rays
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
   bool active = false;
   uint64_t rid = 0;
   RayF r;
@@ -611,11 +614,11 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
         unsigned long long b = 0;
         if (lane == 0) b = atomicAdd(work, (unsigned long long)kChunk);
         b = __shfl_sync(0xFFFFFFFFu, b, 0);
-        if (b >= n) {
+        if (b >= n_work) {
           drained = true;
         } else {
           nb = b;
-          ne = b + kChunk < n ? b + kChunk : n;
+          ne = b + kChunk < n_work ? b + kChunk : n_work;
         }
       }
       if (!active) {
@@ -624,6 +627,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
         if (rank < avail) rid = pool + rank;
         else if (rank - avail < ne - nb) rid = nb + (rank - avail);
         else got = false;
+        if (got && queue) rid = __ldg(queue + rid);
         if (got) {
           active = true;
           r = make_ray(rays, rid);
@@ -690,15 +694,63 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
   }
 }
 
-// Completes the pending hits of raycast_first_persistent_kernel, one ray per thread.
+// Completes the pending hits of raycast_first_persistent_kernel, one ray per thread (grid-stride).
+// With a queue only its entries can be pending; the other rays were finished by classify_kernel.
 __global__ void __launch_bounds__(kBlock) finalize_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
-                                                                bvhc_hit* __restrict__ out) {
+                                                                bvhc_hit* __restrict__ out,
+                                                                const uint32_t* __restrict__ queue,
+                                                                const unsigned int* __restrict__ qcount) {
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_work; k += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = queue ? (uint64_t)__ldg(queue + k) : k;
+    uint32_t rec = __float_as_uint(__ldcs(reinterpret_cast<const float*>(out + i)));
+    if (rec == BVHC_NO_HIT) continue;
+    RayF r = make_ray(rays, i);
+    finish_first(m, rec, r, out + i);
+  }
+}
+
+// Pre-pass for the persistent traversal: a ray whose box tests against every root's two children
+// (with the root's own leaf case always live) all fail cannot hit anything; it is finished here with
+// a coalesced miss record.  The other rays are appended to `queue` (warp-aggregated atomics), so the
+// traversal kernel's warps only carry rays that enter the tree.
+template <bool BATCHED>
+__global__ void __launch_bounds__(kBlock) classify_kernel(MeshDev m, const BatchDev bd, const float* __restrict__ rays,
+                                                          uint64_t n, float near_d, float far_d,
+                                                          bvhc_hit* __restrict__ out, uint32_t* __restrict__ queue,
+                                                          unsigned int* __restrict__ qcount) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t rec = __float_as_uint(__ldcs(reinterpret_cast<const float*>(out + i)));
-  if (rec == BVHC_NO_HIT) return;
-  RayF r = make_ray(rays, i);
-  finish_first(m, rec, r, out + i);
+  bool live = false;
+  if (i < n) {
+    RayF r = make_ray(rays, i);
+    int root = 0, root_end = m.n_roots;
+    if (BATCHED) {
+      int mesh = mesh_of_ray(bd, i);
+      root = (int)__ldg(bd.mesh_root_off + mesh);
+      root_end = (int)__ldg(bd.mesh_root_off + mesh + 1);
+    }
+    for (; root < root_end && !live; ++root) {
+      uint32_t link = __ldg(m.roots + root);
+      if (link & kLeafBit) {
+        live = link != kEmptyLeaf;
+        continue;
+      }
+      Pair p = load_pair(m.nodes, link);
+      float e;
+      live = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e) ||
+             box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e);
+    }
+    if (!live) store_miss(out + i);
+  }
+  unsigned mask = __ballot_sync(0xFFFFFFFFu, live);
+  if (mask) {
+    unsigned lane = threadIdx.x & 31u;
+    int leader = __ffs(mask) - 1;
+    unsigned base = 0;
+    if ((int)lane == leader) base = atomicAdd(qcount, (unsigned)__popc(mask));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (live) queue[base + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+  }
 }
 
 }  // namespace dev
@@ -732,6 +784,8 @@ struct PersistentArgs {
   bvhc_hit* out;
   unsigned long long* work;
   int refill;
+  const uint32_t* queue;
+  const unsigned int* qcount;
 };
 
 template <int ORDER, bool BATCHED, int MINB>
@@ -741,7 +795,7 @@ static void launch_persistent(const PersistentArgs& a, cudaStream_t stream) {
   unsigned int g = persistent_grid(kernel, variant);
   g = (unsigned int)std::min<uint64_t>(g, (a.n + dev::kBlock - 1) / dev::kBlock);
   kernel<<<g, dev::kBlock, 0, stream>>>(a.m, a.bd, a.rays, a.n, a.side, a.sides, a.near_d, a.far_d, a.out, a.work,
-                                        a.refill);
+                                        a.refill, a.queue, a.qcount);
 }
 
 template <int ORDER, bool BATCHED>
@@ -754,12 +808,26 @@ static void launch_persistent_occ(const PersistentArgs& a, int occupancy, cudaSt
 cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
                                             int side, const SideTable& sides, float near_d, float far_d,
                                             bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
-                                            cudaStream_t stream) {
+                                            cudaStream_t stream, uint32_t* queue, unsigned int* qcount) {
   if (n == 0) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
-  PersistentArgs a{m, batch ? *batch : BatchDev{nullptr, nullptr, 0}, rays, n, side, sides, near_d, far_d, out,
-                   work, cfg.refill};
+  const bool compact = queue != nullptr && qcount != nullptr && n < (1ull << 32);
+  BatchDev bd = batch ? *batch : BatchDev{nullptr, nullptr, 0};
+  if (compact) {
+    e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    if (batch)
+      dev::classify_kernel<true><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
+                                                                         qcount);
+    else
+      dev::classify_kernel<false><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
+                                                                          qcount);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  PersistentArgs a{m, bd, rays, n, side, sides, near_d, far_d, out, work, cfg.refill,
+                   compact ? queue : nullptr, compact ? qcount : nullptr};
   if (batch) {
     if (cfg.order == 0) launch_persistent_occ<0, true>(a, cfg.occupancy, stream);
     else launch_persistent_occ<1, true>(a, cfg.occupancy, stream);
@@ -769,7 +837,8 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
   }
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  dev::finalize_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, out);
+  unsigned int fg = (unsigned int)std::min<uint64_t>(grid_for(n), 8192);
+  dev::finalize_first_kernel<<<fg, dev::kBlock, 0, stream>>>(m, rays, n, out, a.queue, a.qcount);
   return cudaGetLastError();
 }
 

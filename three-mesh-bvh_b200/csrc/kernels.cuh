@@ -35,6 +35,7 @@ struct TraversalConfig {
   int order;       // 0: split-axis direction sign (reference order); 1: nearest entry first
   int refill;      // idle lanes (1..32) that trigger a refill in the persistent form
   int occupancy;   // persistent form register budget: 0 compiler's choice, 1 six blocks/SM, 2 eight
+  int compact;     // persistent form: 1 runs the root-box pre-pass and traverses only queued rays
 };
 
 // Many meshes in one node/triangle pool: rays [ray_off[k], ray_off[k+1]) belong to mesh k, whose
@@ -46,10 +47,13 @@ struct BatchDev {
 };
 
 // `batch` null: one mesh (all of m.roots).  The work counter `work` is reset on `stream` first.
+// With `queue` (n entries) and `qcount` given, a pre-pass finishes the rays that miss every root's
+// child boxes and queues the others for the traversal (n must be below 2^32; otherwise no pre-pass).
 cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
                                             int side, const SideTable& sides, float near_d, float far_d,
                                             bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
-                                            cudaStream_t stream);
+                                            cudaStream_t stream, uint32_t* queue = nullptr,
+                                            unsigned int* qcount = nullptr);
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 

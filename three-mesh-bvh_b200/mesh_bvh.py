@@ -200,9 +200,10 @@ class MeshBVH:
         N.check(N.lib().bvhc_mesh_get_info(self._device_mesh(), C.byref(info)), "bvhc_mesh_get_info")
         return {k: getattr(info, k) for k, _ in N.BvhcMeshInfo._fields_}
 
-    def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0) -> None:
+    def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0,
+                      compact: int = 0) -> None:
         """Select the raycastFirst traversal variant (see bvhc_mesh_set_traversal)."""
-        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy)
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     def get_traversal(self) -> dict:
@@ -298,6 +299,55 @@ class MeshBVH:
 
     def synchronize(self, stream=None):
         N.check(N.lib().bvhc_mesh_synchronize(self._device_mesh(), stream), "bvhc_mesh_synchronize")
+
+    # -- gradients (forward/backward pairs; torch CUDA tensors) -----------------------------
+    def _gradients_ready(self):
+        if not getattr(self, "_grad_ready", False):
+            g = self.geometry
+            pos = np.ascontiguousarray(g.position, dtype=np.float32)
+            idx = g.index
+            N.check(N.lib().bvhc_mesh_enable_gradients(self._device_mesh(), _ptr(idx) if idx is not None else None,
+                                                        idx.dtype.itemsize if idx is not None else 0,
+                                                        idx.size if idx is not None else 0, _ptr(pos), pos.shape[0], 3),
+                    "bvhc_mesh_enable_gradients")
+            self._grad_ready = True
+
+    def raycast_first_backward(self, rays, hits, grad_distance=None, grad_barycoord=None, grad_vertices=None,
+                               stream=None):
+        """Backward of raycast_first_batch: dL/d(distance) (n) and/or dL/d(barycoord) (n, 3) ->
+        (grad_vertices (n_verts, 3) accumulated, grad_origins (n, 3), grad_directions (n, 3))."""
+        import torch
+
+        self._gradients_ready()
+        n = rays.shape[0]
+        dev = rays.device
+        if grad_vertices is None:
+            grad_vertices = torch.zeros((self.geometry.position.shape[0], 3), dtype=torch.float32, device=dev)
+        go = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        gd = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        N.check(N.lib().bvhc_raycast_first_backward(
+            self._device_mesh(), rays.data_ptr(), hits.data_ptr(), n,
+            grad_distance.data_ptr() if grad_distance is not None else None,
+            grad_barycoord.data_ptr() if grad_barycoord is not None else None,
+            grad_vertices.data_ptr(), go.data_ptr(), gd.data_ptr(), s), "bvhc_raycast_first_backward")
+        return grad_vertices, go, gd
+
+    def closest_point_backward(self, points, results, grad_distance, grad_vertices=None, stream=None):
+        """Backward of closest_point_batch's distance -> (grad_vertices accumulated, grad_points)."""
+        import torch
+
+        self._gradients_ready()
+        n = points.shape[0]
+        dev = points.device
+        if grad_vertices is None:
+            grad_vertices = torch.zeros((self.geometry.position.shape[0], 3), dtype=torch.float32, device=dev)
+        gp = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        N.check(N.lib().bvhc_closest_point_backward(self._device_mesh(), points.data_ptr(), results.data_ptr(), n,
+                                                     grad_distance.data_ptr(), grad_vertices.data_ptr(),
+                                                     gp.data_ptr(), s), "bvhc_closest_point_backward")
+        return grad_vertices, gp
 
     # -- reference-shaped single queries (MeshBVH.js:532-577, 874-884) ---------------------
     def _material_index(self, face_index: int) -> int:
