@@ -42,8 +42,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched", "adjoint"], default="first",
-                    help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form")
+    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest"], default="first",
+                    help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form; "
+                         "adjoint: forward/backward timing; closest: the 256^3 closest-point grid")
+    ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
     ap.add_argument("--radial", type=int, default=500)
@@ -75,10 +77,32 @@ def dist_setup(args):
     return ws, rank, local
 
 
+def incoherent_seed(rank: int) -> int:
+    """Each rank traces its own incoherent rays (the BVH is replicated; weak scaling)."""
+    return 1 + 1000 * rank
+
+
+def max_over_ranks(value: float, ws: int, device=None) -> float:
+    """The slowest rank's time: all-reduce MAX over the process group (identity for one rank)."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_scaling_rate(ws: int, rays_per_rank: int, steps: int, ms: float) -> float:
+    """Mrays/s of the whole job: every rank's rays over the slowest rank's time."""
+    return ws * rays_per_rank * steps / (ms / 1e3) / 1e6
+
+
 def scene(pkg, args, rank):
     geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
-    inc = pkg.rays_incoherent(1 << args.rays_log2, seed=1 + 1000 * rank)
+    inc = pkg.rays_incoherent(1 << args.rays_log2, seed=incoherent_seed(rank))
     cam = pkg.rays_camera(args.camera, args.camera)
     return geo, bvh, inc, cam
 
@@ -281,35 +305,32 @@ def run_engine(args, ws, rank, local):
     if ws > 1:
         torch.distributed.barrier()
     bvh.synchronize(stream.cuda_stream)
-    ms = t_start.elapsed_time(t_end)
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(t_start.elapsed_time(t_end), ws, dev)
     per_set_ms = [statistics.mean(kev[s][k][0].elapsed_time(kev[s][k][1]) for s in range(args.steps))
                   for k in range(len(sets))]
-    value = ws * n_step * args.steps / (ms / 1e3) / 1e6
+    value = weak_scaling_rate(ws, n_step, args.steps, ms)
 
     # e2e through the public API with pinned host buffers (copies inside the timed region)
     pinned_in = [torch.from_numpy(r).pin_memory() for _, r in sets]
     pinned_out = [torch.empty((r.shape[0] * 32,), dtype=torch.uint8).pin_memory() for _, r in sets]
     host_in = [p.numpy() for p in pinned_in]
     host_out = [p.numpy().view(pkg.HIT_DTYPE) for p in pinned_out]
-    for k in range(len(sets)):
-        bvh.raycast_first_batch(host_in[k], out=host_out[k])
+
+    def e2e_step():
+        for k in range(len(sets)):
+            if configs[k] is not None:
+                bvh.set_traversal(*configs[k])
+            bvh.raycast_first_batch(host_in[k], out=host_out[k])
+
+    e2e_step()
     e2e_steps = max(1, min(args.steps, 3))
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for k in range(len(sets)):
-            bvh.raycast_first_batch(host_in[k], out=host_out[k])
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if ws > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": ws * n_step / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": n_step * BYTES_RAY_IN,
-           "d2h_bytes_per_step": n_step * BYTES_HIT_OUT}
+        e2e_step()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) / e2e_steps * 1e3, ws, dev)
+    e2e = {"value": weak_scaling_rate(ws, n_step, 1, e2e_ms), "unit": UNIT,
+           "h2d_bytes_per_step": n_step * BYTES_RAY_IN, "d2h_bytes_per_step": n_step * BYTES_HIT_OUT}
 
     cpu = None
     roof = None
@@ -421,6 +442,72 @@ def run_batched(args, ws, rank, local):
     batch.dispose()
 
 
+def run_closest(args, ws, rank, local):
+    """Closest point / unsigned SDF: the 80,000-triangle knot, a 256^3 grid over its bounding box
+    padded by 10%, closestPointToPoint with maxThreshold 5 and minThreshold 0."""
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo = pkg.torus_knot(10, 3, 400, 100)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
+    pts_h = pkg.grid_points(geo.position.min(0), geo.position.max(0), args.grid)
+    pts = torch.from_numpy(pts_h).to(dev)
+    out = torch.empty((pts.shape[0], 5), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    n = pts.shape[0]
+    lib = pkg.lib()
+
+    def step():
+        lib.bvhc_closest_point_to_point(bvh._device_mesh(), pts.data_ptr(), n, 0.0, 5.0, out.data_ptr(), 1, s)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        a.record(stream)
+        for _ in range(args.steps):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+    bvh.synchronize(s)
+    ms = max_over_ranks(a.elapsed_time(b) / args.steps, ws, dev)
+    cpu = roof = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle.oracle as orc
+
+        ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, None, geo.position)
+        threads = os.cpu_count() or 1
+        idx = np.linspace(0, n - 1, min(n, 1 << 21)).astype(np.int64)
+        t0 = time.perf_counter()
+        _, nn, nt = ref.closest_point(np.ascontiguousarray(pts_h[idx]), 0.0, 5.0, threads=threads, counters=True)
+        dt = time.perf_counter() - t0
+        cpu = {"value": idx.size / dt / 1e6, "unit": "Mqueries/s", "cores": threads, "kind": "port",
+               "sample": f"{idx.size} evenly strided grid points, float64 oracle"}
+        per_query = 12 + 20 + 32 * float(nn.mean()) + 36 * float(nt.mean())
+        peak, how = measured_peak()
+        achieved = n * per_query / (ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": how, "algorithmic_bytes_per_launch": n * per_query,
+                "reference_node_reads_per_query": float(nn.mean()),
+                "reference_triangle_tests_per_query": float(nt.mean()), "kernel": "closest_point_kernel"}
+    if rank == 0:
+        line = {"metric": "Mqueries/s closestPointToPoint (80k tri, 256^3 grid)",
+                "value": weak_scaling_rate(ws, n, 1, ms), "unit": "Mqueries/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"TorusKnot(10,3,400,100) 80,000 tri, SAH leaf 10; {args.grid}^3 grid over "
+                                       "the AABB padded 10%; maxThreshold 5, minThreshold 0", "queries": int(n)},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+    bvh.dispose()
+
+
 def run_adjoint(args, ws, rank, local):
     """Differentiable depth and SDF on the 2M-triangle knot: forward raycastFirst of a 1024^2 camera
     and backward of L = sum (t - t*)^2 (t* rendered from the mesh with vertices moved by N(0, 0.01),
@@ -507,6 +594,8 @@ def main():
             run_batched(args, ws, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, ws, rank, local)
+        elif args.workload == "closest":
+            run_closest(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:

@@ -126,7 +126,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
 /* Traversal variant used by this mesh's raycastFirst calls (no reference counterpart: the
  * reference has one recursive traversal).  persistent = 1 runs a grid of resident warps that
  * refill idle lanes from a work counter once `refill` (1..32) lanes are idle; 0 runs one ray per
- * thread.  order = 0 visits the near child by the sign of the ray direction on the split axis (the
+ * thread; 2 runs the 32 rays of a warp through one shared traversal (for coherent rays such as a
+ * camera's, in pixel order).  Batched launches always use the persistent form.  order = 0 visits the near child by the sign of the ray direction on the split axis (the
  * reference's order), 1 by the smaller entry distance.  occupancy selects the persistent
  * kernel's register budget: 0 the compiler's choice, 1 at least six and 2 at least eight resident
  * 128-thread blocks per SM.  compact = 1 (persistent form) first finishes, in one coalesced pass,

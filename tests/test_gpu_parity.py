@@ -213,7 +213,7 @@ def test_material_array_random_parity(pkg, orc, cuda):
 
 @pytest.mark.parametrize("persistent,order,refill,occupancy,compact",
                          [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0), (1, 0, 1, 0, 0), (1, 1, 16, 1, 0), (1, 1, 32, 2, 0),
-                          (1, 0, 24, 2, 0), (1, 1, 8, 2, 1), (1, 0, 16, 1, 1)])
+                          (1, 0, 24, 2, 0), (1, 1, 8, 2, 1), (1, 0, 16, 1, 1), (2, 0, 16, 0, 0), (2, 1, 16, 0, 0)])
 def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occupancy, compact):
     geo = pkg.torus_knot(10, 3, 500, 125, noise_sigma=0.02, noise_seed=1)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})

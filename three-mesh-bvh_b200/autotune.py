@@ -15,7 +15,8 @@ import math
 from pathlib import Path
 
 # (persistent, order, refill, occupancy, compact)
-CANDIDATES = [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0)] + [(1, order, refill, occ, compact) for order in (0, 1)
+CANDIDATES = [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0), (2, 0, 16, 0, 0), (2, 1, 16, 0, 0)] + [
+    (1, order, refill, occ, compact) for order in (0, 1)
                                                      for refill in (8, 16, 24, 32) for occ in (1, 2)
                                                      for compact in (0, 1)]
 

@@ -526,6 +526,8 @@ static cudaError_t queue_for(bvhc_mesh* m, int slot, uint64_t n, uint32_t** queu
 static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
                                   float near_d, float far_d, bvhc_hit* out, unsigned long long* work, cudaStream_t s,
                                   int qslot = 0) {
+  if (m->cfg.persistent == 2)
+    return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;
@@ -540,6 +542,8 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
 // raycastFirst over one mesh of a batch (view = that mesh's roots), with the batch's variant.
 static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* rays, uint64_t n, int side,
                                  float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
+  if (m->cfg.persistent == 2)
+    return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;
@@ -573,7 +577,7 @@ static cudaError_t ensure_pipeline(bvhc_mesh* m) {
 }
 
 static bool valid_config(const bvhc_traversal_config* cfg) {
-  return cfg && (cfg->persistent == 0 || cfg->persistent == 1) && (cfg->order == 0 || cfg->order == 1) &&
+  return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1);
 }

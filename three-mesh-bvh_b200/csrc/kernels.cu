@@ -300,6 +300,98 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
 }
 
 // ---------------------------------------------------------------------------------------------
+// raycastFirst, warp-cooperative form for coherent rays (camera rays in pixel order).  The 32
+// rays of a warp walk the tree together with one shared stack: every child pair is fetched once
+// for the warp (a broadcast load), each lane tests it against its own ray, and the warp enters a
+// child if any lane's ray enters it (nearest first by majority vote).  A leaf is tested by all
+// lanes at once, so the triangle tests run at full SIMD width.  Each lane keeps its own entry
+// distance for every stacked child; a stacked child is skipped when no lane still needs it.
+// Visiting a node a lane's ray does not enter costs that lane nothing but idle time, and testing
+// a triangle it would not have reached cannot change its closest hit.
+// ---------------------------------------------------------------------------------------------
+constexpr int kWarps = kBlock / 32;
+
+template <int ORDER>
+__global__ void __launch_bounds__(kBlock) raycast_first_packet_kernel(MeshDev m, const float* __restrict__ rays,
+                                                                      uint64_t n, int side, const SideTable sides,
+                                                                      float near_d, float far_d,
+                                                                      bvhc_hit* __restrict__ out) {
+  __shared__ uint32_t s_link[kWarps][kMaxStack];
+  const unsigned full = 0xFFFFFFFFu;
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  RayF r;
+  float dlen = 1.0f;
+  if (valid) {
+    r = make_ray(rays, i);
+    dlen = sqrtf(r.d.x * r.d.x + r.d.y * r.d.y + r.d.z * r.d.z);
+  } else {
+    r.o = make_float3(0.f, 0.f, 0.f);
+    r.d = make_float3(1.f, 0.f, 0.f);
+    r.inv = make_float3(1.f, 1e30f, 1e30f);
+    r.d_l1 = 1.f;
+  }
+  const unsigned valid_mask = __ballot_sync(full, valid);
+  Best best{kInf, 0.0f, 0xFFFFFFFFu};
+  float lane_t[kMaxStack];
+  for (int root = 0; root < m.n_roots; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      bool pop = false;
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf && valid) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
+        pop = true;
+      } else {
+        Pair p = load_pair(m.nodes, link);
+        float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
+        float e0, e1;
+        bool h0 = valid && box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, lim, e0);
+        bool h1 = valid && box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, lim, e1);
+        unsigned b0 = __ballot_sync(full, h0), b1 = __ballot_sync(full, h1);
+        if (b0 && b1) {
+          bool lf = left_first<ORDER>(p, r, e0, e1);
+          bool left_wins = 2 * __popc(__ballot_sync(full, valid && lf)) >= __popc(valid_mask);
+          if (sp >= kMaxStack) {
+            if (lane == 0) atomicOr(m.err, kErrStackOverflow);
+            best.rec = 0xFFFFFFFFu;
+            root = m.n_roots;
+            break;
+          }
+          if (lane == 0) s_link[w][sp] = left_wins ? p.lr : p.ll;
+          lane_t[sp] = left_wins ? (h1 ? e1 : kInf) : (h0 ? e0 : kInf);
+          ++sp;
+          link = left_wins ? p.ll : p.lr;
+          __syncwarp();
+        } else if (b0) {
+          link = p.ll;
+        } else if (b1) {
+          link = p.lr;
+        } else {
+          pop = true;
+        }
+      }
+      if (pop) {
+        bool found = false;
+        while (sp > 0) {
+          --sp;
+          float lim = (best.t + best.err) * (1.0f + kSlabMargin);
+          if (__ballot_sync(full, valid && lane_t[sp] <= lim)) {
+            link = s_link[w][sp];
+            found = true;
+            break;
+          }
+        }
+        if (!found) break;
+      }
+    }
+  }
+  if (valid) finish_first(m, best.rec, r, out + i);
+}
+
+// ---------------------------------------------------------------------------------------------
 // raycast, all hits (raycast.template.js:15-53): left child then right child, every hit kept
 // in DFS order.  The first `cap` hits are stored; counts[i] is the uncapped total.
 // ---------------------------------------------------------------------------------------------
@@ -448,6 +540,12 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
               take = false;
             } else if (is_vertex && best_vertex && q.x == best_q.x && q.y == best_q.y && q.z == best_q.z) {
               take = false;  // the same vertex: an exact tie, the first one found stays
+            } else if (err + best_err <= 2e-6f * best_d2) {
+              // the two true distances are within 1e-6 relative of each other (typically the same
+              // edge or vertex reached from two triangles): either answer meets the distance
+              // tolerance and the winner's distance is recomputed in float-float, so the first
+              // one found stays, as the reference's strict `<` keeps it on a tie
+              take = false;
             } else {
               if (!best_ff_ok) {
                 Tri bt = load_tri(m.tris, best_rec);
@@ -534,7 +632,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 
 // ---------------------------------------------------------------------------------------------
 // raycastFirst, persistent form.  A fixed grid of warps pulls rays from a global work counter in
-// chunks of kChunk rays per warp (one atomicAdd per chunk); a lane whose ray is finished sits idle
+// chunks of 32..kChunk rays per warp (one atomicAdd per chunk); a lane whose ray is finished sits idle
 // until `refill` lanes of its warp are idle, and then those lanes take the next rays of the warp's
 // chunk together, so warps stay full while rays of very different cost (early misses, deep
 // traversals) are mixed.  Each outer iteration runs the "while-while" phases: every lane walks
@@ -568,6 +666,11 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
   const unsigned lt_mask = (1u << lane) - 1u;
   // with a queue (written by classify_kernel) the work items are its entries, else all rays
   const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
+  // rays per warp fetch: about eight fetches per warp over the launch, between 32 and kChunk, so
+  // that small batches still spread over every resident warp
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  uint64_t chunk = n_work / (warps * 8);
+  chunk = chunk < 32 ? 32 : (chunk > kChunk ? kChunk : (chunk & ~31ull));
   bool active = false;
   uint64_t rid = 0;
   RayF r;
@@ -612,13 +715,13 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
       uint64_t nb = 0, ne = 0;
       if (need > avail && !drained) {
         unsigned long long b = 0;
-        if (lane == 0) b = atomicAdd(work, (unsigned long long)kChunk);
+        if (lane == 0) b = atomicAdd(work, (unsigned long long)chunk);
         b = __shfl_sync(0xFFFFFFFFu, b, 0);
         if (b >= n_work) {
           drained = true;
         } else {
           nb = b;
-          ne = b + kChunk < n_work ? b + kChunk : n_work;
+          ne = b + chunk < n_work ? b + chunk : n_work;
         }
       }
       if (!active) {
@@ -839,6 +942,19 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
   if (e != cudaSuccess) return e;
   unsigned int fg = (unsigned int)std::min<uint64_t>(grid_for(n), 8192);
   dev::finalize_first_kernel<<<fg, dev::kBlock, 0, stream>>>(m, rays, n, out, a.queue, a.qcount);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
+                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
+                                        cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if (order == 0)
+    dev::raycast_first_packet_kernel<0><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
+                                                                                 far_d, out);
+  else
+    dev::raycast_first_packet_kernel<1><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
+                                                                                 far_d, out);
   return cudaGetLastError();
 }
 

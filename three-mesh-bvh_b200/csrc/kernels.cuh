@@ -25,13 +25,17 @@ struct MeshDev {
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                  float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
+// Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).
+cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
+                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
+                                        cudaStream_t stream);
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream);
 // Traversal variant chosen per call (autotuned): persistent vs one-ray-per-thread grid, child
 // order, and the number of idle lanes that triggers a warp refill.
 struct TraversalConfig {
-  int persistent;  // 1: persistent warps with lane refill; 0: one ray per thread
+  int persistent;  // 1: persistent warps with lane refill; 0: one ray per thread; 2: warp-cooperative
   int order;       // 0: split-axis direction sign (reference order); 1: nearest entry first
   int refill;      // idle lanes (1..32) that trigger a refill in the persistent form
   int occupancy;   // persistent form register budget: 0 compiler's choice, 1 six blocks/SM, 2 eight
