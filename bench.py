@@ -261,8 +261,8 @@ def run_engine(args, ws, rank, local):
     d_out = [torch.empty((r.shape[0], 8), dtype=torch.float32, device=dev) for _, r in sets]
     n_step = sum(r.shape[0] for _, r in sets)
     stream = torch.cuda.current_stream(dev)
-    # traversal variant per ray set: forced, autotuned on a strided 2^21-ray sample of the set, or
-    # the library default
+    # traversal variant per ray set: forced, autotuned on a 2^21-ray sample of the set, or the
+    # library default
     tuned = {}
     configs = [None] * len(sets)
     if args.traversal:
@@ -270,9 +270,13 @@ def run_engine(args, ws, rank, local):
     elif not args.no_tune:
         from three_mesh_bvh_b200 import autotune
 
-        k = 1 << 21
         for i, (name, _) in enumerate(sets):
-            sample = d_rays[i][torch.linspace(0, d_rays[i].shape[0] - 1, k, device=dev).long()].contiguous()
+            # 8 contiguous blocks of 2^18 rays spread over the set: keeps the set's ray-to-ray
+            # coherence (a strided sample of a camera is far less coherent than the camera)
+            n_i, blk = d_rays[i].shape[0], 1 << 18
+            starts = torch.linspace(0, max(n_i - blk, 0), 8, device=dev).long()
+            rows = (starts[:, None] + torch.arange(min(blk, n_i), device=dev)[None, :]).reshape(-1)
+            sample = d_rays[i][rows].contiguous()
             tuned[name] = autotune.tune_raycast_first(bvh, sample, tag=f"knot2M-{name}")
             configs[i] = tuned[name]["best"]
             del sample

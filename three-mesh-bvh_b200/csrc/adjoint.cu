@@ -12,6 +12,12 @@
 // each determinant's partials are cross products of the other two arguments, e.g.
 // d det(x,y,z)/dx = y x z.  For g_wb = g_wc = 0 this reduces to dt/dv_k = w_k n / N,
 // dt/do = -n / N and dt/dd = -t n / N with n = e1 x e2.
+// Evaluated as written, the q-terms are products of |o - a| (the ray length scale) with 1 / N (the
+// inverse triangle area scale) that cancel down to the triangle scale, losing about
+// log2(|o - a| / |e|) bits in float32.  The kernel therefore substitutes q = q' - t d with
+// q' = h - a = wb e1 + wc e2 (the hit point, from the recorded barycentrics): the d x d terms vanish,
+// gN - t gT = -(g_wb wb + g_wc wc) / N drops the t-proportional parts, and dL/dd picks up t dL/do.
+// Every remaining term is of the triangle's own scale.
 //
 // Closest point: for the distance dist = |p - c| to the closest point c = sum_k beta_k v_k of the
 // recorded triangle, the envelope theorem gives d dist / dp = (p - c) / dist and
@@ -108,14 +114,24 @@ __global__ void __launch_bounds__(kAdjBlock) raycast_first_backward_kernel(
     float3 a = load_vertex(pos, vid[0]), b = load_vertex(pos, vid[1]), c = load_vertex(pos, vid[2]);
     const float* r = rays + 6 * i;
     float3 o = f3(r[0], r[1], r[2]), d = f3(r[3], r[4], r[5]);
-    float3 q = sub3(o, a), e1 = sub3(b, a), e2 = sub3(c, a);
+    float3 e1 = sub3(b, a), e2 = sub3(c, a);
     float3 nrm = cross3(e1, e2);
     float N = dot3(d, nrm);
-    float U = dot3(d, cross3(q, e2));
-    float V = dot3(d, cross3(e1, q));
-    float T = dot3(q, nrm);
-    float t = -T / N, wb = U / N, wc = V / N;
     float dl = sqrtf(dot3(d, d));
+    // t and the barycentrics of the hit, as recorded by the forward pass (float-float, rounded once)
+    float t = dl > 0.0f ? hits[i].distance / dl : 0.0f;
+    float wb = hits[i].barycoord[1], wc = hits[i].barycoord[2];
+    // q' = h - a, the hit point relative to a: the ray re-anchored at its hit point (o = h - t d)
+    float3 qp;
+    if (hits[i].barycoord[0] == 0.0f && wb == 0.0f && wc == 0.0f) {
+      // the forward reported (0, 0, 0) for a triangle of vanishing area: fall back to q = o - a
+      float3 q = sub3(o, a);
+      wb = dot3(d, cross3(q, e2)) / N;
+      wc = dot3(d, cross3(e1, q)) / N;
+      qp = add3(q, mul3(d, t));
+    } else {
+      qp = add3(mul3(e1, wb), mul3(e2, wc));
+    }
     float gdist = g_dist ? g_dist[i] : 0.0f;
     float gt = gdist * dl;
     float gwa = 0.0f, gwb = 0.0f, gwc = 0.0f;
@@ -126,12 +142,13 @@ __global__ void __launch_bounds__(kAdjBlock) raycast_first_backward_kernel(
     }
     float iN = 1.0f / N;
     float gT = -gt * iN, gU = gwb * iN, gV = gwc * iN;
-    float gN = -(gt * t + gwb * wb + gwc * wc) * iN;
-    gd = add3(add3(mul3(cross3(q, e2), gU), mul3(cross3(e1, q), gV)), mul3(nrm, gN));
-    if (dl > 0.0f) gd = add3(gd, mul3(d, gdist * t / dl));
+    // gN - t gT: the t-proportional parts of gN and of the q-terms cancel analytically
+    float gNp = -(gwb * wb + gwc * wc) * iN;
     float3 gq = add3(add3(mul3(cross3(e2, d), gU), mul3(cross3(d, e1), gV)), mul3(nrm, gT));
-    float3 ge1 = add3(add3(mul3(cross3(q, d), gV), mul3(cross3(e2, d), gN)), mul3(cross3(e2, q), gT));
-    float3 ge2 = add3(add3(mul3(cross3(d, q), gU), mul3(cross3(d, e1), gN)), mul3(cross3(q, e1), gT));
+    float3 ge1 = add3(add3(mul3(cross3(qp, d), gV), mul3(cross3(e2, d), gNp)), mul3(cross3(e2, qp), gT));
+    float3 ge2 = add3(add3(mul3(cross3(d, qp), gU), mul3(cross3(d, e1), gNp)), mul3(cross3(qp, e1), gT));
+    gd = add3(add3(add3(mul3(cross3(qp, e2), gU), mul3(cross3(e1, qp), gV)), mul3(nrm, gNp)), mul3(gq, t));
+    if (dl > 0.0f) gd = add3(gd, mul3(d, gdist * t / dl));
     go = gq;
     gv[0] = mul3(add3(add3(gq, ge1), ge2), -1.0f);
     gv[1] = ge1;
