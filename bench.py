@@ -170,6 +170,29 @@ class ClockSampler:
                 "power_w_max": max(r[2] for r in self.rows)}
 
 
+def traversal_kernel(cfg):
+    """Name of the raycastFirst traversal kernel a variant launches."""
+    p = 1 if cfg is None else cfg[0]
+    return {0: "raycast_first_kernel", 1: "raycast_first_persistent_kernel", 2: "raycast_first_packet_kernel"}[p]
+
+
+def kernel_launches(cfg):
+    """Kernels one raycastFirst call launches with a variant (persistent, order, refill, occupancy,
+    compact, sort): the traversal, the persistent form's finalize pass, the root-box pre-pass and
+    the ray-ordering sort (key pass(es) + 4 radix passes of 3 kernels)."""
+    cfg = list(cfg) if cfg is not None else [1, 1, 16, 0, 0, 0]
+    cfg += [0] * (6 - len(cfg))
+    persistent, compact, sort = cfg[0], cfg[4], cfg[5]
+    if persistent == 0:
+        return 1
+    n = 1 + (1 if persistent == 1 else 0)
+    if compact or sort:
+        n += 1
+    if sort:
+        n += (2 if sort == 1 else 1) + 12
+    return n
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -261,8 +284,7 @@ def run_engine(args, ws, rank, local):
     d_out = [torch.empty((r.shape[0], 8), dtype=torch.float32, device=dev) for _, r in sets]
     n_step = sum(r.shape[0] for _, r in sets)
     stream = torch.cuda.current_stream(dev)
-    # traversal variant per ray set: forced, autotuned on a 2^21-ray sample of the set, or the
-    # library default
+    # traversal variant per ray set: forced, autotuned, or the library default
     tuned = {}
     configs = [None] * len(sets)
     if args.traversal:
@@ -271,15 +293,10 @@ def run_engine(args, ws, rank, local):
         from three_mesh_bvh_b200 import autotune
 
         for i, (name, _) in enumerate(sets):
-            # 8 contiguous blocks of 2^18 rays spread over the set: keeps the set's ray-to-ray
-            # coherence (a strided sample of a camera is far less coherent than the camera)
-            n_i, blk = d_rays[i].shape[0], 1 << 18
-            starts = torch.linspace(0, max(n_i - blk, 0), 8, device=dev).long()
-            rows = (starts[:, None] + torch.arange(min(blk, n_i), device=dev)[None, :]).reshape(-1)
-            sample = d_rays[i][rows].contiguous()
-            tuned[name] = autotune.tune_raycast_first(bvh, sample, tag=f"knot2M-{name}")
+            # tuned on the whole set: ray ordering and the warp-cooperative form depend on the
+            # set's coherence at full size, which no strided or block sample reproduces
+            tuned[name] = autotune.tune_raycast_first(bvh, d_rays[i], tag=f"knot2M-{name}")
             configs[i] = tuned[name]["best"]
-            del sample
 
     def step(ev=None):
         for k in range(len(sets)):
@@ -347,14 +364,17 @@ def run_engine(args, ws, rank, local):
         for (name, rays), (mn, mt) in zip(sets, stats):
             bytes_per_launch.append(rays.shape[0] * (BYTES_RAY_IN + BYTES_HIT_OUT + BYTES_NODE * mn + BYTES_TRI * mt))
         peak, how = measured_peak()
-        achieved = sum(bytes_per_launch) / (sum(per_set_ms) / 1e3) / 1e9
-        traffic = profile_traffic("raycast_first_k2.md")
+        # the dominant kernel: the traversal of the ray set that takes the longest
+        k = max(range(len(sets)), key=lambda j: per_set_ms[j])
+        achieved = bytes_per_launch[k] / (per_set_ms[k] / 1e3) / 1e9
+        both = sum(bytes_per_launch) / (sum(per_set_ms) / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": how,
-                "algorithmic_bytes_per_launch": [float(b) for b in bytes_per_launch],
+                "traffic": profile_traffic(f"raycast_first_k2_{sets[k][0]}.md"), "peak_source": how,
+                "kernel": traversal_kernel(configs[k]), "ray_set": sets[k][0],
+                "both_sets": {"achieved": both, "frac": both / peak},
+                "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], map(float, bytes_per_launch))),
                 "reference_node_reads_per_ray": [s[0] for s in stats],
-                "reference_triangle_tests_per_ray": [s[1] for s in stats],
-                "kernel": "raycast_first_kernel"}
+                "reference_triangle_tests_per_ray": [s[1] for s in stats]}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -365,9 +385,9 @@ def run_engine(args, ws, rank, local):
                            "parallelism": f"replicas x{ws}"},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
-                "traversal": bvh.get_traversal(), "autotune": tuned,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps * sum(2 if (c is None or c[0] == 1) else 1 for c in configs)}
+                "traversal": {n: (list(c) if c is not None else None) for (n, _), c in zip(sets, configs)},
+                "autotune": tuned, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": args.steps * sum(kernel_launches(c) for c in configs)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 
@@ -407,11 +427,13 @@ def run_batched(args, ws, rank, local):
     # autotune the batched launch over the traversal variants
     from three_mesh_bvh_b200.autotune import CANDIDATES
 
+    # (the batched launch always runs the persistent form; ray ordering applies to single meshes)
+    cands = [c for c in CANDIDATES if c[0] == 1 and c[5] == 0]
     timings = {}
-    for cand in CANDIDATES:
+    for cand in cands:
         batch.set_traversal(*cand)
         timings[str(list(cand))] = timed(lambda: batch.raycast_first(d_rays, off, out=out, stream=s), 1, 1)
-    best = min(CANDIDATES, key=lambda c: timings[str(list(c))])
+    best = min(cands, key=lambda c: timings[str(list(c))])
     batch.set_traversal(*best)
     graph = batch.capture(d_rays, off, out)
     with ClockSampler(local) as clk:
@@ -440,7 +462,7 @@ def run_batched(args, ws, rank, local):
                 "per_mesh_persistent_launches": {"ms": ms_pers, "mrays_s": n / (ms_pers / 1e3) / 1e6},
                 "speedup_vs_per_mesh_plain": ms_plain / ms_graph, "traversal": list(best),
                 "autotune_ms": timings, "clocks": clk.summary(),
-                "gpu_launches": args.steps * (2 if best[0] == 1 else 1)}
+                "gpu_launches": args.steps * kernel_launches(best)}
         print(json.dumps(line), flush=True)
     graph.destroy()
     batch.dispose()

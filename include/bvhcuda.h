@@ -127,19 +127,23 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * reference has one recursive traversal).  persistent = 1 runs a grid of resident warps that
  * refill idle lanes from a work counter once `refill` (1..32) lanes are idle; 0 runs one ray per
  * thread; 2 runs the 32 rays of a warp through one shared traversal (for coherent rays such as a
- * camera's, in pixel order).  Batched launches always use the persistent form.  order = 0 visits the near child by the sign of the ray direction on the split axis (the
- * reference's order), 1 by the smaller entry distance.  occupancy selects the persistent
- * kernel's register budget: 0 the compiler's choice, 1 at least six and 2 at least eight resident
- * 128-thread blocks per SM.  compact = 1 (persistent form) first finishes, in one coalesced pass,
- * the rays that miss every root's child boxes and traverses only the others.  Results are the
- * same for every variant (up to exact ties); the autotuner picks the fastest per mesh and
- * workload. */
+ * camera's).  Batched launches always use the persistent form.  order = 0 visits the near child
+ * by the sign of the ray direction on the split axis (the reference's order), 1 by the smaller
+ * entry distance.  occupancy selects the persistent kernel's register budget: 0 the compiler's
+ * choice, 1 at least six and 2 at least eight resident 128-thread blocks per SM.  compact = 1
+ * (persistent = 1 or 2) first finishes, in one coalesced pass, the rays that miss every root's
+ * child boxes and traverses only the others.  sort (persistent = 1 or 2, single meshes; implies
+ * the compaction pass) orders the remaining rays by a 30-bit Morton key before the traversal:
+ * 1 the ray direction, 2 the point where the ray enters the mesh's bounding box, 3 that point
+ * (coarser) followed by the direction; 0 keeps the input order.  Results are the same for every
+ * variant (up to exact ties); the autotuner picks the fastest per mesh and workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;
   int32_t order;
   int32_t refill;
   int32_t occupancy;
   int32_t compact;
+  int32_t sort;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);

@@ -211,16 +211,19 @@ def test_material_array_random_parity(pkg, orc, cuda):
     assert rep["count"] == 0 and rep["set"] == 0, rep
 
 
-@pytest.mark.parametrize("persistent,order,refill,occupancy,compact",
-                         [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0), (1, 0, 1, 0, 0), (1, 1, 16, 1, 0), (1, 1, 32, 2, 0),
-                          (1, 0, 24, 2, 0), (1, 1, 8, 2, 1), (1, 0, 16, 1, 1), (2, 0, 16, 0, 0), (2, 1, 16, 0, 0)])
-def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occupancy, compact):
+@pytest.mark.parametrize("persistent,order,refill,occupancy,compact,sort",
+                         [(0, 0, 16, 0, 0, 0), (0, 1, 16, 0, 0, 0), (1, 0, 1, 0, 0, 0), (1, 1, 16, 1, 0, 0),
+                          (1, 1, 32, 2, 0, 0), (1, 0, 24, 2, 0, 0), (1, 1, 8, 2, 1, 0), (1, 0, 16, 1, 1, 0),
+                          (2, 0, 16, 0, 0, 0), (2, 1, 16, 0, 0, 0), (2, 0, 16, 0, 1, 0), (1, 1, 32, 2, 1, 1),
+                          (1, 1, 16, 1, 0, 2), (1, 0, 32, 2, 1, 3), (2, 0, 16, 0, 1, 1), (2, 1, 16, 0, 0, 2),
+                          (2, 0, 16, 0, 1, 3)])
+def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occupancy, compact, sort):
     geo = pkg.torus_knot(10, 3, 500, 125, noise_sigma=0.02, noise_seed=1)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
     ref = _oracle_for(orc, bvh, geo)
-    bvh.set_traversal(persistent, order, refill, occupancy, compact)
+    bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
-                                       compact=compact)
+                                       compact=compact, sort=sort)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -242,8 +245,9 @@ def test_pipelined_host_path_matches_device(pkg, knot80k, cuda):
     geo, bvh, ref = knot80k
     rays = pkg.rays_sphere_to_box(3_000_000 + 1234, seed=12)
     pinned = torch.from_numpy(rays).pin_memory()
-    for compact in (0, 1):      # the compacting variant keeps one queue per pipeline slot
-        bvh.set_traversal(1, 1, 16, 2, compact)
+    # the compacting and ordering variants keep one queue (and sort scratch) per pipeline slot
+    for persistent, compact, sort in ((1, 0, 0), (1, 1, 0), (1, 1, 3), (2, 0, 1)):
+        bvh.set_traversal(persistent, 1, 16, 2, compact, sort)
         host = bvh.raycast_first_batch(pinned.numpy())
         dev = bvh.raycast_first_batch(torch.from_numpy(rays).to(cuda))
         bvh.synchronize()

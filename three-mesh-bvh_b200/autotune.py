@@ -1,8 +1,8 @@
 """Autotuner for the traversal kernels.
 
 For a mesh and a representative ray batch already on the device, each candidate traversal
-variant (persistent warps with lane refill or one ray per thread, child visiting order, refill
-threshold) is timed with CUDA events on the launching stream after a warm-up launch, and the
+variant (persistent warps with lane refill, warp-cooperative traversal or one ray per thread,
+child visiting order, refill threshold, register budget, compaction and ray-ordering key) is timed with CUDA events on the launching stream after a warm-up launch, and the
 fastest is installed on the mesh.  Results are cached per (GPU name, triangle-count bucket,
 workload tag), in memory and optionally in a JSON file, so a serving process tunes once per
 mesh class.  Every variant returns the same hits (up to exact ties), so tuning never changes
@@ -14,11 +14,13 @@ import json
 import math
 from pathlib import Path
 
-# (persistent, order, refill, occupancy, compact)
-CANDIDATES = [(0, 0, 16, 0, 0), (0, 1, 16, 0, 0), (2, 0, 16, 0, 0), (2, 1, 16, 0, 0)] + [
-    (1, order, refill, occ, compact) for order in (0, 1)
-                                                     for refill in (8, 16, 24, 32) for occ in (1, 2)
-                                                     for compact in (0, 1)]
+# (persistent, order, refill, occupancy, compact, sort): one ray per thread; warp-cooperative
+# traversal; persistent warps with lane refill.  The last two select the root-box compaction pass
+# and the Morton-key ray ordering (0 none, 1 direction, 2 entry point, 3 entry point + direction).
+_QUEUE = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)]
+CANDIDATES = [(0, 0, 16, 0, 0, 0), (0, 1, 16, 0, 0, 0)] + [
+    (2, order, 16, 0, c, s) for order in (0, 1) for c, s in _QUEUE] + [
+    (1, order, refill, occ, c, s) for order in (0, 1) for refill in (16, 32) for occ in (1, 2) for c, s in _QUEUE]
 
 _cache: dict = {}
 

@@ -22,6 +22,9 @@
 // Closest point: for the distance dist = |p - c| to the closest point c = sum_k beta_k v_k of the
 // recorded triangle, the envelope theorem gives d dist / dp = (p - c) / dist and
 // d dist / dv_k = -beta_k (p - c) / dist (beta: barycentrics of c; zero gradient at dist = 0).
+// c and beta are recomputed in float-float from the recorded triangle (Ericson's region method),
+// so p - c carries no rounding of the reported float32 point and beta is exactly 0 for the
+// vertices outside c's edge or vertex region.
 //
 // Vertex gradients are accumulated with atomicAdd; lanes of a warp that recorded the same face are
 // first summed with warp shuffles so that the face's three vertices receive one atomic per
@@ -32,6 +35,7 @@
 
 #include "bvhcuda.h"
 #include "kernels.cuh"
+#include "robust.cuh"
 
 namespace bvhc {
 namespace dev {
@@ -169,16 +173,6 @@ __global__ void __launch_bounds__(kAdjBlock) raycast_first_backward_kernel(
   if (g_vert) scatter_vertex_grads(g_vert, face, valid, vid, gv);
 }
 
-// Barycentric coordinates of a point c of triangle (a, b, c3) by the dot-product solve.
-__device__ __forceinline__ float3 barycentric(float3 p, float3 a, float3 b, float3 c) {
-  float3 v0 = sub3(b, a), v1 = sub3(c, a), v2 = sub3(p, a);
-  float d00 = dot3(v0, v0), d01 = dot3(v0, v1), d11 = dot3(v1, v1), d20 = dot3(v2, v0), d21 = dot3(v2, v1);
-  float den = d00 * d11 - d01 * d01;
-  if (den == 0.0f) return f3(1.0f, 0.0f, 0.0f);
-  float wb = (d11 * d20 - d01 * d21) / den, wc = (d00 * d21 - d01 * d20) / den;
-  return f3(1.0f - wb - wc, wb, wc);
-}
-
 __global__ void __launch_bounds__(kAdjBlock) closest_point_backward_kernel(
     const uint32_t* __restrict__ index, const float* __restrict__ pos, const float* __restrict__ pts,
     const bvhc_closest* __restrict__ res, uint64_t n, const float* __restrict__ g_dist, float* __restrict__ g_vert,
@@ -194,14 +188,21 @@ __global__ void __launch_bounds__(kAdjBlock) closest_point_backward_kernel(
     for (int k = 0; k < 3; ++k) vid[k] = __ldg(index + 3 * (uint64_t)face + k);
     float3 a = load_vertex(pos, vid[0]), b = load_vertex(pos, vid[1]), c = load_vertex(pos, vid[2]);
     float3 p = f3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
-    float3 cp = f3(res[i].point[0], res[i].point[1], res[i].point[2]);
-    float3 u = mul3(sub3(p, cp), 1.0f / res[i].distance);   // unit vector from the closest point
+    // The closest point again, in float-float: p - c without the rounding of the reported point
+    // (whose error divided by the distance would enter u directly), and the barycentrics of its
+    // Voronoi region (exactly zero for the vertices an edge or vertex region leaves out).
+    CPFF cf = closest_ff(p, a, b, c);
+    float dist = ff_to_f(ff_sqrt(cf.d2));
     float g = g_dist[i];
-    gp = mul3(u, g);
-    float3 beta = barycentric(cp, a, b, c);
-    gv[0] = mul3(u, -g * beta.x);
-    gv[1] = mul3(u, -g * beta.y);
-    gv[2] = mul3(u, -g * beta.z);
+    if (dist > 0.0f) {
+      float id = 1.0f / dist;
+      float3 u = f3(ff_to_f(cf.r.x) * id, ff_to_f(cf.r.y) * id, ff_to_f(cf.r.z) * id);
+      gp = mul3(u, g);
+      float wa = 1.0f - cf.wb - cf.wc;
+      gv[0] = mul3(u, -g * wa);
+      gv[1] = mul3(u, -g * cf.wb);
+      gv[2] = mul3(u, -g * cf.wc);
+    }
   }
   if (in && g_pts) {
     g_pts[3 * i] = gp.x;

@@ -26,7 +26,8 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0};
+  float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
   int max_depth = 0;
@@ -48,6 +49,9 @@ struct bvhc_mesh {
   uint32_t* d_queue[3] = {nullptr, nullptr, nullptr};
   size_t queue_cap[3] = {0, 0, 0};
   unsigned int* d_qcount[3] = {nullptr, nullptr, nullptr};
+  // ray-ordering sort scratch per queue slot (grow-only; sized for sort_cap[slot] rays)
+  RaySortScratch sort_s[3] = {};
+  uint64_t sort_cap[3] = {0, 0, 0};
   // batched meshes (bvhc_batch_create): mesh k owns roots [mesh_root_off[k], mesh_root_off[k+1])
   int n_meshes = 0;
   std::vector<uint32_t> mesh_root_off;
@@ -201,6 +205,16 @@ cudaError_t ensure(void** buf, size_t* cap, size_t bytes) {
   return e;
 }
 
+void free_sort_scratch(RaySortScratch& s) {
+  cudaFree(s.keys[0]);
+  cudaFree(s.keys[1]);
+  cudaFree(s.vals);
+  cudaFree(s.hist);
+  cudaFree(s.totals);
+  cudaFree(s.dir_bounds);
+  s = RaySortScratch{};
+}
+
 SideTable single_side() {
   SideTable t{};
   t.n = 0;
@@ -263,6 +277,15 @@ static bvhc_status finish_mesh(int device, const std::vector<PairNode>& pairs, c
   m->device = device;
   m->n_nodes = pairs.size();
   m->n_tris = tris.size();
+  if (!tris.empty()) {
+    for (int a = 0; a < 3; ++a) m->scene_lo[a] = m->scene_hi[a] = tris[0].v[a];
+    for (const TriRecord& t : tris)
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) {
+          m->scene_lo[a] = std::min(m->scene_lo[a], t.v[3 * k + a]);
+          m->scene_hi[a] = std::max(m->scene_hi[a], t.v[3 * k + a]);
+        }
+  }
   m->n_roots = (int)root_links.size();
   m->max_depth = max_depth;
   m->rec_face.resize(tris.size());
@@ -487,6 +510,7 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   for (int k = 0; k < 3; ++k) {
     cudaFree(m->d_queue[k]);
     cudaFree(m->d_qcount[k]);
+    free_sort_scratch(m->sort_s[k]);
   }
   delete m;
 }
@@ -507,11 +531,34 @@ bvhc_status bvhc_mesh_synchronize(bvhc_mesh* m, void* stream) {
   return read_and_clear_error(m, static_cast<cudaStream_t>(stream));
 }
 
-// Compaction queue `slot` with room for n rays when the mesh's variant compacts, else nulls.
-static cudaError_t queue_for(bvhc_mesh* m, int slot, uint64_t n, uint32_t** queue, unsigned int** qcount) {
+static cudaError_t ensure_sort_scratch(bvhc_mesh* m, int slot, uint64_t n) {
+  if (m->sort_cap[slot] >= n) return cudaSuccess;
+  RaySortScratch& s = m->sort_s[slot];
+  free_sort_scratch(s);
+  m->sort_cap[slot] = 0;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&s.keys[0]), n * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.keys[1]), n * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.vals), n * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.hist), 256 * ray_sort_tiles(n) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.totals), 4 * 256 * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.dir_bounds), 6 * 4);
+  if (e != cudaSuccess) {
+    free_sort_scratch(s);
+    return e;
+  }
+  m->sort_cap[slot] = n;
+  return cudaSuccess;
+}
+
+// Compaction queue `slot` with room for n rays when the mesh's variant uses one (persistent or
+// warp-cooperative form with compaction or ordering), else nulls; `sort` is filled when the variant
+// orders the queue (single meshes only) and left untouched otherwise.
+static cudaError_t queue_for(bvhc_mesh* m, int slot, uint64_t n, uint32_t** queue, unsigned int** qcount,
+                             RaySort* sort = nullptr, bool* sorted = nullptr) {
   *queue = nullptr;
   *qcount = nullptr;
-  if (!m->cfg.persistent || !m->cfg.compact || n >= (1ull << 32)) return cudaSuccess;
+  if (sorted) *sorted = false;
+  if (!m->cfg.persistent || !(m->cfg.compact || m->cfg.sort) || n >= (1ull << 32)) return cudaSuccess;
   cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
   if (e != cudaSuccess) return e;
   if (!m->d_qcount[slot]) {
@@ -520,21 +567,35 @@ static cudaError_t queue_for(bvhc_mesh* m, int slot, uint64_t n, uint32_t** queu
   }
   *queue = m->d_queue[slot];
   *qcount = m->d_qcount[slot];
+  if (sort && sorted && m->cfg.sort && m->n_meshes == 0) {
+    e = ensure_sort_scratch(m, slot, n);
+    if (e != cudaSuccess) return e;
+    sort->kind = m->cfg.sort;
+    for (int a = 0; a < 3; ++a) {
+      sort->lo[a] = m->scene_lo[a];
+      sort->hi[a] = m->scene_hi[a];
+    }
+    sort->scratch = m->sort_s[slot];
+    *sorted = true;
+  }
   return cudaSuccess;
 }
 
 static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, int side, const SideTable& tab,
                                   float near_d, float far_d, bvhc_hit* out, unsigned long long* work, cudaStream_t s,
                                   int qslot = 0) {
-  if (m->cfg.persistent == 2)
-    return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;
-    cudaError_t e = queue_for(m, qslot, n, &q, &qc);
+    RaySort sort{};
+    bool sorted = false;
+    cudaError_t e = queue_for(m, qslot, n, &q, &qc, &sort, &sorted);
     if (e != cudaSuccess) return e;
+    if (m->cfg.persistent == 2)
+      return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s, q, qc,
+                                         sorted ? &sort : nullptr);
     return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
-                                           s, q, qc);
+                                           s, q, qc, sorted ? &sort : nullptr);
   }
   return launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
 }
@@ -579,12 +640,12 @@ static cudaError_t ensure_pipeline(bvhc_mesh* m) {
 static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
-         (cfg->compact == 0 || cfg->compact == 1);
+         (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact, cfg->sort};
   return BVHC_OK;
 }
 
@@ -595,6 +656,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->refill = m->cfg.refill;
   cfg->occupancy = m->cfg.occupancy;
   cfg->compact = m->cfg.compact;
+  cfg->sort = m->cfg.sort;
   return BVHC_OK;
 }
 

@@ -315,13 +315,19 @@ template <int ORDER>
 __global__ void __launch_bounds__(kBlock) raycast_first_packet_kernel(MeshDev m, const float* __restrict__ rays,
                                                                       uint64_t n, int side, const SideTable sides,
                                                                       float near_d, float far_d,
-                                                                      bvhc_hit* __restrict__ out) {
+                                                                      bvhc_hit* __restrict__ out,
+                                                                      const uint32_t* __restrict__ queue,
+                                                                      const unsigned int* __restrict__ qcount) {
   __shared__ uint32_t s_link[kWarps][kMaxStack];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
+  // with a queue (root-box pre-pass, optionally sorted) a warp takes 32 consecutive queue entries
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < n;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
+  const bool valid = i < n_work;
+  if (valid && queue) i = __ldg(queue + i);
   RayF r;
   float dlen = 1.0f;
   if (valid) {
@@ -908,25 +914,36 @@ static void launch_persistent_occ(const PersistentArgs& a, int occupancy, cudaSt
   else launch_persistent<ORDER, BATCHED, 8>(a, stream);
 }
 
+// Root-box pre-pass into `queue`, then (single mesh, sort requested) the ray-ordering sort.
+static cudaError_t prepare_queue(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n, float near_d,
+                                 float far_d, bvhc_hit* out, uint32_t* queue, unsigned int* qcount,
+                                 const RaySort* sort, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream);
+  if (e != cudaSuccess) return e;
+  BatchDev bd = batch ? *batch : BatchDev{nullptr, nullptr, 0};
+  if (batch)
+    dev::classify_kernel<true><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
+                                                                       qcount);
+  else
+    dev::classify_kernel<false><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
+                                                                        qcount);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || !sort || batch || sort->kind == 0) return e;
+  return launch_ray_sort(rays, n, sort->kind, sort->lo, sort->hi, queue, qcount, sort->scratch, stream);
+}
+
 cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
                                             int side, const SideTable& sides, float near_d, float far_d,
                                             bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
-                                            cudaStream_t stream, uint32_t* queue, unsigned int* qcount) {
+                                            cudaStream_t stream, uint32_t* queue, unsigned int* qcount,
+                                            const RaySort* sort) {
   if (n == 0) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return e;
   const bool compact = queue != nullptr && qcount != nullptr && n < (1ull << 32);
   BatchDev bd = batch ? *batch : BatchDev{nullptr, nullptr, 0};
   if (compact) {
-    e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream);
-    if (e != cudaSuccess) return e;
-    if (batch)
-      dev::classify_kernel<true><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
-                                                                         qcount);
-    else
-      dev::classify_kernel<false><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
-                                                                          qcount);
-    e = cudaGetLastError();
+    e = prepare_queue(m, batch, rays, n, near_d, far_d, out, queue, qcount, sort, stream);
     if (e != cudaSuccess) return e;
   }
   PersistentArgs a{m, bd, rays, n, side, sides, near_d, far_d, out, work, cfg.refill,
@@ -947,14 +964,23 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        cudaStream_t stream) {
+                                        cudaStream_t stream, uint32_t* queue, unsigned int* qcount,
+                                        const RaySort* sort) {
   if (n == 0) return cudaSuccess;
+  const bool compact = queue != nullptr && qcount != nullptr && n < (1ull << 32);
+  if (compact) {
+    cudaError_t e = prepare_queue(m, nullptr, rays, n, near_d, far_d, out, queue, qcount, sort, stream);
+    if (e != cudaSuccess) return e;
+  } else {
+    queue = nullptr;
+    qcount = nullptr;
+  }
   if (order == 0)
     dev::raycast_first_packet_kernel<0><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
-                                                                                 far_d, out);
+                                                                                 far_d, out, queue, qcount);
   else
     dev::raycast_first_packet_kernel<1><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
-                                                                                 far_d, out);
+                                                                                 far_d, out, queue, qcount);
   return cudaGetLastError();
 }
 

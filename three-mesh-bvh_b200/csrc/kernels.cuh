@@ -26,9 +26,7 @@ struct MeshDev {
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                  float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
 // Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).
-cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
-                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        cudaStream_t stream);
+
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream);
@@ -39,8 +37,33 @@ struct TraversalConfig {
   int order;       // 0: split-axis direction sign (reference order); 1: nearest entry first
   int refill;      // idle lanes (1..32) that trigger a refill in the persistent form
   int occupancy;   // persistent form register budget: 0 compiler's choice, 1 six blocks/SM, 2 eight
-  int compact;     // persistent form: 1 runs the root-box pre-pass and traverses only queued rays
+  int compact;     // 1 runs the root-box pre-pass and traverses only queued rays (persistent and
+                   // warp-cooperative forms)
+  int sort;        // 0: queue in ray order; 1..3: queue sorted by a Morton key (raysort.cu), implies
+                   // the pre-pass
 };
+
+// Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
+struct RaySortScratch {
+  uint32_t* keys[2];     // n entries each
+  uint32_t* vals;        // n entries: the queue's ping-pong partner
+  uint32_t* hist;        // 256 * ray_sort_tiles(n) entries
+  uint32_t* totals;      // 4 * 256 entries
+  uint32_t* dir_bounds;  // 6 entries
+};
+
+// A sort request: key kind (1..3) and the scene box used by the entry-point keys.
+struct RaySort {
+  int kind;
+  float lo[3], hi[3];
+  RaySortScratch scratch;
+};
+
+uint64_t ray_sort_tiles(uint64_t n);
+// Sorts the first *qcount ids of `queue` (rays into the mesh) by the key `kind`; n bounds *qcount.
+cudaError_t launch_ray_sort(const float* rays, uint64_t n, int kind, const float scene_lo[3], const float scene_hi[3],
+                            uint32_t* queue, const unsigned int* qcount, const RaySortScratch& s,
+                            cudaStream_t stream);
 
 // Many meshes in one node/triangle pool: rays [ray_off[k], ray_off[k+1]) belong to mesh k, whose
 // roots are MeshDev::roots[mesh_root_off[k] .. mesh_root_off[k+1]).
@@ -57,7 +80,13 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
                                             int side, const SideTable& sides, float near_d, float far_d,
                                             bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
                                             cudaStream_t stream, uint32_t* queue = nullptr,
-                                            unsigned int* qcount = nullptr);
+                                            unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
+// Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).  With a
+// queue, the same pre-pass (and sort) as the persistent form runs first.
+cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
+                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
+                                        cudaStream_t stream, uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
+                                        const RaySort* sort = nullptr);
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 

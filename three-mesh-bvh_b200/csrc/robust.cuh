@@ -133,7 +133,7 @@ struct TriFF {
   ff N, U, V, W, T;
 };
 
-__device__ __noinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
+static __device__ __noinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
   ff3 e1 = ff3_diff(b, a), e2 = ff3_diff(c, a), q = ff3_diff(o, a);
   ff3 n = ff3_cross(e1, e2);
   TriFF r;
@@ -152,7 +152,7 @@ __device__ __forceinline__ bool tri_decide_ff(const TriFF& r, int side) {
   return sn * ff_sign(r.U) >= 0 && sn * ff_sign(r.V) >= 0 && sn * ff_sign(r.W) >= 0 && -sn * ff_sign(r.T) >= 0;
 }
 
-__device__ __noinline__ bool tri_hit_slow(float3 a, float3 b, float3 c, float3 o, float3 d, int side) {
+static __device__ __noinline__ bool tri_hit_slow(float3 a, float3 b, float3 c, float3 o, float3 d, int side) {
   return tri_decide_ff(tri_eval_ff(a, b, c, o, d), side);
 }
 
@@ -204,7 +204,7 @@ __device__ __forceinline__ ff tri_t_ff(const TriFF& r) { return ff_div(ff_neg(r.
 
 constexpr float kTinyRel = 9.094947017729282e-13f;  // 2^-40: relative error of a float-float t
 
-__device__ __noinline__ bool tri_hit_slow_t(float3 a, float3 b, float3 c, float3 o, float3 d, int side, float& t,
+static __device__ __noinline__ bool tri_hit_slow_t(float3 a, float3 b, float3 c, float3 o, float3 d, int side, float& t,
                                             float& t_err) {
   TriFF r = tri_eval_ff(a, b, c, o, d);
   if (!tri_decide_ff(r, side)) return false;
@@ -312,14 +312,17 @@ __device__ __forceinline__ float closest_sq_f(float3 p, float3 a, float3 b, floa
 }
 
 struct CPFF {
-  ff3 q;   // closest point (world frame)
-  ff d2;   // squared distance
+  ff3 q;    // closest point (world frame)
+  ff d2;    // squared distance
+  ff3 r;    // p - q
+  float wb, wc;  // barycentric weights of q on b and c (exactly 0 off the region's own vertices)
 };
 
 // Float-float version of the same algorithm (used for the final answer and for ties).
-__device__ __noinline__ CPFF closest_ff(float3 p, float3 a, float3 b, float3 c) {
+static __device__ __noinline__ CPFF closest_ff(float3 p, float3 a, float3 b, float3 c) {
   ff3 ab = ff3_diff(b, a), ac = ff3_diff(c, a), ap = ff3_diff(p, a);
   ff3 l;
+  float wb = 0.0f, wc = 0.0f;
   ff d1 = ff3_dot(ab, ap), d2 = ff3_dot(ac, ap);
   ff3 bp = ff3_sub(ap, ab), cp = ff3_sub(ap, ac);
   ff d3 = ff3_dot(ab, bp), d4 = ff3_dot(ac, bp);
@@ -329,26 +332,36 @@ __device__ __noinline__ CPFF closest_ff(float3 p, float3 a, float3 b, float3 c) 
     l = {zero, zero, zero};
   } else if (ff_sign(d3) >= 0 && !ff_lt(d3, d4)) {
     l = ab;
+    wb = 1.0f;
   } else {
     ff vc = ff_sub(ff_mul(d1, d4), ff_mul(d3, d2));
     if (ff_sign(vc) <= 0 && ff_sign(d1) >= 0 && ff_sign(d3) <= 0) {
-      l = ff3_scale(ab, ff_div(d1, ff_sub(d1, d3)));
+      ff v = ff_div(d1, ff_sub(d1, d3));
+      l = ff3_scale(ab, v);
+      wb = v.hi;
     } else if (ff_sign(d6) >= 0 && !ff_lt(d6, d5)) {
       l = ac;
+      wc = 1.0f;
     } else {
       ff vb = ff_sub(ff_mul(d5, d2), ff_mul(d1, d6));
       if (ff_sign(vb) <= 0 && ff_sign(d2) >= 0 && ff_sign(d6) <= 0) {
-        l = ff3_scale(ac, ff_div(d2, ff_sub(d2, d6)));
+        ff w = ff_div(d2, ff_sub(d2, d6));
+        l = ff3_scale(ac, w);
+        wc = w.hi;
       } else {
         ff va = ff_sub(ff_mul(d3, d6), ff_mul(d5, d4));
         ff d43 = ff_sub(d4, d3), d56 = ff_sub(d5, d6);
         if (ff_sign(va) <= 0 && ff_sign(d43) >= 0 && ff_sign(d56) >= 0) {
           ff w = ff_div(d43, ff_add(d43, d56));
           l = ff3_add(ab, ff3_scale(ff3_sub(ac, ab), w));
+          wb = 1.0f - w.hi;
+          wc = w.hi;
         } else {
           ff den = ff_add(ff_add(va, vb), vc);
           ff v = ff_div(vb, den), w = ff_div(vc, den);
           l = ff3_add(ff3_scale(ab, v), ff3_scale(ac, w));
+          wb = v.hi;
+          wc = w.hi;
         }
       }
     }
@@ -356,7 +369,10 @@ __device__ __noinline__ CPFF closest_ff(float3 p, float3 a, float3 b, float3 c) 
   ff3 r = ff3_sub(ap, l);
   CPFF out;
   out.d2 = ff3_dot(r, r);
+  out.r = r;
   out.q = {ff_add(ff_from(a.x), l.x), ff_add(ff_from(a.y), l.y), ff_add(ff_from(a.z), l.z)};
+  out.wb = wb;
+  out.wc = wc;
   return out;
 }
 
