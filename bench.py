@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest"], default="first",
+    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all"], default="first",
                     help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form; "
                          "adjoint: forward/backward timing; closest: the 256^3 closest-point grid")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
@@ -55,7 +55,9 @@ def parse():
     ap.add_argument("--ref-sample", type=int, default=1 << 21, help="rays per set per step in --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default traversal variant)")
-    ap.add_argument("--traversal", default=None, help="force a traversal variant 'persistent,order,refill'")
+    ap.add_argument("--traversal", default=None,
+                    help="force traversal variants: 'p,o,r,occ,compact,sort' for every ray set, or "
+                         "'incoherent=...;camera=...' per set")
     return ap.parse_args()
 
 
@@ -168,6 +170,17 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.smax,
                 "reasons": sorted(reasons), "samples": len(self.rows),
                 "power_w_max": max(r[2] for r in self.rows)}
+
+
+def parse_traversal(spec, names):
+    """'1,1,32,2,1,0' (every set) or 'incoherent=1,1,32,2,1,0;camera=2,1,16,2,1,2' (per set)."""
+    if "=" not in spec:
+        return [[int(x) for x in spec.split(",")]] * len(names)
+    per = {}
+    for part in spec.split(";"):
+        name, cfg = part.split("=")
+        per[name.strip()] = [int(x) for x in cfg.split(",")]
+    return [per.get(n) for n in names]
 
 
 def traversal_kernel(cfg):
@@ -288,7 +301,7 @@ def run_engine(args, ws, rank, local):
     tuned = {}
     configs = [None] * len(sets)
     if args.traversal:
-        configs = [[int(x) for x in args.traversal.split(",")]] * len(sets)
+        configs = parse_traversal(args.traversal, [n for n, _ in sets])
     elif not args.no_tune:
         from three_mesh_bvh_b200 import autotune
 
@@ -534,6 +547,88 @@ def run_closest(args, ws, rank, local):
     bvh.dispose()
 
 
+def run_all_hits(args, ws, rank, local):
+    """raycast (all hits, capped at 64 per ray plus the uncapped count) on the 2M-triangle knot's
+    two ray sets."""
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    from three_mesh_bvh_b200._native import check
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo, bvh, inc, cam = scene(pkg, args, rank)
+    sets = [("incoherent", inc), ("camera", cam)]
+    cap = 64
+    stream = torch.cuda.current_stream(dev)
+    n_max = max(r.shape[0] for _, r in sets)
+    counts = torch.empty(n_max, dtype=torch.int32, device=dev)
+    hits = torch.empty((n_max, cap, 8), dtype=torch.float32, device=dev)   # 32 B per hit slot
+    lib = pkg.lib()
+    per_set_ms, stored = [], []
+    with ClockSampler(local) as clk:
+        for name, r in sets:
+            d = torch.from_numpy(r).to(dev)
+            n = d.shape[0]
+
+            def call():
+                check(lib.bvhc_raycast(bvh._device_mesh(), d.data_ptr(), n, 0, 0.0, math.inf, cap,
+                                       counts.data_ptr(), hits.data_ptr(), 1, stream.cuda_stream), "bvhc_raycast")
+
+            for _ in range(args.warmup):
+                call()
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                call()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            per_set_ms.append(max_over_ranks(a.elapsed_time(b) / args.steps, ws, dev))
+            stored.append(int(counts[:n].clamp(max=cap).sum().item()))
+            del d
+    bvh.synchronize(stream.cuda_stream)
+    n_step = sum(r.shape[0] for _, r in sets)
+    ms = sum(per_set_ms)
+    cpu = roof = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle.oracle as orc
+
+        ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+        threads = os.cpu_count() or 1
+        t_cpu, n_cpu, bytes_per_set = 0.0, 0, []
+        for (name, r), sh in zip(sets, stored):
+            idx = np.linspace(0, r.shape[0] - 1, min(r.shape[0], args.cpu_sample // 4)).astype(np.int64)
+            t0 = time.perf_counter()
+            _, _, nn, nt = ref.raycast_all(np.ascontiguousarray(r[idx]), cap=cap, threads=threads, counters=True)
+            t_cpu += time.perf_counter() - t0
+            n_cpu += idx.size
+            # ray in + uncapped count + 32-byte records of the stored hits + reference node / triangle reads
+            bytes_per_set.append(r.shape[0] * (BYTES_RAY_IN + 4 + BYTES_NODE * float(nn.mean()) +
+                                               BYTES_TRI * float(nt.mean())) + BYTES_HIT_OUT * sh)
+        cpu = {"value": n_cpu / t_cpu / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n_cpu} rays ({args.cpu_sample // 4} evenly strided from each set), float64 oracle"}
+        peak, how = measured_peak()
+        k = max(range(len(sets)), key=lambda j: per_set_ms[j])
+        achieved = bytes_per_set[k] / (per_set_ms[k] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": how, "kernel": "raycast_all_kernel", "ray_set": sets[k][0],
+                "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], bytes_per_set))}
+    if rank == 0:
+        line = {"metric": "Mrays/s raycast all hits (2M tri, cap 64)", "value": weak_scaling_rate(ws, n_step, 1, ms),
+                "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD.replace("raycastFirst", "raycast (all hits, cap 64)"),
+                           "rays_per_step": n_step, "stored_hits": dict(zip([n for n, _ in sets], stored))},
+                "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": 2 * args.steps}
+        print(json.dumps(line), flush=True)
+    bvh.dispose()
+
+
 def run_adjoint(args, ws, rank, local):
     """Differentiable depth and SDF on the 2M-triangle knot: forward raycastFirst of a 1024^2 camera
     and backward of L = sum (t - t*)^2 (t* rendered from the mesh with vertices moved by N(0, 0.01),
@@ -622,6 +717,8 @@ def main():
             run_adjoint(args, ws, rank, local)
         elif args.workload == "closest":
             run_closest(args, ws, rank, local)
+        elif args.workload == "all":
+            run_all_hits(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:

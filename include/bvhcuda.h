@@ -129,8 +129,9 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * thread; 2 runs the 32 rays of a warp through one shared traversal (for coherent rays such as a
  * camera's).  Batched launches always use the persistent form.  order = 0 visits the near child
  * by the sign of the ray direction on the split axis (the reference's order), 1 by the smaller
- * entry distance.  occupancy selects the persistent kernel's register budget: 0 the compiler's
- * choice, 1 at least six and 2 at least eight resident 128-thread blocks per SM.  compact = 1
+ * entry distance.  occupancy selects the register budget of the persistent and warp-cooperative
+ * kernels: 0 the compiler's choice, 1 at least six and 2 at least eight resident 128-thread
+ * blocks per SM.  compact = 1
  * (persistent = 1 or 2) first finishes, in one coalesced pass, the rays that miss every root's
  * child boxes and traverses only the others.  sort (persistent = 1 or 2, single meshes; implies
  * the compaction pass) orders the remaining rays by a 30-bit Morton key before the traversal:

@@ -19,7 +19,7 @@ from pathlib import Path
 # and the Morton-key ray ordering (0 none, 1 direction, 2 entry point, 3 entry point + direction).
 _QUEUE = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)]
 CANDIDATES = [(0, 0, 16, 0, 0, 0), (0, 1, 16, 0, 0, 0)] + [
-    (2, order, 16, 0, c, s) for order in (0, 1) for c, s in _QUEUE] + [
+    (2, order, 16, occ, c, s) for order in (0, 1) for occ in (0, 1, 2) for c, s in _QUEUE] + [
     (1, order, refill, occ, c, s) for order in (0, 1) for refill in (16, 32) for occ in (1, 2) for c, s in _QUEUE]
 
 _cache: dict = {}

@@ -211,7 +211,6 @@ void free_sort_scratch(RaySortScratch& s) {
   cudaFree(s.vals);
   cudaFree(s.hist);
   cudaFree(s.totals);
-  cudaFree(s.dir_bounds);
   s = RaySortScratch{};
 }
 
@@ -540,8 +539,7 @@ static cudaError_t ensure_sort_scratch(bvhc_mesh* m, int slot, uint64_t n) {
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.keys[1]), n * 4);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.vals), n * 4);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.hist), 256 * ray_sort_tiles(n) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.totals), 4 * 256 * 4);
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.dir_bounds), 6 * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.totals), 3 * 256 * 4);
   if (e != cudaSuccess) {
     free_sort_scratch(s);
     return e;
@@ -592,8 +590,8 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
     cudaError_t e = queue_for(m, qslot, n, &q, &qc, &sort, &sorted);
     if (e != cudaSuccess) return e;
     if (m->cfg.persistent == 2)
-      return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s, q, qc,
-                                         sorted ? &sort : nullptr);
+      return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order,
+                                         m->cfg.occupancy, s, q, qc, sorted ? &sort : nullptr);
     return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
                                            s, q, qc, sorted ? &sort : nullptr);
   }
@@ -604,7 +602,8 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
 static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* rays, uint64_t n, int side,
                                  float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
   if (m->cfg.persistent == 2)
-    return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order, s);
+    return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order,
+                                       m->cfg.occupancy, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;

@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "raykey.cuh"
 #include "robust.cuh"
 
 namespace bvhc {
@@ -311,8 +312,8 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
 // ---------------------------------------------------------------------------------------------
 constexpr int kWarps = kBlock / 32;
 
-template <int ORDER>
-__global__ void __launch_bounds__(kBlock) raycast_first_packet_kernel(MeshDev m, const float* __restrict__ rays,
+template <int ORDER, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet_kernel(MeshDev m, const float* __restrict__ rays,
                                                                       uint64_t n, int side, const SideTable sides,
                                                                       float near_d, float far_d,
                                                                       bvhc_hit* __restrict__ out,
@@ -819,46 +820,83 @@ __global__ void __launch_bounds__(kBlock) finalize_first_kernel(MeshDev m, const
   }
 }
 
-// Pre-pass for the persistent traversal: a ray whose box tests against every root's two children
-// (with the root's own leaf case always live) all fail cannot hit anything; it is finished here with
-// a coalesced miss record.  The other rays are appended to `queue` (warp-aggregated atomics), so the
-// traversal kernel's warps only carry rays that enter the tree.
+// Pre-pass for the persistent and warp-cooperative traversals: a ray whose box tests against every
+// root's two children (with the root's own leaf case always live) all fail cannot hit anything; it
+// is finished here with a coalesced miss record.  The other rays are appended to `queue` in ray
+// order (one atomic per block reserves the block's run; positions within it come from ballots), so
+// the traversal kernel's warps only carry rays that enter the tree.  With `keys`, each queued ray's
+// ordering key (raykey.cuh, kind `kind`) is written beside its id.
+constexpr int kClsThreads = 256;
+constexpr int kClsItems = 8;
+constexpr int kClsTile = kClsThreads * kClsItems;  // rays per block
+constexpr int kClsWarps = kClsThreads / 32;
+
 template <bool BATCHED>
-__global__ void __launch_bounds__(kBlock) classify_kernel(MeshDev m, const BatchDev bd, const float* __restrict__ rays,
-                                                          uint64_t n, float near_d, float far_d,
-                                                          bvhc_hit* __restrict__ out, uint32_t* __restrict__ queue,
-                                                          unsigned int* __restrict__ qcount) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = false;
-  if (i < n) {
-    RayF r = make_ray(rays, i);
-    int root = 0, root_end = m.n_roots;
-    if (BATCHED) {
-      int mesh = mesh_of_ray(bd, i);
-      root = (int)__ldg(bd.mesh_root_off + mesh);
-      root_end = (int)__ldg(bd.mesh_root_off + mesh + 1);
-    }
-    for (; root < root_end && !live; ++root) {
-      uint32_t link = __ldg(m.roots + root);
-      if (link & kLeafBit) {
-        live = link != kEmptyLeaf;
-        continue;
+__global__ void __launch_bounds__(kClsThreads) classify_kernel(
+    MeshDev m, const BatchDev bd, const float* __restrict__ rays, uint64_t n, float near_d, float far_d,
+    bvhc_hit* __restrict__ out, uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
+    uint32_t* __restrict__ keys, int kind, SceneBox box) {
+  __shared__ unsigned s_cnt[kClsItems * kClsWarps];  // live rays per (item round, warp), then prefixes
+  __shared__ unsigned s_base;
+  const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * kClsTile;
+  unsigned ballot[kClsItems];
+  uint32_t key[kClsItems];
+#pragma unroll
+  for (int j = 0; j < kClsItems; ++j) {
+    uint64_t i = base + (uint64_t)j * kClsThreads + threadIdx.x;
+    bool live = false;
+    key[j] = 0;
+    if (i < n) {
+      RayF r = make_ray(rays, i);
+      int root = 0, root_end = m.n_roots;
+      if (BATCHED) {
+        int mesh = mesh_of_ray(bd, i);
+        root = (int)__ldg(bd.mesh_root_off + mesh);
+        root_end = (int)__ldg(bd.mesh_root_off + mesh + 1);
       }
-      Pair p = load_pair(m.nodes, link);
-      float e;
-      live = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e) ||
-             box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e);
+      for (; root < root_end && !live; ++root) {
+        uint32_t link = __ldg(m.roots + root);
+        if (link & kLeafBit) {
+          live = link != kEmptyLeaf;
+          continue;
+        }
+        Pair p = load_pair(m.nodes, link);
+        float e;
+        live = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e) ||
+               box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e);
+      }
+      if (!live) store_miss(out + i);
+      else if (keys) key[j] = ray_key(kind, r.o, r.d, box);
     }
-    if (!live) store_miss(out + i);
+    ballot[j] = __ballot_sync(0xFFFFFFFFu, live);
+    if (lane == 0) s_cnt[j * kClsWarps + w] = (unsigned)__popc(ballot[j]);
   }
-  unsigned mask = __ballot_sync(0xFFFFFFFFu, live);
-  if (mask) {
-    unsigned lane = threadIdx.x & 31u;
-    int leader = __ffs(mask) - 1;
-    unsigned base = 0;
-    if ((int)lane == leader) base = atomicAdd(qcount, (unsigned)__popc(mask));
-    base = __shfl_sync(0xFFFFFFFFu, base, leader);
-    if (live) queue[base + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)i;
+  __syncthreads();
+  if (w == 0) {
+    // exclusive scan of the 64 counts in (round, warp) order, which is ray order
+    static_assert(kClsItems * kClsWarps == 64, "two counts per lane");
+    unsigned a = s_cnt[2 * lane], b = s_cnt[2 * lane + 1];
+    unsigned incl = a + b;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= (unsigned)o) incl += y;
+    }
+    unsigned excl = incl - a - b;
+    s_cnt[2 * lane] = excl;
+    s_cnt[2 * lane + 1] = excl + a;
+    unsigned total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (lane == 0) s_base = total ? atomicAdd(qcount, total) : 0u;
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < kClsItems; ++j) {
+    if (ballot[j] & (1u << lane)) {
+      unsigned pos = s_base + s_cnt[j * kClsWarps + w] + (unsigned)__popc(ballot[j] & lt);
+      queue[pos] = (uint32_t)(base + (uint64_t)j * kClsThreads + threadIdx.x);
+      if (keys) keys[pos] = key[j];
+    }
   }
 }
 
@@ -921,15 +959,29 @@ static cudaError_t prepare_queue(const MeshDev& m, const BatchDev* batch, const 
   cudaError_t e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream);
   if (e != cudaSuccess) return e;
   BatchDev bd = batch ? *batch : BatchDev{nullptr, nullptr, 0};
+  const bool sorted = sort && !batch && sort->kind > 0;
+  // a sorted queue is first written (with keys) into the sort's scratch, which the sort drains into
+  // `queue`
+  uint32_t* ids = sorted ? sort->scratch.vals : queue;
+  uint32_t* keys = sorted ? sort->scratch.keys[1] : nullptr;
+  dev::SceneBox box{};
+  if (sorted) {
+    for (int a = 0; a < 3; ++a) {
+      box.lo[a] = sort->lo[a];
+      box.hi[a] = sort->hi[a];
+    }
+  }
+  const int kind = sorted ? sort->kind : 0;
+  const unsigned int g = (unsigned int)((n + dev::kClsTile - 1) / dev::kClsTile);
   if (batch)
-    dev::classify_kernel<true><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
-                                                                       qcount);
+    dev::classify_kernel<true><<<g, dev::kClsThreads, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, ids, qcount,
+                                                                   keys, kind, box);
   else
-    dev::classify_kernel<false><<<grid_for(n), dev::kBlock, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, queue,
-                                                                        qcount);
+    dev::classify_kernel<false><<<g, dev::kClsThreads, 0, stream>>>(m, bd, rays, n, near_d, far_d, out, ids, qcount,
+                                                                    keys, kind, box);
   e = cudaGetLastError();
-  if (e != cudaSuccess || !sort || batch || sort->kind == 0) return e;
-  return launch_ray_sort(rays, n, sort->kind, sort->lo, sort->hi, queue, qcount, sort->scratch, stream);
+  if (e != cudaSuccess || !sorted) return e;
+  return launch_ray_sort(n, qcount, sort->scratch, queue, stream);
 }
 
 cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,
@@ -964,7 +1016,7 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        cudaStream_t stream, uint32_t* queue, unsigned int* qcount,
+                                        int occupancy, cudaStream_t stream, uint32_t* queue, unsigned int* qcount,
                                         const RaySort* sort) {
   if (n == 0) return cudaSuccess;
   const bool compact = queue != nullptr && qcount != nullptr && n < (1ull << 32);
@@ -975,12 +1027,13 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
     queue = nullptr;
     qcount = nullptr;
   }
-  if (order == 0)
-    dev::raycast_first_packet_kernel<0><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
-                                                                                 far_d, out, queue, qcount);
-  else
-    dev::raycast_first_packet_kernel<1><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d,
-                                                                                 far_d, out, queue, qcount);
+  auto kernel = order == 0 ? (occupancy == 0 ? dev::raycast_first_packet_kernel<0, 1>
+                                              : occupancy == 1 ? dev::raycast_first_packet_kernel<0, 6>
+                                                               : dev::raycast_first_packet_kernel<0, 8>)
+                            : (occupancy == 0 ? dev::raycast_first_packet_kernel<1, 1>
+                                              : occupancy == 1 ? dev::raycast_first_packet_kernel<1, 6>
+                                                               : dev::raycast_first_packet_kernel<1, 8>);
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount);
   return cudaGetLastError();
 }
 

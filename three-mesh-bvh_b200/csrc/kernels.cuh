@@ -45,14 +45,13 @@ struct TraversalConfig {
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
 struct RaySortScratch {
-  uint32_t* keys[2];     // n entries each
-  uint32_t* vals;        // n entries: the queue's ping-pong partner
-  uint32_t* hist;        // 256 * ray_sort_tiles(n) entries
-  uint32_t* totals;      // 4 * 256 entries
-  uint32_t* dir_bounds;  // 6 entries
+  uint32_t* keys[2];  // n entries each; the pre-pass writes keys[1]
+  uint32_t* vals;     // n entries: the pre-pass writes the queued ray ids here, the sort ends in the queue
+  uint32_t* hist;     // 256 * ray_sort_tiles(n) entries
+  uint32_t* totals;   // 3 * 256 entries
 };
 
-// A sort request: key kind (1..3) and the scene box used by the entry-point keys.
+// A sort request: key kind (1..3, raykey.cuh) and the scene box used by the entry-point keys.
 struct RaySort {
   int kind;
   float lo[3], hi[3];
@@ -60,9 +59,9 @@ struct RaySort {
 };
 
 uint64_t ray_sort_tiles(uint64_t n);
-// Sorts the first *qcount ids of `queue` (rays into the mesh) by the key `kind`; n bounds *qcount.
-cudaError_t launch_ray_sort(const float* rays, uint64_t n, int kind, const float scene_lo[3], const float scene_hi[3],
-                            uint32_t* queue, const unsigned int* qcount, const RaySortScratch& s,
+// Sorts the *qcount (key, id) pairs the pre-pass left in (scratch.keys[1], scratch.vals) by key,
+// stably, into `queue` (ids); n bounds *qcount.
+cudaError_t launch_ray_sort(uint64_t n, const unsigned int* qcount, const RaySortScratch& s, uint32_t* queue,
                             cudaStream_t stream);
 
 // Many meshes in one node/triangle pool: rays [ray_off[k], ray_off[k+1]) belong to mesh k, whose
@@ -85,8 +84,8 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 // queue, the same pre-pass (and sort) as the persistent form runs first.
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        cudaStream_t stream, uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
-                                        const RaySort* sort = nullptr);
+                                        int occupancy, cudaStream_t stream, uint32_t* queue = nullptr,
+                                        unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream);
 
