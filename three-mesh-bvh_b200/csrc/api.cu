@@ -539,7 +539,7 @@ static cudaError_t ensure_sort_scratch(bvhc_mesh* m, int slot, uint64_t n) {
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.keys[1]), n * 4);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.vals), n * 4);
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.hist), 256 * ray_sort_tiles(n) * 4);
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.totals), 3 * 256 * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s.totals), 4 * 256 * 4);
   if (e != cudaSuccess) {
     free_sort_scratch(s);
     return e;

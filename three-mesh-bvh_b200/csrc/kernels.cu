@@ -960,10 +960,10 @@ static cudaError_t prepare_queue(const MeshDev& m, const BatchDev* batch, const 
   if (e != cudaSuccess) return e;
   BatchDev bd = batch ? *batch : BatchDev{nullptr, nullptr, 0};
   const bool sorted = sort && !batch && sort->kind > 0;
-  // a sorted queue is first written (with keys) into the sort's scratch, which the sort drains into
-  // `queue`
-  uint32_t* ids = sorted ? sort->scratch.vals : queue;
-  uint32_t* keys = sorted ? sort->scratch.keys[1] : nullptr;
+  // a sorted queue is first written (with keys) where the sort's passes start, so they end in `queue`
+  uint32_t* ids = queue;
+  uint32_t* keys = nullptr;
+  if (sorted) ray_sort_input(sort->kind, sort->scratch, queue, &ids, &keys);
   dev::SceneBox box{};
   if (sorted) {
     for (int a = 0; a < 3; ++a) {
@@ -981,7 +981,7 @@ static cudaError_t prepare_queue(const MeshDev& m, const BatchDev* batch, const 
                                                                     keys, kind, box);
   e = cudaGetLastError();
   if (e != cudaSuccess || !sorted) return e;
-  return launch_ray_sort(n, qcount, sort->scratch, queue, stream);
+  return launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream);
 }
 
 cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* batch, const float* rays, uint64_t n,

@@ -45,10 +45,10 @@ struct TraversalConfig {
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
 struct RaySortScratch {
-  uint32_t* keys[2];  // n entries each; the pre-pass writes keys[1]
-  uint32_t* vals;     // n entries: the pre-pass writes the queued ray ids here, the sort ends in the queue
+  uint32_t* keys[2];  // n entries each
+  uint32_t* vals;     // n entries: the queue's ping-pong partner
   uint32_t* hist;     // 256 * ray_sort_tiles(n) entries
-  uint32_t* totals;   // 3 * 256 entries
+  uint32_t* totals;   // 4 * 256 entries (one row per pass)
 };
 
 // A sort request: key kind (1..3, raykey.cuh) and the scene box used by the entry-point keys.
@@ -59,10 +59,13 @@ struct RaySort {
 };
 
 uint64_t ray_sort_tiles(uint64_t n);
-// Sorts the *qcount (key, id) pairs the pre-pass left in (scratch.keys[1], scratch.vals) by key,
-// stably, into `queue` (ids); n bounds *qcount.
-cudaError_t launch_ray_sort(uint64_t n, const unsigned int* qcount, const RaySortScratch& s, uint32_t* queue,
-                            cudaStream_t stream);
+// Where the pre-pass writes the (key, id) pairs for a sort of key `kind`, so that the sort's last
+// pass ends in `queue`.
+void ray_sort_input(int kind, const RaySortScratch& s, uint32_t* queue, uint32_t** ids, uint32_t** keys);
+// Sorts the *qcount (key, id) pairs at ray_sort_input's buffers by key, stably, into `queue` (ids);
+// n bounds *qcount.
+cudaError_t launch_ray_sort(int kind, uint64_t n, const unsigned int* qcount, const RaySortScratch& s,
+                            uint32_t* queue, cudaStream_t stream);
 
 // Many meshes in one node/triangle pool: rays [ray_off[k], ray_off[k+1]) belong to mesh k, whose
 // roots are MeshDev::roots[mesh_root_off[k] .. mesh_root_off[k+1]).

@@ -1,21 +1,23 @@
 // Morton keys that order rays for coherent traversal (computed by the root-box pre-pass, sorted by
-// raysort.cu).  Every key has 24 significant bits (three 8-bit radix passes).
+// raysort.cu, one 8-bit radix pass per started byte of key_bits(kind)).
 //   1  direction as a cube-map coordinate: the face of the dominant axis (3 bits) followed by the
-//      two minor components divided by the major one, 10 bits each over [-1, 1], interleaved
-//      (2-D Morton).  For a pinhole camera this is image space: the order is a Morton walk over
-//      cells of a few pixels, each cell keeping its rays' input order.
+//      two minor components divided by the major one, 13 bits each over [-1, 1], interleaved
+//      (2-D Morton; 29 bits).  For a pinhole camera this is image space: the order is a Morton
+//      walk over cells of about a pixel (a 45-degree view spans ~3400 of the 8192 levels).
 //   2  scene entry point: where the ray enters the mesh's bounding box (its origin if it starts
-//      inside), 8 bits per axis over that box, interleaved (3-D Morton).
+//      inside), 8 bits per axis over that box, interleaved (3-D Morton; 24 bits).
 //   3  entry point (5 bits per axis, interleaved) followed by the normalised direction (3 bits per
-//      axis over [-1, 1], interleaved).
+//      axis over [-1, 1], interleaved; 24 bits).
 #pragma once
 
 #include <cstdint>
 
 namespace bvhc {
-namespace dev {
 
-constexpr int kKeyBits = 24;
+// Radix passes (8-bit digits) that sort keys of `kind`.
+inline int ray_sort_passes(int kind) { return kind == 1 ? 4 : 3; }
+
+namespace dev {
 
 __device__ __forceinline__ uint32_t spread3(uint32_t x) {  // 10 bits -> every third bit of 30
   x &= 0x3FFu;
@@ -66,8 +68,8 @@ __device__ __forceinline__ uint32_t ray_key(int kind, float3 o, float3 d, const 
       u = d.x; v = d.y; m = az;
     }
     float im = m > 0.0f ? 1.0f / m : 0.0f;
-    return (face << 20) | spread2(quantise(u * im, -1.0f, 0.5f, 1024.0f)) |
-           (spread2(quantise(v * im, -1.0f, 0.5f, 1024.0f)) << 1);
+    return (face << 26) | spread2(quantise(u * im, -1.0f, 0.5f, 8192.0f)) |
+           (spread2(quantise(v * im, -1.0f, 0.5f, 8192.0f)) << 1);
   }
   if (kind != 2 && kind != 3) return 0u;
   // entry into the scene box: the largest near-slab distance, not before the origin

@@ -1,11 +1,11 @@
 // Ray ordering for coherence: the root-box pre-pass (classify_kernel) queues the rays that can hit
-// the mesh together with a 24-bit Morton key (raykey.cuh), and this file sorts the queue by that
+// the mesh together with a Morton key (raykey.cuh), and this file sorts the queue by that
 // key, so that the rays a warp takes together start near each other and point the same way.  The
 // traversal kernels then walk the queue in sorted order; results are still written to each ray's
 // own slot, so ordering changes speed only, never results.
 //
-// The sort is a stable least-significant-digit radix sort of (key, ray id) pairs: three passes of
-// 8-bit digits.  Each pass:
+// The sort is a stable least-significant-digit radix sort of (key, ray id) pairs: one pass per
+// 8-bit digit of the key kind's width.  Each pass:
 //   upsweep  counts each tile's digits (4096 items per block) into a digit x tile matrix;
 //   scan     turns the matrix into output offsets (digit-major: all of digit 0, then digit 1, ...);
 //   scatter  ranks each item within its tile (warp match + per-warp counts in shared memory, in
@@ -18,6 +18,7 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "raykey.cuh"
 
 namespace bvhc {
 namespace dev {
@@ -26,7 +27,6 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 items per block
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortPasses = 3;                        // 24-bit keys
 
 // Upsweep: hist[digit * nblocks + block] = count of `digit` in the block's tile; totals[digit] += it.
 __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const uint32_t* __restrict__ keys,
@@ -188,16 +188,26 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(
 
 uint64_t ray_sort_tiles(uint64_t n) { return (n + dev::kSortTile - 1) / dev::kSortTile; }
 
-cudaError_t launch_ray_sort(uint64_t n, const unsigned int* qcount, const RaySortScratch& s, uint32_t* queue,
-                            cudaStream_t stream) {
+void ray_sort_input(int kind, const RaySortScratch& s, uint32_t* queue, uint32_t** ids, uint32_t** keys) {
+  const bool odd = ray_sort_passes(kind) & 1;
+  *ids = odd ? s.vals : queue;
+  *keys = odd ? s.keys[1] : s.keys[0];
+}
+
+cudaError_t launch_ray_sort(int kind, uint64_t n, const unsigned int* qcount, const RaySortScratch& s,
+                            uint32_t* queue, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   const uint32_t nblocks = (uint32_t)ray_sort_tiles(n);
-  cudaError_t e = cudaMemsetAsync(s.totals, 0, dev::kSortPasses * 256 * sizeof(uint32_t), stream);
+  const int passes = ray_sort_passes(kind);
+  cudaError_t e = cudaMemsetAsync(s.totals, 0, passes * 256 * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
-  // the pre-pass wrote (keys[1], vals); an odd number of passes ends in (keys[0], queue)
-  uint32_t* kbuf[2] = {s.keys[1], s.keys[0]};
-  uint32_t* vbuf[2] = {s.vals, queue};
-  for (int pass = 0; pass < dev::kSortPasses; ++pass) {
+  // the pre-pass wrote the pairs where ray_sort_input put them, so the last pass ends in
+  // (keys, queue)
+  uint32_t *ids0, *keys0;
+  ray_sort_input(kind, s, queue, &ids0, &keys0);
+  uint32_t* kbuf[2] = {keys0, keys0 == s.keys[0] ? s.keys[1] : s.keys[0]};
+  uint32_t* vbuf[2] = {ids0, ids0 == queue ? s.vals : queue};
+  for (int pass = 0; pass < passes; ++pass) {
     const int src = pass & 1, dst = src ^ 1;
     uint32_t* totals = s.totals + 256 * pass;
     dev::radix_upsweep_kernel<<<nblocks, dev::kSortThreads, 0, stream>>>(kbuf[src], qcount, 8 * pass, nblocks,
