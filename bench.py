@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--ref-sample", type=int, default=1 << 21, help="rays per set per step in --impl reference")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default traversal variant)")
+    ap.add_argument("--leaf-sizes", default="0,2,4",
+                    help="device leaf layouts the autotuner tries (0: the reference's leaves)")
+    ap.add_argument("--leaf-size", type=int, default=None, help="force a device leaf layout")
     ap.add_argument("--traversal", default=None,
                     help="force traversal variants: 'p,o,r,occ,compact,sort' for every ray set, or "
                          "'incoherent=...;camera=...' per set")
@@ -305,11 +308,16 @@ def run_engine(args, ws, rank, local):
     elif not args.no_tune:
         from three_mesh_bvh_b200 import autotune
 
-        for i, (name, _) in enumerate(sets):
-            # tuned on the whole set: ray ordering and the warp-cooperative form depend on the
-            # set's coherence at full size, which no strided or block sample reproduces
-            tuned[name] = autotune.tune_raycast_first(bvh, d_rays[i], tag=f"knot2M-{name}")
-            configs[i] = tuned[name]["best"]
+        # tuned on the whole sets: ray ordering and the warp-cooperative form depend on a set's
+        # coherence at full size, which no strided or block sample reproduces; one device leaf
+        # layout serves both sets
+        res = autotune.tune_raycast_first_sets(bvh, [(n, d) for (n, _), d in zip(sets, d_rays)],
+                                               leaf_sizes=[int(x) for x in args.leaf_sizes.split(",")],
+                                               tag="knot2M")
+        tuned = {"leaf_size": res["leaf"], "total_ms_by_leaf_size": res["total_ms"], **res["sets"]}
+        configs = [res["sets"][n]["best"] for n, _ in sets]
+    if args.leaf_size is not None:
+        bvh.set_leaf_size(args.leaf_size)
 
     def step(ev=None):
         for k in range(len(sets)):
@@ -399,6 +407,7 @@ def run_engine(args, ws, rank, local):
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
                 "traversal": {n: (list(c) if c is not None else None) for (n, _), c in zip(sets, configs)},
+                "leaf_size": bvh.get_leaf_size(),
                 "autotune": tuned, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
                 "gpu_launches": args.steps * sum(kernel_launches(c) for c in configs)}
         print(json.dumps(line), flush=True)

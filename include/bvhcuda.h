@@ -149,6 +149,15 @@ typedef struct bvhc_traversal_config {
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);
 
+/* Device leaf layout (no reference counterpart; the reference's own leaves are maxLeafSize-bounded,
+ * buildTree.js:64-89): max_leaf > 0 splits every leaf of more than max_leaf triangles into a
+ * subtree of exact-bounds child pairs (median split of the centroids along their longest axis);
+ * 0 restores the reference's leaves.  Only the grouping of triangles changes, so results are the
+ * same up to exact ties.  Waits for the device; graphs captured before must be captured again.
+ * bvhc_mesh_get_leaf_size returns the current setting (-1 for a null mesh). */
+bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* mesh, int max_leaf);
+int bvhc_mesh_get_leaf_size(const bvhc_mesh* mesh);
+
 /* Waits for the mesh's work on `stream` and reports (and clears) the device error word. */
 bvhc_status bvhc_mesh_synchronize(bvhc_mesh* mesh, void* stream);
 

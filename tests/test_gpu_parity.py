@@ -257,3 +257,48 @@ def test_pipelined_host_path_matches_device(pkg, knot80k, cuda):
         ac, ah = ref.raycast_all(rays[sub], cap=64)
         _assert_first_ok(check_first(host[sub], exp, tie_exempt(ac, ah)))
     bvh.set_traversal(1, 1, 16, 0, 0)
+
+
+@pytest.mark.parametrize("leaf", [1, 3, 4])
+def test_split_leaf_layouts_agree(pkg, orc, cuda, leaf):
+    """Device leaves split to at most `leaf` triangles: every query kind still matches the oracle
+    (which keeps the reference's leaves), and the reference layout comes back with leaf size 0."""
+    geo = pkg.torus_knot(10, 3, 300, 60, noise_sigma=0.02, noise_seed=1)
+    n = geo.index.size
+    step = (n // 3 // 5) * 3
+    for g in range(5):
+        geo.add_group(g * step, step if g < 4 else math.inf, g % 3)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = _oracle_for(orc, bvh, geo)
+    base_nodes = bvh.mesh_info()["node_records"]
+    bvh.set_leaf_size(leaf)
+    assert bvh.get_leaf_size() == leaf
+    assert bvh.mesh_info()["node_records"] > base_nodes
+    rays = np.concatenate([pkg.rays_incoherent(60_000, seed=4), pkg.rays_camera(160, 160),
+                           pkg.rays_sphere_to_box(30_000, seed=6)])
+    ac, ah = ref.raycast_all(rays, 0, cap=64)
+    exp = ref.raycast_first(rays, 0)
+    for cfg in ((0, 1, 16, 0, 0, 0), (1, 1, 32, 2, 1, 2), (2, 1, 16, 2, 1, 1)):
+        bvh.set_traversal(*cfg)
+        _assert_first_ok(check_first(bvh.raycast_first_batch(rays, 0), exp, tie_exempt(ac, ah)))
+    counts, hits = bvh.raycast_batch(rays, 0, cap=64)
+    rep = check_all(counts, hits, ac, ah)
+    assert rep["count"] == 0 and rep["set"] == 0, rep
+    sides = [0, 1, 2]
+    ref.set_materials(geo.groups, sides)
+    mexp = ref.raycast_first(rays)
+    mac, mah = ref.raycast_all(rays, cap=64)
+    _assert_first_ok(check_first(bvh.raycast_first_batch(rays, sides), mexp, tie_exempt(mac, mah)))
+    pts = pkg.grid_points(geo.position.min(0), geo.position.max(0), 24)
+
+    def tri_distance(i, face):
+        t = geo.triangle(face)
+        q = orc.closest_point_triangle(pts[i].astype(np.float64), *t)
+        return float(np.linalg.norm(q - pts[i].astype(np.float64)))
+
+    rep = check_closest(bvh.closest_point_batch(pts, 0.0, 5.0), ref.closest_point(pts, 0.0, 5.0), tri_distance)
+    assert rep["null"] == 0 and rep["distance"] == 0 and rep["face"] == 0, rep
+    bvh.set_leaf_size(0)
+    assert bvh.mesh_info()["node_records"] == base_nodes
+    _assert_first_ok(check_first(bvh.raycast_first_batch(rays, 0), exp, tie_exempt(ac, ah)))
+    bvh.dispose()

@@ -66,6 +66,8 @@ SIGNATURES = [
     ("bvhc_raycast_first_noalloc", _I, [_P, _P, _U64, _I, _F, _F, _P, _I, _P]),
     ("bvhc_mesh_set_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_mesh_get_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
+    ("bvhc_mesh_set_leaf_size", _I, [_P, C.c_int]),
+    ("bvhc_mesh_get_leaf_size", C.c_int, [_P]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
 ]

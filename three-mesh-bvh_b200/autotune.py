@@ -68,3 +68,19 @@ def tune_raycast_first(bvh, rays, side: int = 0, near: float = 0.0, far: float =
     if cache_file is not None:
         Path(cache_file).write_text(json.dumps(_cache, indent=1))
     return entry
+
+
+def tune_raycast_first_sets(bvh, named_rays, leaf_sizes=(0,), tag: str = "default", **kw) -> dict:
+    """Tune several ray sets that share one mesh: the device leaf layout (bvh.set_leaf_size; one
+    layout serves every set) is chosen by the sum of the sets' best times, and each set keeps its
+    own traversal variant for that layout.  named_rays: [(name, rays)].  Leaves the chosen layout
+    installed and returns {"leaf": L, "sets": {name: entry}, "total_ms": {L: ms}}."""
+    per_leaf, totals = {}, {}
+    for leaf in leaf_sizes:
+        bvh.set_leaf_size(leaf)
+        per_leaf[leaf] = {name: tune_raycast_first(bvh, rays, tag=f"{tag}-{name}-leaf{leaf}", **kw)
+                          for name, rays in named_rays}
+        totals[leaf] = sum(e["ms"] for e in per_leaf[leaf].values())
+    leaf = min(totals, key=totals.get)
+    bvh.set_leaf_size(leaf)
+    return {"leaf": leaf, "sets": per_leaf[leaf], "total_ms": {str(k): v for k, v in totals.items()}}

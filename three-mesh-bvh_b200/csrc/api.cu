@@ -61,6 +61,13 @@ struct bvhc_mesh {
   uint32_t* d_index32 = nullptr;
   float* d_pos = nullptr;
   uint64_t grad_tris = 0, grad_verts = 0;
+  // the records as converted from the reference's tree (leaf layout 0), kept on the host so that
+  // bvhc_mesh_set_leaf_size can re-lay the device records out; materials follow set_groups
+  std::vector<PairNode> h_pairs;
+  std::vector<TriRecord> h_tris;
+  std::vector<uint32_t> h_roots;
+  int h_max_depth = 0;
+  int leaf_size = 0;
 
   MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
 };
@@ -257,6 +264,100 @@ void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_
   }
 }
 
+// Device leaf layout: every leaf of the reference's tree with more than `max_leaf` triangles becomes
+// a subtree of child-pair records over its triangles (the reference's tree above it is kept as is).
+// A range is split at the median of the triangle centroids along the longest axis of the centroid
+// bounds (ties in input order), and each side gets the exact float32 bounds of its vertices.  Only
+// the grouping of triangles into leaves changes; which triangle is nearest does not, so results are
+// the same up to exact ties.
+struct LeafSplitter {
+  const std::vector<PairNode>& pairs;
+  const std::vector<TriRecord>& tris;
+  int max_leaf;
+  std::vector<PairNode> out_pairs;
+  std::vector<TriRecord> out_tris;
+  int max_depth = 0;
+
+  static void bounds(const TriRecord* t, size_t n, float* box) {
+    for (int a = 0; a < 3; ++a) {
+      box[a] = t[0].v[a];
+      box[3 + a] = t[0].v[a];
+    }
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) {
+          box[a] = std::min(box[a], t[i].v[3 * k + a]);
+          box[3 + a] = std::max(box[3 + a], t[i].v[3 * k + a]);
+        }
+  }
+
+  uint32_t split(std::vector<TriRecord>& run, size_t lo, size_t hi, int depth) {
+    if (depth >= kMaxStack - 1) throw Status{BVHC_ERR_UNSUPPORTED};
+    max_depth = std::max(max_depth, depth);
+    const size_t n = hi - lo;
+    if ((int)n <= max_leaf) {
+      uint32_t first = (uint32_t)out_tris.size();
+      if (out_tris.size() + n >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
+      for (size_t i = lo; i < hi; ++i) {
+        TriRecord r = run[i];
+        r.flags = (i + 1 == hi) ? kTriLast : 0u;
+        out_tris.push_back(r);
+      }
+      return kLeafBit | first;
+    }
+    float c_lo[3], c_hi[3];
+    auto centroid = [](const TriRecord& t, int a) { return t.v[a] + t.v[3 + a] + t.v[6 + a]; };
+    for (int a = 0; a < 3; ++a) c_lo[a] = c_hi[a] = centroid(run[lo], a);
+    for (size_t i = lo; i < hi; ++i)
+      for (int a = 0; a < 3; ++a) {
+        c_lo[a] = std::min(c_lo[a], centroid(run[i], a));
+        c_hi[a] = std::max(c_hi[a], centroid(run[i], a));
+      }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a)
+      if (c_hi[a] - c_lo[a] > c_hi[axis] - c_lo[axis]) axis = a;
+    std::stable_sort(run.begin() + lo, run.begin() + hi, [&](const TriRecord& x, const TriRecord& y) {
+      return centroid(x, axis) < centroid(y, axis);
+    });
+    const size_t mid = lo + n / 2;
+    if (out_pairs.size() >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
+    uint32_t idx = (uint32_t)out_pairs.size();
+    out_pairs.push_back(PairNode{});
+    uint32_t ll = split(run, lo, mid, depth + 1);
+    uint32_t lr = split(run, mid, hi, depth + 1);
+    PairNode& p = out_pairs[idx];
+    bounds(run.data() + lo, mid - lo, &p.f[0]);
+    bounds(run.data() + mid, hi - mid, &p.f[6]);
+    p.link[0] = ll;
+    p.link[1] = lr;
+    p.axis = (uint32_t)axis;
+    p.pad = 0;
+    return idx;
+  }
+
+  uint32_t copy(uint32_t link, int depth) {
+    if (link == kEmptyLeaf) return kEmptyLeaf;
+    if (link & kLeafBit) {
+      uint32_t k = link & ~kLeafBit;
+      std::vector<TriRecord> run;
+      for (;; ++k) {
+        run.push_back(tris[k]);
+        if (tris[k].flags & kTriLast) break;
+      }
+      return split(run, 0, run.size(), depth);
+    }
+    if (depth >= kMaxStack - 1) throw Status{BVHC_ERR_UNSUPPORTED};
+    max_depth = std::max(max_depth, depth);
+    uint32_t idx = (uint32_t)out_pairs.size();
+    out_pairs.push_back(pairs[link]);
+    uint32_t ll = copy(pairs[link].link[0], depth + 1);
+    uint32_t lr = copy(pairs[link].link[1], depth + 1);
+    out_pairs[idx].link[0] = ll;
+    out_pairs[idx].link[1] = lr;
+    return idx;
+  }
+};
+
 }  // namespace
 
 bool bvhc::mesh_launch_info(const bvhc_mesh* m, MeshDev* view, TraversalConfig* cfg, int* device) {
@@ -291,6 +392,10 @@ static bvhc_status finish_mesh(int device, const std::vector<PairNode>& pairs, c
   for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
   m->mesh_root_off = mesh_root_off;
   m->n_meshes = mesh_root_off.empty() ? 0 : (int)mesh_root_off.size() - 1;
+  m->h_pairs = pairs;
+  m->h_tris = tris;
+  m->h_roots = root_links;
+  m->h_max_depth = max_depth;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = upload(&m->d_nodes, pairs);
   if (e == cudaSuccess) e = upload(&m->d_tris, tris);
@@ -648,6 +753,62 @@ bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* c
   return BVHC_OK;
 }
 
+bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* m, int max_leaf) {
+  if (!m || max_leaf < 0 || max_leaf > 0xFFFF) return BVHC_ERR_INVALID_ARGUMENT;
+  if (max_leaf == m->leaf_size) return BVHC_OK;
+  std::vector<PairNode> pairs;
+  std::vector<TriRecord> tris;
+  std::vector<uint32_t> roots(m->h_roots.size());
+  int depth = 0;
+  if (max_leaf == 0) {
+    pairs = m->h_pairs;
+    tris = m->h_tris;
+    roots = m->h_roots;
+    depth = m->h_max_depth;
+  } else {
+    LeafSplitter sp{m->h_pairs, m->h_tris, max_leaf};
+    try {
+      for (size_t r = 0; r < roots.size(); ++r) roots[r] = sp.copy(m->h_roots[r], 0);
+    } catch (const Status& s) {
+      return s.code;
+    } catch (const std::bad_alloc&) {
+      return BVHC_ERR_OUT_OF_MEMORY;
+    }
+    pairs.swap(sp.out_pairs);
+    tris.swap(sp.out_tris);
+    depth = sp.max_depth;
+  }
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  BVHC_CUDA_TRY(cudaDeviceSynchronize());  // no launch may still read the old records
+  PairNode* nodes = nullptr;
+  TriRecord* recs = nullptr;
+  uint32_t* rts = nullptr;
+  cudaError_t e = upload(&nodes, pairs);
+  if (e == cudaSuccess) e = upload(&recs, tris);
+  if (e == cudaSuccess) e = upload(&rts, roots);
+  if (e != cudaSuccess) {
+    cudaFree(nodes);
+    cudaFree(recs);
+    cudaFree(rts);
+    return from_cuda(e);
+  }
+  cudaFree(m->d_nodes);
+  cudaFree(m->d_tris);
+  cudaFree(m->d_roots);
+  m->d_nodes = nodes;
+  m->d_tris = recs;
+  m->d_roots = rts;
+  m->n_nodes = pairs.size();
+  m->n_tris = tris.size();
+  m->max_depth = depth;
+  m->rec_face.resize(tris.size());
+  for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
+  m->leaf_size = max_leaf;
+  return BVHC_OK;
+}
+
+int bvhc_mesh_get_leaf_size(const bvhc_mesh* m) { return m ? m->leaf_size : -1; }
+
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* cfg) {
   if (!m || !cfg) return BVHC_ERR_INVALID_ARGUMENT;
   cfg->persistent = m->cfg.persistent;
@@ -757,17 +918,29 @@ bvhc_status bvhc_raycast_materials(bvhc_mesh* m, const float* rays, uint64_t n, 
 
 bvhc_status bvhc_mesh_set_groups(bvhc_mesh* m, const int64_t* groups, int n_groups) {
   if (!m || n_groups < 0 || (n_groups > 0 && !groups)) return BVHC_ERR_INVALID_ARGUMENT;
-  std::vector<uint32_t> mat(m->rec_face.size(), kNoMaterial);
-  for (size_t k = 0; k < m->rec_face.size(); ++k) {
-    int64_t first = 3 * (int64_t)m->rec_face[k];
+  // material of a triangle: the group holding its first index entry (kNoMaterial: none)
+  auto material_of = [&](uint32_t face, uint32_t* out) -> bvhc_status {
+    int64_t first = 3 * (int64_t)face;
+    uint32_t mat = kNoMaterial;
     for (int g = 0; g < n_groups; ++g) {
       int64_t start = groups[3 * g], count = groups[3 * g + 1], mi = groups[3 * g + 2];
       if (mi < 0 || mi >= (int64_t)kNoMaterial) return BVHC_ERR_INVALID_ARGUMENT;
       if (first >= start && (count < 0 || first < start + count)) {
-        if (mat[k] != kNoMaterial) return BVHC_ERR_UNSUPPORTED;  // triangle in two groups
-        mat[k] = (uint32_t)mi;
+        if (mat != kNoMaterial) return BVHC_ERR_UNSUPPORTED;  // triangle in two groups
+        mat = (uint32_t)mi;
       }
     }
+    *out = mat;
+    return BVHC_OK;
+  };
+  std::vector<uint32_t> mat(m->rec_face.size(), kNoMaterial);
+  for (size_t k = 0; k < m->rec_face.size(); ++k) {
+    bvhc_status st = material_of(m->rec_face[k], &mat[k]);
+    if (st != BVHC_OK) return st;
+  }
+  for (TriRecord& t : m->h_tris) {  // the host copy, for later leaf re-layouts
+    bvhc_status st = material_of(t.face, &t.material);
+    if (st != BVHC_OK) return st;
   }
   if (mat.empty()) return BVHC_OK;
   BVHC_CUDA_TRY(cudaSetDevice(m->device));

@@ -211,6 +211,14 @@ class MeshBVH:
         N.check(N.lib().bvhc_mesh_get_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_get_traversal")
         return {k: getattr(cfg, k) for k, _ in N.BvhcTraversalConfig._fields_}
 
+    def set_leaf_size(self, max_leaf: int) -> None:
+        """Device leaf layout (see bvhc_mesh_set_leaf_size): split leaves above max_leaf triangles;
+        0 restores the reference's leaves."""
+        N.check(N.lib().bvhc_mesh_set_leaf_size(self._device_mesh(), int(max_leaf)), "bvhc_mesh_set_leaf_size")
+
+    def get_leaf_size(self) -> int:
+        return int(N.lib().bvhc_mesh_get_leaf_size(self._device_mesh()))
+
     def dispose(self):
         if self._mesh is not None:
             N.lib().bvhc_mesh_destroy(self._mesh)
