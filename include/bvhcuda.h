@@ -149,12 +149,15 @@ typedef struct bvhc_traversal_config {
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);
 
-/* Device leaf layout (no reference counterpart; the reference's own leaves are maxLeafSize-bounded,
- * buildTree.js:64-89): max_leaf > 0 splits every leaf of more than max_leaf triangles into a
- * subtree of exact-bounds child pairs (median split of the centroids along their longest axis);
- * 0 restores the reference's leaves.  Only the grouping of triangles changes, so results are the
- * same up to exact ties.  Waits for the device; graphs captured before must be captured again.
- * bvhc_mesh_get_leaf_size returns the current setting (-1 for a null mesh). */
+/* Device leaf layout of raycastFirst (no reference counterpart; the reference's own leaves are
+ * maxLeafSize-bounded, buildTree.js:64-89): max_leaf > 0 gives raycastFirst (single, material,
+ * batched and no-alloc forms) its own copy of the tree in which every leaf of more than max_leaf
+ * triangles is a subtree of exact-bounds child pairs (median split of the centroids along their
+ * longest axis); 0 drops the copy.  The nearest hit does not depend on how triangles are grouped
+ * into leaves, so results are the same up to exact ties.  raycast and closestPointToPoint keep the
+ * reference's leaves (their hit order and maxThreshold / minThreshold rules follow them).  Waits for
+ * the device; graphs captured before must be captured again.  bvhc_mesh_get_leaf_size returns the
+ * current setting (-1 for a null mesh); bvhc_mesh_get_info describes raycastFirst's records. */
 bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* mesh, int max_leaf);
 int bvhc_mesh_get_leaf_size(const bvhc_mesh* mesh);
 

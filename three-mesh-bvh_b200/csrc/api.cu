@@ -67,7 +67,22 @@ struct bvhc_mesh {
   std::vector<TriRecord> h_tris;
   std::vector<uint32_t> h_roots;
   int h_max_depth = 0;
+  // raycastFirst's own copy of the tree with split leaves (bvhc_mesh_set_leaf_size > 0).  Only
+  // raycastFirst uses it: its result does not depend on the grouping of triangles into leaves,
+  // while closestPointToPoint's maxThreshold / minThreshold rules and raycast's hit order follow
+  // the reference's leaves, so those queries keep the records above.
   int leaf_size = 0;
+  PairNode* d_nodes_f = nullptr;
+  TriRecord* d_tris_f = nullptr;
+  uint32_t* d_roots_f = nullptr;
+  uint64_t n_nodes_f = 0, n_tris_f = 0;
+  int max_depth_f = 0;
+  std::vector<uint32_t> rec_face_f;
+
+  // the records raycastFirst traverses
+  MeshDev view_first() const {
+    return leaf_size ? MeshDev{d_nodes_f, d_tris_f, d_roots_f, n_roots, d_err} : view();
+  }
 
   MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
 };
@@ -362,7 +377,7 @@ struct LeafSplitter {
 
 bool bvhc::mesh_launch_info(const bvhc_mesh* m, MeshDev* view, TraversalConfig* cfg, int* device) {
   if (!m) return false;
-  *view = m->view();
+  *view = m->view_first();
   *cfg = m->cfg;
   *device = m->device;
   return true;
@@ -596,6 +611,9 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_nodes);
   cudaFree(m->d_tris);
   cudaFree(m->d_roots);
+  cudaFree(m->d_nodes_f);
+  cudaFree(m->d_tris_f);
+  cudaFree(m->d_roots_f);
   cudaFree(m->d_err);
   cudaFree(m->d_work);
   cudaFree(m->d_in);
@@ -621,10 +639,13 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
 
 bvhc_status bvhc_mesh_get_info(const bvhc_mesh* m, bvhc_mesh_info* info) {
   if (!m || !info) return BVHC_ERR_INVALID_ARGUMENT;
-  info->node_records = m->n_nodes;
-  info->triangle_records = m->n_tris;
-  info->device_bytes = m->n_nodes * sizeof(PairNode) + m->n_tris * sizeof(TriRecord) + m->n_roots * 4 + 4;
-  info->max_depth = m->max_depth;
+  // the records raycastFirst traverses (the split-leaf copy when one is installed)
+  const bool f = m->leaf_size > 0;
+  info->node_records = f ? m->n_nodes_f : m->n_nodes;
+  info->triangle_records = f ? m->n_tris_f : m->n_tris;
+  info->device_bytes = m->n_nodes * sizeof(PairNode) + m->n_tris * sizeof(TriRecord) + m->n_roots * 4 + 4 +
+                       (f ? m->n_nodes_f * sizeof(PairNode) + m->n_tris_f * sizeof(TriRecord) + m->n_roots * 4 : 0);
+  info->max_depth = f ? m->max_depth_f : m->max_depth;
   info->root_count = m->n_roots;
   return BVHC_OK;
 }
@@ -695,12 +716,12 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
     cudaError_t e = queue_for(m, qslot, n, &q, &qc, &sort, &sorted);
     if (e != cudaSuccess) return e;
     if (m->cfg.persistent == 2)
-      return launch_raycast_first_packet(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order,
+      return launch_raycast_first_packet(m->view_first(), rays, n, side, tab, near_d, far_d, out, m->cfg.order,
                                          m->cfg.occupancy, s, q, qc, sorted ? &sort : nullptr);
-    return launch_raycast_first_persistent(m->view(), nullptr, rays, n, side, tab, near_d, far_d, out, work, m->cfg,
-                                           s, q, qc, sorted ? &sort : nullptr);
+    return launch_raycast_first_persistent(m->view_first(), nullptr, rays, n, side, tab, near_d, far_d, out, work,
+                                           m->cfg, s, q, qc, sorted ? &sort : nullptr);
   }
-  return launch_raycast_first(m->view(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
+  return launch_raycast_first(m->view_first(), rays, n, side, tab, near_d, far_d, out, m->cfg.order, s);
 }
 
 // raycastFirst over one mesh of a batch (view = that mesh's roots), with the batch's variant.
@@ -760,12 +781,7 @@ bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* m, int max_leaf) {
   std::vector<TriRecord> tris;
   std::vector<uint32_t> roots(m->h_roots.size());
   int depth = 0;
-  if (max_leaf == 0) {
-    pairs = m->h_pairs;
-    tris = m->h_tris;
-    roots = m->h_roots;
-    depth = m->h_max_depth;
-  } else {
+  if (max_leaf > 0) {
     LeafSplitter sp{m->h_pairs, m->h_tris, max_leaf};
     try {
       for (size_t r = 0; r < roots.size(); ++r) roots[r] = sp.copy(m->h_roots[r], 0);
@@ -783,26 +799,28 @@ bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* m, int max_leaf) {
   PairNode* nodes = nullptr;
   TriRecord* recs = nullptr;
   uint32_t* rts = nullptr;
-  cudaError_t e = upload(&nodes, pairs);
-  if (e == cudaSuccess) e = upload(&recs, tris);
-  if (e == cudaSuccess) e = upload(&rts, roots);
-  if (e != cudaSuccess) {
-    cudaFree(nodes);
-    cudaFree(recs);
-    cudaFree(rts);
-    return from_cuda(e);
+  if (max_leaf > 0) {
+    cudaError_t e = upload(&nodes, pairs);
+    if (e == cudaSuccess) e = upload(&recs, tris);
+    if (e == cudaSuccess) e = upload(&rts, roots);
+    if (e != cudaSuccess) {
+      cudaFree(nodes);
+      cudaFree(recs);
+      cudaFree(rts);
+      return from_cuda(e);
+    }
   }
-  cudaFree(m->d_nodes);
-  cudaFree(m->d_tris);
-  cudaFree(m->d_roots);
-  m->d_nodes = nodes;
-  m->d_tris = recs;
-  m->d_roots = rts;
-  m->n_nodes = pairs.size();
-  m->n_tris = tris.size();
-  m->max_depth = depth;
-  m->rec_face.resize(tris.size());
-  for (size_t k = 0; k < tris.size(); ++k) m->rec_face[k] = tris[k].face;
+  cudaFree(m->d_nodes_f);
+  cudaFree(m->d_tris_f);
+  cudaFree(m->d_roots_f);
+  m->d_nodes_f = nodes;
+  m->d_tris_f = recs;
+  m->d_roots_f = rts;
+  m->n_nodes_f = pairs.size();
+  m->n_tris_f = tris.size();
+  m->max_depth_f = depth;
+  m->rec_face_f.resize(tris.size());
+  for (size_t k = 0; k < tris.size(); ++k) m->rec_face_f[k] = tris[k].face;
   m->leaf_size = max_leaf;
   return BVHC_OK;
 }
@@ -946,6 +964,16 @@ bvhc_status bvhc_mesh_set_groups(bvhc_mesh* m, const int64_t* groups, int n_grou
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   BVHC_CUDA_TRY(cudaMemcpy2D(reinterpret_cast<char*>(m->d_tris) + offsetof(TriRecord, material), sizeof(TriRecord),
                              mat.data(), sizeof(uint32_t), sizeof(uint32_t), mat.size(), cudaMemcpyHostToDevice));
+  if (m->leaf_size > 0 && !m->rec_face_f.empty()) {  // raycastFirst's split-leaf copy
+    std::vector<uint32_t> mat_f(m->rec_face_f.size());
+    for (size_t k = 0; k < mat_f.size(); ++k) {
+      bvhc_status st = material_of(m->rec_face_f[k], &mat_f[k]);
+      if (st != BVHC_OK) return st;
+    }
+    BVHC_CUDA_TRY(cudaMemcpy2D(reinterpret_cast<char*>(m->d_tris_f) + offsetof(TriRecord, material),
+                               sizeof(TriRecord), mat_f.data(), sizeof(uint32_t), sizeof(uint32_t), mat_f.size(),
+                               cudaMemcpyHostToDevice));
+  }
   return BVHC_OK;
 }
 
@@ -993,8 +1021,8 @@ bvhc_status bvhc_batch_raycast_first(bvhc_mesh* m, const float* rays, const uint
   uint32_t* q;
   unsigned int* qc;
   BVHC_CUDA_TRY(queue_for(m, 0, n, &q, &qc));
-  return from_cuda(launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d, out,
-                                                   m->d_work, m->cfg, s, q, qc));
+  return from_cuda(launch_raycast_first_persistent(m->view_first(), &bd, rays, n, side, single_side(), near_d, far_d,
+                                                   out, m->d_work, m->cfg, s, q, qc));
 }
 
 bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* m, const float* rays, const uint64_t* ray_offsets, int side,
@@ -1008,7 +1036,7 @@ bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* m, const float* rays, c
   for (int k = 0; k < m->n_meshes; ++k) {
     uint64_t off = ray_offsets[k], cnt = ray_offsets[k + 1] - off;
     if (cnt == 0) continue;
-    MeshDev v = m->view();
+    MeshDev v = m->view_first();
     v.roots = m->d_roots + m->mesh_root_off[k];
     v.n_roots = (int)(m->mesh_root_off[k + 1] - m->mesh_root_off[k]);
     BVHC_CUDA_TRY(dispatch_view(m, v, rays + 6 * off, cnt, side, near_d, far_d, out + off, s));
@@ -1043,7 +1071,7 @@ bvhc_status bvhc_batch_graph_create(bvhc_mesh* m, const float* rays, const uint6
   cudaError_t e = queue_for(m, 0, n, &q, &qc);  // allocated before capture: captured work cannot allocate
   if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    cudaError_t le = launch_raycast_first_persistent(m->view(), &bd, rays, n, side, single_side(), near_d, far_d,
+    cudaError_t le = launch_raycast_first_persistent(m->view_first(), &bd, rays, n, side, single_side(), near_d, far_d,
                                                      out, m->d_work, m->cfg, cs, q, qc);
     e = cudaStreamEndCapture(cs, &g->graph);
     if (le != cudaSuccess) e = le;
