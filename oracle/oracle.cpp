@@ -868,6 +868,57 @@ orc_bvh* orc_from_serialized(const void* const* roots, const int64_t* root_bytes
 
 void orc_free(orc_bvh* h) { delete h; }
 
+// MeshBVH#refit() with no node set (src/core/cast/refit.template.js:4-196, MeshBVH.js:504-508): new
+// vertex positions, then per root a post-order walk.  A leaf's box becomes the min / max of its
+// triangles' vertex coordinates (float32 values, compared and stored in a Float32Array), and it
+// reports a change only when some bound differs from the stored one (`!==`); an internal node is
+// rewritten as the union of its children's stored boxes only when a child changed.
+static bool refit_node(Bvh& g, uint8_t* buf, int64_t n32) {
+  NodeView v{buf};
+  float* f = reinterpret_cast<float*>(buf);
+  if (v.is_leaf(n32)) {
+    const int64_t off = v.offset(n32), cnt = v.count(n32);
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = off; i < off + cnt; ++i) {
+      int64_t abc[3];
+      g.tri_vertices(g.resolve(i), abc);
+      for (int k = 0; k < 3; ++k) {
+        const float* p = &g.pos[(size_t)abc[k] * g.stride];
+        for (int a = 0; a < 3; ++a) {
+          if (p[a] < lo[a]) lo[a] = p[a];
+          if (p[a] > hi[a]) hi[a] = p[a];
+        }
+      }
+    }
+    bool changed = false;
+    for (int a = 0; a < 3; ++a) changed |= f[n32 + a] != lo[a] || f[n32 + 3 + a] != hi[a];
+    if (!changed) return false;
+    for (int a = 0; a < 3; ++a) {
+      f[n32 + a] = lo[a];
+      f[n32 + 3 + a] = hi[a];
+    }
+    return true;
+  }
+  const int64_t l = v.left(n32), r = v.right(n32);
+  const bool lc = refit_node(g, buf, l);
+  const bool rc = refit_node(g, buf, r);
+  if (lc || rc) {
+    for (int a = 0; a < 3; ++a) {
+      f[n32 + a] = f[l + a] < f[r + a] ? f[l + a] : f[r + a];
+      f[n32 + 3 + a] = f[l + 3 + a] > f[r + 3 + a] ? f[l + 3 + a] : f[r + 3 + a];
+    }
+  }
+  return lc || rc;
+}
+
+void orc_refit(orc_bvh* h, const float* pos, int64_t n_verts, int stride) {
+  Bvh& g = h->b;
+  g.pos.assign(pos, pos + (size_t)n_verts * stride);
+  g.stride = stride;
+  g.n_verts = n_verts;
+  for (auto& root : g.roots) refit_node(g, root.data(), 0);
+}
+
 // Material-array mode for raycast queries: `groups` holds (start, count, materialIndex) triplets in
 // index units (count < 0 = Infinity) and `sides` one side per material; n_sides = 0 turns it off.
 void orc_set_materials(orc_bvh* h, const int64_t* groups, int n_groups, const int* sides, int n_sides) {

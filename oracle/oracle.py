@@ -65,6 +65,7 @@ def lib():
         L.orc_ray_triangle_jacobian.argtypes = [P, P, P, P, P, P, P]
         L.orc_point_triangle_distance.restype = D
         L.orc_point_triangle_distance.argtypes = [P, P, P, P]
+        L.orc_refit.argtypes = [P, P, I64, I]
         _lib = L
     return _lib
 
@@ -126,6 +127,11 @@ class OracleBVH:
         sd = np.asarray(sides, dtype=np.int32)
         self._mat = (g, sd)
         lib().orc_set_materials(self.h, _p(g) if g.size else None, len(groups), _p(sd) if sd.size else None, sd.size)
+
+    def refit(self, position):
+        """MeshBVH#refit() after the vertex positions changed to `position` (n x 3 float32)."""
+        pos = np.ascontiguousarray(position, dtype=np.float32).reshape(-1, 3)
+        lib().orc_refit(self.h, _p(pos), pos.shape[0], 3)
 
     def roots(self):
         L = lib()
