@@ -223,7 +223,7 @@ def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occ
     ref = _oracle_for(orc, bvh, geo)
     bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
-                                       compact=compact, sort=sort)
+                                       compact=compact, sort=sort, closest=0)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -302,3 +302,33 @@ def test_split_leaf_layouts_agree(pkg, orc, cuda, leaf):
     assert bvh.mesh_info()["node_records"] == base_nodes
     _assert_first_ok(check_first(bvh.raycast_first_batch(rays, 0), exp, tie_exempt(ac, ah)))
     bvh.dispose()
+
+
+@pytest.mark.parametrize("closest,occupancy", [(1, 0), (2, 0), (2, 2)])
+def test_closest_point_warp_cooperative(pkg, orc, knot80k, closest, occupancy):
+    """The warp-cooperative closest-point kernels (input order and Morton-sorted queries) against the
+    oracle: grid queries with maxThreshold 5 (nulls beyond it), unbounded, and a sparse random set;
+    minThreshold > 0 falls back to the per-query kernel and must match too."""
+    geo, bvh, ref = knot80k
+    bvh.set_traversal(1, 1, 16, occupancy, 0, 0, closest)
+    rng = np.random.default_rng(21)
+    lo, hi = geo.position.min(0), geo.position.max(0)
+    sets = [pkg.grid_points(lo, hi, 40),
+            (lo - 8 + rng.random((20_000, 3)) * (hi - lo + 16)).astype(np.float32)]
+
+    def tri_distance(pts):
+        def f(i, face):
+            t = geo.triangle(face)
+            q = orc.closest_point_triangle(pts[i].astype(np.float64), *t)
+            return float(np.linalg.norm(q - pts[i].astype(np.float64)))
+        return f
+
+    for pts in sets:
+        for lo_t, hi_t in ((0.0, 5.0), (0.0, math.inf), (0.5, 3.0)):
+            got = bvh.closest_point_batch(pts, lo_t, hi_t)
+            exp = ref.closest_point(pts, lo_t, hi_t)
+            rep = check_closest(got, exp, tri_distance(pts))
+            assert rep["null"] == 0 and rep["face"] == 0, (lo_t, hi_t, rep)
+            if lo_t == 0.0:
+                assert rep["distance"] == 0, (lo_t, hi_t, rep)
+    bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)

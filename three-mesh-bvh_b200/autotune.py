@@ -70,6 +70,33 @@ def tune_raycast_first(bvh, rays, side: int = 0, near: float = 0.0, far: float =
     return entry
 
 
+def tune_closest_point(bvh, points, min_t: float = 0.0, max_t: float = math.inf, reps: int = 3,
+                       candidates=(0, 1, 2)) -> dict:
+    """Time closestPointToPoint's kernels (the `closest` field: per query, warp-cooperative,
+    warp-cooperative over Morton-sorted queries) on `points` (torch CUDA tensor, n x 3), keeping
+    the mesh's other traversal fields, and install the fastest."""
+    import torch
+
+    cur = bvh.get_traversal()
+    stream = torch.cuda.current_stream(points.device)
+    out = torch.empty((points.shape[0], 5), dtype=torch.float32, device=points.device)
+    timings = {}
+    for c in candidates:
+        bvh.set_traversal(**{**cur, "closest": c})
+        bvh.closest_point_batch(points, min_t, max_t, out=out, stream=stream.cuda_stream)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(reps):
+            bvh.closest_point_batch(points, min_t, max_t, out=out, stream=stream.cuda_stream)
+        end.record(stream)
+        end.synchronize()
+        timings[c] = start.elapsed_time(end) / reps
+    bvh.synchronize(stream.cuda_stream)
+    best = min(candidates, key=lambda c: timings[c])
+    bvh.set_traversal(**{**cur, "closest": best})
+    return {"best": best, "timings_ms": {str(k): v for k, v in timings.items()}}
+
+
 def tune_raycast_first_sets(bvh, named_rays, leaf_sizes=(0,), tag: str = "default", **kw) -> dict:
     """Tune several ray sets that share one mesh: the device leaf layout (bvh.set_leaf_size; one
     layout serves every set) is chosen by the sum of the sets' best times, and each set keeps its

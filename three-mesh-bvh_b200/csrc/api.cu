@@ -26,7 +26,7 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
@@ -44,14 +44,15 @@ struct bvhc_mesh {
   void* slot_in[2] = {nullptr, nullptr};
   void* slot_out[2] = {nullptr, nullptr};
   unsigned long long* d_work2 = nullptr;
-  // compaction queues of the persistent path (grow-only): [0] direct calls, [1], [2] the two
-  // pipeline slots, so that concurrently running chunks never share a queue
-  uint32_t* d_queue[3] = {nullptr, nullptr, nullptr};
-  size_t queue_cap[3] = {0, 0, 0};
-  unsigned int* d_qcount[3] = {nullptr, nullptr, nullptr};
-  // ray-ordering sort scratch per queue slot (grow-only; sized for sort_cap[slot] rays)
-  RaySortScratch sort_s[3] = {};
-  uint64_t sort_cap[3] = {0, 0, 0};
+  // work queues (grow-only): [0] direct raycastFirst calls, [1], [2] the two pipeline slots (so
+  // that concurrently running chunks never share a queue), [3] closestPointToPoint
+  static constexpr int kSlots = 4;
+  uint32_t* d_queue[kSlots] = {};
+  size_t queue_cap[kSlots] = {};
+  unsigned int* d_qcount[kSlots] = {};
+  // ordering-sort scratch per queue slot (grow-only; sized for sort_cap[slot] queries)
+  RaySortScratch sort_s[kSlots] = {};
+  uint64_t sort_cap[kSlots] = {};
   // batched meshes (bvhc_batch_create): mesh k owns roots [mesh_root_off[k], mesh_root_off[k+1])
   int n_meshes = 0;
   std::vector<uint32_t> mesh_root_off;
@@ -629,7 +630,7 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_ray_off);
   cudaFree(m->d_index32);
   cudaFree(m->d_pos);
-  for (int k = 0; k < 3; ++k) {
+  for (int k = 0; k < bvhc_mesh::kSlots; ++k) {
     cudaFree(m->d_queue[k]);
     cudaFree(m->d_qcount[k]);
     free_sort_scratch(m->sort_s[k]);
@@ -765,12 +766,14 @@ static cudaError_t ensure_pipeline(bvhc_mesh* m) {
 static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
-         (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3;
+         (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
+         cfg->closest <= 2;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact, cfg->sort};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy,
+                           cfg->compact,    cfg->sort,  cfg->closest};
   return BVHC_OK;
 }
 
@@ -835,6 +838,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->occupancy = m->cfg.occupancy;
   cfg->compact = m->cfg.compact;
   cfg->sort = m->cfg.sort;
+  cfg->closest = m->cfg.closest;
   return BVHC_OK;
 }
 
@@ -984,15 +988,36 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
   if (!points || !out) return BVHC_ERR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
-  if (mem == BVHC_MEM_DEVICE) {
-    if (!aligned(points, 4) || !aligned(out, 4)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s));
+  if (mem == BVHC_MEM_DEVICE && (!aligned(points, 4) || !aligned(out, 4))) return BVHC_ERR_INVALID_ARGUMENT;
+  // the warp-cooperative variant over Morton-sorted queries uses queue slot 3 and its sort scratch
+  const int variant = m->cfg.closest;
+  uint32_t* q = nullptr;
+  unsigned int* qc = nullptr;
+  RaySort sort{};
+  const int slot = 3;
+  if (variant == 2 && n < (1ull << 32) && min_threshold <= 0.0f) {
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
+    if (!m->d_qcount[slot])
+      BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
+    BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
+    q = m->d_queue[slot];
+    qc = m->d_qcount[slot];
+    sort.kind = 2;
+    for (int a = 0; a < 3; ++a) {
+      sort.lo[a] = m->scene_lo[a];
+      sort.hi[a] = m->scene_hi[a];
+    }
+    sort.scratch = m->sort_s[slot];
   }
+  if (mem == BVHC_MEM_DEVICE)
+    return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s, variant,
+                                          m->cfg.occupancy, q, qc, q ? &sort : nullptr));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold, max_threshold,
-                                     static_cast<bvhc_closest*>(m->d_out), s));
+                                     static_cast<bvhc_closest*>(m->d_out), s, variant, m->cfg.occupancy, q, qc,
+                                     q ? &sort : nullptr));
   BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
 }

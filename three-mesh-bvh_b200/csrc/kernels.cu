@@ -501,6 +501,95 @@ __device__ __forceinline__ bool under_max(float s, const float* b, float3 p, ff 
   return ff_lt(box_score_ff(b, p), max2);
 }
 
+// The best candidate of one query so far.
+struct CPBest {
+  float d2, err;     // float32 squared distance and its error bound
+  uint32_t rec;      // triangle record (0xFFFFFFFF: none yet)
+  float3 q;          // float32 closest point
+  bool vertex;       // q is an input vertex, bit-exact
+  bool ff_ok;        // ffv holds the float-float squared distance
+  ff ffv;
+};
+
+__device__ __forceinline__ CPBest cp_none() {
+  CPBest b;
+  b.d2 = kInf;
+  b.err = 0.0f;
+  b.rec = 0xFFFFFFFFu;
+  b.q = make_float3(0.f, 0.f, 0.f);
+  b.vertex = false;
+  b.ff_ok = false;
+  b.ffv = {kInf, 0.0f};
+  return b;
+}
+
+// Offers triangle record k to the query at p (the reference's strict `<` on distSq).  Returns the
+// candidate's float32 squared distance and bound, and its float-float value when one was needed.
+__device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
+                                         float& err, bool& have_ff, ff& cand_ff) {
+  float3 q;
+  float sc;
+  d2 = closest_sq_f(p, t.a, t.b, t.c, q, sc);
+  // |error| of each closest-point coordinate <= e (local-frame evaluation)
+  float e = 32.0f * kU * sc;
+  err = 3.5f * e * sqrtf(d2) + 3.0f * e * e;
+  bool is_vertex = (q.x == t.a.x && q.y == t.a.y && q.z == t.a.z) ||
+                   (q.x == t.b.x && q.y == t.b.y && q.z == t.b.z) ||
+                   (q.x == t.c.x && q.y == t.c.y && q.z == t.c.z);
+  bool take;
+  have_ff = false;
+  if (b.rec == 0xFFFFFFFFu) {
+    take = d2 < kInf;  // the first finite candidate (distSq < Infinity)
+  } else if (d2 + err < b.d2 - b.err) {
+    take = true;
+  } else if (d2 - err > b.d2 + b.err) {
+    take = false;
+  } else if (is_vertex && b.vertex && q.x == b.q.x && q.y == b.q.y && q.z == b.q.z) {
+    take = false;  // the same vertex: an exact tie, the first one found stays
+  } else if (err + b.err <= 2e-6f * b.d2) {
+    // the two true distances are within 1e-6 relative of each other (typically the same edge or
+    // vertex reached from two triangles): either answer meets the distance tolerance and the
+    // winner's distance is recomputed in float-float, so the first one found stays, as the
+    // reference's strict `<` keeps it on a tie
+    take = false;
+  } else {
+    if (!b.ff_ok) {
+      Tri bt = load_tri(m.tris, b.rec);
+      b.ffv = closest_ff(p, bt.a, bt.b, bt.c).d2;
+      b.ff_ok = true;
+    }
+    cand_ff = closest_ff(p, t.a, t.b, t.c).d2;
+    have_ff = true;
+    take = ff_lt(cand_ff, b.ffv);
+  }
+  if (take) {
+    b.d2 = d2;
+    b.err = err;
+    b.rec = k;
+    b.q = q;
+    b.vertex = is_vertex;
+    b.ff_ok = have_ff;
+    b.ffv = cand_ff;
+  }
+}
+
+// The reported record: distance and closest point in float-float, rounded once.
+__device__ __forceinline__ void cp_store(const MeshDev& m, float3 p, const CPBest& b, bvhc_closest* o) {
+  if (b.rec == 0xFFFFFFFFu) {
+    o->face_index = BVHC_NO_HIT;
+    o->distance = kInf;
+    o->point[0] = o->point[1] = o->point[2] = 0.0f;
+    return;
+  }
+  Tri t = load_tri(m.tris, b.rec);
+  CPFF c = closest_ff(p, t.a, t.b, t.c);
+  o->face_index = t.face;
+  o->distance = ff_to_f(ff_sqrt(c.d2));
+  o->point[0] = ff_to_f(c.q.x);
+  o->point[1] = ff_to_f(c.q.y);
+  o->point[2] = ff_to_f(c.q.z);
+}
+
 __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const float* __restrict__ pts, uint64_t n,
                                                                float min_t, float max_t,
                                                                bvhc_closest* __restrict__ out) {
@@ -509,12 +598,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
   float3 p = make_float3(__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2));
   ff max2 = two_prod(max_t, max_t);
   ff min2 = two_prod(min_t, min_t);
-  float best_d2 = kInf, best_err = 0.0f;
-  uint32_t best_rec = 0xFFFFFFFFu;
-  float3 best_q = make_float3(0.f, 0.f, 0.f);
-  bool best_vertex = false;  // best_q is an input vertex, bit-exact
-  bool best_ff_ok = false;
-  ff best_ff = {kInf, 0.0f};
+  CPBest b = cp_none();
   bool stop = false;
   uint32_t stack_link[kMaxStack];
   float stack_s[kMaxStack];
@@ -527,51 +611,10 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
           uint32_t k = link & ~kLeafBit;
           for (;;) {
             Tri t = load_tri(m.tris, k);
-            float3 q;
-            float sc;
-            float d2 = closest_sq_f(p, t.a, t.b, t.c, q, sc);
-            // |error| of each closest-point coordinate <= e (local-frame evaluation)
-            float e = 32.0f * kU * sc;
-            float err = 3.5f * e * sqrtf(d2) + 3.0f * e * e;
-            bool is_vertex = (q.x == t.a.x && q.y == t.a.y && q.z == t.a.z) ||
-                             (q.x == t.b.x && q.y == t.b.y && q.z == t.b.z) ||
-                             (q.x == t.c.x && q.y == t.c.y && q.z == t.c.z);
-            bool take;
-            bool have_ff = false;
+            float d2, err;
+            bool have_ff;
             ff cand_ff;
-            if (best_rec == 0xFFFFFFFFu) {
-              take = d2 < kInf;  // the first finite candidate (distSq < Infinity)
-            } else if (d2 + err < best_d2 - best_err) {
-              take = true;
-            } else if (d2 - err > best_d2 + best_err) {
-              take = false;
-            } else if (is_vertex && best_vertex && q.x == best_q.x && q.y == best_q.y && q.z == best_q.z) {
-              take = false;  // the same vertex: an exact tie, the first one found stays
-            } else if (err + best_err <= 2e-6f * best_d2) {
-              // the two true distances are within 1e-6 relative of each other (typically the same
-              // edge or vertex reached from two triangles): either answer meets the distance
-              // tolerance and the winner's distance is recomputed in float-float, so the first
-              // one found stays, as the reference's strict `<` keeps it on a tie
-              take = false;
-            } else {
-              if (!best_ff_ok) {
-                Tri bt = load_tri(m.tris, best_rec);
-                best_ff = closest_ff(p, bt.a, bt.b, bt.c).d2;
-                best_ff_ok = true;
-              }
-              cand_ff = closest_ff(p, t.a, t.b, t.c).d2;
-              have_ff = true;
-              take = ff_lt(cand_ff, best_ff);
-            }
-            if (take) {
-              best_d2 = d2;
-              best_err = err;
-              best_rec = k;
-              best_q = q;
-              best_vertex = is_vertex;
-              best_ff_ok = have_ff;
-              best_ff = cand_ff;
-            }
+            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff);
             // early out below minThreshold (closestPointToPoint.js:55-57)
             if (min2.hi > 0.0f) {
               bool below;
@@ -593,7 +636,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
         const float* b2 = swap ? pr.l : pr.r;
         float sc1 = swap ? s1 : s0, sc2 = swap ? s0 : s1;
         uint32_t c1 = swap ? pr.lr : pr.ll, c2 = swap ? pr.ll : pr.lr;
-        float best_hi = best_d2 + best_err;
+        float best_hi = b.d2 + b.err;
         if (under_max(sc2, b2, p, max2)) {
           if (sp >= kMaxStack) {
             atomicOr(m.err, kErrStackOverflow);
@@ -612,7 +655,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
       bool found = false;
       while (sp > 0) {
         --sp;
-        if (stack_s[sp] * (1.0f - kSlabMargin) <= best_d2 + best_err) {
+        if (stack_s[sp] * (1.0f - kSlabMargin) <= b.d2 + b.err) {
           link = stack_link[sp];
           found = true;
           break;
@@ -621,20 +664,130 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
       if (!found) break;
     }
   }
-  bvhc_closest* o = out + i;
-  if (best_rec == 0xFFFFFFFFu) {
-    o->face_index = BVHC_NO_HIT;
-    o->distance = kInf;
-    o->point[0] = o->point[1] = o->point[2] = 0.0f;
-    return;
+  cp_store(m, p, b, out + i);
+}
+
+// ---------------------------------------------------------------------------------------------
+// closestPointToPoint, warp-cooperative form for spatially coherent queries (grids, SDF samples)
+// with minThreshold 0.  The 32 queries of a warp walk the tree together with one shared stack of
+// links: a child is entered when any lane wants it (its score under maxThreshold^2, decided
+// exactly, and not certainly above that lane's best), and each lane keeps, for the current node
+// and for every stacked child, whether it wants it (its own score, or NaN for "no").  A lane only
+// tests the triangles of leaves it wants, so every lane reaches exactly the leaves its own
+// traversal would and its result is the minimum over the same candidates: which leaves a query
+// reaches, and so the "null iff no leaf is reached" rule, does not depend on the visiting order,
+// and leaves skipped because of the best distance cannot hold a strictly closer triangle.  (With
+// minThreshold > 0 the reference stops at the first triangle below it in its own order, which a
+// shared order would not reproduce; those calls use the per-query kernel.)
+// ---------------------------------------------------------------------------------------------
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
+    MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
+    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
+  __shared__ uint32_t s_link[kBlock / 32][kMaxStack];
+  const unsigned full = 0xFFFFFFFFu;
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n_work;
+  if (valid && queue) i = __ldg(queue + i);
+  float3 p = make_float3(0.f, 0.f, 0.f);
+  if (valid) p = make_float3(__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2));
+  const ff max2 = two_prod(max_t, max_t);
+  const float kNo = __int_as_float(0x7FFFFFFF);  // NaN: "this lane does not want the entry"
+  CPBest b = cp_none();
+  float lane_s[kMaxStack];
+  bool overflow = false;
+  for (int root = 0; root < m.n_roots && !overflow; ++root) {
+    uint32_t link = m.roots[root];
+    bool act = valid;  // this lane wants the current node (a root leaf has no bounds test)
+    int sp = 0;
+    for (;;) {
+      bool pop = false;
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf && act) {
+          uint32_t k = link & ~kLeafBit;
+          for (;;) {
+            Tri t = load_tri(m.tris, k);
+            float d2, err;
+            bool have_ff;
+            ff cand_ff;
+            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff);
+            if (t.flags & kTriLast) break;
+            ++k;
+          }
+        }
+        pop = true;
+      } else {
+        Pair pr = load_pair(m.nodes, link);
+        float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
+        float best_hi = b.d2 + b.err;
+        bool w0 = act && s0 * (1.0f - kSlabMargin) <= best_hi && under_max(s0, pr.l, p, max2);
+        bool w1 = act && s1 * (1.0f - kSlabMargin) <= best_hi && under_max(s1, pr.r, p, max2);
+        unsigned b0 = __ballot_sync(full, w0), b1 = __ballot_sync(full, w1);
+        if (b0 && b1) {
+          // nearer child first by majority of the lanes that want both (a lane wanting one prefers it)
+          bool pref_right = (w0 && w1) ? s1 < s0 : w1;
+          unsigned voters = __ballot_sync(full, w0 || w1);
+          bool right_first = 2 * __popc(__ballot_sync(full, (w0 || w1) && pref_right)) > __popc(voters);
+          if (sp >= kMaxStack) {
+            if (lane == 0) atomicOr(m.err, kErrStackOverflow);
+            b = cp_none();
+            overflow = true;
+            break;
+          }
+          if (lane == 0) s_link[w][sp] = right_first ? pr.ll : pr.lr;
+          lane_s[sp] = right_first ? (w0 ? s0 : kNo) : (w1 ? s1 : kNo);
+          ++sp;
+          link = right_first ? pr.lr : pr.ll;
+          act = right_first ? w1 : w0;
+          __syncwarp();
+        } else if (b0) {
+          link = pr.ll;
+          act = w0;
+        } else if (b1) {
+          link = pr.lr;
+          act = w1;
+        } else {
+          pop = true;
+        }
+      }
+      if (pop) {
+        bool found = false;
+        while (sp > 0) {
+          --sp;
+          bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= b.d2 + b.err;  // false for NaN
+          if (__ballot_sync(full, ok)) {
+            link = s_link[w][sp];
+            act = ok;
+            found = true;
+            break;
+          }
+        }
+        if (!found) break;
+      }
+    }
   }
-  Tri t = load_tri(m.tris, best_rec);
-  CPFF c = closest_ff(p, t.a, t.b, t.c);
-  o->face_index = t.face;
-  o->distance = ff_to_f(ff_sqrt(c.d2));
-  o->point[0] = ff_to_f(c.q.x);
-  o->point[1] = ff_to_f(c.q.y);
-  o->point[2] = ff_to_f(c.q.z);
+  if (valid) cp_store(m, p, b, out + i);
+}
+
+// Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
+// queue length; the queue is then sorted by key so that a warp takes 32 nearby points.
+__global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n, SceneBox box,
+                                                          uint32_t* __restrict__ ids, uint32_t* __restrict__ keys,
+                                                          unsigned int* __restrict__ qcount) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *qcount = (unsigned int)n;
+  if (i >= n) return;
+  float sx = box.hi[0] > box.lo[0] ? 1.0f / (box.hi[0] - box.lo[0]) : 0.0f;
+  float sy = box.hi[1] > box.lo[1] ? 1.0f / (box.hi[1] - box.lo[1]) : 0.0f;
+  float sz = box.hi[2] > box.lo[2] ? 1.0f / (box.hi[2] - box.lo[2]) : 0.0f;
+  ids[i] = (uint32_t)i;
+  keys[i] = morton3(quantise(__ldg(pts + 3 * i), box.lo[0], sx, 256.0f),
+                    quantise(__ldg(pts + 3 * i + 1), box.lo[1], sy, 256.0f),
+                    quantise(__ldg(pts + 3 * i + 2), box.lo[2], sz, 256.0f));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1057,9 +1210,34 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
 }
 
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
-                                 bvhc_closest* out, cudaStream_t stream) {
+                                 bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
+                                 unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
+  // the warp-cooperative form needs minThreshold 0 (see closest_point_packet_kernel)
+  if (variant == 0 || !(min_t <= 0.0f) || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
+    dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
+    return cudaGetLastError();
+  }
+  cudaError_t e;
+  if (variant == 2) {
+    uint32_t *ids, *keys;
+    ray_sort_input(2, sort->scratch, queue, &ids, &keys);
+    dev::SceneBox box{};
+    for (int a = 0; a < 3; ++a) {
+      box.lo[a] = sort->lo[a];
+      box.hi[a] = sort->hi[a];
+    }
+    dev::point_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(pts, n, box, ids, keys, qcount);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_ray_sort(2, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
+  } else {
+    queue = nullptr;
+    qcount = nullptr;
+  }
+  auto kernel = occupancy == 0   ? dev::closest_point_packet_kernel<1>
+                : occupancy == 1 ? dev::closest_point_packet_kernel<6>
+                                 : dev::closest_point_packet_kernel<8>;
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
   return cudaGetLastError();
 }
 

@@ -25,8 +25,6 @@ struct MeshDev {
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                  float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
-// Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).
-
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream);
@@ -41,6 +39,8 @@ struct TraversalConfig {
                    // warp-cooperative forms)
   int sort;        // 0: queue in ray order; 1..3: queue sorted by a Morton key (raysort.cu), implies
                    // the pre-pass
+  int closest;     // closestPointToPoint: 0 one query per thread, 1 warp-cooperative, 2 warp-cooperative
+                   // over Morton-sorted queries (1 and 2 only with minThreshold 0)
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -89,8 +89,13 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
                                         int occupancy, cudaStream_t stream, uint32_t* queue = nullptr,
                                         unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
+// closestPointToPoint.  variant 0: one query per thread; 1: warp-cooperative in input order; 2:
+// warp-cooperative over the queries sorted by a Morton key of the point (queue, qcount and sort
+// scratch for n queries required).  Variants 1 and 2 apply only with min_t <= 0 (else variant 0).
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
-                                 bvhc_closest* out, cudaStream_t stream);
+                                 bvhc_closest* out, cudaStream_t stream, int variant = 0, int occupancy = 0,
+                                 uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
+                                 const RaySort* sort = nullptr);
 
 // What another translation unit needs to launch on a mesh: its device view, traversal variant and
 // device ordinal (defined in api.cu).  Returns false for a null mesh.

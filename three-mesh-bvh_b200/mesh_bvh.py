@@ -201,9 +201,9 @@ class MeshBVH:
         return {k: getattr(info, k) for k, _ in N.BvhcMeshInfo._fields_}
 
     def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0,
-                      compact: int = 0, sort: int = 0) -> None:
-        """Select the raycastFirst traversal variant (see bvhc_mesh_set_traversal)."""
-        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort)
+                      compact: int = 0, sort: int = 0, closest: int = 0) -> None:
+        """Select the traversal variants (see bvhc_mesh_set_traversal)."""
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     def get_traversal(self) -> dict:
@@ -286,13 +286,14 @@ class MeshBVH:
                                  _ptr(hits), N.MEM_HOST, None), "bvhc_raycast")
         return counts, hits
 
-    def closest_point_batch(self, points, min_threshold=0.0, max_threshold=math.inf, stream=None):
+    def closest_point_batch(self, points, min_threshold=0.0, max_threshold=math.inf, stream=None, out=None):
         """closestPointToPoint for every row of `points` (n x 3 float32)."""
         lib, mesh = N.lib(), self._device_mesh()
         if self._is_torch(points):
             import torch
             n = points.shape[0]
-            out = torch.empty((n, 5), dtype=torch.float32, device=points.device)
+            if out is None:
+                out = torch.empty((n, 5), dtype=torch.float32, device=points.device)
             s = stream if stream is not None else torch.cuda.current_stream(points.device).cuda_stream
             N.check(lib.bvhc_closest_point_to_point(mesh, points.data_ptr(), n, float(min_threshold),
                                                     float(max_threshold), out.data_ptr(), N.MEM_DEVICE, s),
