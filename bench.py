@@ -669,6 +669,13 @@ def run_adjoint(args, ws, rank, local):
     gv = torch.zeros((geo.position.shape[0], 3), dtype=torch.float32, device=dev)
     pts = torch.from_numpy(pkg.grid_points(geo.position.min(0), geo.position.max(0), 128)).to(dev)
     ones = torch.ones(pts.shape[0], dtype=torch.float32, device=dev)
+    # the forward passes run their autotuned variants (the backward replays recorded triangles and
+    # has no variants)
+    from three_mesh_bvh_b200 import autotune
+
+    tuned_ray = autotune.tune_raycast_first_sets(bvh, [("camera1024", rays)], leaf_sizes=(0, 2, 4), tag="adjoint")
+    bvh.set_traversal(*tuned_ray["sets"]["camera1024"]["best"])
+    tuned_cp = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
 
     def fwd():
         return bvh.raycast_first_batch(rays, stream=s)
@@ -714,6 +721,8 @@ def run_adjoint(args, ws, rank, local):
                                        "128^3 grid closest point, max 5, L = sum distance"},
                 "raycast": {"fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f},
                 "closest_point": {"fwd_ms": ms_cf, "fwd_bwd_ms": ms_cfb, "ratio": ms_cfb / ms_cf},
+                "forward_variants": {"raycast": tuned_ray["sets"]["camera1024"]["best"],
+                                     "leaf_size": tuned_ray["leaf"], "closest": tuned_cp["best"]},
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     bvh.dispose()
