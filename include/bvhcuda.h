@@ -166,6 +166,22 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config
 bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* mesh, int max_leaf);
 int bvhc_mesh_get_leaf_size(const bvhc_mesh* mesh);
 
+/* MeshBVH#refit() (src/core/MeshBVH.js:504-508, src/core/cast/refit.template.js:4-196) on the
+ * device, after the geometry's vertices moved: `positions` (n_verts >= the mesh's vertex count,
+ * `stride_floats` apart; host or device memory per `mem`) replace the vertices of every triangle
+ * record, and the boxes are rebuilt bottom-up with the reference's rule (a leaf box is rewritten
+ * only when it differs from the stored one, a parent's only when a child changed), so the boxes
+ * are bit-identical to the reference's refit of the same buffers.  raycastFirst's split-leaf copy,
+ * if any, is refit too, and the gradient vertex copy (bvhc_mesh_enable_gradients) follows.  The
+ * topology (index, triangle count) must not change.  Device-memory calls only enqueue on `stream`.
+ * bvhc_mesh_read_root copies root `root`'s serialized buffer (version 1 layout) with the boxes as
+ * the last refit left them (MeshBVH.serialize after refit); it waits for the device. */
+bvhc_status bvhc_mesh_refit(bvhc_mesh* mesh, const float* positions, uint64_t n_verts, int stride_floats, int mem,
+                            void* stream);
+int bvhc_mesh_root_count(const bvhc_mesh* mesh);
+uint64_t bvhc_mesh_root_bytes(const bvhc_mesh* mesh, int root);
+bvhc_status bvhc_mesh_read_root(bvhc_mesh* mesh, int root, void* dst, uint64_t bytes);
+
 /* Waits for the mesh's work on `stream` and reports (and clears) the device error word. */
 bvhc_status bvhc_mesh_synchronize(bvhc_mesh* mesh, void* stream);
 

@@ -68,6 +68,10 @@ SIGNATURES = [
     ("bvhc_mesh_get_traversal", _I, [_P, C.POINTER(BvhcTraversalConfig)]),
     ("bvhc_mesh_set_leaf_size", _I, [_P, C.c_int]),
     ("bvhc_mesh_get_leaf_size", C.c_int, [_P]),
+    ("bvhc_mesh_refit", _I, [_P, _P, C.c_uint64, C.c_int, C.c_int, _P]),
+    ("bvhc_mesh_root_count", C.c_int, [_P]),
+    ("bvhc_mesh_root_bytes", C.c_uint64, [_P, C.c_int]),
+    ("bvhc_mesh_read_root", _I, [_P, C.c_int, _P, C.c_uint64]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
 ]

@@ -79,6 +79,17 @@ struct bvhc_mesh {
   uint64_t n_nodes_f = 0, n_tris_f = 0;
   int max_depth_f = 0;
   std::vector<uint32_t> rec_face_f;
+  // refit (bvhc_mesh_refit): the serialized root buffers (version 1 layout) with the position of
+  // every pair's child boxes in them, the geometry index (empty: non-indexed), and per layout
+  // ([0] reference records, [1] raycastFirst's split copy) the bottom-up plan
+  std::vector<std::vector<uint8_t>> h_root_bytes;
+  std::vector<uint64_t> slot_nodes;
+  std::vector<uint32_t> h_index;
+  uint64_t n_verts_geo = 0;
+  RefitPlan refit[2];
+  uint32_t* d_tri_vid = nullptr;
+  void* d_refit_pos = nullptr;
+  size_t refit_pos_cap = 0;
 
   // the records raycastFirst traverses
   MeshDev view_first() const {
@@ -133,6 +144,11 @@ struct Converter {
   std::vector<TriRecord>& tris;
   uint64_t visits = 0;
   int max_depth = 0;
+  // where each pair's child boxes live in the serialized buffers: (root << 40) | node, two per pair
+  std::vector<uint64_t>* slot_nodes = nullptr;
+  uint64_t root_id = 0;
+  // a copy of this root's buffer in the current (version 1) format, for reading refit boxes back
+  uint8_t* v1_copy = nullptr;
 
   Converter(std::vector<PairNode>& p, std::vector<TriRecord>& t) : pairs(p), tris(t) {}
 
@@ -196,6 +212,14 @@ struct Converter {
     if (pairs.size() >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
     uint32_t idx = (uint32_t)pairs.size();
     pairs.push_back(PairNode{});
+    if (slot_nodes) {
+      slot_nodes->push_back((root_id << 40) | left);
+      slot_nodes->push_back((root_id << 40) | right);
+    }
+    if (v1_copy && version == 0) {  // the right child as a relative node offset (MeshBVH.js:206-230)
+      uint32_t rel = (uint32_t)(right - node);
+      std::memcpy(v1_copy + node * 32 + 24, &rel, 4);
+    }
     uint32_t ll = convert(left, depth + 1);
     uint32_t lr = convert(right, depth + 1);
     PairNode& p = pairs[idx];
@@ -431,6 +455,82 @@ static bvhc_status finish_mesh(int device, const std::vector<PairNode>& pairs, c
   return BVHC_OK;
 }
 
+// Keeps what a refit needs on the host: the serialized roots (version 1 layout), where each pair's
+// child boxes sit in them, and the geometry index as uint32.
+static void keep_serialized(bvhc_mesh* m, std::vector<std::vector<uint8_t>> roots, std::vector<uint64_t> slot_nodes,
+                            const void* index, int index_elem, uint64_t index_count, uint64_t n_verts) {
+  m->h_root_bytes = std::move(roots);
+  m->slot_nodes = std::move(slot_nodes);
+  m->n_verts_geo = n_verts;
+  if (index) {
+    m->h_index.resize(index_count);
+    for (uint64_t i = 0; i < index_count; ++i) m->h_index[i] = read_index(index, index_elem, i);
+  }
+}
+
+static void free_refit_plan(RefitPlan& p) {
+  cudaFree(p.leaves);
+  cudaFree(p.parent);
+  cudaFree(p.arrive);
+  cudaFree(p.flags);
+  cudaFree(p.root_box);
+  p = RefitPlan{};
+}
+
+// The bottom-up plan of one record layout: every leaf (a leaf child of a pair, or a root that is a
+// leaf) with its triangle-record run and box slot, and every pair's parent slot.  root_boxes: 6
+// floats per root (the roots' own boxes, which the child-pair records do not hold).
+static cudaError_t build_refit_plan(const std::vector<PairNode>& pairs, const std::vector<TriRecord>& tris,
+                                    const std::vector<uint32_t>& roots, const std::vector<float>& root_boxes,
+                                    RefitPlan& plan) {
+  std::vector<RefitLeaf> leaves;
+  std::vector<uint32_t> parent(pairs.size(), kRootSlot);
+  auto leaf_of = [&](uint32_t link, uint32_t slot) {
+    RefitLeaf l{0, 0, slot};
+    if (link != kEmptyLeaf) {
+      l.first = link & ~kLeafBit;
+      uint32_t k = l.first;
+      while (!(tris[k].flags & kTriLast)) ++k;
+      l.count = k - l.first + 1;
+    }
+    leaves.push_back(l);
+  };
+  for (size_t p = 0; p < pairs.size(); ++p)
+    for (uint32_t s = 0; s < 2; ++s) {
+      uint32_t link = pairs[p].link[s];
+      uint32_t slot = (uint32_t)(2 * p + s);
+      if (link & kLeafBit) leaf_of(link, slot);
+      else parent[link] = slot;
+    }
+  for (size_t r = 0; r < roots.size(); ++r) {
+    uint32_t slot = kRootSlot | (uint32_t)r;
+    if (roots[r] & kLeafBit) leaf_of(roots[r], slot);
+    else parent[roots[r]] = slot;
+  }
+  RefitPlan np;
+  np.n_leaves = (uint32_t)leaves.size();
+  np.n_pairs = (uint32_t)pairs.size();
+  cudaError_t e = upload(&np.leaves, leaves);
+  if (e == cudaSuccess) e = upload(&np.parent, parent);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&np.arrive), std::max<size_t>(pairs.size(), 1) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&np.flags), std::max<size_t>(pairs.size(), 1) * 4);
+  if (e == cudaSuccess) e = upload(&np.root_box, root_boxes);
+  if (e != cudaSuccess) {
+    free_refit_plan(np);
+    return e;
+  }
+  free_refit_plan(plan);
+  plan = np;
+  return cudaSuccess;
+}
+
+// The roots' own boxes, from the kept serialized buffers (node 0 of each root).
+static std::vector<float> serialized_root_boxes(const bvhc_mesh* m) {
+  std::vector<float> boxes(6 * m->h_root_bytes.size());
+  for (size_t r = 0; r < m->h_root_bytes.size(); ++r) std::memcpy(&boxes[6 * r], m->h_root_bytes[r].data(), 24);
+  return boxes;
+}
+
 extern "C" {
 
 const char* bvhc_status_string(bvhc_status s) {
@@ -528,11 +628,18 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
   std::vector<PairNode> pairs;
   std::vector<TriRecord> tris;
   std::vector<uint32_t> root_links;
+  std::vector<uint64_t> slot_nodes;
+  std::vector<std::vector<uint8_t>> copies;
   int max_depth = 0;
   try {
     for (int r = 0; r < n_roots; ++r) {
       if (!roots[r] || root_bytes[r] == 0 || root_bytes[r] % 32 != 0) return BVHC_ERR_INVALID_BVH;
       Converter c(pairs, tris);
+      const uint8_t* src = static_cast<const uint8_t*>(roots[r]);
+      copies.emplace_back(src, src + root_bytes[r]);
+      c.slot_nodes = &slot_nodes;
+      c.root_id = (uint64_t)r;
+      c.v1_copy = copies.back().data();
       c.buf = static_cast<const uint8_t*>(roots[r]);
       c.n_nodes = root_bytes[r] / 32;
       c.version = version;
@@ -555,7 +662,10 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
   } catch (const std::bad_alloc&) {
     return BVHC_ERR_OUT_OF_MEMORY;
   }
-  return finish_mesh(device, pairs, tris, root_links, max_depth, {}, out);
+  bvhc_status st = finish_mesh(device, pairs, tris, root_links, max_depth, {}, out);
+  if (st == BVHC_OK)
+    keep_serialized(*out, std::move(copies), std::move(slot_nodes), index, index_elem_bytes, index_count, n_verts);
+  return st;
 }
 
 bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per_mesh, const void* const* roots,
@@ -571,6 +681,8 @@ bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per
   std::vector<TriRecord> tris;
   std::vector<uint32_t> root_links;
   std::vector<uint32_t> mesh_root_off{0};
+  std::vector<uint64_t> slot_nodes;
+  std::vector<std::vector<uint8_t>> copies;
   int max_depth = 0;
   try {
     int r = 0;
@@ -579,6 +691,11 @@ bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per
       for (int j = 0; j < roots_per_mesh[k]; ++j, ++r) {
         if (!roots[r] || root_bytes[r] == 0 || root_bytes[r] % 32 != 0) return BVHC_ERR_INVALID_BVH;
         Converter c(pairs, tris);
+        const uint8_t* src = static_cast<const uint8_t*>(roots[r]);
+        copies.emplace_back(src, src + root_bytes[r]);
+        c.slot_nodes = &slot_nodes;
+        c.root_id = (uint64_t)r;
+        c.v1_copy = copies.back().data();
         c.buf = static_cast<const uint8_t*>(roots[r]);
         c.n_nodes = root_bytes[r] / 32;
         c.version = 1;
@@ -603,7 +720,10 @@ bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per
   } catch (const std::bad_alloc&) {
     return BVHC_ERR_OUT_OF_MEMORY;
   }
-  return finish_mesh(device, pairs, tris, root_links, max_depth, mesh_root_off, out);
+  bvhc_status st = finish_mesh(device, pairs, tris, root_links, max_depth, mesh_root_off, out);
+  if (st == BVHC_OK)
+    keep_serialized(*out, std::move(copies), std::move(slot_nodes), index, index_elem_bytes, index_count, n_verts);
+  return st;
 }
 
 void bvhc_mesh_destroy(bvhc_mesh* m) {
@@ -615,6 +735,10 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_nodes_f);
   cudaFree(m->d_tris_f);
   cudaFree(m->d_roots_f);
+  free_refit_plan(m->refit[0]);
+  free_refit_plan(m->refit[1]);
+  cudaFree(m->d_tri_vid);
+  cudaFree(m->d_refit_pos);
   cudaFree(m->d_err);
   cudaFree(m->d_work);
   cudaFree(m->d_in);
@@ -825,10 +949,80 @@ bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* m, int max_leaf) {
   m->rec_face_f.resize(tris.size());
   for (size_t k = 0; k < tris.size(); ++k) m->rec_face_f[k] = tris[k].face;
   m->leaf_size = max_leaf;
+  free_refit_plan(m->refit[1]);
+  if (max_leaf > 0 && !m->h_root_bytes.empty())  // so that a refit keeps this copy in step
+    BVHC_CUDA_TRY(build_refit_plan(pairs, tris, roots, serialized_root_boxes(m), m->refit[1]));
   return BVHC_OK;
 }
 
 int bvhc_mesh_get_leaf_size(const bvhc_mesh* m) { return m ? m->leaf_size : -1; }
+
+bvhc_status bvhc_mesh_refit(bvhc_mesh* m, const float* positions, uint64_t n_verts, int stride_floats, int mem,
+                            void* stream) {
+  if (!m || !positions || stride_floats < 3 || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (n_verts < m->n_verts_geo || m->h_root_bytes.empty()) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (!m->d_tri_vid) {  // 3 vertex ids per triangle, from the geometry index (or 3t + k)
+    uint64_t n_tri = m->h_index.empty() ? m->n_verts_geo / 3 : m->h_index.size() / 3;
+    std::vector<uint32_t> vid(3 * n_tri);
+    for (uint64_t i = 0; i < vid.size(); ++i) vid[i] = m->h_index.empty() ? (uint32_t)i : m->h_index[i];
+    BVHC_CUDA_TRY(upload(&m->d_tri_vid, vid));
+  }
+  if (!m->refit[0].leaves)
+    BVHC_CUDA_TRY(build_refit_plan(m->h_pairs, m->h_tris, m->h_roots, serialized_root_boxes(m), m->refit[0]));
+  const float* pos = positions;
+  if (mem == BVHC_MEM_HOST) {
+    const size_t bytes = n_verts * (size_t)stride_floats * sizeof(float);
+    BVHC_CUDA_TRY(ensure(&m->d_refit_pos, &m->refit_pos_cap, bytes));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_refit_pos, positions, bytes, cudaMemcpyHostToDevice, s));
+    pos = static_cast<const float*>(m->d_refit_pos);
+  } else if (!aligned(positions, 4)) {
+    return BVHC_ERR_INVALID_ARGUMENT;
+  }
+  BVHC_CUDA_TRY(launch_refit(m->refit[0], m->d_nodes, m->d_tris, m->d_tri_vid, pos, stride_floats, false, s));
+  if (m->leaf_size > 0 && m->refit[1].leaves)  // raycastFirst's copy: every box recomputed
+    BVHC_CUDA_TRY(launch_refit(m->refit[1], m->d_nodes_f, m->d_tris_f, m->d_tri_vid, pos, stride_floats, true, s));
+  if (m->d_pos && m->grad_verts <= n_verts) {  // the adjoint's vertex copy follows the geometry
+    BVHC_CUDA_TRY(cudaMemcpy2DAsync(m->d_pos, 3 * sizeof(float), pos, stride_floats * sizeof(float),
+                                    3 * sizeof(float), m->grad_verts, cudaMemcpyDeviceToDevice, s));
+  }
+  if (mem == BVHC_MEM_HOST) return read_and_clear_error(m, s);
+  return BVHC_OK;
+}
+
+int bvhc_mesh_root_count(const bvhc_mesh* m) { return m ? (int)m->h_root_bytes.size() : -1; }
+
+uint64_t bvhc_mesh_root_bytes(const bvhc_mesh* m, int root) {
+  if (!m || root < 0 || root >= (int)m->h_root_bytes.size()) return 0;
+  return m->h_root_bytes[root].size();
+}
+
+bvhc_status bvhc_mesh_read_root(bvhc_mesh* m, int root, void* dst, uint64_t bytes) {
+  if (!m || !dst || root < 0 || root >= (int)m->h_root_bytes.size() || bytes != m->h_root_bytes[root].size())
+    return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  std::vector<uint8_t> buf = m->h_root_bytes[root];
+  if (m->refit[0].leaves) {  // boxes as the last refit left them
+    std::vector<PairNode> pairs(m->n_nodes);
+    std::vector<float> root_box(6 * m->h_root_bytes.size());
+    BVHC_CUDA_TRY(cudaDeviceSynchronize());
+    if (!pairs.empty())
+      BVHC_CUDA_TRY(cudaMemcpy(pairs.data(), m->d_nodes, pairs.size() * sizeof(PairNode), cudaMemcpyDeviceToHost));
+    BVHC_CUDA_TRY(cudaMemcpy(root_box.data(), m->refit[0].root_box, root_box.size() * sizeof(float),
+                             cudaMemcpyDeviceToHost));
+    std::memcpy(buf.data(), &root_box[6 * root], 24);
+    for (size_t k = 0; k < m->slot_nodes.size(); ++k) {
+      uint64_t key = m->slot_nodes[k];
+      if ((int)(key >> 40) != root) continue;
+      uint64_t node = key & ((1ull << 40) - 1);
+      std::memcpy(buf.data() + node * 32, pairs[k >> 1].f + 6 * (k & 1), 24);
+    }
+  }
+  std::memcpy(dst, buf.data(), bytes);
+  return BVHC_OK;
+}
 
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* cfg) {
   if (!m || !cfg) return BVHC_ERR_INVALID_ARGUMENT;

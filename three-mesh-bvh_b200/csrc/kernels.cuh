@@ -97,6 +97,32 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
                                  const RaySort* sort = nullptr);
 
+// Refit (refit.cu).  A box "slot" is where a node's box lives on the device: 2 * pair + side for a
+// child box in a child-pair record, or kRootSlot | root for a root's own box (kept in root_box).
+constexpr uint32_t kRootSlot = 0x80000000u;
+
+struct RefitLeaf {
+  uint32_t first, count, slot;  // triangle records [first, first + count); count 0 for an empty leaf
+};
+
+struct RefitPlan {
+  RefitLeaf* leaves = nullptr;  // one per leaf, including empty leaves and root leaves
+  uint32_t n_leaves = 0;
+  uint32_t* parent = nullptr;   // per pair record: the slot holding the pair's own box
+  uint32_t* arrive = nullptr;   // per pair record: children finished (zeroed before each refit)
+  uint32_t* flags = nullptr;    // per pair record: bit s = child s's box changed
+  uint32_t n_pairs = 0;
+  float* root_box = nullptr;    // 6 floats per root
+};
+
+// New vertex positions into the triangle records, leaf boxes from them, and pair boxes bottom-up
+// (one thread per leaf; the second child to finish a pair carries on upward).  force = false
+// follows the reference's rule (MeshBVH#refit, refit.template.js:4-196): a leaf box is rewritten
+// and reported changed only when it differs, a parent's box is recomputed only when a child
+// changed; force = true recomputes every box.  tri_vid: 3 vertex ids per triangle (faceIndex).
+cudaError_t launch_refit(const RefitPlan& plan, PairNode* pairs, TriRecord* tris, const uint32_t* tri_vid,
+                         const float* pos, int stride, bool force, cudaStream_t stream);
+
 // What another translation unit needs to launch on a mesh: its device view, traversal variant and
 // device ordinal (defined in api.cu).  Returns false for a null mesh.
 bool mesh_launch_info(const bvhc_mesh* mesh, MeshDev* view, TraversalConfig* cfg, int* device);
