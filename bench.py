@@ -707,9 +707,16 @@ def run_adjoint(args, ws, rank, local):
         torch.cuda.synchronize(dev)
         return a.elapsed_time(b) / args.steps
 
+    # refit after a gradient step (the vertices moved a little): boxes rebuilt on the device
+    pos_step = torch.from_numpy(geo.position).to(dev) - 1e-4 * gv
+
+    def refit():
+        bvh.refit(pos_step, stream=s, read_back=False)
+
     with ClockSampler(local) as clk:
         ms_f, ms_fb = timed(fwd), timed(fwd_bwd)
         ms_cf, ms_cfb = timed(cp_fwd), timed(cp_fwd_bwd)
+        ms_refit = timed(refit)
     bvh.synchronize(s)
     if rank == 0:
         line = {"metric": "fwd+bwd / fwd time, raycastFirst depth loss (2M tri, 1024^2 camera)",
@@ -723,6 +730,7 @@ def run_adjoint(args, ws, rank, local):
                 "closest_point": {"fwd_ms": ms_cf, "fwd_bwd_ms": ms_cfb, "ratio": ms_cfb / ms_cf},
                 "forward_variants": {"raycast": tuned_ray["sets"]["camera1024"]["best"],
                                      "leaf_size": tuned_ray["leaf"], "closest": tuned_cp["best"]},
+                "refit_ms": ms_refit,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     bvh.dispose()

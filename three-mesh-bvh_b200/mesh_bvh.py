@@ -211,24 +211,28 @@ class MeshBVH:
         N.check(N.lib().bvhc_mesh_get_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_get_traversal")
         return {k: getattr(cfg, k) for k, _ in N.BvhcTraversalConfig._fields_}
 
-    def refit(self, positions=None, stream=None) -> None:
+    def refit(self, positions=None, stream=None, read_back: bool = True) -> None:
         """MeshBVH#refit() (MeshBVH.js:504-508) on the GPU after the vertices moved.  positions:
         None (the geometry's position array, host memory), a numpy array, or a torch CUDA tensor
-        (n x 3, on the device; enqueued on `stream`).  The serialized roots are read back, so
-        serialize() returns the refit boxes as the reference's would."""
+        (n x 3, on the device; enqueued on `stream`).  With read_back the serialized roots are
+        copied back (waiting for the device), so serialize() returns the refit boxes as the
+        reference's would; without it a device-memory refit only enqueues."""
         lib, mesh = N.lib(), self._device_mesh()
         if positions is not None and self._is_torch(positions):
             import torch
             p = positions.contiguous()
             s = stream if stream is not None else torch.cuda.current_stream(p.device).cuda_stream
             N.check(lib.bvhc_mesh_refit(mesh, p.data_ptr(), p.shape[0], 3, N.MEM_DEVICE, s), "bvhc_mesh_refit")
-            N.check(lib.bvhc_mesh_synchronize(mesh, s), "bvhc_mesh_synchronize")
+            if read_back:
+                N.check(lib.bvhc_mesh_synchronize(mesh, s), "bvhc_mesh_synchronize")
         else:
             pos = self.geometry.position if positions is None else positions
             pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
             if positions is not None:
                 self.geometry.position = pos
             N.check(lib.bvhc_mesh_refit(mesh, _ptr(pos), pos.shape[0], 3, N.MEM_HOST, None), "bvhc_mesh_refit")
+        if not read_back:
+            return
         roots = []
         for r in range(lib.bvhc_mesh_root_count(mesh)):
             buf = np.empty(lib.bvhc_mesh_root_bytes(mesh, r), dtype=np.uint8)
