@@ -189,6 +189,8 @@ def parse_traversal(spec, names):
 def traversal_kernel(cfg):
     """Name of the raycastFirst traversal kernel a variant launches."""
     p = 1 if cfg is None else cfg[0]
+    if p == 2 and cfg is not None and len(cfg) > 7 and cfg[7]:
+        return "raycast_first_packet4_kernel"
     return {0: "raycast_first_kernel", 1: "raycast_first_persistent_kernel", 2: "raycast_first_packet_kernel"}[p]
 
 

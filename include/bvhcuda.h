@@ -134,14 +134,15 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * blocks per SM.  compact = 1
  * (persistent = 1 or 2) first finishes, in one coalesced pass, the rays that miss every root's
  * child boxes and traverses only the others.  sort (persistent = 1 or 2, single meshes; implies
- * the compaction pass) orders the remaining rays by a 30-bit Morton key before the traversal:
- * 1 the ray direction, 2 the point where the ray enters the mesh's bounding box, 3 that point
- * (coarser) followed by the direction; 0 keeps the input order.  closest selects
- * closestPointToPoint's kernel: 0 one query per thread, 1 the 32 queries of a warp through one
- * shared traversal (for spatially coherent queries such as grids), 2 the same over the queries
- * sorted by a Morton key of the point; 1 and 2 apply with minThreshold 0 (otherwise 0 runs), and
- * use the occupancy setting too.  Results are the same for every variant (up to exact ties); the
- * autotuner picks the fastest per mesh and workload. */
+ * the compaction pass) orders the remaining rays by a Morton key before the traversal: 1 the ray
+ * direction (cube-map coordinates), 2 the point where the ray enters the mesh's bounding box, 3
+ * that point (coarser) followed by the direction; 0 keeps the input order.  wide = 1 makes the
+ * warp-cooperative form walk four-child records (collapsed from raycastFirst's child pairs, same
+ * leaves).  closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32
+ * queries of a warp through one shared traversal (for spatially coherent queries such as grids),
+ * 2 the same over the queries sorted by a Morton key of the point; 1 and 2 apply with
+ * minThreshold 0 (otherwise 0 runs), and use the occupancy setting too.  Results are the same for
+ * every variant (up to exact ties); the autotuner picks the fastest per mesh and workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;
   int32_t order;
@@ -150,6 +151,7 @@ typedef struct bvhc_traversal_config {
   int32_t compact;
   int32_t sort;
   int32_t closest;
+  int32_t wide;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);

@@ -223,7 +223,7 @@ def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occ
     ref = _oracle_for(orc, bvh, geo)
     bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
-                                       compact=compact, sort=sort, closest=0)
+                                       compact=compact, sort=sort, closest=0, wide=0)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -278,7 +278,7 @@ def test_split_leaf_layouts_agree(pkg, orc, cuda, leaf):
                            pkg.rays_sphere_to_box(30_000, seed=6)])
     ac, ah = ref.raycast_all(rays, 0, cap=64)
     exp = ref.raycast_first(rays, 0)
-    for cfg in ((0, 1, 16, 0, 0, 0), (1, 1, 32, 2, 1, 2), (2, 1, 16, 2, 1, 1)):
+    for cfg in ((0, 1, 16, 0, 0, 0), (1, 1, 32, 2, 1, 2), (2, 1, 16, 2, 1, 1), (2, 1, 16, 2, 1, 1, 0, 1)):
         bvh.set_traversal(*cfg)
         _assert_first_ok(check_first(bvh.raycast_first_batch(rays, 0), exp, tie_exempt(ac, ah)))
     counts, hits = bvh.raycast_batch(rays, 0, cap=64)
@@ -332,3 +332,30 @@ def test_closest_point_warp_cooperative(pkg, orc, knot80k, closest, occupancy):
             if lo_t == 0.0:
                 assert rep["distance"] == 0, (lo_t, hi_t, rep)
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
+
+
+@pytest.mark.parametrize("leaf,occupancy,compact,sort", [(0, 0, 0, 0), (0, 2, 1, 1), (4, 1, 1, 2), (2, 2, 0, 0),
+                                                         (3, 0, 1, 3)])
+def test_wide_warp_cooperative_raycast_first(pkg, orc, cuda, leaf, occupancy, compact, sort):
+    """raycastFirst over the four-child records (with the reference's or split leaves), against the
+    oracle, including near/far limits and a double-sided pass; the records follow a refit."""
+    geo = pkg.torus_knot(10, 3, 400, 80, noise_sigma=0.02, noise_seed=1)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = _oracle_for(orc, bvh, geo)
+    bvh.set_leaf_size(leaf)
+    bvh.set_traversal(2, 1, 16, occupancy, compact, sort, 0, 1)
+    assert bvh.get_traversal()["wide"] == 1
+    rays = np.concatenate([pkg.rays_incoherent(60_000, seed=9), pkg.rays_camera(200, 200),
+                           pkg.rays_sphere_to_box(30_000, seed=10)])
+    for side, near, far in ((0, 0.0, math.inf), (2, 0.0, math.inf), (0, 30.0, 45.0)):
+        got = bvh.raycast_first_batch(rays, side, near, far)
+        exp = ref.raycast_first(rays, side, near, far)
+        ac, ah = ref.raycast_all(rays, side, near, far, cap=64)
+        _assert_first_ok(check_first(got, exp, tie_exempt(ac, ah)))
+    pos = (geo.position * np.float32(1.25)).astype(np.float32)
+    bvh.refit(pos)
+    ref.refit(pos)
+    got = bvh.raycast_first_batch(rays)
+    ac, ah = ref.raycast_all(rays, cap=64)
+    _assert_first_ok(check_first(got, ref.raycast_first(rays), tie_exempt(ac, ah)))
+    bvh.dispose()

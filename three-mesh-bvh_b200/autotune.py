@@ -14,13 +14,17 @@ import json
 import math
 from pathlib import Path
 
-# (persistent, order, refill, occupancy, compact, sort): one ray per thread; warp-cooperative
-# traversal; persistent warps with lane refill.  The last two select the root-box compaction pass
-# and the Morton-key ray ordering (0 none, 1 direction, 2 entry point, 3 entry point + direction).
+# (persistent, order, refill, occupancy, compact, sort, closest, wide): one ray per thread;
+# warp-cooperative traversal over child pairs (wide 0; order 0 / 1) or four-child records (wide 1);
+# persistent warps with lane refill.  compact / sort select the root-box compaction pass and the
+# Morton-key ray ordering (0 none, 1 direction, 2 entry point, 3 entry point + direction); closest
+# is closestPointToPoint's kernel and is tuned separately (tune_closest_point).
 _QUEUE = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)]
-CANDIDATES = [(0, 0, 16, 0, 0, 0), (0, 1, 16, 0, 0, 0)] + [
-    (2, order, 16, occ, c, s) for order in (0, 1) for occ in (0, 1, 2) for c, s in _QUEUE] + [
-    (1, order, refill, occ, c, s) for order in (0, 1) for refill in (16, 32) for occ in (1, 2) for c, s in _QUEUE]
+CANDIDATES = [(0, 0, 16, 0, 0, 0, 0, 0), (0, 1, 16, 0, 0, 0, 0, 0)] + [
+    (2, order, 16, occ, c, s, 0, 0) for order in (0, 1) for occ in (0, 1, 2) for c, s in _QUEUE] + [
+    (2, 1, 16, occ, c, s, 0, 1) for occ in (0, 1, 2) for c, s in _QUEUE] + [
+    (1, order, refill, occ, c, s, 0, 0) for order in (0, 1) for refill in (16, 32) for occ in (1, 2)
+    for c, s in _QUEUE]
 
 _cache: dict = {}
 

@@ -26,7 +26,7 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
@@ -91,9 +91,19 @@ struct bvhc_mesh {
   void* d_refit_pos = nullptr;
   size_t refit_pos_cap = 0;
 
+  // four-child records over raycastFirst's child-pair records (same triangle records), with the
+  // child-pair slot each quad child's box comes from
+  QuadNode* d_quads = nullptr;
+  uint32_t* d_quad_roots = nullptr;
+  uint32_t* d_quad_src = nullptr;
+  uint64_t n_quads = 0;
+
   // the records raycastFirst traverses
   MeshDev view_first() const {
-    return leaf_size ? MeshDev{d_nodes_f, d_tris_f, d_roots_f, n_roots, d_err} : view();
+    MeshDev v = leaf_size ? MeshDev{d_nodes_f, d_tris_f, d_roots_f, n_roots, d_err} : view();
+    v.quads = d_quads;
+    v.quad_roots = d_quad_roots;
+    return v;
   }
 
   MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
@@ -398,6 +408,71 @@ struct LeafSplitter {
   }
 };
 
+// Four-child records from a child-pair tree: starting from a pair's two children, the internal
+// child with the largest box surface area is replaced by its own two children until there are
+// four children or only leaves.  `src` keeps, per quad child, the child-pair slot its box comes
+// from (2 * pair + side; kEmptyLeaf for an unused child), so refits can copy boxes over.
+struct QuadBuilder {
+  const std::vector<PairNode>& pairs;
+  std::vector<QuadNode> quads;
+  std::vector<uint32_t> src;
+
+  static float area(const float* b) {
+    float dx = std::max(b[3] - b[0], 0.0f), dy = std::max(b[4] - b[1], 0.0f), dz = std::max(b[5] - b[2], 0.0f);
+    return dx * dy + dy * dz + dz * dx;
+  }
+
+  uint32_t build(uint32_t pair) {
+    struct Child {
+      uint32_t link, slot;
+      const float* box;
+    };
+    Child ch[4];
+    int n = 2;
+    ch[0] = {pairs[pair].link[0], 2 * pair, pairs[pair].f};
+    ch[1] = {pairs[pair].link[1], 2 * pair + 1, pairs[pair].f + 6};
+    while (n < 4) {
+      int pick = -1;
+      float best = -1.0f;
+      for (int k = 0; k < n; ++k) {
+        if (ch[k].link & kLeafBit) continue;
+        float a = area(ch[k].box);
+        if (a > best) {
+          best = a;
+          pick = k;
+        }
+      }
+      if (pick < 0) break;
+      const uint32_t p = ch[pick].link;
+      ch[pick] = {pairs[p].link[0], 2 * p, pairs[p].f};
+      ch[n++] = {pairs[p].link[1], 2 * p + 1, pairs[p].f + 6};
+    }
+    if (quads.size() >= (uint64_t)kLeafBit) throw Status{BVHC_ERR_UNSUPPORTED};
+    const uint32_t idx = (uint32_t)quads.size();
+    quads.push_back(QuadNode{});
+    src.resize(4 * (size_t)(idx + 1), kEmptyLeaf);
+    for (int k = 0; k < 4; ++k) {
+      QuadNode& q = quads[idx];
+      if (k < n) {
+        for (int a = 0; a < 3; ++a) {
+          q.lo[a][k] = ch[k].box[a];
+          q.hi[a][k] = ch[k].box[3 + a];
+        }
+        q.link[k] = ch[k].link;
+        src[4 * (size_t)idx + k] = ch[k].slot;
+      } else {
+        q.link[k] = kEmptyLeaf;
+      }
+    }
+    for (int k = 0; k < n; ++k)
+      if (!(ch[k].link & kLeafBit)) {
+        uint32_t q = build(ch[k].link);
+        quads[idx].link[k] = q;
+      }
+    return idx;
+  }
+};
+
 }  // namespace
 
 bool bvhc::mesh_launch_info(const bvhc_mesh* m, MeshDev* view, TraversalConfig* cfg, int* device) {
@@ -466,6 +541,38 @@ static void keep_serialized(bvhc_mesh* m, std::vector<std::vector<uint8_t>> root
     m->h_index.resize(index_count);
     for (uint64_t i = 0; i < index_count; ++i) m->h_index[i] = read_index(index, index_elem, i);
   }
+}
+
+// Four-child records over raycastFirst's child-pair layout (pairs + roots), replacing any before.
+static cudaError_t install_quads(bvhc_mesh* m, const std::vector<PairNode>& pairs, const std::vector<uint32_t>& roots) {
+  QuadBuilder qb{pairs};
+  std::vector<uint32_t> qroots(roots.size());
+  try {
+    for (size_t r = 0; r < roots.size(); ++r) qroots[r] = (roots[r] & kLeafBit) ? roots[r] : qb.build(roots[r]);
+  } catch (const Status&) {
+    return cudaErrorInvalidValue;
+  } catch (const std::bad_alloc&) {
+    return cudaErrorMemoryAllocation;
+  }
+  QuadNode* q = nullptr;
+  uint32_t *qr = nullptr, *qs = nullptr;
+  cudaError_t e = upload(&q, qb.quads);
+  if (e == cudaSuccess) e = upload(&qr, qroots);
+  if (e == cudaSuccess) e = upload(&qs, qb.src);
+  if (e != cudaSuccess) {
+    cudaFree(q);
+    cudaFree(qr);
+    cudaFree(qs);
+    return e;
+  }
+  cudaFree(m->d_quads);
+  cudaFree(m->d_quad_roots);
+  cudaFree(m->d_quad_src);
+  m->d_quads = q;
+  m->d_quad_roots = qr;
+  m->d_quad_src = qs;
+  m->n_quads = qb.quads.size();
+  return cudaSuccess;
 }
 
 static void free_refit_plan(RefitPlan& p) {
@@ -663,8 +770,15 @@ bvhc_status bvhc_mesh_create(int device, int version, const void* const* roots, 
     return BVHC_ERR_OUT_OF_MEMORY;
   }
   bvhc_status st = finish_mesh(device, pairs, tris, root_links, max_depth, {}, out);
-  if (st == BVHC_OK)
+  if (st == BVHC_OK) {
     keep_serialized(*out, std::move(copies), std::move(slot_nodes), index, index_elem_bytes, index_count, n_verts);
+    cudaError_t e = install_quads(*out, (*out)->h_pairs, (*out)->h_roots);
+    if (e != cudaSuccess) {
+      bvhc_mesh_destroy(*out);
+      *out = nullptr;
+      return from_cuda(e);
+    }
+  }
   return st;
 }
 
@@ -721,8 +835,15 @@ bvhc_status bvhc_batch_create(int device, int n_meshes, const int32_t* roots_per
     return BVHC_ERR_OUT_OF_MEMORY;
   }
   bvhc_status st = finish_mesh(device, pairs, tris, root_links, max_depth, mesh_root_off, out);
-  if (st == BVHC_OK)
+  if (st == BVHC_OK) {
     keep_serialized(*out, std::move(copies), std::move(slot_nodes), index, index_elem_bytes, index_count, n_verts);
+    cudaError_t e = install_quads(*out, (*out)->h_pairs, (*out)->h_roots);
+    if (e != cudaSuccess) {
+      bvhc_mesh_destroy(*out);
+      *out = nullptr;
+      return from_cuda(e);
+    }
+  }
   return st;
 }
 
@@ -737,6 +858,9 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_roots_f);
   free_refit_plan(m->refit[0]);
   free_refit_plan(m->refit[1]);
+  cudaFree(m->d_quads);
+  cudaFree(m->d_quad_roots);
+  cudaFree(m->d_quad_src);
   cudaFree(m->d_tri_vid);
   cudaFree(m->d_refit_pos);
   cudaFree(m->d_err);
@@ -842,7 +966,7 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
     if (e != cudaSuccess) return e;
     if (m->cfg.persistent == 2)
       return launch_raycast_first_packet(m->view_first(), rays, n, side, tab, near_d, far_d, out, m->cfg.order,
-                                         m->cfg.occupancy, s, q, qc, sorted ? &sort : nullptr);
+                                         m->cfg.occupancy, m->cfg.wide, s, q, qc, sorted ? &sort : nullptr);
     return launch_raycast_first_persistent(m->view_first(), nullptr, rays, n, side, tab, near_d, far_d, out, work,
                                            m->cfg, s, q, qc, sorted ? &sort : nullptr);
   }
@@ -854,7 +978,7 @@ static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* ra
                                  float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
   if (m->cfg.persistent == 2)
     return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order,
-                                       m->cfg.occupancy, s);
+                                       m->cfg.occupancy, m->cfg.wide, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;
@@ -891,13 +1015,13 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1);
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy,
-                           cfg->compact,    cfg->sort,  cfg->closest};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill,  cfg->occupancy,
+                           cfg->compact,    cfg->sort,  cfg->closest, cfg->wide};
   return BVHC_OK;
 }
 
@@ -952,6 +1076,8 @@ bvhc_status bvhc_mesh_set_leaf_size(bvhc_mesh* m, int max_leaf) {
   free_refit_plan(m->refit[1]);
   if (max_leaf > 0 && !m->h_root_bytes.empty())  // so that a refit keeps this copy in step
     BVHC_CUDA_TRY(build_refit_plan(pairs, tris, roots, serialized_root_boxes(m), m->refit[1]));
+  if (max_leaf > 0) BVHC_CUDA_TRY(install_quads(m, pairs, roots));
+  else BVHC_CUDA_TRY(install_quads(m, m->h_pairs, m->h_roots));
   return BVHC_OK;
 }
 
@@ -984,6 +1110,9 @@ bvhc_status bvhc_mesh_refit(bvhc_mesh* m, const float* positions, uint64_t n_ver
   BVHC_CUDA_TRY(launch_refit(m->refit[0], m->d_nodes, m->d_tris, m->d_tri_vid, pos, stride_floats, false, s));
   if (m->leaf_size > 0 && m->refit[1].leaves)  // raycastFirst's copy: every box recomputed
     BVHC_CUDA_TRY(launch_refit(m->refit[1], m->d_nodes_f, m->d_tris_f, m->d_tri_vid, pos, stride_floats, true, s));
+  if (m->d_quads)  // the four-child records take their boxes from raycastFirst's child pairs
+    BVHC_CUDA_TRY(launch_quad_boxes(m->d_quads, m->n_quads, m->d_quad_src, m->leaf_size > 0 ? m->d_nodes_f : m->d_nodes,
+                                    s));
   if (m->d_pos && m->grad_verts <= n_verts) {  // the adjoint's vertex copy follows the geometry
     BVHC_CUDA_TRY(cudaMemcpy2DAsync(m->d_pos, 3 * sizeof(float), pos, stride_floats * sizeof(float),
                                     3 * sizeof(float), m->grad_verts, cudaMemcpyDeviceToDevice, s));
@@ -1033,6 +1162,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->compact = m->cfg.compact;
   cfg->sort = m->cfg.sort;
   cfg->closest = m->cfg.closest;
+  cfg->wide = m->cfg.wide;
   return BVHC_OK;
 }
 
@@ -1256,7 +1386,8 @@ bvhc_status bvhc_batch_raycast_first_per_mesh(bvhc_mesh* m, const float* rays, c
     uint64_t off = ray_offsets[k], cnt = ray_offsets[k + 1] - off;
     if (cnt == 0) continue;
     MeshDev v = m->view_first();
-    v.roots = m->d_roots + m->mesh_root_off[k];
+    v.roots += m->mesh_root_off[k];  // this geometry's roots, in whichever layout the view uses
+    if (v.quad_roots) v.quad_roots += m->mesh_root_off[k];
     v.n_roots = (int)(m->mesh_root_off[k + 1] - m->mesh_root_off[k]);
     BVHC_CUDA_TRY(dispatch_view(m, v, rays + 6 * off, cnt, side, near_d, far_d, out + off, s));
   }

@@ -399,6 +399,137 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet_kernel(Mesh
 }
 
 // ---------------------------------------------------------------------------------------------
+// raycastFirst, warp-cooperative over the four-child records (m.quads): the same shared traversal
+// as above with half as many node visits.  At a record each lane tests the four child boxes (one
+// 16-byte load per bound plane serves all four); the children any lane enters are ordered by the
+// entry distances of the first lane that enters one (the warp's rays are coherent), the nearest is
+// visited and the others are stacked farthest first, each with every lane's own entry distance.
+// ---------------------------------------------------------------------------------------------
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
+    MeshDev m, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides, float near_d,
+    float far_d, bvhc_hit* __restrict__ out, const uint32_t* __restrict__ queue,
+    const unsigned int* __restrict__ qcount) {
+  __shared__ uint32_t s_link[kWarps][kMaxStack];
+  const unsigned full = 0xFFFFFFFFu;
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
+  const bool valid = i < n_work;
+  if (valid && queue) i = __ldg(queue + i);
+  RayF r;
+  float dlen = 1.0f;
+  if (valid) {
+    r = make_ray(rays, i);
+    dlen = sqrtf(r.d.x * r.d.x + r.d.y * r.d.y + r.d.z * r.d.z);
+  } else {
+    r.o = make_float3(0.f, 0.f, 0.f);
+    r.d = make_float3(1.f, 0.f, 0.f);
+    r.inv = make_float3(1.f, 1e30f, 1e30f);
+    r.d_l1 = 1.f;
+  }
+  Best best{kInf, 0.0f, 0xFFFFFFFFu};
+  float lane_t[kMaxStack];
+  for (int root = 0; root < m.n_roots; ++root) {
+    uint32_t link = m.quad_roots[root];
+    int sp = 0;
+    for (;;) {
+      bool pop = false;
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf && valid) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
+        pop = true;
+      } else {
+        const QuadNode* qn = m.quads + link;
+        const float4 lx = ld4(qn->lo[0]), ly = ld4(qn->lo[1]), lz = ld4(qn->lo[2]);
+        const float4 hx = ld4(qn->hi[0]), hy = ld4(qn->hi[1]), hz = ld4(qn->hi[2]);
+        const float4 lk = ld4(qn->link);
+        const uint32_t ck[4] = {__float_as_uint(lk.x), __float_as_uint(lk.y), __float_as_uint(lk.z),
+                                __float_as_uint(lk.w)};
+        const float blo[3][4] = {{lx.x, lx.y, lx.z, lx.w}, {ly.x, ly.y, ly.z, ly.w}, {lz.x, lz.y, lz.z, lz.w}};
+        const float bhi[3][4] = {{hx.x, hx.y, hx.z, hx.w}, {hy.x, hy.y, hy.z, hy.w}, {hz.x, hz.y, hz.z, hz.w}};
+        const float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
+        float e[4];
+        bool h[4];
+        unsigned b[4];
+        unsigned any = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          h[c] = valid && ck[c] != kEmptyLeaf &&
+                 box_hit(blo[0][c], blo[1][c], blo[2][c], bhi[0][c], bhi[1][c], bhi[2][c], r, near_d, lim, e[c]);
+          b[c] = __ballot_sync(full, h[c]);
+          any |= b[c];
+        }
+        if (!any) {
+          pop = true;
+        } else {
+          const int leader = __ffs(any) - 1;
+          float key[4];
+          int idx[4];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float kc = __shfl_sync(full, h[c] ? e[c] : kInf, leader);
+            key[c] = b[c] ? kc : kInf;
+            idx[c] = c;
+          }
+          // sort the four (key, child) pairs, nearest first (warp-uniform values)
+          auto cas = [&](int a, int c) {
+            if (key[c] < key[a]) {
+              float tk = key[a]; key[a] = key[c]; key[c] = tk;
+              int ti = idx[a]; idx[a] = idx[c]; idx[c] = ti;
+            }
+          };
+          cas(0, 1); cas(2, 3); cas(0, 2); cas(1, 3); cas(1, 2);
+          if (sp + 3 > kMaxStack) {
+            if (lane == 0) atomicOr(m.err, kErrStackOverflow);
+            best.rec = 0xFFFFFFFFu;
+            root = m.n_roots;
+            break;
+          }
+          // children that some lane enters, farthest pushed first; the nearest is visited now
+          uint32_t next = kEmptyLeaf;
+          bool have_next = false;
+#pragma unroll
+          for (int j = 3; j >= 0; --j) {
+            const int c = idx[j];
+            if (!b[c]) continue;
+            if (j == 0) {
+              next = ck[c];
+              have_next = true;
+            } else {
+              if (lane == 0) s_link[w][sp] = ck[c];
+              lane_t[sp] = h[c] ? e[c] : kInf;
+              ++sp;
+            }
+          }
+          if (have_next) {
+            link = next;
+          } else {  // the first key belonged to a child no lane enters: every entered one was stacked
+            pop = true;
+          }
+          __syncwarp();
+        }
+      }
+      if (pop) {
+        bool found = false;
+        while (sp > 0) {
+          --sp;
+          float plim = (best.t + best.err) * (1.0f + kSlabMargin);
+          if (__ballot_sync(full, valid && lane_t[sp] <= plim)) {
+            link = s_link[w][sp];
+            found = true;
+            break;
+          }
+        }
+        if (!found) break;
+      }
+    }
+  }
+  if (valid) finish_first(m, best.rec, r, out + i);
+}
+
+// ---------------------------------------------------------------------------------------------
 // raycast, all hits (raycast.template.js:15-53): left child then right child, every hit kept
 // in DFS order.  The first `cap` hits are stored; counts[i] is the uncapped total.
 // ---------------------------------------------------------------------------------------------
@@ -1169,8 +1300,8 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        int occupancy, cudaStream_t stream, uint32_t* queue, unsigned int* qcount,
-                                        const RaySort* sort) {
+                                        int occupancy, int wide, cudaStream_t stream, uint32_t* queue,
+                                        unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
   const bool compact = queue != nullptr && qcount != nullptr && n < (1ull << 32);
   if (compact) {
@@ -1179,6 +1310,13 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
   } else {
     queue = nullptr;
     qcount = nullptr;
+  }
+  if (wide && m.quads && m.quad_roots) {
+    auto k4 = occupancy == 0   ? dev::raycast_first_packet4_kernel<1>
+              : occupancy == 1 ? dev::raycast_first_packet4_kernel<6>
+                               : dev::raycast_first_packet4_kernel<8>;
+    k4<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount);
+    return cudaGetLastError();
   }
   auto kernel = order == 0 ? (occupancy == 0 ? dev::raycast_first_packet_kernel<0, 1>
                                               : occupancy == 1 ? dev::raycast_first_packet_kernel<0, 6>

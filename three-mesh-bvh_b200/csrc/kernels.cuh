@@ -21,6 +21,8 @@ struct MeshDev {
   const uint32_t* roots;  // one link per root
   int n_roots;
   unsigned int* err;
+  const QuadNode* quads = nullptr;     // four-child copy of `nodes` (same triangle records), if any
+  const uint32_t* quad_roots = nullptr;
 };
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
@@ -41,6 +43,7 @@ struct TraversalConfig {
                    // the pre-pass
   int closest;     // closestPointToPoint: 0 one query per thread, 1 warp-cooperative, 2 warp-cooperative
                    // over Morton-sorted queries (1 and 2 only with minThreshold 0)
+  int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -85,9 +88,10 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
                                             unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 // Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).  With a
 // queue, the same pre-pass (and sort) as the persistent form runs first.
+// wide = 1 with m.quads set runs over the four-child records.
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
                                         const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        int occupancy, cudaStream_t stream, uint32_t* queue = nullptr,
+                                        int occupancy, int wide, cudaStream_t stream, uint32_t* queue = nullptr,
                                         unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 // closestPointToPoint.  variant 0: one query per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the queries sorted by a Morton key of the point (queue, qcount and sort
@@ -122,6 +126,10 @@ struct RefitPlan {
 // changed; force = true recomputes every box.  tri_vid: 3 vertex ids per triangle (faceIndex).
 cudaError_t launch_refit(const RefitPlan& plan, PairNode* pairs, TriRecord* tris, const uint32_t* tri_vid,
                          const float* pos, int stride, bool force, cudaStream_t stream);
+// Copies every four-child record's child boxes from the child-pair slots they were collapsed from
+// (src: 4 per record, kEmptyLeaf for an unused child).
+cudaError_t launch_quad_boxes(QuadNode* quads, uint64_t n_quads, const uint32_t* src, const PairNode* pairs,
+                              cudaStream_t stream);
 
 // What another translation unit needs to launch on a mesh: its device view, traversal variant and
 // device ordinal (defined in api.cu).  Returns false for a null mesh.

@@ -32,6 +32,18 @@ struct alignas(16) PairNode {
 };
 static_assert(sizeof(PairNode) == 64, "PairNode must be 64 bytes");
 
+// Four-child record for raycastFirst's warp-cooperative traversal, collapsed from the child-pair
+// tree (each internal child replaced by its own two children, largest surface area first, until
+// four children or only leaves remain).  Planes are stored per axis for the four children, so one
+// 16-byte load gives one bound of all four boxes.  Unused children have link kEmptyLeaf.
+struct alignas(64) QuadNode {
+  float lo[3][4];     // lo[axis][child]
+  float hi[3][4];     // hi[axis][child]
+  uint32_t link[4];   // internal child -> quad record index; leaf -> kLeafBit | first triangle record
+  uint32_t pad[4];
+};
+static_assert(sizeof(QuadNode) == 128, "QuadNode must be 128 bytes");
+
 struct alignas(16) TriRecord {
   // v[0..8] = a.xyz, b.xyz, c.xyz ; face = reference faceIndex ; flags bit 0 = last in leaf ;
   // material = materialIndex of the geometry group holding the triangle (kNoMaterial: none)

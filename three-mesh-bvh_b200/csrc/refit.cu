@@ -82,7 +82,32 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(RefitPlan plan, Pair
   }
 }
 
+// Four-child records: each child box is copied from the child-pair slot it was collapsed from.
+__global__ void __launch_bounds__(kRefitBlock) quad_boxes_kernel(QuadNode* __restrict__ quads, uint64_t n_quads,
+                                                                 const uint32_t* __restrict__ src,
+                                                                 const PairNode* __restrict__ pairs) {
+  const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 4 * n_quads) return;
+  const uint32_t slot = __ldg(src + k);
+  if (slot == kEmptyLeaf) return;
+  const float* b = pairs[slot >> 1].f + 6 * (slot & 1u);
+  QuadNode& q = quads[k >> 2];
+  const int c = (int)(k & 3u);
+  for (int a = 0; a < 3; ++a) {
+    q.lo[a][c] = b[a];
+    q.hi[a][c] = b[3 + a];
+  }
+}
+
 }  // namespace dev
+
+cudaError_t launch_quad_boxes(QuadNode* quads, uint64_t n_quads, const uint32_t* src, const PairNode* pairs,
+                              cudaStream_t stream) {
+  if (n_quads == 0) return cudaSuccess;
+  const unsigned int grid = (unsigned int)((4 * n_quads + dev::kRefitBlock - 1) / dev::kRefitBlock);
+  dev::quad_boxes_kernel<<<grid, dev::kRefitBlock, 0, stream>>>(quads, n_quads, src, pairs);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_refit(const RefitPlan& plan, PairNode* pairs, TriRecord* tris, const uint32_t* tri_vid,
                          const float* pos, int stride, bool force, cudaStream_t stream) {
