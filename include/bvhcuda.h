@@ -289,6 +289,13 @@ bvhc_status bvhc_closest_point_backward(bvhc_mesh* mesh, const float* points, co
                                         const float* grad_distance, float* grad_vertices, float* grad_points,
                                         void* stream);
 
+/* MeshBVH#intersectsSphere(sphere) for every sphere (src/core/MeshBVH.js:796-809: shapecast with
+ * the sphere/box and sphere/triangle tests, src/math/MathUtilities.js:167-201).  spheres: n x 4
+ * float32 (centre xyz, radius; device buffers 16-byte aligned); out[i] = 1 when some triangle lies
+ * within the radius of the centre, else 0. */
+bvhc_status bvhc_intersects_sphere(bvhc_mesh* mesh, const float* spheres, uint64_t n, uint8_t* out, int mem,
+                                   void* stream);
+
 /* MeshBVH#closestPointToPoint(point, target, minThreshold, maxThreshold) for every point
  * (src/core/MeshBVH.js:874-884, src/core/cast/closestPointToPoint.js:6-78). */
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* mesh, const float* points, uint64_t n, float min_threshold,

@@ -781,6 +781,66 @@ void closest_point(const Bvh& g, V3 p, double min_t, double max_t, orc_cp* out, 
   out->point[0] = st.closest_point.x; out->point[1] = st.closest_point.y; out->point[2] = st.closest_point.z;
 }
 
+// ---------------------------------------------------------------------------------------------
+// MeshBVH#intersectsSphere (MeshBVH.js:796-809): shapecast with intersectsBounds = the sphere meets
+// the box (squared distance from the centre to the clamped centre <= r^2) and intersectsTriangle =
+// sphereIntersectTriangle (src/math/MathUtilities.js:167-201): the sphere meets one of the three
+// edges (closest point of the segment within r), or the triangle's plane is within r and the
+// centre's projection on it lies in the triangle (barycentric test, Ericson RTCD 3.4; a triangle
+// with a zero Gram determinant contains nothing).  The result does not depend on the visiting
+// order: it is whether any reached triangle meets the sphere.
+// ---------------------------------------------------------------------------------------------
+// JavaScript Math.min / Math.max (NaN propagates)
+inline double js_min(double a, double b) { return (a != a || b != b) ? NAN : (a < b ? a : b); }
+inline double js_max(double a, double b) { return (a != a || b != b) ? NAN : (a > b ? a : b); }
+
+double segment_distance(V3 p, V3 s, V3 e) {
+  V3 d = sub(e, s);
+  double t = dot(sub(p, s), d) / dot(d, d);
+  t = js_max(0.0, js_min(1.0, t));
+  return std::sqrt(dist_sq(add(s, scale(d, t)), p));
+}
+
+bool sphere_meets_triangle(V3 c, double r, V3 a, V3 b, V3 cc) {
+  if (segment_distance(c, a, b) <= r) return true;
+  if (segment_distance(c, a, cc) <= r) return true;
+  if (segment_distance(c, b, cc) <= r) return true;
+  V3 n = cross(sub(cc, b), sub(a, b));
+  double len = std::sqrt(dot(n, n));
+  if (len > 0) n = scale(n, 1.0 / len);
+  double constant = -dot(a, n);
+  double dp = dot(n, c) + constant;
+  if (std::fabs(dp) <= r) {
+    V3 pp = add(c, scale(n, -dp));
+    V3 v0 = sub(cc, a), v1 = sub(b, a), v2 = sub(pp, a);
+    double d00 = dot(v0, v0), d01 = dot(v0, v1), d02 = dot(v0, v2), d11 = dot(v1, v1), d12 = dot(v1, v2);
+    double den = d00 * d11 - d01 * d01;
+    if (den == 0) return false;
+    double u = (d11 * d02 - d01 * d12) / den, v = (d00 * d12 - d01 * d02) / den;
+    double wa = 1 - u - v, wb = v;
+    if (wa >= 0 && wb >= 0 && wa + wb <= 1) return true;
+  }
+  return false;
+}
+
+bool sphere_traverse(const Bvh& g, const NodeView& nv, int64_t n32, V3 c, double r, Counters& ctr) {
+  if (nv.is_leaf(n32)) {
+    for (int64_t i = nv.offset(n32); i < nv.offset(n32) + nv.count(n32); ++i) {
+      int64_t abc[3];
+      g.tri_vertices(g.resolve(i), abc);
+      ctr.tris++;
+      if (sphere_meets_triangle(c, r, g.vertex(abc[0]), g.vertex(abc[1]), g.vertex(abc[2]))) return true;
+    }
+    return false;
+  }
+  const int64_t kids[2] = {nv.left(n32), nv.right(n32)};
+  for (int64_t k : kids) {
+    ctr.nodes++;
+    if (box_score(nv, k, c) <= r * r && sphere_traverse(g, nv, k, c, r, ctr)) return true;
+  }
+  return false;
+}
+
 template <class F>
 void parallel_for(int64_t n, int threads, F f) {
   if (threads <= 1 || n < 64) { f(0, n); return; }
@@ -980,6 +1040,31 @@ void orc_closest_point(const orc_bvh* h, const float* pts, int64_t n, double min
       Counters c;
       V3 p{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
       closest_point(h->b, p, min_t, max_t, &out[i], c);
+      if (node_reads) node_reads[i] = c.nodes;
+      if (tri_tests) tri_tests[i] = c.tris;
+    }
+  });
+}
+
+// intersectsSphere for n spheres (cx, cy, cz, r as float32); out[i] = 1 if the mesh meets sphere i.
+// The roots are tried in order (BVH.js:396-411); a root that is a leaf is tested without a box.
+void orc_intersects_sphere(const orc_bvh* h, const float* spheres, int64_t n, uint8_t* out, int64_t* node_reads,
+                           int64_t* tri_tests, int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      Counters c;
+      V3 p{spheres[4 * i], spheres[4 * i + 1], spheres[4 * i + 2]};
+      double r = spheres[4 * i + 3];
+      bool hit = false;
+      for (const auto& root : h->b.roots) {
+        NodeView nv{root.data()};
+        c.nodes++;
+        if (sphere_traverse(h->b, nv, 0, p, r, c)) {
+          hit = true;
+          break;
+        }
+      }
+      out[i] = hit ? 1 : 0;
       if (node_reads) node_reads[i] = c.nodes;
       if (tri_tests) tri_tests[i] = c.tris;
     }

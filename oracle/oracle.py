@@ -66,6 +66,7 @@ def lib():
         L.orc_point_triangle_distance.restype = D
         L.orc_point_triangle_distance.argtypes = [P, P, P, P]
         L.orc_refit.argtypes = [P, P, I64, I]
+        L.orc_intersects_sphere.argtypes = [P, P, I64, P, P, P, I]
         _lib = L
     return _lib
 
@@ -127,6 +128,16 @@ class OracleBVH:
         sd = np.asarray(sides, dtype=np.int32)
         self._mat = (g, sd)
         lib().orc_set_materials(self.h, _p(g) if g.size else None, len(groups), _p(sd) if sd.size else None, sd.size)
+
+    def intersects_sphere(self, spheres, threads=None, counters=False):
+        """MeshBVH#intersectsSphere for each row (cx, cy, cz, radius) -> bool array."""
+        sp = np.ascontiguousarray(spheres, dtype=np.float32).reshape(-1, 4)
+        n = sp.shape[0]
+        out = np.empty(n, dtype=np.uint8)
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_intersects_sphere(self.h, _p(sp), n, _p(out), _p(nn), _p(nt), threads or _threads())
+        return (out.astype(bool), nn, nt) if counters else out.astype(bool)
 
     def refit(self, position):
         """MeshBVH#refit() after the vertex positions changed to `position` (n x 3 float32)."""

@@ -1,0 +1,49 @@
+"""GPU intersectsSphere (bvhc_intersects_sphere) against the oracle, and the reference's known
+answers (test/ShapeCasts.test.js:565-604) through the MeshBVH mirror."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_intersects_sphere_known_answers_gpu(pkg, cuda):
+    geo = pkg.sphere(1, 50, 50)
+    bvh = pkg.MeshBVH(geo, {"verbose": False})
+    assert bvh.intersectsSphere(((0, 1, 0), 0.01)) is True
+    assert bvh.intersectsSphere(((0, 0, 0), 0.9)) is False
+    assert bvh.intersectsSphere(((0, 2.01, 0), 0.9)) is False
+
+
+@pytest.mark.parametrize("indirect", [False, True])
+def test_intersects_sphere_matches_oracle(pkg, orc, cuda, indirect):
+    import torch
+
+    geo = pkg.torus_knot(10, 3, 300, 60, noise_sigma=0.02, noise_seed=3)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "indirect": indirect})
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+    rng = np.random.default_rng(17)
+    lo, hi = geo.position.min(0) - 4, geo.position.max(0) + 4
+    n = 200_000
+    c = lo + rng.random((n, 3)) * (hi - lo)
+    r = np.exp(rng.uniform(np.log(0.01), np.log(6.0), n))
+    spheres = np.concatenate([c, r[:, None]], 1).astype(np.float32)
+    # spheres that just touch a vertex (the boundary): the GPU must not miss a touching triangle
+    v = geo.position[rng.choice(geo.position.shape[0], 2000, replace=False)]
+    touch = np.concatenate([v + np.float32(0.5), np.full((2000, 1), np.float32(0.5 * np.sqrt(3) + 1e-3))], 1)
+    spheres = np.concatenate([spheres, touch.astype(np.float32)])
+    exp = ref.intersects_sphere(spheres)
+    got = bvh.intersects_sphere_batch(spheres)
+    dev = bvh.intersects_sphere_batch(torch.from_numpy(spheres).to(cuda)).cpu().numpy().astype(bool)
+    bvh.synchronize()
+    assert np.array_equal(got, dev)
+    bad = np.nonzero(got != exp)[0]
+    # a disagreement is allowed only on the boundary: the nearest triangle within 1e-6 relative of r
+    tri = geo.position[geo.index.astype(np.int64).reshape(-1, 3)].astype(np.float64)
+    for i in bad[:50]:
+        p = spheres[i, :3].astype(np.float64)
+        rad = float(spheres[i, 3])
+        cp = ref.closest_point(spheres[i:i + 1, :3])
+        d = float(cp["distance"][0])
+        assert abs(d - rad) <= 1e-6 * max(rad, 1.0), (i, d, rad, got[i], exp[i])
+    assert bad.size <= 5, bad.size
+    assert 0.05 < exp.mean() < 0.95

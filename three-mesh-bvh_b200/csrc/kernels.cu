@@ -904,6 +904,78 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   if (valid) cp_store(m, p, b, out + i);
 }
 
+// ---------------------------------------------------------------------------------------------
+// intersectsSphere (MeshBVH.js:796-809 through shapecast.js:41-214), one sphere per thread.  A
+// child is entered when its box may meet the sphere (box score against r^2 with 2^-20 relative
+// slack, a superset of the reference's `<=`), and a triangle meets the sphere when its closest
+// point lies within r (sphereIntersectTriangle, MathUtilities.js:167-201, is that predicate
+// evaluated through the edges and the plane): decided on the float32 squared distance with its
+// error bound, else in float-float.  The answer, whether any triangle meets the sphere, does not
+// depend on the visiting order; the first triangle found ends the query.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool sphere_meets(float3 c, ff r2, const Tri& t) {
+  float3 q;
+  float sc;
+  float d2 = closest_sq_f(c, t.a, t.b, t.c, q, sc);
+  float e = 32.0f * kU * sc;
+  float err = 3.5f * e * sqrtf(d2) + 3.0f * e * e;
+  const float kR = 1.1920928955078125e-07f;  // 2^-23: r2.hi against the exact r^2
+  if (d2 + err < r2.hi * (1.0f - kR)) return true;
+  if (d2 - err > r2.hi * (1.0f + kR)) return false;
+  return !ff_lt(r2, closest_ff(c, t.a, t.b, t.c).d2);
+}
+
+__global__ void __launch_bounds__(kBlock) intersects_sphere_kernel(MeshDev m, const float* __restrict__ spheres,
+                                                                   uint64_t n, uint8_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 sph = ld4(spheres + 4 * i);
+  const float3 c = make_float3(sph.x, sph.y, sph.z);
+  const ff r2 = two_prod(sph.w, sph.w);
+  const float lim = r2.hi * (1.0f + kSlabMargin);
+  bool hit = false;
+  uint32_t stack[kMaxStack];
+  for (int root = 0; root < m.n_roots && !hit; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) {
+          for (uint32_t k = link & ~kLeafBit;; ++k) {
+            Tri t = load_tri(m.tris, k);
+            if (sphere_meets(c, r2, t)) {
+              hit = true;
+              break;
+            }
+            if (t.flags & kTriLast) break;
+          }
+          if (hit) break;
+        }
+      } else {
+        Pair pr = load_pair(m.nodes, link);
+        bool w0 = box_score(pr.l, c) * (1.0f - kSlabMargin) <= lim;
+        bool w1 = box_score(pr.r, c) * (1.0f - kSlabMargin) <= lim;
+        if (w0 && w1) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            break;
+          }
+          stack[sp++] = pr.lr;
+          link = pr.ll;
+          continue;
+        }
+        if (w0 || w1) {
+          link = w0 ? pr.ll : pr.lr;
+          continue;
+        }
+      }
+      if (sp == 0) break;
+      link = stack[--sp];
+    }
+  }
+  out[i] = hit ? 1 : 0;
+}
+
 // Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
 // queue length; the queue is then sorted by key so that a warp takes 32 nearby points.
 __global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n, SceneBox box,
@@ -1376,6 +1448,13 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                 : occupancy == 1 ? dev::closest_point_packet_kernel<6>
                                  : dev::closest_point_packet_kernel<8>;
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
+                                     cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::intersects_sphere_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, out);
   return cudaGetLastError();
 }
 

@@ -101,6 +101,11 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
                                  const RaySort* sort = nullptr);
 
+// intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
+// sphere i.
+cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
+                                     cudaStream_t stream);
+
 // Refit (refit.cu).  A box "slot" is where a node's box lives on the device: 2 * pair + side for a
 // child box in a child-pair record, or kRootSlot | root for a root's own box (kept in root_box).
 constexpr uint32_t kRootSlot = 0x80000000u;

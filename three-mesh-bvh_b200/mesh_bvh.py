@@ -438,3 +438,28 @@ class MeshBVH:
         target.distance = float(rec["distance"])
         target.faceIndex = int(rec["face_index"])
         return target
+
+    def intersects_sphere_batch(self, spheres, stream=None):
+        """intersectsSphere for every row (cx, cy, cz, radius) of `spheres`: numpy -> bool array;
+        torch CUDA tensor (n x 4, float32) -> uint8 tensor, enqueued on `stream`."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(spheres):
+            import torch
+            sp = spheres.contiguous()
+            out = torch.empty(sp.shape[0], dtype=torch.uint8, device=sp.device)
+            s = stream if stream is not None else torch.cuda.current_stream(sp.device).cuda_stream
+            N.check(lib.bvhc_intersects_sphere(mesh, sp.data_ptr(), sp.shape[0], out.data_ptr(), N.MEM_DEVICE, s),
+                    "bvhc_intersects_sphere")
+            return out
+        sp = np.ascontiguousarray(spheres, dtype=np.float32).reshape(-1, 4)
+        out = np.empty(sp.shape[0], dtype=np.uint8)
+        N.check(lib.bvhc_intersects_sphere(mesh, _ptr(sp), sp.shape[0], _ptr(out), N.MEM_HOST, None),
+                "bvhc_intersects_sphere")
+        return out.astype(bool)
+
+    def intersectsSphere(self, sphere) -> bool:
+        """MeshBVH#intersectsSphere (MeshBVH.js:796-809); sphere: (center, radius) or an object
+        with `center` and `radius`."""
+        center, radius = (sphere.center, sphere.radius) if hasattr(sphere, "center") else sphere
+        row = np.array([[*center, radius]], dtype=np.float32)
+        return bool(self.intersects_sphere_batch(row)[0])
