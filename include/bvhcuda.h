@@ -289,6 +289,16 @@ bvhc_status bvhc_closest_point_backward(bvhc_mesh* mesh, const float* points, co
                                         const float* grad_distance, float* grad_vertices, float* grad_points,
                                         void* stream);
 
+/* Intersection attribute fields (src/utils/ThreeRayIntersectUtilities.js:59-117): for every hit,
+ * a vertex attribute (`item_size` 1..4 floats per vertex, `stride_floats` apart, n_verts >= the
+ * mesh's vertex count) interpolated at the hit point with the hit's barycoord
+ * (Triangle.getInterpolation) — uv, uv1, normal or any other attribute.  With `rays` given (the
+ * hits' rays, n x 6) a 3-component result pointing along its ray is negated, as the reference does
+ * for `normal`.  out: n x item_size floats; misses give zeros. */
+bvhc_status bvhc_hit_interpolate(bvhc_mesh* mesh, const bvhc_hit* hits, uint64_t n, const float* attribute,
+                                 uint64_t n_verts, int item_size, int stride_floats, const float* rays, float* out,
+                                 int mem, void* stream);
+
 /* MeshBVH#intersectsSphere(sphere) for every sphere (src/core/MeshBVH.js:796-809: shapecast with
  * the sphere/box and sphere/triangle tests, src/math/MathUtilities.js:167-201).  spheres: n x 4
  * float32 (centre xyz, radius; device buffers 16-byte aligned); out[i] = 1 when some triangle lies

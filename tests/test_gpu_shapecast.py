@@ -1,5 +1,6 @@
 """GPU intersectsSphere (bvhc_intersects_sphere) against the oracle, and the reference's known
-answers (test/ShapeCasts.test.js:565-604) through the MeshBVH mirror."""
+answers (test/ShapeCasts.test.js:565-604) through the MeshBVH mirror; Intersection attribute
+fields (uv, normal) interpolated at the hits (bvhc_hit_interpolate)."""
 import numpy as np
 import pytest
 
@@ -47,3 +48,35 @@ def test_intersects_sphere_matches_oracle(pkg, orc, cuda, indirect):
         assert abs(d - rad) <= 1e-6 * max(rad, 1.0), (i, d, rad, got[i], exp[i])
     assert bad.size <= 5, bad.size
     assert 0.05 < exp.mean() < 0.95
+
+
+def test_hit_attribute_interpolation(pkg, cuda):
+    """uv and normal at the hit point (ThreeRayIntersectUtilities.js:59-117): the barycentric
+    combination of the hit triangle's vertex attributes, the normal turned against the ray."""
+    import torch
+
+    geo = pkg.torus_knot(10, 3, 200, 40)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    rays = np.concatenate([pkg.rays_camera(96, 96), pkg.rays_sphere_to_box(5000, seed=2)])
+    hits = bvh.raycast_first_batch(rays, 2)                 # double sided: back faces too
+    hit = hits["face_index"] != 0xFFFFFFFF
+    assert hit.sum() > 2000
+    tri = geo.index.astype(np.int64).reshape(-1, 3)[np.where(hit, hits["face_index"], 0)]
+    w = hits["barycoord"].astype(np.float64)[..., None]
+    exp_uv = (w * geo.uv[tri].astype(np.float64)).sum(1)
+    exp_n = (w * geo.normal[tri].astype(np.float64)).sum(1)
+    flip = (exp_n * rays[:, 3:]).sum(1) > 0
+    exp_n[flip] *= -1
+    uv = bvh.hit_interpolate(hits, geo.uv)
+    nrm = bvh.hit_interpolate(hits, geo.normal, rays)
+    assert np.abs(uv[hit] - exp_uv[hit]).max() <= 1e-5
+    assert np.abs(nrm[hit] - exp_n[hit]).max() <= 1e-5
+    assert not uv[~hit].any() and not nrm[~hit].any()
+    d_hits = bvh.raycast_first_batch(torch.from_numpy(rays).to(cuda), 2)
+    d_uv = bvh.hit_interpolate(d_hits, torch.from_numpy(geo.uv).to(cuda))
+    bvh.synchronize()
+    assert np.array_equal(d_uv.cpu().numpy(), uv)
+    first = bvh.raycastFirst((rays[0, :3], rays[0, 3:]), 2)
+    if first is not None:
+        assert first.uv is not None and first.normal is not None
+        assert float(np.dot(first.normal, rays[0, 3:])) <= 0

@@ -575,6 +575,15 @@ static cudaError_t install_quads(bvhc_mesh* m, const std::vector<PairNode>& pair
   return cudaSuccess;
 }
 
+// 3 vertex ids per triangle on the device, from the geometry index (or 3t + k without one).
+static cudaError_t ensure_tri_vid(bvhc_mesh* m) {
+  if (m->d_tri_vid) return cudaSuccess;
+  uint64_t n_tri = m->h_index.empty() ? m->n_verts_geo / 3 : m->h_index.size() / 3;
+  std::vector<uint32_t> vid(3 * n_tri);
+  for (uint64_t i = 0; i < vid.size(); ++i) vid[i] = m->h_index.empty() ? (uint32_t)i : m->h_index[i];
+  return upload(&m->d_tri_vid, vid);
+}
+
 static void free_refit_plan(RefitPlan& p) {
   cudaFree(p.leaves);
   cudaFree(p.parent);
@@ -1090,12 +1099,7 @@ bvhc_status bvhc_mesh_refit(bvhc_mesh* m, const float* positions, uint64_t n_ver
   if (n_verts < m->n_verts_geo || m->h_root_bytes.empty()) return BVHC_ERR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
-  if (!m->d_tri_vid) {  // 3 vertex ids per triangle, from the geometry index (or 3t + k)
-    uint64_t n_tri = m->h_index.empty() ? m->n_verts_geo / 3 : m->h_index.size() / 3;
-    std::vector<uint32_t> vid(3 * n_tri);
-    for (uint64_t i = 0; i < vid.size(); ++i) vid[i] = m->h_index.empty() ? (uint32_t)i : m->h_index[i];
-    BVHC_CUDA_TRY(upload(&m->d_tri_vid, vid));
-  }
+  BVHC_CUDA_TRY(ensure_tri_vid(m));
   if (!m->refit[0].leaves)
     BVHC_CUDA_TRY(build_refit_plan(m->h_pairs, m->h_tris, m->h_roots, serialized_root_boxes(m), m->refit[0]));
   const float* pos = positions;
@@ -1303,6 +1307,39 @@ bvhc_status bvhc_mesh_set_groups(bvhc_mesh* m, const int64_t* groups, int n_grou
                                cudaMemcpyHostToDevice));
   }
   return BVHC_OK;
+}
+
+bvhc_status bvhc_hit_interpolate(bvhc_mesh* m, const bvhc_hit* hits, uint64_t n, const float* attribute,
+                                 uint64_t n_verts, int item_size, int stride_floats, const float* rays, float* out,
+                                 int mem, void* stream) {
+  if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE) || item_size < 1 || item_size > 4 ||
+      stride_floats < item_size || n_verts < m->n_verts_geo)
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!hits || !attribute || !out) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  BVHC_CUDA_TRY(ensure_tri_vid(m));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(hits, 4) || !aligned(attribute, 4) || !aligned(out, 4) || (rays && !aligned(rays, 4)))
+      return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_hit_interpolate(hits, n, m->d_tri_vid, attribute, item_size, stride_floats, rays, out, s));
+  }
+  // host memory: hits, rays and the attribute go through one staging buffer, the result another
+  const size_t hb = n * sizeof(bvhc_hit), rb = rays ? n * 24 : 0;
+  const size_t ab = n_verts * (size_t)stride_floats * sizeof(float), ob = n * item_size * sizeof(float);
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, hb + rb + ab));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, ob));
+  char* base = static_cast<char*>(m->d_in);
+  BVHC_CUDA_TRY(cudaMemcpyAsync(base, hits, hb, cudaMemcpyHostToDevice, s));
+  if (rays) BVHC_CUDA_TRY(cudaMemcpyAsync(base + hb, rays, rb, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(base + hb + rb, attribute, ab, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_hit_interpolate(reinterpret_cast<const bvhc_hit*>(base), n, m->d_tri_vid,
+                                       reinterpret_cast<const float*>(base + hb + rb), item_size, stride_floats,
+                                       rays ? reinterpret_cast<const float*>(base + hb) : nullptr,
+                                       static_cast<float*>(m->d_out), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, ob, cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
 }
 
 bvhc_status bvhc_intersects_sphere(bvhc_mesh* m, const float* spheres, uint64_t n, uint8_t* out, int mem,

@@ -1451,6 +1451,47 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
   return cudaGetLastError();
 }
 
+namespace dev {
+
+// Intersection attribute fields (ThreeRayIntersectUtilities.js:59-117): a vertex attribute at the
+// hit point, Triangle.getInterpolation with the recorded barycentrics; with rays given (normals),
+// the result is negated when it points along the ray.  Misses give zeros.
+__global__ void __launch_bounds__(kBlock) hit_interpolate_kernel(const bvhc_hit* __restrict__ hits, uint64_t n,
+                                                                 const uint32_t* __restrict__ tri_vid,
+                                                                 const float* __restrict__ attr, int item_size,
+                                                                 int stride, const float* __restrict__ rays,
+                                                                 float* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bvhc_hit h = hits[i];
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  if (h.face_index != BVHC_NO_HIT) {
+    for (int k = 0; k < 3; ++k) {
+      const float* a = attr + (uint64_t)__ldg(tri_vid + 3 * (uint64_t)h.face_index + k) * stride;
+      for (int c = 0; c < item_size; ++c) v[c] += h.barycoord[k] * __ldg(a + c);
+    }
+    if (rays && item_size == 3) {
+      const float* r = rays + 6 * i;
+      if (v[0] * r[3] + v[1] * r[4] + v[2] * r[5] > 0.0f) {
+        v[0] = -v[0];
+        v[1] = -v[1];
+        v[2] = -v[2];
+      }
+    }
+  }
+  for (int c = 0; c < item_size; ++c) out[i * item_size + c] = v[c];
+}
+
+}  // namespace dev
+
+cudaError_t launch_hit_interpolate(const bvhc_hit* hits, uint64_t n, const uint32_t* tri_vid, const float* attr,
+                                   int item_size, int stride, const float* rays, float* out, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::hit_interpolate_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(hits, n, tri_vid, attr, item_size, stride,
+                                                                       rays, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
                                      cudaStream_t stream) {
   if (n == 0) return cudaSuccess;

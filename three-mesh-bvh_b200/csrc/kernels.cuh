@@ -106,6 +106,12 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
                                      cudaStream_t stream);
 
+// Vertex attribute at each hit (barycentric interpolation over the hit triangle's vertices, via
+// tri_vid: 3 vertex ids per triangle); rays (nullable, item_size 3) flip results that point along
+// the ray.  out: n x item_size.
+cudaError_t launch_hit_interpolate(const bvhc_hit* hits, uint64_t n, const uint32_t* tri_vid, const float* attr,
+                                   int item_size, int stride, const float* rays, float* out, cudaStream_t stream);
+
 // Refit (refit.cu).  A box "slot" is where a node's box lives on the device: 2 * pair + side for a
 // child box in a child-pair record, or kRootSlot | root for a root's own box (kept in root_box).
 constexpr uint32_t kRootSlot = 0x80000000u;

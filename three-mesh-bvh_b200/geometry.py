@@ -24,9 +24,17 @@ class Geometry:
     index: np.ndarray | None = None           # uint16 / uint32, length multiple of 3
     groups: list = field(default_factory=list)  # [(start, count, materialIndex)] in index units
     draw_range: tuple = (0, math.inf)         # (start, count) in index units
+    # optional vertex attributes reported on hits (Intersection.normal / uv / uv1)
+    normal: np.ndarray | None = None          # (n_verts, 3) float32
+    uv: np.ndarray | None = None              # (n_verts, 2) float32
+    uv1: np.ndarray | None = None             # (n_verts, 2) float32
 
     def __post_init__(self):
         self.position = np.ascontiguousarray(self.position, dtype=np.float32).reshape(-1, 3)
+        for name, k in (("normal", 3), ("uv", 2), ("uv1", 2)):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.float32).reshape(-1, k))
         if self.index is not None:
             self.index = np.ascontiguousarray(self.index)
             if self.index.dtype not in (np.uint16, np.uint32):
@@ -41,8 +49,9 @@ class Geometry:
         self.groups.append((int(start), count, int(material_index)))
 
     def clone(self) -> "Geometry":
-        return Geometry(self.position.copy(), None if self.index is None else self.index.copy(), list(self.groups),
-                        self.draw_range)
+        cp = (lambda a: None if a is None else a.copy())
+        return Geometry(self.position.copy(), cp(self.index), list(self.groups), self.draw_range, cp(self.normal),
+                        cp(self.uv), cp(self.uv1))
 
     def triangle(self, face_index: int) -> np.ndarray:
         """Vertices (3, 3) float64 of triangle `face_index` (through the index when present)."""
@@ -103,7 +112,10 @@ def torus_knot(radius=1.0, tube=0.4, tubular_segments=64, radial_segments=8, p=2
     if np.dot(nrm, normal.reshape(-1, 3)[tri[0]]) < 0:
         index = index.reshape(-1, 3)[:, [0, 2, 1]].reshape(-1)
     n_verts = pos.shape[0] * pos.shape[1]
-    return Geometry(p0.astype(np.float32), index.astype(index_dtype(n_verts)))
+    uv = np.stack(np.meshgrid(np.arange(tubular_segments + 1) / tubular_segments,
+                              np.arange(radial_segments + 1) / radial_segments, indexing="ij"), -1)
+    return Geometry(p0.astype(np.float32), index.astype(index_dtype(n_verts)),
+                    normal=normal.reshape(-1, 3).astype(np.float32), uv=uv.reshape(-1, 2).astype(np.float32))
 
 
 def torus(radius=1.0, tube=0.4, radial_segments=12, tubular_segments=48) -> Geometry:

@@ -45,6 +45,11 @@ class Intersection:
     face: Face
     faceIndex: int
     barycoord: np.ndarray
+    # vertex attributes at the hit point (ThreeRayIntersectUtilities.js:59-117), when the geometry
+    # has them; `normal` faces against the ray
+    uv: np.ndarray | None = None
+    uv1: np.ndarray | None = None
+    normal: np.ndarray | None = None
 
 
 @dataclass
@@ -395,7 +400,7 @@ class MeshBVH:
                 return int(mi)
         return 0
 
-    def _intersection(self, rec, materials=False) -> Intersection:
+    def _intersection(self, rec, materials=False, direction=None) -> Intersection:
         f = int(rec["face_index"])
         tri = self.geometry.triangle(f)
         base = 3 * f
@@ -406,9 +411,18 @@ class MeshBVH:
         n = np.cross(tri[2] - tri[1], tri[0] - tri[1])       # Triangle.getNormal
         ln = float(np.dot(n, n))
         n = n / math.sqrt(ln) if ln > 0 else np.zeros(3)
+        bary = np.array(rec["barycoord"], dtype=np.float64)
+        g = self.geometry
+
+        def interp(attr):                                     # Triangle.getInterpolation
+            return None if attr is None else bary @ attr[[a, b, c]].astype(np.float64)
+
+        normal = interp(g.normal)
+        if normal is not None and direction is not None and float(np.dot(normal, direction)) > 0:
+            normal = -normal
         return Intersection(distance=float(rec["distance"]), point=np.array(rec["point"], dtype=np.float64),
                             face=Face(a, b, c, n, self._material_index(f) if materials else 0), faceIndex=f,
-                            barycoord=np.array(rec["barycoord"], dtype=np.float64))
+                            barycoord=bary, uv=interp(g.uv), uv1=interp(g.uv1), normal=normal)
 
     @staticmethod
     def _ray_row(ray) -> np.ndarray:
@@ -420,13 +434,15 @@ class MeshBVH:
         rec = self.raycast_first_batch(self._ray_row(ray), materialOrSide, near, far)[0]
         if int(rec["face_index"]) == N.NO_HIT:
             return None
-        return self._intersection(rec, isinstance(materialOrSide, (list, tuple)))
+        mats = isinstance(materialOrSide, (list, tuple))
+        return self._intersection(rec, mats, np.asarray(ray[1], dtype=np.float64))
 
     def raycast(self, ray, materialOrSide=FrontSide, near=0.0, far=math.inf, cap=1024):
         """All hits of one ray, unsorted (DFS order), as a list of Intersection."""
         counts, hits = self.raycast_batch(self._ray_row(ray), materialOrSide, near, far, cap=cap)
         mats = isinstance(materialOrSide, (list, tuple))
-        return [self._intersection(hits[0, k], mats) for k in range(min(int(counts[0]), cap))]
+        d = np.asarray(ray[1], dtype=np.float64)
+        return [self._intersection(hits[0, k], mats, d) for k in range(min(int(counts[0]), cap))]
 
     def closestPointToPoint(self, point, target: HitPointInfo | None = None, minThreshold=0.0,
                             maxThreshold=math.inf):
@@ -438,6 +454,34 @@ class MeshBVH:
         target.distance = float(rec["distance"])
         target.faceIndex = int(rec["face_index"])
         return target
+
+    def hit_interpolate(self, hits, attribute, rays=None, stream=None):
+        """A vertex attribute (n_verts x k, k <= 4) at every hit of raycast_first_batch's records
+        (Intersection.uv / uv1 / normal in batch form, bvhc_hit_interpolate); with `rays`, a
+        3-component result pointing along its ray is negated (the reference's normal).  torch CUDA
+        tensors -> (n, k) tensor enqueued on `stream`; numpy -> (n, k) array."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(hits):
+            import torch
+            attr = attribute.contiguous()
+            n, k = hits.shape[0], attr.shape[1]
+            out = torch.empty((n, k), dtype=torch.float32, device=hits.device)
+            s = stream if stream is not None else torch.cuda.current_stream(hits.device).cuda_stream
+            N.check(lib.bvhc_hit_interpolate(mesh, hits.data_ptr(), n, attr.data_ptr(), attr.shape[0], k, k,
+                                             rays.data_ptr() if rays is not None else None, out.data_ptr(),
+                                             N.MEM_DEVICE, s), "bvhc_hit_interpolate")
+            return out
+        h = np.ascontiguousarray(hits).view(np.uint8).reshape(-1)
+        n = h.size // 32
+        attr = np.ascontiguousarray(attribute, dtype=np.float32)
+        attr = attr.reshape(attr.shape[0], -1)
+        k = attr.shape[1]
+        r = None if rays is None else np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        out = np.empty((n, k), dtype=np.float32)
+        N.check(lib.bvhc_hit_interpolate(mesh, _ptr(h), n, _ptr(attr), attr.shape[0], k, k,
+                                         _ptr(r) if r is not None else None, _ptr(out), N.MEM_HOST, None),
+                "bvhc_hit_interpolate")
+        return out
 
     def intersects_sphere_batch(self, spheres, stream=None):
         """intersectsSphere for every row (cx, cy, cz, radius) of `spheres`: numpy -> bool array;
