@@ -584,7 +584,9 @@ def run_all_hits(args, ws, rank, local):
     counts = torch.empty(n_max, dtype=torch.int32, device=dev)
     hits = torch.empty((n_max, cap, 8), dtype=torch.float32, device=dev)   # 32 B per hit slot
     lib = pkg.lib()
-    per_set_ms, stored = [], []
+    per_set_ms, stored, variants = [], [], {}
+    bvh.set_traversal(1, 1, 16, 2)   # register budget shared with the warp-cooperative kernels
+    cur = bvh.get_traversal()
     with ClockSampler(local) as clk:
         for name, r in sets:
             d = torch.from_numpy(r).to(dev)
@@ -594,6 +596,20 @@ def run_all_hits(args, ws, rank, local):
                 check(lib.bvhc_raycast(bvh._device_mesh(), d.data_ptr(), n, 0, 0.0, math.inf, cap,
                                        counts.data_ptr(), hits.data_ptr(), 1, stream.cuda_stream), "bvhc_raycast")
 
+            # the all-hits kernel variant for this set (one call each, on the same buffers)
+            t_var = {}
+            for v in (0, 1, 2):
+                bvh.set_traversal(**{**cur, "all": v})
+                call()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                call()
+                e1.record(stream)
+                e1.synchronize()
+                t_var[v] = e0.elapsed_time(e1)
+            best = min(t_var, key=t_var.get)
+            bvh.set_traversal(**{**cur, "all": best})
+            variants[name] = {"best": best, "timings_ms": {str(k): x for k, x in t_var.items()}}
             for _ in range(args.warmup):
                 call()
             torch.cuda.synchronize(dev)
@@ -631,7 +647,8 @@ def run_all_hits(args, ws, rank, local):
         k = max(range(len(sets)), key=lambda j: per_set_ms[j])
         achieved = bytes_per_set[k] / (per_set_ms[k] / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_source": how, "kernel": "raycast_all_kernel", "ray_set": sets[k][0],
+                "traffic": None, "peak_source": how, "ray_set": sets[k][0],
+                "kernel": "raycast_all_kernel" if variants[sets[k][0]]["best"] == 0 else "raycast_all_packet_kernel",
                 "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], bytes_per_set))}
     if rank == 0:
         line = {"metric": "Mrays/s raycast all hits (2M tri, cap 64)", "value": weak_scaling_rate(ws, n_step, 1, ms),
@@ -641,7 +658,8 @@ def run_all_hits(args, ws, rank, local):
                 "config": {"workload": WORKLOAD.replace("raycastFirst", "raycast (all hits, cap 64)"),
                            "rays_per_step": n_step, "stored_hits": dict(zip([n for n, _ in sets], stored))},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
-                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": 2 * args.steps}
+                "all_hits_variant": variants, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": args.steps * sum(15 if v["best"] == 2 else 1 for v in variants.values())}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 

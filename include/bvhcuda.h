@@ -141,8 +141,11 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * leaves).  closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32
  * queries of a warp through one shared traversal (for spatially coherent queries such as grids),
  * 2 the same over the queries sorted by a Morton key of the point; 1 and 2 apply with
- * minThreshold 0 (otherwise 0 runs), and use the occupancy setting too.  Results are the same for
- * every variant (up to exact ties); the autotuner picks the fastest per mesh and workload. */
+ * minThreshold 0 (otherwise 0 runs), and use the occupancy setting too.  all selects raycast's
+ * (all hits) kernel: 0 one ray per thread, 1 the rays of a warp through one shared left-first
+ * traversal (each ray's hits stay in the reference's DFS order), 2 the same over the rays sorted by
+ * the cube-map direction key.  Results are the same for every variant (up to exact ties); the
+ * autotuner picks the fastest per mesh and workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;
   int32_t order;
@@ -152,6 +155,7 @@ typedef struct bvhc_traversal_config {
   int32_t sort;
   int32_t closest;
   int32_t wide;
+  int32_t all;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);

@@ -223,7 +223,7 @@ def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occ
     ref = _oracle_for(orc, bvh, geo)
     bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
-                                       compact=compact, sort=sort, closest=0, wide=0)
+                                       compact=compact, sort=sort, closest=0, wide=0, all=0)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):

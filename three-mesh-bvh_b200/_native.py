@@ -28,7 +28,7 @@ class BvhcClosest(C.Structure):
 class BvhcTraversalConfig(C.Structure):
     _fields_ = [("persistent", C.c_int32), ("order", C.c_int32), ("refill", C.c_int32), ("occupancy", C.c_int32),
                 ("compact", C.c_int32), ("sort", C.c_int32), ("closest", C.c_int32),
-                ("wide", C.c_int32)]
+                ("wide", C.c_int32), ("all", C.c_int32)]
 
 
 class BvhcMeshInfo(C.Structure):

@@ -74,6 +74,33 @@ def tune_raycast_first(bvh, rays, side: int = 0, near: float = 0.0, far: float =
     return entry
 
 
+def tune_raycast_all(bvh, rays, cap: int = 64, reps: int = 3, candidates=(0, 1, 2)) -> dict:
+    """Time raycast's (all hits) kernels (the `all` field: per ray, warp-cooperative,
+    warp-cooperative over direction-sorted rays) on `rays` (torch CUDA tensor, n x 6), keeping the
+    mesh's other traversal fields, and install the fastest."""
+    import torch
+
+    cur = bvh.get_traversal()
+    stream = torch.cuda.current_stream(rays.device)
+    out = (torch.empty(rays.shape[0], dtype=torch.int32, device=rays.device),
+           torch.empty((rays.shape[0], cap, 8), dtype=torch.float32, device=rays.device))
+    timings = {}
+    for c in candidates:
+        bvh.set_traversal(**{**cur, "all": c})
+        bvh.raycast_batch(rays, cap=cap, stream=stream.cuda_stream, out=out)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(reps):
+            bvh.raycast_batch(rays, cap=cap, stream=stream.cuda_stream, out=out)
+        end.record(stream)
+        end.synchronize()
+        timings[c] = start.elapsed_time(end) / reps
+    bvh.synchronize(stream.cuda_stream)
+    best = min(candidates, key=lambda c: timings[c])
+    bvh.set_traversal(**{**cur, "all": best})
+    return {"best": best, "timings_ms": {str(k): v for k, v in timings.items()}}
+
+
 def tune_closest_point(bvh, points, min_t: float = 0.0, max_t: float = math.inf, reps: int = 3,
                        candidates=(0, 1, 2)) -> dict:
     """Time closestPointToPoint's kernels (the `closest` field: per query, warp-cooperative,

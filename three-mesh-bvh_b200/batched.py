@@ -76,8 +76,9 @@ class BatchedMeshBVH:
             self._mesh = out
         return self._mesh
 
-    def set_traversal(self, persistent=1, order=1, refill=16, occupancy=0, compact=0, sort=0, closest=0, wide=0):
-        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide)
+    def set_traversal(self, persistent=1, order=1, refill=16, occupancy=0, compact=0, sort=0, closest=0, wide=0,
+                      all=0):
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide, all)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     @staticmethod

@@ -26,7 +26,7 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
@@ -45,8 +45,8 @@ struct bvhc_mesh {
   void* slot_out[2] = {nullptr, nullptr};
   unsigned long long* d_work2 = nullptr;
   // work queues (grow-only): [0] direct raycastFirst calls, [1], [2] the two pipeline slots (so
-  // that concurrently running chunks never share a queue), [3] closestPointToPoint
-  static constexpr int kSlots = 4;
+  // that concurrently running chunks never share a queue), [3] closestPointToPoint, [4] raycast
+  static constexpr int kSlots = 5;
   uint32_t* d_queue[kSlots] = {};
   size_t queue_cap[kSlots] = {};
   unsigned int* d_qcount[kSlots] = {};
@@ -1024,13 +1024,13 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1);
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 2;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
   m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill,  cfg->occupancy,
-                           cfg->compact,    cfg->sort,  cfg->closest, cfg->wide};
+                           cfg->compact,    cfg->sort,  cfg->closest, cfg->wide,     cfg->all};
   return BVHC_OK;
 }
 
@@ -1167,6 +1167,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->sort = m->cfg.sort;
   cfg->closest = m->cfg.closest;
   cfg->wide = m->cfg.wide;
+  cfg->all = m->cfg.all;
   return BVHC_OK;
 }
 
@@ -1224,16 +1225,38 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   if (!rays || !counts || (cap > 0 && !hits)) return BVHC_ERR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
-  if (mem == BVHC_MEM_DEVICE) {
-    if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s));
+  if (mem == BVHC_MEM_DEVICE && (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  // the warp-cooperative variant over sorted rays uses queue slot 4 and its sort scratch
+  const int variant = m->cfg.all;
+  uint32_t* q = nullptr;
+  unsigned int* qc = nullptr;
+  RaySort sort{};
+  const int slot = 4;
+  if (variant == 2 && n < (1ull << 32)) {
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
+    if (!m->d_qcount[slot])
+      BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
+    BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
+    q = m->d_queue[slot];
+    qc = m->d_qcount[slot];
+    sort.kind = 1;
+    for (int a = 0; a < 3; ++a) {
+      sort.lo[a] = m->scene_lo[a];
+      sort.hi[a] = m->scene_hi[a];
+    }
+    sort.scratch = m->sort_s[slot];
   }
+  if (mem == BVHC_MEM_DEVICE)
+    return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s, variant,
+                                        m->cfg.occupancy, q, qc, q ? &sort : nullptr));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
-                                   static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s));
+                                   static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s, variant,
+                                   m->cfg.occupancy, q, qc, q ? &sort : nullptr));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));

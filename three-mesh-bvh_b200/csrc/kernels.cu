@@ -600,6 +600,114 @@ __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const fl
 }
 
 // ---------------------------------------------------------------------------------------------
+// raycast (all hits), warp-cooperative: the 32 rays of a warp walk the tree together, left child
+// before right child as the reference does, entering a child when any lane's ray enters its box
+// (one shared stack of links; there is no early out, so no per-lane distances).  A lane that tests
+// the triangles of a leaf its own traversal would not have reached finds no hit there (a ray that
+// hits a triangle enters every box on its path), so each lane reports exactly its own hits, in its
+// own DFS order.  With a queue (rays sorted by a Morton key), a warp takes 32 consecutive entries.
+// ---------------------------------------------------------------------------------------------
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
+    MeshDev m, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides, float near_d,
+    float far_d, uint32_t cap, uint32_t* __restrict__ counts, bvhc_hit* __restrict__ hits,
+    const uint32_t* __restrict__ queue) {
+  __shared__ uint32_t s_link[kWarps][kMaxStack];
+  const unsigned full = 0xFFFFFFFFu;
+  const int w = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n) return;  // block-uniform
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = i < n;
+  if (valid && queue) i = __ldg(queue + i);
+  RayF r;
+  if (valid) {
+    r = make_ray(rays, i);
+  } else {
+    r.o = make_float3(0.f, 0.f, 0.f);
+    r.d = make_float3(1.f, 0.f, 0.f);
+    r.inv = make_float3(1.f, 1e30f, 1e30f);
+    r.d_l1 = 1.f;
+  }
+  const ff dlen = dir_length(r.d);
+  uint32_t cnt = 0;
+  bvhc_hit* out = hits + i * (uint64_t)cap;
+  bool overflow = false;
+  for (int root = 0; root < m.n_roots && !overflow; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      bool pop = false;
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf && valid) {
+          for (uint32_t k = link & ~kLeafBit;; ++k) {
+            Tri t = load_tri(m.tris, k);
+            int ts = tri_side(t, side, sides);
+            if (ts >= 0 && tri_hit(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts)) {
+              ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+              ff dist = ff_mul(tt, dlen);
+              if (!ff_lt(dist, ff_from(near_d)) && !ff_lt(ff_from(far_d), dist)) {
+                if (cnt < cap) {
+                  bvhc_hit h;
+                  make_hit(t, r, tt, dist, h);
+                  store_hit(out + cnt, h);
+                }
+                ++cnt;
+              }
+            }
+            if (t.flags & kTriLast) break;
+          }
+        }
+        pop = true;
+      } else {
+        Pair p = load_pair(m.nodes, link);
+        float e0, e1;
+        bool h0 = valid && box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e0);
+        bool h1 = valid && box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e1);
+        unsigned b0 = __ballot_sync(full, h0), b1 = __ballot_sync(full, h1);
+        if (b0 && b1) {
+          if (sp >= kMaxStack) {
+            if (lane == 0) atomicOr(m.err, kErrStackOverflow);
+            overflow = true;
+            break;
+          }
+          if (lane == 0) s_link[w][sp] = p.lr;
+          ++sp;
+          link = p.ll;
+          __syncwarp();
+        } else if (b0) {
+          link = p.ll;
+        } else if (b1) {
+          link = p.lr;
+        } else {
+          pop = true;
+        }
+      }
+      if (pop) {
+        if (sp == 0) break;
+        link = s_link[w][--sp];
+      }
+    }
+  }
+  if (valid) counts[i] = cnt;
+}
+
+// Morton key of every ray (raykey.cuh, kind `kind`), ids in input order, and the queue length:
+// the ordering pass of the warp-cooperative all-hits raycast (no ray is finished early there).
+__global__ void __launch_bounds__(kBlock) ray_key_all_kernel(const float* __restrict__ rays, uint64_t n, int kind,
+                                                            SceneBox box, uint32_t* __restrict__ ids,
+                                                            uint32_t* __restrict__ keys,
+                                                            unsigned int* __restrict__ qcount) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *qcount = (unsigned int)n;
+  if (i >= n) return;
+  const float* r = rays + 6 * i;
+  ids[i] = (uint32_t)i;
+  keys[i] = ray_key(kind, make_float3(__ldg(r), __ldg(r + 1), __ldg(r + 2)),
+                    make_float3(__ldg(r + 3), __ldg(r + 4), __ldg(r + 5)), box);
+}
+
+// ---------------------------------------------------------------------------------------------
 // closestPointToPoint (closestPointToPoint.js:6-78 through shapecast.js:41-214).
 // At an internal node both child scores (squared distance from the point to the box) are
 // computed; the lower-scoring child is visited first (left on ties), and a child is entered
@@ -1412,10 +1520,33 @@ cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n
 
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, int variant, int occupancy, uint32_t* queue, unsigned int* qcount,
+                               const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts,
-                                                                    hits);
+  if (variant == 0 || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
+    dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap,
+                                                                      counts, hits);
+    return cudaGetLastError();
+  }
+  cudaError_t e;
+  if (variant == 2) {
+    uint32_t *ids, *keys;
+    ray_sort_input(sort->kind, sort->scratch, queue, &ids, &keys);
+    dev::SceneBox box{};
+    for (int a = 0; a < 3; ++a) {
+      box.lo[a] = sort->lo[a];
+      box.hi[a] = sort->hi[a];
+    }
+    dev::ray_key_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(rays, n, sort->kind, box, ids, keys, qcount);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
+  } else {
+    queue = nullptr;
+  }
+  auto kernel = occupancy == 0   ? dev::raycast_all_packet_kernel<1>
+                : occupancy == 1 ? dev::raycast_all_packet_kernel<6>
+                                 : dev::raycast_all_packet_kernel<8>;
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts, hits, queue);
   return cudaGetLastError();
 }
 

@@ -27,9 +27,6 @@ struct MeshDev {
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                  float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
-cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
-                               float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
-                               cudaStream_t stream);
 // Traversal variant chosen per call (autotuned): persistent vs one-ray-per-thread grid, child
 // order, and the number of idle lanes that triggers a warp refill.
 struct TraversalConfig {
@@ -44,6 +41,8 @@ struct TraversalConfig {
   int closest;     // closestPointToPoint: 0 one query per thread, 1 warp-cooperative, 2 warp-cooperative
                    // over Morton-sorted queries (1 and 2 only with minThreshold 0)
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
+  int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2 warp-cooperative
+                   // over rays sorted by the cube-map direction key
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -100,6 +99,14 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  bvhc_closest* out, cudaStream_t stream, int variant = 0, int occupancy = 0,
                                  uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
                                  const RaySort* sort = nullptr);
+
+// raycast (all hits).  variant 0: one ray per thread; 1: warp-cooperative in input order; 2:
+// warp-cooperative over the rays sorted by the key sort->kind (queue, qcount and sort scratch for
+// n rays required, else variant 0 runs).
+cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
+                               float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
+                               cudaStream_t stream, int variant = 0, int occupancy = 0, uint32_t* queue = nullptr,
+                               unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 
 // intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
 // sphere i.

@@ -206,9 +206,9 @@ class MeshBVH:
         return {k: getattr(info, k) for k, _ in N.BvhcMeshInfo._fields_}
 
     def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0,
-                      compact: int = 0, sort: int = 0, closest: int = 0, wide: int = 0) -> None:
+                      compact: int = 0, sort: int = 0, closest: int = 0, wide: int = 0, all: int = 0) -> None:
         """Select the traversal variants (see bvhc_mesh_set_traversal)."""
-        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide)
+        cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide, all)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     def get_traversal(self) -> dict:
@@ -294,14 +294,18 @@ class MeshBVH:
                                        _ptr(res), N.MEM_HOST, None), "bvhc_raycast_first")
         return res
 
-    def raycast_batch(self, rays, side=FrontSide, near=0.0, far=math.inf, cap=64, stream=None):
-        """All hits for every ray: (counts[n] uncapped, hits[n, cap]) in the reference's DFS order."""
+    def raycast_batch(self, rays, side=FrontSide, near=0.0, far=math.inf, cap=64, stream=None, out=None):
+        """All hits for every ray: (counts[n] uncapped, hits[n, cap]) in the reference's DFS order.
+        out: optional (counts, hits) torch tensors to fill (device calls)."""
         lib, mesh = N.lib(), self._device_mesh()
         if self._is_torch(rays):
             import torch
             n = rays.shape[0]
-            counts = torch.empty(n, dtype=torch.int32, device=rays.device)
-            hits = torch.empty((n, cap, 8), dtype=torch.float32, device=rays.device)
+            if out is not None:
+                counts, hits = out
+            else:
+                counts = torch.empty(n, dtype=torch.int32, device=rays.device)
+                hits = torch.empty((n, cap, 8), dtype=torch.float32, device=rays.device)
             s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
             N.check(lib.bvhc_raycast(mesh, rays.data_ptr(), n, _side_of(side), float(near), float(far), cap,
                                      counts.data_ptr(), hits.data_ptr(), N.MEM_DEVICE, s), "bvhc_raycast")
