@@ -611,14 +611,15 @@ template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
     MeshDev m, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides, float near_d,
     float far_d, uint32_t cap, uint32_t* __restrict__ counts, bvhc_hit* __restrict__ hits,
-    const uint32_t* __restrict__ queue) {
+    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
   __shared__ uint32_t s_link[kWarps][kMaxStack];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
-  if ((uint64_t)blockIdx.x * blockDim.x >= n) return;  // block-uniform
+  const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
+  if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = i < n;
+  const bool valid = i < n_work;
   if (valid && queue) i = __ldg(queue + i);
   RayF r;
   if (valid) {
@@ -692,20 +693,6 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
   if (valid) counts[i] = cnt;
 }
 
-// Morton key of every ray (raykey.cuh, kind `kind`), ids in input order, and the queue length:
-// the ordering pass of the warp-cooperative all-hits raycast (no ray is finished early there).
-__global__ void __launch_bounds__(kBlock) ray_key_all_kernel(const float* __restrict__ rays, uint64_t n, int kind,
-                                                            SceneBox box, uint32_t* __restrict__ ids,
-                                                            uint32_t* __restrict__ keys,
-                                                            unsigned int* __restrict__ qcount) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *qcount = (unsigned int)n;
-  if (i >= n) return;
-  const float* r = rays + 6 * i;
-  ids[i] = (uint32_t)i;
-  keys[i] = ray_key(kind, make_float3(__ldg(r), __ldg(r + 1), __ldg(r + 2)),
-                    make_float3(__ldg(r + 3), __ldg(r + 4), __ldg(r + 5)), box);
-}
 
 // ---------------------------------------------------------------------------------------------
 // closestPointToPoint (closestPointToPoint.js:6-78 through shapecast.js:41-214).
@@ -1289,7 +1276,8 @@ __global__ void __launch_bounds__(kBlock) finalize_first_kernel(MeshDev m, const
 // is finished here with a coalesced miss record.  The other rays are appended to `queue` in ray
 // order (one atomic per block reserves the block's run; positions within it come from ballots), so
 // the traversal kernel's warps only carry rays that enter the tree.  With `keys`, each queued ray's
-// ordering key (raykey.cuh, kind `kind`) is written beside its id.
+// ordering key (raykey.cuh, kind `kind`) is written beside its id.  With `miss_counts` (all-hits
+// raycast) a ray that misses gets a hit count of 0 instead of a miss record.
 constexpr int kClsThreads = 256;
 constexpr int kClsItems = 8;
 constexpr int kClsTile = kClsThreads * kClsItems;  // rays per block
@@ -1299,7 +1287,7 @@ template <bool BATCHED>
 __global__ void __launch_bounds__(kClsThreads) classify_kernel(
     MeshDev m, const BatchDev bd, const float* __restrict__ rays, uint64_t n, float near_d, float far_d,
     bvhc_hit* __restrict__ out, uint32_t* __restrict__ queue, unsigned int* __restrict__ qcount,
-    uint32_t* __restrict__ keys, int kind, SceneBox box) {
+    uint32_t* __restrict__ keys, int kind, SceneBox box, uint32_t* __restrict__ miss_counts = nullptr) {
   __shared__ unsigned s_cnt[kClsItems * kClsWarps];  // live rays per (item round, warp), then prefixes
   __shared__ unsigned s_base;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
@@ -1330,7 +1318,10 @@ __global__ void __launch_bounds__(kClsThreads) classify_kernel(
         live = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, far_d, e) ||
                box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, far_d, e);
       }
-      if (!live) store_miss(out + i);
+      if (!live) {
+        if (miss_counts) miss_counts[i] = 0;  // all hits: the uncapped count of a ray that misses
+        else store_miss(out + i);
+      }
       else if (keys) key[j] = ray_key(kind, r.o, r.d, box);
     }
     ballot[j] = __ballot_sync(0xFFFFFFFFu, live);
@@ -1530,6 +1521,8 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
   }
   cudaError_t e;
   if (variant == 2) {
+    // the root-box pre-pass gives the rays that miss a count of 0 and queues the others with their
+    // keys, which are then sorted
     uint32_t *ids, *keys;
     ray_sort_input(sort->kind, sort->scratch, queue, &ids, &keys);
     dev::SceneBox box{};
@@ -1537,16 +1530,22 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
       box.lo[a] = sort->lo[a];
       box.hi[a] = sort->hi[a];
     }
-    dev::ray_key_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(rays, n, sort->kind, box, ids, keys, qcount);
+    if ((e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    const unsigned int g = (unsigned int)((n + dev::kClsTile - 1) / dev::kClsTile);
+    dev::classify_kernel<false><<<g, dev::kClsThreads, 0, stream>>>(m, BatchDev{nullptr, nullptr, 0}, rays, n, near_d,
+                                                                    far_d, nullptr, ids, qcount, keys, sort->kind, box,
+                                                                    counts);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
   } else {
     queue = nullptr;
+    qcount = nullptr;
   }
   auto kernel = occupancy == 0   ? dev::raycast_all_packet_kernel<1>
                 : occupancy == 1 ? dev::raycast_all_packet_kernel<6>
                                  : dev::raycast_all_packet_kernel<8>;
-  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts, hits, queue);
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts, hits, queue,
+                                                  qcount);
   return cudaGetLastError();
 }
 
