@@ -1,6 +1,7 @@
 """raycast (all hits) kernel variants against the oracle: the counts, and each ray's stored hits
 in the reference's order (left child before right child), for one ray per thread, the
-warp-cooperative form, and the warp-cooperative form over rays sorted by the direction key."""
+warp-cooperative form, and the warp-cooperative form over rays sorted by each ray key (direction,
+entry point, entry point and direction)."""
 import math
 
 import numpy as np
@@ -9,7 +10,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("variant,occupancy", [(0, 0), (1, 0), (1, 2), (2, 2)])
+@pytest.mark.parametrize("variant,occupancy", [(0, 0), (1, 0), (1, 2), (2, 2), (3, 2), (4, 0)])
 def test_all_hits_variants_keep_reference_order(pkg, orc, cuda, variant, occupancy):
     import torch
 

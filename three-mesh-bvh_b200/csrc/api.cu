@@ -1024,7 +1024,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 2;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 4;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
@@ -1227,8 +1227,9 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE && (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))))
     return BVHC_ERR_INVALID_ARGUMENT;
-  // the warp-cooperative variant over sorted rays uses queue slot 4 and its sort scratch
-  const int variant = m->cfg.all;
+  // the warp-cooperative variants over sorted rays (all = 2..4: key kind all - 1) use queue slot 4
+  // and its sort scratch
+  const int variant = m->cfg.all >= 2 ? 2 : m->cfg.all;
   uint32_t* q = nullptr;
   unsigned int* qc = nullptr;
   RaySort sort{};
@@ -1240,7 +1241,7 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
     BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
     q = m->d_queue[slot];
     qc = m->d_qcount[slot];
-    sort.kind = 1;
+    sort.kind = m->cfg.all - 1;
     for (int a = 0; a < 3; ++a) {
       sort.lo[a] = m->scene_lo[a];
       sort.hi[a] = m->scene_hi[a];

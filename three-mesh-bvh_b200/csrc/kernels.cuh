@@ -41,8 +41,8 @@ struct TraversalConfig {
   int closest;     // closestPointToPoint: 0 one query per thread, 1 warp-cooperative, 2 warp-cooperative
                    // over Morton-sorted queries (1 and 2 only with minThreshold 0)
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
-  int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2 warp-cooperative
-                   // over rays sorted by the cube-map direction key
+  int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2..4 warp-cooperative
+                   // over the rays that enter the tree, sorted by key kind all - 1
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
