@@ -103,6 +103,15 @@ bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floa
                        int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
                        int64_t range_start, int64_t range_count, int strategy, int max_depth,
                        int target_leaf_size, int indirect, bvhc_serialized** out);
+/* The same build on GPU `device`, enqueued on `stream` (a cudaStream_t; NULL = the default stream)
+ * and waited for before returning.  Same arguments and the same serialized bytes (roots and the
+ * reordered index / indirect buffer) as bvhc_build, for BVHC_SAH and BVHC_CENTER; BVHC_AVERAGE
+ * (a sequential double sum per node) returns BVHC_ERR_UNSUPPORTED.  Split decisions are made
+ * with the reference's binary64 rounding, computed in integer arithmetic on the device. */
+bvhc_status bvhc_build_device(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                              int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                              int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                              int target_leaf_size, int indirect, int device, void* stream, bvhc_serialized** out);
 int bvhc_serialized_root_count(const bvhc_serialized* s);
 bvhc_status bvhc_serialized_root(const bvhc_serialized* s, int i, const void** data, uint64_t* bytes);
 /* elem_bytes is 0 when there is no index / no indirect buffer. */

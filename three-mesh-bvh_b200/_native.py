@@ -41,6 +41,7 @@ _P, _U64, _I64, _I, _F = C.c_void_p, C.c_uint64, C.c_int64, C.c_int, C.c_float
 SIGNATURES = [
     ("bvhc_status_string", C.c_char_p, [_I]),
     ("bvhc_build", _I, [_P, _U64, _I, _P, _I, _U64, _P, _I, _I64, _I64, _I, _I, _I, _I, C.POINTER(_P)]),
+    ("bvhc_build_device", _I, [_P, _U64, _I, _P, _I, _U64, _P, _I, _I64, _I64, _I, _I, _I, _I, _I, _P, C.POINTER(_P)]),
     ("bvhc_serialized_root_count", _I, [_P]),
     ("bvhc_serialized_root", _I, [_P, _I, C.POINTER(_P), C.POINTER(_U64)]),
     ("bvhc_serialized_index", _I, [_P, C.POINTER(_P), C.POINTER(_I), C.POINTER(_U64)]),

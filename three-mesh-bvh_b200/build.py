@@ -13,7 +13,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 LIB = PKG / "libbvhcuda.so"
 SOURCES = [PKG / "csrc" / "api.cu", PKG / "csrc" / "kernels.cu", PKG / "csrc" / "adjoint.cu", PKG / "csrc" / "noalloc.cu",
-           PKG / "csrc" / "raysort.cu", PKG / "csrc" / "refit.cu", PKG / "csrc" / "builder.cpp"]
+           PKG / "csrc" / "raysort.cu", PKG / "csrc" / "refit.cu", PKG / "csrc" / "gpubuild.cu",
+           PKG / "csrc" / "builder.cpp"]
 HEADERS = [ROOT / "include" / "bvhcuda.h"] + sorted((PKG / "csrc").glob("*.h")) + sorted((PKG / "csrc").glob("*.cuh"))
 
 NVCC_FLAGS = [

@@ -665,14 +665,16 @@ const char* bvhc_status_string(bvhc_status s) {
   return "unknown status";
 }
 
-bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
-                       int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
-                       int64_t range_start, int64_t range_count, int strategy, int max_depth, int target_leaf_size,
-                       int indirect, bvhc_serialized** out) {
+static bvhc_status build_impl(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                              int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                              int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                              int target_leaf_size, int indirect, bool on_device, int device, void* stream,
+                              bvhc_serialized** out) {
   if (!out || !positions || stride_floats < 3 || n_verts == 0) return BVHC_ERR_INVALID_ARGUMENT;
   if (index && index_elem_bytes != 2 && index_elem_bytes != 4) return BVHC_ERR_INVALID_ARGUMENT;
   if (strategy < BVHC_CENTER || strategy > BVHC_SAH || max_depth < 0 || target_leaf_size < 0) return BVHC_ERR_INVALID_ARGUMENT;
   if (n_groups > 0 && !groups) return BVHC_ERR_INVALID_ARGUMENT;
+  if (on_device && strategy == BVHC_AVERAGE) return BVHC_ERR_UNSUPPORTED;
   *out = nullptr;
   try {
     auto* s = new bvhc_serialized();
@@ -686,11 +688,18 @@ bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floa
       }
     }
     try {
-      build_serialized(*s, positions, n_verts, stride_floats, groups, n_groups, range_start, range_count, strategy,
-                       max_depth, target_leaf_size, indirect != 0);
+      if (on_device)
+        build_serialized_device(*s, positions, n_verts, stride_floats, groups, n_groups, range_start, range_count,
+                                strategy, max_depth, target_leaf_size, indirect != 0, device, stream);
+      else
+        build_serialized(*s, positions, n_verts, stride_floats, groups, n_groups, range_start, range_count, strategy,
+                         max_depth, target_leaf_size, indirect != 0);
     } catch (const std::bad_alloc&) {
       delete s;
       return BVHC_ERR_OUT_OF_MEMORY;
+    } catch (const DeviceBuildError&) {
+      delete s;
+      return BVHC_ERR_CUDA;
     } catch (...) {
       delete s;
       return BVHC_ERR_BUILD;
@@ -702,6 +711,23 @@ bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floa
   } catch (const std::bad_alloc&) {
     return BVHC_ERR_OUT_OF_MEMORY;
   }
+}
+
+bvhc_status bvhc_build(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                       int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                       int64_t range_start, int64_t range_count, int strategy, int max_depth, int target_leaf_size,
+                       int indirect, bvhc_serialized** out) {
+  return build_impl(positions, n_verts, stride_floats, index, index_elem_bytes, index_count, groups, n_groups,
+                    range_start, range_count, strategy, max_depth, target_leaf_size, indirect, false, 0, nullptr, out);
+}
+
+bvhc_status bvhc_build_device(const float* positions, uint64_t n_verts, int stride_floats, const void* index,
+                              int index_elem_bytes, uint64_t index_count, const int64_t* groups, int n_groups,
+                              int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                              int target_leaf_size, int indirect, int device, void* stream, bvhc_serialized** out) {
+  return build_impl(positions, n_verts, stride_floats, index, index_elem_bytes, index_count, groups, n_groups,
+                    range_start, range_count, strategy, max_depth, target_leaf_size, indirect, true, device, stream,
+                    out);
 }
 
 int bvhc_serialized_root_count(const bvhc_serialized* s) { return s ? (int)s->roots.size() : 0; }

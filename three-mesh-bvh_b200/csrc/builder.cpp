@@ -342,9 +342,8 @@ std::vector<Range> root_ranges(int64_t vertex_count, int64_t draw_start, int64_t
   return out;
 }
 
-void build_serialized(Serialized& s, const float* pos, uint64_t n_verts, int stride, const int64_t* groups,
-                      int n_groups, int64_t range_start, int64_t range_count, int strategy, int max_depth,
-                      int leaf, bool indirect) {
+std::vector<Range> prepare_build(Serialized& s, uint64_t n_verts, const int64_t* groups, int n_groups,
+                                 int64_t range_start, int64_t range_count, bool indirect) {
   std::vector<Range> ranges;
   if (indirect) {
     // generateIndirectBuffer (GeometryBVH.js:9-37)
@@ -367,6 +366,13 @@ void build_serialized(Serialized& s, const float* pos, uint64_t n_verts, int str
     ranges = root_ranges((int64_t)s.index.size(), range_start, range_count, groups, n_groups);
   }
   if (ranges.empty()) throw std::runtime_error("geometry has no triangles in its draw range / groups");
+  return ranges;
+}
+
+void build_serialized(Serialized& s, const float* pos, uint64_t n_verts, int stride, const int64_t* groups,
+                      int n_groups, int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                      int leaf, bool indirect) {
+  std::vector<Range> ranges = prepare_build(s, n_verts, groups, n_groups, range_start, range_count, indirect);
   Builder b(s, pos, stride, strategy, max_depth, leaf);
   b.run(ranges);
 }

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <stdexcept>
 #include <vector>
 
 #include "bvhcuda.h"
@@ -32,8 +33,23 @@ struct Range {
 std::vector<Range> root_ranges(int64_t vertex_count, int64_t draw_start, int64_t draw_count, const int64_t* groups,
                                int n_groups);
 
+// generateIndirectBuffer / ensureIndex (GeometryBVH.js:9-37, geometryUtils.js:15-47) on `s`, and
+// the root primitive ranges to build over.
+std::vector<Range> prepare_build(Serialized& s, uint64_t n_verts, const int64_t* groups, int n_groups,
+                                 int64_t range_start, int64_t range_count, bool indirect);
+
 void build_serialized(Serialized& s, const float* pos, uint64_t n_verts, int stride, const int64_t* groups,
                       int n_groups, int64_t range_start, int64_t range_count, int strategy, int max_depth,
                       int leaf, bool indirect);
+
+// A CUDA runtime failure inside the device build.
+struct DeviceBuildError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// The same build on a GPU (gpubuild.cu), byte-identical output; SAH and CENTER only.
+void build_serialized_device(Serialized& s, const float* pos, uint64_t n_verts, int stride, const int64_t* groups,
+                             int n_groups, int64_t range_start, int64_t range_count, int strategy, int max_depth,
+                             int leaf, bool indirect, int device, void* stream);
 
 }  // namespace bvhc

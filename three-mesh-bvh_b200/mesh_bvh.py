@@ -109,12 +109,18 @@ class MeshBVH:
         groups = np.array([[s, -1 if (isinstance(c, float) and math.isinf(c)) else int(c)] for s, c, *_ in g.groups],
                           dtype=np.int64).reshape(-1)
         out = C.c_void_p()
-        st = lib.bvhc_build(_ptr(pos), pos.shape[0], 3, _ptr(idx) if idx is not None else None,
-                            idx.dtype.itemsize if idx is not None else 0, idx.size if idx is not None else 0,
-                            _ptr(groups) if groups.size else None, len(g.groups), int(start), count,
-                            int(opts["strategy"]), int(opts["maxDepth"]), int(opts["targetLeafSize"]),
-                            1 if opts.get("indirect") else 0, C.byref(out))
-        N.check(st, "bvhc_build")
+        args = (_ptr(pos), pos.shape[0], 3, _ptr(idx) if idx is not None else None,
+                idx.dtype.itemsize if idx is not None else 0, idx.size if idx is not None else 0,
+                _ptr(groups) if groups.size else None, len(g.groups), int(start), count,
+                int(opts["strategy"]), int(opts["maxDepth"]), int(opts["targetLeafSize"]),
+                1 if opts.get("indirect") else 0)
+        if opts.get("deviceBuild"):
+            # the same tree built on the GPU (SAH / CENTER), byte-identical serialized output
+            st = lib.bvhc_build_device(*args, int(self.device), None, C.byref(out))
+            N.check(st, "bvhc_build_device")
+        else:
+            st = lib.bvhc_build(*args, C.byref(out))
+            N.check(st, "bvhc_build")
         try:
             self._adopt_serialized(out)
         finally:
