@@ -127,16 +127,14 @@ __device__ float area_f(const float* lo, const float* hi, bool& ok) {
 
 // Bin index `~~((c - left) / width)` clamped to 31 (splitUtils.js:199-204).
 struct AxisBin {
-  float l, lenf;
-  f64 L, W;
+  float l, r, lenf;
   bool fast;
 };
 __device__ AxisBin axis_bin(float l, float r) {
   AxisBin ab;
   ab.l = l;
+  ab.r = r;
   ab.lenf = __fsub_rn(r, l);
-  ab.L = sf::from_f32(l);
-  ab.W = sf::mul(sf::sub(sf::from_f32(r), ab.L), kInvBinsD);
   ab.fast = ab.lenf >= 0x1p-90f && ab.lenf <= 0x1p120f;
   return ab;
 }
@@ -150,7 +148,9 @@ __device__ int bin_of(float c, const AxisBin& ab) {
     const float t = truncf(q);
     if ((t == 0.0f || q - t > kBinEps) && (t + 1.0f) - q > kBinEps) return (int)t;
   }
-  const int b = sf::to_i32_trunc(sf::div(sf::sub(sf::from_f32(c), ab.L), ab.W));
+  const f64 left = sf::from_f32(ab.l);
+  const f64 width = sf::mul(sf::sub(sf::from_f32(ab.r), left), kInvBinsD);
+  const int b = sf::to_i32_trunc(sf::div(sf::sub(sf::from_f32(c), left), width));
   return b >= kBins ? kBins - 1 : (b < 0 ? 0 : b);
 }
 
@@ -759,59 +759,45 @@ __device__ void warp_bounds(const float* C, const float* L, const float* H, int6
   }
 }
 
-struct SubRoot {
-  uint32_t node, off, cnt, depth, temp_base, stack_base, stack_cap, pad;
-};
-struct StackEnt {
-  uint32_t off, cnt, depth;
-  int32_t parent;
+// A node of the small-node phase.  Nodes of one level occupy a contiguous id range (children are
+// allocated in pairs by the level that splits their parent); the small roots are ids [0, n_roots).
+struct SmallNode {
   float box[6], cbox[6];
+  uint32_t off, cnt, depth;
+  int32_t left;   // first child id (the right child is left + 1); -1 for a leaf
+  int32_t axis;
+  uint32_t size;  // nodes in the subtree
+  uint32_t dest;  // pre-order slot in the output
+  uint32_t pad;
 };
 
-// One warp per subtree of at most kSmall primitives: the reference's splitNode recursion depth
-// first, records in local pre-order at temp[temp_base ...]; sizes[k] = the subtree's node count.
-__global__ void __launch_bounds__(kSubWarps * 32) k_subtree(const SubRoot* __restrict__ roots, int n_roots,
-                                                            const float* __restrict__ nbox, float* C, float* L,
-                                                            float* H, uint32_t* perm, int64_t n, uint32_t* partner,
-                                                            uint32_t* temp, uint32_t* sizes, StackEnt* stack,
-                                                            int strategy, int max_depth, int leaf, uint32_t base,
-                                                            unsigned int* err) {
+// One warp per node of level [lv[level], lv[level + 1]): the reference's splitNode step (leaf
+// test, split choice, Hoare partition, child bounds); children are appended for the next level.
+__global__ void __launch_bounds__(kSubWarps * 32, 8) k_small_level(SmallNode* nodes, const uint32_t* __restrict__ lv,
+                                                                   int level, unsigned int* counter, float* C, float* L,
+                                                                   float* H, uint32_t* perm, int64_t n,
+                                                                   uint32_t* partner, int strategy, int max_depth,
+                                                                   int leaf) {
   __shared__ uint32_t s_bins[kSubWarps][kNodeBinWords];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int wid = blockIdx.x * kSubWarps + wib;
-  if (wid >= n_roots) return;
   uint32_t* bins = s_bins[wib];
-  const SubRoot r = roots[wid];
-  StackEnt* st = stack + r.stack_base;
-  uint32_t* out = temp + (size_t)r.temp_base * 8;
-  if (lane == 0) {
-    StackEnt e0;
-    e0.off = r.off;
-    e0.cnt = r.cnt;
-    e0.depth = r.depth;
-    e0.parent = -1;
+  const uint32_t first = lv[level], last = lv[level + 1];
+  const uint32_t n_warps = gridDim.x * kSubWarps;
+  for (uint32_t id = first + blockIdx.x * kSubWarps + wib; id < last; id += n_warps) {
+    SmallNode* nd = nodes + id;
+    const uint32_t off = nd->off, cnt = nd->cnt, depth = nd->depth;
+    float box[6], cbox[6];
+#pragma unroll
     for (int k = 0; k < 6; ++k) {
-      e0.box[k] = nbox[r.node * 12 + k];
-      e0.cbox[k] = nbox[r.node * 12 + 6 + k];
+      box[k] = nd->box[k];
+      cbox[k] = nd->cbox[k];
     }
-    st[0] = e0;
-  }
-  __syncwarp();
-  uint32_t sp = 1, next = 0;
-  while (sp > 0) {
-    --sp;
-    const StackEnt ent = st[sp];
-    __syncwarp();
-    const uint32_t idx = next++;
-    uint32_t* rec = out + (size_t)idx * 8;
-    if (lane < 6) rec[lane] = __float_as_uint(ent.box[lane]);
-    if (lane == 0 && ent.parent >= 0) out[(size_t)ent.parent * 8 + 6] = idx - (uint32_t)ent.parent;
-    bool leaf_node = ent.cnt <= (uint32_t)leaf || (int)ent.depth >= max_depth;
+    bool leaf_node = cnt <= (uint32_t)leaf || (int)depth >= max_depth;
     Split s{-1, 0};
     uint32_t nl = 0;
     if (!leaf_node) {
-      if (strategy == kSah && ent.cnt < kBins / 4) {
-        if (lane == 0) s = sah_small(C, L, H, n, ent.off, ent.cnt, ent.box);
+      if (strategy == kSah && cnt < kBins / 4) {
+        if (lane == 0) s = sah_small(C, L, H, n, off, cnt, box);
         s.axis = __shfl_sync(kFull, s.axis, 0);
         s.pos = (f64)__shfl_sync(kFull, (long long)s.pos, 0);
       } else if (strategy == kSah) {
@@ -820,17 +806,21 @@ __global__ void __launch_bounds__(kSubWarps * 32) k_subtree(const SubRoot* __res
           bins[i] = w == 0 ? 0u : (w < 4 ? kEncPosInf : kEncNegInf);
         }
         AxisBin ab[3];
-        for (int a = 0; a < 3; ++a) ab[a] = axis_bin(ent.cbox[a], ent.cbox[a + 3]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ab[a] = axis_bin(cbox[a], cbox[a + 3]);
         __syncwarp();
-        for (uint32_t e = ent.off + lane; e < ent.off + ent.cnt; e += 32) {
+        for (uint32_t e = off + lane; e < off + cnt; e += 32) {
           float lo[3], hi[3];
+#pragma unroll
           for (int d = 0; d < 3; ++d) {
             lo[d] = L[d * n + e];
             hi[d] = H[d * n + e];
           }
+#pragma unroll
           for (int a = 0; a < 3; ++a) {
             uint32_t* b = bins + (a * kBins + bin_of(C[a * n + e], ab[a])) * kBinWords;
             atomicAdd(b, 1u);
+#pragma unroll
             for (int d = 0; d < 3; ++d) {
               atomicMin(b + 1 + d, fenc(lo[d]));
               atomicMax(b + 4 + d, fenc(hi[d]));
@@ -838,78 +828,134 @@ __global__ void __launch_bounds__(kSubWarps * 32) k_subtree(const SubRoot* __res
           }
         }
         __syncwarp();
-        s = warp_sah_binned(bins, ent.cnt, ent.box, ent.cbox);
+        s = warp_sah_binned(bins, cnt, box, cbox);
         __syncwarp();
       } else {
-        s = center_split(ent.cbox);
+        s = center_split(cbox);
       }
       if (s.axis >= 0) {
-        for (uint32_t k = 0; k < ent.cnt; k += 32) {
-          const uint32_t e = ent.off + k + lane;
-          nl += __popc(__ballot_sync(kFull, k + lane < ent.cnt && goes_left(C[s.axis * n + e], s.pos)));
+        for (uint32_t k = 0; k < cnt; k += 32) {
+          const uint32_t e = off + k + lane;
+          nl += __popc(__ballot_sync(kFull, k + lane < cnt && goes_left(C[s.axis * n + e], s.pos)));
         }
       }
-      leaf_node = s.axis < 0 || nl == 0 || nl == ent.cnt;
+      leaf_node = s.axis < 0 || nl == 0 || nl == cnt;
     }
     if (leaf_node) {
-      if (lane == 0) {
-        rec[6] = base + ent.off;
-        rec[7] = (ent.cnt & 0xFFFFu) | 0xFFFF0000u;
-      }
-      __syncwarp();
+      if (lane == 0) nd->left = -1;
       continue;
     }
-    if (lane == 0) rec[7] = (uint32_t)s.axis;
     // Hoare pairing: the k-th left-part primitive going right swaps with the k-th right-part
     // primitive (from the end) going left
-    const uint32_t end = ent.off + ent.cnt, nr = ent.cnt - nl;
+    const uint32_t end = off + cnt, nr = cnt - nl;
     uint32_t rank = 0;
     for (uint32_t k = 0; k < nr; k += 32) {
       const uint32_t e = end - 1 - (k + lane);
       const bool mis = k + lane < nr && goes_left(C[s.axis * n + e], s.pos);
       const unsigned bal = __ballot_sync(kFull, mis);
-      if (mis) partner[ent.off + rank + __popc(bal & ((1u << lane) - 1u))] = e;
+      if (mis) partner[off + rank + __popc(bal & ((1u << lane) - 1u))] = e;
       rank += __popc(bal);
     }
     __syncwarp();
     rank = 0;
     for (uint32_t k = 0; k < nl; k += 32) {
-      const uint32_t e = ent.off + k + lane;
+      const uint32_t e = off + k + lane;
       const bool mis = k + lane < nl && !goes_left(C[s.axis * n + e], s.pos);
       const unsigned bal = __ballot_sync(kFull, mis);
-      if (mis) swap_prims(C, L, H, perm, n, e, partner[ent.off + rank + __popc(bal & ((1u << lane) - 1u))]);
+      if (mis) swap_prims(C, L, H, perm, n, e, partner[off + rank + __popc(bal & ((1u << lane) - 1u))]);
       rank += __popc(bal);
     }
     __syncwarp();
-    StackEnt le, re;
-    warp_bounds(C, L, H, n, ent.off, nl, le.box, le.cbox);
-    warp_bounds(C, L, H, n, ent.off + nl, nr, re.box, re.cbox);
-    le.off = ent.off;
-    le.cnt = nl;
-    re.off = ent.off + nl;
-    re.cnt = nr;
-    le.depth = re.depth = ent.depth + 1;
-    le.parent = -1;  // the left child directly follows its parent in pre-order
-    re.parent = (int32_t)idx;
-    if (sp + 2 > r.stack_cap) {  // cannot happen: the stack holds one pending node per level
-      if (lane == 0) atomicOr(err, 1u);
-      break;
+    float lbox[6], lcbox[6], rbox[6], rcbox[6];
+    warp_bounds(C, L, H, n, off, nl, lbox, lcbox);
+    warp_bounds(C, L, H, n, off + nl, nr, rbox, rcbox);
+    uint32_t child = 0;
+    if (lane == 0) child = atomicAdd(counter, 2u);
+    child = __shfl_sync(kFull, child, 0);
+    if (lane < 2) {
+      SmallNode c;
+      for (int k = 0; k < 6; ++k) {
+        c.box[k] = lane == 0 ? lbox[k] : rbox[k];
+        c.cbox[k] = lane == 0 ? lcbox[k] : rcbox[k];
+      }
+      c.off = lane == 0 ? off : off + nl;
+      c.cnt = lane == 0 ? nl : nr;
+      c.depth = depth + 1;
+      c.left = -1;
+      c.axis = -1;
+      c.size = 0;
+      c.dest = 0;
+      c.pad = 0;
+      nodes[child + lane] = c;
     }
     if (lane == 0) {
-      st[sp] = re;
-      st[sp + 1] = le;
+      nd->left = (int32_t)child;
+      nd->axis = s.axis;
     }
-    __syncwarp();
-    sp += 2;
   }
-  if (lane == 0) sizes[wid] = next;
+}
+
+// The small roots' boxes from the large-node table.
+__global__ void k_small_boxes(const uint32_t* __restrict__ ids, int n_roots, const float* __restrict__ nbox,
+                              SmallNode* nodes) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_roots) return;
+  for (int k = 0; k < 6; ++k) {
+    nodes[i].box[k] = nbox[ids[i] * 12 + k];
+    nodes[i].cbox[k] = nbox[ids[i] * 12 + 6 + k];
+  }
+}
+
+// lv[level + 2] = the node count once level `level` has appended its children.
+__global__ void k_level_close(uint32_t* lv, int level, const unsigned int* counter) { lv[level + 2] = *counter; }
+
+// Subtree sizes, deepest level first.
+__global__ void k_sizes(SmallNode* nodes, const uint32_t* __restrict__ lv, int level) {
+  const uint32_t first = lv[level], last = lv[level + 1];
+  for (uint32_t id = first + blockIdx.x * blockDim.x + threadIdx.x; id < last; id += gridDim.x * blockDim.x) {
+    SmallNode* nd = nodes + id;
+    nd->size = nd->left < 0 ? 1u : 1u + nodes[nd->left].size + nodes[nd->left + 1].size;
+  }
+}
+
+__global__ void k_set_dest(SmallNode* nodes, const uint32_t* __restrict__ dest, int n_roots) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_roots) nodes[i].dest = dest[i];
+}
+
+// Pre-order slots, top level first: the left child follows its parent, the right child follows
+// the left subtree (buildUtils.js:35-92).
+__global__ void k_dests(SmallNode* nodes, const uint32_t* __restrict__ lv, int level) {
+  const uint32_t first = lv[level], last = lv[level + 1];
+  for (uint32_t id = first + blockIdx.x * blockDim.x + threadIdx.x; id < last; id += gridDim.x * blockDim.x) {
+    const SmallNode* nd = nodes + id;
+    if (nd->left < 0) continue;
+    nodes[nd->left].dest = nd->dest + 1;
+    nodes[nd->left + 1].dest = nd->dest + 1 + nodes[nd->left].size;
+  }
+}
+
+// The 32-byte records of every small-phase node (_populateBuffer, buildUtils.js:35-92).
+__global__ void k_write_small(const SmallNode* __restrict__ nodes, const unsigned int* __restrict__ counter,
+                              uint32_t base, uint32_t* out) {
+  const uint32_t total = *counter;
+  for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < total; id += gridDim.x * blockDim.x) {
+    const SmallNode& nd = nodes[id];
+    uint32_t* o = out + (size_t)nd.dest * 8;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) o[k] = __float_as_uint(nd.box[k]);
+    if (nd.left < 0) {
+      o[6] = base + nd.off;
+      o[7] = (nd.cnt & 0xFFFFu) | 0xFFFF0000u;
+    } else {
+      o[6] = 1u + nodes[nd.left].size;
+      o[7] = (uint32_t)nd.axis;
+    }
+  }
 }
 
 struct PlaceRec {
   uint32_t node, dest, w6, w7;
-};
-struct SubCopy {
-  uint32_t src, count, dest, pad;
 };
 
 __global__ void k_place(const PlaceRec* __restrict__ recs, int n_recs, const float* __restrict__ nbox, uint32_t* out) {
@@ -920,11 +966,6 @@ __global__ void k_place(const PlaceRec* __restrict__ recs, int n_recs, const flo
   for (int k = 0; k < 6; ++k) o[k] = __float_as_uint(nbox[r.node * 12 + k]);
   o[6] = r.w6;
   o[7] = r.w7;
-}
-
-__global__ void k_copy_subtrees(const SubCopy* __restrict__ copies, const uint32_t* __restrict__ temp, uint32_t* out) {
-  const SubCopy c = copies[blockIdx.x];
-  for (uint32_t w = threadIdx.x; w < c.count * 8; w += blockDim.x) out[(size_t)c.dest * 8 + w] = temp[(size_t)c.src * 8 + w];
 }
 
 __global__ void k_reorder(const uint32_t* __restrict__ perm, const uint32_t* __restrict__ in, uint32_t* out, int64_t n,
@@ -976,7 +1017,6 @@ class DeviceBuilder {
     n_ = ranges.back().offset + ranges.back().count - base_;
     if (n_ < 0 || n_ >= (int64_t)0xFFFFFFFF) throw std::runtime_error("device build: primitive count out of range");
     const bool ind = s_.indirect;
-    const std::vector<uint32_t>& buf = ind ? s_.indirect_buf : s_.index;
     const int width = ind ? 1 : 3;
 
     DevBuf<float> d_pos;
@@ -1001,14 +1041,22 @@ class DeviceBuilder {
                                                 ind ? d_indirect.p : nullptr, base_, n_, C_, L_, H_, perm_.p);
     GB_TRY(cudaGetLastError());
 
-    // node table: roots plus two children per large split (each level's large nodes are disjoint
-    // ranges of more than kSmall primitives, and only depths below max_depth split)
-    const int64_t levels = std::max(1, max_depth_);
-    const int64_t cap = (int64_t)ranges.size() + 2 * std::min<int64_t>(n_, levels * (n_ / (kSmall + 1) + 1));
+    // large-node scratch, sized once: each level's large nodes are disjoint ranges of more than
+    // kSmall primitives, and only depths below max_depth split
+    const int64_t nf_max = (int64_t)ranges.size() + n_ / (kSmall + 1) + 1;
+    const int64_t blocks_max = n_ / kChunk + nf_max + 1;
+    const int64_t cap = (int64_t)ranges.size() + 2 * std::min<int64_t>(n_, std::max(1, max_depth_) * (n_ / (kSmall + 1) + 1));
     nbox_.alloc((size_t)cap * 12);
     keys_.alloc((size_t)cap);
-    err_.alloc(1);
-    GB_TRY(cudaMemsetAsync(err_.p, 0, sizeof(unsigned int), st_));
+    segs_.alloc((size_t)2 * nf_max);
+    ids_.alloc((size_t)2 * nf_max);
+    axis_.alloc((size_t)nf_max);
+    posd_.alloc((size_t)nf_max);
+    nl_.alloc((size_t)nf_max);
+    split_.alloc((size_t)nf_max);
+    cc_.alloc((size_t)2 * blocks_max);
+    cb_.alloc((size_t)2 * blocks_max);
+    if (strategy_ == kSah) bins_.alloc((size_t)nf_max * kNodeBinWords);
 
     std::vector<int> frontier;
     std::vector<uint32_t> fresh;
@@ -1025,22 +1073,18 @@ class DeviceBuilder {
     for (uint32_t id : fresh) classify((int)id, frontier);
     while (!frontier.empty()) split_level(frontier);
 
-    build_subtrees();
+    small_phase();
     assemble(ranges.size());
 
     // the reordered partition buffer (index triples or indirect entries of [base, base + n))
-    DevBuf<uint32_t> d_in, d_out;
-    d_in.alloc((size_t)n_ * width);
+    DevBuf<uint32_t> d_out;
     d_out.alloc((size_t)n_ * width);
-    GB_TRY(cudaMemcpyAsync(d_in.p, buf.data() + (size_t)base_ * width, (size_t)n_ * width * 4, cudaMemcpyHostToDevice, st_));
-    k_reorder<<<grid_for(n_, 256), 256, 0, st_>>>(perm_.p, d_in.p, d_out.p, n_, width);
+    const uint32_t* d_in = (ind ? d_indirect.p : d_index.p) + (size_t)base_ * width;
+    k_reorder<<<grid_for(n_, 256), 256, 0, st_>>>(perm_.p, d_in, d_out.p, n_, width);
     GB_TRY(cudaGetLastError());
     std::vector<uint32_t>& dst = ind ? s_.indirect_buf : s_.index;
     GB_TRY(cudaMemcpyAsync(dst.data() + (size_t)base_ * width, d_out.p, (size_t)n_ * width * 4, cudaMemcpyDeviceToHost, st_));
-    unsigned int err = 0;
-    GB_TRY(cudaMemcpyAsync(&err, err_.p, sizeof err, cudaMemcpyDeviceToHost, st_));
     GB_TRY(cudaStreamSynchronize(st_));
-    if (err) throw std::runtime_error("device build: subtree stack overflow");
   }
 
  private:
@@ -1049,12 +1093,16 @@ class DeviceBuilder {
   int strategy_, max_depth_, leaf_;
   int64_t base_ = 0, n_ = 0;
   DevBuf<float> prims_, nbox_;
-  DevBuf<uint32_t> perm_, partner_;
+  DevBuf<uint32_t> perm_, partner_, ids_, cc_, cb_, bins_;
   DevBuf<BoundKeys> keys_;
-  DevBuf<unsigned int> err_;
+  DevBuf<Seg> segs_;
+  DevBuf<int> axis_;
+  DevBuf<f64> posd_;
+  DevBuf<unsigned int> nl_;
+  DevBuf<uint8_t> split_;
   float *C_ = nullptr, *L_ = nullptr, *H_ = nullptr;
   std::vector<HostNode> nodes_;
-  std::vector<int> subs_;  // node ids of the warp-built subtrees
+  std::vector<int> subs_;  // node ids of the small-phase roots
 
   // One segment per node, cut into kChunk blocks; returns the block count.
   uint32_t make_segs(const std::vector<int>& ids, std::vector<Seg>& segs) {
@@ -1069,25 +1117,22 @@ class DeviceBuilder {
   }
 
   template <class T>
-  void upload(DevBuf<T>& d, const std::vector<T>& h) {
-    d.alloc(h.size());
-    GB_TRY(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st_));
+  void upload(T* d, const std::vector<T>& h, size_t cap) {
+    if (h.size() > cap) throw std::runtime_error("device build: scratch overflow");
+    if (!h.empty()) GB_TRY(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st_));
   }
 
   void compute_bounds(const std::vector<uint32_t>& ids) {
     std::vector<int> iv(ids.begin(), ids.end());
     std::vector<Seg> segs;
     const uint32_t blocks = make_segs(iv, segs);
-    DevBuf<Seg> d_segs;
-    DevBuf<uint32_t> d_ids;
-    upload(d_segs, segs);
-    upload(d_ids, ids);
+    upload(segs_.p, segs, segs_.n);
+    upload(ids_.p, ids, ids_.n);
     const int n = (int)ids.size();
-    k_bounds_init<<<(n + 255) / 256, 256, 0, st_>>>(d_ids.p, n, keys_.p);
-    if (blocks > 0) k_bounds<<<blocks, kThreads, 0, st_>>>(d_segs.p, (int)segs.size(), C_, L_, H_, n_, keys_.p);
-    k_bounds_finish<<<(n + 255) / 256, 256, 0, st_>>>(d_ids.p, n, keys_.p, L_, H_, n_, nbox_.p);
+    k_bounds_init<<<(n + 255) / 256, 256, 0, st_>>>(ids_.p, n, keys_.p);
+    if (blocks > 0) k_bounds<<<blocks, kThreads, 0, st_>>>(segs_.p, (int)segs.size(), C_, L_, H_, n_, keys_.p);
+    k_bounds_finish<<<(n + 255) / 256, 256, 0, st_>>>(ids_.p, n, keys_.p, L_, H_, n_, nbox_.p);
     GB_TRY(cudaGetLastError());
-    GB_TRY(cudaStreamSynchronize(st_));  // the id / segment uploads above are pageable
   }
 
   void classify(int id, std::vector<int>& frontier) {
@@ -1107,33 +1152,24 @@ class DeviceBuilder {
     std::vector<Seg> segs;
     const uint32_t blocks = make_segs(frontier, segs);
     const int nf = (int)frontier.size();
-    DevBuf<Seg> d_segs;
-    upload(d_segs, segs);
-    DevBuf<int> d_axis;
-    DevBuf<f64> d_pos;
-    DevBuf<unsigned int> d_nl;
-    d_axis.alloc(nf);
-    d_pos.alloc(nf);
-    d_nl.alloc(nf);
-    DevBuf<uint32_t> d_bins;
+    if (nf > (int)axis_.n || 2 * (size_t)blocks > cc_.n) throw std::runtime_error("device build: scratch overflow");
+    upload(segs_.p, segs, segs_.n);
     if (strategy_ == kSah) {
-      d_bins.alloc((size_t)nf * kNodeBinWords);
-      k_bins_init<<<grid_for((int64_t)nf * kNodeBinWords, 256), 256, 0, st_>>>(d_bins.p, (int64_t)nf * kNodeBinWords);
-      k_bins<<<blocks, kThreads, 0, st_>>>(d_segs.p, nf, nbox_.p, C_, L_, H_, n_, d_bins.p);
+      k_bins_init<<<grid_for((int64_t)nf * kNodeBinWords, 256), 256, 0, st_>>>(bins_.p, (int64_t)nf * kNodeBinWords);
+      k_bins<<<blocks, kThreads, 0, st_>>>(segs_.p, nf, nbox_.p, C_, L_, H_, n_, bins_.p);
     }
-    k_choose<<<(nf + 3) / 4, 128, 0, st_>>>(d_segs.p, nf, nbox_.p, d_bins.p, strategy_, d_axis.p, d_pos.p);
-    GB_TRY(cudaMemsetAsync(d_nl.p, 0, nf * sizeof(unsigned int), st_));
-    k_count<<<blocks, kThreads, 0, st_>>>(d_segs.p, nf, C_, n_, d_axis.p, d_pos.p, d_nl.p);
+    k_choose<<<(nf + 3) / 4, 128, 0, st_>>>(segs_.p, nf, nbox_.p, bins_.p, strategy_, axis_.p, posd_.p);
+    GB_TRY(cudaMemsetAsync(nl_.p, 0, nf * sizeof(unsigned int), st_));
+    k_count<<<blocks, kThreads, 0, st_>>>(segs_.p, nf, C_, n_, axis_.p, posd_.p, nl_.p);
     GB_TRY(cudaGetLastError());
     std::vector<int> axis(nf);
     std::vector<unsigned int> nl(nf);
-    GB_TRY(cudaMemcpyAsync(axis.data(), d_axis.p, nf * sizeof(int), cudaMemcpyDeviceToHost, st_));
-    GB_TRY(cudaMemcpyAsync(nl.data(), d_nl.p, nf * sizeof(unsigned int), cudaMemcpyDeviceToHost, st_));
+    GB_TRY(cudaMemcpyAsync(axis.data(), axis_.p, nf * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    GB_TRY(cudaMemcpyAsync(nl.data(), nl_.p, nf * sizeof(unsigned int), cudaMemcpyDeviceToHost, st_));
     GB_TRY(cudaStreamSynchronize(st_));
 
     std::vector<uint8_t> split(nf, 0);
     std::vector<uint32_t> children;
-    bool any = false;
     for (int i = 0; i < nf; ++i) {
       HostNode& h = nodes_[frontier[i]];
       if (axis[i] < 0 || nl[i] == 0 || nl[i] == h.cnt) {  // buildTree.js:60-72: no useful split
@@ -1141,7 +1177,6 @@ class DeviceBuilder {
         continue;
       }
       split[i] = 1;
-      any = true;
       h.kind = kNodeInner;
       h.axis = axis[i];
       HostNode l, r;
@@ -1159,71 +1194,87 @@ class DeviceBuilder {
       children.push_back((uint32_t)h.right);
     }
     std::vector<int> next;
-    if (any) {
+    if (!children.empty()) {
       if (nodes_.size() > keys_.n) throw std::runtime_error("device build: node table overflow");
-      DevBuf<uint8_t> d_split;
-      upload(d_split, split);
-      DevBuf<uint32_t> d_cc, d_cb;
-      d_cc.alloc((size_t)blocks * 2);
-      d_cb.alloc((size_t)blocks * 2);
-      k_pair_counts<<<blocks, kThreads, 0, st_>>>(d_segs.p, nf, C_, n_, d_axis.p, d_pos.p, d_nl.p, d_split.p, d_cc.p);
-      k_pair_scan<<<(nf + 3) / 4, 128, 0, st_>>>(d_segs.p, nf, d_split.p, d_cc.p, d_cb.p);
-      k_pair_mark<<<blocks, kThreads, 0, st_>>>(d_segs.p, nf, C_, n_, d_axis.p, d_pos.p, d_nl.p, d_split.p, d_cc.p,
-                                                d_cb.p, partner_.p);
-      k_pair_swap<<<blocks, kThreads, 0, st_>>>(d_segs.p, nf, C_, L_, H_, perm_.p, n_, d_axis.p, d_pos.p, d_nl.p,
-                                                d_split.p, d_cb.p, partner_.p);
+      upload(split_.p, split, split_.n);
+      k_pair_counts<<<blocks, kThreads, 0, st_>>>(segs_.p, nf, C_, n_, axis_.p, posd_.p, nl_.p, split_.p, cc_.p);
+      k_pair_scan<<<(nf + 3) / 4, 128, 0, st_>>>(segs_.p, nf, split_.p, cc_.p, cb_.p);
+      k_pair_mark<<<blocks, kThreads, 0, st_>>>(segs_.p, nf, C_, n_, axis_.p, posd_.p, nl_.p, split_.p, cc_.p, cb_.p,
+                                                partner_.p);
+      k_pair_swap<<<blocks, kThreads, 0, st_>>>(segs_.p, nf, C_, L_, H_, perm_.p, n_, axis_.p, posd_.p, nl_.p,
+                                                split_.p, cb_.p, partner_.p);
       GB_TRY(cudaGetLastError());
       compute_bounds(children);
       for (uint32_t id : children) classify((int)id, next);
     }
-    GB_TRY(cudaStreamSynchronize(st_));
     frontier.swap(next);
   }
 
+  DevBuf<SmallNode> small_;
+  DevBuf<uint32_t> lv_;
+  DevBuf<unsigned int> counter_;
+  int levels_ = 0;
   std::vector<uint32_t> sub_sizes_;
-  DevBuf<uint32_t> temp_;
-  std::vector<uint32_t> temp_base_;
 
-  void build_subtrees() {
+  // Every small root's subtree, level by level on the device.
+  void small_phase() {
     const int ns = (int)subs_.size();
     sub_sizes_.assign(ns, 0);
     if (ns == 0) return;
-    std::vector<SubRoot> roots(ns);
-    uint64_t tb = 0, sb = 0;
-    temp_base_.resize(ns);
+    uint64_t cells = ns;
+    int min_depth = max_depth_;
+    std::vector<SmallNode> roots(ns);
+    std::vector<uint32_t> root_ids(ns);
     for (int k = 0; k < ns; ++k) {
       const HostNode& h = nodes_[subs_[k]];
-      SubRoot& r = roots[k];
-      r.node = (uint32_t)subs_[k];
+      SmallNode& r = roots[k];
+      std::memset(&r, 0, sizeof r);
       r.off = h.off;
       r.cnt = h.cnt;
       r.depth = (uint32_t)h.depth;
-      r.temp_base = (uint32_t)tb;
-      r.stack_base = (uint32_t)sb;
-      r.stack_cap = std::min<uint32_t>(h.cnt, (uint32_t)std::max(0, max_depth_ - h.depth) + 1) + 2;
-      r.pad = 0;
-      temp_base_[k] = (uint32_t)tb;
-      tb += 2 * (uint64_t)h.cnt - 1;
-      sb += r.stack_cap;
+      r.left = -1;
+      r.axis = -1;
+      root_ids[k] = (uint32_t)subs_[k];
+      cells += 2 * (uint64_t)h.cnt;
+      min_depth = std::min(min_depth, h.depth);
     }
-    if (tb >= 0xFFFFFFFFull || sb >= 0xFFFFFFFFull) throw std::runtime_error("device build: subtree scratch too large");
-    DevBuf<SubRoot> d_roots;
-    upload(d_roots, roots);
-    temp_.alloc((size_t)tb * 8);
-    DevBuf<StackEnt> d_stack;
-    d_stack.alloc((size_t)sb);
-    DevBuf<uint32_t> d_sizes;
-    d_sizes.alloc(ns);
-    k_subtree<<<(ns + kSubWarps - 1) / kSubWarps, kSubWarps * 32, 0, st_>>>(
-        d_roots.p, ns, nbox_.p, C_, L_, H_, perm_.p, n_, partner_.p, temp_.p, d_sizes.p, d_stack.p, strategy_,
-        max_depth_, leaf_, (uint32_t)base_, err_.p);
+    if (cells >= 0xFFFFFFFFull) throw std::runtime_error("device build: too many nodes");
+    small_.alloc((size_t)cells);
+    GB_TRY(cudaMemcpyAsync(small_.p, roots.data(), ns * sizeof(SmallNode), cudaMemcpyHostToDevice, st_));
+    DevBuf<uint32_t> d_root_ids;
+    d_root_ids.alloc(ns);
+    GB_TRY(cudaMemcpyAsync(d_root_ids.p, root_ids.data(), ns * 4, cudaMemcpyHostToDevice, st_));
+    k_small_boxes<<<(ns + 255) / 256, 256, 0, st_>>>(d_root_ids.p, ns, nbox_.p, small_.p);
+    const int max_levels = std::max(1, max_depth_ - min_depth + 1);
+    lv_.alloc((size_t)max_levels + 2);
+    counter_.alloc(1);
+    const uint32_t init[2] = {0u, (uint32_t)ns};
+    GB_TRY(cudaMemcpyAsync(lv_.p, init, sizeof init, cudaMemcpyHostToDevice, st_));
+    GB_TRY(cudaMemcpyAsync(counter_.p, &init[1], sizeof(unsigned int), cudaMemcpyHostToDevice, st_));
+    const int grid = 148 * 8;
+    levels_ = 0;
+    for (int level = 0; level < max_levels; ++level) {
+      k_small_level<<<grid, kSubWarps * 32, 0, st_>>>(small_.p, lv_.p, level, counter_.p, C_, L_, H_, perm_.p, n_,
+                                                      partner_.p, strategy_, max_depth_, leaf_);
+      k_level_close<<<1, 1, 0, st_>>>(lv_.p, level, counter_.p);
+      GB_TRY(cudaGetLastError());
+      levels_ = level + 1;
+      if (level % 8 == 7) {  // stop once a level appends no children
+        uint32_t b[2];
+        GB_TRY(cudaMemcpyAsync(b, lv_.p + level + 1, sizeof b, cudaMemcpyDeviceToHost, st_));
+        GB_TRY(cudaStreamSynchronize(st_));
+        if (b[0] == b[1]) break;
+      }
+    }
+    for (int level = levels_ - 1; level >= 0; --level) k_sizes<<<grid, 256, 0, st_>>>(small_.p, lv_.p, level);
     GB_TRY(cudaGetLastError());
-    GB_TRY(cudaMemcpyAsync(sub_sizes_.data(), d_sizes.p, ns * sizeof(uint32_t), cudaMemcpyDeviceToHost, st_));
+    GB_TRY(cudaMemcpy2DAsync(sub_sizes_.data(), sizeof(uint32_t), &small_.p[0].size, sizeof(SmallNode),
+                             sizeof(uint32_t), ns, cudaMemcpyDeviceToHost, st_));
     GB_TRY(cudaStreamSynchronize(st_));
   }
 
-  // Pre-order placement (buildUtils.js:35-92): sizes bottom-up, positions top-down (children
-  // always have larger ids than their parent).
+  // Pre-order placement (buildUtils.js:35-92): the large nodes on the host (children always have
+  // larger ids than their parent), the small-phase subtrees on the device.
   void assemble(size_t n_roots) {
     const size_t nn = nodes_.size();
     std::vector<uint64_t> size(nn), pre(nn);
@@ -1233,8 +1284,10 @@ class DeviceBuilder {
     }
     std::vector<uint64_t> root_first(n_roots + 1, 0);
     for (size_t r = 0; r < n_roots; ++r) root_first[r + 1] = root_first[r] + size[r];
+    const uint64_t total = root_first[n_roots];
+    if (total >= 0xFFFFFFFFull) throw std::runtime_error("device build: too many nodes");
     std::vector<PlaceRec> recs;
-    std::vector<SubCopy> copies;
+    std::vector<uint32_t> sub_dest(subs_.size());
     for (size_t i = 0; i < nn; ++i) {
       const HostNode& h = nodes_[i];
       if (i < n_roots) pre[i] = 0;
@@ -1244,28 +1297,29 @@ class DeviceBuilder {
         pre[h.right] = pre[i] + 1 + size[h.left];
         recs.push_back({(uint32_t)i, dest, (uint32_t)(1 + size[h.left]), (uint32_t)h.axis});
       } else if (h.kind == kNodeSub) {
-        copies.push_back({temp_base_[h.sub], sub_sizes_[h.sub], dest, 0});
+        sub_dest[h.sub] = dest;
       } else {
         recs.push_back({(uint32_t)i, dest, (uint32_t)(base_ + h.off), (h.cnt & 0xFFFFu) | 0xFFFF0000u});
       }
     }
-    const uint64_t total = root_first[n_roots];
     DevBuf<uint32_t> d_out;
     d_out.alloc((size_t)total * 8);
+    DevBuf<PlaceRec> d_recs;
     if (!recs.empty()) {
-      DevBuf<PlaceRec> d_recs;
-      upload(d_recs, recs);
+      d_recs.alloc(recs.size());
+      upload(d_recs.p, recs, d_recs.n);
       k_place<<<((int)recs.size() + 255) / 256, 256, 0, st_>>>(d_recs.p, (int)recs.size(), nbox_.p, d_out.p);
-      GB_TRY(cudaGetLastError());
-      GB_TRY(cudaStreamSynchronize(st_));
     }
-    if (!copies.empty()) {
-      DevBuf<SubCopy> d_copies;
-      upload(d_copies, copies);
-      k_copy_subtrees<<<(unsigned)copies.size(), 256, 0, st_>>>(d_copies.p, temp_.p, d_out.p);
-      GB_TRY(cudaGetLastError());
-      GB_TRY(cudaStreamSynchronize(st_));
+    DevBuf<uint32_t> d_dest;
+    if (!subs_.empty()) {
+      const int ns = (int)subs_.size();
+      d_dest.alloc(ns);
+      upload(d_dest.p, sub_dest, d_dest.n);
+      k_set_dest<<<(ns + 255) / 256, 256, 0, st_>>>(small_.p, d_dest.p, ns);
+      for (int level = 0; level < levels_; ++level) k_dests<<<148 * 8, 256, 0, st_>>>(small_.p, lv_.p, level);
+      k_write_small<<<148 * 8, 256, 0, st_>>>(small_.p, counter_.p, (uint32_t)base_, d_out.p);
     }
+    GB_TRY(cudaGetLastError());
     std::vector<uint32_t> words((size_t)total * 8);
     GB_TRY(cudaMemcpyAsync(words.data(), d_out.p, words.size() * 4, cudaMemcpyDeviceToHost, st_));
     GB_TRY(cudaStreamSynchronize(st_));
