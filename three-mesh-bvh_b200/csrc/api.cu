@@ -682,10 +682,15 @@ static bvhc_status build_impl(const float* positions, uint64_t n_verts, int stri
       s->has_index = true;
       s->index_elem_bytes = index_elem_bytes;
       s->index.resize(index_count);
-      for (uint64_t i = 0; i < index_count; ++i) {
-        s->index[i] = read_index(index, index_elem_bytes, i);
-        if (s->index[i] >= n_verts) { delete s; return BVHC_ERR_INVALID_ARGUMENT; }
+      uint32_t top = 0;
+      if (index_elem_bytes == 4) {
+        std::memcpy(s->index.data(), index, index_count * 4);
+        for (uint64_t i = 0; i < index_count; ++i) top = std::max(top, s->index[i]);
+      } else {
+        const uint16_t* p16 = static_cast<const uint16_t*>(index);
+        for (uint64_t i = 0; i < index_count; ++i) top = std::max(top, s->index[i] = p16[i]);
       }
+      if (index_count && top >= n_verts) { delete s; return BVHC_ERR_INVALID_ARGUMENT; }
     }
     try {
       if (on_device)

@@ -46,6 +46,11 @@
 #include "bvhc_internal.h"
 #include "softf64.cuh"
 
+#ifdef BVHC_BUILD_TRACE
+#include <chrono>
+#include <cstdio>
+#endif
+
 namespace bvhc {
 namespace {
 
@@ -100,7 +105,7 @@ __device__ __forceinline__ float fmax_gt(float a, float b) { return b > a ? b : 
 __device__ __forceinline__ bool goes_left(float c, f64 pos) { return sf::lt(sf::from_f32(c), pos); }
 
 // computeSurfaceArea (ArrayBoxUtilities.js:101-108) in binary64.
-__device__ f64 area_d(const float* lo, const float* hi) {
+__device__ __noinline__ f64 area_d(const float* lo, const float* hi) {
   const f64 d0 = sf::sub(sf::from_f32(hi[0]), sf::from_f32(lo[0]));
   const f64 d1 = sf::sub(sf::from_f32(hi[1]), sf::from_f32(lo[1]));
   const f64 d2 = sf::sub(sf::from_f32(hi[2]), sf::from_f32(lo[2]));
@@ -108,7 +113,7 @@ __device__ f64 area_d(const float* lo, const float* hi) {
 }
 
 // The split cost of splitUtils.js:162-166 / :268-272 in binary64.
-__device__ f64 cost_d(const float* llo, const float* lhi, uint32_t lc, const float* rlo, const float* rhi, uint32_t rc,
+__device__ __noinline__ f64 cost_d(const float* llo, const float* lhi, uint32_t lc, const float* rlo, const float* rhi, uint32_t rc,
                       f64 root_area) {
   f64 lp = 0, rp = 0;
   if (lc != 0) lp = sf::div(area_d(llo, lhi), root_area);
@@ -138,7 +143,13 @@ __device__ AxisBin axis_bin(float l, float r) {
   ab.fast = ab.lenf >= 0x1p-90f && ab.lenf <= 0x1p120f;
   return ab;
 }
-__device__ int bin_of(float c, const AxisBin& ab) {
+__device__ __noinline__ int bin_exact(float c, float l, float r) {  // the binary64 quotient
+  const f64 left = sf::from_f32(l);
+  const f64 width = sf::mul(sf::sub(sf::from_f32(r), left), kInvBinsD);
+  const int b = sf::to_i32_trunc(sf::div(sf::sub(sf::from_f32(c), left), width));
+  return b >= kBins ? kBins - 1 : (b < 0 ? 0 : b);
+}
+__device__ __forceinline__ int bin_of(float c, const AxisBin& ab) {
   if (ab.lenf == 0.0f) return 0;  // zero width: (c - left) / 0 is NaN, `~~NaN` is 0
   if (ab.fast) {
     if (c == ab.l) return 0;
@@ -148,10 +159,7 @@ __device__ int bin_of(float c, const AxisBin& ab) {
     const float t = truncf(q);
     if ((t == 0.0f || q - t > kBinEps) && (t + 1.0f) - q > kBinEps) return (int)t;
   }
-  const f64 left = sf::from_f32(ab.l);
-  const f64 width = sf::mul(sf::sub(sf::from_f32(ab.r), left), kInvBinsD);
-  const int b = sf::to_i32_trunc(sf::div(sf::sub(sf::from_f32(c), left), width));
-  return b >= kBins ? kBins - 1 : (b < 0 ? 0 : b);
+  return bin_exact(c, ab.l, ab.r);
 }
 
 struct Split {
@@ -159,7 +167,7 @@ struct Split {
   f64 pos;
 };
 
-__device__ Split binned_split_at(const float* cbox, int a, int i) {  // splitUtils.js:183
+__device__ __noinline__ Split binned_split_at(const float* cbox, int a, int i) {  // splitUtils.js:183
   const f64 L = sf::from_f32(cbox[a]);
   const f64 W = sf::mul(sf::sub(sf::from_f32(cbox[a + 3]), L), kInvBinsD);
   return {a, sf::add(sf::add(L, W), sf::mul(sf::from_u64((uint64_t)i), W))};
@@ -246,12 +254,37 @@ __device__ Split warp_sah_binned(const uint32_t* bins, uint32_t cnt, const float
       want[a] = valid[a] && cf[a] <= hi;
       ncont += __popc(__ballot_sync(kFull, want[a]));
     }
-    if (ncont == 1 && m < __fmul_rn(best0f, 1.0f - kCostTol)) {
+    if (m < __fmul_rn(best0f, 1.0f - kCostTol)) {
+      // the first contender in the reference's scan order (axis, then bin)
+      int wa = 0, wl = 0;
+      bool found = false;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const unsigned bal = __ballot_sync(kFull, want[a]);
-        if (bal) return binned_split_at(cbox, a, __ffs(bal) - 1);
+        if (bal && !found) {
+          found = true;
+          wa = a;
+          wl = __ffs(bal) - 1;
+        }
       }
+      if (ncont == 1) return binned_split_at(cbox, wa, wl);
+      // contenders with the same counts and boxes as the first one have exactly its binary64
+      // cost (the same partition reached along another axis, typically), so it wins the scan
+      const uint32_t tlc = __shfl_sync(kFull, wa == 0 ? lc[0] : (wa == 1 ? lc[1] : lc[2]), wl);
+      bool same = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) same = same && (!want[a] || lc[a] == tlc);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float t0 = __shfl_sync(kFull, wa == 0 ? llo[0][d] : (wa == 1 ? llo[1][d] : llo[2][d]), wl);
+        const float t1 = __shfl_sync(kFull, wa == 0 ? lhi[0][d] : (wa == 1 ? lhi[1][d] : lhi[2][d]), wl);
+        const float t2 = __shfl_sync(kFull, wa == 0 ? rlo[0][d] : (wa == 1 ? rlo[1][d] : rlo[2][d]), wl);
+        const float t3 = __shfl_sync(kFull, wa == 0 ? rhi[0][d] : (wa == 1 ? rhi[1][d] : rhi[2][d]), wl);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          same = same && (!want[a] || (llo[a][d] == t0 && lhi[a][d] == t1 && rlo[a][d] == t2 && rhi[a][d] == t3));
+      }
+      if (__all_sync(kFull, same)) return binned_split_at(cbox, wa, wl);
     }
   }
   // binary64 over the contenders (all valid candidates when the float32 bound did not apply)
@@ -283,7 +316,7 @@ __device__ Split warp_sah_binned(const uint32_t* bins, uint32_t cnt, const float
 }
 
 // Every primitive center a candidate (splitUtils.js:63-174), for count < BIN_COUNT / 4.  One thread.
-__device__ Split sah_small(const float* C, const float* L, const float* H, int64_t n, uint32_t off, uint32_t cnt,
+__device__ __noinline__ Split sah_small(const float* C, const float* L, const float* H, int64_t n, uint32_t off, uint32_t cnt,
                            const float* box) {
   const f64 root_area = area_d(box, box + 3);
   f64 best = sf::mul(kPrimCostD, sf::from_u64(cnt));
@@ -338,7 +371,7 @@ __device__ Split sah_small(const float* C, const float* L, const float* H, int64
 }
 
 // CENTER (splitUtils.js:25-35): longest centroid extent (strict `>`), split at its middle.
-__device__ Split center_split(const float* cbox) {
+__device__ __noinline__ Split center_split(const float* cbox) {
   Split s{-1, 0};
   f64 best = sf::neg(sf::kInf);
   for (int i = 0; i < 3; ++i) {
@@ -722,7 +755,7 @@ __global__ void k_bounds_finish(const uint32_t* __restrict__ ids, int n_ids, con
 }
 
 // One warp: box (first primitive for each extreme) and centroid box of [off, off + cnt).
-__device__ void warp_bounds(const float* C, const float* L, const float* H, int64_t n, uint32_t off, uint32_t cnt,
+__device__ __noinline__ void warp_bounds(const float* C, const float* L, const float* H, int64_t n, uint32_t off, uint32_t cnt,
                             float* box, float* cbox) {
   const int lane = threadIdx.x & 31;
   float bmin[3], bmax[3], cmin[3], cmax[3];
@@ -1007,6 +1040,12 @@ struct HostNode {
 
 int grid_for(int64_t n, int threads) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 64)); }
 
+#ifdef BVHC_BUILD_TRACE
+#define GB_TRACE(what) trace(what)
+#else
+#define GB_TRACE(what) ((void)0)
+#endif
+
 class DeviceBuilder {
  public:
   DeviceBuilder(Serialized& s, cudaStream_t stream, int strategy, int max_depth, int leaf)
@@ -1034,6 +1073,7 @@ class DeviceBuilder {
     prims_.alloc((size_t)n_ * 9);
     perm_.alloc((size_t)n_);
     partner_.alloc((size_t)n_);
+    GB_TRACE("upload+alloc");
     C_ = prims_.p;
     L_ = prims_.p + 3 * n_;
     H_ = prims_.p + 6 * n_;
@@ -1071,10 +1111,13 @@ class DeviceBuilder {
     }
     compute_bounds(fresh);
     for (uint32_t id : fresh) classify((int)id, frontier);
+    GB_TRACE("prims+scratch");
     while (!frontier.empty()) split_level(frontier);
-
+    GB_TRACE("large nodes");
     small_phase();
+    GB_TRACE("small nodes");
     assemble(ranges.size());
+    GB_TRACE("assemble+d2h");
 
     // the reordered partition buffer (index triples or indirect entries of [base, base + n))
     DevBuf<uint32_t> d_out;
@@ -1085,9 +1128,19 @@ class DeviceBuilder {
     std::vector<uint32_t>& dst = ind ? s_.indirect_buf : s_.index;
     GB_TRY(cudaMemcpyAsync(dst.data() + (size_t)base_ * width, d_out.p, (size_t)n_ * width * 4, cudaMemcpyDeviceToHost, st_));
     GB_TRY(cudaStreamSynchronize(st_));
+    GB_TRACE("reorder+d2h");
   }
 
  private:
+#ifdef BVHC_BUILD_TRACE
+  std::chrono::steady_clock::time_point t_ = std::chrono::steady_clock::now();
+  void trace(const char* what) {  // phase timing for development builds
+    cudaStreamSynchronize(st_);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "device build %-14s %8.3f ms\n", what, std::chrono::duration<double, std::milli>(now - t_).count());
+    t_ = now;
+  }
+#endif
   Serialized& s_;
   cudaStream_t st_;
   int strategy_, max_depth_, leaf_;
@@ -1320,16 +1373,13 @@ class DeviceBuilder {
       k_write_small<<<148 * 8, 256, 0, st_>>>(small_.p, counter_.p, (uint32_t)base_, d_out.p);
     }
     GB_TRY(cudaGetLastError());
-    std::vector<uint32_t> words((size_t)total * 8);
-    GB_TRY(cudaMemcpyAsync(words.data(), d_out.p, words.size() * 4, cudaMemcpyDeviceToHost, st_));
-    GB_TRY(cudaStreamSynchronize(st_));
-    s_.roots.clear();
+    s_.roots.assign(n_roots, {});
     for (size_t r = 0; r < n_roots; ++r) {
-      const size_t bytes = (size_t)size[r] * 32;
-      std::vector<uint8_t> b(bytes);
-      std::memcpy(b.data(), words.data() + (size_t)root_first[r] * 8, bytes);
-      s_.roots.push_back(std::move(b));
+      s_.roots[r].resize((size_t)size[r] * 32);
+      GB_TRY(cudaMemcpyAsync(s_.roots[r].data(), d_out.p + (size_t)root_first[r] * 8, s_.roots[r].size(),
+                             cudaMemcpyDeviceToHost, st_));
     }
+    GB_TRY(cudaStreamSynchronize(st_));
   }
 };
 

@@ -20,10 +20,15 @@
 
 #include <cstdint>
 
+// Small helpers are inlined; the arithmetic routines are kept out of line (one copy per
+// translation unit) so that kernels calling them from many places stay small in the
+// instruction cache.
 #ifdef __CUDACC__
 #define BVHC_SF_HD __host__ __device__ __forceinline__
+#define BVHC_SF_NI static __host__ __device__ __noinline__
 #else
 #define BVHC_SF_HD inline
+#define BVHC_SF_NI [[maybe_unused]] static
 #endif
 
 namespace bvhc {
@@ -75,7 +80,7 @@ BVHC_SF_HD uint64_t shr_jam(uint64_t x, int n) {
 }
 
 // Rounds sign * m * 2^(e-1023-62) to binary64 (m normalised to bit 62 when e >= 1).
-BVHC_SF_HD f64 round_pack(uint64_t sign, int e, uint64_t m) {
+BVHC_SF_NI f64 round_pack(uint64_t sign, int e, uint64_t m) {
   if (e >= 0x7FF) return sign | kInf;
   if (e < 1) {  // below the normal range: denormalise to the scale of e = 1
     m = shr_jam(m, 1 - e);
@@ -106,7 +111,7 @@ BVHC_SF_HD int unpack(f64 a, uint64_t& m) {
   return 1 - (52 - lead);
 }
 
-BVHC_SF_HD f64 add(f64 a, f64 b) {
+BVHC_SF_NI f64 add(f64 a, f64 b) {
   if (is_nan(a) || is_nan(b)) return kNaN;
   uint64_t sa = a & kSign, sb = b & kSign;
   if (is_inf(a)) return (is_inf(b) && sa != sb) ? kNaN : a;
@@ -137,7 +142,7 @@ BVHC_SF_HD f64 add(f64 a, f64 b) {
 
 BVHC_SF_HD f64 sub(f64 a, f64 b) { return add(a, is_nan(b) ? b : neg(b)); }
 
-BVHC_SF_HD f64 mul(f64 a, f64 b) {
+BVHC_SF_NI f64 mul(f64 a, f64 b) {
   if (is_nan(a) || is_nan(b)) return kNaN;
   const uint64_t s = (a ^ b) & kSign;
   if (is_inf(a) || is_inf(b)) return (is_zero(a) || is_zero(b)) ? kNaN : (s | kInf);
@@ -154,7 +159,7 @@ BVHC_SF_HD f64 mul(f64 a, f64 b) {
   return round_pack(s, e, m);
 }
 
-BVHC_SF_HD f64 div(f64 a, f64 b) {
+BVHC_SF_NI f64 div(f64 a, f64 b) {
   if (is_nan(a) || is_nan(b)) return kNaN;
   const uint64_t s = (a ^ b) & kSign;
   if (is_inf(a)) return is_inf(b) ? kNaN : (s | kInf);
@@ -185,7 +190,7 @@ BVHC_SF_HD f64 div(f64 a, f64 b) {
   return round_pack(s, e, q);
 }
 
-BVHC_SF_HD f64 sqrt(f64 a) {
+BVHC_SF_NI f64 sqrt(f64 a) {
   if (is_nan(a)) return kNaN;
   if (is_zero(a)) return a;
   if (a & kSign) return kNaN;
@@ -255,7 +260,7 @@ BVHC_SF_HD f64 from_f32(float x) {
 }
 
 // Round to the nearest float32, ties to even (JavaScript's Math.fround / a Float32Array store).
-BVHC_SF_HD float to_f32(f64 a) {
+BVHC_SF_NI float to_f32(f64 a) {
   const uint32_t s = (uint32_t)(a >> 63) << 31;
   if (is_nan(a)) return f32_from_bits(0x7FC00000u);
   if (is_inf(a)) return f32_from_bits(s | 0x7F800000u);
@@ -280,7 +285,7 @@ BVHC_SF_HD float to_f32(f64 a) {
 }
 
 // Nonnegative integers (exact below 2^53, rounded above).
-BVHC_SF_HD f64 from_u64(uint64_t x) {
+BVHC_SF_NI f64 from_u64(uint64_t x) {
   if (x == 0) return 0;
   const int lead = 63 - clz64(x);
   const uint64_t m = lead <= 62 ? x << (62 - lead) : shr_jam(x, lead - 62);
@@ -288,7 +293,7 @@ BVHC_SF_HD f64 from_u64(uint64_t x) {
 }
 
 // Truncation toward zero for |a| < 2^31 (JavaScript's `~~a` there); NaN gives 0.
-BVHC_SF_HD int to_i32_trunc(f64 a) {
+BVHC_SF_NI int to_i32_trunc(f64 a) {
   if (is_nan(a)) return 0;
   const int e = (int)((a >> 52) & 0x7FF);
   if (e < 1023) return 0;
