@@ -42,9 +42,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all"], default="first",
+    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all", "build"], default="first",
                     help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form; "
-                         "adjoint: forward/backward timing; closest: the 256^3 closest-point grid")
+                         "adjoint: forward/backward timing; closest: the 256^3 closest-point grid; all: raycast "
+                         "(all hits); build: the device SAH build")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
@@ -757,6 +758,89 @@ def run_adjoint(args, ws, rank, local):
     bvh_star.dispose()
 
 
+def run_build(args, ws, rank, local):
+    """SAH build of the 2M-triangle knot on the device (bvhc_build_device), host buffers in and
+    out (the call uploads positions and index, builds, and returns the serialized roots and the
+    reordered index), against the library's CPU builder; the serialized bytes must be identical."""
+    import ctypes as C
+
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
+    lib = pkg.lib()
+    pos = np.ascontiguousarray(geo.position, dtype=np.float32)
+    idx = geo.index
+    n_tri = idx.size // 3
+
+    def build(device: bool):
+        out = C.c_void_p()
+        args_ = (pos.ctypes.data, pos.shape[0], 3, idx.ctypes.data, idx.dtype.itemsize, idx.size, None, 0, 0, -1,
+                 int(pkg.SAH), 40, 10, 0)
+        st = (lib.bvhc_build_device(*args_, local, None, C.byref(out)) if device else lib.bvhc_build(*args_, C.byref(out)))
+        if st != 0:
+            raise RuntimeError(f"build failed with status {st}")
+        return out
+
+    def blob(s):
+        parts = []
+        for i in range(lib.bvhc_serialized_root_count(s)):
+            p, nb = C.c_void_p(), C.c_uint64()
+            lib.bvhc_serialized_root(s, i, C.byref(p), C.byref(nb))
+            parts.append(C.string_at(p, nb.value))
+        p, eb, cnt = C.c_void_p(), C.c_int(), C.c_uint64()
+        lib.bvhc_serialized_index(s, C.byref(p), C.byref(eb), C.byref(cnt))
+        parts.append(C.string_at(p, cnt.value * eb.value))
+        return b"".join(parts)
+
+    for _ in range(args.warmup):
+        lib.bvhc_serialized_free(build(True))
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            s = build(True)
+            times.append((time.perf_counter() - t0) * 1e3)
+            if len(times) < args.steps:
+                lib.bvhc_serialized_free(s)
+    ms = max_over_ranks(float(np.median(times)), ws, dev)
+    d2h_bytes = len(blob(s))
+    cpu = None
+    identical = None
+    if rank == 0:
+        t0 = time.perf_counter()
+        sc = build(False)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        identical = blob(sc) == blob(s)
+        lib.bvhc_serialized_free(sc)
+        cpu = {"value": n_tri / (cpu_ms / 1e3) / 1e6, "unit": "Mtris/s", "cores": 1, "kind": "port",
+               "sample": "the whole mesh, the library's single-threaded CPU builder (byte-identical to the "
+                         "oracle's restatement of the reference build)", "ms": cpu_ms}
+    lib.bvhc_serialized_free(s)
+    if rank == 0:
+        line = {"metric": "Mtris/s SAH build (2M tri, host buffers in and out)",
+                "value": weak_scaling_rate(ws, n_tri, 1, ms), "unit": "Mtris/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+binary64 (integer-emulated decisions)", "data": "synthetic",
+                "config": {"workload": f"TorusKnot(10,3,{args.tubular},{args.radial}) {n_tri:,} tri + N(0,0.02) "
+                                       "normal noise (seed 1), SAH, maxLeafSize 10, maxDepth 40",
+                           "timing": "wall clock around bvhc_build_device (it synchronizes), median of steps"},
+                "serialized_identical_to_cpu_build": identical,
+                "e2e": {"value": weak_scaling_rate(ws, n_tri, 1, ms), "unit": "Mtris/s",
+                        "h2d_bytes_per_step": int(pos.nbytes + idx.nbytes),
+                        "d2h_bytes_per_step": d2h_bytes},
+                "roofline": None, "roofline_note": "tree construction is latency-bound (level-synchronous "
+                "kernels, 227 launches per build); kernel shares in profiles/device_build_k2_launches.md",
+                "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": 227 * args.steps, "gpu_launches_source": "ncu launch list of this workload"}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -771,6 +855,8 @@ def main():
             run_closest(args, ws, rank, local)
         elif args.workload == "all":
             run_all_hits(args, ws, rank, local)
+        elif args.workload == "build":
+            run_build(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:
