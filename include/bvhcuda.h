@@ -18,8 +18,10 @@
  *     bvhc_mesh_synchronize to wait and collect device-side errors).
  *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
  *   - One bvhc_mesh may be queried from one host thread at a time.
- *   - All GPU arithmetic is float32 (no FP64 on the device); decisions whose float32 error
- *     bound does not settle them are re-evaluated in double-float (float-float) arithmetic.
+ *   - All GPU arithmetic is float32 (no FP64 instruction on the device); decisions whose float32
+ *     error bound does not settle them are re-evaluated in double-float (float-float) arithmetic,
+ *     and where the reference's exact binary64 rounding decides (the device build's splits, close
+ *     calls of the oriented-box tests) in binary64 emulated with integer operations.
  */
 #ifndef BVHCUDA_H
 #define BVHCUDA_H
@@ -90,7 +92,8 @@ const char* bvhc_status_string(bvhc_status status);
 /* ---------------------------------------------------------------------------------------------
  * Build: `new MeshBVH(geometry, options)` followed by `MeshBVH.serialize(bvh)`
  * (src/core/GeometryBVH.js:93-163, src/core/build/buildTree.js:123-152,
- * src/core/MeshBVH.js:112-145).  CPU, run once per mesh; not part of the query path.
+ * src/core/MeshBVH.js:112-145).  bvhc_build runs on the CPU, bvhc_build_device on a GPU; run once
+ * per mesh (or after the geometry changes); not part of the query path.
  *   positions        n_verts vertices, `stride_floats` floats apart (xyz first)
  *   index            optional geometry index (elem 2 or 4 bytes); NULL for non-indexed geometry,
  *                    in which case a non-indirect build creates one (geometryUtils.js:15-47)
@@ -319,6 +322,15 @@ bvhc_status bvhc_hit_interpolate(bvhc_mesh* mesh, const bvhc_hit* hits, uint64_t
  * within the radius of the centre, else 0. */
 bvhc_status bvhc_intersects_sphere(bvhc_mesh* mesh, const float* spheres, uint64_t n, uint8_t* out, int mem,
                                    void* stream);
+
+/* MeshBVH#intersectsBox(box, boxToMesh) for every box (src/core/MeshBVH.js:780-792: shapecast
+ * with OrientedBox.intersectsBox / intersectsTriangle, src/math/OrientedBox.js:78-260).  boxes:
+ * n x 24 float32 (min xyz, pad, max xyz, pad, then the column-major box-to-mesh matrix as three.js
+ * Matrix4.elements; device buffers 16-byte aligned); out[i] = 1 when some triangle meets the
+ * oriented box, else 0.  Decisions follow the reference's binary64 arithmetic (float-float with
+ * an exact binary64 recheck of close calls). */
+bvhc_status bvhc_intersects_box(bvhc_mesh* mesh, const float* boxes, uint64_t n, uint8_t* out, int mem,
+                                void* stream);
 
 /* MeshBVH#closestPointToPoint(point, target, minThreshold, maxThreshold) for every point
  * (src/core/MeshBVH.js:874-884, src/core/cast/closestPointToPoint.js:6-78). */

@@ -841,6 +841,117 @@ bool sphere_traverse(const Bvh& g, const NodeView& nv, int64_t n32, V3 c, double
   return false;
 }
 
+// ---------------------------------------------------------------------------------------------
+// intersectsBox (MeshBVH.js:780-792): OrientedBox (src/math/OrientedBox.js:78-260) against the
+// node boxes and triangles, with SeparatingAxisBounds (src/math/SeparatingAxisBounds.js:1-81) and
+// ExtendedTriangle's separating axes (src/math/ExtendedTriangle.js:57-86).
+// ---------------------------------------------------------------------------------------------
+struct SatB { double mn, mx; };
+inline bool separated(SatB a, SatB b) { return a.mn > b.mx || b.mn > a.mx; }  // isSeparated
+
+SatB sat_points(V3 axis, const V3* pts, int n) {  // setFromPoints
+  SatB r{INF, -INF};
+  for (int i = 0; i < n; ++i) {
+    double v = dot(axis, pts[i]);
+    r.mn = v < r.mn ? v : r.mn;
+    r.mx = v > r.mx ? v : r.mx;
+  }
+  return r;
+}
+
+SatB sat_box(V3 axis, const double* bmin, const double* bmax) {  // setFromBox (Math.min / Math.max)
+  SatB r{INF, -INF};
+  for (int x = 0; x <= 1; ++x)
+    for (int y = 0; y <= 1; ++y)
+      for (int z = 0; z <= 1; ++z) {
+        V3 p{bmin[0] * x + bmax[0] * (1 - x), bmin[1] * y + bmax[1] * (1 - y), bmin[2] * z + bmax[2] * (1 - z)};
+        double v = dot(axis, p);
+        r.mn = js_min(v, r.mn);
+        r.mx = js_max(v, r.mx);
+      }
+  return r;
+}
+
+// The homogeneous transform of a point by a column-major 4x4 matrix, divided by w.
+V3 apply_matrix4(V3 v, const double* e) {
+  double w = 1 / (e[3] * v.x + e[7] * v.y + e[11] * v.z + e[15]);
+  return {(e[0] * v.x + e[4] * v.y + e[8] * v.z + e[12]) * w, (e[1] * v.x + e[5] * v.y + e[9] * v.z + e[13]) * w,
+          (e[2] * v.x + e[6] * v.y + e[10] * v.z + e[14]) * w};
+}
+
+struct Obb {
+  V3 p[8];     // points
+  V3 ax[3];    // satAxes
+  SatB sb[3];  // satBounds
+  SatB al[3];  // alignedSatBounds
+};
+
+Obb obb_make(const double* mn, const double* mx, const double* e) {  // OrientedBox.update
+  Obb o;
+  for (int x = 0; x <= 1; ++x)
+    for (int y = 0; y <= 1; ++y)
+      for (int z = 0; z <= 1; ++z) {
+        V3 v{x ? mx[0] : mn[0], y ? mx[1] : mn[1], z ? mx[2] : mn[2]};
+        o.p[x | (y << 1) | (z << 2)] = apply_matrix4(v, e);
+      }
+  for (int i = 0; i < 3; ++i) {
+    o.ax[i] = sub(o.p[0], o.p[1 << i]);
+    o.sb[i] = sat_points(o.ax[i], o.p, 8);
+  }
+  for (int d = 0; d < 3; ++d) {
+    SatB r{INF, -INF};
+    for (int k = 0; k < 8; ++k) {
+      double v = d == 0 ? o.p[k].x : (d == 1 ? o.p[k].y : o.p[k].z);
+      r.mn = v < r.mn ? v : r.mn;
+      r.mx = v > r.mx ? v : r.mx;
+    }
+    o.al[d] = r;
+  }
+  return o;
+}
+
+bool obb_meets_box(const Obb& o, const double* bmin, const double* bmax) {  // OrientedBox.intersectsBox
+  for (int d = 0; d < 3; ++d)
+    if (separated(o.al[d], SatB{bmin[d], bmax[d]})) return false;
+  for (int i = 0; i < 3; ++i)
+    if (separated(o.sb[i], sat_box(o.ax[i], bmin, bmax))) return false;
+  return true;
+}
+
+bool obb_meets_triangle(const Obb& o, V3 a, V3 b, V3 c) {  // OrientedBox.intersectsTriangle
+  const V3 tp[3] = {a, b, c};
+  const V3 ta[4] = {face_normal(a, b, c), sub(a, b), sub(b, c), sub(c, a)};
+  for (int i = 0; i < 3; ++i)
+    if (separated(o.sb[i], sat_points(o.ax[i], tp, 3))) return false;
+  for (int i = 0; i < 3; ++i)
+    if (separated(sat_points(ta[i], tp, 3), sat_points(ta[i], o.p, 8))) return false;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 4; ++j) {
+      V3 ax = cross(o.ax[i], ta[j]);
+      if (separated(sat_points(ax, tp, 3), sat_points(ax, o.p, 8))) return false;
+    }
+  return true;
+}
+
+bool box_traverse(const Bvh& g, const NodeView& nv, int64_t n32, const Obb& o, Counters& ctr) {
+  if (nv.is_leaf(n32)) {
+    for (int64_t i = nv.offset(n32); i < nv.offset(n32) + nv.count(n32); ++i) {
+      int64_t abc[3];
+      g.tri_vertices(g.resolve(i), abc);
+      ctr.tris++;
+      if (obb_meets_triangle(o, g.vertex(abc[0]), g.vertex(abc[1]), g.vertex(abc[2]))) return true;
+    }
+    return false;
+  }
+  const int64_t kids[2] = {nv.left(n32), nv.right(n32)};
+  for (int64_t k : kids) {
+    ctr.nodes++;
+    const double bmin[3] = {nv.f(k), nv.f(k + 1), nv.f(k + 2)}, bmax[3] = {nv.f(k + 3), nv.f(k + 4), nv.f(k + 5)};
+    if (obb_meets_box(o, bmin, bmax) && box_traverse(g, nv, k, o, ctr)) return true;
+  }
+  return false;
+}
+
 template <class F>
 void parallel_for(int64_t n, int threads, F f) {
   if (threads <= 1 || n < 64) { f(0, n); return; }
@@ -1060,6 +1171,33 @@ void orc_intersects_sphere(const orc_bvh* h, const float* spheres, int64_t n, ui
         NodeView nv{root.data()};
         c.nodes++;
         if (sphere_traverse(h->b, nv, 0, p, r, c)) {
+          hit = true;
+          break;
+        }
+      }
+      out[i] = hit ? 1 : 0;
+      if (node_reads) node_reads[i] = c.nodes;
+      if (tri_tests) tri_tests[i] = c.tris;
+    }
+  });
+}
+
+// boxes: n x 24 float32 (min xyz, pad, max xyz, pad, the column-major box-to-mesh matrix).
+void orc_intersects_box(const orc_bvh* h, const float* boxes, int64_t n, uint8_t* out, int64_t* node_reads,
+                        int64_t* tri_tests, int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      const float* q = boxes + 24 * i;
+      const double mn[3] = {q[0], q[1], q[2]}, mx[3] = {q[4], q[5], q[6]};
+      double m[16];
+      for (int k = 0; k < 16; ++k) m[k] = q[8 + k];
+      const Obb o = obb_make(mn, mx, m);
+      Counters c;
+      bool hit = false;
+      for (const auto& root : h->b.roots) {
+        NodeView nv{root.data()};
+        c.nodes++;
+        if (box_traverse(h->b, nv, 0, o, c)) {
           hit = true;
           break;
         }

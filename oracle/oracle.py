@@ -67,6 +67,7 @@ def lib():
         L.orc_point_triangle_distance.argtypes = [P, P, P, P]
         L.orc_refit.argtypes = [P, P, I64, I]
         L.orc_intersects_sphere.argtypes = [P, P, I64, P, P, P, I]
+        L.orc_intersects_box.argtypes = [P, P, I64, P, P, P, I]
         _lib = L
     return _lib
 
@@ -137,6 +138,17 @@ class OracleBVH:
         nn = np.empty(n, dtype=np.int64) if counters else None
         nt = np.empty(n, dtype=np.int64) if counters else None
         lib().orc_intersects_sphere(self.h, _p(sp), n, _p(out), _p(nn), _p(nt), threads or _threads())
+        return (out.astype(bool), nn, nt) if counters else out.astype(bool)
+
+    def intersects_box(self, boxes, threads=None, counters=False):
+        """MeshBVH#intersectsBox for each row of 24 float32 (min xyz, pad, max xyz, pad, the
+        column-major box-to-mesh matrix) -> bool array."""
+        bx = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 24)
+        n = bx.shape[0]
+        out = np.empty(n, dtype=np.uint8)
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_intersects_box(self.h, _p(bx), n, _p(out), _p(nn), _p(nt), threads or _threads())
         return (out.astype(bool), nn, nt) if counters else out.astype(bool)
 
     def refit(self, position):

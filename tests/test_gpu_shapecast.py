@@ -1,8 +1,12 @@
-"""GPU intersectsSphere (bvhc_intersects_sphere) against the oracle, and the reference's known
-answers (test/ShapeCasts.test.js:565-604) through the MeshBVH mirror; Intersection attribute
-fields (uv, normal) interpolated at the hits (bvhc_hit_interpolate)."""
+"""GPU intersectsSphere (bvhc_intersects_sphere) and intersectsBox (bvhc_intersects_box) against
+the oracle, and the reference's known answers (test/ShapeCasts.test.js:565-696) through the MeshBVH
+mirror; Intersection attribute fields (uv, normal) interpolated at the hits (bvhc_hit_interpolate)."""
+import math
+
 import numpy as np
 import pytest
+
+from obb_util import compose, quaternion_xyz, random_boxes, record
 
 pytestmark = pytest.mark.gpu
 
@@ -80,3 +84,88 @@ def test_hit_attribute_interpolation(pkg, cuda):
     if first is not None:
         assert first.uv is not None and first.normal is not None
         assert float(np.dot(first.normal, rays[0, 3:])) <= 0
+
+
+def test_intersects_box_known_answers_gpu(pkg, cuda):
+    geo = pkg.sphere(1, 50, 50)
+    bvh = pkg.MeshBVH(geo, {"verbose": False})
+    q = quaternion_xyz(math.pi / 4, math.pi / 4, 0)
+    assert bvh.intersectsBox(((-1, -1, -1), (1, 1, 1)), compose((0, 3, 0), q)) is False
+    assert bvh.intersectsBox(((-1, -1, -1), (1, 1, 1)), compose((0, 2, 0), q)) is True
+    assert bvh.intersectsBox(((-10, -10, -10), (10, 10, 10)), compose((0, 0, 0), q)) is True
+    assert bvh.intersectsBox(((-.5, -.5, -.5), (.5, .5, .5)), compose((0, 0, 0), q)) is False
+    assert bvh.intersectsBox(((-10, 0, -10), (10, 10, 10)), compose((0, 0, 0), q)) is True
+
+
+def _touching_boxes(rng, geo, n):
+    """Axis-aligned boxes (identity matrix) whose faces sit exactly on vertex coordinates: every
+    decision there is an exact tie that the float-float margin hands to binary64."""
+    v = geo.position[rng.integers(0, geo.position.shape[0], (n, 2))]
+    lo, hi = np.minimum(v[:, 0], v[:, 1]), np.maximum(v[:, 0], v[:, 1])
+    side = rng.integers(0, 3, n)
+    far = geo.position.max(0) + 5
+    hi2 = hi.copy()
+    lo2 = lo.copy()
+    # half the boxes end exactly at a vertex coordinate on one axis and extend away from the mesh
+    for i in range(n // 2):
+        lo2[i, side[i]] = hi[i, side[i]]
+        hi2[i, side[i]] = far[side[i]]
+    eye = np.eye(4).reshape(-1)
+    return np.stack([record(lo2[i], hi2[i], eye) for i in range(n)])
+
+
+def _projective(rng, n, spread):
+    out = random_boxes(rng, n, np.zeros(3), spread)
+    out[:, 8 + 3] = rng.uniform(-0.01, 0.01, n)   # e[3]: a perspective term (non-affine)
+    out[:, 8 + 15] = rng.uniform(0.9, 1.1, n)
+    return out
+
+
+@pytest.mark.parametrize("indirect", [False, True])
+def test_intersects_box_matches_oracle(pkg, orc, cuda, indirect):
+    import torch
+
+    geo = pkg.torus_knot(10, 3, 300, 60, noise_sigma=0.02, noise_seed=3)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "indirect": indirect})
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+    rng = np.random.default_rng(23)
+    boxes = np.concatenate([random_boxes(rng, 20_000, np.zeros(3), 16.0),
+                            random_boxes(rng, 4_000, np.zeros(3), 16.0, shear=True),
+                            _projective(rng, 1_000, 16.0),
+                            _touching_boxes(rng, geo, 4_000)])
+    want = ref.intersects_box(boxes)
+    got = bvh.intersects_box_batch(boxes)
+    bad = np.nonzero(got != want)[0]
+    assert bad.size == 0, (bad[:10], boxes[bad[:2]])
+    assert 0.05 < want.mean() < 0.95
+    d = torch.from_numpy(boxes).to(cuda)
+    dev = bvh.intersects_box_batch(d)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy().astype(bool), got)
+    bvh.dispose()
+
+
+def test_intersects_box_lattice_ties(pkg, orc, cuda):
+    """Unit cubes on an integer lattice and integer-aligned boxes: faces coincide exactly."""
+    cube = pkg.box()
+    pos, idx, k = [], [], 0
+    for x in range(5):
+        for y in range(5):
+            for z in range(5):
+                pos.append(cube.position + np.array([x, y, z], np.float32) * 2)
+                idx.append(cube.index.astype(np.int64) + k)
+                k += cube.position.shape[0]
+    geo = pkg.Geometry(np.concatenate(pos), np.concatenate(idx).astype(np.uint32))
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, None, geo.position)
+    rng = np.random.default_rng(29)
+    n = 5000
+    lo = rng.integers(-2, 10, (n, 3)).astype(np.float32) - 0.5 * rng.integers(0, 2, (n, 3))
+    hi = lo + rng.integers(0, 3, (n, 3)).astype(np.float32) * 0.5
+    eye = np.eye(4).reshape(-1)
+    boxes = np.stack([record(lo[i], hi[i], eye) for i in range(n)])
+    want = ref.intersects_box(boxes)
+    got = bvh.intersects_box_batch(boxes)
+    assert np.array_equal(got, want), np.nonzero(got != want)[0][:10]
+    assert 0.05 < want.mean() < 0.95
+    bvh.dispose()

@@ -75,6 +75,7 @@ SIGNATURES = [
     ("bvhc_mesh_root_bytes", C.c_uint64, [_P, C.c_int]),
     ("bvhc_mesh_read_root", _I, [_P, C.c_int, _P, C.c_uint64]),
     ("bvhc_intersects_sphere", _I, [_P, _P, _U64, _P, _I, _P]),
+    ("bvhc_intersects_box", _I, [_P, _P, _U64, _P, _I, _P]),
     ("bvhc_hit_interpolate", _I, [_P, _P, _U64, _P, _U64, _I, _I, _P, _P, _I, _P]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),

@@ -1417,6 +1417,25 @@ bvhc_status bvhc_intersects_sphere(bvhc_mesh* m, const float* spheres, uint64_t 
   return read_and_clear_error(m, s);
 }
 
+bvhc_status bvhc_intersects_box(bvhc_mesh* m, const float* boxes, uint64_t n, uint8_t* out, int mem, void* stream) {
+  if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!boxes || !out) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(boxes, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_intersects_box(m->view(), boxes, n, out, s));
+  }
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 96));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, boxes, n * 96, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_intersects_box(m->view(), static_cast<const float*>(m->d_in), n,
+                                      static_cast<uint8_t*>(m->d_out), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n, cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint64_t n, float min_threshold,
                                         float max_threshold, bvhc_closest* out, int mem, void* stream) {
   if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;

@@ -14,6 +14,7 @@
 #include "kernels.cuh"
 #include "raykey.cuh"
 #include "robust.cuh"
+#include "softf64.cuh"
 
 namespace bvhc {
 namespace dev {
@@ -1071,6 +1072,359 @@ __global__ void __launch_bounds__(kBlock) intersects_sphere_kernel(MeshDev m, co
   out[i] = hit ? 1 : 0;
 }
 
+// ---------------------------------------------------------------------------------------------
+// intersectsBox (MeshBVH.js:780-792): an OrientedBox (src/math/OrientedBox.js:78-260) tested
+// against node boxes (OrientedBox.intersectsBox: the three aligned extents, then the box's three
+// edge directions) and triangles (OrientedBox.intersectsTriangle: the box's axes, the triangle's
+// normal and two edges (ExtendedTriangle.js:57-86), then the twelve cross products), every test a
+// SeparatingAxisBounds.isSeparated of two projection intervals.
+//
+// Each interval comparison is taken in float-float, whose values differ from the reference's
+// binary64 ones by less than 2^-37 M^k (M bounds every coordinate and transform term involved,
+// k the degree of the projection); it stands when the gap exceeds 2^-36 M^k (2^-34 M^3 for the
+// cross axes; a margin grown by the unit normal's direction error for axes built on it).  A test
+// with any comparison inside its margin, and every test of a non-affine box matrix, is evaluated
+// again with the reference's exact binary64 operation sequence (softf64.cuh).  A query is 24
+// floats: min xyz, pad, max xyz, pad, the column-major box-to-mesh matrix (three.js
+// Matrix4.elements).
+// ---------------------------------------------------------------------------------------------
+namespace obb {
+
+using sf::f64;
+
+struct ObbF {
+  ff3 p[8];               // corners, OrientedBox.update
+  ff3 ax[3];              // satAxes: p[0] - p[1 << i]
+  ff smin[3], smax[3];    // satBounds
+  ff amin[3], amax[3];    // alignedSatBounds
+  float mag;              // >= every |corner coordinate| and transform term
+  bool exact;             // non-affine matrix: binary64 throughout
+};
+
+__device__ __forceinline__ ff ff_min(ff a, ff b) { return ff_lt(b, a) ? b : a; }
+__device__ __forceinline__ ff ff_max(ff a, ff b) { return ff_lt(a, b) ? b : a; }
+__device__ __forceinline__ ff ff3_get(const ff3& v, int d) { return d == 0 ? v.x : (d == 1 ? v.y : v.z); }
+__device__ __forceinline__ float absmax3(float3 v) { return fmaxf(fabsf(v.x), fmaxf(fabsf(v.y), fabsf(v.z))); }
+
+__device__ __noinline__ void make_ff(const float* q, ObbF& o) {
+  const float* e = q + 8;
+  o.exact = !(e[3] == 0.0f && e[7] == 0.0f && e[11] == 0.0f && e[15] == 1.0f);
+  float mag = 0.0f;
+  for (int i = 0; i < 8; ++i) {
+    const float x = (i & 1) ? q[4] : q[0], y = (i & 2) ? q[5] : q[1], z = (i & 4) ? q[6] : q[2];
+    ff c[3];
+    for (int k = 0; k < 3; ++k) {
+      c[k] = ff_add(ff_add(ff_add(two_prod(e[k], x), two_prod(e[4 + k], y)), two_prod(e[8 + k], z)), ff_from(e[12 + k]));
+      mag = fmaxf(mag, fabsf(e[k] * x) + fabsf(e[4 + k] * y) + fabsf(e[8 + k] * z) + fabsf(e[12 + k]));
+    }
+    o.p[i] = {c[0], c[1], c[2]};
+  }
+  o.mag = mag * (1.0f + 0x1p-20f);
+  for (int i = 0; i < 3; ++i) {
+    o.ax[i] = ff3_sub(o.p[0], o.p[1 << i]);
+    o.smin[i] = o.smax[i] = ff3_dot(o.ax[i], o.p[0]);
+    for (int k = 1; k < 8; ++k) {
+      const ff v = ff3_dot(o.ax[i], o.p[k]);
+      o.smin[i] = ff_min(o.smin[i], v);
+      o.smax[i] = ff_max(o.smax[i], v);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    o.amin[d] = o.amax[d] = ff3_get(o.p[0], d);
+    for (int k = 1; k < 8; ++k) {
+      o.amin[d] = ff_min(o.amin[d], ff3_get(o.p[k], d));
+      o.amax[d] = ff_max(o.amax[d], ff3_get(o.p[k], d));
+    }
+  }
+}
+
+// 1: the intervals are separated, 0: they overlap, -1: within the margin.
+__device__ __forceinline__ int sep(ff amn, ff amx, ff bmn, ff bmx, float margin) {
+  const float d1 = ff_to_f(ff_sub(amn, bmx)), d2 = ff_to_f(ff_sub(bmn, amx));
+  if (d1 > margin || d2 > margin) return 1;
+  if (d1 < -margin && d2 < -margin) return 0;
+  return -1;
+}
+
+__device__ __forceinline__ void interval(const ff3& axis, const ff3* pts, int n, ff& mn, ff& mx) {
+  mn = mx = ff3_dot(axis, pts[0]);
+  for (int k = 1; k < n; ++k) {
+    const ff v = ff3_dot(axis, pts[k]);
+    mn = ff_min(mn, v);
+    mx = ff_max(mx, v);
+  }
+}
+
+// OrientedBox.intersectsBox on a node box: 1 meets, 0 separated, -1 undecided.
+__device__ __noinline__ int box_ff(const ObbF& o, const float* b) {
+  float m = o.mag;
+  for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(b[k]));
+  const float m1 = 0x1p-36f * m, m2 = 0x1p-36f * m * m;
+  bool undecided = false;
+  for (int d = 0; d < 3; ++d) {
+    const int r = sep(o.amin[d], o.amax[d], ff_from(b[d]), ff_from(b[d + 3]), m1);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  ff3 corners[8];
+  for (int k = 0; k < 8; ++k)
+    corners[k] = {ff_from((k & 1) ? b[0] : b[3]), ff_from((k & 2) ? b[1] : b[4]), ff_from((k & 4) ? b[2] : b[5])};
+  for (int i = 0; i < 3; ++i) {
+    ff mn, mx;
+    interval(o.ax[i], corners, 8, mn, mx);
+    const int r = sep(o.smin[i], o.smax[i], mn, mx, m2);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  return undecided ? -1 : 1;
+}
+
+// OrientedBox.intersectsTriangle: 1 meets, 0 separated, -1 undecided.
+__device__ __noinline__ int tri_ff(const ObbF& o, float3 a, float3 b, float3 c) {
+  const float m = fmaxf(o.mag, fmaxf(absmax3(a), fmaxf(absmax3(b), absmax3(c))));
+  const float m2 = 0x1p-36f * m * m, m3 = 0x1p-34f * m * m * m;
+  const ff3 tp[3] = {{ff_from(a.x), ff_from(a.y), ff_from(a.z)}, {ff_from(b.x), ff_from(b.y), ff_from(b.z)},
+                     {ff_from(c.x), ff_from(c.y), ff_from(c.z)}};
+  // the triangle's axes: unit normal (Triangle.getNormal), a - b, b - c, c - a (exact in float-float)
+  ff3 ta[4];
+  ta[1] = ff3_diff(a, b);
+  ta[2] = ff3_diff(b, c);
+  ta[3] = ff3_diff(c, a);
+  const ff3 raw = ff3_cross(ff3_diff(c, b), ff3_diff(a, b));
+  const ff l2 = ff3_dot(raw, raw);
+  // both cross products (the reference's binary64 one and this float-float one) are within
+  // 2^-43 M^2 of the exact one per component, so the unit normals differ in direction by at most
+  // rel = 2^-40 M^2 / |n|; a normal shorter than 2^-20 M^2 (or zero) goes to binary64
+  if (!(l2.hi > 0x1p-40f * m * m * m * m)) return -1;
+  const ff inv = ff_div(ff_from(1.0f), ff_sqrt(l2));
+  ta[0] = ff3_scale(raw, inv);
+  const float rel = 0x1p-40f * m * m * rsqrtf(l2.hi);
+  const float mn_normal = (0x1p-36f + 8.0f * rel) * 4.0f * m;
+  const float mn_cross_n = (0x1p-34f + 8.0f * rel) * 16.0f * m * m;
+  bool undecided = false;
+  for (int i = 0; i < 3; ++i) {
+    ff mn, mx;
+    interval(o.ax[i], tp, 3, mn, mx);
+    const int r = sep(o.smin[i], o.smax[i], mn, mx, m2);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  for (int i = 0; i < 3; ++i) {
+    ff tmn, tmx, bmn, bmx;
+    interval(ta[i], tp, 3, tmn, tmx);
+    interval(ta[i], o.p, 8, bmn, bmx);
+    const int r = sep(tmn, tmx, bmn, bmx, i == 0 ? mn_normal : m2);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 4; ++j) {
+      const ff3 axis = ff3_cross(o.ax[i], ta[j]);
+      ff tmn, tmx, bmn, bmx;
+      interval(axis, tp, 3, tmn, tmx);
+      interval(axis, o.p, 8, bmn, bmx);
+      const int r = sep(tmn, tmx, bmn, bmx, j == 0 ? mn_cross_n : m3);
+      if (r == 1) return 0;
+      undecided |= r < 0;
+    }
+  }
+  return undecided ? -1 : 1;
+}
+
+// --- the reference's exact binary64 sequence --------------------------------------------------
+
+struct V { f64 x, y, z; };
+__device__ __forceinline__ V vsub(V a, V b) { return {sf::sub(a.x, b.x), sf::sub(a.y, b.y), sf::sub(a.z, b.z)}; }
+__device__ __forceinline__ f64 vdot(V a, V b) {
+  return sf::add(sf::add(sf::mul(a.x, b.x), sf::mul(a.y, b.y)), sf::mul(a.z, b.z));
+}
+__device__ __forceinline__ V vcross(V a, V b) {
+  return {sf::sub(sf::mul(a.y, b.z), sf::mul(a.z, b.y)), sf::sub(sf::mul(a.z, b.x), sf::mul(a.x, b.z)),
+          sf::sub(sf::mul(a.x, b.y), sf::mul(a.y, b.x))};
+}
+__device__ __forceinline__ V vf(float3 p) { return {sf::from_f32(p.x), sf::from_f32(p.y), sf::from_f32(p.z)}; }
+__device__ __forceinline__ f64 vget(const V& v, int d) { return d == 0 ? v.x : (d == 1 ? v.y : v.z); }
+__device__ __forceinline__ bool separated(f64 amn, f64 amx, f64 bmn, f64 bmx) {  // isSeparated
+  return sf::lt(bmx, amn) || sf::lt(amx, bmn);
+}
+__device__ __forceinline__ void interval_d(V axis, const V* pts, int n, f64& mn, f64& mx) {  // setFromPoints
+  mn = sf::kInf;
+  mx = sf::neg(sf::kInf);
+  for (int k = 0; k < n; ++k) {
+    const f64 v = vdot(axis, pts[k]);
+    if (sf::lt(v, mn)) mn = v;
+    if (sf::lt(mx, v)) mx = v;
+  }
+}
+
+struct ObbD {
+  V p[8], ax[3];
+  f64 smin[3], smax[3], amin[3], amax[3];
+};
+
+__device__ __noinline__ void make_d(const float* q, ObbD& o) {
+  f64 e[16];
+  for (int k = 0; k < 16; ++k) e[k] = sf::from_f32(q[8 + k]);
+  for (int i = 0; i < 8; ++i) {
+    const f64 x = sf::from_f32((i & 1) ? q[4] : q[0]), y = sf::from_f32((i & 2) ? q[5] : q[1]),
+              z = sf::from_f32((i & 4) ? q[6] : q[2]);
+    const f64 w = sf::div(sf::kOne, sf::add(sf::add(sf::add(sf::mul(e[3], x), sf::mul(e[7], y)), sf::mul(e[11], z)), e[15]));
+    f64 c[3];
+    for (int k = 0; k < 3; ++k)
+      c[k] = sf::mul(sf::add(sf::add(sf::add(sf::mul(e[k], x), sf::mul(e[4 + k], y)), sf::mul(e[8 + k], z)), e[12 + k]), w);
+    o.p[i] = {c[0], c[1], c[2]};
+  }
+  for (int i = 0; i < 3; ++i) {
+    o.ax[i] = vsub(o.p[0], o.p[1 << i]);
+    interval_d(o.ax[i], o.p, 8, o.smin[i], o.smax[i]);
+  }
+  for (int d = 0; d < 3; ++d) {
+    o.amin[d] = sf::kInf;
+    o.amax[d] = sf::neg(sf::kInf);
+    for (int k = 0; k < 8; ++k) {
+      const f64 v = vget(o.p[k], d);
+      if (sf::lt(v, o.amin[d])) o.amin[d] = v;
+      if (sf::lt(o.amax[d], v)) o.amax[d] = v;
+    }
+  }
+}
+
+__device__ __forceinline__ f64 js_min(f64 a, f64 b) { return (sf::is_nan(a) || sf::is_nan(b)) ? sf::kNaN : (sf::lt(b, a) ? b : a); }
+__device__ __forceinline__ f64 js_max(f64 a, f64 b) { return (sf::is_nan(a) || sf::is_nan(b)) ? sf::kNaN : (sf::lt(a, b) ? b : a); }
+
+__device__ __noinline__ bool box_d(const ObbD& o, const float* b) {
+  for (int d = 0; d < 3; ++d)
+    if (separated(o.amin[d], o.amax[d], sf::from_f32(b[d]), sf::from_f32(b[d + 3]))) return false;
+  const f64 zero = 0, one = sf::kOne;
+  for (int i = 0; i < 3; ++i) {  // setFromBox: p = min * t + max * (1 - t), Math.min / Math.max
+    f64 mn = sf::kInf, mx = sf::neg(sf::kInf);
+    for (int x = 0; x <= 1; ++x)
+      for (int y = 0; y <= 1; ++y)
+        for (int z = 0; z <= 1; ++z) {
+          const f64 tx = x ? one : zero, ty = y ? one : zero, tz = z ? one : zero;
+          const V p{sf::add(sf::mul(sf::from_f32(b[0]), tx), sf::mul(sf::from_f32(b[3]), sf::sub(one, tx))),
+                    sf::add(sf::mul(sf::from_f32(b[1]), ty), sf::mul(sf::from_f32(b[4]), sf::sub(one, ty))),
+                    sf::add(sf::mul(sf::from_f32(b[2]), tz), sf::mul(sf::from_f32(b[5]), sf::sub(one, tz)))};
+          const f64 v = vdot(o.ax[i], p);
+          mn = js_min(v, mn);
+          mx = js_max(v, mx);
+        }
+    if (separated(o.smin[i], o.smax[i], mn, mx)) return false;
+  }
+  return true;
+}
+
+__device__ __noinline__ bool tri_d(const ObbD& o, float3 fa, float3 fb, float3 fc) {
+  const V a = vf(fa), b = vf(fb), c = vf(fc);
+  const V tp[3] = {a, b, c};
+  V n = vcross(vsub(c, b), vsub(a, b));  // Triangle.getNormal
+  const f64 l2 = vdot(n, n);
+  if (sf::lt(0, l2)) {
+    const f64 s = sf::div(sf::kOne, sf::sqrt(l2));
+    n = {sf::mul(n.x, s), sf::mul(n.y, s), sf::mul(n.z, s)};
+  } else {
+    n = {0, 0, 0};
+  }
+  const V ta[4] = {n, vsub(a, b), vsub(b, c), vsub(c, a)};
+  f64 mn, mx, mn2, mx2;
+  for (int i = 0; i < 3; ++i) {
+    interval_d(o.ax[i], tp, 3, mn, mx);
+    if (separated(o.smin[i], o.smax[i], mn, mx)) return false;
+  }
+  for (int i = 0; i < 3; ++i) {
+    interval_d(ta[i], tp, 3, mn, mx);
+    interval_d(ta[i], o.p, 8, mn2, mx2);
+    if (separated(mn, mx, mn2, mx2)) return false;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 4; ++j) {
+      const V axis = vcross(o.ax[i], ta[j]);
+      interval_d(axis, tp, 3, mn, mx);
+      interval_d(axis, o.p, 8, mn2, mx2);
+      if (separated(mn, mx, mn2, mx2)) return false;
+    }
+  return true;
+}
+
+}  // namespace obb
+
+__global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const float* __restrict__ boxes,
+                                                                uint64_t n, uint8_t* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float q[24];
+  for (int k = 0; k < 6; ++k) {
+    const float4 v = ld4(boxes + 24 * i + 4 * k);
+    q[4 * k] = v.x;
+    q[4 * k + 1] = v.y;
+    q[4 * k + 2] = v.z;
+    q[4 * k + 3] = v.w;
+  }
+  obb::ObbF o;
+  obb::make_ff(q, o);
+  obb::ObbD od;
+  bool have_d = false;
+  bool hit = false;
+  uint32_t stack[kMaxStack];
+  for (int root = 0; root < m.n_roots && !hit; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) {
+          for (uint32_t k = link & ~kLeafBit;; ++k) {
+            const Tri t = load_tri(m.tris, k);
+            int r = o.exact ? -1 : obb::tri_ff(o, t.a, t.b, t.c);
+            if (r < 0) {
+              if (!have_d) {
+                obb::make_d(q, od);
+                have_d = true;
+              }
+              r = obb::tri_d(od, t.a, t.b, t.c) ? 1 : 0;
+            }
+            if (r == 1) {
+              hit = true;
+              break;
+            }
+            if (t.flags & kTriLast) break;
+          }
+          if (hit) break;
+        }
+      } else {
+        const Pair pr = load_pair(m.nodes, link);
+        bool w[2];
+        for (int s = 0; s < 2; ++s) {
+          int r = o.exact ? -1 : obb::box_ff(o, s == 0 ? pr.l : pr.r);
+          if (r < 0) {
+            if (!have_d) {
+              obb::make_d(q, od);
+              have_d = true;
+            }
+            r = obb::box_d(od, s == 0 ? pr.l : pr.r) ? 1 : 0;
+          }
+          w[s] = r == 1;
+        }
+        if (w[0] && w[1]) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            break;
+          }
+          stack[sp++] = pr.lr;
+          link = pr.ll;
+          continue;
+        }
+        if (w[0] || w[1]) {
+          link = w[0] ? pr.ll : pr.lr;
+          continue;
+        }
+      }
+      if (sp == 0) break;
+      link = stack[--sp];
+    }
+  }
+  out[i] = hit ? 1 : 0;
+}
+
 // Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
 // queue length; the queue is then sorted by key so that a warp takes 32 nearby points.
 __global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n, SceneBox box,
@@ -1626,6 +1980,12 @@ cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uin
                                      cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   dev::intersects_sphere_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::intersects_box_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, boxes, n, out);
   return cudaGetLastError();
 }
 

@@ -113,6 +113,11 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
                                      cudaStream_t stream);
 
+// intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
+// 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.
+cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
+                                  cudaStream_t stream);
+
 // Vertex attribute at each hit (barycentric interpolation over the hit triangle's vertices, via
 // tri_vid: 3 vertex ids per triangle); rays (nullable, item_size 3) flip results that point along
 // the ray.  out: n x item_size.

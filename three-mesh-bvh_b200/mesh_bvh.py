@@ -511,6 +511,43 @@ class MeshBVH:
                 "bvhc_intersects_sphere")
         return out.astype(bool)
 
+    @staticmethod
+    def box_records(box_min, box_max, box_to_mesh) -> np.ndarray:
+        """Pack oriented boxes for intersects_box_batch: (n x 3) min, (n x 3) max and (n x 16)
+        column-major box-to-mesh matrices (three.js Matrix4.elements) -> (n x 24) float32."""
+        mn = np.asarray(box_min, dtype=np.float32).reshape(-1, 3)
+        mx = np.asarray(box_max, dtype=np.float32).reshape(-1, 3)
+        m = np.asarray(box_to_mesh, dtype=np.float32).reshape(-1, 16)
+        n = max(mn.shape[0], mx.shape[0], m.shape[0])
+        out = np.zeros((n, 24), dtype=np.float32)
+        out[:, 0:3], out[:, 4:7], out[:, 8:24] = mn, mx, m
+        return out
+
+    def intersects_box_batch(self, boxes, stream=None):
+        """intersectsBox for every row of `boxes` (n x 24, see box_records): numpy -> bool array;
+        torch CUDA tensor (float32) -> uint8 tensor, enqueued on `stream`."""
+        lib, mesh = N.lib(), self._device_mesh()
+        if self._is_torch(boxes):
+            import torch
+            bx = boxes.contiguous()
+            out = torch.empty(bx.shape[0], dtype=torch.uint8, device=bx.device)
+            s = stream if stream is not None else torch.cuda.current_stream(bx.device).cuda_stream
+            N.check(lib.bvhc_intersects_box(mesh, bx.data_ptr(), bx.shape[0], out.data_ptr(), N.MEM_DEVICE, s),
+                    "bvhc_intersects_box")
+            return out
+        bx = np.ascontiguousarray(boxes, dtype=np.float32).reshape(-1, 24)
+        out = np.empty(bx.shape[0], dtype=np.uint8)
+        N.check(lib.bvhc_intersects_box(mesh, _ptr(bx), bx.shape[0], _ptr(out), N.MEM_HOST, None),
+                "bvhc_intersects_box")
+        return out.astype(bool)
+
+    def intersectsBox(self, box, box_to_mesh) -> bool:
+        """MeshBVH#intersectsBox (MeshBVH.js:780-792); box: (min, max) or an object with `min` and
+        `max`; box_to_mesh: 16 column-major matrix elements (or an object with `elements`)."""
+        mn, mx = (box.min, box.max) if hasattr(box, "min") else box
+        el = getattr(box_to_mesh, "elements", box_to_mesh)
+        return bool(self.intersects_box_batch(self.box_records(mn, mx, el))[0])
+
     def intersectsSphere(self, sphere) -> bool:
         """MeshBVH#intersectsSphere (MeshBVH.js:796-809); sphere: (center, radius) or an object
         with `center` and `radius`."""
