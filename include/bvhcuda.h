@@ -269,6 +269,30 @@ bvhc_status bvhc_batch_graph_create(bvhc_mesh* batch, const float* rays, const u
 bvhc_status bvhc_graph_launch(bvhc_graph* graph, void* stream);
 void bvhc_graph_destroy(bvhc_graph* graph);
 
+/* Instances of a batch's geometries: the BatchedMesh raycast (acceleratedBatchedMeshRaycast,
+ * src/utils/ExtensionUtilities.js:87-161) with Raycaster.firstHitOnly, on world-space rays.
+ * Instance j shows geometry geometry[j] under the world matrix matrices[16 j .. 16 j + 15]
+ * (float64, column-major as three.js Matrix4.elements: the BatchedMesh's matrixWorld times the
+ * instance matrix; affine, else BVHC_ERR_UNSUPPORTED); visible (n bytes, NULL = all) is
+ * getVisibleAt.  The scene keeps a pointer to `batch`, which must outlive it; a tree over the
+ * instances' world boxes is built on the host.  bvhc_scene_set_instances replaces the instances
+ * (after the queries already enqueued have finished). */
+typedef struct bvhc_scene bvhc_scene;
+bvhc_status bvhc_scene_create(bvhc_mesh* batch, int n_instances, const uint32_t* geometry, const double* matrices,
+                              const uint8_t* visible, bvhc_scene** out);
+bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const uint32_t* geometry,
+                                     const double* matrices, const uint8_t* visible);
+/* For each world ray (n x 6 float32): each visible instance's raycastFirst in its local frame
+ * (MeshBVH.raycastObject3D, src/core/MeshBVH.js:447-494: the ray through the inverse matrix,
+ * direction normalised, near / far divided by |direction * world scale|), the hit point mapped
+ * back to world space with its distance from the ray origin (convertRaycastIntersect,
+ * src/utils/GeometryRayIntersectUtilities.js:3-17), and the closest of them (equal distances
+ * keep the lower instance).  hits: world distance and point, the geometry's faceIndex and local
+ * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none. */
+bvhc_status bvhc_scene_raycast_first(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
+                                     float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream);
+void bvhc_scene_destroy(bvhc_scene* scene);
+
 /* raycastFirst that allocates nothing.  No counterpart in the reference: it exists for callers
  * that must not call cudaMalloc -- code inside someone else's fixed device-memory budget, a
  * latency-critical thread where an allocation could stall or fail, or a host that allocates only

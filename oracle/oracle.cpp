@@ -1182,6 +1182,107 @@ void orc_intersects_sphere(const orc_bvh* h, const float* spheres, int64_t n, ui
   });
 }
 
+// ---------------------------------------------------------------------------------------------
+// Instanced raycastFirst: acceleratedBatchedMeshRaycast (ExtensionUtilities.js:87-161) with
+// firstHitOnly.  Every visible instance in order: the world ray into the instance's frame
+// (MeshBVH.raycastObject3D, MeshBVH.js:447-494: Ray.applyMatrix4 with the inverse matrix, the
+// direction normalised; near / far divided by |direction * world scale|), raycastFirst there, the
+// hit point back through the world matrix and the distance recomputed from the world origin
+// (convertRaycastIntersect, GeometryRayIntersectUtilities.js:3-17); then the closest hit, equal
+// distances keeping the lower instance (the raycaster's stable sort).
+// ---------------------------------------------------------------------------------------------
+// Inverse of a column-major 4x4 matrix by cofactors; all zeros when the determinant is 0.
+void invert4(const double* m, double* r) {
+  double inv[16];
+  inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] +
+           m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
+  inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] -
+           m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
+  inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] +
+           m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
+  inv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] -
+            m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
+  inv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] -
+           m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
+  inv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] +
+           m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
+  inv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] -
+           m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
+  inv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] +
+            m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
+  inv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] +
+           m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
+  inv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] -
+           m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
+  inv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] +
+            m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
+  inv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] -
+            m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
+  inv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] -
+           m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
+  inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] +
+           m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
+  inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] -
+            m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
+  inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] +
+            m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
+  double det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
+  if (det == 0) {
+    for (int k = 0; k < 16; ++k) r[k] = 0;
+    return;
+  }
+  for (int k = 0; k < 16; ++k) r[k] = inv[k] / det;
+}
+
+V3 transform_direction(V3 v, const double* e) {  // Vector3.transformDirection: 3x3 part, then normalise
+  V3 d{e[0] * v.x + e[4] * v.y + e[8] * v.z, e[1] * v.x + e[5] * v.y + e[9] * v.z, e[2] * v.x + e[6] * v.y + e[10] * v.z};
+  double len = std::sqrt(dot(d, d));
+  double s = 1 / (len != 0 ? len : 1);
+  return {d.x * s, d.y * s, d.z * s};
+}
+
+void orc_scene_raycast_first(const orc_bvh* const* geoms, int n_instances, const uint32_t* geometry,
+                             const double* matrices, const uint8_t* visible, const float* rays, int64_t n, int side,
+                             double near, double far, orc_hit* out, int64_t* instance, int threads) {
+  std::vector<double> inv((size_t)n_instances * 16);
+  for (int j = 0; j < n_instances; ++j) invert4(matrices + 16 * j, &inv[(size_t)16 * j]);
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    for (int64_t i = s; i < e; ++i) {
+      const Ray w = load_ray(rays + 6 * i);
+      orc_hit best;
+      best.face_index = -1;
+      best.distance = INF;
+      int64_t best_j = -1;
+      for (int j = 0; j < n_instances; ++j) {
+        if (visible && !visible[j]) continue;
+        const double* M = matrices + 16 * j;
+        const double* Mi = &inv[(size_t)16 * j];
+        Ray lr{apply_matrix4(w.o, Mi), transform_direction(w.d, Mi)};
+        const V3 ws{std::sqrt(M[0] * M[0] + M[1] * M[1] + M[2] * M[2]), std::sqrt(M[4] * M[4] + M[5] * M[5] + M[6] * M[6]),
+                    std::sqrt(M[8] * M[8] + M[9] * M[9] + M[10] * M[10])};
+        const V3 sd{lr.d.x * ws.x, lr.d.y * ws.y, lr.d.z * ws.z};
+        const double scale = std::sqrt(dot(sd, sd));
+        orc_hit h;
+        Counters c;
+        raycast_first(geoms[geometry[j]]->b, side, lr, near / scale, far / scale, &h, c);
+        if (h.face_index < 0) continue;
+        const V3 pw = apply_matrix4(V3{h.point[0], h.point[1], h.point[2]}, M);
+        const double dist = std::sqrt(dist_sq(pw, w.o));
+        if (best_j < 0 || dist < best.distance) {
+          best = h;
+          best.distance = dist;
+          best.point[0] = pw.x;
+          best.point[1] = pw.y;
+          best.point[2] = pw.z;
+          best_j = j;
+        }
+      }
+      out[i] = best;
+      instance[i] = best_j;
+    }
+  });
+}
+
 // boxes: n x 24 float32 (min xyz, pad, max xyz, pad, the column-major box-to-mesh matrix).
 void orc_intersects_box(const orc_bvh* h, const float* boxes, int64_t n, uint8_t* out, int64_t* node_reads,
                         int64_t* tri_tests, int threads) {

@@ -68,6 +68,7 @@ def lib():
         L.orc_refit.argtypes = [P, P, I64, I]
         L.orc_intersects_sphere.argtypes = [P, P, I64, P, P, P, I]
         L.orc_intersects_box.argtypes = [P, P, I64, P, P, P, I]
+        L.orc_scene_raycast_first.argtypes = [P, I, P, P, P, P, I64, I, D, D, P, P, I]
         _lib = L
     return _lib
 
@@ -254,3 +255,20 @@ def closest_point_triangle(p, a, b, c):
     out = np.zeros(3)
     lib().orc_closest_point_triangle(*[_p(x) for x in arrs], _p(out))
     return out
+
+
+def scene_raycast_first(geoms, geometry, matrices, rays, visible=None, side=0, near=0.0, far=math.inf, threads=None):
+    """Instanced raycastFirst (acceleratedBatchedMeshRaycast with firstHitOnly): geoms a list of
+    OracleBVH (one per geometry), geometry the geometry of each instance, matrices (n x 16,
+    column-major float64 world matrices), rays (m x 6 float32, world space).  Returns the world-space
+    hits (HIT_DTYPE, barycoord and face_index local) and the hit instance (-1: none)."""
+    gs = (C.c_void_p * len(geoms))(*[g.h for g in geoms])
+    geo = np.ascontiguousarray(geometry, dtype=np.uint32)
+    mats = np.ascontiguousarray(matrices, dtype=np.float64).reshape(-1, 16)
+    vis = None if visible is None else np.ascontiguousarray(visible, dtype=np.uint8)
+    r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+    out = np.empty(r.shape[0], dtype=HIT_DTYPE)
+    inst = np.empty(r.shape[0], dtype=np.int64)
+    lib().orc_scene_raycast_first(gs, mats.shape[0], _p(geo), _p(mats), _p(vis), _p(r), r.shape[0], side, near, far,
+                                  _p(out), _p(inst), threads or _threads())
+    return out, inst

@@ -128,6 +128,12 @@ class BatchedMeshBVH:
     def synchronize(self, stream=None):
         N.check(N.lib().bvhc_mesh_synchronize(self._device_mesh(), stream), "bvhc_mesh_synchronize")
 
+    def instances(self, geometry, matrices, visible=None) -> "InstancedScene":
+        """The BatchedMesh's instances: instance j shows geometry[j] under the world matrix
+        matrices[j] (16 column-major float64 elements: matrixWorld times the instance matrix);
+        visible: per-instance flags (getVisibleAt), None for all."""
+        return InstancedScene(self, geometry, matrices, visible)
+
     def dispose(self):
         for g in self._graphs:
             g.destroy()
@@ -154,3 +160,66 @@ class _Graph:
         if self.h:
             N.lib().bvhc_graph_destroy(self.h)
             self.h = None
+
+
+class InstancedScene:
+    """acceleratedBatchedMeshRaycast (ExtensionUtilities.js:87-161) with firstHitOnly on world
+    rays: each visible instance's raycastFirst in its own frame, hits back in world space, the
+    closest one kept, plus its instance (the Intersection's batchId)."""
+
+    def __init__(self, batch: BatchedMeshBVH, geometry, matrices, visible=None):
+        self.batch = batch  # the scene reads the batch's trees: keep it alive
+        self.h = None
+        out = C.c_void_p()
+        g, m, v = self._arrays(geometry, matrices, visible)
+        N.check(N.lib().bvhc_scene_create(batch._device_mesh(), g.size, g.ctypes.data, m.ctypes.data,
+                                          None if v is None else v.ctypes.data, C.byref(out)), "bvhc_scene_create")
+        self.h = out
+
+    @staticmethod
+    def _arrays(geometry, matrices, visible):
+        g = np.ascontiguousarray(geometry, dtype=np.uint32).reshape(-1)
+        m = np.ascontiguousarray(matrices, dtype=np.float64).reshape(-1, 16)
+        if m.shape[0] != g.size:
+            raise ValueError("one 16-element matrix per instance")
+        v = None if visible is None else np.ascontiguousarray(visible, dtype=np.uint8).reshape(-1)
+        return g, m, v
+
+    def set_instances(self, geometry, matrices, visible=None):
+        g, m, v = self._arrays(geometry, matrices, visible)
+        N.check(N.lib().bvhc_scene_set_instances(self.h, g.size, g.ctypes.data, m.ctypes.data,
+                                                 None if v is None else v.ctypes.data), "bvhc_scene_set_instances")
+
+    def raycast_first(self, rays, side=FrontSide, near=0.0, far=float("inf"), stream=None):
+        """World rays (n x 6 float32): numpy -> (hits structured array, instance ids); torch CUDA
+        tensor -> ((n, 8) float32 hit tensor, int32 instance tensor), enqueued on `stream`."""
+        lib = N.lib()
+        if hasattr(rays, "data_ptr"):
+            import torch
+            r = rays.contiguous()
+            hits = torch.empty((r.shape[0], 8), dtype=torch.float32, device=r.device)
+            inst = torch.empty(r.shape[0], dtype=torch.int32, device=r.device)
+            s = stream if stream is not None else torch.cuda.current_stream(r.device).cuda_stream
+            N.check(lib.bvhc_scene_raycast_first(self.h, r.data_ptr(), r.shape[0], _side_of(side), float(near),
+                                                 float(far), hits.data_ptr(), inst.data_ptr(), N.MEM_DEVICE, s),
+                    "bvhc_scene_raycast_first")
+            return hits, inst
+        from .mesh_bvh import HIT_DTYPE
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        hits = np.empty(r.shape[0], dtype=HIT_DTYPE)
+        inst = np.empty(r.shape[0], dtype=np.uint32)
+        N.check(lib.bvhc_scene_raycast_first(self.h, r.ctypes.data, r.shape[0], _side_of(side), float(near),
+                                             float(far), hits.ctypes.data, inst.ctypes.data, N.MEM_HOST, None),
+                "bvhc_scene_raycast_first")
+        return hits, inst
+
+    def dispose(self):
+        if self.h:
+            N.lib().bvhc_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass

@@ -1584,6 +1584,239 @@ void bvhc_graph_destroy(bvhc_graph* g) {
 int bvhc_batch_mesh_count(const bvhc_mesh* m) { return m ? m->n_meshes : 0; }
 
 // ---------------------------------------------------------------------------------------------
+// Instances (acceleratedBatchedMeshRaycast, ExtensionUtilities.js:87-161): world matrices of a
+// batch's geometries and a tree over their world boxes.
+// ---------------------------------------------------------------------------------------------
+struct bvhc_scene {
+  bvhc_mesh* batch = nullptr;
+  int n_instances = 0;
+  InstanceDev* d_inst = nullptr;
+  size_t inst_cap = 0;
+  PairNode* d_tlas = nullptr;
+  size_t tlas_cap = 0;
+  uint32_t root = kEmptyLeaf;
+  void* d_in = nullptr;
+  size_t in_cap = 0;
+  void* d_out = nullptr;
+  size_t out_cap = 0;
+  void* d_ids = nullptr;
+  size_t ids_cap = 0;
+};
+
+namespace {
+
+struct InstBox {
+  float lo[3], hi[3];
+  uint32_t id;
+};
+
+// Median split on the longest centroid extent down to one instance per leaf; the root record is
+// written first.  Returns the link of the subtree over boxes [a, b).
+uint32_t build_tlas(std::vector<InstBox>& boxes, size_t a, size_t b, std::vector<PairNode>& out) {
+  if (b - a == 1) return kLeafBit | boxes[a].id;
+  float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (size_t i = a; i < b; ++i)
+    for (int d = 0; d < 3; ++d) {
+      const float c = 0.5f * boxes[i].lo[d] + 0.5f * boxes[i].hi[d];
+      clo[d] = std::min(clo[d], c);
+      chi[d] = std::max(chi[d], c);
+    }
+  int axis = 0;
+  for (int d = 1; d < 3; ++d)
+    if (chi[d] - clo[d] > chi[axis] - clo[axis]) axis = d;
+  const size_t mid = a + (b - a) / 2;
+  std::nth_element(boxes.begin() + a, boxes.begin() + mid, boxes.begin() + b, [axis](const InstBox& x, const InstBox& y) {
+    return x.lo[axis] + x.hi[axis] < y.lo[axis] + y.hi[axis];
+  });
+  const size_t me = out.size();
+  out.emplace_back();
+  const uint32_t l = build_tlas(boxes, a, mid, out), r = build_tlas(boxes, mid, b, out);
+  PairNode& n = out[me];
+  for (int side = 0; side < 2; ++side) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = side ? mid : a; i < (side ? b : mid); ++i)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], boxes[i].lo[d]);
+        hi[d] = std::max(hi[d], boxes[i].hi[d]);
+      }
+    for (int d = 0; d < 3; ++d) {
+      n.f[6 * side + d] = lo[d];
+      n.f[6 * side + 3 + d] = hi[d];
+    }
+  }
+  n.link[0] = l;
+  n.link[1] = r;
+  n.axis = (uint32_t)axis;
+  n.pad = 0;
+  return (uint32_t)me;
+}
+
+void split_ff(double x, float& hi, float& lo) {
+  hi = (float)x;
+  lo = (float)(x - (double)hi);
+}
+
+float round_down(double x) {
+  float f = (float)x;
+  return (double)f > x ? std::nextafter(f, -INFINITY) : f;
+}
+float round_up(double x) {
+  float f = (float)x;
+  return (double)f < x ? std::nextafter(f, INFINITY) : f;
+}
+
+bvhc_status set_instances(bvhc_scene* sc, int n, const uint32_t* geometry, const double* matrices,
+                          const uint8_t* visible) {
+  bvhc_mesh* m = sc->batch;
+  if (n < 0 || (n > 0 && (!geometry || !matrices))) return BVHC_ERR_INVALID_ARGUMENT;
+  // each geometry's local box: the union of its roots' boxes
+  const std::vector<float> root_boxes = serialized_root_boxes(m);
+  std::vector<double> gbox((size_t)m->n_meshes * 6);
+  for (int g = 0; g < m->n_meshes; ++g) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t r = m->mesh_root_off[g]; r < m->mesh_root_off[g + 1]; ++r)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(lo[d], (double)root_boxes[6 * r + d]);
+        hi[d] = std::max(hi[d], (double)root_boxes[6 * r + 3 + d]);
+      }
+    for (int d = 0; d < 3; ++d) {
+      gbox[6 * g + d] = lo[d];
+      gbox[6 * g + 3 + d] = hi[d];
+    }
+  }
+  std::vector<InstanceDev> inst((size_t)n);
+  std::vector<InstBox> boxes;
+  for (int j = 0; j < n; ++j) {
+    if (geometry[j] >= (uint32_t)m->n_meshes) return BVHC_ERR_INVALID_ARGUMENT;
+    const double* e = matrices + 16 * (size_t)j;  // column-major: e[col * 4 + row]
+    for (int k = 0; k < 16; ++k)
+      if (!std::isfinite(e[k])) return BVHC_ERR_INVALID_ARGUMENT;
+    if (e[3] != 0 || e[7] != 0 || e[11] != 0 || e[15] != 1) return BVHC_ERR_UNSUPPORTED;  // affine only
+    InstanceDev& I = inst[j];
+    I.geometry = geometry[j];
+    // inverse of the affine matrix: inverse 3x3 (adjugate / determinant), translation -inv * t
+    const double a00 = e[0], a01 = e[4], a02 = e[8], a10 = e[1], a11 = e[5], a12 = e[9], a20 = e[2], a21 = e[6],
+                 a22 = e[10];
+    const double c00 = a11 * a22 - a12 * a21, c01 = a02 * a21 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+    const double c10 = a12 * a20 - a10 * a22, c11 = a00 * a22 - a02 * a20, c12 = a02 * a10 - a00 * a12;
+    const double c20 = a10 * a21 - a11 * a20, c21 = a01 * a20 - a00 * a21, c22 = a00 * a11 - a01 * a10;
+    const double det = a00 * c00 + a01 * c10 + a02 * c20;
+    const double rows[3][4] = {{a00, a01, a02, e[12]}, {a10, a11, a12, e[13]}, {a20, a21, a22, e[14]}};
+    double inv[3][4] = {{c00, c01, c02, 0}, {c10, c11, c12, 0}, {c20, c21, c22, 0}};
+    for (int r = 0; r < 3; ++r) {
+      for (int c = 0; c < 3; ++c) inv[r][c] = det != 0 ? inv[r][c] / det : 0;
+      inv[r][3] = -(inv[r][0] * e[12] + inv[r][1] * e[13] + inv[r][2] * e[14]);
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) {
+        split_ff(rows[r][c], I.m_hi[4 * r + c], I.m_lo[4 * r + c]);
+        split_ff(inv[r][c], I.inv_hi[4 * r + c], I.inv_lo[4 * r + c]);
+      }
+    for (int c = 0; c < 3; ++c)
+      I.scale[c] = (float)std::sqrt(e[4 * c] * e[4 * c] + e[4 * c + 1] * e[4 * c + 1] + e[4 * c + 2] * e[4 * c + 2]);
+    // a singular matrix maps every ray to a zero direction: the instance is never hit
+    if ((visible && !visible[j]) || det == 0) continue;
+    const double* gb = &gbox[6 * (size_t)geometry[j]];
+    if (!(gb[0] <= gb[3])) continue;
+    InstBox b;
+    b.id = (uint32_t)j;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int k = 0; k < 8; ++k) {
+      const double x = gb[(k & 1) ? 3 : 0], y = gb[(k & 2) ? 4 : 1], z = gb[(k & 4) ? 5 : 2];
+      for (int r = 0; r < 3; ++r) {
+        const double v = rows[r][0] * x + rows[r][1] * y + rows[r][2] * z + rows[r][3];
+        lo[r] = std::min(lo[r], v);
+        hi[r] = std::max(hi[r], v);
+      }
+    }
+    for (int d = 0; d < 3; ++d) {  // widened so that rounding of the corners cannot cut a hit
+      const double pad = 1e-6 * (hi[d] - lo[d]) + 1e-6 * std::max(std::fabs(lo[d]), std::fabs(hi[d]));
+      b.lo[d] = round_down(lo[d] - pad);
+      b.hi[d] = round_up(hi[d] + pad);
+    }
+    boxes.push_back(b);
+  }
+  std::vector<PairNode> nodes;
+  uint32_t root = kEmptyLeaf;
+  if (!boxes.empty()) root = build_tlas(boxes, 0, boxes.size(), nodes);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  if (n > 0) {
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&sc->d_inst), &sc->inst_cap, inst.size() * sizeof(InstanceDev)));
+    BVHC_CUDA_TRY(cudaMemcpy(sc->d_inst, inst.data(), inst.size() * sizeof(InstanceDev), cudaMemcpyHostToDevice));
+  }
+  if (!nodes.empty()) {
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&sc->d_tlas), &sc->tlas_cap, nodes.size() * sizeof(PairNode)));
+    BVHC_CUDA_TRY(cudaMemcpy(sc->d_tlas, nodes.data(), nodes.size() * sizeof(PairNode), cudaMemcpyHostToDevice));
+  }
+  sc->root = root;
+  sc->n_instances = n;
+  return BVHC_OK;
+}
+
+}  // namespace
+
+bvhc_status bvhc_scene_create(bvhc_mesh* batch, int n_instances, const uint32_t* geometry, const double* matrices,
+                              const uint8_t* visible, bvhc_scene** out) {
+  if (!batch || !out || batch->n_meshes <= 0 || batch->h_root_bytes.empty()) return BVHC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  auto* sc = new (std::nothrow) bvhc_scene();
+  if (!sc) return BVHC_ERR_OUT_OF_MEMORY;
+  sc->batch = batch;
+  bvhc_status st = set_instances(sc, n_instances, geometry, matrices, visible);
+  if (st != BVHC_OK) {
+    bvhc_scene_destroy(sc);
+    return st;
+  }
+  *out = sc;
+  return BVHC_OK;
+}
+
+bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const uint32_t* geometry,
+                                     const double* matrices, const uint8_t* visible) {
+  if (!scene) return BVHC_ERR_INVALID_ARGUMENT;
+  BVHC_CUDA_TRY(cudaSetDevice(scene->batch->device));
+  BVHC_CUDA_TRY(cudaDeviceSynchronize());  // earlier queries may still read the instance arrays
+  return set_instances(scene, n_instances, geometry, matrices, visible);
+}
+
+bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t n, int side, float near_dist,
+                                     float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream) {
+  if (!sc || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
+  if (side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!rays || !hits || !instance) return BVHC_ERR_INVALID_ARGUMENT;
+  bvhc_mesh* m = sc->batch;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  const SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(rays, 8) || !aligned(hits, 16) || !aligned(instance, 4)) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_scene_raycast_first(m->view(), sd, rays, n, side, near_dist, far_dist, hits, instance, s));
+  }
+  BVHC_CUDA_TRY(ensure(&sc->d_in, &sc->in_cap, n * 24));
+  BVHC_CUDA_TRY(ensure(&sc->d_out, &sc->out_cap, n * sizeof(bvhc_hit)));
+  BVHC_CUDA_TRY(ensure(&sc->d_ids, &sc->ids_cap, n * 4));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(sc->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_scene_raycast_first(m->view(), sd, static_cast<const float*>(sc->d_in), n, side, near_dist,
+                                           far_dist, static_cast<bvhc_hit*>(sc->d_out),
+                                           static_cast<uint32_t*>(sc->d_ids), s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(hits, sc->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(instance, sc->d_ids, n * 4, cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
+void bvhc_scene_destroy(bvhc_scene* sc) {
+  if (!sc) return;
+  if (sc->batch) cudaSetDevice(sc->batch->device);
+  cudaFree(sc->d_inst);
+  cudaFree(sc->d_tlas);
+  cudaFree(sc->d_in);
+  cudaFree(sc->d_out);
+  cudaFree(sc->d_ids);
+  delete sc;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Gradients
 // ---------------------------------------------------------------------------------------------
 bvhc_status bvhc_mesh_enable_gradients(bvhc_mesh* m, const void* index, int index_elem_bytes, uint64_t index_count,

@@ -1425,6 +1425,214 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
   out[i] = hit ? 1 : 0;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Instanced raycastFirst: acceleratedBatchedMeshRaycast (ExtensionUtilities.js:87-161) with
+// firstHitOnly, each instance through MeshBVH.raycastObject3D (MeshBVH.js:447-494) and
+// convertRaycastIntersect (GeometryRayIntersectUtilities.js:3-17), then the closest world hit
+// (the raycaster's stable sort by distance: equal distances keep the lower instance index).
+//
+// Two levels: a tree over the instances' world boxes, and for every instance box the ray enters,
+// the instance's geometry tree in its local frame.  The local ray is the reference's: origin
+// through the inverse matrix, direction through its 3 x 3 part and normalised
+// (Ray.applyMatrix4 / Vector3.transformDirection), computed in float-float from the binary64
+// inverse and rounded once; near and far are divided by |direction * world scale|.  The local
+// hit point goes back through the world matrix and the world distance is |point - origin|.
+// Instance boxes and local traversals are pruned by the closest world hit so far.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ RayF ray_from(float3 o, float3 d) {
+  RayF r;
+  r.o = o;
+  r.d = d;
+  const float dx = fabsf(d.x) < kTiny ? copysignf(kTiny, d.x) : d.x;
+  const float dy = fabsf(d.y) < kTiny ? copysignf(kTiny, d.y) : d.y;
+  const float dz = fabsf(d.z) < kTiny ? copysignf(kTiny, d.z) : d.z;
+  r.inv = make_float3(__frcp_rn(dx), __frcp_rn(dy), __frcp_rn(dz));
+  r.d_l1 = fabsf(d.x) + fabsf(d.y) + fabsf(d.z);
+  return r;
+}
+
+__device__ __forceinline__ ff row_apply(const float* hi, const float* lo, int row, ff x, ff y, ff z, bool affine_t) {
+  const int k = row * 4;
+  ff s = ff_add(ff_add(ff_mul({hi[k], lo[k]}, x), ff_mul({hi[k + 1], lo[k + 1]}, y)), ff_mul({hi[k + 2], lo[k + 2]}, z));
+  return affine_t ? ff_add(s, ff{hi[k + 3], lo[k + 3]}) : s;
+}
+
+// The per-thread raycastFirst walk of one geometry's roots (the simple kernel's loop, nearest
+// child first).  Returns false on a stack overflow.
+__device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const RayF& r, float dlen, int side,
+                           const SideTable& sides, float near_d, float far_d, Best& best) {
+  uint32_t stack_link[kMaxStack];
+  float stack_t[kMaxStack];
+  for (uint32_t root = r0; root < r1; ++root) {
+    uint32_t link = m.roots[root];
+    int sp = 0;
+    for (;;) {
+      if (link & kLeafBit) {
+        if (link != kEmptyLeaf) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
+      } else {
+        const Pair p = load_pair(m.nodes, link);
+        const float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
+        float e0, e1;
+        const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, near_d, lim, e0);
+        const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, near_d, lim, e1);
+        const bool lf = e0 <= e1;
+        const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+        const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+        if (h1st) {
+          if (h2nd) {
+            if (sp >= kMaxStack) return false;
+            stack_link[sp] = c2;
+            stack_t[sp] = lf ? e1 : e0;
+            ++sp;
+          }
+          link = c1;
+          continue;
+        }
+        if (h2nd) {
+          link = c2;
+          continue;
+        }
+      }
+      bool found = false;
+      const float lim = (best.t + best.err) * (1.0f + kSlabMargin);
+      while (sp > 0) {
+        --sp;
+        if (stack_t[sp] <= lim) {
+          link = stack_link[sp];
+          found = true;
+          break;
+        }
+      }
+      if (!found) break;
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kBlock) scene_raycast_first_kernel(MeshDev m, SceneDev sc, const float* __restrict__ rays,
+                                                                     uint64_t n, int side, float near_d, float far_d,
+                                                                     bvhc_hit* __restrict__ out,
+                                                                     uint32_t* __restrict__ inst_out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RayF w = make_ray(rays, i);
+  const float wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
+  const SideTable no_sides{};
+  bvhc_hit best_hit;
+  ff best_dist = ff_from(kInf);
+  uint32_t best_inst = 0xFFFFFFFFu;
+  uint32_t stack_link[kMaxStack];
+  float stack_t[kMaxStack];
+  int sp = 0;
+  uint32_t link = sc.root;
+  if (link == kEmptyLeaf) {
+    store_miss(out + i);
+    inst_out[i] = 0xFFFFFFFFu;
+    return;
+  }
+  const ff ox = ff_from(w.o.x), oy = ff_from(w.o.y), oz = ff_from(w.o.z);
+  const ff dx = ff_from(w.d.x), dy = ff_from(w.d.y), dz = ff_from(w.d.z);
+  for (;;) {
+    if (link & kLeafBit) {
+      const uint32_t j = link & ~kLeafBit;
+      const InstanceDev& I = sc.inst[j];
+      // the local ray (Ray.applyMatrix4 with the inverse world matrix)
+      const ff lox = row_apply(I.inv_hi, I.inv_lo, 0, ox, oy, oz, true);
+      const ff loy = row_apply(I.inv_hi, I.inv_lo, 1, ox, oy, oz, true);
+      const ff loz = row_apply(I.inv_hi, I.inv_lo, 2, ox, oy, oz, true);
+      const ff vx = row_apply(I.inv_hi, I.inv_lo, 0, dx, dy, dz, false);
+      const ff vy = row_apply(I.inv_hi, I.inv_lo, 1, dx, dy, dz, false);
+      const ff vz = row_apply(I.inv_hi, I.inv_lo, 2, dx, dy, dz, false);
+      const ff vlen = ff_sqrt(ff_add(ff_add(ff_mul(vx, vx), ff_mul(vy, vy)), ff_mul(vz, vz)));
+      if (vlen.hi > 0.0f) {
+        const float3 ld = make_float3(ff_to_f(ff_div(vx, vlen)), ff_to_f(ff_div(vy, vlen)), ff_to_f(ff_div(vz, vlen)));
+        const float3 lo = make_float3(ff_to_f(lox), ff_to_f(loy), ff_to_f(loz));
+        const float sx = ld.x * I.scale[0], sy = ld.y * I.scale[1], sz = ld.z * I.scale[2];
+        const float sf_ = sqrtf(sx * sx + sy * sy + sz * sz);
+        const float lnear = near_d / sf_, lfar = far_d / sf_;
+        // local t per world distance: world distance = t |d| / |v| (affine matrix)
+        const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * vlen.hi / wlen * (1.0f + 0x1p-16f);
+        const RayF lr = ray_from(lo, ld);
+        const float llen = sqrtf(ld.x * ld.x + ld.y * ld.y + ld.z * ld.z);
+        Best b{kInf, 0.0f, 0xFFFFFFFFu};
+        const uint32_t g = I.geometry;
+        if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], lr, llen, side, no_sides, lnear,
+                        fminf(lfar, tlim), b)) {
+          atomicOr(m.err, kErrStackOverflow);
+          break;
+        }
+        if (b.rec != 0xFFFFFFFFu) {
+          const Tri t = load_tri(m.tris, b.rec);
+          const ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, lr.o, lr.d));
+          bvhc_hit h;
+          make_hit(t, lr, tt, ff_mul(tt, dir_length(lr.d)), h);
+          // the local point (Ray.at) back to world space, and its distance from the world origin
+          const ff px = ff_add(ff_from(lr.o.x), ff_mul_f(tt, lr.d.x));
+          const ff py = ff_add(ff_from(lr.o.y), ff_mul_f(tt, lr.d.y));
+          const ff pz = ff_add(ff_from(lr.o.z), ff_mul_f(tt, lr.d.z));
+          const ff wx = row_apply(I.m_hi, I.m_lo, 0, px, py, pz, true);
+          const ff wy = row_apply(I.m_hi, I.m_lo, 1, px, py, pz, true);
+          const ff wz = row_apply(I.m_hi, I.m_lo, 2, px, py, pz, true);
+          const ff ex = ff_sub(wx, ox), ey = ff_sub(wy, oy), ez = ff_sub(wz, oz);
+          const ff dist = ff_sqrt(ff_add(ff_add(ff_mul(ex, ex), ff_mul(ey, ey)), ff_mul(ez, ez)));
+          if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
+            best_dist = dist;
+            best_inst = j;
+            best_hit = h;
+            best_hit.distance = ff_to_f(dist);
+            best_hit.point[0] = ff_to_f(wx);
+            best_hit.point[1] = ff_to_f(wy);
+            best_hit.point[2] = ff_to_f(wz);
+          }
+        }
+      }
+    } else {
+      const Pair p = load_pair(sc.nodes, link);
+      const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+      float e0, e1;
+      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e0);
+      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e1);
+      const bool lf = e0 <= e1;
+      const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+      const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+      if (h1st) {
+        if (h2nd) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            break;
+          }
+          stack_link[sp] = c2;
+          stack_t[sp] = lf ? e1 : e0;
+          ++sp;
+        }
+        link = c1;
+        continue;
+      }
+      if (h2nd) {
+        link = c2;
+        continue;
+      }
+    }
+    bool found = false;
+    const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= lim) {
+        link = stack_link[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  if (best_inst == 0xFFFFFFFFu) {
+    store_miss(out + i);
+  } else {
+    store_hit(out + i, best_hit);
+  }
+  inst_out[i] = best_inst;
+}
+
 // Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
 // queue length; the queue is then sorted by key so that a warp takes 32 nearby points.
 __global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n, SceneBox box,
@@ -1980,6 +2188,15 @@ cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uin
                                      cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   dev::intersects_sphere_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
+                                       int side, float near_d, float far_d, bvhc_hit* hits, uint32_t* instance,
+                                       cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::scene_raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, side, near_d, far_d,
+                                                                          hits, instance);
   return cudaGetLastError();
 }
 

@@ -113,6 +113,29 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
                                      cudaStream_t stream);
 
+// Instances of a batch's geometries (bvhc_scene_*).  Matrices are the affine rows 0..2 of the
+// instance's world matrix, row-major 3 x 4 (x' = r0 x + r1 y + r2 z + r3), as float-float pairs
+// of the binary64 values, and the same for its inverse.
+struct InstanceDev {
+  float m_hi[12], m_lo[12];
+  float inv_hi[12], inv_lo[12];
+  float scale[3];     // column lengths of the world matrix (Vector3.setFromMatrixScale)
+  uint32_t geometry;  // batch geometry: roots [mesh_root_off[g], mesh_root_off[g + 1])
+};
+// The instance tree (TLAS): child-pair records over instance world boxes; a leaf link is
+// kLeafBit | instance.  root == kEmptyLeaf: no visible instance.
+struct SceneDev {
+  const PairNode* nodes;
+  uint32_t root;
+  const InstanceDev* inst;
+  const uint32_t* mesh_root_off;
+};
+// World-space raycastFirst over the instances: hits[i] in world space (distance, point; local
+// barycoord and faceIndex), instance[i] the hit instance (0xFFFFFFFF: none).
+cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
+                                       int side, float near_d, float far_d, bvhc_hit* hits, uint32_t* instance,
+                                       cudaStream_t stream);
+
 // intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
 // 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.
 cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
