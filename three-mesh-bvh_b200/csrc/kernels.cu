@@ -1566,13 +1566,42 @@ __global__ void __launch_bounds__(kBlock) scene_raycast_first_kernel(MeshDev m, 
           const ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, lr.o, lr.d));
           bvhc_hit h;
           make_hit(t, lr, tt, ff_mul(tt, dir_length(lr.d)), h);
-          // the local point (Ray.at) back to world space, and its distance from the world origin
-          const ff px = ff_add(ff_from(lr.o.x), ff_mul_f(tt, lr.d.x));
-          const ff py = ff_add(ff_from(lr.o.y), ff_mul_f(tt, lr.d.y));
-          const ff pz = ff_add(ff_from(lr.o.z), ff_mul_f(tt, lr.d.z));
-          const ff wx = row_apply(I.m_hi, I.m_lo, 0, px, py, pz, true);
-          const ff wy = row_apply(I.m_hi, I.m_lo, 1, px, py, pz, true);
-          const ff wz = row_apply(I.m_hi, I.m_lo, 2, px, py, pz, true);
+          // The reported record in world space: an affine map keeps barycentric coordinates and
+          // maps the local hit point to the world one, so the triangle is carried to world space
+          // (float-float) and met with the exact world ray.  This avoids the rounding of the
+          // local ray to float32, which the reference (local ray in float64) does not have.
+          ff3 P[3];
+          const float3 V3s[3] = {t.a, t.b, t.c};
+          for (int k = 0; k < 3; ++k) {
+            const ff vx = ff_from(V3s[k].x), vy = ff_from(V3s[k].y), vz = ff_from(V3s[k].z);
+            P[k] = {row_apply(I.m_hi, I.m_lo, 0, vx, vy, vz, true), row_apply(I.m_hi, I.m_lo, 1, vx, vy, vz, true),
+                    row_apply(I.m_hi, I.m_lo, 2, vx, vy, vz, true)};
+          }
+          const ff3 O{ox, oy, oz}, D{dx, dy, dz};
+          const ff3 e1 = ff3_sub(P[1], P[0]), e2 = ff3_sub(P[2], P[0]), qv = ff3_sub(O, P[0]);
+          const ff3 nn = ff3_cross(e1, e2);
+          const ff N = ff3_dot(D, nn);
+          ff wx, wy, wz;
+          if (N.hi != 0.0f) {
+            const ff U = ff3_dot(D, ff3_cross(qv, e2)), Vv = ff3_dot(D, ff3_cross(e1, qv));
+            const ff W = ff_sub(ff_sub(N, U), Vv);
+            const ff tw = ff_div(ff_neg(ff3_dot(qv, nn)), N);
+            wx = ff_add(ox, ff_mul(tw, dx));
+            wy = ff_add(oy, ff_mul(tw, dy));
+            wz = ff_add(oz, ff_mul(tw, dz));
+            if (h.barycoord[0] != 0.0f || h.barycoord[1] != 0.0f || h.barycoord[2] != 0.0f) {
+              h.barycoord[0] = ff_to_f(ff_div(W, N));
+              h.barycoord[1] = ff_to_f(ff_div(U, N));
+              h.barycoord[2] = ff_to_f(ff_div(Vv, N));
+            }
+          } else {  // the world ray lies in the triangle's plane at float-float resolution
+            const ff px = ff_add(ff_from(lr.o.x), ff_mul_f(tt, lr.d.x));
+            const ff py = ff_add(ff_from(lr.o.y), ff_mul_f(tt, lr.d.y));
+            const ff pz = ff_add(ff_from(lr.o.z), ff_mul_f(tt, lr.d.z));
+            wx = row_apply(I.m_hi, I.m_lo, 0, px, py, pz, true);
+            wy = row_apply(I.m_hi, I.m_lo, 1, px, py, pz, true);
+            wz = row_apply(I.m_hi, I.m_lo, 2, px, py, pz, true);
+          }
           const ff ex = ff_sub(wx, ox), ey = ff_sub(wy, oy), ez = ff_sub(wz, oz);
           const ff dist = ff_sqrt(ff_add(ff_add(ff_mul(ex, ex), ff_mul(ey, ey)), ff_mul(ez, ez)));
           if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
