@@ -42,10 +42,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all", "build"], default="first",
+    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all", "build", "scene"],
+                    default="first",
                     help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form; "
                          "adjoint: forward/backward timing; closest: the 256^3 closest-point grid; all: raycast "
-                         "(all hits); build: the device SAH build")
+                         "(all hits); build: the device SAH build; scene: instanced BatchedMesh raycastFirst")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
@@ -758,6 +759,115 @@ def run_adjoint(args, ws, rank, local):
     bvh_star.dispose()
 
 
+def run_scene(args, ws, rank, local):
+    """Instanced BatchedMesh raycastFirst on world rays: 256 geometries (the batched generator:
+    torus knots and icospheres, log-uniform 200..200,000 triangles), 4096 instances with random
+    rotations, uniform scales 0.5..2 and positions in [-1000, 1000]^3, 2^22 world rays from a
+    sphere of radius 2500 towards uniform points of the instance cube."""
+    import torch
+
+    import __graft_entry__ as ge
+    from three_mesh_bvh_b200.batched import BatchedMeshBVH
+
+    pkg = ge.load_package()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_geo, n_inst, n_rays = 256, 4096, 1 << 22
+    geoms, _, _, _ = pkg.batched_scene(n_geometries=n_geo, tri_range=(200, 200_000), seed=2, make_rays=False)
+    batch = BatchedMeshBVH(geoms, {"strategy": pkg.SAH, "maxLeafSize": 10}, threads=os.cpu_count() or 1)
+    rng = np.random.default_rng(3 + rank)
+    geometry = rng.integers(0, n_geo, n_inst).astype(np.uint32)
+    mats = np.zeros((n_inst, 16))
+    for j in range(n_inst):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        x, y, z, w = q
+        rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                        [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                        [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]]) * rng.uniform(0.5, 2.0)
+        m = np.eye(4)
+        m[:3, :3] = rot
+        m[:3, 3] = rng.uniform(-1000, 1000, 3)
+        mats[j] = m.T.reshape(-1)
+    u = rng.normal(size=(n_rays, 3))
+    o = u / np.linalg.norm(u, axis=1, keepdims=True) * 2500.0
+    d = rng.uniform(-1000, 1000, (n_rays, 3)) - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays_h = np.concatenate([o, d], 1).astype(np.float32)
+    scene = batch.instances(geometry, mats)
+    rays = torch.from_numpy(rays_h).to(dev)
+    hits = torch.empty((n_rays, 8), dtype=torch.float32, device=dev)
+    inst = torch.empty(n_rays, dtype=torch.int32, device=dev)
+    lib = pkg.lib()
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+
+    def step():
+        lib.bvhc_scene_raycast_first(scene.h, rays.data_ptr(), n_rays, 0, 0.0, math.inf, hits.data_ptr(),
+                                     inst.data_ptr(), 1, s)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        a.record(stream)
+        for _ in range(args.steps):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = max_over_ranks(a.elapsed_time(b) / args.steps, ws, dev)
+    hit_frac = float((inst.cpu().numpy() >= 0).mean())
+    # end to end: host rays in, host hits and instance ids out (pinned), through the public call
+    pin_r = torch.from_numpy(rays_h).pin_memory()
+    pin_h = torch.empty((n_rays, 8), dtype=torch.float32).pin_memory()
+    pin_i = torch.empty(n_rays, dtype=torch.int32).pin_memory()
+    e2e = []
+    for _ in range(max(1, args.steps // 2)):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        lib.bvhc_scene_raycast_first(scene.h, pin_r.data_ptr(), n_rays, 0, 0.0, math.inf, pin_h.data_ptr(),
+                                     pin_i.data_ptr(), 0, None)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(float(np.median(e2e)), ws, dev)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle.oracle as orc
+
+        oracles, r0 = [], 0
+        for k in range(batch.n_meshes):
+            roots = batch.roots[r0:r0 + batch.roots_per_mesh[k]]
+            r0 += batch.roots_per_mesh[k]
+            oracles.append(orc.OracleBVH.from_serialized(roots, batch.index, None, batch.position))
+        idx = np.linspace(0, n_rays - 1, 1 << 14).astype(np.int64)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        orc.scene_raycast_first(oracles, geometry, mats, rays_h[idx], threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": idx.size / dt / 1e6, "unit": "Mrays/s", "cores": threads, "kind": "port",
+               "sample": f"{idx.size} evenly strided rays; the float64 oracle loops over every instance per ray, "
+                         "as the reference's BatchedMesh raycast does"}
+    if rank == 0:
+        line = {"metric": "Mrays/s instanced raycastFirst (256 geometries, 4096 instances)",
+                "value": weak_scaling_rate(ws, n_rays, 1, ms), "unit": "Mrays/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "BatchedMesh instances: 256 geometries (torus knots / icospheres, log-uniform "
+                                       "200..200,000 tri, seed 2), 4096 instances (random rotation, uniform scale "
+                                       "0.5..2, position in [-1000,1000]^3), 2^22 world rays (sphere r=2500 towards "
+                                       "the instance cube), firstHitOnly",
+                           "geometry_triangles": int(sum(g.triangle_count for g in geoms)),
+                           "hit_fraction": hit_frac, "l2": "inputs (100 MB rays + 134 MB hits) exceed L2"},
+                "e2e": {"value": weak_scaling_rate(ws, n_rays, 1, e2e_ms), "unit": "Mrays/s",
+                        "h2d_bytes_per_step": int(rays_h.nbytes), "d2h_bytes_per_step": int(n_rays * 36)},
+                "roofline": None, "roofline_note": "two-level traversal (instance tree, then a geometry tree per "
+                "entered instance box) is latency-bound", "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+    scene.dispose()
+    batch.dispose()
+
+
 def run_build(args, ws, rank, local):
     """SAH build of the 2M-triangle knot on the device (bvhc_build_device), host buffers in and
     out (the call uploads positions and index, builds, and returns the serialized roots and the
@@ -857,6 +967,8 @@ def main():
             run_all_hits(args, ws, rank, local)
         elif args.workload == "build":
             run_build(args, ws, rank, local)
+        elif args.workload == "scene":
+            run_scene(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:
