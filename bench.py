@@ -767,9 +767,10 @@ def run_scene(args, ws, rank, local):
     import torch
 
     import __graft_entry__ as ge
-    from three_mesh_bvh_b200.batched import BatchedMeshBVH
 
     pkg = ge.load_package()
+    from three_mesh_bvh_b200.batched import BatchedMeshBVH
+
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n_geo, n_inst, n_rays = 256, 4096, 1 << 22
