@@ -108,3 +108,27 @@ def test_scene_rejects_bad_input(pkg, batch, cuda):
         batch.instances([0], bad[None, :])
     with pytest.raises(Exception):
         batch.instances([batch.n_meshes], np.eye(4).reshape(1, -1))
+
+
+def test_scene_many_overlapping_instances(pkg, orc, batch, cuda):
+    """100 copies of one geometry at the same place, rays starting inside every instance box: more
+    candidates than one listing round holds, all entered at distance 0, and equal hit distances,
+    which the lowest instance index wins (the raycaster's stable sort)."""
+    rng = np.random.default_rng(91)
+    n = 100
+    geometry = np.zeros(n, dtype=np.uint32)
+    mats = np.tile(np.eye(4).reshape(-1), (n, 1))
+    rays = world_rays(rng, 4_000, radius=2.0, half=12.0)
+    scene = batch.instances(geometry, mats)
+    got, ginst = scene.raycast_first(rays)
+    exp, einst = orc.scene_raycast_first(_oracles(orc, batch), geometry, mats, rays)
+    assert not _compare(got, ginst, exp, einst)
+    hit = ginst != 0xFFFFFFFF
+    assert hit.mean() > 0.3 and (ginst[hit] == 0).all()
+    # hiding the first instances moves every hit to the first visible one
+    vis = (np.arange(n) >= 37).astype(np.uint8)
+    scene.set_instances(geometry, mats, vis)
+    got2, ginst2 = scene.raycast_first(rays)
+    assert (ginst2[hit] == 37).all() and (ginst2[~hit] == 0xFFFFFFFF).all()
+    assert np.array_equal(got2["face_index"], got["face_index"])
+    scene.dispose()

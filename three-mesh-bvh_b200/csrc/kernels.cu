@@ -1509,10 +1509,101 @@ __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const Ray
   return true;
 }
 
-__global__ void __launch_bounds__(kBlock) scene_raycast_first_kernel(MeshDev m, SceneDev sc, const float* __restrict__ rays,
-                                                                     uint64_t n, int side, float near_d, float far_d,
-                                                                     bvhc_hit* __restrict__ out,
-                                                                     uint32_t* __restrict__ inst_out) {
+// The local ray of instance I (Ray.applyMatrix4 with the inverse world matrix, direction
+// normalised), near / far in local units, and |v| (the unnormalised local direction's length:
+// world distance = local t |d| / |v|).  False for a zero local direction.
+struct LocalRay {
+  RayF r;
+  float len, near_d, far_d, vlen;
+};
+__device__ __noinline__ bool local_ray(const InstanceDev& I, const RayF& w, float near_d, float far_d, LocalRay& L) {
+  const ff ox = ff_from(w.o.x), oy = ff_from(w.o.y), oz = ff_from(w.o.z);
+  const ff dx = ff_from(w.d.x), dy = ff_from(w.d.y), dz = ff_from(w.d.z);
+  const ff lox = row_apply(I.inv_hi, I.inv_lo, 0, ox, oy, oz, true);
+  const ff loy = row_apply(I.inv_hi, I.inv_lo, 1, ox, oy, oz, true);
+  const ff loz = row_apply(I.inv_hi, I.inv_lo, 2, ox, oy, oz, true);
+  const ff vx = row_apply(I.inv_hi, I.inv_lo, 0, dx, dy, dz, false);
+  const ff vy = row_apply(I.inv_hi, I.inv_lo, 1, dx, dy, dz, false);
+  const ff vz = row_apply(I.inv_hi, I.inv_lo, 2, dx, dy, dz, false);
+  const ff vlen = ff_sqrt(ff_add(ff_add(ff_mul(vx, vx), ff_mul(vy, vy)), ff_mul(vz, vz)));
+  if (!(vlen.hi > 0.0f)) return false;
+  const float3 ld = make_float3(ff_to_f(ff_div(vx, vlen)), ff_to_f(ff_div(vy, vlen)), ff_to_f(ff_div(vz, vlen)));
+  L.r = ray_from(make_float3(ff_to_f(lox), ff_to_f(loy), ff_to_f(loz)), ld);
+  const float sx = ld.x * I.scale[0], sy = ld.y * I.scale[1], sz = ld.z * I.scale[2];
+  const float sf_ = sqrtf(sx * sx + sy * sy + sz * sz);
+  L.near_d = near_d / sf_;
+  L.far_d = far_d / sf_;
+  L.len = sqrtf(ld.x * ld.x + ld.y * ld.y + ld.z * ld.z);
+  L.vlen = vlen.hi;
+  return true;
+}
+
+// The reported record of instance I's hit on triangle record `rec`, in world space: an affine map
+// keeps barycentric coordinates and carries the local hit point to the world one, so the
+// triangle is carried to world space (float-float) and met with the exact world ray; this avoids
+// the rounding of the local ray to float32, which the reference (local ray in float64) does not
+// have.  Returns the world distance.
+__device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, uint32_t rec, const RayF& w,
+                                        const RayF& lr, bvhc_hit& h) {
+  const Tri t = load_tri(m.tris, rec);
+  const ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, lr.o, lr.d));
+  make_hit(t, lr, tt, ff_mul(tt, dir_length(lr.d)), h);
+  const ff ox = ff_from(w.o.x), oy = ff_from(w.o.y), oz = ff_from(w.o.z);
+  const ff dx = ff_from(w.d.x), dy = ff_from(w.d.y), dz = ff_from(w.d.z);
+  ff3 P[3];
+  const float3 V3s[3] = {t.a, t.b, t.c};
+  for (int k = 0; k < 3; ++k) {
+    const ff vx = ff_from(V3s[k].x), vy = ff_from(V3s[k].y), vz = ff_from(V3s[k].z);
+    P[k] = {row_apply(I.m_hi, I.m_lo, 0, vx, vy, vz, true), row_apply(I.m_hi, I.m_lo, 1, vx, vy, vz, true),
+            row_apply(I.m_hi, I.m_lo, 2, vx, vy, vz, true)};
+  }
+  const ff3 O{ox, oy, oz}, D{dx, dy, dz};
+  const ff3 e1 = ff3_sub(P[1], P[0]), e2 = ff3_sub(P[2], P[0]), qv = ff3_sub(O, P[0]);
+  const ff3 nn = ff3_cross(e1, e2);
+  const ff N = ff3_dot(D, nn);
+  ff wx, wy, wz;
+  if (N.hi != 0.0f) {
+    const ff U = ff3_dot(D, ff3_cross(qv, e2)), Vv = ff3_dot(D, ff3_cross(e1, qv));
+    const ff W = ff_sub(ff_sub(N, U), Vv);
+    const ff tw = ff_div(ff_neg(ff3_dot(qv, nn)), N);
+    wx = ff_add(ox, ff_mul(tw, dx));
+    wy = ff_add(oy, ff_mul(tw, dy));
+    wz = ff_add(oz, ff_mul(tw, dz));
+    if (h.barycoord[0] != 0.0f || h.barycoord[1] != 0.0f || h.barycoord[2] != 0.0f) {
+      h.barycoord[0] = ff_to_f(ff_div(W, N));
+      h.barycoord[1] = ff_to_f(ff_div(U, N));
+      h.barycoord[2] = ff_to_f(ff_div(Vv, N));
+    }
+  } else {  // the world ray lies in the triangle's plane at float-float resolution
+    const ff px = ff_add(ff_from(lr.o.x), ff_mul_f(tt, lr.d.x));
+    const ff py = ff_add(ff_from(lr.o.y), ff_mul_f(tt, lr.d.y));
+    const ff pz = ff_add(ff_from(lr.o.z), ff_mul_f(tt, lr.d.z));
+    wx = row_apply(I.m_hi, I.m_lo, 0, px, py, pz, true);
+    wy = row_apply(I.m_hi, I.m_lo, 1, px, py, pz, true);
+    wz = row_apply(I.m_hi, I.m_lo, 2, px, py, pz, true);
+  }
+  const ff ex = ff_sub(wx, ox), ey = ff_sub(wy, oy), ez = ff_sub(wz, oz);
+  const ff dist = ff_sqrt(ff_add(ff_add(ff_mul(ex, ex), ff_mul(ey, ey)), ff_mul(ez, ez)));
+  h.distance = ff_to_f(dist);
+  h.point[0] = ff_to_f(wx);
+  h.point[1] = ff_to_f(wy);
+  h.point[2] = ff_to_f(wz);
+  return dist;
+}
+
+constexpr int kSceneCand = 32;
+
+// Two phases per ray, so that the lanes of a warp stay in step: first the instance tree, which
+// lists the instances whose world boxes the ray enters, ordered by (entry distance, instance) and
+// strictly after the key `from` processed last; then the candidates in that order, each a local
+// traversal, until the next entry lies beyond the closest world hit.  More than kSceneCand
+// candidates: the rest are listed in the next round (the key strictly grows, so every round
+// makes progress).
+__global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
+                                                                        const float* __restrict__ rays, uint64_t n,
+                                                                        int side, float near_d, float far_d,
+                                                                        bvhc_hit* __restrict__ out,
+                                                                        uint32_t* __restrict__ inst_out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const RayF w = make_ray(rays, i);
@@ -1521,138 +1612,102 @@ __global__ void __launch_bounds__(kBlock) scene_raycast_first_kernel(MeshDev m, 
   bvhc_hit best_hit;
   ff best_dist = ff_from(kInf);
   uint32_t best_inst = 0xFFFFFFFFu;
+  uint32_t cand[kSceneCand];
+  float cand_t[kSceneCand];
   uint32_t stack_link[kMaxStack];
-  float stack_t[kMaxStack];
-  int sp = 0;
-  uint32_t link = sc.root;
-  if (link == kEmptyLeaf) {
-    store_miss(out + i);
-    inst_out[i] = 0xFFFFFFFFu;
-    return;
-  }
-  const ff ox = ff_from(w.o.x), oy = ff_from(w.o.y), oz = ff_from(w.o.z);
-  const ff dx = ff_from(w.d.x), dy = ff_from(w.d.y), dz = ff_from(w.d.z);
-  for (;;) {
-    if (link & kLeafBit) {
-      const uint32_t j = link & ~kLeafBit;
-      const InstanceDev& I = sc.inst[j];
-      // the local ray (Ray.applyMatrix4 with the inverse world matrix)
-      const ff lox = row_apply(I.inv_hi, I.inv_lo, 0, ox, oy, oz, true);
-      const ff loy = row_apply(I.inv_hi, I.inv_lo, 1, ox, oy, oz, true);
-      const ff loz = row_apply(I.inv_hi, I.inv_lo, 2, ox, oy, oz, true);
-      const ff vx = row_apply(I.inv_hi, I.inv_lo, 0, dx, dy, dz, false);
-      const ff vy = row_apply(I.inv_hi, I.inv_lo, 1, dx, dy, dz, false);
-      const ff vz = row_apply(I.inv_hi, I.inv_lo, 2, dx, dy, dz, false);
-      const ff vlen = ff_sqrt(ff_add(ff_add(ff_mul(vx, vx), ff_mul(vy, vy)), ff_mul(vz, vz)));
-      if (vlen.hi > 0.0f) {
-        const float3 ld = make_float3(ff_to_f(ff_div(vx, vlen)), ff_to_f(ff_div(vy, vlen)), ff_to_f(ff_div(vz, vlen)));
-        const float3 lo = make_float3(ff_to_f(lox), ff_to_f(loy), ff_to_f(loz));
-        const float sx = ld.x * I.scale[0], sy = ld.y * I.scale[1], sz = ld.z * I.scale[2];
-        const float sf_ = sqrtf(sx * sx + sy * sy + sz * sz);
-        const float lnear = near_d / sf_, lfar = far_d / sf_;
-        // local t per world distance: world distance = t |d| / |v| (affine matrix)
-        const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * vlen.hi / wlen * (1.0f + 0x1p-16f);
-        const RayF lr = ray_from(lo, ld);
-        const float llen = sqrtf(ld.x * ld.x + ld.y * ld.y + ld.z * ld.z);
-        Best b{kInf, 0.0f, 0xFFFFFFFFu};
-        const uint32_t g = I.geometry;
-        if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], lr, llen, side, no_sides, lnear,
-                        fminf(lfar, tlim), b)) {
-          atomicOr(m.err, kErrStackOverflow);
-          break;
+  float from = -kInf;
+  uint32_t from_id = 0;
+  bool more = sc.root != kEmptyLeaf;
+  while (more) {
+    // phase 1: the entered instance boxes at or beyond `from`, nearest first
+    int nc = 0;
+    more = false;
+    const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+    int sp = 0;
+    uint32_t link = sc.root;
+    for (;;) {
+      if (link & kLeafBit) {
+        // a root that is itself a leaf: one instance, entered at its box (not stored); list it
+        if (nc < kSceneCand) {
+          cand[nc] = link & ~kLeafBit;
+          cand_t[nc] = from;
+          ++nc;
         }
-        if (b.rec != 0xFFFFFFFFu) {
-          const Tri t = load_tri(m.tris, b.rec);
-          const ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, lr.o, lr.d));
-          bvhc_hit h;
-          make_hit(t, lr, tt, ff_mul(tt, dir_length(lr.d)), h);
-          // The reported record in world space: an affine map keeps barycentric coordinates and
-          // maps the local hit point to the world one, so the triangle is carried to world space
-          // (float-float) and met with the exact world ray.  This avoids the rounding of the
-          // local ray to float32, which the reference (local ray in float64) does not have.
-          ff3 P[3];
-          const float3 V3s[3] = {t.a, t.b, t.c};
-          for (int k = 0; k < 3; ++k) {
-            const ff vx = ff_from(V3s[k].x), vy = ff_from(V3s[k].y), vz = ff_from(V3s[k].z);
-            P[k] = {row_apply(I.m_hi, I.m_lo, 0, vx, vy, vz, true), row_apply(I.m_hi, I.m_lo, 1, vx, vy, vz, true),
-                    row_apply(I.m_hi, I.m_lo, 2, vx, vy, vz, true)};
-          }
-          const ff3 O{ox, oy, oz}, D{dx, dy, dz};
-          const ff3 e1 = ff3_sub(P[1], P[0]), e2 = ff3_sub(P[2], P[0]), qv = ff3_sub(O, P[0]);
-          const ff3 nn = ff3_cross(e1, e2);
-          const ff N = ff3_dot(D, nn);
-          ff wx, wy, wz;
-          if (N.hi != 0.0f) {
-            const ff U = ff3_dot(D, ff3_cross(qv, e2)), Vv = ff3_dot(D, ff3_cross(e1, qv));
-            const ff W = ff_sub(ff_sub(N, U), Vv);
-            const ff tw = ff_div(ff_neg(ff3_dot(qv, nn)), N);
-            wx = ff_add(ox, ff_mul(tw, dx));
-            wy = ff_add(oy, ff_mul(tw, dy));
-            wz = ff_add(oz, ff_mul(tw, dz));
-            if (h.barycoord[0] != 0.0f || h.barycoord[1] != 0.0f || h.barycoord[2] != 0.0f) {
-              h.barycoord[0] = ff_to_f(ff_div(W, N));
-              h.barycoord[1] = ff_to_f(ff_div(U, N));
-              h.barycoord[2] = ff_to_f(ff_div(Vv, N));
-            }
-          } else {  // the world ray lies in the triangle's plane at float-float resolution
-            const ff px = ff_add(ff_from(lr.o.x), ff_mul_f(tt, lr.d.x));
-            const ff py = ff_add(ff_from(lr.o.y), ff_mul_f(tt, lr.d.y));
-            const ff pz = ff_add(ff_from(lr.o.z), ff_mul_f(tt, lr.d.z));
-            wx = row_apply(I.m_hi, I.m_lo, 0, px, py, pz, true);
-            wy = row_apply(I.m_hi, I.m_lo, 1, px, py, pz, true);
-            wz = row_apply(I.m_hi, I.m_lo, 2, px, py, pz, true);
-          }
-          const ff ex = ff_sub(wx, ox), ey = ff_sub(wy, oy), ez = ff_sub(wz, oz);
-          const ff dist = ff_sqrt(ff_add(ff_add(ff_mul(ex, ex), ff_mul(ey, ey)), ff_mul(ez, ez)));
-          if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
-            best_dist = dist;
-            best_inst = j;
-            best_hit = h;
-            best_hit.distance = ff_to_f(dist);
-            best_hit.point[0] = ff_to_f(wx);
-            best_hit.point[1] = ff_to_f(wy);
-            best_hit.point[2] = ff_to_f(wz);
-          }
-        }
+        if (sp == 0) break;
+        link = stack_link[--sp];
+        continue;
       }
-    } else {
       const Pair p = load_pair(sc.nodes, link);
-      const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
-      float e0, e1;
-      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e0);
-      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e1);
-      const bool lf = e0 <= e1;
-      const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
-      const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
-      if (h1st) {
-        if (h2nd) {
+      float e[2];
+      bool h[2];
+      h[0] = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e[0]);
+      h[1] = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e[1]);
+      const uint32_t kids[2] = {p.ll, p.lr};
+      for (int k = 0; k < 2; ++k) {
+        if (!h[k]) continue;
+        if (kids[k] & kLeafBit) {
+          const float et = fmaxf(e[k], 0.0f);
+          const uint32_t id = kids[k] & ~kLeafBit;
+          if (et < from || (et == from && id <= from_id)) continue;
+          // sorted insert by (entry, instance); when full, keep the first ones and come back
+          int pos = nc;
+          while (pos > 0 && (cand_t[pos - 1] > et || (cand_t[pos - 1] == et && cand[pos - 1] > id))) --pos;
+          if (nc == kSceneCand) {
+            more = true;
+            if (pos == kSceneCand) continue;
+          } else {
+            ++nc;
+          }
+          for (int q = nc - 1; q > pos; --q) {
+            cand[q] = cand[q - 1];
+            cand_t[q] = cand_t[q - 1];
+          }
+          cand[pos] = id;
+          cand_t[pos] = et;
+        } else {
           if (sp >= kMaxStack) {
             atomicOr(m.err, kErrStackOverflow);
+            more = false;
             break;
           }
-          stack_link[sp] = c2;
-          stack_t[sp] = lf ? e1 : e0;
-          ++sp;
+          stack_link[sp++] = kids[k];
         }
-        link = c1;
-        continue;
       }
-      if (h2nd) {
-        link = c2;
-        continue;
-      }
+      if (sp == 0) break;
+      link = stack_link[--sp];
     }
-    bool found = false;
-    const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
-    while (sp > 0) {
-      --sp;
-      if (stack_t[sp] <= lim) {
-        link = stack_link[sp];
-        found = true;
+    // phase 2: the candidates in entry order
+    for (int c = 0; c < nc; ++c) {
+      if (best_dist.hi != kInf && cand_t[c] * wlen > best_dist.hi * (1.0f + 0x1p-16f)) {
+        more = false;
         break;
       }
+      const uint32_t j = cand[c];
+      const InstanceDev& I = sc.inst[j];
+      LocalRay L;
+      if (!local_ray(I, w, near_d, far_d, L)) continue;
+      const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * L.vlen / wlen * (1.0f + 0x1p-16f);
+      Best b{kInf, 0.0f, 0xFFFFFFFFu};
+      const uint32_t g = I.geometry;
+      if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
+                      fminf(L.far_d, tlim), b)) {
+        atomicOr(m.err, kErrStackOverflow);
+        more = false;
+        break;
+      }
+      if (b.rec == 0xFFFFFFFFu) continue;
+      bvhc_hit h;
+      const ff dist = world_record(m, I, b.rec, w, L.r, h);
+      if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
+        best_dist = dist;
+        best_inst = j;
+        best_hit = h;
+      }
     }
-    if (!found) break;
+    if (more) {
+      from = cand_t[nc - 1];
+      from_id = cand[nc - 1];
+    }
   }
   if (best_inst == 0xFFFFFFFFu) {
     store_miss(out + i);
