@@ -807,6 +807,19 @@ def run_scene(args, ws, rank, local):
         lib.bvhc_scene_raycast_first(scene.h, rays.data_ptr(), n_rays, 0, 0.0, math.inf, hits.data_ptr(),
                                      inst.data_ptr(), 1, s)
 
+    # ray order: input order or one of the Morton keys, whichever is fastest here
+    order_ms = {}
+    for order in (0, 1, 2, 3):
+        scene.set_order(order)
+        step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        order_ms[order] = e0.elapsed_time(e1)
+    best_order = min(order_ms, key=order_ms.get)
+    scene.set_order(best_order)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
@@ -858,12 +871,13 @@ def run_scene(args, ws, rank, local):
                                        "0.5..2, position in [-1000,1000]^3), 2^22 world rays (sphere r=2500 towards "
                                        "the instance cube), firstHitOnly",
                            "geometry_triangles": int(sum(g.triangle_count for g in geoms)),
-                           "hit_fraction": hit_frac, "l2": "inputs (100 MB rays + 134 MB hits) exceed L2"},
+                           "hit_fraction": hit_frac, "l2": "inputs (100 MB rays + 134 MB hits) exceed L2",
+                           "ray_order": best_order, "order_ms": {str(k): v for k, v in order_ms.items()}},
                 "e2e": {"value": weak_scaling_rate(ws, n_rays, 1, e2e_ms), "unit": "Mrays/s",
                         "h2d_bytes_per_step": int(rays_h.nbytes), "d2h_bytes_per_step": int(n_rays * 36)},
                 "roofline": None, "roofline_note": "two-level traversal (instance tree, then a geometry tree per "
                 "entered instance box) is latency-bound", "cpu_baseline": cpu, "clocks": clk.summary(),
-                "gpu_launches": args.steps}
+                "gpu_launches": args.steps * (1 if best_order == 0 else 6)}
         print(json.dumps(line), flush=True)
     scene.dispose()
     batch.dispose()

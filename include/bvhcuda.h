@@ -292,6 +292,10 @@ bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const u
 bvhc_status bvhc_scene_raycast_first(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
                                      float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream);
 void bvhc_scene_destroy(bvhc_scene* scene);
+/* Ray order of bvhc_scene_raycast_first: 0 input order; 1, 2, 3 the rays sorted by a Morton key
+ * (direction; entry point into the instances' world box; that point and the direction) so that
+ * the rays of a warp share their paths.  Results are the same; results land in the rays' rows. */
+bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind);
 
 /* raycastFirst that allocates nothing.  No counterpart in the reference: it exists for callers
  * that must not call cudaMalloc -- code inside someone else's fixed device-memory budget, a

@@ -1601,6 +1601,14 @@ struct bvhc_scene {
   size_t out_cap = 0;
   void* d_ids = nullptr;
   size_t ids_cap = 0;
+  // ray ordering (bvhc_scene_set_order): key kind, the instances' world box, sort scratch, queue
+  int order = 0;
+  float box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
+  RaySortScratch sort_s = {};
+  uint64_t sort_cap = 0;
+  uint32_t* d_queue = nullptr;
+  size_t queue_cap = 0;
+  unsigned int* d_qcount = nullptr;
 };
 
 namespace {
@@ -1736,6 +1744,14 @@ bvhc_status set_instances(bvhc_scene* sc, int n, const uint32_t* geometry, const
     }
     boxes.push_back(b);
   }
+  for (int d = 0; d < 3; ++d) {
+    sc->box_lo[d] = INFINITY;
+    sc->box_hi[d] = -INFINITY;
+    for (const InstBox& b : boxes) {
+      sc->box_lo[d] = std::min(sc->box_lo[d], b.lo[d]);
+      sc->box_hi[d] = std::max(sc->box_hi[d], b.hi[d]);
+    }
+  }
   std::vector<PairNode> nodes;
   uint32_t root = kEmptyLeaf;
   if (!boxes.empty()) root = build_tlas(boxes, 0, boxes.size(), nodes);
@@ -1789,9 +1805,37 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   const SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
+  RaySort sort{};
+  if (sc->order > 0 && n < (1ull << 32) && sc->root != kEmptyLeaf) {
+    if (sc->sort_cap < n) {
+      free_sort_scratch(sc->sort_s);
+      sc->sort_cap = 0;
+      RaySortScratch& t = sc->sort_s;
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&t.keys[0]), n * 4);
+      if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&t.keys[1]), n * 4);
+      if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&t.vals), n * 4);
+      if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&t.hist), 256 * ray_sort_tiles(n) * 4);
+      if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&t.totals), 4 * 256 * 4);
+      if (e != cudaSuccess) {
+        free_sort_scratch(t);
+        return from_cuda(e);
+      }
+      sc->sort_cap = n;
+    }
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&sc->d_queue), &sc->queue_cap, n * 4));
+    if (!sc->d_qcount) BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&sc->d_qcount), sizeof(unsigned int)));
+    sort.kind = sc->order;
+    for (int a = 0; a < 3; ++a) {
+      sort.lo[a] = sc->box_lo[a];
+      sort.hi[a] = sc->box_hi[a];
+    }
+    sort.scratch = sc->sort_s;
+  }
+  const RaySort* sp = sort.kind ? &sort : nullptr;
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(hits, 16) || !aligned(instance, 4)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_scene_raycast_first(m->view(), sd, rays, n, side, near_dist, far_dist, hits, instance, s));
+    return from_cuda(launch_scene_raycast_first(m->view(), sd, rays, n, side, near_dist, far_dist, hits, instance, s,
+                                                sp, sc->d_queue, sc->d_qcount));
   }
   BVHC_CUDA_TRY(ensure(&sc->d_in, &sc->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&sc->d_out, &sc->out_cap, n * sizeof(bvhc_hit)));
@@ -1799,7 +1843,7 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   BVHC_CUDA_TRY(cudaMemcpyAsync(sc->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_scene_raycast_first(m->view(), sd, static_cast<const float*>(sc->d_in), n, side, near_dist,
                                            far_dist, static_cast<bvhc_hit*>(sc->d_out),
-                                           static_cast<uint32_t*>(sc->d_ids), s));
+                                           static_cast<uint32_t*>(sc->d_ids), s, sp, sc->d_queue, sc->d_qcount));
   BVHC_CUDA_TRY(cudaMemcpyAsync(hits, sc->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
   BVHC_CUDA_TRY(cudaMemcpyAsync(instance, sc->d_ids, n * 4, cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
@@ -1813,7 +1857,16 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
   cudaFree(sc->d_in);
   cudaFree(sc->d_out);
   cudaFree(sc->d_ids);
+  cudaFree(sc->d_queue);
+  cudaFree(sc->d_qcount);
+  free_sort_scratch(sc->sort_s);
   delete sc;
+}
+
+bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind) {
+  if (!scene || kind < 0 || kind > 3) return BVHC_ERR_INVALID_ARGUMENT;
+  scene->order = kind;
+  return BVHC_OK;
 }
 
 // ---------------------------------------------------------------------------------------------

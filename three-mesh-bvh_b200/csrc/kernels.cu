@@ -1591,122 +1591,90 @@ __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, 
   return dist;
 }
 
-constexpr int kSceneCand = 32;
-
-// Two phases per ray, so that the lanes of a warp stay in step: first the instance tree, which
-// lists the instances whose world boxes the ray enters, ordered by (entry distance, instance) and
-// strictly after the key `from` processed last; then the candidates in that order, each a local
-// traversal, until the next entry lies beyond the closest world hit.  More than kSceneCand
-// candidates: the rest are listed in the next round (the key strictly grows, so every round
-// makes progress).
+// One ray per thread: the instance tree nearest box first, pruned by the closest world hit so
+// far; each entered instance box is walked in the instance's frame right away.  With a queue,
+// thread i takes ray queue[i] (rays ordered by a Morton key, so that a warp's rays share paths)
+// and writes that ray's row.
 __global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
                                                                         const float* __restrict__ rays, uint64_t n,
-                                                                        int side, float near_d, float far_d,
+                                                                        const uint32_t* __restrict__ queue, int side,
+                                                                        float near_d, float far_d,
                                                                         bvhc_hit* __restrict__ out,
                                                                         uint32_t* __restrict__ inst_out) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint64_t i = queue ? queue[t] : t;
   const RayF w = make_ray(rays, i);
   const float wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
   const SideTable no_sides{};
   bvhc_hit best_hit;
   ff best_dist = ff_from(kInf);
   uint32_t best_inst = 0xFFFFFFFFu;
-  uint32_t cand[kSceneCand];
-  float cand_t[kSceneCand];
   uint32_t stack_link[kMaxStack];
-  float from = -kInf;
-  uint32_t from_id = 0;
-  bool more = sc.root != kEmptyLeaf;
-  while (more) {
-    // phase 1: the entered instance boxes at or beyond `from`, nearest first
-    int nc = 0;
-    more = false;
-    const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
-    int sp = 0;
-    uint32_t link = sc.root;
-    for (;;) {
-      if (link & kLeafBit) {
-        // a root that is itself a leaf: one instance, entered at its box (not stored); list it
-        if (nc < kSceneCand) {
-          cand[nc] = link & ~kLeafBit;
-          cand_t[nc] = from;
-          ++nc;
-        }
-        if (sp == 0) break;
-        link = stack_link[--sp];
-        continue;
-      }
-      const Pair p = load_pair(sc.nodes, link);
-      float e[2];
-      bool h[2];
-      h[0] = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e[0]);
-      h[1] = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e[1]);
-      const uint32_t kids[2] = {p.ll, p.lr};
-      for (int k = 0; k < 2; ++k) {
-        if (!h[k]) continue;
-        if (kids[k] & kLeafBit) {
-          const float et = fmaxf(e[k], 0.0f);
-          const uint32_t id = kids[k] & ~kLeafBit;
-          if (et < from || (et == from && id <= from_id)) continue;
-          // sorted insert by (entry, instance); when full, keep the first ones and come back
-          int pos = nc;
-          while (pos > 0 && (cand_t[pos - 1] > et || (cand_t[pos - 1] == et && cand[pos - 1] > id))) --pos;
-          if (nc == kSceneCand) {
-            more = true;
-            if (pos == kSceneCand) continue;
-          } else {
-            ++nc;
-          }
-          for (int q = nc - 1; q > pos; --q) {
-            cand[q] = cand[q - 1];
-            cand_t[q] = cand_t[q - 1];
-          }
-          cand[pos] = id;
-          cand_t[pos] = et;
-        } else {
-          if (sp >= kMaxStack) {
-            atomicOr(m.err, kErrStackOverflow);
-            more = false;
-            break;
-          }
-          stack_link[sp++] = kids[k];
-        }
-      }
-      if (sp == 0) break;
-      link = stack_link[--sp];
-    }
-    // phase 2: the candidates in entry order
-    for (int c = 0; c < nc; ++c) {
-      if (best_dist.hi != kInf && cand_t[c] * wlen > best_dist.hi * (1.0f + 0x1p-16f)) {
-        more = false;
-        break;
-      }
-      const uint32_t j = cand[c];
+  float stack_t[kMaxStack];
+  int sp = 0;
+  uint32_t link = sc.root;
+  bool go = link != kEmptyLeaf;
+  while (go) {
+    if (link & kLeafBit) {
+      const uint32_t j = link & ~kLeafBit;
       const InstanceDev& I = sc.inst[j];
       LocalRay L;
-      if (!local_ray(I, w, near_d, far_d, L)) continue;
-      const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * L.vlen / wlen * (1.0f + 0x1p-16f);
-      Best b{kInf, 0.0f, 0xFFFFFFFFu};
-      const uint32_t g = I.geometry;
-      if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
-                      fminf(L.far_d, tlim), b)) {
-        atomicOr(m.err, kErrStackOverflow);
-        more = false;
-        break;
+      if (local_ray(I, w, near_d, far_d, L)) {
+        const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * L.vlen / wlen * (1.0f + 0x1p-16f);
+        Best b{kInf, 0.0f, 0xFFFFFFFFu};
+        const uint32_t g = I.geometry;
+        if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
+                        fminf(L.far_d, tlim), b)) {
+          atomicOr(m.err, kErrStackOverflow);
+          break;
+        }
+        if (b.rec != 0xFFFFFFFFu) {
+          bvhc_hit h;
+          const ff dist = world_record(m, I, b.rec, w, L.r, h);
+          if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
+            best_dist = dist;
+            best_inst = j;
+            best_hit = h;
+          }
+        }
       }
-      if (b.rec == 0xFFFFFFFFu) continue;
-      bvhc_hit h;
-      const ff dist = world_record(m, I, b.rec, w, L.r, h);
-      if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
-        best_dist = dist;
-        best_inst = j;
-        best_hit = h;
+    } else {
+      const Pair p = load_pair(sc.nodes, link);
+      const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+      float e0, e1;
+      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e0);
+      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e1);
+      const bool lf = e0 <= e1;
+      const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+      const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+      if (h1st) {
+        if (h2nd) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            break;
+          }
+          stack_link[sp] = c2;
+          stack_t[sp] = lf ? e1 : e0;
+          ++sp;
+        }
+        link = c1;
+        continue;
+      }
+      if (h2nd) {
+        link = c2;
+        continue;
       }
     }
-    if (more) {
-      from = cand_t[nc - 1];
-      from_id = cand[nc - 1];
+    go = false;
+    const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+    while (sp > 0) {
+      --sp;
+      if (stack_t[sp] <= lim) {
+        link = stack_link[sp];
+        go = true;
+        break;
+      }
     }
   }
   if (best_inst == 0xFFFFFFFFu) {
@@ -1715,6 +1683,18 @@ __global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev 
     store_hit(out + i, best_hit);
   }
   inst_out[i] = best_inst;
+}
+
+// Morton keys of world rays over the instances' box (ray_key), ids in input order.
+__global__ void __launch_bounds__(kBlock) scene_key_kernel(const float* __restrict__ rays, uint64_t n, int kind,
+                                                           SceneBox box, uint32_t* __restrict__ ids,
+                                                           uint32_t* __restrict__ keys, unsigned int* qcount) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *qcount = (unsigned int)n;
+  if (i >= n) return;
+  const RayF r = make_ray(rays, i);
+  ids[i] = (uint32_t)i;
+  keys[i] = ray_key(kind, r.o, r.d, box);
 }
 
 // Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
@@ -2277,10 +2257,25 @@ cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uin
 
 cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
                                        int side, float near_d, float far_d, bvhc_hit* hits, uint32_t* instance,
-                                       cudaStream_t stream) {
+                                       cudaStream_t stream, const RaySort* sort, uint32_t* queue,
+                                       unsigned int* qcount) {
   if (n == 0) return cudaSuccess;
-  dev::scene_raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, side, near_d, far_d,
-                                                                          hits, instance);
+  const bool sorted = sort && sort->kind > 0 && queue && qcount && n < (1ull << 32);
+  if (sorted) {
+    uint32_t *ids, *keys;
+    ray_sort_input(sort->kind, sort->scratch, queue, &ids, &keys);
+    dev::SceneBox box;
+    for (int a = 0; a < 3; ++a) {
+      box.lo[a] = sort->lo[a];
+      box.hi[a] = sort->hi[a];
+    }
+    dev::scene_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(rays, n, sort->kind, box, ids, keys, qcount);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
+  }
+  dev::scene_raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(
+      blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d, hits, instance);
   return cudaGetLastError();
 }
 
