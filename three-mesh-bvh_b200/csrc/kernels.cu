@@ -1615,8 +1615,49 @@ __global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev 
   int sp = 0;
   uint32_t link = sc.root;
   bool go = link != kEmptyLeaf;
+  // "while-while": every lane descends the instance tree until it holds an instance (or has none
+  // left), then the lanes holding one walk their instances together, so the heavy local traversal
+  // is not serialised across lanes that reach their instances at different steps
   while (go) {
-    if (link & kLeafBit) {
+    while (go && !(link & kLeafBit)) {
+      const Pair p = load_pair(sc.nodes, link);
+      const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
+      float e0, e1;
+      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e0);
+      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e1);
+      const bool lf = e0 <= e1;
+      const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+      const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+      if (h1st) {
+        if (h2nd) {
+          if (sp >= kMaxStack) {
+            atomicOr(m.err, kErrStackOverflow);
+            go = false;
+            break;
+          }
+          stack_link[sp] = c2;
+          stack_t[sp] = lf ? e1 : e0;
+          ++sp;
+        }
+        link = c1;
+        continue;
+      }
+      if (h2nd) {
+        link = c2;
+        continue;
+      }
+      go = false;
+      while (sp > 0) {
+        --sp;
+        if (stack_t[sp] <= lim) {
+          link = stack_link[sp];
+          go = true;
+          break;
+        }
+      }
+    }
+    if (!go) break;
+    {
       const uint32_t j = link & ~kLeafBit;
       const InstanceDev& I = sc.inst[j];
       LocalRay L;
@@ -1638,32 +1679,6 @@ __global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev 
             best_hit = h;
           }
         }
-      }
-    } else {
-      const Pair p = load_pair(sc.nodes, link);
-      const float lim = best_dist.hi == kInf ? kInf : best_dist.hi / wlen * (1.0f + 0x1p-16f);
-      float e0, e1;
-      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, lim, e0);
-      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, lim, e1);
-      const bool lf = e0 <= e1;
-      const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
-      const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
-      if (h1st) {
-        if (h2nd) {
-          if (sp >= kMaxStack) {
-            atomicOr(m.err, kErrStackOverflow);
-            break;
-          }
-          stack_link[sp] = c2;
-          stack_t[sp] = lf ? e1 : e0;
-          ++sp;
-        }
-        link = c1;
-        continue;
-      }
-      if (h2nd) {
-        link = c2;
-        continue;
       }
     }
     go = false;
