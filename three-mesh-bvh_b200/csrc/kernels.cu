@@ -1457,8 +1457,9 @@ __device__ __forceinline__ ff row_apply(const float* hi, const float* lo, int ro
   return affine_t ? ff_add(s, ff{hi[k + 3], lo[k + 3]}) : s;
 }
 
-// The per-thread raycastFirst walk of one geometry's roots (the simple kernel's loop, nearest
-// child first).  Returns false on a stack overflow.
+// The per-thread raycastFirst walk of one geometry's roots, nearest child first, in "while-while"
+// form (each lane descends internal nodes until it holds a leaf, then the lanes holding one test
+// their triangles together).  Returns false on a stack overflow.
 __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const RayF& r, float dlen, int side,
                            const SideTable& sides, float near_d, float far_d, Best& best) {
   uint32_t stack_link[kMaxStack];
@@ -1466,10 +1467,9 @@ __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const Ray
   for (uint32_t root = r0; root < r1; ++root) {
     uint32_t link = m.roots[root];
     int sp = 0;
-    for (;;) {
-      if (link & kLeafBit) {
-        if (link != kEmptyLeaf) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
-      } else {
+    bool go = true;
+    while (go) {
+      while (go && !(link & kLeafBit)) {
         const Pair p = load_pair(m.nodes, link);
         const float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
         float e0, e1;
@@ -1492,18 +1492,29 @@ __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const Ray
           link = c2;
           continue;
         }
+        go = false;
+        const float plim = (best.t + best.err) * (1.0f + kSlabMargin);
+        while (sp > 0) {
+          --sp;
+          if (stack_t[sp] <= plim) {
+            link = stack_link[sp];
+            go = true;
+            break;
+          }
+        }
       }
-      bool found = false;
-      const float lim = (best.t + best.err) * (1.0f + kSlabMargin);
+      if (!go) break;
+      if (link != kEmptyLeaf) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
+      go = false;
+      const float plim = (best.t + best.err) * (1.0f + kSlabMargin);
       while (sp > 0) {
         --sp;
-        if (stack_t[sp] <= lim) {
+        if (stack_t[sp] <= plim) {
           link = stack_link[sp];
-          found = true;
+          go = true;
           break;
         }
       }
-      if (!found) break;
     }
   }
   return true;
