@@ -752,8 +752,25 @@ __device__ __forceinline__ CPBest cp_none() {
 
 // Offers triangle record k to the query at p (the reference's strict `<` on distSq).  Returns the
 // candidate's float32 squared distance and bound, and its float-float value when one was needed.
+// With `cull`, a triangle whose bounding box is already farther than the best candidate is
+// passed over without its closest point: its distance exceeds the best one, so the reference's
+// strict `<` would not take it (callers that test minThreshold on every triangle pass false).
 __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
-                                         float& err, bool& have_ff, ff& cand_ff) {
+                                         float& err, bool& have_ff, ff& cand_ff, bool cull = false) {
+  if (cull && b.rec != 0xFFFFFFFFu) {
+    // squared distance to the triangle's box: at most 4 roundings above the exact value's
+    // relative 2^-22, so the 2^-20 shrink keeps it a lower bound
+    const float dx = fmaxf(fmaxf(fminf(t.a.x, fminf(t.b.x, t.c.x)) - p.x, p.x - fmaxf(t.a.x, fmaxf(t.b.x, t.c.x))), 0.0f);
+    const float dy = fmaxf(fmaxf(fminf(t.a.y, fminf(t.b.y, t.c.y)) - p.y, p.y - fmaxf(t.a.y, fmaxf(t.b.y, t.c.y))), 0.0f);
+    const float dz = fmaxf(fmaxf(fminf(t.a.z, fminf(t.b.z, t.c.z)) - p.z, p.z - fmaxf(t.a.z, fmaxf(t.b.z, t.c.z))), 0.0f);
+    const float lb = dx * dx + dy * dy + dz * dz;
+    if (lb * (1.0f - 0x1p-20f) > b.d2 + b.err) {
+      d2 = lb;
+      err = 0.0f;
+      have_ff = false;
+      return;
+    }
+  }
   float3 q;
   float sc;
   d2 = closest_sq_f(p, t.a, t.b, t.c, q, sc);
@@ -841,7 +858,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
             float d2, err;
             bool have_ff;
             ff cand_ff;
-            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff);
+            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff, !(min2.hi > 0.0f));
             // early out below minThreshold (closestPointToPoint.js:55-57)
             if (min2.hi > 0.0f) {
               bool below;
@@ -941,7 +958,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
             float d2, err;
             bool have_ff;
             ff cand_ff;
-            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff);
+            cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff, true);
             if (t.flags & kTriLast) break;
             ++k;
           }
