@@ -291,6 +291,14 @@ bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const u
  * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none. */
 bvhc_status bvhc_scene_raycast_first(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
                                      float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream);
+/* The same without firstHitOnly (the BatchedMesh raycast, then the raycaster's sort): every hit of
+ * every visible instance, in world space, ordered by distance (equal distances: instance order,
+ * then each instance's DFS order).  Stores the first `cap` hits per ray at hits[i * cap ..] and
+ * their instances at instance[i * cap ..] (BVHC_NO_HIT past the count); counts[i] receives the
+ * total.  cap 0 computes the counts only. */
+bvhc_status bvhc_scene_raycast(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
+                               float far_dist, uint32_t cap, uint32_t* counts, bvhc_hit* hits, uint32_t* instance,
+                               int mem, void* stream);
 void bvhc_scene_destroy(bvhc_scene* scene);
 /* Ray order of bvhc_scene_raycast_first: 0 input order; 1, 2, 3 the rays sorted by a Morton key
  * (direction; entry point into the instances' world box; that point and the direction) so that

@@ -1283,6 +1283,64 @@ void orc_scene_raycast_first(const orc_bvh* const* geoms, int n_instances, const
   });
 }
 
+// The same without firstHitOnly: every visible instance's MeshBVH.raycast hits (DFS order) in
+// instance order, each converted to world space, then the raycaster's stable sort by distance.
+// Stores the first `cap` per ray (instance[i * cap + k] their instances) and the total count.
+void orc_scene_raycast_all(const orc_bvh* const* geoms, int n_instances, const uint32_t* geometry,
+                           const double* matrices, const uint8_t* visible, const float* rays, int64_t n, int side,
+                           double near, double far, int cap, int32_t* counts, orc_hit* hits, int64_t* instance,
+                           int threads) {
+  std::vector<double> inv((size_t)n_instances * 16);
+  for (int j = 0; j < n_instances; ++j) invert4(matrices + 16 * j, &inv[(size_t)16 * j]);
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    std::vector<orc_hit> local;
+    std::vector<std::pair<orc_hit, int64_t>> all;
+    for (int64_t i = s; i < e; ++i) {
+      const Ray w = load_ray(rays + 6 * i);
+      all.clear();
+      for (int j = 0; j < n_instances; ++j) {
+        if (visible && !visible[j]) continue;
+        const double* M = matrices + 16 * j;
+        const double* Mi = &inv[(size_t)16 * j];
+        Ray lr{apply_matrix4(w.o, Mi), transform_direction(w.d, Mi)};
+        const V3 ws{std::sqrt(M[0] * M[0] + M[1] * M[1] + M[2] * M[2]), std::sqrt(M[4] * M[4] + M[5] * M[5] + M[6] * M[6]),
+                    std::sqrt(M[8] * M[8] + M[9] * M[9] + M[10] * M[10])};
+        const V3 sd{lr.d.x * ws.x, lr.d.y * ws.y, lr.d.z * ws.z};
+        const double scale = std::sqrt(dot(sd, sd));
+        const Bvh& g = geoms[geometry[j]]->b;
+        local.clear();
+        Counters c;
+        for (const auto& root : g.roots) {
+          NodeView nv{root.data()};
+          raycast_all_rec(g, nv, 0, side, lr, near / scale, far / scale, local, c);
+        }
+        for (orc_hit h : local) {
+          const V3 pw = apply_matrix4(V3{h.point[0], h.point[1], h.point[2]}, M);
+          h.distance = std::sqrt(dist_sq(pw, w.o));
+          h.point[0] = pw.x;
+          h.point[1] = pw.y;
+          h.point[2] = pw.z;
+          all.emplace_back(h, (int64_t)j);
+        }
+      }
+      std::stable_sort(all.begin(), all.end(), [](const std::pair<orc_hit, int64_t>& a,
+                                                  const std::pair<orc_hit, int64_t>& b) {
+        return a.first.distance < b.first.distance;
+      });
+      counts[i] = (int32_t)all.size();
+      for (int k = 0; k < cap; ++k) {
+        if (k < (int)all.size()) {
+          hits[i * cap + k] = all[k].first;
+          instance[i * cap + k] = all[k].second;
+        } else {
+          hits[i * cap + k].face_index = -1;
+          instance[i * cap + k] = -1;
+        }
+      }
+    }
+  });
+}
+
 // boxes: n x 24 float32 (min xyz, pad, max xyz, pad, the column-major box-to-mesh matrix).
 void orc_intersects_box(const orc_bvh* h, const float* boxes, int64_t n, uint8_t* out, int64_t* node_reads,
                         int64_t* tri_tests, int threads) {

@@ -69,6 +69,7 @@ def lib():
         L.orc_intersects_sphere.argtypes = [P, P, I64, P, P, P, I]
         L.orc_intersects_box.argtypes = [P, P, I64, P, P, P, I]
         L.orc_scene_raycast_first.argtypes = [P, I, P, P, P, P, I64, I, D, D, P, P, I]
+        L.orc_scene_raycast_all.argtypes = [P, I, P, P, P, P, I64, I, D, D, I, P, P, P, I]
         _lib = L
     return _lib
 
@@ -272,3 +273,20 @@ def scene_raycast_first(geoms, geometry, matrices, rays, visible=None, side=0, n
     lib().orc_scene_raycast_first(gs, mats.shape[0], _p(geo), _p(mats), _p(vis), _p(r), r.shape[0], side, near, far,
                                   _p(out), _p(inst), threads or _threads())
     return out, inst
+
+
+def scene_raycast_all(geoms, geometry, matrices, rays, visible=None, side=0, near=0.0, far=math.inf, cap=64,
+                      threads=None):
+    """Instanced raycast (all hits): per ray the total count, and the first `cap` world-space hits
+    by distance (stable: instance order, then DFS order) with their instances (-1 past the count)."""
+    gs = (C.c_void_p * len(geoms))(*[g.h for g in geoms])
+    geo = np.ascontiguousarray(geometry, dtype=np.uint32)
+    mats = np.ascontiguousarray(matrices, dtype=np.float64).reshape(-1, 16)
+    vis = None if visible is None else np.ascontiguousarray(visible, dtype=np.uint8)
+    r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+    counts = np.empty(r.shape[0], dtype=np.int32)
+    hits = np.empty((r.shape[0], cap), dtype=HIT_DTYPE)
+    inst = np.empty((r.shape[0], cap), dtype=np.int64)
+    lib().orc_scene_raycast_all(gs, mats.shape[0], _p(geo), _p(mats), _p(vis), _p(r), r.shape[0], side, near, far,
+                                cap, _p(counts), _p(hits), _p(inst), threads or _threads())
+    return counts, hits, inst

@@ -134,3 +134,38 @@ def test_scene_many_overlapping_instances(pkg, orc, batch, cuda):
     assert (ginst2[hit] == 37).all() and (ginst2[~hit] == 0xFFFFFFFF).all()
     assert np.array_equal(got2["face_index"], got["face_index"])
     scene.dispose()
+
+
+def test_scene_all_hits_match_oracle(pkg, orc, batch, cuda):
+    rng = np.random.default_rng(61)
+    geometry, mats = instance_matrices(rng, 150, batch.n_meshes, scaled=True)
+    vis = (rng.random(150) > 0.1).astype(np.uint8)
+    rays = world_rays(rng, 6_000)
+    scene = batch.instances(geometry, mats, vis)
+    cap = 12
+    counts, hits, inst = scene.raycast(rays, cap=cap)
+    ec, eh, ei = orc.scene_raycast_all(_oracles(orc, batch), geometry, mats, rays, visible=vis, cap=cap)
+    bad = 0
+    for i in range(rays.shape[0]):
+        if counts[i] != ec[i]:
+            k = min(int(max(counts[i], ec[i])), cap)
+            edge = (eh[i, :min(int(ec[i]), cap)]["barycoord"].min(initial=1) < 1e-4 or
+                    hits[i, :min(int(counts[i]), cap)]["barycoord"].min(initial=1) < 1e-4)
+            bad += 0 if edge else 1
+            continue
+        k = min(int(counts[i]), cap)
+        d = eh[i, :k]["distance"]
+        assert np.all(np.abs(hits[i, :k]["distance"] - d) <= 1e-5 * d), i
+        same = (inst[i, :k].astype(np.int64) == ei[i, :k]) & (hits[i, :k]["face_index"].astype(np.int64) ==
+                                                               eh[i, :k]["face_index"])
+        if not same.all():  # equal distances can swap two hits
+            for q in np.nonzero(~same)[0]:
+                dd = d[q]
+                assert (np.abs(d - dd) <= 1e-6 * dd).sum() > 1 or eh[i, q]["barycoord"].min() < 1e-4, (i, q)
+        assert np.all(inst[i, k:] == 0xFFFFFFFF)
+    assert bad == 0
+    assert (ec > 1).mean() > 0.1
+    # counts only
+    c0, _, _ = scene.raycast(rays, cap=0)
+    assert np.array_equal(c0, counts)
+    scene.dispose()

@@ -218,6 +218,20 @@ class InstancedScene:
                 "bvhc_scene_raycast_first")
         return hits, inst
 
+    def raycast(self, rays, side=FrontSide, near=0.0, far=float("inf"), cap=64):
+        """Every hit of every instance (no firstHitOnly), world space, sorted by distance: numpy
+        rays -> (counts, hits (n, cap) structured, instances (n, cap))."""
+        from .mesh_bvh import HIT_DTYPE
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = r.shape[0]
+        counts = np.empty(n, dtype=np.uint32)
+        hits = np.empty((n, cap), dtype=HIT_DTYPE)
+        inst = np.empty((n, cap), dtype=np.uint32)
+        N.check(N.lib().bvhc_scene_raycast(self.h, r.ctypes.data, n, _side_of(side), float(near), float(far), cap,
+                                           counts.ctypes.data, hits.ctypes.data, inst.ctypes.data, N.MEM_HOST, None),
+                "bvhc_scene_raycast")
+        return counts, hits, inst
+
     def dispose(self):
         if self.h:
             N.lib().bvhc_scene_destroy(self.h)

@@ -1609,6 +1609,8 @@ struct bvhc_scene {
   uint32_t* d_queue = nullptr;
   size_t queue_cap = 0;
   unsigned int* d_qcount = nullptr;
+  void* d_cnt = nullptr;  // host-memory bvhc_scene_raycast: per-ray counts
+  size_t cnt_cap = 0;
 };
 
 namespace {
@@ -1849,6 +1851,44 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   return read_and_clear_error(m, s);
 }
 
+bvhc_status bvhc_scene_raycast(bvhc_scene* sc, const float* rays, uint64_t n, int side, float near_dist,
+                               float far_dist, uint32_t cap, uint32_t* counts, bvhc_hit* hits, uint32_t* instance,
+                               int mem, void* stream) {
+  if (!sc || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
+  if (side < BVHC_FRONT_SIDE || side > BVHC_DOUBLE_SIDE) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!rays || !counts || (cap > 0 && (!hits || !instance))) return BVHC_ERR_INVALID_ARGUMENT;
+  bvhc_mesh* m = sc->batch;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  const SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
+  const uint32_t c = cap > 0 ? cap : 1;  // cap 0: counts only (one scratch slot per ray)
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && (!aligned(hits, 16) || !aligned(instance, 4))))
+      return BVHC_ERR_INVALID_ARGUMENT;
+    if (cap > 0)
+      return from_cuda(launch_scene_raycast_all(m->view(), sd, rays, n, side, near_dist, far_dist, cap, counts, hits,
+                                                instance, s));
+  }
+  const bool host = mem == BVHC_MEM_HOST;
+  if (host) BVHC_CUDA_TRY(ensure(&sc->d_in, &sc->in_cap, n * 24));
+  BVHC_CUDA_TRY(ensure(&sc->d_out, &sc->out_cap, n * c * sizeof(bvhc_hit)));
+  BVHC_CUDA_TRY(ensure(&sc->d_ids, &sc->ids_cap, n * c * 4));
+  if (host) BVHC_CUDA_TRY(ensure(&sc->d_cnt, &sc->cnt_cap, n * 4));
+  if (host) BVHC_CUDA_TRY(cudaMemcpyAsync(sc->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
+  const float* d_rays = host ? static_cast<const float*>(sc->d_in) : rays;
+  uint32_t* d_counts = host ? static_cast<uint32_t*>(sc->d_cnt) : counts;
+  BVHC_CUDA_TRY(launch_scene_raycast_all(m->view(), sd, d_rays, n, side, near_dist, far_dist, c, d_counts,
+                                         static_cast<bvhc_hit*>(sc->d_out), static_cast<uint32_t*>(sc->d_ids), s));
+  if (!host) return BVHC_OK;  // counts only, on the device
+  BVHC_CUDA_TRY(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
+  if (cap > 0) {
+    BVHC_CUDA_TRY(cudaMemcpyAsync(hits, sc->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(instance, sc->d_ids, n * cap * 4, cudaMemcpyDeviceToHost, s));
+  }
+  return read_and_clear_error(m, s);
+}
+
 void bvhc_scene_destroy(bvhc_scene* sc) {
   if (!sc) return;
   if (sc->batch) cudaSetDevice(sc->batch->device);
@@ -1859,6 +1899,7 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
   cudaFree(sc->d_ids);
   cudaFree(sc->d_queue);
   cudaFree(sc->d_qcount);
+  cudaFree(sc->d_cnt);
   free_sort_scratch(sc->sort_s);
   delete sc;
 }

@@ -1728,6 +1728,133 @@ __global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev 
   inst_out[i] = best_inst;
 }
 
+// Instanced raycast (all hits): the BatchedMesh raycast without firstHitOnly.  Every entered
+// instance box (no pruning: the count covers every hit) is walked in the instance's frame with the
+// reference's all-hits DFS (left child before right), each hit converted to world space and
+// inserted into the ray's row kept sorted by (world distance, instance): the raycaster's stable
+// sort of the per-instance hit lists concatenated in instance order.  Stores the first `cap`,
+// counts[i] the total.
+__global__ void __launch_bounds__(kBlock, 5) scene_raycast_all_kernel(MeshDev m, SceneDev sc,
+                                                                      const float* __restrict__ rays, uint64_t n,
+                                                                      int side, float near_d, float far_d, uint32_t cap,
+                                                                      uint32_t* __restrict__ counts,
+                                                                      bvhc_hit* __restrict__ hits,
+                                                                      uint32_t* __restrict__ inst_out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RayF w = make_ray(rays, i);
+  const SideTable no_sides{};
+  bvhc_hit* row = hits + i * (uint64_t)cap;
+  uint32_t* irow = inst_out + i * (uint64_t)cap;
+  uint32_t cnt = 0, stored = 0;
+  uint32_t tstack[kMaxStack];
+  uint32_t bstack[kMaxStack];
+  int tsp = 0;
+  uint32_t link = sc.root;
+  bool go = link != kEmptyLeaf;
+  while (go) {
+    while (go && !(link & kLeafBit)) {
+      const Pair p = load_pair(sc.nodes, link);
+      float e0, e1;
+      const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, kInf, e0);
+      const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, kInf, e1);
+      if (h0 && h1) {
+        if (tsp >= kMaxStack) {
+          atomicOr(m.err, kErrStackOverflow);
+          go = false;
+          break;
+        }
+        tstack[tsp++] = p.lr;
+        link = p.ll;
+      } else if (h0 || h1) {
+        link = h0 ? p.ll : p.lr;
+      } else if (tsp > 0) {
+        link = tstack[--tsp];
+      } else {
+        go = false;
+      }
+    }
+    if (!go) break;
+    const uint32_t j = link & ~kLeafBit;
+    const InstanceDev& I = sc.inst[j];
+    LocalRay L;
+    if (local_ray(I, w, near_d, far_d, L)) {
+      const ff dlen = dir_length(L.r.d);
+      const uint32_t g = I.geometry;
+      for (uint32_t root = sc.mesh_root_off[g]; root < sc.mesh_root_off[g + 1]; ++root) {
+        uint32_t bl = m.roots[root];
+        int bsp = 0;
+        for (;;) {
+          if (bl & kLeafBit) {
+            if (bl != kEmptyLeaf) {
+              for (uint32_t k = bl & ~kLeafBit;; ++k) {
+                const Tri t = load_tri(m.tris, k);
+                const int ts = tri_side(t, side, no_sides);
+                if (ts >= 0 && tri_hit(t.a, t.b, t.c, L.r.o, L.r.d, L.r.d_l1, ts)) {
+                  const ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, L.r.o, L.r.d));
+                  const ff dist = ff_mul(tt, dlen);
+                  if (!ff_lt(dist, ff_from(L.near_d)) && !ff_lt(ff_from(L.far_d), dist)) {
+                    ++cnt;
+                    bvhc_hit h;
+                    world_record(m, I, k, w, L.r, h);
+                    // stable sorted insert by (distance, instance)
+                    uint32_t pos = stored;
+                    while (pos > 0) {
+                      const float pd = row[pos - 1].distance;
+                      if (pd < h.distance || (pd == h.distance && irow[pos - 1] <= j)) break;
+                      --pos;
+                    }
+                    if (pos < cap) {
+                      const uint32_t last = stored < cap ? stored : cap - 1;
+                      for (uint32_t q = last; q > pos; --q) {
+                        row[q] = row[q - 1];
+                        irow[q] = irow[q - 1];
+                      }
+                      row[pos] = h;
+                      irow[pos] = j;
+                      if (stored < cap) ++stored;
+                    }
+                  }
+                }
+                if (t.flags & kTriLast) break;
+              }
+            }
+          } else {
+            const Pair p = load_pair(m.nodes, bl);
+            float e0, e1;
+            const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], L.r, L.near_d, L.far_d, e0);
+            const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], L.r, L.near_d, L.far_d, e1);
+            if (h0) {
+              if (h1) {
+                if (bsp >= kMaxStack) {
+                  atomicOr(m.err, kErrStackOverflow);
+                  break;
+                }
+                bstack[bsp++] = p.lr;
+              }
+              bl = p.ll;
+              continue;
+            }
+            if (h1) {
+              bl = p.lr;
+              continue;
+            }
+          }
+          if (bsp == 0) break;
+          bl = bstack[--bsp];
+        }
+      }
+    }
+    if (tsp == 0) break;
+    link = tstack[--tsp];
+  }
+  for (uint32_t q = stored; q < cap; ++q) {
+    store_miss(row + q);
+    irow[q] = 0xFFFFFFFFu;
+  }
+  counts[i] = cnt;
+}
+
 // Morton keys of world rays over the instances' box (ray_key), ids in input order.
 __global__ void __launch_bounds__(kBlock) scene_key_kernel(const float* __restrict__ rays, uint64_t n, int kind,
                                                            SceneBox box, uint32_t* __restrict__ ids,
@@ -2319,6 +2446,15 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
   }
   dev::scene_raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(
       blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d, hits, instance);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
+                                     int side, float near_d, float far_d, uint32_t cap, uint32_t* counts,
+                                     bvhc_hit* hits, uint32_t* instance, cudaStream_t stream) {
+  if (n == 0 || cap == 0) return cudaSuccess;
+  dev::scene_raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, side, near_d, far_d,
+                                                                        cap, counts, hits, instance);
   return cudaGetLastError();
 }
 

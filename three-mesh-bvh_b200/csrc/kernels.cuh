@@ -139,6 +139,12 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
                                        cudaStream_t stream, const RaySort* sort = nullptr, uint32_t* queue = nullptr,
                                        unsigned int* qcount = nullptr);
 
+// Instanced raycast (all hits): per ray the total count and the first `cap` world-space hits by
+// (distance, instance); instance n x cap (0xFFFFFFFF past the count).
+cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
+                                     int side, float near_d, float far_d, uint32_t cap, uint32_t* counts,
+                                     bvhc_hit* hits, uint32_t* instance, cudaStream_t stream);
+
 // intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
 // 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.
 cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
