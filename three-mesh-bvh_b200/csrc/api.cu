@@ -1055,7 +1055,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 4;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 5;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
@@ -1259,12 +1259,19 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   if (mem == BVHC_MEM_DEVICE && (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))))
     return BVHC_ERR_INVALID_ARGUMENT;
   // the warp-cooperative variants over sorted rays (all = 2..4: key kind all - 1) use queue slot 4
-  // and its sort scratch
-  const int variant = m->cfg.all >= 2 ? 2 : m->cfg.all;
+  // and its sort scratch; all = 5 (one ray per thread over the rays that enter the tree) the queue
+  const int variant = m->cfg.all == 5 ? 5 : (m->cfg.all >= 2 ? 2 : m->cfg.all);
   uint32_t* q = nullptr;
   unsigned int* qc = nullptr;
   RaySort sort{};
   const int slot = 4;
+  if (variant == 5 && n < (1ull << 32)) {
+    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
+    if (!m->d_qcount[slot])
+      BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
+    q = m->d_queue[slot];
+    qc = m->d_qcount[slot];
+  }
   if (variant == 2 && n < (1ull << 32)) {
     BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
     if (!m->d_qcount[slot])
@@ -1281,14 +1288,14 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   }
   if (mem == BVHC_MEM_DEVICE)
     return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s, variant,
-                                        m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+                                        m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
                                    static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s, variant,
-                                   m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+                                   m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));

@@ -537,8 +537,15 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
 __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
                                                              int side, const SideTable sides, float near_d,
                                                              float far_d, uint32_t cap, uint32_t* __restrict__ counts,
-                                                             bvhc_hit* __restrict__ hits) {
+                                                             bvhc_hit* __restrict__ hits,
+                                                             const uint32_t* __restrict__ queue = nullptr,
+                                                             const unsigned int* __restrict__ qcount = nullptr) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // with a queue, thread i traces ray queue[i] (the rays the pre-pass found entering the tree)
+  if (queue) {
+    if (i >= (uint64_t)__ldg(qcount)) return;
+    i = __ldg(queue + i);
+  }
   if (i >= n) return;
   RayF r = make_ray(rays, i);
   ff dlen = dir_length(r.d);
@@ -2310,12 +2317,26 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
                                cudaStream_t stream, int variant, int occupancy, uint32_t* queue, unsigned int* qcount,
                                const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  if (variant == 0 || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
+  if (variant == 0 || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32))) ||
+      (variant == 5 && (!queue || !qcount || n >= (1ull << 32)))) {
     dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap,
                                                                       counts, hits);
     return cudaGetLastError();
   }
   cudaError_t e;
+  if (variant == 5) {
+    // the root-box pre-pass gives the rays that miss a count of 0 and queues the others, in ray
+    // order, for one ray per thread: a warp then holds 32 rays that enter the tree
+    if ((e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+    const unsigned int g = (unsigned int)((n + dev::kClsTile - 1) / dev::kClsTile);
+    dev::classify_kernel<false><<<g, dev::kClsThreads, 0, stream>>>(m, BatchDev{nullptr, nullptr, 0}, rays, n, near_d,
+                                                                    far_d, nullptr, queue, qcount, nullptr, 0,
+                                                                    dev::SceneBox{}, counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap,
+                                                                      counts, hits, queue, qcount);
+    return cudaGetLastError();
+  }
   if (variant == 2) {
     // the root-box pre-pass gives the rays that miss a count of 0 and queues the others with their
     // keys, which are then sorted

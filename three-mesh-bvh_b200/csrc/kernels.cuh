@@ -42,7 +42,8 @@ struct TraversalConfig {
                    // over Morton-sorted queries (1 and 2 only with minThreshold 0)
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
   int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2..4 warp-cooperative
-                   // over the rays that enter the tree, sorted by key kind all - 1
+                   // over the rays that enter the tree, sorted by key kind all - 1, 5 one ray per thread
+                   // over the rays that enter the tree
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -102,7 +103,8 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
 
 // raycast (all hits).  variant 0: one ray per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the rays sorted by the key sort->kind (queue, qcount and sort scratch for
-// n rays required, else variant 0 runs).
+// n rays required, else variant 0 runs); 5: one ray per thread over the rays the root-box pre-pass
+// queues (queue and qcount for n rays required).
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream, int variant = 0, int occupancy = 0, uint32_t* queue = nullptr,
