@@ -1055,7 +1055,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 5;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 8;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
@@ -1259,8 +1259,9 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   if (mem == BVHC_MEM_DEVICE && (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && !aligned(hits, 16))))
     return BVHC_ERR_INVALID_ARGUMENT;
   // the warp-cooperative variants over sorted rays (all = 2..4: key kind all - 1) use queue slot 4
-  // and its sort scratch; all = 5 (one ray per thread over the rays that enter the tree) the queue
-  const int variant = m->cfg.all == 5 ? 5 : (m->cfg.all >= 2 ? 2 : m->cfg.all);
+  // and its sort scratch; one ray per thread over the rays that enter the tree (all = 5 in ray
+  // order, 6..8 sorted by key kind all - 5) too
+  const int variant = m->cfg.all >= 5 ? 5 : (m->cfg.all >= 2 ? 2 : m->cfg.all);
   uint32_t* q = nullptr;
   unsigned int* qc = nullptr;
   RaySort sort{};
@@ -1271,6 +1272,15 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
       BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
     q = m->d_queue[slot];
     qc = m->d_qcount[slot];
+    if (m->cfg.all > 5) {
+      BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
+      sort.kind = m->cfg.all - 5;
+      for (int a = 0; a < 3; ++a) {
+        sort.lo[a] = m->scene_lo[a];
+        sort.hi[a] = m->scene_hi[a];
+      }
+      sort.scratch = m->sort_s[slot];
+    }
   }
   if (variant == 2 && n < (1ull << 32)) {
     BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));

@@ -2325,14 +2325,26 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
   }
   cudaError_t e;
   if (variant == 5) {
-    // the root-box pre-pass gives the rays that miss a count of 0 and queues the others, in ray
-    // order, for one ray per thread: a warp then holds 32 rays that enter the tree
+    // the root-box pre-pass gives the rays that miss a count of 0 and queues the others (in ray
+    // order, or sorted by the key sort->kind) for one ray per thread: a warp then holds 32 rays
+    // that enter the tree (neighbouring ones with a key)
     if ((e = cudaMemsetAsync(qcount, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
     const unsigned int g = (unsigned int)((n + dev::kClsTile - 1) / dev::kClsTile);
+    const bool keyed = sort && sort->kind > 0;
+    uint32_t *ids = queue, *keys = nullptr;
+    dev::SceneBox box{};
+    if (keyed) {
+      ray_sort_input(sort->kind, sort->scratch, queue, &ids, &keys);
+      for (int a = 0; a < 3; ++a) {
+        box.lo[a] = sort->lo[a];
+        box.hi[a] = sort->hi[a];
+      }
+    }
     dev::classify_kernel<false><<<g, dev::kClsThreads, 0, stream>>>(m, BatchDev{nullptr, nullptr, 0}, rays, n, near_d,
-                                                                    far_d, nullptr, queue, qcount, nullptr, 0,
-                                                                    dev::SceneBox{}, counts);
+                                                                    far_d, nullptr, ids, qcount, keys,
+                                                                    keyed ? sort->kind : 0, box, counts);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (keyed && (e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
     dev::raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap,
                                                                       counts, hits, queue, qcount);
     return cudaGetLastError();

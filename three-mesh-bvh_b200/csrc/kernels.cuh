@@ -42,8 +42,8 @@ struct TraversalConfig {
                    // over Morton-sorted queries (1 and 2 only with minThreshold 0)
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
   int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2..4 warp-cooperative
-                   // over the rays that enter the tree, sorted by key kind all - 1, 5 one ray per thread
-                   // over the rays that enter the tree
+                   // over the rays that enter the tree, sorted by key kind all - 1, 5..8 one ray per
+                   // thread over the rays that enter the tree (6..8 sorted by key kind all - 5)
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
