@@ -600,7 +600,7 @@ def run_all_hits(args, ws, rank, local):
 
             # the all-hits kernel variant for this set (one call each, on the same buffers)
             t_var = {}
-            for v in (0, 1, 2, 3, 4, 5, 6, 7, 8):
+            for v in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12):
                 bvh.set_traversal(**{**cur, "all": v})
                 call()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

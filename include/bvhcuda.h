@@ -159,7 +159,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * that enter the tree (the others get a zero count), sorted by the key sort = all - 1 names above
  * (the direction, the entry point, the entry point and the direction), 5 one ray per thread over
  * the rays that enter the tree (the others get a zero count), 6, 7 and 8 the same sorted by key
- * sort = all - 5.  Results are the same for every variant (up to exact ties); the
+ * sort = all - 5, 9 to 12 the same walked by persistent warps that refill idle lanes (10 to 12
+ * sorted by key all - 9).  Results are the same for every variant (up to exact ties); the
  * autotuner picks the fastest per mesh and workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;

@@ -10,7 +10,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("variant,occupancy", [(0, 0), (1, 0), (1, 2), (2, 2), (3, 2), (4, 0), (5, 0), (6, 0), (8, 0)])
+@pytest.mark.parametrize("variant,occupancy", [(0, 0), (1, 0), (1, 2), (2, 2), (3, 2), (4, 0), (5, 0), (6, 0), (8, 0), (9, 0), (11, 0)])
 def test_all_hits_variants_keep_reference_order(pkg, orc, cuda, variant, occupancy):
     import torch
 

@@ -74,10 +74,11 @@ def tune_raycast_first(bvh, rays, side: int = 0, near: float = 0.0, far: float =
     return entry
 
 
-def tune_raycast_all(bvh, rays, cap: int = 64, reps: int = 3, candidates=(0, 1, 2, 3, 4, 5, 6, 7, 8)) -> dict:
+def tune_raycast_all(bvh, rays, cap: int = 64, reps: int = 3, candidates=tuple(range(13))) -> dict:
     """Time raycast's (all hits) kernels (the `all` field: per ray, warp-cooperative,
     warp-cooperative over rays sorted by the direction / entry-point / entry-point-and-direction
-    key, one ray per thread over the rays that enter the tree, in ray order or sorted by each key)
+    key, one ray per thread over the rays that enter the tree, in ray order or sorted by each key,
+    and the same with persistent warps)
     on `rays` (torch CUDA tensor,
     n x 6), keeping the mesh's other traversal fields, and install the fastest."""
     import torch

@@ -26,6 +26,7 @@ struct bvhc_mesh {
   uint32_t* d_roots = nullptr;
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
+  unsigned long long* d_work_all = nullptr;  // work counter of the persistent raycast (all hits) kernel
   TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
@@ -905,6 +906,7 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_refit_pos);
   cudaFree(m->d_err);
   cudaFree(m->d_work);
+  cudaFree(m->d_work_all);
   cudaFree(m->d_in);
   cudaFree(m->d_out);
   cudaFree(m->d_out2);
@@ -1055,7 +1057,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 8;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12;
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
@@ -1261,20 +1263,23 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   // the warp-cooperative variants over sorted rays (all = 2..4: key kind all - 1) use queue slot 4
   // and its sort scratch; one ray per thread over the rays that enter the tree (all = 5 in ray
   // order, 6..8 sorted by key kind all - 5) too
-  const int variant = m->cfg.all >= 5 ? 5 : (m->cfg.all >= 2 ? 2 : m->cfg.all);
+  const int variant = m->cfg.all >= 9 ? 9 : (m->cfg.all >= 5 ? 5 : (m->cfg.all >= 2 ? 2 : m->cfg.all));
+  const int key_of_variant = m->cfg.all >= 9 ? m->cfg.all - 9 : m->cfg.all - 5;
   uint32_t* q = nullptr;
   unsigned int* qc = nullptr;
   RaySort sort{};
   const int slot = 4;
-  if (variant == 5 && n < (1ull << 32)) {
+  if ((variant == 5 || variant == 9) && n < (1ull << 32)) {
     BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
     if (!m->d_qcount[slot])
       BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
+    if (variant == 9 && !m->d_work_all)
+      BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_work_all), sizeof(unsigned long long)));
     q = m->d_queue[slot];
     qc = m->d_qcount[slot];
-    if (m->cfg.all > 5) {
+    if (key_of_variant > 0) {
       BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
-      sort.kind = m->cfg.all - 5;
+      sort.kind = key_of_variant;
       for (int a = 0; a < 3; ++a) {
         sort.lo[a] = m->scene_lo[a];
         sort.hi[a] = m->scene_hi[a];
@@ -1298,14 +1303,14 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   }
   if (mem == BVHC_MEM_DEVICE)
     return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s, variant,
-                                        m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr));
+                                        m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
                                    static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s, variant,
-                                   m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr));
+                                   m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));

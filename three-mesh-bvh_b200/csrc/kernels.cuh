@@ -43,7 +43,8 @@ struct TraversalConfig {
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
   int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2..4 warp-cooperative
                    // over the rays that enter the tree, sorted by key kind all - 1, 5..8 one ray per
-                   // thread over the rays that enter the tree (6..8 sorted by key kind all - 5)
+                   // thread over the rays that enter the tree (6..8 sorted by key kind all - 5), 9..12
+                   // the same with persistent warps and lane refill (10..12 sorted by key all - 9)
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -104,11 +105,13 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
 // raycast (all hits).  variant 0: one ray per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the rays sorted by the key sort->kind (queue, qcount and sort scratch for
 // n rays required, else variant 0 runs); 5: one ray per thread over the rays the root-box pre-pass
-// queues (queue and qcount for n rays required).
+// queues (queue and qcount for n rays required; sorted by sort->kind when given); 9: the same
+// queue walked by persistent warps with lane refill (also a zeroed-per-call work counter).
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream, int variant = 0, int occupancy = 0, uint32_t* queue = nullptr,
-                               unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
+                               unsigned int* qcount = nullptr, const RaySort* sort = nullptr,
+                               unsigned long long* work = nullptr);
 
 // intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
 // sphere i.
