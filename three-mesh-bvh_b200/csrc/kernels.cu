@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const fl
 // lengths from ~10 to ~1000 node reads, so a warp that only took new rays when all 32 were done
 // would spend most of its time waiting on its longest one.  Each lane walks its ray exactly as
 // raycast_all_kernel does (left child before right, every hit in DFS order).
-constexpr int kAllRefill = 16;
+constexpr int kAllRefill = 8;
 
 __global__ void __launch_bounds__(kBlock) raycast_all_persistent_kernel(
     MeshDev m, const float* __restrict__ rays, int side, const SideTable sides, float near_d, float far_d, uint32_t cap,
