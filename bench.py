@@ -809,7 +809,7 @@ def run_scene(args, ws, rank, local):
 
     # ray order: input order or one of the Morton keys, whichever is fastest here
     order_ms = {}
-    for order in (0, 1, 2, 3):
+    for order in (0, 1, 2, 3, 4):
         scene.set_order(order)
         step()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

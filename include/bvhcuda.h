@@ -304,8 +304,9 @@ bvhc_status bvhc_scene_raycast(bvhc_scene* scene, const float* rays, uint64_t n,
                                int mem, void* stream);
 void bvhc_scene_destroy(bvhc_scene* scene);
 /* Ray order of bvhc_scene_raycast_first: 0 input order; 1, 2, 3 the rays sorted by a Morton key
- * (direction; entry point into the instances' world box; that point and the direction) so that
- * the rays of a warp share their paths.  Results are the same; results land in the rays' rows. */
+ * (direction; entry point into the instances' world box; that point and the direction); 4 sorted
+ * by the first instance the ray reaches in the instance tree, so that the rays of a warp walk the
+ * same geometry tree.  Results are the same; results land in the rays' rows. */
 bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind);
 
 /* raycastFirst that allocates nothing.  No counterpart in the reference: it exists for callers

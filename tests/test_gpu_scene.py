@@ -72,7 +72,7 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
     assert not bad, bad[:10]
     assert (einst >= 0).mean() > 0.2
     # device buffers, and every ray order, give the same records
-    for order in (0, 1, 2, 3):
+    for order in (0, 1, 2, 3, 4):
         scene.set_order(order)
         dh, di = scene.raycast_first(torch.from_numpy(rays).to(cuda))
         torch.cuda.synchronize()

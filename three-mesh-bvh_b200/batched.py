@@ -191,8 +191,9 @@ class InstancedScene:
                                                  None if v is None else v.ctypes.data), "bvhc_scene_set_instances")
 
     def set_order(self, kind: int):
-        """Traverse the rays in input order (0) or sorted by a Morton key: 1 direction, 2 entry
-        point into the instances' box, 3 entry point and direction.  Results do not change."""
+        """Traverse the rays in input order (0), sorted by a Morton key (1 direction, 2 entry point
+        into the instances' box, 3 entry point and direction) or by the first instance they reach
+        (4).  Results do not change."""
         N.check(N.lib().bvhc_scene_set_order(self.h, int(kind)), "bvhc_scene_set_order")
 
     def raycast_first(self, rays, side=FrontSide, near=0.0, far=float("inf"), stream=None):

@@ -1927,7 +1927,7 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
 }
 
 bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind) {
-  if (!scene || kind < 0 || kind > 3) return BVHC_ERR_INVALID_ARGUMENT;
+  if (!scene || kind < 0 || kind > 4) return BVHC_ERR_INVALID_ARGUMENT;
   scene->order = kind;
   return BVHC_OK;
 }

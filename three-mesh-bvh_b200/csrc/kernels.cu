@@ -1972,16 +1972,50 @@ __global__ void __launch_bounds__(kBlock, 5) scene_raycast_all_kernel(MeshDev m,
   counts[i] = cnt;
 }
 
-// Morton keys of world rays over the instances' box (ray_key), ids in input order.
+// Keys of world rays, ids in input order: kinds 1..3 a Morton key over the instances' box
+// (ray_key); kind 4 the first instance the ray's nearest-first descent of the instance tree
+// reaches (0xFFFFFF: none), so that a warp's rays walk the same geometry tree.
 __global__ void __launch_bounds__(kBlock) scene_key_kernel(const float* __restrict__ rays, uint64_t n, int kind,
-                                                           SceneBox box, uint32_t* __restrict__ ids,
+                                                           SceneBox box, SceneDev sc, uint32_t* __restrict__ ids,
                                                            uint32_t* __restrict__ keys, unsigned int* qcount) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *qcount = (unsigned int)n;
   if (i >= n) return;
   const RayF r = make_ray(rays, i);
   ids[i] = (uint32_t)i;
-  keys[i] = ray_key(kind, r.o, r.d, box);
+  if (kind != 4) {
+    keys[i] = ray_key(kind, r.o, r.d, box);
+    return;
+  }
+  uint32_t key = 0xFFFFFFu;
+  uint32_t stack_link[kMaxStack];
+  int sp = 0;
+  uint32_t link = sc.root;
+  bool go = link != kEmptyLeaf;
+  while (go) {
+    if (link & kLeafBit) {
+      key = (link & ~kLeafBit) & 0xFFFFFFu;
+      break;
+    }
+    const Pair p = load_pair(sc.nodes, link);
+    float e0, e1;
+    const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], r, 0.0f, kInf, e0);
+    const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], r, 0.0f, kInf, e1);
+    const bool lf = e0 <= e1;
+    const uint32_t c1 = lf ? p.ll : p.lr, c2 = lf ? p.lr : p.ll;
+    const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
+    if (h1st) {
+      if (h2nd && sp < kMaxStack) stack_link[sp++] = c2;
+      link = c1;
+    } else if (h2nd) {
+      link = c2;
+    } else if (sp > 0) {
+      link = stack_link[--sp];
+    } else {
+      go = false;
+    }
+  }
+  keys[i] = key;
 }
 
 // Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
@@ -2593,7 +2627,8 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
       box.lo[a] = sort->lo[a];
       box.hi[a] = sort->hi[a];
     }
-    dev::scene_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(rays, n, sort->kind, box, ids, keys, qcount);
+    dev::scene_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(rays, n, sort->kind, box, scene, ids, keys,
+                                                                     qcount);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;

@@ -138,7 +138,7 @@ struct SceneDev {
 // World-space raycastFirst over the instances: hits[i] in world space (distance, point; local
 // barycoord and faceIndex), instance[i] the hit instance (0xFFFFFFFF: none).  With `sort` (kind
 // 1..3, its box the instances' world box, scratch and a queue / qcount for n rays) the rays are
-// traversed in the order of their Morton keys.
+// traversed in the order of their Morton keys; kind 4 orders them by the first instance reached.
 cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scene, const float* rays, uint64_t n,
                                        int side, float near_d, float far_d, bvhc_hit* hits, uint32_t* instance,
                                        cudaStream_t stream, const RaySort* sort = nullptr, uint32_t* queue = nullptr,
