@@ -363,6 +363,18 @@ bvhc_status bvhc_hit_interpolate(bvhc_mesh* mesh, const bvhc_hit* hits, uint64_t
 bvhc_status bvhc_intersects_sphere(bvhc_mesh* mesh, const float* spheres, uint64_t n, uint8_t* out, int mem,
                                    void* stream);
 
+/* The triangles within each sphere, collected through shapecast's CONTAINED path (src/core/cast/
+ * shapecast.js:41-214: a node box the sphere contains hands its whole triangle range on with
+ * contained = true, :111-117) with the callbacks of the reference's sculpting / selection use:
+ * a box the sphere misses is skipped (Sphere.intersectsBox), one whose 8 corners lie within the
+ * radius is CONTAINED (Sphere.containsPoint), other boxes' triangles are tested one by one
+ * (ExtendedTriangle.intersectsSphere).  spheres: n x 4 float32 (centre, radius; device buffers
+ * 16-byte aligned); counts[i] the number collected; faces[i * cap ..] the first cap faceIndex
+ * values in the reference's traversal order (left child before right, a range in buffer order),
+ * BVHC_NO_HIT past the count.  cap 0 computes the counts only. */
+bvhc_status bvhc_sphere_triangles(bvhc_mesh* mesh, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
+                                  uint32_t* faces, int mem, void* stream);
+
 /* MeshBVH#intersectsBox(box, boxToMesh) for every box (src/core/MeshBVH.js:780-792: shapecast
  * with OrientedBox.intersectsBox / intersectsTriangle, src/math/OrientedBox.js:78-260).  boxes:
  * n x 24 float32 (min xyz, pad, max xyz, pad, then the column-major box-to-mesh matrix as three.js

@@ -952,6 +952,67 @@ bool box_traverse(const Bvh& g, const NodeView& nv, int64_t n32, const Obb& o, C
   return false;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Triangles within a sphere through shapecast's CONTAINED path (shapecast.js:41-214, the range
+// of a CONTAINED node passed on with contained = true, :111-117), with the callbacks of the
+// reference's sculpt / selection use: a node box is NOT_INTERSECTED when the sphere misses it
+// (Sphere.intersectsBox: the centre clamped to the box within r), CONTAINED when all 8 corners
+// lie within r (Sphere.containsPoint), else INTERSECTED; a triangle is collected when contained
+// or when it meets the sphere (ExtendedTriangle.intersectsSphere).
+// ---------------------------------------------------------------------------------------------
+int sphere_box_relation(const NodeView& nv, int64_t n32, V3 c, double r) {
+  const double r2 = r * r;
+  const double lo[3] = {nv.f(n32), nv.f(n32 + 1), nv.f(n32 + 2)}, hi[3] = {nv.f(n32 + 3), nv.f(n32 + 4), nv.f(n32 + 5)};
+  const double cc[3] = {c.x, c.y, c.z};
+  double q[3];
+  for (int d = 0; d < 3; ++d) q[d] = std::max(lo[d], std::min(hi[d], cc[d]));  // Vector3.clamp
+  if (!(dist_sq(V3{q[0], q[1], q[2]}, c) <= r2)) return 0;
+  for (int k = 0; k < 8; ++k) {
+    V3 p{(k & 1) ? hi[0] : lo[0], (k & 2) ? hi[1] : lo[1], (k & 4) ? hi[2] : lo[2]};
+    if (!(dist_sq(p, c) <= r2)) return 1;
+  }
+  return 2;
+}
+
+void subtree_range(const NodeView& nv, int64_t n32, int64_t& first, int64_t& end) {  // getLeft/RightEndOffset
+  int64_t l = n32;
+  while (!nv.is_leaf(l)) l = nv.left(l);
+  first = nv.offset(l);
+  int64_t r = n32;
+  while (!nv.is_leaf(r)) r = nv.right(r);
+  end = nv.offset(r) + nv.count(r);
+}
+
+void sphere_collect(const Bvh& g, const NodeView& nv, int64_t n32, V3 c, double r, bool contained,
+                    std::vector<int64_t>& out) {
+  if (contained || nv.is_leaf(n32)) {
+    int64_t first, end;
+    if (nv.is_leaf(n32)) {
+      first = nv.offset(n32);
+      end = first + nv.count(n32);
+    } else {
+      subtree_range(nv, n32, first, end);
+    }
+    for (int64_t i = first; i < end; ++i) {
+      const int64_t tri = g.resolve(i);
+      if (contained) {
+        out.push_back(tri);
+        continue;
+      }
+      int64_t abc[3];
+      g.tri_vertices(tri, abc);
+      if (sphere_meets_triangle(c, r, g.vertex(abc[0]), g.vertex(abc[1]), g.vertex(abc[2]))) out.push_back(tri);
+    }
+    return;
+  }
+  const int64_t kids[2] = {nv.left(n32), nv.right(n32)};
+  for (int64_t k : kids) {
+    const int rel = sphere_box_relation(nv, k, c, r);
+    if (rel == 2) sphere_collect(g, nv, k, c, r, true, out);
+    else if (rel == 1) sphere_collect(g, nv, k, c, r, false, out);
+  }
+}
+
 template <class F>
 void parallel_for(int64_t n, int threads, F f) {
   if (threads <= 1 || n < 64) { f(0, n); return; }
@@ -1337,6 +1398,26 @@ void orc_scene_raycast_all(const orc_bvh* const* geoms, int n_instances, const u
           instance[i * cap + k] = -1;
         }
       }
+    }
+  });
+}
+
+// spheres: n x 4 float32.  counts[i] = triangles collected; faces[i * cap ..] the first cap of them
+// in traversal order (-1 past the count).
+void orc_sphere_triangles(const orc_bvh* h, const float* spheres, int64_t n, int cap, int32_t* counts, int64_t* faces,
+                          int threads) {
+  parallel_for(n, threads, [&](int64_t s, int64_t e) {
+    std::vector<int64_t> out;
+    for (int64_t i = s; i < e; ++i) {
+      out.clear();
+      const V3 c{spheres[4 * i], spheres[4 * i + 1], spheres[4 * i + 2]};
+      const double r = spheres[4 * i + 3];
+      for (const auto& root : h->b.roots) {
+        NodeView nv{root.data()};
+        sphere_collect(h->b, nv, 0, c, r, false, out);
+      }
+      counts[i] = (int32_t)out.size();
+      for (int k = 0; k < cap; ++k) faces[i * cap + k] = k < (int)out.size() ? out[k] : -1;
     }
   });
 }

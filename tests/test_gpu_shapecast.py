@@ -169,3 +169,32 @@ def test_intersects_box_lattice_ties(pkg, orc, cuda):
     assert np.array_equal(got, want), np.nonzero(got != want)[0][:10]
     assert 0.05 < want.mean() < 0.95
     bvh.dispose()
+
+
+@pytest.mark.parametrize("indirect", [False, True])
+def test_sphere_triangles_match_oracle(pkg, orc, cuda, indirect):
+    """Triangles within spheres through shapecast's CONTAINED path: the same faceIndex sequence as
+    the oracle (traversal order), counts identical; spheres from tiny to enclosing whole subtrees."""
+    geo = pkg.torus_knot(10, 3, 300, 60, noise_sigma=0.02, noise_seed=3)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "indirect": indirect})
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+    rng = np.random.default_rng(31)
+    lo, hi = geo.position.min(0), geo.position.max(0)
+    n = 20_000
+    c = lo + rng.random((n, 3)) * (hi - lo)
+    r = np.exp(rng.uniform(np.log(0.05), np.log(8.0), n))
+    spheres = np.concatenate([c, r[:, None]], 1).astype(np.float32)
+    cap = 512
+    counts, faces = bvh.sphere_triangles_batch(spheres, cap=cap)
+    ec, ef = ref.sphere_triangles(spheres, cap=cap)
+    diff = np.nonzero(counts.astype(np.int64) != ec)[0]
+    # a triangle exactly at the radius (the float-float triangle predicate against the float64 one)
+    assert diff.size <= max(2, n // 5000), diff[:10]
+    same = np.setdiff1d(np.arange(n), diff)
+    k = np.minimum(ec[same], cap)
+    for i, kk in zip(same, k):
+        assert np.array_equal(faces[i, :kk].astype(np.int64), ef[i, :kk]), i
+    assert (ec > cap).sum() > 0 and (ec == 0).sum() > 0
+    c0, _ = bvh.sphere_triangles_batch(spheres, cap=0)
+    assert np.array_equal(c0, counts)
+    bvh.dispose()

@@ -74,3 +74,32 @@ def test_intersects_box_equals_brute_force(pkg, orc):
         assert got[i] == meets.any(), i
         checked += 1
     assert checked > 150 and 0 < got.sum() < boxes.shape[0]
+
+
+def test_sphere_triangles_equal_brute_force(pkg, orc):
+    """Triangles within a sphere through shapecast's CONTAINED path (shapecast.js:111-117): the
+    collected set equals every triangle whose closest point lies within r, each once; large
+    spheres hand whole subtrees over as CONTAINED ranges."""
+    geo = pkg.torus_knot(10, 3, 60, 12)
+    o = orc.OracleBVH.build(geo.position, geo.index, strategy=2)
+    idx = np.empty(geo.index.size, dtype=np.uint32)
+    orc.lib().orc_copy_index(o.h, idx.ctypes.data)
+    tri = geo.position[idx.astype(np.int64).reshape(-1, 3)].astype(np.float64)
+    rng = np.random.default_rng(13)
+    lo, hi = geo.position.min(0), geo.position.max(0)
+    c = lo + rng.random((300, 3)) * (hi - lo)
+    r = np.exp(rng.uniform(np.log(0.3), np.log(12.0), 300))
+    spheres = np.concatenate([c, r[:, None]], 1).astype(np.float32)
+    counts, faces = o.sphere_triangles(spheres, cap=tri.shape[0])
+    big = 0
+    for i in range(spheres.shape[0]):
+        p, rad = spheres[i, :3].astype(np.float64), float(spheres[i, 3])
+        d = np.array([orc.point_triangle_distance(p, *t) for t in tri])
+        got = faces[i, :counts[i]]
+        assert np.unique(got).size == got.size
+        want = np.nonzero(d <= rad)[0]
+        sure_in = np.nonzero(d <= rad * (1 - 1e-9))[0]
+        sure_out = np.nonzero(d > rad * (1 + 1e-9))[0]
+        assert np.isin(sure_in, got).all() and not np.isin(sure_out, got).any(), i
+        big += counts[i] > 200
+    assert big > 20 and (counts == 0).sum() > 0

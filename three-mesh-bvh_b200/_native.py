@@ -76,6 +76,7 @@ SIGNATURES = [
     ("bvhc_mesh_read_root", _I, [_P, C.c_int, _P, C.c_uint64]),
     ("bvhc_intersects_sphere", _I, [_P, _P, _U64, _P, _I, _P]),
     ("bvhc_intersects_box", _I, [_P, _P, _U64, _P, _I, _P]),
+    ("bvhc_sphere_triangles", _I, [_P, _P, _U64, C.c_uint32, _P, _P, _I, _P]),
     ("bvhc_scene_create", _I, [_P, _I, _P, _P, _P, C.POINTER(_P)]),
     ("bvhc_scene_set_instances", _I, [_P, _I, _P, _P, _P]),
     ("bvhc_scene_raycast_first", _I, [_P, _P, _U64, _I, _F, _F, _P, _P, _I, _P]),

@@ -1458,6 +1458,32 @@ bvhc_status bvhc_intersects_box(bvhc_mesh* m, const float* boxes, uint64_t n, ui
   return read_and_clear_error(m, s);
 }
 
+bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
+                                  uint32_t* faces, int mem, void* stream) {
+  if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BVHC_OK;
+  if (!spheres || !counts || (cap > 0 && !faces)) return BVHC_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  const uint32_t c = cap > 0 ? cap : 1;
+  if (mem == BVHC_MEM_DEVICE && cap > 0) {
+    if (!aligned(spheres, 16) || !aligned(counts, 4) || !aligned(faces, 4)) return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_sphere_triangles(m->view(), spheres, n, cap, counts, faces, s));
+  }
+  const bool host = mem == BVHC_MEM_HOST;
+  if (host) BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 16));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * c * 4));
+  if (host) BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
+  if (host) BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, spheres, n * 16, cudaMemcpyHostToDevice, s));
+  uint32_t* d_counts = host ? static_cast<uint32_t*>(m->d_out2) : counts;
+  BVHC_CUDA_TRY(launch_sphere_triangles(m->view(), host ? static_cast<const float*>(m->d_in) : spheres, n, c, d_counts,
+                                        static_cast<uint32_t*>(m->d_out), s));
+  if (!host) return BVHC_OK;  // counts only, on the device
+  BVHC_CUDA_TRY(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
+  if (cap > 0) BVHC_CUDA_TRY(cudaMemcpyAsync(faces, m->d_out, n * cap * 4, cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint64_t n, float min_threshold,
                                         float max_threshold, bvhc_closest* out, int mem, void* stream) {
   if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;

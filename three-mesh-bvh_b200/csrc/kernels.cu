@@ -1207,6 +1207,115 @@ __global__ void __launch_bounds__(kBlock) intersects_sphere_kernel(MeshDev m, co
 }
 
 // ---------------------------------------------------------------------------------------------
+// Triangles within a sphere through shapecast's CONTAINED path (shapecast.js:41-214; a CONTAINED
+// node's whole range goes to the triangle callback with contained = true, :111-117), with the
+// callbacks of the reference's sculpt / selection use: a node box is skipped when the sphere
+// misses it (Sphere.intersectsBox), CONTAINED when its 8 corners lie within r
+// (Sphere.containsPoint), else its triangles are tested (ExtendedTriangle.intersectsSphere).  One
+// sphere per thread, left child before right; the triangles come out in the reference's order.
+// The box relations decide which triangles enter untested, so they follow the reference's
+// binary64 comparisons exactly: float32 with an error bound, else the binary64 sequence.
+// ---------------------------------------------------------------------------------------------
+// |p - c|^2 <= r^2 as the reference evaluates it (Vector3.distanceToSquared, radius * radius).
+__device__ __forceinline__ bool within_r(float3 p, float3 c, float r) {
+  const float dx = p.x - c.x, dy = p.y - c.y, dz = p.z - c.z;
+  const float d2 = dx * dx + dy * dy + dz * dz, r2 = r * r;
+  if (d2 * (1.0f + 0x1p-20f) < r2 * (1.0f - 0x1p-22f)) return true;
+  if (d2 * (1.0f - 0x1p-20f) > r2 * (1.0f + 0x1p-22f)) return false;
+  const sf::f64 ex = sf::sub(sf::from_f32(p.x), sf::from_f32(c.x)), ey = sf::sub(sf::from_f32(p.y), sf::from_f32(c.y)),
+                ez = sf::sub(sf::from_f32(p.z), sf::from_f32(c.z)), R = sf::from_f32(r);
+  return sf::le(sf::add(sf::add(sf::mul(ex, ex), sf::mul(ey, ey)), sf::mul(ez, ez)), sf::mul(R, R));
+}
+
+// 0 the sphere misses the box, 1 it meets it, 2 the box lies within the sphere.
+__device__ int sphere_box_relation(const float* b, float3 c, float r) {
+  const float3 q = make_float3(fmaxf(b[0], fminf(b[3], c.x)), fmaxf(b[1], fminf(b[4], c.y)), fmaxf(b[2], fminf(b[5], c.z)));
+  if (!within_r(q, c, r)) return 0;
+  for (int k = 0; k < 8; ++k)
+    if (!within_r(make_float3((k & 1) ? b[3] : b[0], (k & 2) ? b[4] : b[1], (k & 4) ? b[5] : b[2]), c, r)) return 1;
+  return 2;
+}
+
+__global__ void __launch_bounds__(kBlock) sphere_triangles_kernel(MeshDev m, const float* __restrict__ spheres,
+                                                                  uint64_t n, uint32_t cap,
+                                                                  uint32_t* __restrict__ counts,
+                                                                  uint32_t* __restrict__ faces) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 sph = ld4(spheres + 4 * i);
+  const float3 c = make_float3(sph.x, sph.y, sph.z);
+  const ff r2 = two_prod(sph.w, sph.w);
+  uint32_t* out = faces + i * (uint64_t)cap;
+  uint32_t cnt = 0;
+  uint32_t stack_link[kMaxStack];
+  uint8_t stack_rel[kMaxStack];
+  uint32_t sub[kMaxStack];
+  bool overflow = false;
+  for (int root = 0; root < m.n_roots && !overflow; ++root) {
+    int sp = 0;
+    stack_link[sp] = m.roots[root];
+    stack_rel[sp++] = 1;  // the root has no bounds test
+    while (sp > 0 && !overflow) {
+      --sp;
+      const uint32_t link = stack_link[sp];
+      const int rel = stack_rel[sp];
+      if (rel == 2) {  // CONTAINED: every triangle of the subtree, in order, untested
+        int ssp = 0;
+        sub[ssp++] = link;
+        while (ssp > 0) {
+          const uint32_t l = sub[--ssp];
+          if (l & kLeafBit) {
+            if (l == kEmptyLeaf) continue;
+            for (uint32_t k = l & ~kLeafBit;; ++k) {
+              const Tri t = load_tri(m.tris, k);
+              if (cnt < cap) out[cnt] = t.face;
+              ++cnt;
+              if (t.flags & kTriLast) break;
+            }
+          } else {
+            if (ssp + 2 > kMaxStack) {
+              overflow = true;
+              break;
+            }
+            const Pair p = load_pair(m.nodes, l);
+            sub[ssp++] = p.lr;
+            sub[ssp++] = p.ll;
+          }
+        }
+      } else if (link & kLeafBit) {
+        if (link == kEmptyLeaf) continue;
+        for (uint32_t k = link & ~kLeafBit;; ++k) {
+          const Tri t = load_tri(m.tris, k);
+          if (sphere_meets(c, r2, t)) {
+            if (cnt < cap) out[cnt] = t.face;
+            ++cnt;
+          }
+          if (t.flags & kTriLast) break;
+        }
+      } else {
+        const Pair p = load_pair(m.nodes, link);
+        const int rl = sphere_box_relation(p.l, c, sph.w), rr = sphere_box_relation(p.r, c, sph.w);
+        if (sp + 2 > kMaxStack) {
+          overflow = true;
+          break;
+        }
+        if (rr) {
+          stack_link[sp] = p.lr;
+          stack_rel[sp++] = (uint8_t)rr;
+        }
+        if (rl) {
+          stack_link[sp] = p.ll;
+          stack_rel[sp++] = (uint8_t)rl;
+        }
+      }
+    }
+  }
+  if (overflow) atomicOr(m.err, kErrStackOverflow);
+  for (uint32_t q = cnt; q < cap; ++q) out[q] = 0xFFFFFFFFu;
+  counts[i] = cnt;
+}
+
+// ---------------------------------------------------------------------------------------------
 // intersectsBox (MeshBVH.js:780-792): an OrientedBox (src/math/OrientedBox.js:78-260) tested
 // against node boxes (OrientedBox.intersectsBox: the three aligned extents, then the box's three
 // edge directions) and triangles (OrientedBox.intersectsTriangle: the box's axes, the triangle's
@@ -2644,6 +2753,13 @@ cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene,
   if (n == 0 || cap == 0) return cudaSuccess;
   dev::scene_raycast_all_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, side, near_d, far_d,
                                                                         cap, counts, hits, instance);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
+                                    uint32_t* faces, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::sphere_triangles_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, cap, counts, faces);
   return cudaGetLastError();
 }
 

@@ -150,6 +150,11 @@ cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene,
                                      int side, float near_d, float far_d, uint32_t cap, uint32_t* counts,
                                      bvhc_hit* hits, uint32_t* instance, cudaStream_t stream);
 
+// Triangles within each sphere (n x 4, 16-byte aligned) through shapecast's CONTAINED path:
+// counts[i] the total, faces[i * cap ..] the first cap faceIndex values in traversal order.
+cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
+                                    uint32_t* faces, cudaStream_t stream);
+
 // intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
 // 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.
 cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,

@@ -511,6 +511,18 @@ class MeshBVH:
                 "bvhc_intersects_sphere")
         return out.astype(bool)
 
+    def sphere_triangles_batch(self, spheres, cap: int = 256):
+        """The triangles within each sphere (cx, cy, cz, r), collected through shapecast's CONTAINED
+        path as in the reference's sculpting / selection use: numpy -> (counts, faces (n, cap)) with
+        faceIndex values in traversal order, 0xFFFFFFFF past the count."""
+        lib, mesh = N.lib(), self._device_mesh()
+        sp = np.ascontiguousarray(spheres, dtype=np.float32).reshape(-1, 4)
+        counts = np.empty(sp.shape[0], dtype=np.uint32)
+        faces = np.empty((sp.shape[0], cap), dtype=np.uint32)
+        N.check(lib.bvhc_sphere_triangles(mesh, _ptr(sp), sp.shape[0], cap, _ptr(counts), _ptr(faces), N.MEM_HOST,
+                                          None), "bvhc_sphere_triangles")
+        return counts, faces
+
     @staticmethod
     def box_records(box_min, box_max, box_to_mesh) -> np.ndarray:
         """Pack oriented boxes for intersects_box_batch: (n x 3) min, (n x 3) max and (n x 16)
