@@ -42,11 +42,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--workload", choices=["first", "batched", "adjoint", "closest", "all", "build", "scene"],
+    ap.add_argument("--workload",
+                    choices=["first", "batched", "adjoint", "closest", "all", "build", "scene", "shapecast"],
                     default="first",
                     help="first: the headline raycastFirst line; batched: the 1024-geometry BatchedMesh form; "
                          "adjoint: forward/backward timing; closest: the 256^3 closest-point grid; all: raycast "
-                         "(all hits); build: the device SAH build; scene: instanced BatchedMesh raycastFirst")
+                         "(all hits); build: the device SAH build; scene: instanced BatchedMesh raycastFirst; "
+                         "shapecast: triangles within spheres, intersectsSphere, intersectsBox")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
@@ -966,6 +968,152 @@ def run_build(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def shapecast_queries(geo, rng, n_brush, n_sphere, n_box):
+    """Query sets on the mesh: sculpt brushes (spheres centred on random triangle centroids,
+    radius log-uniform 0.03..0.3, i.e. a few to a few hundred triangles), spheres anywhere in the
+    bounding box (radius log-uniform 0.01..2) and oriented boxes (random rotation, half extents
+    0.05..1) as rows of 24 float32 (min xyz, 0, max xyz, 0, column-major box-to-mesh matrix)."""
+    pos, idx = geo.position.astype(np.float64), geo.index.reshape(-1, 3)
+    t = rng.integers(0, idx.shape[0], n_brush)
+    cen = pos[idx[t]].mean(1)
+    brush = np.concatenate([cen, np.exp(rng.uniform(np.log(0.03), np.log(0.3), n_brush))[:, None]], 1)
+    lo, hi = pos.min(0), pos.max(0)
+    sph = np.concatenate([lo + rng.random((n_sphere, 3)) * (hi - lo),
+                          np.exp(rng.uniform(np.log(0.01), np.log(2.0), n_sphere))[:, None]], 1)
+    q = rng.normal(size=(n_box, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    x, y, z, w = q.T
+    m = np.zeros((n_box, 16))
+    m[:, 0], m[:, 1], m[:, 2] = 1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)
+    m[:, 4], m[:, 5], m[:, 6] = 2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x)
+    m[:, 8], m[:, 9], m[:, 10] = 2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)
+    m[:, 12:15] = lo + rng.random((n_box, 3)) * (hi - lo)
+    m[:, 15] = 1
+    half = rng.uniform(0.05, 1.0, (n_box, 3))
+    box = np.zeros((n_box, 24))
+    box[:, 0:3], box[:, 4:7], box[:, 8:24] = -half, half, m
+    f = np.float32
+    return brush.astype(f), sph.astype(f), box.astype(f)
+
+
+def run_shapecast(args, ws, rank, local):
+    """Shapecast queries on the 2M-triangle knot: triangles within sculpt-brush spheres (shapecast's
+    CONTAINED path), intersectsSphere and intersectsBox (oriented boxes)."""
+    import torch
+
+    import __graft_entry__ as ge
+
+    pkg = ge.load_package()
+    from three_mesh_bvh_b200._native import check
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
+    n_brush, n_sphere, n_box, cap = 1 << 18, 1 << 22, 1 << 20, 256
+    brush_h, sph_h, box_h = shapecast_queries(geo, np.random.default_rng(7 + rank), n_brush, n_sphere, n_box)
+    lib = pkg.lib()
+    mesh = bvh._device_mesh()
+    stream = torch.cuda.current_stream(dev)
+    s = stream.cuda_stream
+    brush, sph, box = (torch.from_numpy(x).to(dev) for x in (brush_h, sph_h, box_h))
+    counts = torch.empty(n_brush, dtype=torch.int32, device=dev)
+    faces = torch.empty((n_brush, cap), dtype=torch.int32, device=dev)
+    flags = torch.empty(max(n_sphere, n_box), dtype=torch.uint8, device=dev)
+    calls = {
+        "sphere_triangles": (n_brush, lambda: check(lib.bvhc_sphere_triangles(
+            mesh, brush.data_ptr(), n_brush, cap, counts.data_ptr(), faces.data_ptr(), 1, s), "bvhc_sphere_triangles")),
+        "intersects_sphere": (n_sphere, lambda: check(lib.bvhc_intersects_sphere(
+            mesh, sph.data_ptr(), n_sphere, flags.data_ptr(), 1, s), "bvhc_intersects_sphere")),
+        "intersects_box": (n_box, lambda: check(lib.bvhc_intersects_box(
+            mesh, box.data_ptr(), n_box, flags.data_ptr(), 1, s), "bvhc_intersects_box")),
+    }
+    ms = {}
+    with ClockSampler(local) as clk:
+        for name, (n, call) in calls.items():
+            for _ in range(args.warmup):
+                call()
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                call()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            ms[name] = max_over_ranks(a.elapsed_time(b) / args.steps, ws, dev)
+    bvh.synchronize(s)
+    cnt = counts.cpu().numpy()
+    # end to end: host spheres in, host counts and faces out (pinned), through the public call
+    pin_b = torch.from_numpy(brush_h).pin_memory()
+    pin_c = torch.empty(n_brush, dtype=torch.int32).pin_memory()
+    pin_f = torch.empty((n_brush, cap), dtype=torch.int32).pin_memory()
+    e2e = []
+    for _ in range(max(1, args.steps // 2)):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        check(lib.bvhc_sphere_triangles(mesh, pin_b.data_ptr(), n_brush, cap, pin_c.data_ptr(), pin_f.data_ptr(), 0,
+                                        None), "bvhc_sphere_triangles")
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(float(np.median(e2e)), ws, dev)
+    cpu = roof = None
+    sets = {k: {"queries": calls[k][0], "ms": v, "Mqueries_per_s": weak_scaling_rate(ws, calls[k][0], 1, v)}
+            for k, v in ms.items()}
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle.oracle as orc
+
+        ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, None, geo.position)
+        threads = os.cpu_count() or 1
+        peak, how = measured_peak()
+        samples = {}
+        # oracle over evenly strided samples of each set: CPU rate and the traversal counters
+        idx = np.linspace(0, n_brush - 1, 1 << 15).astype(np.int64)
+        t0 = time.perf_counter()
+        ec, _, nn, nt = ref.sphere_triangles(brush_h[idx], cap=cap, threads=threads, counters=True)
+        samples["sphere_triangles"] = (idx.size, time.perf_counter() - t0,
+                                       16 + 4 + 4 * cap + 32 * nn.mean() + 36 * nt.mean() + 4 * ec.mean(), nn, nt)
+        idx = np.linspace(0, n_sphere - 1, 1 << 17).astype(np.int64)
+        t0 = time.perf_counter()
+        _, nn, nt = ref.intersects_sphere(sph_h[idx], threads=threads, counters=True)
+        samples["intersects_sphere"] = (idx.size, time.perf_counter() - t0, 16 + 1 + 32 * nn.mean() + 36 * nt.mean(),
+                                        nn, nt)
+        idx = np.linspace(0, n_box - 1, 1 << 16).astype(np.int64)
+        t0 = time.perf_counter()
+        _, nn, nt = ref.intersects_box(box_h[idx], threads=threads, counters=True)
+        samples["intersects_box"] = (idx.size, time.perf_counter() - t0, 96 + 1 + 32 * nn.mean() + 36 * nt.mean(),
+                                     nn, nt)
+        for k, (m, dt, per, nn, nt) in samples.items():
+            sets[k].update({"cpu_Mqueries_per_s": m / dt / 1e6, "cpu_sample": m,
+                            "reference_node_reads_per_query": float(nn.mean()),
+                            "reference_triangle_tests_per_query": float(nt.mean()),
+                            "algorithmic_bytes_per_query": float(per),
+                            "roofline_frac": calls[k][0] * per / (ms[k] / 1e3) / 1e9 / peak})
+        m, dt, per, nn, nt = samples["sphere_triangles"]
+        cpu = {"value": m / dt / 1e6, "unit": "Mqueries/s", "cores": threads, "kind": "port",
+               "sample": f"{m} evenly strided brush spheres, float64 oracle"}
+        achieved = n_brush * per / (ms["sphere_triangles"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": how, "algorithmic_bytes_per_launch": n_brush * per,
+                "kernel": "sphere_triangles_kernel"}
+    if rank == 0:
+        line = {"metric": "Mqueries/s triangles within sculpt-brush spheres (2M tri)",
+                "value": weak_scaling_rate(ws, n_brush, 1, ms["sphere_triangles"]), "unit": "Mqueries/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms["sphere_triangles"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"TorusKnot(10,3,{args.tubular},{args.radial}) + N(0,0.02) noise, SAH leaf "
+                                       "10; 2^18 brush spheres on random triangle centroids, radius log-uniform "
+                                       "0.03..0.3, first 256 faces per sphere; plus 2^22 spheres in the AABB "
+                                       "(intersectsSphere) and 2^20 oriented boxes (intersectsBox)",
+                           "mean_triangles_per_brush": float(cnt.mean()), "sets": sets,
+                           "l2": "outputs (256 MB face rows) and sphere / box sets (64 / 96 MB) exceed or fill L2"},
+                "e2e": {"value": weak_scaling_rate(ws, n_brush, 1, e2e_ms), "unit": "Mqueries/s",
+                        "h2d_bytes_per_step": int(brush_h.nbytes), "d2h_bytes_per_step": int(n_brush * (1 + cap) * 4)},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+    bvh.dispose()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -984,6 +1132,8 @@ def main():
             run_build(args, ws, rank, local)
         elif args.workload == "scene":
             run_scene(args, ws, rank, local)
+        elif args.workload == "shapecast":
+            run_shapecast(args, ws, rank, local)
         else:
             run_engine(args, ws, rank, local)
     finally:

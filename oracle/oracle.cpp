@@ -974,24 +974,27 @@ int sphere_box_relation(const NodeView& nv, int64_t n32, V3 c, double r) {
   return 2;
 }
 
-void subtree_range(const NodeView& nv, int64_t n32, int64_t& first, int64_t& end) {  // getLeft/RightEndOffset
+void subtree_range(const NodeView& nv, int64_t n32, int64_t& first, int64_t& end, Counters& ctr) {
+  // getLeftEndOffset / getRightEndOffset: the outermost leaves of the subtree
   int64_t l = n32;
-  while (!nv.is_leaf(l)) l = nv.left(l);
+  while (!nv.is_leaf(l)) l = nv.left(l), ctr.nodes++;
   first = nv.offset(l);
   int64_t r = n32;
-  while (!nv.is_leaf(r)) r = nv.right(r);
+  while (!nv.is_leaf(r)) r = nv.right(r), ctr.nodes++;
   end = nv.offset(r) + nv.count(r);
 }
 
+// ctr.nodes counts the child boxes tested plus the records walked to a contained subtree's end
+// leaves; ctr.tris the triangles tested one by one.
 void sphere_collect(const Bvh& g, const NodeView& nv, int64_t n32, V3 c, double r, bool contained,
-                    std::vector<int64_t>& out) {
+                    std::vector<int64_t>& out, Counters& ctr) {
   if (contained || nv.is_leaf(n32)) {
     int64_t first, end;
     if (nv.is_leaf(n32)) {
       first = nv.offset(n32);
       end = first + nv.count(n32);
     } else {
-      subtree_range(nv, n32, first, end);
+      subtree_range(nv, n32, first, end, ctr);
     }
     for (int64_t i = first; i < end; ++i) {
       const int64_t tri = g.resolve(i);
@@ -1001,15 +1004,17 @@ void sphere_collect(const Bvh& g, const NodeView& nv, int64_t n32, V3 c, double 
       }
       int64_t abc[3];
       g.tri_vertices(tri, abc);
+      ctr.tris++;
       if (sphere_meets_triangle(c, r, g.vertex(abc[0]), g.vertex(abc[1]), g.vertex(abc[2]))) out.push_back(tri);
     }
     return;
   }
   const int64_t kids[2] = {nv.left(n32), nv.right(n32)};
   for (int64_t k : kids) {
+    ctr.nodes++;
     const int rel = sphere_box_relation(nv, k, c, r);
-    if (rel == 2) sphere_collect(g, nv, k, c, r, true, out);
-    else if (rel == 1) sphere_collect(g, nv, k, c, r, false, out);
+    if (rel == 2) sphere_collect(g, nv, k, c, r, true, out, ctr);
+    else if (rel == 1) sphere_collect(g, nv, k, c, r, false, out, ctr);
   }
 }
 
@@ -1405,17 +1410,20 @@ void orc_scene_raycast_all(const orc_bvh* const* geoms, int n_instances, const u
 // spheres: n x 4 float32.  counts[i] = triangles collected; faces[i * cap ..] the first cap of them
 // in traversal order (-1 past the count).
 void orc_sphere_triangles(const orc_bvh* h, const float* spheres, int64_t n, int cap, int32_t* counts, int64_t* faces,
-                          int threads) {
+                          int64_t* node_reads, int64_t* tri_tests, int threads) {
   parallel_for(n, threads, [&](int64_t s, int64_t e) {
     std::vector<int64_t> out;
     for (int64_t i = s; i < e; ++i) {
       out.clear();
+      Counters ctr;
       const V3 c{spheres[4 * i], spheres[4 * i + 1], spheres[4 * i + 2]};
       const double r = spheres[4 * i + 3];
       for (const auto& root : h->b.roots) {
         NodeView nv{root.data()};
-        sphere_collect(h->b, nv, 0, c, r, false, out);
+        sphere_collect(h->b, nv, 0, c, r, false, out, ctr);
       }
+      if (node_reads) node_reads[i] = ctr.nodes;
+      if (tri_tests) tri_tests[i] = ctr.tris;
       counts[i] = (int32_t)out.size();
       for (int k = 0; k < cap; ++k) faces[i * cap + k] = k < (int)out.size() ? out[k] : -1;
     }

@@ -68,7 +68,7 @@ def lib():
         L.orc_refit.argtypes = [P, P, I64, I]
         L.orc_intersects_sphere.argtypes = [P, P, I64, P, P, P, I]
         L.orc_intersects_box.argtypes = [P, P, I64, P, P, P, I]
-        L.orc_sphere_triangles.argtypes = [P, P, I64, I, P, P, I]
+        L.orc_sphere_triangles.argtypes = [P, P, I64, I, P, P, P, P, I]
         L.orc_scene_raycast_first.argtypes = [P, I, P, P, P, P, I64, I, D, D, P, P, I]
         L.orc_scene_raycast_all.argtypes = [P, I, P, P, P, P, I64, I, D, D, I, P, P, P, I]
         _lib = L
@@ -143,15 +143,19 @@ class OracleBVH:
         lib().orc_intersects_sphere(self.h, _p(sp), n, _p(out), _p(nn), _p(nt), threads or _threads())
         return (out.astype(bool), nn, nt) if counters else out.astype(bool)
 
-    def sphere_triangles(self, spheres, cap=256, threads=None):
+    def sphere_triangles(self, spheres, cap=256, threads=None, counters=False):
         """Triangles within each sphere (cx, cy, cz, r) through shapecast's CONTAINED path: counts
-        and the first `cap` triangle indices in traversal order (-1 past the count)."""
+        and the first `cap` triangle indices in traversal order (-1 past the count); with counters,
+        also the boxes read and the triangles tested one by one per sphere."""
         sp = np.ascontiguousarray(spheres, dtype=np.float32).reshape(-1, 4)
         n = sp.shape[0]
         counts = np.empty(n, dtype=np.int32)
         faces = np.empty((n, cap), dtype=np.int64)
-        lib().orc_sphere_triangles(self.h, _p(sp), n, cap, _p(counts), _p(faces), threads or _threads())
-        return counts, faces
+        nn = np.empty(n, dtype=np.int64) if counters else None
+        nt = np.empty(n, dtype=np.int64) if counters else None
+        lib().orc_sphere_triangles(self.h, _p(sp), n, cap, _p(counts), _p(faces), _p(nn), _p(nt),
+                                   threads or _threads())
+        return (counts, faces, nn, nt) if counters else (counts, faces)
 
     def intersects_box(self, boxes, threads=None, counters=False):
         """MeshBVH#intersectsBox for each row of 24 float32 (min xyz, pad, max xyz, pad, the

@@ -171,6 +171,48 @@ def test_intersects_box_lattice_ties(pkg, orc, cuda):
     bvh.dispose()
 
 
+def _near_plane_boxes(rng, geo, n):
+    """Rotated boxes resting on a triangle's plane: the box's bottom face is parallel to the
+    triangle, offset along its normal by +-1e-5 .. 0 of the mesh scale, box rotated about the normal
+    and slid so a vertex or an edge is near its rim.  Decisions there sit on the normal and
+    cross-product axes' margins."""
+    pos, tri = geo.position.astype(np.float64), geo.index.reshape(-1, 3)
+    scale = np.abs(pos).max()
+    out = np.zeros((n, 24), np.float32)
+    for i in range(n):
+        a, b, c = pos[tri[rng.integers(0, tri.shape[0])]]
+        nrm = np.cross(b - a, c - a)
+        nrm /= np.linalg.norm(nrm)
+        u = (b - a) / np.linalg.norm(b - a)
+        ang = rng.uniform(0, 2 * np.pi)
+        u = u * np.cos(ang) + np.cross(nrm, u) * np.sin(ang)
+        nrm = nrm * rng.choice([-1.0, 1.0])
+        w = np.cross(nrm, u)
+        h = rng.uniform(0.002, 0.05)
+        delta = rng.choice([-1e-5, -1e-6, -1e-7, 0.0, 1e-7, 1e-6, 1e-5]) * scale
+        anchor = (a, (a + b) / 2, (a + b + c) / 3)[rng.integers(0, 3)]
+        m = np.eye(4)
+        m[:3, 0], m[:3, 1], m[:3, 2] = u, w, nrm
+        m[:3, 3] = anchor + nrm * delta + (u * rng.uniform(-h, h) + w * rng.uniform(-h, h)) * rng.integers(0, 2)
+        out[i] = record(np.array([-h, -h, 0.0]), np.array([h, h, 2 * h]), m.T.reshape(-1))
+    return out
+
+
+def test_intersects_box_near_contact(pkg, orc, cuda):
+    """Rotated boxes within 1e-5 of the mesh scale of a triangle's plane: the float32 and
+    float-float tiers must hand every close call on; results identical to the oracle."""
+    geo = pkg.torus_knot(10, 3, 300, 60, noise_sigma=0.02, noise_seed=3)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, None, geo.position)
+    boxes = _near_plane_boxes(np.random.default_rng(37), geo, 20_000)
+    want = ref.intersects_box(boxes)
+    got = bvh.intersects_box_batch(boxes)
+    bad = np.nonzero(got != want)[0]
+    assert bad.size == 0, (bad[:10], boxes[bad[:2]])
+    assert 0.05 < want.mean() < 0.95
+    bvh.dispose()
+
+
 @pytest.mark.parametrize("indirect", [False, True])
 def test_sphere_triangles_match_oracle(pkg, orc, cuda, indirect):
     """Triangles within spheres through shapecast's CONTAINED path: the same faceIndex sequence as

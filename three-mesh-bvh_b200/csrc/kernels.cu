@@ -1381,6 +1381,146 @@ __device__ __noinline__ void make_ff(const float* q, ObbF& o) {
   }
 }
 
+// --- float32 tier ------------------------------------------------------------------------------
+// The same separating-axis tests in float32, from the float-float box rounded once (corners,
+// axes and bounds each within 1.01 u of their exact values, u = 2^-24, relative per component).
+// Every margin below is twice a bound on |float gap - exact gap| built from the L1 norm of the
+// tested axis and the largest coordinate m, so a gap beyond it has the sign the reference's
+// binary64 gap has (whose own error, ~2^-50 of the same scale, is far inside the factor 2).
+// Undecided tests go on to the float-float tier.
+struct ObbS {
+  float3 p[8], ax[3];
+  float smin[3], smax[3], amin[3], amax[3];
+  float n1[3];  // L1 norms of the axes
+  float mag;    // >= every |corner coordinate| (and finite: 0 when the box is too large)
+};
+
+__device__ __forceinline__ float3 ff3_hi(const ff3& v) { return make_float3(v.x.hi, v.y.hi, v.z.hi); }
+__device__ __forceinline__ float dotf(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ float l1f(float3 a) { return fabsf(a.x) + fabsf(a.y) + fabsf(a.z); }
+__device__ __forceinline__ float3 crossf(float3 a, float3 b) {
+  return make_float3(fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x)));
+}
+__device__ __forceinline__ float3 subf(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+
+__device__ __forceinline__ int sep_f(float amn, float amx, float bmn, float bmx, float margin) {
+  const float d1 = amn - bmx, d2 = bmn - amx;
+  if (d1 > margin || d2 > margin) return 1;
+  if (d1 < -margin && d2 < -margin) return 0;
+  return -1;
+}
+
+__device__ __forceinline__ void interval_f(float3 axis, const float3* pts, int n, float& mn, float& mx) {
+  mn = mx = dotf(axis, pts[0]);
+  for (int k = 1; k < n; ++k) {
+    const float v = dotf(axis, pts[k]);
+    mn = fminf(mn, v);
+    mx = fmaxf(mx, v);
+  }
+}
+
+__device__ __forceinline__ void make_s(const ObbF& o, ObbS& s) {
+  for (int k = 0; k < 8; ++k) s.p[k] = ff3_hi(o.p[k]);
+  for (int i = 0; i < 3; ++i) {
+    s.ax[i] = ff3_hi(o.ax[i]);
+    s.n1[i] = l1f(s.ax[i]);
+    s.smin[i] = o.smin[i].hi;
+    s.smax[i] = o.smax[i].hi;
+    s.amin[i] = o.amin[i].hi;
+    s.amax[i] = o.amax[i].hi;
+  }
+  s.mag = o.mag < 1e30f ? o.mag : 0.0f;
+}
+
+// OrientedBox.intersectsBox on a node box: 1 meets, 0 separated, -1 undecided.
+__device__ __forceinline__ int box_f(const ObbS& o, const float* b) {
+  float m = o.mag;
+  for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(b[k]));
+  if (!(o.mag > 0.0f) || !(m < 1e30f)) return -1;
+  // aligned bounds: |error| <= 2 u (|amin| + |bmax|) <= 4 u m
+  const float md = 0x1p-21f * m + 0x1p-120f;
+  bool undecided = false;
+  for (int d = 0; d < 3; ++d) {
+    const int r = sep_f(o.amin[d], o.amax[d], b[d], b[d + 3], md);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  // the node box's interval on a box axis is sum_d min / max(a_d lo_d, a_d hi_d) (the extremes
+  // over its 8 corners); |error| <= |a|_1 (5.1 u B + 2.02 u M) <= 8 u |a|_1 m
+  for (int i = 0; i < 3; ++i) {
+    const float3 a = o.ax[i];
+    const float x0 = a.x * b[0], x1 = a.x * b[3], y0 = a.y * b[1], y1 = a.y * b[4], z0 = a.z * b[2], z1 = a.z * b[5];
+    const float mn = fminf(x0, x1) + fminf(y0, y1) + fminf(z0, z1);
+    const float mx = fmaxf(x0, x1) + fmaxf(y0, y1) + fmaxf(z0, z1);
+    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-20f * o.n1[i] * m + 0x1p-120f);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  return undecided ? -1 : 1;
+}
+
+// OrientedBox.intersectsTriangle: 1 meets, 0 separated, -1 undecided.
+__device__ __forceinline__ int tri_f(const ObbS& o, float3 a, float3 b, float3 c) {
+  const float m = fmaxf(o.mag, fmaxf(absmax3(a), fmaxf(absmax3(b), absmax3(c))));
+  if (!(o.mag > 0.0f) || !(m < 1e30f)) return -1;
+  const float3 tp[3] = {a, b, c};
+  bool undecided = false;
+  // the box's axes against the triangle: |error| <= |a|_1 (5.01 u T + 2.01 u M)
+  for (int i = 0; i < 3; ++i) {
+    float mn, mx;
+    interval_f(o.ax[i], tp, 3, mn, mx);
+    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-20f * o.n1[i] * m + 0x1p-120f);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  // unit normal of cross(c - b, a - b) (Triangle.getNormal): with S the sums of the cross
+  // product's term magnitudes, its direction is within rho = 8.2 u |S|_1 / |raw| + 4 u
+  const float3 e1 = subf(c, b), e2 = subf(a, b);
+  const float3 raw = crossf(e1, e2);
+  const float s1 = fabsf(e1.y * e2.z) + fabsf(e1.z * e2.y) + fabsf(e1.z * e2.x) + fabsf(e1.x * e2.z) +
+                   fabsf(e1.x * e2.y) + fabsf(e1.y * e2.x);
+  const float l2 = dotf(raw, raw);
+  const float inv = l2 > 0.0f ? rsqrtf(l2) : 0.0f;
+  const float rho = 0x1p-20f * s1 * inv + 0x1p-21f;
+  const bool normal_ok = l2 > 0x1p-100f && rho < 0x1p-10f;
+  const float3 ta[4] = {make_float3(raw.x * inv, raw.y * inv, raw.z * inv), subf(a, b), subf(b, c), subf(c, a)};
+  const float t1[4] = {1.7321f, l1f(ta[1]), l1f(ta[2]), l1f(ta[3])};
+  // the normal: |error| <= 3.5 m (rho + 4 u); an edge: |error| <= 12 u |e|_1 m
+  for (int i = 0; i < 3; ++i) {
+    if (i == 0 && !normal_ok) {
+      undecided = true;
+      continue;
+    }
+    float tmn, tmx, bmn, bmx;
+    interval_f(ta[i], tp, 3, tmn, tmx);
+    interval_f(ta[i], o.p, 8, bmn, bmx);
+    const float margin = (i == 0 ? m * (8.0f * rho + 0x1p-19f) : 0x1p-19f * t1[i] * m) + 0x1p-120f;
+    const int r = sep_f(tmn, tmx, bmn, bmx, margin);
+    if (r == 1) return 0;
+    undecided |= r < 0;
+  }
+  // box axis x triangle axis: |error| <= 16.2 u |a|_1 |e|_1 m for an edge,
+  // m |a|_1 (3.5 rho + 28 u) for the normal
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 4; ++j) {
+      if (j == 0 && !normal_ok) {
+        undecided = true;
+        continue;
+      }
+      const float3 axis = crossf(o.ax[i], ta[j]);
+      float tmn, tmx, bmn, bmx;
+      interval_f(axis, tp, 3, tmn, tmx);
+      interval_f(axis, o.p, 8, bmn, bmx);
+      const float margin =
+          (j == 0 ? m * o.n1[i] * (8.0f * rho + 0x1p-18f) : 0x1p-19f * o.n1[i] * t1[j] * m) + 0x1p-120f;
+      const int r = sep_f(tmn, tmx, bmn, bmx, margin);
+      if (r == 1) return 0;
+      undecided |= r < 0;
+    }
+  }
+  return undecided ? -1 : 1;
+}
+
 // 1: the intervals are separated, 0: they overlap, -1: within the margin.
 __device__ __forceinline__ int sep(ff amn, ff amx, ff bmn, ff bmx, float margin) {
   const float d1 = ff_to_f(ff_sub(amn, bmx)), d2 = ff_to_f(ff_sub(bmn, amx));
@@ -1605,6 +1745,8 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
   }
   obb::ObbF o;
   obb::make_ff(q, o);
+  obb::ObbS os;
+  obb::make_s(o, os);
   obb::ObbD od;
   bool have_d = false;
   bool hit = false;
@@ -1617,7 +1759,8 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
         if (link != kEmptyLeaf) {
           for (uint32_t k = link & ~kLeafBit;; ++k) {
             const Tri t = load_tri(m.tris, k);
-            int r = o.exact ? -1 : obb::tri_ff(o, t.a, t.b, t.c);
+            int r = o.exact ? -1 : obb::tri_f(os, t.a, t.b, t.c);
+            if (r < 0 && !o.exact) r = obb::tri_ff(o, t.a, t.b, t.c);
             if (r < 0) {
               if (!have_d) {
                 obb::make_d(q, od);
@@ -1637,7 +1780,8 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
         const Pair pr = load_pair(m.nodes, link);
         bool w[2];
         for (int s = 0; s < 2; ++s) {
-          int r = o.exact ? -1 : obb::box_ff(o, s == 0 ? pr.l : pr.r);
+          int r = o.exact ? -1 : obb::box_f(os, s == 0 ? pr.l : pr.r);
+          if (r < 0 && !o.exact) r = obb::box_ff(o, s == 0 ? pr.l : pr.r);
           if (r < 0) {
             if (!have_d) {
               obb::make_d(q, od);
