@@ -1382,20 +1382,24 @@ __device__ __noinline__ void make_ff(const float* q, ObbF& o) {
 }
 
 // --- float32 tier ------------------------------------------------------------------------------
-// The same separating-axis tests in float32, from the float-float box rounded once (corners,
-// axes and bounds each within 1.01 u of their exact values, u = 2^-24, relative per component).
-// Every margin below is twice a bound on |float gap - exact gap| built from the L1 norm of the
-// tested axis and the largest coordinate m, so a gap beyond it has the sign the reference's
-// binary64 gap has (whose own error, ~2^-50 of the same scale, is far inside the factor 2).
-// Undecided tests go on to the float-float tier.
+// The same separating-axis tests in float32, built straight from the query (u = 2^-24):
+//   corners    fma chains, within 3.01 u M of the exact ones (M >= every |corner coordinate|,
+//              the sum of its terms' magnitudes),
+//   axes       p[0] - p[1 << i] = -(max_i - min_i) * column i of the matrix, within 2.01 u of
+//              each exact component,
+//   bounds     dot products / extremes of those.
+// Every margin below is about twice a bound on |float gap - exact gap| (the derivation is given
+// per test), plus an absolute term for the reference's own binary64 rounding of its corners
+// (~2^-51 M per coordinate, which a thin box's axes inherit).  A gap beyond the margin has the
+// sign the reference's binary64 gap has; undecided tests go on to the float-float tier.
 struct ObbS {
   float3 p[8], ax[3];
   float smin[3], smax[3], amin[3], amax[3];
   float n1[3];  // L1 norms of the axes
-  float mag;    // >= every |corner coordinate| (and finite: 0 when the box is too large)
+  float mag;    // >= every corner's sum of term magnitudes; 0 when the box is too large (undecided)
+  bool exact;   // non-affine matrix: every test goes to binary64
 };
 
-__device__ __forceinline__ float3 ff3_hi(const ff3& v) { return make_float3(v.x.hi, v.y.hi, v.z.hi); }
 __device__ __forceinline__ float dotf(float3 a, float3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
 __device__ __forceinline__ float l1f(float3 a) { return fabsf(a.x) + fabsf(a.y) + fabsf(a.z); }
 __device__ __forceinline__ float3 crossf(float3 a, float3 b) {
@@ -1419,17 +1423,37 @@ __device__ __forceinline__ void interval_f(float3 axis, const float3* pts, int n
   }
 }
 
-__device__ __forceinline__ void make_s(const ObbF& o, ObbS& s) {
-  for (int k = 0; k < 8; ++k) s.p[k] = ff3_hi(o.p[k]);
-  for (int i = 0; i < 3; ++i) {
-    s.ax[i] = ff3_hi(o.ax[i]);
-    s.n1[i] = l1f(s.ax[i]);
-    s.smin[i] = o.smin[i].hi;
-    s.smax[i] = o.smax[i].hi;
-    s.amin[i] = o.amin[i].hi;
-    s.amax[i] = o.amax[i].hi;
+__device__ __forceinline__ void make_s(const float* q, ObbS& s) {
+  const float* e = q + 8;
+  s.exact = !(e[3] == 0.0f && e[7] == 0.0f && e[11] == 0.0f && e[15] == 1.0f);
+  float mag = 0.0f;
+  for (int i = 0; i < 8; ++i) {
+    const float x = (i & 1) ? q[4] : q[0], y = (i & 2) ? q[5] : q[1], z = (i & 4) ? q[6] : q[2];
+    float c[3];
+    for (int k = 0; k < 3; ++k) {
+      c[k] = fmaf(e[k], x, fmaf(e[4 + k], y, fmaf(e[8 + k], z, e[12 + k])));
+      mag = fmaxf(mag, fabsf(e[k] * x) + fabsf(e[4 + k] * y) + fabsf(e[8 + k] * z) + fabsf(e[12 + k]));
+    }
+    s.p[i] = make_float3(c[0], c[1], c[2]);
   }
-  s.mag = o.mag < 1e30f ? o.mag : 0.0f;
+  mag *= 1.0f + 0x1p-20f;
+  for (int i = 0; i < 3; ++i) {
+    const float w = q[4 + i] - q[i];
+    s.ax[i] = make_float3(-e[4 * i] * w, -e[4 * i + 1] * w, -e[4 * i + 2] * w);
+    s.n1[i] = l1f(s.ax[i]);
+    interval_f(s.ax[i], s.p, 8, s.smin[i], s.smax[i]);
+  }
+  for (int d = 0; d < 3; ++d) {
+    float mn = d == 0 ? s.p[0].x : (d == 1 ? s.p[0].y : s.p[0].z), mx = mn;
+    for (int k = 1; k < 8; ++k) {
+      const float v = d == 0 ? s.p[k].x : (d == 1 ? s.p[k].y : s.p[k].z);
+      mn = fminf(mn, v);
+      mx = fmaxf(mx, v);
+    }
+    s.amin[d] = mn;
+    s.amax[d] = mx;
+  }
+  s.mag = mag < 1e30f ? mag : 0.0f;
 }
 
 // OrientedBox.intersectsBox on a node box: 1 meets, 0 separated, -1 undecided.
@@ -1437,8 +1461,8 @@ __device__ __forceinline__ int box_f(const ObbS& o, const float* b) {
   float m = o.mag;
   for (int k = 0; k < 6; ++k) m = fmaxf(m, fabsf(b[k]));
   if (!(o.mag > 0.0f) || !(m < 1e30f)) return -1;
-  // aligned bounds: |error| <= 2 u (|amin| + |bmax|) <= 4 u m
-  const float md = 0x1p-21f * m + 0x1p-120f;
+  // aligned bounds: |error| <= 3.01 u M + 2 u m
+  const float md = 0x1p-20f * m + 0x1p-120f;
   bool undecided = false;
   for (int d = 0; d < 3; ++d) {
     const int r = sep_f(o.amin[d], o.amax[d], b[d], b[d + 3], md);
@@ -1446,13 +1470,14 @@ __device__ __forceinline__ int box_f(const ObbS& o, const float* b) {
     undecided |= r < 0;
   }
   // the node box's interval on a box axis is sum_d min / max(a_d lo_d, a_d hi_d) (the extremes
-  // over its 8 corners); |error| <= |a|_1 (5.1 u B + 2.02 u M) <= 8 u |a|_1 m
+  // over its 8 corners); |error| <= |a|_1 (6.02 u B + 9.02 u M)
+  const float mr = 0x1p-36f * m * m + 0x1p-120f;
   for (int i = 0; i < 3; ++i) {
     const float3 a = o.ax[i];
     const float x0 = a.x * b[0], x1 = a.x * b[3], y0 = a.y * b[1], y1 = a.y * b[4], z0 = a.z * b[2], z1 = a.z * b[5];
     const float mn = fminf(x0, x1) + fminf(y0, y1) + fminf(z0, z1);
     const float mx = fmaxf(x0, x1) + fmaxf(y0, y1) + fmaxf(z0, z1);
-    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-20f * o.n1[i] * m + 0x1p-120f);
+    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-19f * o.n1[i] * m + mr);
     if (r == 1) return 0;
     undecided |= r < 0;
   }
@@ -1463,29 +1488,31 @@ __device__ __forceinline__ int box_f(const ObbS& o, const float* b) {
 __device__ __forceinline__ int tri_f(const ObbS& o, float3 a, float3 b, float3 c) {
   const float m = fmaxf(o.mag, fmaxf(absmax3(a), fmaxf(absmax3(b), absmax3(c))));
   if (!(o.mag > 0.0f) || !(m < 1e30f)) return -1;
+  const float mr = 0x1p-36f * m * m + 0x1p-120f;
   const float3 tp[3] = {a, b, c};
   bool undecided = false;
-  // the box's axes against the triangle: |error| <= |a|_1 (5.01 u T + 2.01 u M)
+  // the box's axes against the triangle: |error| <= |a|_1 (6.01 u T + 9.02 u M)
   for (int i = 0; i < 3; ++i) {
     float mn, mx;
     interval_f(o.ax[i], tp, 3, mn, mx);
-    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-20f * o.n1[i] * m + 0x1p-120f);
+    const int r = sep_f(o.smin[i], o.smax[i], mn, mx, 0x1p-19f * o.n1[i] * m + mr);
     if (r == 1) return 0;
     undecided |= r < 0;
   }
   // unit normal of cross(c - b, a - b) (Triangle.getNormal): with S the sums of the cross
-  // product's term magnitudes, its direction is within rho = 8.2 u |S|_1 / |raw| + 4 u
+  // product's term magnitudes, its direction is within 8.2 u |S|_1 / |raw| + 4.5 u;
+  // rho is twice that
   const float3 e1 = subf(c, b), e2 = subf(a, b);
   const float3 raw = crossf(e1, e2);
   const float s1 = fabsf(e1.y * e2.z) + fabsf(e1.z * e2.y) + fabsf(e1.z * e2.x) + fabsf(e1.x * e2.z) +
                    fabsf(e1.x * e2.y) + fabsf(e1.y * e2.x);
   const float l2 = dotf(raw, raw);
   const float inv = l2 > 0.0f ? rsqrtf(l2) : 0.0f;
-  const float rho = 0x1p-20f * s1 * inv + 0x1p-21f;
+  const float rho = 0x1p-20f * s1 * inv + 0x1p-20f;
   const bool normal_ok = l2 > 0x1p-100f && rho < 0x1p-10f;
   const float3 ta[4] = {make_float3(raw.x * inv, raw.y * inv, raw.z * inv), subf(a, b), subf(b, c), subf(c, a)};
   const float t1[4] = {1.7321f, l1f(ta[1]), l1f(ta[2]), l1f(ta[3])};
-  // the normal: |error| <= 3.5 m (rho + 4 u); an edge: |error| <= 12 u |e|_1 m
+  // the normal: |error| <= m (3.46 rho_dir + 39.8 u); an edge: |error| <= 13.01 u |e|_1 m
   for (int i = 0; i < 3; ++i) {
     if (i == 0 && !normal_ok) {
       undecided = true;
@@ -1494,13 +1521,13 @@ __device__ __forceinline__ int tri_f(const ObbS& o, float3 a, float3 b, float3 c
     float tmn, tmx, bmn, bmx;
     interval_f(ta[i], tp, 3, tmn, tmx);
     interval_f(ta[i], o.p, 8, bmn, bmx);
-    const float margin = (i == 0 ? m * (8.0f * rho + 0x1p-19f) : 0x1p-19f * t1[i] * m) + 0x1p-120f;
+    const float margin = (i == 0 ? m * (8.0f * rho + 0x1p-19f) : 0x1p-19f * t1[i] * m) + mr;
     const int r = sep_f(tmn, tmx, bmn, bmx, margin);
     if (r == 1) return 0;
     undecided |= r < 0;
   }
-  // box axis x triangle axis: |error| <= 16.2 u |a|_1 |e|_1 m for an edge,
-  // m |a|_1 (3.5 rho + 28 u) for the normal
+  // box axis x triangle axis: |error| <= 21 u |a|_1 |e|_1 m for an edge,
+  // m |a|_1 (3.46 rho_dir + 48.5 u) for the normal
   for (int i = 0; i < 3; ++i) {
     for (int j = 0; j < 4; ++j) {
       if (j == 0 && !normal_ok) {
@@ -1512,7 +1539,7 @@ __device__ __forceinline__ int tri_f(const ObbS& o, float3 a, float3 b, float3 c
       interval_f(axis, tp, 3, tmn, tmx);
       interval_f(axis, o.p, 8, bmn, bmx);
       const float margin =
-          (j == 0 ? m * o.n1[i] * (8.0f * rho + 0x1p-18f) : 0x1p-19f * o.n1[i] * t1[j] * m) + 0x1p-120f;
+          (j == 0 ? m * o.n1[i] * (8.0f * rho + 0x1p-18f) : 0x1p-18f * o.n1[i] * t1[j] * m) + mr * t1[j];
       const int r = sep_f(tmn, tmx, bmn, bmx, margin);
       if (r == 1) return 0;
       undecided |= r < 0;
@@ -1731,24 +1758,69 @@ __device__ __noinline__ bool tri_d(const ObbD& o, float3 fa, float3 fb, float3 f
 
 }  // namespace obb
 
+// One oriented box's predicates with the three tiers: float32, float-float (built on first
+// need), the reference's binary64 sequence (built on first need; always for non-affine boxes).
+struct BoxAny {
+  float q[24];
+  obb::ObbS s;
+  obb::ObbF f;
+  obb::ObbD d;
+  bool have_f, have_d;
+  __device__ void init(const float* __restrict__ boxes, uint64_t i) {
+    for (int k = 0; k < 6; ++k) {
+      const float4 v = ld4(boxes + 24 * i + 4 * k);
+      q[4 * k] = v.x;
+      q[4 * k + 1] = v.y;
+      q[4 * k + 2] = v.z;
+      q[4 * k + 3] = v.w;
+    }
+    obb::make_s(q, s);
+    have_f = have_d = false;
+  }
+  __device__ void need_f() {
+    if (!have_f) {
+      obb::make_ff(q, f);
+      have_f = true;
+    }
+  }
+  __device__ void need_d() {
+    if (!have_d) {
+      obb::make_d(q, d);
+      have_d = true;
+    }
+  }
+  __device__ bool box(const float* b) {
+    int r = s.exact ? -1 : obb::box_f(s, b);
+    if (r < 0 && !s.exact) {
+      need_f();
+      r = obb::box_ff(f, b);
+    }
+    if (r < 0) {
+      need_d();
+      r = obb::box_d(d, b) ? 1 : 0;
+    }
+    return r == 1;
+  }
+  __device__ bool tri(const Tri& t) {
+    int r = s.exact ? -1 : obb::tri_f(s, t.a, t.b, t.c);
+    if (r < 0 && !s.exact) {
+      need_f();
+      r = obb::tri_ff(f, t.a, t.b, t.c);
+    }
+    if (r < 0) {
+      need_d();
+      r = obb::tri_d(d, t.a, t.b, t.c) ? 1 : 0;
+    }
+    return r == 1;
+  }
+};
+
 __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const float* __restrict__ boxes,
                                                                 uint64_t n, uint8_t* __restrict__ out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float q[24];
-  for (int k = 0; k < 6; ++k) {
-    const float4 v = ld4(boxes + 24 * i + 4 * k);
-    q[4 * k] = v.x;
-    q[4 * k + 1] = v.y;
-    q[4 * k + 2] = v.z;
-    q[4 * k + 3] = v.w;
-  }
-  obb::ObbF o;
-  obb::make_ff(q, o);
-  obb::ObbS os;
-  obb::make_s(o, os);
-  obb::ObbD od;
-  bool have_d = false;
+  BoxAny q;
+  q.init(boxes, i);
   bool hit = false;
   uint32_t stack[kMaxStack];
   for (int root = 0; root < m.n_roots && !hit; ++root) {
@@ -1759,16 +1831,7 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
         if (link != kEmptyLeaf) {
           for (uint32_t k = link & ~kLeafBit;; ++k) {
             const Tri t = load_tri(m.tris, k);
-            int r = o.exact ? -1 : obb::tri_f(os, t.a, t.b, t.c);
-            if (r < 0 && !o.exact) r = obb::tri_ff(o, t.a, t.b, t.c);
-            if (r < 0) {
-              if (!have_d) {
-                obb::make_d(q, od);
-                have_d = true;
-              }
-              r = obb::tri_d(od, t.a, t.b, t.c) ? 1 : 0;
-            }
-            if (r == 1) {
+            if (q.tri(t)) {
               hit = true;
               break;
             }
@@ -1778,20 +1841,8 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
         }
       } else {
         const Pair pr = load_pair(m.nodes, link);
-        bool w[2];
-        for (int s = 0; s < 2; ++s) {
-          int r = o.exact ? -1 : obb::box_f(os, s == 0 ? pr.l : pr.r);
-          if (r < 0 && !o.exact) r = obb::box_ff(o, s == 0 ? pr.l : pr.r);
-          if (r < 0) {
-            if (!have_d) {
-              obb::make_d(q, od);
-              have_d = true;
-            }
-            r = obb::box_d(od, s == 0 ? pr.l : pr.r) ? 1 : 0;
-          }
-          w[s] = r == 1;
-        }
-        if (w[0] && w[1]) {
+        const bool w0 = q.box(pr.l), w1 = q.box(pr.r);
+        if (w0 && w1) {
           if (sp >= kMaxStack) {
             atomicOr(m.err, kErrStackOverflow);
             break;
@@ -1800,8 +1851,8 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
           link = pr.ll;
           continue;
         }
-        if (w[0] || w[1]) {
-          link = w[0] ? pr.ll : pr.lr;
+        if (w0 || w1) {
+          link = w0 ? pr.ll : pr.lr;
           continue;
         }
       }
