@@ -998,7 +998,7 @@ def shapecast_queries(geo, rng, n_brush, n_sphere, n_box):
 
 def run_shapecast(args, ws, rank, local):
     """Shapecast queries on the 2M-triangle knot: triangles within sculpt-brush spheres (shapecast's
-    CONTAINED path), intersectsSphere and intersectsBox (oriented boxes)."""
+    CONTAINED path), intersectsSphere, intersectsBox (oriented boxes), and getTriangleHitPointInfo."""
     import torch
 
     import __graft_entry__ as ge
@@ -1028,6 +1028,20 @@ def run_shapecast(args, ws, rank, local):
         "intersects_box": (n_box, lambda: check(lib.bvhc_intersects_box(
             mesh, box.data_ptr(), n_box, flags.data_ptr(), 1, s), "bvhc_intersects_box")),
     }
+    # getTriangleHitPointInfo on 2^20 (point, face) pairs: random faces, points at their centroids,
+    # a uv attribute
+    n_hpi = 1 << 20
+    rng_h = np.random.default_rng(11 + rank)
+    hpi_f = rng_h.integers(0, geo.triangle_count, n_hpi).astype(np.uint32)
+    tri = geo.index.reshape(-1, 3).astype(np.int64)[hpi_f]
+    hpi_p_h = geo.position[tri].astype(np.float64).mean(1).astype(np.float32)
+    uv_h = rng_h.random((geo.position.shape[0], 2)).astype(np.float32)
+    hpi_p, hpi_fd = torch.from_numpy(hpi_p_h).to(dev), torch.from_numpy(hpi_f.view(np.int32)).to(dev)
+    pos_d, uv_d = torch.from_numpy(geo.position).to(dev), torch.from_numpy(uv_h).to(dev)
+    hpi_out = torch.empty((n_hpi, 12), dtype=torch.int32, device=dev)   # 48-byte records
+    calls["hit_point_info"] = (n_hpi, lambda: check(lib.bvhc_triangle_hit_point_info(
+        mesh, hpi_p.data_ptr(), hpi_fd.data_ptr(), n_hpi, pos_d.data_ptr(), 3, uv_d.data_ptr(), 2,
+        geo.position.shape[0], None, 0, hpi_out.data_ptr(), 1, s), "bvhc_triangle_hit_point_info"))
     ms = {}
     with ClockSampler(local) as clk:
         for name, (n, call) in calls.items():
@@ -1081,6 +1095,13 @@ def run_shapecast(args, ws, rank, local):
         _, nn, nt = ref.intersects_box(box_h[idx], threads=threads, counters=True)
         samples["intersects_box"] = (idx.size, time.perf_counter() - t0, 96 + 1 + 32 * nn.mean() + 36 * nt.mean(),
                                      nn, nt)
+        m_h = 1 << 18
+        t0 = time.perf_counter()
+        orc.triangle_hit_point_info(hpi_p_h[:m_h], hpi_f[:m_h], geo.index, geo.position, uv_h)
+        sets["hit_point_info"].update({"algorithmic_bytes_per_query": 136.0, "roofline_frac":
+                                       n_hpi * 136.0 / (ms["hit_point_info"] / 1e3) / 1e9 / peak,
+                                       "cpu_Mqueries_per_s": m_h / (time.perf_counter() - t0) / 1e6,
+                                       "cpu_sample": m_h, "cpu_kind": "float64 numpy oracle, 1 thread"})
         for k, (m, dt, per, nn, nt) in samples.items():
             sets[k].update({"cpu_Mqueries_per_s": m / dt / 1e6, "cpu_sample": m,
                             "reference_node_reads_per_query": float(nn.mean()),
@@ -1103,7 +1124,8 @@ def run_shapecast(args, ws, rank, local):
                 "config": {"workload": f"TorusKnot(10,3,{args.tubular},{args.radial}) + N(0,0.02) noise, SAH leaf "
                                        "10; 2^18 brush spheres on random triangle centroids, radius log-uniform "
                                        "0.03..0.3, first 256 faces per sphere; plus 2^22 spheres in the AABB "
-                                       "(intersectsSphere) and 2^20 oriented boxes (intersectsBox)",
+                                       "(intersectsSphere), 2^20 oriented boxes (intersectsBox) and 2^20 "
+                                       "(centroid, face) pairs with a uv attribute (getTriangleHitPointInfo)",
                            "mean_triangles_per_brush": float(cnt.mean()), "sets": sets,
                            "l2": "outputs (256 MB face rows) and sphere / box sets (64 / 96 MB) exceed or fill L2"},
                 "e2e": {"value": weak_scaling_rate(ws, n_brush, 1, e2e_ms), "unit": "Mqueries/s",

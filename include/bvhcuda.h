@@ -75,6 +75,16 @@ typedef struct bvhc_closest {
   float point[3];
 } bvhc_closest;
 
+/* getTriangleHitPointInfo's result (src/utils/TriangleUtilities.js:65-147): face.a / b / c,
+ * face.materialIndex, face.normal, barycoord, uv ((0, 0) without a uv attribute). */
+typedef struct bvhc_hit_point_info {
+  uint32_t a, b, c;
+  uint32_t material_index;
+  float normal[3];
+  float barycoord[3];
+  float uv[2];
+} bvhc_hit_point_info;
+
 typedef struct bvhc_mesh_info {
   uint64_t node_records;     /* 64-byte child-pair records on the device */
   uint64_t triangle_records; /* 48-byte leaf-ordered triangle records on the device */
@@ -355,6 +365,22 @@ bvhc_status bvhc_closest_point_backward(bvhc_mesh* mesh, const float* points, co
 bvhc_status bvhc_hit_interpolate(bvhc_mesh* mesh, const bvhc_hit* hits, uint64_t n, const float* attribute,
                                  uint64_t n_verts, int item_size, int stride_floats, const float* rays, float* out,
                                  int mem, void* stream);
+
+/* getTriangleHitPointInfo(point, geometry, triangleIndex) (src/utils/TriangleUtilities.js:65-147)
+ * for n (point, faceIndex) pairs, e.g. closestPointToPoint's results: face a / b / c from the
+ * mesh's (reordered) index, materialIndex of the first of n_groups (start, count, materialIndex)
+ * triplets (index units, count < 0 = Infinity; host memory, at most 64) holding the triangle's first
+ * index (0 when none does), the face normal (Triangle.getNormal), barycoord (Triangle.getBarycoord)
+ * and uv (Triangle.getInterpolation; (0, 0) when `uv` is null), computed in integer-emulated
+ * binary64 so degenerate triangles give the reference's zeros.  points n x 3, faces n, positions
+ * and uv with n_verts >= the mesh's vertex count rows `pos_stride` / `uv_stride` floats apart.
+ * A faceIndex past the geometry's triangles: BVHC_ERR_INVALID_ARGUMENT for host memory; in
+ * device memory it gives a zero record with a, b, c = BVHC_NO_HIT and the device error word
+ * reports it. */
+bvhc_status bvhc_triangle_hit_point_info(bvhc_mesh* mesh, const float* points, const uint32_t* faces, uint64_t n,
+                                         const float* positions, int pos_stride, const float* uv, int uv_stride,
+                                         uint64_t n_verts, const int64_t* groups, int n_groups,
+                                         bvhc_hit_point_info* out, int mem, void* stream);
 
 /* MeshBVH#intersectsSphere(sphere) for every sphere (src/core/MeshBVH.js:796-809: shapecast with
  * the sphere/box and sphere/triangle tests, src/math/MathUtilities.js:167-201).  spheres: n x 4

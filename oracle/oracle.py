@@ -305,3 +305,54 @@ def scene_raycast_all(geoms, geometry, matrices, rays, visible=None, side=0, nea
     lib().orc_scene_raycast_all(gs, mats.shape[0], _p(geo), _p(mats), _p(vis), _p(r), r.shape[0], side, near, far,
                                 cap, _p(counts), _p(hits), _p(inst), threads or _threads())
     return counts, hits, inst
+
+
+def triangle_hit_point_info(points, faces, index, position, uv=None, groups=()):
+    """getTriangleHitPointInfo(point, geometry, triangleIndex) (src/utils/TriangleUtilities.js:65-147)
+    in float64 for each (point, faceIndex) pair: dict of a, b, c, materialIndex (first group whose
+    [start, start + count) holds 3 * triangle, else 0, :80-93), normal ((c - b) x (a - b) made unit,
+    zeros when its squared length is 0), barycoord (dot-product solve with v0 = c - a, v1 = b - a,
+    v2 = p - a; zeros when the Gram determinant is exactly 0), uv (barycentric weights on the uv
+    attribute; zeros for a degenerate triangle; None without uv).  Evaluation order is left to
+    right, as the reference's Vector3 arithmetic."""
+    p = np.asarray(points, dtype=np.float32).astype(np.float64).reshape(-1, 3)
+    f = np.asarray(faces, dtype=np.int64).reshape(-1)
+    idx = (np.asarray(index, dtype=np.int64).reshape(-1, 3) if index is not None
+           else np.arange(np.asarray(position).shape[0], dtype=np.int64).reshape(-1, 3))
+    pos = np.asarray(position, dtype=np.float32).astype(np.float64).reshape(-1, 3)
+    va, vb, vc = idx[f, 0], idx[f, 1], idx[f, 2]
+    A, B, C = pos[va], pos[vb], pos[vc]
+
+    def dot(x, y):
+        return x[:, 0] * y[:, 0] + x[:, 1] * y[:, 1] + x[:, 2] * y[:, 2]
+
+    def cross(x, y):
+        return np.stack([x[:, 1] * y[:, 2] - x[:, 2] * y[:, 1], x[:, 2] * y[:, 0] - x[:, 0] * y[:, 2],
+                         x[:, 0] * y[:, 1] - x[:, 1] * y[:, 0]], 1)
+
+    v0, v1, v2 = C - A, B - A, p - A
+    d00, d01, d02, d11, d12 = dot(v0, v0), dot(v0, v1), dot(v0, v2), dot(v1, v1), dot(v1, v2)
+    denom = d00 * d11 - d01 * d01
+    ok = denom != 0
+    inv = np.where(ok, 1.0 / np.where(ok, denom, 1.0), 0.0)
+    u = (d11 * d02 - d01 * d12) * inv
+    v = (d00 * d12 - d01 * d02) * inv
+    bary = np.where(ok[:, None], np.stack([1.0 - u - v, v, u], 1), 0.0)
+    n = cross(C - B, A - B)
+    l2 = dot(n, n)
+    pos_l = l2 > 0
+    normal = np.where(pos_l[:, None], n * (1.0 / np.sqrt(np.where(pos_l, l2, 1.0)))[:, None], 0.0)
+    mat = np.zeros(f.shape[0], dtype=np.int64)
+    found = np.zeros(f.shape[0], dtype=bool)
+    first = 3 * f
+    for start, count, material in groups:
+        end = math.inf if count is None or count < 0 or math.isinf(count) else start + count
+        hit = ~found & (first >= start) & (first < end)
+        mat[hit] = material
+        found |= hit
+    out = {"a": va, "b": vb, "c": vc, "materialIndex": mat, "normal": normal, "barycoord": bary, "uv": None}
+    if uv is not None:
+        t = np.asarray(uv, dtype=np.float32).astype(np.float64).reshape(-1, 2)
+        w = bary
+        out["uv"] = np.where(ok[:, None], t[va] * w[:, 0:1] + t[vb] * w[:, 1:2] + t[vc] * w[:, 2:3], 0.0)
+    return out

@@ -25,6 +25,11 @@ class BvhcClosest(C.Structure):
     _fields_ = [("face_index", C.c_uint32), ("distance", C.c_float), ("point", C.c_float * 3)]
 
 
+class BvhcHitPointInfo(C.Structure):
+    _fields_ = [("a", C.c_uint32), ("b", C.c_uint32), ("c", C.c_uint32), ("material_index", C.c_uint32),
+                ("normal", C.c_float * 3), ("barycoord", C.c_float * 3), ("uv", C.c_float * 2)]
+
+
 class BvhcTraversalConfig(C.Structure):
     _fields_ = [("persistent", C.c_int32), ("order", C.c_int32), ("refill", C.c_int32), ("occupancy", C.c_int32),
                 ("compact", C.c_int32), ("sort", C.c_int32), ("closest", C.c_int32),
@@ -84,6 +89,7 @@ SIGNATURES = [
     ("bvhc_scene_set_order", _I, [_P, _I]),
     ("bvhc_scene_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _P, _I, _P]),
     ("bvhc_hit_interpolate", _I, [_P, _P, _U64, _P, _U64, _I, _I, _P, _P, _I, _P]),
+    ("bvhc_triangle_hit_point_info", _I, [_P, _P, _P, _U64, _P, _I, _P, _I, _U64, _P, _I, _P, _I, _P]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
 ]

@@ -1419,6 +1419,56 @@ bvhc_status bvhc_hit_interpolate(bvhc_mesh* m, const bvhc_hit* hits, uint64_t n,
   return read_and_clear_error(m, s);
 }
 
+bvhc_status bvhc_triangle_hit_point_info(bvhc_mesh* m, const float* points, const uint32_t* faces, uint64_t n,
+                                         const float* positions, int pos_stride, const float* uv, int uv_stride,
+                                         uint64_t n_verts, const int64_t* groups, int n_groups,
+                                         bvhc_hit_point_info* out, int mem, void* stream) {
+  if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE) || pos_stride < 3 || (uv && uv_stride < 2) ||
+      n_verts < m->n_verts_geo || n_groups < 0 || (n_groups > 0 && !groups))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  if (n_groups > kMaxMaterials) return BVHC_ERR_UNSUPPORTED;
+  if (n == 0) return BVHC_OK;
+  if (!points || !faces || !positions || !out) return BVHC_ERR_INVALID_ARGUMENT;
+  GroupTable gt{};
+  gt.n = n_groups;
+  for (int g = 0; g < n_groups; ++g) {
+    gt.start[g] = groups[3 * g];
+    gt.count[g] = groups[3 * g + 1];
+    gt.material[g] = (int32_t)groups[3 * g + 2];
+  }
+  const uint64_t n_tri = m->h_index.empty() ? m->n_verts_geo / 3 : m->h_index.size() / 3;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BVHC_CUDA_TRY(cudaSetDevice(m->device));
+  BVHC_CUDA_TRY(ensure_tri_vid(m));
+  if (mem == BVHC_MEM_DEVICE) {
+    if (!aligned(points, 4) || !aligned(faces, 4) || !aligned(positions, 4) || (uv && !aligned(uv, 4)) ||
+        !aligned(out, 4))
+      return BVHC_ERR_INVALID_ARGUMENT;
+    return from_cuda(launch_triangle_hit_point_info(points, faces, n, m->d_tri_vid, n_tri, positions, pos_stride, uv,
+                                                    uv_stride, gt, out, m->d_err, s));
+  }
+  for (uint64_t i = 0; i < n; ++i)
+    if (faces[i] >= n_tri) return BVHC_ERR_INVALID_ARGUMENT;
+  // host memory: points, faces, positions and uv through one staging buffer (16-byte aligned parts)
+  auto up16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+  const size_t pb = up16(n * 12), fb = up16(n * 4), vb = up16(n_verts * (size_t)pos_stride * 4),
+               ub = uv ? n_verts * (size_t)uv_stride * 4 : 0, ob = n * sizeof(bvhc_hit_point_info);
+  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, pb + fb + vb + ub));
+  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, ob));
+  char* base = static_cast<char*>(m->d_in);
+  BVHC_CUDA_TRY(cudaMemcpyAsync(base, points, n * 12, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(base + pb, faces, n * 4, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(base + pb + fb, positions, n_verts * (size_t)pos_stride * 4, cudaMemcpyHostToDevice, s));
+  if (uv) BVHC_CUDA_TRY(cudaMemcpyAsync(base + pb + fb + vb, uv, ub, cudaMemcpyHostToDevice, s));
+  BVHC_CUDA_TRY(launch_triangle_hit_point_info(
+      reinterpret_cast<const float*>(base), reinterpret_cast<const uint32_t*>(base + pb), n, m->d_tri_vid, n_tri,
+      reinterpret_cast<const float*>(base + pb + fb), pos_stride,
+      uv ? reinterpret_cast<const float*>(base + pb + fb + vb) : nullptr, uv_stride, gt,
+      static_cast<bvhc_hit_point_info*>(m->d_out), m->d_err, s));
+  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, ob, cudaMemcpyDeviceToHost, s));
+  return read_and_clear_error(m, s);
+}
+
 bvhc_status bvhc_intersects_sphere(bvhc_mesh* m, const float* spheres, uint64_t n, uint8_t* out, int mem,
                                    void* stream) {
   if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;

@@ -2874,6 +2874,111 @@ namespace dev {
 // Intersection attribute fields (ThreeRayIntersectUtilities.js:59-117): a vertex attribute at the
 // hit point, Triangle.getInterpolation with the recorded barycentrics; with rays given (normals),
 // the result is negated when it points along the ray.  Misses give zeros.
+// ---------------------------------------------------------------------------------------------
+// getTriangleHitPointInfo (src/utils/TriangleUtilities.js:65-147) for a batch of (point,
+// triangle) pairs, in the integer-emulated binary64 of softf64.cuh so that the degenerate cases
+// fall exactly as the reference's float64 arithmetic has them:
+//   barycoord  the dot-product solve with v0 = c - a, v1 = b - a, v2 = p - a:
+//              denom = (v0.v0)(v1.v1) - (v0.v1)^2, u = ((v1.v1)(v0.v2) - (v0.v1)(v1.v2)) / denom,
+//              v = ((v0.v0)(v1.v2) - (v0.v1)(v0.v2)) / denom, barycoord = (1 - u - v, v, u);
+//              (0, 0, 0) when denom is exactly 0 (Triangle.getBarycoord),
+//   uv         the uvs weighted by that barycoord, (0, 0) for a degenerate triangle
+//              (Triangle.getInterpolation),
+//   normal     (c - b) x (a - b) scaled by 1 / |.|, (0, 0, 0) when its squared length is 0
+//              (Triangle.getNormal),
+//   face       the index's three vertex ids and the material of the first group that holds the
+//              triangle's first index (0 when none does).
+// ---------------------------------------------------------------------------------------------
+namespace hpi {
+using sf::f64;
+struct V {
+  f64 x, y, z;
+};
+__device__ __forceinline__ V load(const float* p) {
+  return {sf::from_f32(__ldg(p)), sf::from_f32(__ldg(p + 1)), sf::from_f32(__ldg(p + 2))};
+}
+__device__ __forceinline__ V sub(V a, V b) { return {sf::sub(a.x, b.x), sf::sub(a.y, b.y), sf::sub(a.z, b.z)}; }
+__device__ __forceinline__ f64 dot(V a, V b) {
+  return sf::add(sf::add(sf::mul(a.x, b.x), sf::mul(a.y, b.y)), sf::mul(a.z, b.z));
+}
+__device__ __forceinline__ V cross(V a, V b) {
+  return {sf::sub(sf::mul(a.y, b.z), sf::mul(a.z, b.y)), sf::sub(sf::mul(a.z, b.x), sf::mul(a.x, b.z)),
+          sf::sub(sf::mul(a.x, b.y), sf::mul(a.y, b.x))};
+}
+}  // namespace hpi
+
+__global__ void __launch_bounds__(kBlock) triangle_hit_point_info_kernel(
+    const float* __restrict__ points, const uint32_t* __restrict__ faces, uint64_t n,
+    const uint32_t* __restrict__ tri_vid, uint64_t n_tri, const float* __restrict__ pos, int pos_stride,
+    const float* __restrict__ uv, int uv_stride, const GroupTable groups, bvhc_hit_point_info* __restrict__ out,
+    unsigned int* err) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bvhc_hit_point_info r;
+  r.a = r.b = r.c = BVHC_NO_HIT;
+  r.material_index = 0;
+  for (int k = 0; k < 3; ++k) r.normal[k] = r.barycoord[k] = 0.0f;
+  r.uv[0] = r.uv[1] = 0.0f;
+  const uint32_t f = __ldg(faces + i);
+  if (f >= n_tri) {
+    atomicOr(err, kErrBadFace);
+    out[i] = r;
+    return;
+  }
+  const uint32_t va = __ldg(tri_vid + 3 * (uint64_t)f), vb = __ldg(tri_vid + 3 * (uint64_t)f + 1),
+                 vc = __ldg(tri_vid + 3 * (uint64_t)f + 2);
+  r.a = va;
+  r.b = vb;
+  r.c = vc;
+  const int64_t first = 3 * (int64_t)f;
+  for (int g = 0; g < groups.n; ++g) {
+    if (first >= groups.start[g] && (groups.count[g] < 0 || first < groups.start[g] + groups.count[g])) {
+      r.material_index = (uint32_t)groups.material[g];
+      break;
+    }
+  }
+  const hpi::V A = hpi::load(pos + (uint64_t)va * pos_stride), B = hpi::load(pos + (uint64_t)vb * pos_stride),
+               C = hpi::load(pos + (uint64_t)vc * pos_stride), P = hpi::load(points + 3 * i);
+  // barycoord
+  const hpi::V v0 = hpi::sub(C, A), v1 = hpi::sub(B, A), v2 = hpi::sub(P, A);
+  const sf::f64 d00 = hpi::dot(v0, v0), d01 = hpi::dot(v0, v1), d02 = hpi::dot(v0, v2), d11 = hpi::dot(v1, v1),
+                d12 = hpi::dot(v1, v2);
+  const sf::f64 denom = sf::sub(sf::mul(d00, d11), sf::mul(d01, d01));
+  const bool degenerate = sf::is_zero(denom);
+  sf::f64 w[3] = {0, 0, 0};
+  if (!degenerate) {
+    const sf::f64 inv = sf::div(sf::kOne, denom);
+    const sf::f64 u = sf::mul(sf::sub(sf::mul(d11, d02), sf::mul(d01, d12)), inv);
+    const sf::f64 v = sf::mul(sf::sub(sf::mul(d00, d12), sf::mul(d01, d02)), inv);
+    w[0] = sf::sub(sf::sub(sf::kOne, u), v);
+    w[1] = v;
+    w[2] = u;
+    for (int k = 0; k < 3; ++k) r.barycoord[k] = sf::to_f32(w[k]);
+  }
+  // uv
+  if (uv && !degenerate) {
+    const float* ua = uv + (uint64_t)va * uv_stride;
+    const float* ub = uv + (uint64_t)vb * uv_stride;
+    const float* uc = uv + (uint64_t)vc * uv_stride;
+    for (int k = 0; k < 2; ++k) {
+      sf::f64 acc = sf::mul(sf::from_f32(__ldg(ua + k)), w[0]);
+      acc = sf::add(acc, sf::mul(sf::from_f32(__ldg(ub + k)), w[1]));
+      acc = sf::add(acc, sf::mul(sf::from_f32(__ldg(uc + k)), w[2]));
+      r.uv[k] = sf::to_f32(acc);
+    }
+  }
+  // normal
+  const hpi::V nr = hpi::cross(hpi::sub(C, B), hpi::sub(A, B));
+  const sf::f64 l2 = hpi::dot(nr, nr);
+  if (sf::lt(0, l2)) {
+    const sf::f64 s = sf::div(sf::kOne, sf::sqrt(l2));
+    r.normal[0] = sf::to_f32(sf::mul(nr.x, s));
+    r.normal[1] = sf::to_f32(sf::mul(nr.y, s));
+    r.normal[2] = sf::to_f32(sf::mul(nr.z, s));
+  }
+  out[i] = r;
+}
+
 __global__ void __launch_bounds__(kBlock) hit_interpolate_kernel(const bvhc_hit* __restrict__ hits, uint64_t n,
                                                                  const uint32_t* __restrict__ tri_vid,
                                                                  const float* __restrict__ attr, int item_size,
@@ -2955,6 +3060,16 @@ cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint
                                     uint32_t* faces, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   dev::sphere_triangles_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, cap, counts, faces);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_triangle_hit_point_info(const float* points, const uint32_t* faces, uint64_t n,
+                                           const uint32_t* tri_vid, uint64_t n_tri, const float* pos, int pos_stride,
+                                           const float* uv, int uv_stride, const GroupTable& groups,
+                                           bvhc_hit_point_info* out, unsigned int* err, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  dev::triangle_hit_point_info_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(
+      points, faces, n, tri_vid, n_tri, pos, pos_stride, uv, uv_stride, groups, out, err);
   return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@ namespace bvhc {
 // Device error word bits (set with atomicOr; read and cleared by bvhc_mesh_synchronize).
 enum : unsigned int {
   kErrStackOverflow = 1u,  // a traversal needed more than kMaxStack entries
+  kErrBadFace = 2u,        // a faceIndex argument past the geometry's triangles
 };
 
 struct MeshDev {
@@ -154,6 +155,20 @@ cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene,
 // counts[i] the total, faces[i * cap ..] the first cap faceIndex values in traversal order.
 cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
                                     uint32_t* faces, cudaStream_t stream);
+
+// getTriangleHitPointInfo's material lookup: the first of n groups whose [start, start + count)
+// (index units, count < 0 = Infinity) holds the triangle's first index gives its materialIndex.
+struct GroupTable {
+  int64_t start[kMaxMaterials], count[kMaxMaterials];
+  int32_t material[kMaxMaterials];
+  int32_t n;
+};
+// getTriangleHitPointInfo for n (point, faceIndex) pairs over the geometry index tri_vid (n_tri
+// triangles), positions and optional uv (stride in floats); out-of-range faces set kErrBadFace.
+cudaError_t launch_triangle_hit_point_info(const float* points, const uint32_t* faces, uint64_t n,
+                                           const uint32_t* tri_vid, uint64_t n_tri, const float* pos, int pos_stride,
+                                           const float* uv, int uv_stride, const GroupTable& groups,
+                                           bvhc_hit_point_info* out, unsigned int* err, cudaStream_t stream);
 
 // intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
 // 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.

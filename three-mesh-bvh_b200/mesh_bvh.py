@@ -75,6 +75,11 @@ def _material_sides(materials) -> np.ndarray | None:
     return None
 
 
+# bvhc_hit_point_info as a numpy record
+_HPI_DTYPE = np.dtype([("a", np.uint32), ("b", np.uint32), ("c", np.uint32), ("material_index", np.uint32),
+                       ("normal", np.float32, 3), ("barycoord", np.float32, 3), ("uv", np.float32, 2)])
+
+
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
 
@@ -559,6 +564,41 @@ class MeshBVH:
         mn, mx = (box.min, box.max) if hasattr(box, "min") else box
         el = getattr(box_to_mesh, "elements", box_to_mesh)
         return bool(self.intersects_box_batch(self.box_records(mn, mx, el))[0])
+
+    def triangle_hit_point_info_batch(self, points, faces) -> dict:
+        """getTriangleHitPointInfo (src/utils/TriangleUtilities.js:65-147) for every (point,
+        faceIndex) pair over this BVH's geometry (its index, positions, uv and groups), e.g. on
+        closestPointToPoint results: numpy -> dict of arrays a, b, c, materialIndex (n,), normal and
+        barycoord (n, 3), uv (n, 2) or None without a uv attribute."""
+        lib, mesh, g = N.lib(), self._device_mesh(), self.geometry
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        fc = np.ascontiguousarray(faces, dtype=np.uint32).reshape(-1)
+        if fc.shape[0] != pts.shape[0]:
+            raise ValueError("points and faces differ in length")
+        grp = np.array([[s0, -1 if math.isinf(c0) else c0, mi] for s0, c0, mi in g.groups],
+                       dtype=np.int64).reshape(-1)
+        uv = g.uv
+        out = np.empty(pts.shape[0], dtype=_HPI_DTYPE)
+        N.check(lib.bvhc_triangle_hit_point_info(mesh, _ptr(pts), _ptr(fc), pts.shape[0], _ptr(g.position), 3,
+                                                 _ptr(uv) if uv is not None else None, 2, g.position.shape[0],
+                                                 _ptr(grp) if grp.size else None, len(g.groups), _ptr(out),
+                                                 N.MEM_HOST, None), "bvhc_triangle_hit_point_info")
+        return {"a": out["a"], "b": out["b"], "c": out["c"], "materialIndex": out["material_index"],
+                "normal": out["normal"], "barycoord": out["barycoord"],
+                "uv": out["uv"] if uv is not None else None}
+
+    def getTriangleHitPointInfo(self, point, triangleIndex: int, target: dict | None = None) -> dict:
+        """getTriangleHitPointInfo(point, geometry, triangleIndex, target) on this BVH's geometry:
+        {"face": {"a", "b", "c", "materialIndex", "normal"}, "uv", "barycoord"}; an existing
+        `target` dict is filled in and returned."""
+        r = self.triangle_hit_point_info_batch(np.asarray(point, dtype=np.float32).reshape(1, 3), [triangleIndex])
+        face = {"a": int(r["a"][0]), "b": int(r["b"][0]), "c": int(r["c"][0]),
+                "materialIndex": int(r["materialIndex"][0]), "normal": r["normal"][0].copy()}
+        info = target if target is not None else {}
+        info["face"] = face
+        info["uv"] = r["uv"][0].copy() if r["uv"] is not None else None
+        info["barycoord"] = r["barycoord"][0].copy()
+        return info
 
     def intersectsSphere(self, sphere) -> bool:
         """MeshBVH#intersectsSphere (MeshBVH.js:796-809); sphere: (center, radius) or an object
