@@ -1815,6 +1815,9 @@ struct BoxAny {
   }
 };
 
+// One box per thread in the "while-while" form: every lane walks child pairs until it holds a
+// non-empty leaf (or its traversal ends), then the lanes holding leaves test their triangles
+// together, so the costly triangle tests of a few lanes are not paid at every node step.
 __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const float* __restrict__ boxes,
                                                                 uint64_t n, uint8_t* __restrict__ out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1826,37 +1829,48 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
   for (int root = 0; root < m.n_roots && !hit; ++root) {
     uint32_t link = m.roots[root];
     int sp = 0;
-    for (;;) {
-      if (link & kLeafBit) {
-        if (link != kEmptyLeaf) {
-          for (uint32_t k = link & ~kLeafBit;; ++k) {
-            const Tri t = load_tri(m.tris, k);
-            if (q.tri(t)) {
-              hit = true;
-              break;
-            }
-            if (t.flags & kTriLast) break;
+    bool live = true;  // this root's traversal has work left
+    while (live) {
+      // node phase: down to a non-empty leaf, or to the end of the traversal
+      while (!(link & kLeafBit) || link == kEmptyLeaf) {
+        if (link & kLeafBit) {  // empty leaf: next entry
+          if (sp == 0) {
+            live = false;
+            break;
           }
-          if (hit) break;
+          link = stack[--sp];
+          continue;
         }
-      } else {
         const Pair pr = load_pair(m.nodes, link);
         const bool w0 = q.box(pr.l), w1 = q.box(pr.r);
         if (w0 && w1) {
           if (sp >= kMaxStack) {
             atomicOr(m.err, kErrStackOverflow);
+            live = false;
             break;
           }
           stack[sp++] = pr.lr;
           link = pr.ll;
-          continue;
-        }
-        if (w0 || w1) {
+        } else if (w0 || w1) {
           link = w0 ? pr.ll : pr.lr;
-          continue;
+        } else if (sp > 0) {
+          link = stack[--sp];
+        } else {
+          live = false;
+          break;
         }
       }
-      if (sp == 0) break;
+      if (!live) break;
+      // leaf phase
+      for (uint32_t k = link & ~kLeafBit;; ++k) {
+        const Tri t = load_tri(m.tris, k);
+        if (q.tri(t)) {
+          hit = true;
+          break;
+        }
+        if (t.flags & kTriLast) break;
+      }
+      if (hit || sp == 0) break;
       link = stack[--sp];
     }
   }
@@ -3073,7 +3087,8 @@ cudaError_t launch_triangle_hit_point_info(const float* points, const uint32_t* 
   return cudaGetLastError();
 }
 
-cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out, cudaStream_t stream) {
+cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
+                                  cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   dev::intersects_box_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, boxes, n, out);
   return cudaGetLastError();
