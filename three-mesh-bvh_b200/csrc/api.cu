@@ -40,14 +40,17 @@ struct bvhc_mesh {
   size_t out_cap = 0;
   void* d_out2 = nullptr;
   size_t out2_cap = 0;
-  // pipelined host-memory raycastFirst: two streams, staging slots and work counters
-  cudaStream_t pipe[2] = {nullptr, nullptr};
-  void* slot_in[2] = {nullptr, nullptr};
-  void* slot_out[2] = {nullptr, nullptr};
-  unsigned long long* d_work2 = nullptr;
-  // work queues (grow-only): [0] direct raycastFirst calls, [1], [2] the two pipeline slots (so
-  // that concurrently running chunks never share a queue), [3] closestPointToPoint, [4] raycast
-  static constexpr int kSlots = 5;
+  // pipelined host-memory raycastFirst: kPipes streams, staging slots and work counters (slot 0
+  // uses d_work)
+  static constexpr int kPipes = 3;
+  cudaStream_t pipe[kPipes] = {};
+  void* slot_in[kPipes] = {};
+  void* slot_out[kPipes] = {};
+  unsigned long long* d_work_pipe[kPipes] = {};
+  // work queues (grow-only): [0] direct raycastFirst calls, [1], [2], [5] the three pipeline slots
+  // (so that concurrently running chunks never share a queue), [3] closestPointToPoint, [4] raycast
+  // (all hits)
+  static constexpr int kSlots = 6;
   uint32_t* d_queue[kSlots] = {};
   size_t queue_cap[kSlots] = {};
   unsigned int* d_qcount[kSlots] = {};
@@ -910,12 +913,12 @@ void bvhc_mesh_destroy(bvhc_mesh* m) {
   cudaFree(m->d_in);
   cudaFree(m->d_out);
   cudaFree(m->d_out2);
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) {
     cudaFree(m->slot_in[k]);
     cudaFree(m->slot_out[k]);
     if (m->pipe[k]) cudaStreamDestroy(m->pipe[k]);
+    if (k > 0) cudaFree(m->d_work_pipe[k]);
   }
-  cudaFree(m->d_work2);
   cudaFree(m->d_mesh_root_off);
   cudaFree(m->d_ray_off);
   cudaFree(m->d_index32);
@@ -1034,7 +1037,7 @@ static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* ra
 
 // Streams, staging slots and the second work counter of the pipelined host-memory path.
 static cudaError_t ensure_pipeline(bvhc_mesh* m) {
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) {
     if (!m->pipe[k]) {
       cudaError_t e = cudaStreamCreateWithFlags(&m->pipe[k], cudaStreamNonBlocking);
       if (e != cudaSuccess) return e;
@@ -1048,8 +1051,13 @@ static cudaError_t ensure_pipeline(bvhc_mesh* m) {
       cudaError_t e = ensure(&m->slot_out[k], &cap_out, kPipeChunk * sizeof(bvhc_hit));
       if (e != cudaSuccess) return e;
     }
+    if (k == 0) {
+      m->d_work_pipe[0] = m->d_work;
+    } else if (!m->d_work_pipe[k]) {
+      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&m->d_work_pipe[k]), sizeof(unsigned long long));
+      if (e != cudaSuccess) return e;
+    }
   }
-  if (!m->d_work2) return cudaMalloc(reinterpret_cast<void**>(&m->d_work2), sizeof(unsigned long long));
   return cudaSuccess;
 }
 
@@ -1225,27 +1233,28 @@ static bvhc_status raycast_first_impl(bvhc_mesh* m, const float* rays, uint64_t 
     BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
     return read_and_clear_error(m, s);
   }
-  // Large host batches: chunks alternate between two streams, each with its own staging slot and
-  // work counter, so the host->device copy of one chunk, the traversal of another and the
-  // device->host copy of a third overlap (copies overlap only for page-locked host memory).
+  // Large host batches: chunks rotate over three streams, each with its own staging slot and work
+  // counter, so the host->device copy of one chunk, the traversal of another and the device->host
+  // copy of a third overlap (copies overlap only for page-locked host memory); with a third slot a
+  // chunk's upload no longer waits for the download of the chunk two before it, and the
+  // device->host link, the busiest, stays fed.
   BVHC_CUDA_TRY(ensure_pipeline(m));
   cudaEvent_t ready;
   BVHC_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
   cudaEventRecord(ready, s);
-  for (int k = 0; k < 2; ++k) cudaStreamWaitEvent(m->pipe[k], ready, 0);
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) cudaStreamWaitEvent(m->pipe[k], ready, 0);
   cudaEventDestroy(ready);
-  unsigned long long* works[2] = {m->d_work, m->d_work2};
+  const int qslots[bvhc_mesh::kPipes] = {1, 2, 5};
   for (uint64_t j = 0, off = 0; off < n; ++j, off += kPipeChunk) {
-    int k = (int)(j & 1);
+    const int k = (int)(j % bvhc_mesh::kPipes);
     uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
     cudaStream_t st = m->pipe[k];
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], rays + 6 * off, cnt * 24, cudaMemcpyHostToDevice, st));
     BVHC_CUDA_TRY(dispatch_first(m, static_cast<const float*>(m->slot_in[k]), cnt, side, tab, near_d, far_d,
-                                 static_cast<bvhc_hit*>(m->slot_out[k]), works[k], st, 1 + k));
+                                 static_cast<bvhc_hit*>(m->slot_out[k]), m->d_work_pipe[k], st, qslots[k]));
     BVHC_CUDA_TRY(cudaMemcpyAsync(out + off, m->slot_out[k], cnt * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, st));
   }
-  BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[0]));
-  BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[1]));
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[k]));
   return read_and_clear_error(m, s);
 }
 
