@@ -8,6 +8,7 @@
 #include <exception>
 #include <new>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 #include "bvhc_internal.h"
@@ -306,16 +307,42 @@ bvhc_status read_and_clear_error(bvhc_mesh* m, cudaStream_t s) {
   return BVHC_OK;
 }
 
-void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_t>& dst) {
-  dst.resize(src.size() * (size_t)elem);
-  if (elem == 4) {
-    std::memcpy(dst.data(), src.data(), dst.size());
-  } else {
-    for (size_t i = 0; i < src.size(); ++i) {
-      uint16_t v = (uint16_t)src[i];
-      std::memcpy(dst.data() + 2 * i, &v, 2);
+// fn(k, begin, end) over [0, n) in up to kHostThreads pieces of at least 1M elements, one host
+// thread each (pieces whose thread cannot start run on the calling thread); returns the number
+// of pieces.  Used for the passes over whole index buffers.
+constexpr unsigned kHostThreads = 16;
+template <class F>
+static unsigned parallel_pieces(uint64_t n, F fn) {
+  const uint64_t min_piece = 1ull << 20;
+  const unsigned hw = std::max(1u, std::min(kHostThreads, std::thread::hardware_concurrency()));
+  const unsigned t = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(hw, n / min_piece));
+  const uint64_t piece = (n + t - 1) / t;
+  std::vector<std::thread> pool;
+  for (unsigned k = 1; k < t; ++k) {
+    const uint64_t b = std::min(n, k * piece), e = std::min(n, b + piece);
+    try {
+      pool.emplace_back(fn, k, b, e);
+    } catch (...) {
+      fn(k, b, e);
     }
   }
+  fn(0u, 0ull, std::min(n, piece));
+  for (auto& th : pool) th.join();
+  return t;
+}
+
+void export_width(const std::vector<uint32_t>& src, int elem, std::vector<uint8_t>& dst) {
+  dst.resize(src.size() * (size_t)elem);
+  parallel_pieces(src.size(), [&](unsigned, uint64_t b, uint64_t e) {
+    if (elem == 4) {
+      std::memcpy(dst.data() + 4 * b, src.data() + b, (e - b) * 4);
+    } else {
+      for (uint64_t i = b; i < e; ++i) {
+        const uint16_t v = (uint16_t)src[i];
+        std::memcpy(dst.data() + 2 * i, &v, 2);
+      }
+    }
+  });
 }
 
 // Device leaf layout: every leaf of the reference's tree with more than `max_leaf` triangles becomes
@@ -686,14 +713,20 @@ static bvhc_status build_impl(const float* positions, uint64_t n_verts, int stri
       s->has_index = true;
       s->index_elem_bytes = index_elem_bytes;
       s->index.resize(index_count);
+      uint32_t tops[kHostThreads] = {};
+      const unsigned pieces = parallel_pieces(index_count, [&](unsigned k, uint64_t b, uint64_t e) {
+        uint32_t top = 0;
+        if (index_elem_bytes == 4) {
+          const uint32_t* p32 = static_cast<const uint32_t*>(index);
+          for (uint64_t i = b; i < e; ++i) top = std::max(top, s->index[i] = p32[i]);
+        } else {
+          const uint16_t* p16 = static_cast<const uint16_t*>(index);
+          for (uint64_t i = b; i < e; ++i) top = std::max(top, s->index[i] = p16[i]);
+        }
+        tops[k] = top;
+      });
       uint32_t top = 0;
-      if (index_elem_bytes == 4) {
-        std::memcpy(s->index.data(), index, index_count * 4);
-        for (uint64_t i = 0; i < index_count; ++i) top = std::max(top, s->index[i]);
-      } else {
-        const uint16_t* p16 = static_cast<const uint16_t*>(index);
-        for (uint64_t i = 0; i < index_count; ++i) top = std::max(top, s->index[i] = p16[i]);
-      }
+      for (unsigned k = 0; k < pieces; ++k) top = std::max(top, tops[k]);
       if (index_count && top >= n_verts) { delete s; return BVHC_ERR_INVALID_ARGUMENT; }
     }
     try {
