@@ -535,6 +535,17 @@ def run_closest(args, ws, rank, local):
         torch.cuda.synchronize(dev)
     bvh.synchronize(s)
     ms = max_over_ranks(a.elapsed_time(b) / args.steps, ws, dev)
+    # end to end: pinned host points in, pinned host results out, through the public call (chunks
+    # pipelined over three streams inside the library)
+    pin_p = torch.from_numpy(pts_h).pin_memory()
+    pin_o = torch.empty((n, 5), dtype=torch.float32).pin_memory()
+    e2e = []
+    for _ in range(max(1, args.steps // 2)):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        lib.bvhc_closest_point_to_point(bvh._device_mesh(), pin_p.data_ptr(), n, 0.0, 5.0, pin_o.data_ptr(), 0, None)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(float(np.median(e2e)), ws, dev)
     cpu = roof = None
     if rank == 0 and not args.no_cpu_baseline:
         import oracle.oracle as orc
@@ -563,6 +574,8 @@ def run_closest(args, ws, rank, local):
                 "config": {"workload": f"TorusKnot(10,3,400,100) 80,000 tri, SAH leaf 10; {args.grid}^3 grid over "
                                        "the AABB padded 10%; maxThreshold 5, minThreshold 0", "queries": int(n)},
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
+                        "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
                 "gpu_launches": args.steps * (14 if tuned["best"] == 2 else 1)}
         print(json.dumps(line), flush=True)
     bvh.dispose()

@@ -359,3 +359,48 @@ def test_wide_warp_cooperative_raycast_first(pkg, orc, cuda, leaf, occupancy, co
     ac, ah = ref.raycast_all(rays, cap=64)
     _assert_first_ok(check_first(got, ref.raycast_first(rays), tie_exempt(ac, ah)))
     bvh.dispose()
+
+
+@pytest.mark.parametrize("closest", [0, 2])
+def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
+    """closestPointToPoint through host memory for more than one pipeline chunk (2.5M points: three
+    1M-point chunks on three streams, the last one partial) gives the device-memory call's results,
+    and a strided sample of them matches the oracle."""
+    import torch
+
+    geo, bvh, ref = knot80k
+    bvh.set_traversal(1, 1, 16, 0, 0, 0, closest)
+    rng = np.random.default_rng(23)
+    lo, hi = geo.position.min(0), geo.position.max(0)
+    pts = (lo - 2 + rng.random((2_500_000, 3)) * (hi - lo + 4)).astype(np.float32)
+    host = bvh.closest_point_batch(pts, 0.0, 5.0)
+    d = bvh.closest_point_batch(torch.from_numpy(pts).to(cuda), 0.0, 5.0)
+    torch.cuda.synchronize()
+    dev = d.cpu().numpy().view(np.uint8).reshape(-1)
+    dev = np.frombuffer(dev.tobytes(), dtype=host.dtype)
+    assert np.array_equal(host["face_index"] == 0xFFFFFFFF, dev["face_index"] == 0xFFFFFFFF)
+    hit = host["face_index"] != 0xFFFFFFFF
+    def tri_distance(p):
+        def f(i, face):
+            q = orc.closest_point_triangle(p[i].astype(np.float64), *geo.triangle(face))
+            return float(np.linalg.norm(q - p[i].astype(np.float64)))
+        return f
+
+    # faces agree except between triangles at the same distance (a point nearest to a shared vertex
+    # or edge; the sorted form groups queries per chunk, so a warp's shared order, which picks among
+    # tied triangles, can differ from the one-call run's)
+    dh, dd = host["distance"][hit].astype(np.float64), dev["distance"][hit].astype(np.float64)
+    assert (np.abs(dh - dd) <= 1e-6 * np.maximum(1.0, np.abs(dd))).all()
+    diff = np.nonzero(hit & (host["face_index"] != dev["face_index"]))[0]
+    if closest == 0:
+        assert diff.size == 0
+    dist = tri_distance(pts)
+    for i in diff[:: max(1, diff.size // 2000)]:
+        a, b = dist(i, int(host["face_index"][i])), dist(i, int(dev["face_index"][i]))
+        assert abs(a - b) <= 1e-5 * max(1.0, b), (i, a, b)
+    idx = np.arange(0, pts.shape[0], 97)
+    exp = ref.closest_point(pts[idx], 0.0, 5.0)
+
+    rep = check_closest(host[idx], exp, tri_distance(pts[idx]))
+    assert rep["null"] == 0 and rep["face"] == 0 and rep["distance"] == 0, rep
+    bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)

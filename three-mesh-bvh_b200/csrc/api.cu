@@ -1576,6 +1576,29 @@ bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n
   return read_and_clear_error(m, s);
 }
 
+// The warp-cooperative closest-point variant over Morton-sorted queries (closest = 2, minThreshold
+// 0): queue slot `slot` with its sort scratch sized for n queries; nulls for the other variants.
+static cudaError_t closest_sort(bvhc_mesh* m, int slot, uint64_t n, float min_threshold, uint32_t** q,
+                                unsigned int** qc, RaySort* sort) {
+  *q = nullptr;
+  *qc = nullptr;
+  if (m->cfg.closest != 2 || n >= (1ull << 32) || !(min_threshold <= 0.0f)) return cudaSuccess;
+  cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
+  if (e == cudaSuccess && !m->d_qcount[slot])
+    e = cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int));
+  if (e == cudaSuccess) e = ensure_sort_scratch(m, slot, n);
+  if (e != cudaSuccess) return e;
+  *q = m->d_queue[slot];
+  *qc = m->d_qcount[slot];
+  sort->kind = 2;
+  for (int a = 0; a < 3; ++a) {
+    sort->lo[a] = m->scene_lo[a];
+    sort->hi[a] = m->scene_hi[a];
+  }
+  sort->scratch = m->sort_s[slot];
+  return cudaSuccess;
+}
+
 bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint64_t n, float min_threshold,
                                         float max_threshold, bvhc_closest* out, int mem, void* stream) {
   if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
@@ -1584,36 +1607,53 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE && (!aligned(points, 4) || !aligned(out, 4))) return BVHC_ERR_INVALID_ARGUMENT;
-  // the warp-cooperative variant over Morton-sorted queries uses queue slot 3 and its sort scratch
   const int variant = m->cfg.closest;
-  uint32_t* q = nullptr;
-  unsigned int* qc = nullptr;
+  uint32_t* q;
+  unsigned int* qc;
   RaySort sort{};
-  const int slot = 3;
-  if (variant == 2 && n < (1ull << 32) && min_threshold <= 0.0f) {
-    BVHC_CUDA_TRY(ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t)));
-    if (!m->d_qcount[slot])
-      BVHC_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int)));
-    BVHC_CUDA_TRY(ensure_sort_scratch(m, slot, n));
-    q = m->d_queue[slot];
-    qc = m->d_qcount[slot];
-    sort.kind = 2;
-    for (int a = 0; a < 3; ++a) {
-      sort.lo[a] = m->scene_lo[a];
-      sort.hi[a] = m->scene_hi[a];
-    }
-    sort.scratch = m->sort_s[slot];
+  if (mem == BVHC_MEM_DEVICE || n <= kPipeChunk) {
+    // one launch; the sorted variant uses queue slot 3
+    BVHC_CUDA_TRY(closest_sort(m, 3, n, min_threshold, &q, &qc, &sort));
+    if (mem == BVHC_MEM_DEVICE)
+      return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s, variant,
+                                            m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+    BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
+    BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
+    BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold,
+                                       max_threshold, static_cast<bvhc_closest*>(m->d_out), s, variant,
+                                       m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+    BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
+    return read_and_clear_error(m, s);
   }
-  if (mem == BVHC_MEM_DEVICE)
-    return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s, variant,
-                                          m->cfg.occupancy, q, qc, q ? &sort : nullptr));
-  BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
-  BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
-  BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
-  BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold, max_threshold,
-                                     static_cast<bvhc_closest*>(m->d_out), s, variant, m->cfg.occupancy, q, qc,
-                                     q ? &sort : nullptr));
-  BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
+  // Large host batches: chunks of kPipeChunk points rotate over the raycastFirst pipeline's three
+  // streams and staging slots (12 B in and 20 B out per point fit its 24 B / 32 B per ray), so the
+  // copies of some chunks overlap the traversal of others; each stream sorts its own chunk in its
+  // own queue slot.
+  BVHC_CUDA_TRY(ensure_pipeline(m));
+  const int qslots[bvhc_mesh::kPipes] = {1, 2, 5};
+  uint32_t* qs[bvhc_mesh::kPipes];
+  unsigned int* qcs[bvhc_mesh::kPipes];
+  RaySort sorts[bvhc_mesh::kPipes] = {};
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k)
+    BVHC_CUDA_TRY(closest_sort(m, qslots[k], kPipeChunk, min_threshold, &qs[k], &qcs[k], &sorts[k]));
+  cudaEvent_t ready;
+  BVHC_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  cudaEventRecord(ready, s);
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) cudaStreamWaitEvent(m->pipe[k], ready, 0);
+  cudaEventDestroy(ready);
+  for (uint64_t j = 0, off = 0; off < n; ++j, off += kPipeChunk) {
+    const int k = (int)(j % bvhc_mesh::kPipes);
+    const uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
+    cudaStream_t st = m->pipe[k];
+    BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], points + 3 * off, cnt * 12, cudaMemcpyHostToDevice, st));
+    BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->slot_in[k]), cnt, min_threshold,
+                                       max_threshold, static_cast<bvhc_closest*>(m->slot_out[k]), st, variant,
+                                       m->cfg.occupancy, qs[k], qcs[k], qs[k] ? &sorts[k] : nullptr));
+    BVHC_CUDA_TRY(
+        cudaMemcpyAsync(out + off, m->slot_out[k], cnt * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, st));
+  }
+  for (int k = 0; k < bvhc_mesh::kPipes; ++k) BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[k]));
   return read_and_clear_error(m, s);
 }
 
