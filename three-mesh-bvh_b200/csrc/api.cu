@@ -50,8 +50,8 @@ struct bvhc_mesh {
   unsigned long long* d_work_pipe[kPipes] = {};
   // work queues (grow-only): [0] direct raycastFirst calls, [1], [2], [5] the three pipeline slots
   // (so that concurrently running chunks never share a queue), [3] closestPointToPoint, [4] raycast
-  // (all hits)
-  static constexpr int kSlots = 6;
+  // (all hits), [6] the shapecasts' query order
+  static constexpr int kSlots = 7;
   uint32_t* d_queue[kSlots] = {};
   size_t queue_cap[kSlots] = {};
   unsigned int* d_qcount[kSlots] = {};
@@ -1511,6 +1511,30 @@ bvhc_status bvhc_triangle_hit_point_info(bvhc_mesh* m, const float* points, cons
   return read_and_clear_error(m, s);
 }
 
+// Batches of at least kShapeSortMin shapecast queries are taken in the Morton order of their
+// centres (queue slot 6 and its sort scratch); smaller ones in input order.
+constexpr uint64_t kShapeSortMin = 4096;
+static cudaError_t shape_order(bvhc_mesh* m, uint64_t n, uint32_t** q, unsigned int** qc, RaySort* sort) {
+  *q = nullptr;
+  *qc = nullptr;
+  if (n < kShapeSortMin || n >= (1ull << 32)) return cudaSuccess;
+  const int slot = 6;
+  cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
+  if (e == cudaSuccess && !m->d_qcount[slot])
+    e = cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int));
+  if (e == cudaSuccess) e = ensure_sort_scratch(m, slot, n);
+  if (e != cudaSuccess) return e;
+  *q = m->d_queue[slot];
+  *qc = m->d_qcount[slot];
+  sort->kind = 2;
+  for (int a = 0; a < 3; ++a) {
+    sort->lo[a] = m->scene_lo[a];
+    sort->hi[a] = m->scene_hi[a];
+  }
+  sort->scratch = m->sort_s[slot];
+  return cudaSuccess;
+}
+
 bvhc_status bvhc_intersects_sphere(bvhc_mesh* m, const float* spheres, uint64_t n, uint8_t* out, int mem,
                                    void* stream) {
   if (!m || (mem != BVHC_MEM_HOST && mem != BVHC_MEM_DEVICE)) return BVHC_ERR_INVALID_ARGUMENT;
@@ -1518,15 +1542,17 @@ bvhc_status bvhc_intersects_sphere(bvhc_mesh* m, const float* spheres, uint64_t 
   if (!spheres || !out) return BVHC_ERR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
-  if (mem == BVHC_MEM_DEVICE) {
-    if (!aligned(spheres, 16)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_intersects_sphere(m->view(), spheres, n, out, s));
-  }
+  if (mem == BVHC_MEM_DEVICE && !aligned(spheres, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+  uint32_t* q;
+  unsigned int* qc;
+  RaySort sort{};
+  BVHC_CUDA_TRY(shape_order(m, n, &q, &qc, &sort));
+  if (mem == BVHC_MEM_DEVICE) return from_cuda(launch_intersects_sphere(m->view(), spheres, n, out, s, q, qc, &sort));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 16));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, spheres, n * 16, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_intersects_sphere(m->view(), static_cast<const float*>(m->d_in), n,
-                                         static_cast<uint8_t*>(m->d_out), s));
+                                         static_cast<uint8_t*>(m->d_out), s, q, qc, &sort));
   BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n, cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
 }
@@ -1537,15 +1563,17 @@ bvhc_status bvhc_intersects_box(bvhc_mesh* m, const float* boxes, uint64_t n, ui
   if (!boxes || !out) return BVHC_ERR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
-  if (mem == BVHC_MEM_DEVICE) {
-    if (!aligned(boxes, 16)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_intersects_box(m->view(), boxes, n, out, s));
-  }
+  if (mem == BVHC_MEM_DEVICE && !aligned(boxes, 16)) return BVHC_ERR_INVALID_ARGUMENT;
+  uint32_t* q;
+  unsigned int* qc;
+  RaySort sort{};
+  BVHC_CUDA_TRY(shape_order(m, n, &q, &qc, &sort));
+  if (mem == BVHC_MEM_DEVICE) return from_cuda(launch_intersects_box(m->view(), boxes, n, out, s, q, qc, &sort));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 96));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, boxes, n * 96, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_intersects_box(m->view(), static_cast<const float*>(m->d_in), n,
-                                      static_cast<uint8_t*>(m->d_out), s));
+                                      static_cast<uint8_t*>(m->d_out), s, q, qc, &sort));
   BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n, cudaMemcpyDeviceToHost, s));
   return read_and_clear_error(m, s);
 }
@@ -1558,10 +1586,14 @@ bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   const uint32_t c = cap > 0 ? cap : 1;
-  if (mem == BVHC_MEM_DEVICE && cap > 0) {
-    if (!aligned(spheres, 16) || !aligned(counts, 4) || !aligned(faces, 4)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_sphere_triangles(m->view(), spheres, n, cap, counts, faces, s));
-  }
+  if (mem == BVHC_MEM_DEVICE && (!aligned(spheres, 16) || !aligned(counts, 4) || (cap > 0 && !aligned(faces, 4))))
+    return BVHC_ERR_INVALID_ARGUMENT;
+  uint32_t* q;
+  unsigned int* qc;
+  RaySort sort{};
+  BVHC_CUDA_TRY(shape_order(m, n, &q, &qc, &sort));
+  if (mem == BVHC_MEM_DEVICE && cap > 0)
+    return from_cuda(launch_sphere_triangles(m->view(), spheres, n, cap, counts, faces, s, q, qc, &sort));
   const bool host = mem == BVHC_MEM_HOST;
   if (host) BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 16));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * c * 4));
@@ -1569,7 +1601,7 @@ bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n
   if (host) BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, spheres, n * 16, cudaMemcpyHostToDevice, s));
   uint32_t* d_counts = host ? static_cast<uint32_t*>(m->d_out2) : counts;
   BVHC_CUDA_TRY(launch_sphere_triangles(m->view(), host ? static_cast<const float*>(m->d_in) : spheres, n, c, d_counts,
-                                        static_cast<uint32_t*>(m->d_out), s));
+                                        static_cast<uint32_t*>(m->d_out), s, q, qc, &sort));
   if (!host) return BVHC_OK;  // counts only, on the device
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, d_counts, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0) BVHC_CUDA_TRY(cudaMemcpyAsync(faces, m->d_out, n * cap * 4, cudaMemcpyDeviceToHost, s));

@@ -1156,9 +1156,11 @@ __device__ __forceinline__ bool sphere_meets(float3 c, ff r2, const Tri& t) {
 }
 
 __global__ void __launch_bounds__(kBlock) intersects_sphere_kernel(MeshDev m, const float* __restrict__ spheres,
-                                                                   uint64_t n, uint8_t* __restrict__ out) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                                                   uint64_t n, uint8_t* __restrict__ out,
+                                                                   const uint32_t* __restrict__ queue) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint64_t i = queue ? (uint64_t)__ldg(queue + t) : t;
   const float4 sph = ld4(spheres + 4 * i);
   const float3 c = make_float3(sph.x, sph.y, sph.z);
   const ff r2 = two_prod(sph.w, sph.w);
@@ -1239,9 +1241,11 @@ __device__ int sphere_box_relation(const float* b, float3 c, float r) {
 __global__ void __launch_bounds__(kBlock) sphere_triangles_kernel(MeshDev m, const float* __restrict__ spheres,
                                                                   uint64_t n, uint32_t cap,
                                                                   uint32_t* __restrict__ counts,
-                                                                  uint32_t* __restrict__ faces) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                                                  uint32_t* __restrict__ faces,
+                                                                  const uint32_t* __restrict__ queue) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint64_t i = queue ? (uint64_t)__ldg(queue + t) : t;
   const float4 sph = ld4(spheres + 4 * i);
   const float3 c = make_float3(sph.x, sph.y, sph.z);
   const ff r2 = two_prod(sph.w, sph.w);
@@ -1819,9 +1823,11 @@ struct BoxAny {
 // non-empty leaf (or its traversal ends), then the lanes holding leaves test their triangles
 // together, so the costly triangle tests of a few lanes are not paid at every node step.
 __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const float* __restrict__ boxes,
-                                                                uint64_t n, uint8_t* __restrict__ out) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                                                uint64_t n, uint8_t* __restrict__ out,
+                                                                const uint32_t* __restrict__ queue) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint64_t i = queue ? (uint64_t)__ldg(queue + t) : t;
   BoxAny q;
   q.init(boxes, i);
   bool hit = false;
@@ -2351,6 +2357,40 @@ __global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restri
   keys[i] = morton3(quantise(__ldg(pts + 3 * i), box.lo[0], sx, 256.0f),
                     quantise(__ldg(pts + 3 * i + 1), box.lo[1], sy, 256.0f),
                     quantise(__ldg(pts + 3 * i + 2), box.lo[2], sz, 256.0f));
+}
+
+// Morton key of each shape's centre over the mesh box (8 bits per axis), ids in input order, and
+// the queue length: kind 0 spheres (cx, cy, cz, r), kind 1 oriented boxes (the box-to-mesh matrix
+// applied to the centre of the local box).  The shapecast kernels then take the queries in key
+// order, so the 32 lanes of a warp hold nearby shapes whose traversals mostly coincide.
+__global__ void __launch_bounds__(kBlock) shape_key_kernel(const float* __restrict__ q, uint64_t n, int kind,
+                                                          SceneBox box, uint32_t* __restrict__ ids,
+                                                          uint32_t* __restrict__ keys,
+                                                          unsigned int* __restrict__ qcount) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *qcount = (unsigned int)n;
+  if (i >= n) return;
+  float p[3];
+  if (kind == 0) {
+    const float4 v = ld4(q + 4 * i);
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+  } else {
+    const float* b = q + 24 * i;
+    const float* e = b + 8;
+    const float x = 0.5f * (__ldg(b) + __ldg(b + 4)), y = 0.5f * (__ldg(b + 1) + __ldg(b + 5)),
+                z = 0.5f * (__ldg(b + 2) + __ldg(b + 6));
+    for (int k = 0; k < 3; ++k)
+      p[k] = fmaf(__ldg(e + k), x, fmaf(__ldg(e + 4 + k), y, fmaf(__ldg(e + 8 + k), z, __ldg(e + 12 + k))));
+  }
+  uint32_t c[3];
+  for (int a = 0; a < 3; ++a) {
+    const float inv = box.hi[a] > box.lo[a] ? 1.0f / (box.hi[a] - box.lo[a]) : 0.0f;
+    c[a] = quantise(p[a], box.lo[a], inv, 256.0f);
+  }
+  ids[i] = (uint32_t)i;
+  keys[i] = morton3(c[0], c[1], c[2]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -3029,10 +3069,31 @@ cudaError_t launch_hit_interpolate(const bvhc_hit* hits, uint64_t n, const uint3
   return cudaGetLastError();
 }
 
+// Sorts the n shapes' ids by the Morton key of their centres into `queue`.
+static cudaError_t sort_shapes(const float* shapes, uint64_t n, int kind, uint32_t* queue, unsigned int* qcount,
+                               const RaySort& sort, cudaStream_t stream) {
+  uint32_t *ids, *keys;
+  ray_sort_input(2, sort.scratch, queue, &ids, &keys);
+  dev::SceneBox box{};
+  for (int a = 0; a < 3; ++a) {
+    box.lo[a] = sort.lo[a];
+    box.hi[a] = sort.hi[a];
+  }
+  dev::shape_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(shapes, n, kind, box, ids, keys, qcount);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_ray_sort(2, n, qcount, sort.scratch, queue, stream);
+}
+
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
-                                     cudaStream_t stream) {
+                                     cudaStream_t stream, uint32_t* queue, unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  dev::intersects_sphere_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, out);
+  const bool sorted = queue && qcount && sort;
+  if (sorted) {
+    cudaError_t e = sort_shapes(spheres, n, 0, queue, qcount, *sort, stream);
+    if (e != cudaSuccess) return e;
+  }
+  dev::intersects_sphere_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, out, sorted ? queue : nullptr);
   return cudaGetLastError();
 }
 
@@ -3070,10 +3131,17 @@ cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene,
   return cudaGetLastError();
 }
 
-cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
-                                    uint32_t* faces, cudaStream_t stream) {
+cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap,
+                                    uint32_t* counts, uint32_t* faces, cudaStream_t stream, uint32_t* queue,
+                                    unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  dev::sphere_triangles_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, cap, counts, faces);
+  const bool sorted = queue && qcount && sort;
+  if (sorted) {
+    cudaError_t e = sort_shapes(spheres, n, 0, queue, qcount, *sort, stream);
+    if (e != cudaSuccess) return e;
+  }
+  dev::sphere_triangles_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, spheres, n, cap, counts, faces,
+                                                                       sorted ? queue : nullptr);
   return cudaGetLastError();
 }
 
@@ -3088,9 +3156,14 @@ cudaError_t launch_triangle_hit_point_info(const float* points, const uint32_t* 
 }
 
 cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
-                                  cudaStream_t stream) {
+                                  cudaStream_t stream, uint32_t* queue, unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  dev::intersects_box_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, boxes, n, out);
+  const bool sorted = queue && qcount && sort;
+  if (sorted) {
+    cudaError_t e = sort_shapes(boxes, n, 1, queue, qcount, *sort, stream);
+    if (e != cudaSuccess) return e;
+  }
+  dev::intersects_box_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, boxes, n, out, sorted ? queue : nullptr);
   return cudaGetLastError();
 }
 

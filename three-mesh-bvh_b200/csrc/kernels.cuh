@@ -116,8 +116,12 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
 
 // intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
 // sphere i.
+// Shapecasts (intersectsSphere, triangles within spheres, intersectsBox): with queue, qcount and
+// sort scratch for n queries, the queries are first sorted by the Morton key of their centres over
+// sort->lo..hi and taken in that order (results stay in input order); otherwise in input order.
 cudaError_t launch_intersects_sphere(const MeshDev& m, const float* spheres, uint64_t n, uint8_t* out,
-                                     cudaStream_t stream);
+                                     cudaStream_t stream, uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
+                                     const RaySort* sort = nullptr);
 
 // Instances of a batch's geometries (bvhc_scene_*).  Matrices are the affine rows 0..2 of the
 // instance's world matrix, row-major 3 x 4 (x' = r0 x + r1 y + r2 z + r3), as float-float pairs
@@ -154,7 +158,8 @@ cudaError_t launch_scene_raycast_all(const MeshDev& blas, const SceneDev& scene,
 // Triangles within each sphere (n x 4, 16-byte aligned) through shapecast's CONTAINED path:
 // counts[i] the total, faces[i * cap ..] the first cap faceIndex values in traversal order.
 cudaError_t launch_sphere_triangles(const MeshDev& m, const float* spheres, uint64_t n, uint32_t cap, uint32_t* counts,
-                                    uint32_t* faces, cudaStream_t stream);
+                                    uint32_t* faces, cudaStream_t stream, uint32_t* queue = nullptr,
+                                    unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 
 // getTriangleHitPointInfo's material lookup: the first of n groups whose [start, start + count)
 // (index units, count < 0 = Infinity) holds the triangle's first index gives its materialIndex.
@@ -173,7 +178,8 @@ cudaError_t launch_triangle_hit_point_info(const float* points, const uint32_t* 
 // intersectsBox: boxes n x 24 (min xyz, pad, max xyz, pad, column-major box-to-mesh matrix),
 // 16-byte aligned; out[i] = 1 if the oriented box meets the mesh.
 cudaError_t launch_intersects_box(const MeshDev& m, const float* boxes, uint64_t n, uint8_t* out,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
+                                  const RaySort* sort = nullptr);
 
 // Vertex attribute at each hit (barycentric interpolation over the hit triangle's vertices, via
 // tri_vid: 3 vertex ids per triangle); rays (nullable, item_size 3) flip results that point along
