@@ -2064,7 +2064,10 @@ __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, 
 // far; each entered instance box is walked in the instance's frame right away.  With a queue,
 // thread i takes ray queue[i] (rays ordered by a Morton key, so that a warp's rays share paths)
 // and writes that ray's row.
-__global__ void __launch_bounds__(kBlock, 5) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
+// 14 resident blocks per SM (36 registers, some spilled): the kernel stalls on fetching its own
+// large body and on its scattered loads, and more resident warps hide both; the instanced bench
+// measured 35.6 / 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks.
+__global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
                                                                         const float* __restrict__ rays, uint64_t n,
                                                                         const uint32_t* __restrict__ queue, int side,
                                                                         float near_d, float far_d,
