@@ -169,3 +169,21 @@ def test_scene_all_hits_match_oracle(pkg, orc, batch, cuda):
     c0, _, _ = scene.raycast(rays, cap=0)
     assert np.array_equal(c0, counts)
     scene.dispose()
+
+
+def test_scene_host_pipeline(pkg, batch, cuda):
+    """World rays through host memory in more than one pipeline chunk (2.5M rays: three 1M-ray
+    chunks on three streams, the last partial) give exactly the device-memory call's records."""
+    import torch
+
+    rng = np.random.default_rng(77)
+    geometry, mats = instance_matrices(rng, 300, batch.n_meshes, spread=150.0)
+    scene = batch.instances(geometry, mats)
+    rays = world_rays(rng, 2_500_000)
+    got, ginst = scene.raycast_first(rays)
+    dh, di = scene.raycast_first(torch.from_numpy(rays).to(cuda))
+    torch.cuda.synchronize()
+    assert np.array_equal(di.cpu().numpy().view(np.uint32), ginst)
+    assert np.array_equal(dh.cpu().numpy().view(np.uint8).reshape(-1), got.view(np.uint8).reshape(-1))
+    assert (ginst != 0xFFFFFFFF).mean() > 0.2
+    scene.dispose()

@@ -1823,6 +1823,7 @@ struct bvhc_scene {
   unsigned int* d_qcount = nullptr;
   void* d_cnt = nullptr;  // host-memory bvhc_scene_raycast: per-ray counts
   size_t cnt_cap = 0;
+  void* inst_slot[bvhc_mesh::kPipes] = {};  // pipelined host-memory raycastFirst: instance ids per stream
 };
 
 namespace {
@@ -2019,6 +2020,33 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   const SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
+  if (mem == BVHC_MEM_HOST && n > kPipeChunk) {
+    // Large host batches: chunks of kPipeChunk rays rotate over the batch mesh's three pipeline
+    // streams and staging slots (instance ids in a slot of the scene's own), so the copies of some
+    // chunks overlap the traversal of others.  Each chunk keeps its input order (the ray sort of
+    // bvhc_scene_set_order changes the traversal time by a few percent at most).
+    BVHC_CUDA_TRY(ensure_pipeline(m));
+    for (int k = 0; k < bvhc_mesh::kPipes; ++k)
+      if (!sc->inst_slot[k]) BVHC_CUDA_TRY(cudaMalloc(&sc->inst_slot[k], kPipeChunk * 4));
+    cudaEvent_t ready;
+    BVHC_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    cudaEventRecord(ready, s);
+    for (int k = 0; k < bvhc_mesh::kPipes; ++k) cudaStreamWaitEvent(m->pipe[k], ready, 0);
+    cudaEventDestroy(ready);
+    for (uint64_t j = 0, off = 0; off < n; ++j, off += kPipeChunk) {
+      const int k = (int)(j % bvhc_mesh::kPipes);
+      const uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
+      cudaStream_t st = m->pipe[k];
+      BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], rays + 6 * off, cnt * 24, cudaMemcpyHostToDevice, st));
+      BVHC_CUDA_TRY(launch_scene_raycast_first(m->view(), sd, static_cast<const float*>(m->slot_in[k]), cnt, side,
+                                               near_dist, far_dist, static_cast<bvhc_hit*>(m->slot_out[k]),
+                                               static_cast<uint32_t*>(sc->inst_slot[k]), st));
+      BVHC_CUDA_TRY(cudaMemcpyAsync(hits + off, m->slot_out[k], cnt * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, st));
+      BVHC_CUDA_TRY(cudaMemcpyAsync(instance + off, sc->inst_slot[k], cnt * 4, cudaMemcpyDeviceToHost, st));
+    }
+    for (int k = 0; k < bvhc_mesh::kPipes; ++k) BVHC_CUDA_TRY(cudaStreamSynchronize(m->pipe[k]));
+    return read_and_clear_error(m, s);
+  }
   RaySort sort{};
   if (sc->order > 0 && n < (1ull << 32) && sc->root != kEmptyLeaf) {
     if (sc->sort_cap < n) {
@@ -2112,6 +2140,7 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
   cudaFree(sc->d_queue);
   cudaFree(sc->d_qcount);
   cudaFree(sc->d_cnt);
+  for (void* p : sc->inst_slot) cudaFree(p);
   free_sort_scratch(sc->sort_s);
   delete sc;
 }
