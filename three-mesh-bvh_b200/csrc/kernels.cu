@@ -2069,6 +2069,11 @@ __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, 
 // far; each entered instance box is walked in the instance's frame right away.  With a queue,
 // thread i takes ray queue[i] (rays ordered by a Morton key, so that a warp's rays share paths)
 // and writes that ray's row.
+// Instance-tree stack: the tree is a median split (bvhc_scene_set_instances), so its depth is at most
+// log2 of the instance count, below 32 for any instance count the ABI takes; half the geometry
+// trees' kMaxStack keeps the per-thread frame (and its spill traffic at high occupancy) smaller.
+constexpr int kTlasStack = 32;
+
 // 14 resident blocks per SM (36 registers, some spilled): the kernel stalls on fetching its own
 // large body and on its scattered loads, and more resident warps hide both; the instanced bench
 // measured 35.6 / 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks.
@@ -2087,8 +2092,8 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
   bvhc_hit best_hit;
   ff best_dist = ff_from(kInf);
   uint32_t best_inst = 0xFFFFFFFFu;
-  uint32_t stack_link[kMaxStack];
-  float stack_t[kMaxStack];
+  uint32_t stack_link[kTlasStack];
+  float stack_t[kTlasStack];
   int sp = 0;
   uint32_t link = sc.root;
   bool go = link != kEmptyLeaf;
@@ -2107,7 +2112,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
       const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
       if (h1st) {
         if (h2nd) {
-          if (sp >= kMaxStack) {
+          if (sp >= kTlasStack) {
             atomicOr(m.err, kErrStackOverflow);
             go = false;
             break;
@@ -2198,7 +2203,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_all_kernel(MeshDev m
   bvhc_hit* row = hits + i * (uint64_t)cap;
   uint32_t* irow = inst_out + i * (uint64_t)cap;
   uint32_t cnt = 0, stored = 0;
-  uint32_t tstack[kMaxStack];
+  uint32_t tstack[kTlasStack];
   uint32_t bstack[kMaxStack];
   int tsp = 0;
   uint32_t link = sc.root;
@@ -2210,7 +2215,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_all_kernel(MeshDev m
       const bool h0 = box_hit(p.l[0], p.l[1], p.l[2], p.l[3], p.l[4], p.l[5], w, 0.0f, kInf, e0);
       const bool h1 = box_hit(p.r[0], p.r[1], p.r[2], p.r[3], p.r[4], p.r[5], w, 0.0f, kInf, e1);
       if (h0 && h1) {
-        if (tsp >= kMaxStack) {
+        if (tsp >= kTlasStack) {
           atomicOr(m.err, kErrStackOverflow);
           go = false;
           break;
