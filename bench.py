@@ -308,9 +308,9 @@ def run_engine(args, ws, rank, local):
     stream = torch.cuda.current_stream(dev)
     # traversal variant per ray set: forced, autotuned, or the library default
     tuned = {}
-    configs = [None] * len(sets)
+    set_configs = [None] * len(sets)
     if args.traversal:
-        configs = parse_traversal(args.traversal, [n for n, _ in sets])
+        set_configs = parse_traversal(args.traversal, [n for n, _ in sets])
     elif not args.no_tune:
         from three_mesh_bvh_b200 import autotune
 
@@ -321,14 +321,14 @@ def run_engine(args, ws, rank, local):
                                                leaf_sizes=[int(x) for x in args.leaf_sizes.split(",")],
                                                tag="knot2M")
         tuned = {"leaf_size": res["leaf"], "total_ms_by_leaf_size": res["total_ms"], **res["sets"]}
-        configs = [res["sets"][n]["best"] for n, _ in sets]
+        set_configs = [res["sets"][n]["best"] for n, _ in sets]
     if args.leaf_size is not None:
         bvh.set_leaf_size(args.leaf_size)
 
     def step(ev=None):
         for k in range(len(sets)):
-            if configs[k] is not None:
-                bvh.set_traversal(*configs[k])
+            if set_configs[k] is not None:
+                bvh.set_traversal(*set_configs[k])
             if ev is not None:
                 ev[k][0].record(stream)
             bvh.raycast_first_batch(d_rays[k], out=d_out[k], stream=stream.cuda_stream)
@@ -366,8 +366,8 @@ def run_engine(args, ws, rank, local):
 
     def e2e_step():
         for k in range(len(sets)):
-            if configs[k] is not None:
-                bvh.set_traversal(*configs[k])
+            if set_configs[k] is not None:
+                bvh.set_traversal(*set_configs[k])
             bvh.raycast_first_batch(host_in[k], out=host_out[k])
 
     e2e_step()
@@ -397,7 +397,7 @@ def run_engine(args, ws, rank, local):
         both = sum(bytes_per_launch) / (sum(per_set_ms) / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": profile_traffic(f"raycast_first_k2_{sets[k][0]}.md"), "peak_source": how,
-                "kernel": traversal_kernel(configs[k]), "ray_set": sets[k][0],
+                "kernel": traversal_kernel(set_configs[k]), "ray_set": sets[k][0],
                 "both_sets": {"achieved": both, "frac": both / peak},
                 "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], map(float, bytes_per_launch))),
                 "reference_node_reads_per_ray": [s[0] for s in stats],
@@ -412,10 +412,10 @@ def run_engine(args, ws, rank, local):
                            "parallelism": f"replicas x{ws}"},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
-                "traversal": {n: (list(c) if c is not None else None) for (n, _), c in zip(sets, configs)},
+                "traversal": {n: (list(c) if c is not None else None) for (n, _), c in zip(sets, set_configs)},
                 "leaf_size": bvh.get_leaf_size(),
                 "autotune": tuned, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": args.steps * sum(kernel_launches(c) for c in configs)}
+                "gpu_launches": args.steps * sum(kernel_launches(c) for c in set_configs)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 
