@@ -56,8 +56,11 @@ def parse():
     ap.add_argument("--rays-log2", type=int, default=24)
     ap.add_argument("--camera", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=1 << 25, help="rays (both sets together) timed on the CPU baseline")
-    ap.add_argument("--ref-sample", type=int, default=1 << 21, help="rays per set per step in --impl reference")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="rays (both sets together) per step in --impl reference; 0: the whole workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="first workload: skip the batched and forward/backward parts of the line")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default traversal variant)")
     ap.add_argument("--leaf-sizes", default="0,2,4",
                     help="device leaf layouts the autotuner tries (0: the reference's leaves)")
@@ -108,12 +111,38 @@ def weak_scaling_rate(ws: int, rays_per_rank: int, steps: int, ms: float) -> flo
     return ws * rays_per_rank * steps / (ms / 1e3) / 1e6
 
 
-def scene(pkg, args, rank):
+BUILD_OPTIONS = {"maxLeafSize": 10, "maxDepth": 40}   # with strategy SAH
+
+
+def scene_inputs(pkg, args, rank):
+    """The noisy knot and the two ray sets (numpy generators only: no library is loaded)."""
     geo = pkg.torus_knot(10, 3, args.tubular, args.radial, noise_sigma=0.02, noise_seed=1)
-    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, "maxLeafSize": 10, "maxDepth": 40})
     inc = pkg.rays_incoherent(1 << args.rays_log2, seed=incoherent_seed(rank))
     cam = pkg.rays_camera(args.camera, args.camera)
+    return geo, inc, cam
+
+
+def scene(pkg, args, rank):
+    geo, inc, cam = scene_inputs(pkg, args, rank)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH, **BUILD_OPTIONS})
     return geo, bvh, inc, cam
+
+
+def headline_config(triangles, rays_per_step, ws):
+    """The headline line's config, identical in the engine and reference arms."""
+    return {"workload": WORKLOAD, "triangles": int(triangles), "rays_per_step": int(rays_per_step),
+            "l2": "inputs larger than L2 (805 MB of rays + 1.07 GB of hits per step)",
+            "parallelism": f"replicas x{ws}"}
+
+
+def sample_index(n, sample, block=1 << 16):
+    """Ray ids of a bounded sample of a set of n: every ray when sample >= n, else contiguous
+    blocks of `block` rays spread evenly over the set (coherence within a block is kept)."""
+    if sample >= n:
+        return np.arange(n, dtype=np.int64)
+    nb = max(1, sample // block)
+    starts = np.linspace(0, n - block, nb).astype(np.int64)
+    return (starts[:, None] + np.arange(block)[None, :]).reshape(-1)
 
 
 class ClockSampler:
@@ -232,61 +261,94 @@ def profile_traffic(name):
     return float(m.group(1)) if m else None
 
 
-def cpu_reference(pkg, bvh, geo, sets, sample, threads):
-    """The oracle (C++ float64 restatement of the reference) on a bounded sample of each ray set.
-    Returns rays/s over the sample plus the reference traversal's mean node reads and triangle
-    tests per ray (the algorithmic-bytes counters)."""
-    import oracle.oracle as orc
+def parity_module():
+    """tests/parity.py: the parity bar of the engine's contract, shared with the tests."""
+    if str(ROOT / "tests") not in sys.path:
+        sys.path.insert(0, str(ROOT / "tests"))
+    import parity
 
-    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
-    stats = []
+    return parity
+
+
+def cpu_reference(ref, sets, got_sets, sample, threads):
+    """The oracle (C++ float64 restatement of the reference path) timed on a bounded sample of
+    each ray set (the whole set by default), and the engine's hits for the same rays checked
+    against its results (outside the timed region; tests/parity.py's bar).  Returns rays/s over
+    the sample, the reference traversal's mean node reads and triangle tests per ray (the
+    algorithmic-bytes counters), the sample size and the parity counts per set."""
+    par_mod = parity_module()
+    stats, parity = [], {}
     total_rays, total_s = 0, 0.0
     chunk = 1 << 21
-    for rays in sets:
-        idx = np.linspace(0, rays.shape[0] - 1, min(sample, rays.shape[0])).astype(np.int64)
+    for (name, rays), got in zip(sets, got_sets):
+        idx = sample_index(rays.shape[0], sample)
         sn = st = 0
+        tot = {}
         for c0 in range(0, idx.size, chunk):
-            sub = np.ascontiguousarray(rays[idx[c0:c0 + chunk]])
+            ii = idx[c0:c0 + chunk]
+            sub = np.ascontiguousarray(rays[ii])
             t0 = time.perf_counter()
-            _, nn, nt = ref.raycast_first(sub, 0, 0.0, math.inf, threads=threads, counters=True)
+            exp, nn, nt = ref.raycast_first(sub, 0, 0.0, math.inf, threads=threads, counters=True)
             total_s += time.perf_counter() - t0
             sn += int(nn.sum())
             st += int(nt.sum())
+            if got is not None:
+                par_mod.add_counts(tot, par_mod.first_parity_chunk(ref, sub, got[ii], exp, threads=threads))
         total_rays += idx.size
         stats.append((sn / idx.size, st / idx.size))
-    return total_rays / total_s, stats, total_rays
+        if got is not None:
+            parity[name] = tot
+    return total_rays / total_s, stats, total_rays, parity
 
 
 def run_reference(args, ws, rank):
-    """--impl reference: the reference path's CPU implementation (the oracle port; the JS
-    reference cannot run without Node and three.js) on all host threads, bounded per step."""
+    """--impl reference: the reference path's CPU implementation on all host threads.  That is
+    the oracle, a C++ float64 restatement of three-mesh-bvh's build and raycastFirst (the JS
+    reference itself needs Node and three.js, neither of which is on this machine).  The BVH comes
+    from the oracle's own builder (SAH, maxLeafSize 10, maxDepth 40; byte-identical to the
+    engine's), and each step traces the engine arm's exact workload: both whole ray sets, in
+    order.  Only rank 0 runs; it prints the line."""
     if rank != 0:
         return
     import __graft_entry__ as ge
 
-    pkg = ge.load_package()
-    geo, bvh, inc, cam = scene(pkg, args, 0)
+    pkg = ge.load_package()          # numpy generators only; libbvhcuda is never loaded here
+    geo, inc, cam = scene_inputs(pkg, args, 0)
     threads = os.cpu_count() or 1
     import oracle.oracle as orc
 
-    ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
-    per = max(1, args.ref_sample)
-    sub = np.concatenate([inc[np.linspace(0, inc.shape[0] - 1, per).astype(np.int64)],
-                          cam[np.linspace(0, cam.shape[0] - 1, per).astype(np.int64)]])
+    ref = orc.OracleBVH.build(geo.position, geo.index.copy(), strategy=2, max_depth=BUILD_OPTIONS["maxDepth"],
+                              target_leaf=BUILD_OPTIONS["maxLeafSize"])
+    sets = [inc, cam]
+    n_step = sum(r.shape[0] for r in sets)
+    sample = args.ref_sample if args.ref_sample > 0 else n_step
+    idx = [sample_index(r.shape[0], sample // len(sets)) for r in sets]
+    chunk = 1 << 21
+
+    def step():
+        for r, ii in zip(sets, idx):
+            for c0 in range(0, ii.size, chunk):
+                ref.raycast_first(np.ascontiguousarray(r[ii[c0:c0 + chunk]]), threads=threads)
+
     for _ in range(args.warmup):
-        ref.raycast_first(sub[: min(4096, sub.shape[0])], threads=threads)
+        step()
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        ref.raycast_first(sub, threads=threads)
+        step()
         times.append(time.perf_counter() - t0)
-    rate = sub.shape[0] / statistics.mean(times) / 1e6
-    sample = f"{sub.shape[0]} rays per step ({per} incoherent + {per} camera, evenly strided)"
+    traced = sum(ii.size for ii in idx)
+    rate = traced / statistics.mean(times) / 1e6
+    what = ("both whole ray sets" if traced == n_step else
+            f"{traced} rays (contiguous 65536-ray blocks spread over both sets)")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "implementation": "oracle C++ float64 restatement (port)"},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "config": headline_config(geo.triangle_count, n_step, 1),
+            "implementation": "oracle: C++ float64 restatement of the reference's build and raycastFirst (port); "
+                              "BVH from the oracle's builder",
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{what} per step, {threads} threads"},
             "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -320,7 +382,8 @@ def run_engine(args, ws, rank, local):
         res = autotune.tune_raycast_first_sets(bvh, [(n, d) for (n, _), d in zip(sets, d_rays)],
                                                leaf_sizes=[int(x) for x in args.leaf_sizes.split(",")],
                                                tag="knot2M")
-        tuned = {"leaf_size": res["leaf"], "total_ms_by_leaf_size": res["total_ms"], **res["sets"]}
+        tuned = {"leaf_size": res["leaf"], "total_ms_by_leaf_size": res["total_ms"],
+                 **{n: {"best": e["best"], "ms": e["ms"]} for n, e in res["sets"].items()}}
         set_configs = [res["sets"][n]["best"] for n, _ in sets]
     if args.leaf_size is not None:
         bvh.set_leaf_size(args.leaf_size)
@@ -358,6 +421,9 @@ def run_engine(args, ws, rank, local):
                   for k in range(len(sets))]
     value = weak_scaling_rate(ws, n_step, args.steps, ms)
 
+    # the timed run's hits, kept for the parity check against the oracle
+    got = [np.frombuffer(d.cpu().numpy().tobytes(), dtype=pkg.HIT_DTYPE) for d in d_out]
+
     # e2e through the public API with pinned host buffers (copies inside the timed region)
     pinned_in = [torch.from_numpy(r).pin_memory() for _, r in sets]
     pinned_out = [torch.empty((r.shape[0] * 32,), dtype=torch.uint8).pin_memory() for _, r in sets]
@@ -378,15 +444,30 @@ def run_engine(args, ws, rank, local):
         e2e_step()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) / e2e_steps * 1e3, ws, dev)
     e2e = {"value": weak_scaling_rate(ws, n_step, 1, e2e_ms), "unit": UNIT,
-           "h2d_bytes_per_step": n_step * BYTES_RAY_IN, "d2h_bytes_per_step": n_step * BYTES_HIT_OUT}
+           "h2d_bytes_per_step": n_step * BYTES_RAY_IN, "d2h_bytes_per_step": n_step * BYTES_HIT_OUT,
+           "same_bytes_as_device_run": all(np.array_equal(h.view(np.uint8), g.view(np.uint8))
+                                           for h, g in zip(host_out, got))}
+    del pinned_in, pinned_out, host_in, host_out
 
-    cpu = None
-    roof = None
+    cpu = roof = parity = None
     if rank == 0 and not args.no_cpu_baseline:
+        import oracle.oracle as orc
+
         threads = os.cpu_count() or 1
-        rate, stats, nsample = cpu_reference(pkg, bvh, geo, [r for _, r in sets], args.cpu_sample // 2, threads)
+        ref = orc.OracleBVH.from_serialized(bvh._roots, geo.index, bvh._indirectBuffer, geo.position)
+        rate, stats, nsample, per_set = cpu_reference(ref, sets, got, args.cpu_sample // 2, threads)
         cpu = {"value": rate / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{nsample} rays ({args.cpu_sample // 2} evenly strided from each set), float64 oracle"}
+               "sample": (f"{nsample} rays: both whole sets" if nsample == n_step else
+                          f"{nsample} rays in contiguous 65536-ray blocks spread over both sets") + ", float64 oracle"}
+        keys = parity_module().FIRST_KEYS
+        parity = {"rays_checked": int(sum(r["rays"] for r in per_set.values())),
+                  "mismatches": {k: int(sum(r[k] for r in per_set.values())) for k in keys},
+                  "tie_exempt": int(sum(r["exempt"] for r in per_set.values())),
+                  "per_set": per_set,
+                  "bar": "hit/miss and faceIndex identical except rays whose two nearest reference hits are "
+                         "within 1e-6 t; distance within 1e-5 relative; point and barycoord within "
+                         "1e-5 max(1, |ref|)"}
+        parity["ok"] = not any(parity["mismatches"].values())
         bytes_per_launch = []
         for (name, rays), (mn, mt) in zip(sets, stats):
             bytes_per_launch.append(rays.shape[0] * (BYTES_RAY_IN + BYTES_HIT_OUT + BYTES_NODE * mn + BYTES_TRI * mt))
@@ -402,27 +483,71 @@ def run_engine(args, ws, rank, local):
                 "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], map(float, bytes_per_launch))),
                 "reference_node_reads_per_ray": [s[0] for s in stats],
                 "reference_triangle_tests_per_ray": [s[1] for s in stats]}
+        del ref
+    del got
+    line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "triangles": geo.triangle_count, "rays_per_step": n_step,
-                           "node_records": info["node_records"], "max_depth": info["max_depth"],
-                           "l2": "inputs larger than L2 (805 MB of rays + 1.07 GB of hits per step)",
-                           "parallelism": f"replicas x{ws}"},
+                "config": headline_config(geo.triangle_count, n_step, ws),
+                "mesh": {"node_records": info["node_records"], "max_depth": info["max_depth"]},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "per_set_mrays_s": {n: r.shape[0] / (t / 1e3) / 1e6 for (n, r), t in zip(sets, per_set_ms)},
                 "traversal": {n: (list(c) if c is not None else None) for (n, _), c in zip(sets, set_configs)},
                 "leaf_size": bvh.get_leaf_size(),
-                "autotune": tuned, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "autotune": tuned, "roofline": roof, "cpu_baseline": cpu, "parity": parity, "e2e": e2e,
+                "clocks": clk.summary(),
                 "gpu_launches": args.steps * sum(kernel_launches(c) for c in set_configs)}
-        print(json.dumps(line), flush=True)
     bvh.dispose()
+    del d_rays, d_out
+    torch.cuda.empty_cache()
+    # the metric's other two parts, measured in the same run: the batched BatchedMesh launch
+    # against per-mesh launches, and forward+backward against forward
+    if not args.headline_only:
+        line_b = measure_batched(args, ws, rank, local)
+        torch.cuda.empty_cache()
+        line_a = measure_adjoint(args, ws, rank, local)
+        torch.cuda.empty_cache()
+        if rank == 0:
+            line["batched"] = line_b
+            line["adjoint"] = line_a
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
-def run_batched(args, ws, rank, local):
+def batched_oracle_check(batch, rays, off, got, per_geometry, threads):
+    """Each geometry's hits against its own oracle (the reference's per-mesh raycast with the
+    geometry's draw range, ExtensionUtilities.js:87-161,216-268): an evenly strided sample of up to
+    `per_geometry` of its rays.  `got` holds faceIndex in the shared index."""
+    import oracle.oracle as orc
+
+    from three_mesh_bvh_b200.batched import shift_triangle_offsets
+
+    par_mod = parity_module()
+    tot, r0 = {}, 0
+    for k in range(batch.n_meshes):
+        nr = batch.roots_per_mesh[k]
+        tb = int(batch.triangle_base[k])
+        roots = [shift_triangle_offsets(r, (-tb) & 0xFFFFFFFF) for r in batch.roots[r0:r0 + nr]]
+        r0 += nr
+        g = batch.geometries[k]
+        ref = orc.OracleBVH.from_serialized(roots, g.index, None, g.position)
+        a, b = int(off[k]), int(off[k + 1])
+        ii = np.linspace(a, b - 1, min(per_geometry, b - a)).astype(np.int64)
+        sub = np.ascontiguousarray(rays[ii])
+        gk = got[ii].copy()
+        hit = gk["face_index"] != 0xFFFFFFFF
+        gk["face_index"][hit] -= np.uint32(tb)
+        exp = ref.raycast_first(sub, threads=threads)
+        par_mod.add_counts(tot, par_mod.first_parity_chunk(ref, sub, gk, exp, threads=threads))
+    return tot
+
+
+def measure_batched(args, ws, rank, local):
     """BatchedMesh form (1024 sub-geometries, log-uniform 200..200,000 triangles and 1,000..1,000,000
-    rays each): one graph-captured persistent launch versus one plain launch per geometry."""
+    rays each): one graph-captured persistent launch versus one plain launch per geometry; returns
+    the result dict on rank 0."""
     import torch
 
     import __graft_entry__ as ge
@@ -432,6 +557,7 @@ def run_batched(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    t_setup = time.perf_counter()
     geoms, _, rays, off = pkg.batched_scene(n_geometries=args.batch_meshes, seed=2)
     batch = BatchedMeshBVH(geoms, {"strategy": pkg.SAH, "maxLeafSize": 10}, threads=os.cpu_count())
     n = rays.shape[0]
@@ -439,6 +565,7 @@ def run_batched(args, ws, rank, local):
     out = torch.empty((n, 8), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     s = stream.cuda_stream
+    t_setup = time.perf_counter() - t_setup
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -465,37 +592,56 @@ def run_batched(args, ws, rank, local):
     batch.set_traversal(*best)
     graph = batch.capture(d_rays, off, out)
     with ClockSampler(local) as clk:
-        ms_graph = timed(lambda: graph.launch(s), args.steps, args.warmup)
+        ms_graph = max_over_ranks(timed(lambda: graph.launch(s), args.steps, args.warmup), ws, dev)
     batch.synchronize(s)
     ref_out = out.clone()
     # per-geometry launches: plain one-ray-per-thread kernel (same child order), and persistent
     batch.set_traversal(0, best[1], 16, 0)
-    ms_plain = timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s), max(1, args.steps // 2), 1)
+    ms_plain = max_over_ranks(timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s),
+                                    max(1, args.steps // 2), 1), ws, dev)
     batch.synchronize(s)
     same_plain = bool(torch.equal(out.view(torch.int32)[:, 0], ref_out.view(torch.int32)[:, 0]))
     batch.set_traversal(*best)
-    ms_pers = timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s), max(1, args.steps // 2), 1)
+    ms_pers = max_over_ranks(timed(lambda: batch.raycast_first_per_mesh(d_rays, off, out=out, stream=s),
+                                   max(1, args.steps // 2), 1), ws, dev)
     batch.synchronize(s)
+    res = None
     if rank == 0:
-        line = {"metric": "Mrays/s batched raycastFirst (1024 meshes)", "value": n / (ms_graph / 1e3) / 1e6,
-                "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_graph,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic",
-                "config": {"workload": f"{args.batch_meshes} geometries alternating TorusKnot / Icosahedron, "
-                                       "triangles log-uniform 200..200000, rays log-uniform 1e3..1e6 per geometry "
-                                       "(seed 2), SAH leaf 10; one CUDA-graph persistent launch",
-                           "triangles": int(batch.triangle_base[-1]), "rays_per_step": int(n)},
-                "per_mesh_plain_launches": {"ms": ms_plain, "mrays_s": n / (ms_plain / 1e3) / 1e6,
-                                            "same_face_indices": same_plain},
-                "per_mesh_persistent_launches": {"ms": ms_pers, "mrays_s": n / (ms_pers / 1e3) / 1e6},
-                "speedup_vs_per_mesh_plain": ms_plain / ms_graph, "traversal": list(best),
-                "autotune_ms": timings, "clocks": clk.summary(),
-                "gpu_launches": args.steps * kernel_launches(best),
+        par = None
+        if not args.no_cpu_baseline:
+            got = np.frombuffer(ref_out.cpu().numpy().tobytes(), dtype=pkg.HIT_DTYPE)
+            per = 256
+            tot = batched_oracle_check(batch, rays, off, got, per, os.cpu_count() or 1)
+            keys = parity_module().FIRST_KEYS
+            par = {"rays_checked": tot["rays"], "per_geometry": f"up to {per} evenly strided rays of each geometry",
+                   "mismatches": {k: tot[k] for k in keys}, "tie_exempt": tot["exempt"],
+                   "ok": not any(tot[k] for k in keys)}
+        res = {"metric": "Mrays/s batched raycastFirst (1024 meshes)", "value": n / (ms_graph / 1e3) / 1e6,
+               "unit": UNIT, "ms_per_step": ms_graph, "steps": args.steps, "warmup": args.warmup,
+               "config": {"workload": f"{args.batch_meshes} geometries alternating TorusKnot / Icosahedron, "
+                                      "triangles log-uniform 200..200000, rays log-uniform 1e3..1e6 per geometry "
+                                      "(seed 2), SAH leaf 10; one CUDA-graph persistent launch",
+                          "triangles": int(batch.triangle_base[-1]), "rays_per_step": int(n)},
+               "per_mesh_plain_launches": {"ms": ms_plain, "mrays_s": n / (ms_plain / 1e3) / 1e6,
+                                           "same_face_indices": same_plain},
+               "per_mesh_persistent_launches": {"ms": ms_pers, "mrays_s": n / (ms_pers / 1e3) / 1e6},
+               "speedup_vs_per_mesh_plain": ms_plain / ms_graph, "same_face_indices": same_plain,
+               "parity": par, "traversal": list(best), "autotune_ms": timings, "clocks": clk.summary(),
+               "setup_s": t_setup, "gpu_launches": args.steps * kernel_launches(best)}
+    graph.destroy()
+    batch.dispose()
+    del d_rays, out, ref_out
+    return res
+
+
+def run_batched(args, ws, rank, local):
+    res = measure_batched(args, ws, rank, local)
+    if rank == 0:
+        line = {**res, "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
                 "e2e": None, "e2e_note": "not measured: the rays and hits of all 1024 geometries (~1.5e8 rays) "
                                          "would need ~8.4 GB of page-locked host memory"}
         print(json.dumps(line), flush=True)
-    graph.destroy()
-    batch.dispose()
 
 
 def run_closest(args, ws, rank, local):
@@ -685,10 +831,11 @@ def run_all_hits(args, ws, rank, local):
     bvh.dispose()
 
 
-def run_adjoint(args, ws, rank, local):
+def measure_adjoint(args, ws, rank, local):
     """Differentiable depth and SDF on the 2M-triangle knot: forward raycastFirst of a 1024^2 camera
     and backward of L = sum (t - t*)^2 (t* rendered from the mesh with vertices moved by N(0, 0.01),
-    seed 3); forward closestPointToPoint of a 128^3 grid and backward of sum distance."""
+    seed 3); forward closestPointToPoint of a 128^3 grid and backward of sum distance.  Returns the
+    result dict on rank 0."""
     import torch
 
     import __graft_entry__ as ge
@@ -759,24 +906,32 @@ def run_adjoint(args, ws, rank, local):
         ms_cf, ms_cfb = timed(cp_fwd), timed(cp_fwd_bwd)
         ms_refit = timed(refit)
     bvh.synchronize(s)
+    ms_f, ms_fb, ms_cf, ms_cfb = (max_over_ranks(x, ws, dev) for x in (ms_f, ms_fb, ms_cf, ms_cfb))
+    res = None
     if rank == 0:
-        line = {"metric": "fwd+bwd / fwd time, raycastFirst depth loss (2M tri, 1024^2 camera)",
-                "value": ms_fb / ms_f, "unit": "ratio", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": ms_fb, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "TorusKnot(10,3,2000,500) + N(0,0.02) noise, SAH leaf 10; 1024^2 camera; "
-                                       "L = sum (t - t*)^2, t* from vertices + N(0,0.01) (seed 3); "
-                                       "128^3 grid closest point, max 5, L = sum distance"},
-                "raycast": {"fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f},
-                "closest_point": {"fwd_ms": ms_cf, "fwd_bwd_ms": ms_cfb, "ratio": ms_cfb / ms_cf},
-                "forward_variants": {"raycast": tuned_ray["sets"]["camera1024"]["best"],
-                                     "leaf_size": tuned_ray["leaf"], "closest": tuned_cp["best"]},
-                "refit_ms": ms_refit,
-                "clocks": clk.summary(),
-                "e2e": None, "e2e_note": "the metric is a ratio of device times (backward over forward)"}
-        print(json.dumps(line), flush=True)
+        res = {"metric": "fwd+bwd / fwd time, raycastFirst depth loss (2M tri, 1024^2 camera)",
+               "value": ms_fb / ms_f, "ratio": ms_fb / ms_f, "unit": "ratio", "ms_per_step": ms_fb,
+               "steps": args.steps, "warmup": args.warmup, "target": "<= 2.5",
+               "config": {"workload": "TorusKnot(10,3,2000,500) + N(0,0.02) noise, SAH leaf 10; 1024^2 camera; "
+                                      "L = sum (t - t*)^2, t* from vertices + N(0,0.01) (seed 3); "
+                                      "128^3 grid closest point, max 5, L = sum distance"},
+               "raycast": {"fwd_ms": ms_f, "fwd_bwd_ms": ms_fb, "ratio": ms_fb / ms_f},
+               "closest_point": {"fwd_ms": ms_cf, "fwd_bwd_ms": ms_cfb, "ratio": ms_cfb / ms_cf},
+               "forward_variants": {"raycast": tuned_ray["sets"]["camera1024"]["best"],
+                                    "leaf_size": tuned_ray["leaf"], "closest": tuned_cp["best"]},
+               "refit_ms": ms_refit, "clocks": clk.summary()}
     bvh.dispose()
     bvh_star.dispose()
+    return res
+
+
+def run_adjoint(args, ws, rank, local):
+    res = measure_adjoint(args, ws, rank, local)
+    if rank == 0:
+        line = {**res, "n_gpus": ws, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "e2e": None, "e2e_note": "the metric is a ratio of device times (backward over forward)"}
+        print(json.dumps(line), flush=True)
 
 
 def run_scene(args, ws, rank, local):

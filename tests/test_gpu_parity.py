@@ -378,26 +378,16 @@ def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
     torch.cuda.synchronize()
     dev = d.cpu().numpy().view(np.uint8).reshape(-1)
     dev = np.frombuffer(dev.tobytes(), dtype=host.dtype)
-    assert np.array_equal(host["face_index"] == 0xFFFFFFFF, dev["face_index"] == 0xFFFFFFFF)
-    hit = host["face_index"] != 0xFFFFFFFF
+    # byte-identical: exact distance ties go to the earlier triangle in leaf order whatever the
+    # grouping of the queries (chunks, Morton sort per chunk or over the whole call)
+    assert np.array_equal(host.view(np.uint8), dev.view(np.uint8))
+
     def tri_distance(p):
         def f(i, face):
             q = orc.closest_point_triangle(p[i].astype(np.float64), *geo.triangle(face))
             return float(np.linalg.norm(q - p[i].astype(np.float64)))
         return f
 
-    # faces agree except between triangles at the same distance (a point nearest to a shared vertex
-    # or edge; the sorted form groups queries per chunk, so a warp's shared order, which picks among
-    # tied triangles, can differ from the one-call run's)
-    dh, dd = host["distance"][hit].astype(np.float64), dev["distance"][hit].astype(np.float64)
-    assert (np.abs(dh - dd) <= 1e-6 * np.maximum(1.0, np.abs(dd))).all()
-    diff = np.nonzero(hit & (host["face_index"] != dev["face_index"]))[0]
-    if closest == 0:
-        assert diff.size == 0
-    dist = tri_distance(pts)
-    for i in diff[:: max(1, diff.size // 2000)]:
-        a, b = dist(i, int(host["face_index"][i])), dist(i, int(dev["face_index"][i]))
-        assert abs(a - b) <= 1e-5 * max(1.0, b), (i, a, b)
     idx = np.arange(0, pts.shape[0], 97)
     exp = ref.closest_point(pts[idx], 0.0, 5.0)
 

@@ -870,11 +870,14 @@ __device__ __forceinline__ CPBest cp_none() {
   return b;
 }
 
-// Offers triangle record k to the query at p (the reference's strict `<` on distSq).  Returns the
-// candidate's float32 squared distance and bound, and its float-float value when one was needed.
+// Offers triangle record k to the query at p: a strictly smaller squared distance replaces the
+// best (the reference's strict `<` on distSq), and an exact tie goes to the earlier record in
+// leaf order (the reference keeps whichever its own traversal reached first; a fixed rule keeps
+// the answer independent of how queries are grouped).  Returns the candidate's float32 squared
+// distance and bound, and its float-float value when one was needed.
 // With `cull`, a triangle whose bounding box is already farther than the best candidate is
-// passed over without its closest point: its distance exceeds the best one, so the reference's
-// strict `<` would not take it (callers that test minThreshold on every triangle pass false).
+// passed over without its closest point: its distance exceeds the best one, so it cannot win
+// (callers that test minThreshold on every triangle pass false).
 __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
                                          float& err, bool& have_ff, ff& cand_ff, bool cull = false) {
   if (cull && b.rec != 0xFFFFFFFFu) {
@@ -909,14 +912,13 @@ __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& 
   } else if (d2 - err > b.d2 + b.err) {
     take = false;
   } else if (is_vertex && b.vertex && q.x == b.q.x && q.y == b.q.y && q.z == b.q.z) {
-    take = false;  // the same vertex: an exact tie, the first one found stays
-  } else if (err + b.err <= 2e-6f * b.d2) {
-    // the two true distances are within 1e-6 relative of each other (typically the same edge or
-    // vertex reached from two triangles): either answer meets the distance tolerance and the
-    // winner's distance is recomputed in float-float, so the first one found stays, as the
-    // reference's strict `<` keeps it on a tie
-    take = false;
+    take = k < b.rec;  // the same vertex: an exact tie, the earlier record in leaf order wins
   } else {
+    // Undecided in float32: the float-float squared distances decide, and an exact tie goes to
+    // the earlier record in leaf order.  Candidates are thus ranked by a total order that does
+    // not depend on the order they are offered in, and every box that could hold a candidate at
+    // the best distance is entered (box tests keep a relative slack), so the answer is the same
+    // for any traversal order: per query, warp-shared, sorted or chunked.
     if (!b.ff_ok) {
       Tri bt = load_tri(m.tris, b.rec);
       b.ffv = closest_ff(p, bt.a, bt.b, bt.c).d2;
@@ -924,7 +926,7 @@ __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& 
     }
     cand_ff = closest_ff(p, t.a, t.b, t.c).d2;
     have_ff = true;
-    take = ff_lt(cand_ff, b.ffv);
+    take = ff_lt(cand_ff, b.ffv) || (!ff_lt(b.ffv, cand_ff) && k < b.rec);
   }
   if (take) {
     b.d2 = d2;

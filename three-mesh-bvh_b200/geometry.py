@@ -13,6 +13,8 @@ vertex positions: three.js is not available here, and nothing on the query path 
 from __future__ import annotations
 
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -180,13 +182,16 @@ def icosahedron(radius=1.0, detail=0) -> Geometry:
     ii, jj = ii[keep], jj[keep]
     lid = -np.ones((n + 1, n + 1), dtype=np.int64)
     lid[ii, jj] = np.arange(ii.size)
-    small = []
-    for i in range(n):
-        for j in range(n - i):
-            small.append((lid[i, j], lid[i + 1, j], lid[i, j + 1]))
-            if i + j + 1 < n:
-                small.append((lid[i + 1, j], lid[i + 1, j + 1], lid[i, j + 1]))
-    small = np.array(small)
+    # lattice cells (i, j), i + j < n, row by row: the upward triangle, then the downward one
+    # where it exists (i + j + 1 < n)
+    ci, cj = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    cell = ci + cj < n
+    ci, cj = ci[cell], cj[cell]
+    up = np.stack([lid[ci, cj], lid[ci + 1, cj], lid[ci, cj + 1]], -1)
+    has_down = ci + cj + 1 < n
+    dn_i, dn_j = np.minimum(ci + 1, n), np.minimum(cj + 1, n)
+    down = np.stack([lid[dn_i, cj], lid[dn_i, dn_j], lid[ci, dn_j]], -1)
+    small = np.stack([up, down], 1)[np.stack([np.ones_like(has_down), has_down], 1)]
     pos, idx = [], []
     for k, (a, b, c) in enumerate(f):
         pts = v[a][None] + (ii[:, None] / n) * (v[b] - v[a])[None] + (jj[:, None] / n) * (v[c] - v[a])[None]
@@ -300,16 +305,17 @@ def batched_scene(n_geometries=1024, tri_range=(200, 200_000), ray_range=(1_000,
     lo_r, hi_r = ray_range
     tri_target = np.exp(rng.uniform(math.log(lo_t), math.log(hi_t), n_geometries))
     ray_counts = np.exp(rng.uniform(math.log(lo_r), math.log(hi_r), n_geometries)).astype(np.int64)
-    geoms = []
-    for k in range(n_geometries):
+    def make(k):
         t = float(tri_target[k])
         if k % 2 == 0:
             radial = max(3, int(round(math.sqrt(t / 8))))
             tubular = max(3, int(round(t / (2 * radial))))
-            geoms.append(torus_knot(10, 3, tubular, radial))
-        else:
-            detail = max(0, int(round(math.sqrt(t / 20))) - 1)
-            geoms.append(icosahedron(10.0, detail))
+            return torus_knot(10, 3, tubular, radial)
+        detail = max(0, int(round(math.sqrt(t / 20))) - 1)
+        return icosahedron(10.0, detail)
+
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        geoms = list(ex.map(make, range(n_geometries)))
     transforms = np.zeros((n_geometries, 4, 4))
     for k in range(n_geometries):
         q = rng.normal(size=4)
@@ -325,6 +331,10 @@ def batched_scene(n_geometries=1024, tri_range=(200, 200_000), ray_range=(1_000,
     rays = None
     if make_rays:
         rays = np.empty((int(offsets[-1]), 6), dtype=np.float32)
-        for k in range(n_geometries):
+
+        def fill(k):   # each geometry's rays come from their own seed, so threads may fill them
             rays[int(offsets[k]):int(offsets[k + 1])] = rays_sphere_to_box(int(ray_counts[k]), seed=10_000 + k)
+
+        with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+            list(ex.map(fill, range(n_geometries)))
     return geoms, transforms, rays, offsets
