@@ -379,9 +379,11 @@ def run_engine(args, ws, rank, local):
         # tuned on the whole sets: ray ordering and the warp-cooperative form depend on a set's
         # coherence at full size, which no strided or block sample reproduces; one device leaf
         # layout serves both sets
+        # the camera's rays come one per pixel in row-major order: its width is the tiled order's
+        # row pitch, as a renderer would pass it
         res = autotune.tune_raycast_first_sets(bvh, [(n, d) for (n, _), d in zip(sets, d_rays)],
                                                leaf_sizes=[int(x) for x in args.leaf_sizes.split(",")],
-                                               tag="knot2M")
+                                               tag="knot2M", tile_pitches=(args.camera,))
         tuned = {"leaf_size": res["leaf"], "total_ms_by_leaf_size": res["total_ms"],
                  **{n: {"best": e["best"], "ms": e["ms"]} for n, e in res["sets"].items()}}
         set_configs = [res["sets"][n]["best"] for n, _ in sets]
@@ -580,10 +582,10 @@ def measure_batched(args, ws, rank, local):
         return a.elapsed_time(b) / steps
 
     # autotune the batched launch over the traversal variants
-    from three_mesh_bvh_b200.autotune import CANDIDATES
+    from three_mesh_bvh_b200 import autotune
 
     # (the batched launch always runs the persistent form; ray ordering applies to single meshes)
-    cands = [c for c in CANDIDATES if c[0] == 1 and c[5] == 0]
+    cands = [c for c in autotune.candidates() if c[0] == 1 and c[5] == 0]
     timings = {}
     for cand in cands:
         batch.set_traversal(*cand)
@@ -861,7 +863,8 @@ def measure_adjoint(args, ws, rank, local):
     # has no variants)
     from three_mesh_bvh_b200 import autotune
 
-    tuned_ray = autotune.tune_raycast_first_sets(bvh, [("camera1024", rays)], leaf_sizes=(0, 2, 4), tag="adjoint")
+    tuned_ray = autotune.tune_raycast_first_sets(bvh, [("camera1024", rays)], leaf_sizes=(0, 2, 4), tag="adjoint",
+                                                 tile_pitches=(1024,))
     bvh.set_traversal(*tuned_ray["sets"]["camera1024"]["best"])
     tuned_cp = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
 

@@ -170,8 +170,14 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * (the direction, the entry point, the entry point and the direction), 5 one ray per thread over
  * the rays that enter the tree (the others get a zero count), 6, 7 and 8 the same sorted by key
  * sort = all - 5, 9 to 12 the same walked by persistent warps that refill idle lanes (10 to 12
- * sorted by key all - 9).  Results are the same for every variant (up to exact ties); the
- * autotuner picks the fastest per mesh and workload. */
+ * sorted by key all - 9).  tile (warp-cooperative raycastFirst without compaction or ordering):
+ * 0 gives each warp 32 consecutive rays; a multiple of 8 (at most 2^24) reads the rays as rows of
+ * `tile` rays and gives each warp a tile of 4 rows x 8 rays, for rays generated per pixel of a
+ * row-major image of that width (the ray-sort granularity without a sort).  block: threads per
+ * block of the warp-cooperative raycastFirst (64, 128 or 256; 0 = 128).  stack: traversal stack
+ * entries of the warp-cooperative and persistent raycastFirst (32 or 64; 0 = 64); 32 applies to
+ * trees of depth 30 or less and 64 runs otherwise.  Results are the same for every variant (up to
+ * exact ties); the autotuner picks the fastest per mesh and workload. */
 typedef struct bvhc_traversal_config {
   int32_t persistent;
   int32_t order;
@@ -182,9 +188,35 @@ typedef struct bvhc_traversal_config {
   int32_t closest;
   int32_t wide;
   int32_t all;
+  int32_t tile;
+  int32_t block;
+  int32_t stack;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);
+
+/* raycastFirst autotuner (no reference counterpart: the reference has one recursive traversal;
+ * its only traversal knobs are the build's maxDepth / maxLeafSize, src/core/Constants.js:74-85,
+ * and the shader stack depth, src/webgl/glsl/bvh_ray_functions.glsl.js:14-16).  Times the
+ * traversal variants with CUDA events on `stream` over the caller's ray sets (device memory,
+ * n_sets sets of counts[k] rays) and installs the fastest.  Stage 1: every candidate (one ray per
+ * thread; warp-cooperative over child pairs or four-child records; persistent warps; with and
+ * without the root-box compaction and each ordering key; register budgets; the tiled ray order for
+ * each row pitch in tile_pitches, e.g. an image width) for every device leaf layout in leaf_sizes
+ * (NULL / 0: the current one); the layout with the smallest sum of the sets' best times wins.
+ * Stage 2: threads per block and the 32-entry stack around each set's best.  Each variant is run
+ * once untimed, then `reps` times.  Outputs: best[k] and best_ms[k] per set (best_ms nullable),
+ * the chosen layout (nullable) and each layout's total (leaf_total_ms[n_leaf_sizes], nullable).
+ * The mesh is left with the chosen layout and set 0's variant; callers switch variants per set
+ * with bvhc_mesh_set_traversal.  Waits for the device; allocates a hit buffer for the largest set. */
+bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const float* const* rays, const uint64_t* counts, int side,
+                               float near_dist, float far_dist, const int32_t* leaf_sizes, int n_leaf_sizes,
+                               const int32_t* tile_pitches, int n_tile_pitches, int reps, void* stream,
+                               bvhc_traversal_config* best, float* best_ms, int32_t* leaf_size_out,
+                               float* leaf_total_ms);
+/* bvhc_mesh_autotune's stage-1 candidates for these row pitches, in the order it times them: the
+ * first min(count, cap) are written to out; returns the count (-1 for invalid arguments). */
+int bvhc_autotune_candidates(const int32_t* tile_pitches, int n_tile_pitches, bvhc_traversal_config* out, int cap);
 
 /* Device leaf layout of raycastFirst (no reference counterpart; the reference's own leaves are
  * maxLeafSize-bounded, buildTree.js:64-89): max_leaf > 0 gives raycastFirst (single, material,
@@ -329,7 +361,9 @@ bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind);
  *   - device-memory calls are not size-limited;
  *   - all calls share the array: calls that overlap on the GPU (other streams or threads) race;
  *   - the first call on a device looks the array up on that device: make it before any stream
- *     capture. */
+ *     capture.  A cudaDeviceReset ends the context the address belongs to (and every mesh made on
+ *     the device before it); the next call on that device, with a mesh made after the reset, looks
+ *     the array up again and is a set-up call in the same sense. */
 bvhc_status bvhc_raycast_first_noalloc(bvhc_mesh* mesh, const float* rays, uint64_t n, int side, float near_dist,
                                        float far_dist, bvhc_hit* out, int mem, void* stream);
 

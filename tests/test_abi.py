@@ -114,3 +114,33 @@ def test_invalid_arguments(pkg, knot):
     assert lib.bvhc_mesh_create(0, 1, None, None, 0, None, 0, 0, None, 0, 0, None, 0, 3, C.byref(out)) == 1
     assert lib.bvhc_raycast_first(None, None, 1, 0, 0.0, 1.0, None, 0, None) == 1
     assert lib.bvhc_build(None, 0, 3, None, 0, 0, None, 0, 0, -1, 2, 40, 10, 0, C.byref(out)) == 1
+
+
+def test_autotune_candidates_and_argument_checks(pkg):
+    """bvhc_autotune_candidates lists the autotuner's stage-1 variants without a GPU; the autotuner
+    itself rejects bad arguments before touching the device."""
+    from three_mesh_bvh_b200 import _native as N
+    from three_mesh_bvh_b200 import autotune
+
+    lib = pkg.lib()
+    base = autotune.candidates()
+    assert len(base) == 87 and len({tuple(c) for c in base}) == 87
+    fields = autotune.FIELDS
+    assert fields[:6] == ["persistent", "order", "refill", "occupancy", "compact", "sort"]
+    assert fields[9:] == ["tile", "block", "stack"]
+    forms = {c[0] for c in base}
+    assert forms == {0, 1, 2}
+    assert any(c[7] == 1 for c in base)                                    # four-child records
+    assert {(c[4], c[5]) for c in base if c[0] == 1} == {(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)}
+    tiled = autotune.candidates((4096, 1920))
+    assert tiled[:87] == base and len(tiled) == 87 + 12
+    assert {c[9] for c in tiled[87:]} == {4096, 1920} and all(c[0] == 2 and c[4] == 0 for c in tiled[87:])
+    with pytest.raises(ValueError):
+        autotune.candidates((-8,))
+    assert lib.bvhc_autotune_candidates(None, 1, None, 0) == -1
+    best = (N.BvhcTraversalConfig * 1)()
+    counts = (C.c_uint64 * 1)(16)
+    rays = (C.c_void_p * 1)(None)
+    assert lib.bvhc_mesh_autotune(None, 1, rays, counts, 0, 0.0, 1.0, None, 0, None, 0, 3, None, best, None, None,
+                                  None) == 1                                  # BVHC_ERR_INVALID_ARGUMENT
+

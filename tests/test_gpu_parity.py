@@ -223,7 +223,8 @@ def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occ
     ref = _oracle_for(orc, bvh, geo)
     bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
-                                       compact=compact, sort=sort, closest=0, wide=0, all=0)
+                                       compact=compact, sort=sort, closest=0, wide=0, all=0, tile=0,
+                                       block=0, stack=0)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -394,3 +395,17 @@ def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
     rep = check_closest(host[idx], exp, tri_distance(pts[idx]))
     assert rep["null"] == 0 and rep["face"] == 0 and rep["distance"] == 0, rep
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
+
+
+def test_traversal_config_rejects_bad_fields(pkg, cuda):
+    """Tile pitches that are not a positive multiple of 8, block sizes other than 64 / 128 / 256 and
+    stacks other than 32 / 64 are rejected."""
+    geo = pkg.torus_knot(10, 3, 32, 8)
+    bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
+    for bad in (dict(tile=12), dict(tile=-8), dict(block=96), dict(stack=48), dict(stack=16)):
+        with pytest.raises(pkg.BVHCError):
+            bvh.set_traversal(2, 1, 16, 0, **bad)
+    bvh.set_traversal(2, 1, 16, 2, tile=4096, block=256, stack=32)
+    assert bvh.get_traversal() == dict(persistent=2, order=1, refill=16, occupancy=2, compact=0, sort=0, closest=0,
+                                       wide=0, all=0, tile=4096, block=256, stack=32)
+    bvh.dispose()

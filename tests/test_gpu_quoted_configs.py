@@ -91,14 +91,28 @@ def _first_sample(bvh, d, stride):
     return _rows(out.index_select(0, idx), HIT)
 
 
+def _stage2(cands):
+    """The autotuner's stage-2 forms of its stage-1 candidates: threads per block 64 / 256 for the
+    warp-cooperative form over child pairs, and the 32-entry stack for it and the persistent form."""
+    out = []
+    for c in cands:
+        if c[0] == 2 and not c[7]:
+            out += [c[:10] + [64, 0], c[:10] + [256, 32], c[:10] + [0, 32]]
+        elif c[0] == 1:
+            out.append(c[:10] + [0, 32])
+    return out
+
+
 @pytest.mark.parametrize("leaf", [0, 2, 4])
 def test_knot2m_first_hit_every_variant(knot2m, leaf):
-    from three_mesh_bvh_b200.autotune import CANDIDATES
+    from three_mesh_bvh_b200 import autotune
 
     geo, bvh, ref, sets, dev, samples, stride = knot2m
     bvh.set_leaf_size(leaf)
+    cands = autotune.candidates(tile_pitches=(4096, 2048))
+    cands += _stage2([c for c in cands if c[3] == 2])
     bad = {}
-    for cand in CANDIDATES:
+    for cand in cands:
         bvh.set_traversal(*cand)
         for name, d in dev.items():
             rep = samples[name].check(_first_sample(bvh, d, stride))
@@ -116,7 +130,8 @@ def test_knot2m_first_hit_tuned_whole_sets(knot2m):
     from three_mesh_bvh_b200 import autotune
 
     geo, bvh, ref, sets, dev, samples, stride = knot2m
-    res = autotune.tune_raycast_first_sets(bvh, list(dev.items()), leaf_sizes=[0, 2, 4], tag="parity-knot2M")
+    res = autotune.tune_raycast_first_sets(bvh, list(dev.items()), leaf_sizes=[0, 2, 4], tag="parity-knot2M",
+                                           tile_pitches=(4096,))
     for name, d in dev.items():
         bvh.set_traversal(*res["sets"][name]["best"])
         got = _rows(bvh.raycast_first_batch(d), HIT)
@@ -186,7 +201,7 @@ def knot80k_full(pkg, orc, cuda):
 def test_knot80k_million_rays_every_variant(knot80k_full, cuda):
     import torch
 
-    from three_mesh_bvh_b200.autotune import CANDIDATES
+    from three_mesh_bvh_b200 import autotune
 
     geo, bvh, ref = knot80k_full
     rays = __import__("__graft_entry__").load_package().rays_sphere_to_box(1_000_000, seed=0)
@@ -196,7 +211,9 @@ def test_knot80k_million_rays_every_variant(knot80k_full, cuda):
     bad = {}
     for leaf in (0, 2, 4):
         bvh.set_leaf_size(leaf)
-        for cand in CANDIDATES:
+        # tiled orders of any row pitch (a multiple of 8) are permutations: still every ray's own hit
+        cands = autotune.candidates(tile_pitches=(8, 1000, 4096))
+        for cand in cands + _stage2(cands):
             bvh.set_traversal(*cand)
             got = _rows(bvh.raycast_first_batch(d), HIT)
             bvh.synchronize()

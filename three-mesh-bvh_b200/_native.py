@@ -33,7 +33,8 @@ class BvhcHitPointInfo(C.Structure):
 class BvhcTraversalConfig(C.Structure):
     _fields_ = [("persistent", C.c_int32), ("order", C.c_int32), ("refill", C.c_int32), ("occupancy", C.c_int32),
                 ("compact", C.c_int32), ("sort", C.c_int32), ("closest", C.c_int32),
-                ("wide", C.c_int32), ("all", C.c_int32)]
+                ("wide", C.c_int32), ("all", C.c_int32), ("tile", C.c_int32),
+                ("block", C.c_int32), ("stack", C.c_int32)]
 
 
 class BvhcMeshInfo(C.Structure):
@@ -92,6 +93,9 @@ SIGNATURES = [
     ("bvhc_triangle_hit_point_info", _I, [_P, _P, _P, _U64, _P, _I, _P, _I, _U64, _P, _I, _P, _I, _P]),
     ("bvhc_raycast_first_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, _P, _I, _P]),
     ("bvhc_raycast_materials", _I, [_P, _P, _U64, _P, _I, _F, _F, C.c_uint32, _P, _P, _I, _P]),
+    ("bvhc_mesh_autotune", _I, [_P, _I, _P, _P, _I, _F, _F, _P, _I, _P, _I, _I, _P, C.POINTER(BvhcTraversalConfig),
+                                _P, _P, _P]),
+    ("bvhc_autotune_candidates", _I, [_P, _I, C.POINTER(BvhcTraversalConfig), _I]),
 ]
 
 _lib = None

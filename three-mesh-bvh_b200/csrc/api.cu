@@ -28,7 +28,7 @@ struct bvhc_mesh {
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
   unsigned long long* d_work_all = nullptr;  // work counter of the persistent raycast (all hits) kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
@@ -108,10 +108,15 @@ struct bvhc_mesh {
     MeshDev v = leaf_size ? MeshDev{d_nodes_f, d_tris_f, d_roots_f, n_roots, d_err} : view();
     v.quads = d_quads;
     v.quad_roots = d_quad_roots;
+    v.depth = leaf_size ? max_depth_f : max_depth;
     return v;
   }
 
-  MeshDev view() const { return MeshDev{d_nodes, d_tris, d_roots, n_roots, d_err}; }
+  MeshDev view() const {
+    MeshDev v{d_nodes, d_tris, d_roots, n_roots, d_err};
+    v.depth = max_depth;
+    return v;
+  }
 };
 
 namespace {
@@ -1043,8 +1048,8 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
     cudaError_t e = queue_for(m, qslot, n, &q, &qc, &sort, &sorted);
     if (e != cudaSuccess) return e;
     if (m->cfg.persistent == 2)
-      return launch_raycast_first_packet(m->view_first(), rays, n, side, tab, near_d, far_d, out, m->cfg.order,
-                                         m->cfg.occupancy, m->cfg.wide, s, q, qc, sorted ? &sort : nullptr);
+      return launch_raycast_first_packet(m->view_first(), rays, n, side, tab, near_d, far_d, out, m->cfg, s, q, qc,
+                                         sorted ? &sort : nullptr);
     return launch_raycast_first_persistent(m->view_first(), nullptr, rays, n, side, tab, near_d, far_d, out, work,
                                            m->cfg, s, q, qc, sorted ? &sort : nullptr);
   }
@@ -1055,8 +1060,7 @@ static cudaError_t dispatch_first(bvhc_mesh* m, const float* rays, uint64_t n, i
 static cudaError_t dispatch_view(bvhc_mesh* m, const MeshDev& v, const float* rays, uint64_t n, int side,
                                  float near_d, float far_d, bvhc_hit* out, cudaStream_t s) {
   if (m->cfg.persistent == 2)
-    return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg.order,
-                                       m->cfg.occupancy, m->cfg.wide, s);
+    return launch_raycast_first_packet(v, rays, n, side, single_side(), near_d, far_d, out, m->cfg, s);
   if (m->cfg.persistent) {
     uint32_t* q;
     unsigned int* qc;
@@ -1098,13 +1102,16 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12;
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
+         (cfg->tile == 0 || (cfg->tile >= 8 && cfg->tile <= (1 << 24) && cfg->tile % 8 == 0)) &&
+         (cfg->block == 0 || cfg->block == 64 || cfg->block == 128 || cfg->block == 256) &&
+         (cfg->stack == 0 || cfg->stack == 32 || cfg->stack == 64);
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill,  cfg->occupancy,
-                           cfg->compact,    cfg->sort,  cfg->closest, cfg->wide,     cfg->all};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact, cfg->sort,
+                           cfg->closest,    cfg->wide,  cfg->all,    cfg->tile,      cfg->block,   cfg->stack};
   return BVHC_OK;
 }
 
@@ -1242,6 +1249,9 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->closest = m->cfg.closest;
   cfg->wide = m->cfg.wide;
   cfg->all = m->cfg.all;
+  cfg->tile = m->cfg.tile;
+  cfg->block = m->cfg.block;
+  cfg->stack = m->cfg.stack;
   return BVHC_OK;
 }
 

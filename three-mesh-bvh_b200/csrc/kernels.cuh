@@ -24,6 +24,7 @@ struct MeshDev {
   unsigned int* err;
   const QuadNode* quads = nullptr;     // four-child copy of `nodes` (same triangle records), if any
   const uint32_t* quad_roots = nullptr;
+  int depth = kMaxStack - 2;           // deepest node level of these records (bounds the stack use)
 };
 
 cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
@@ -46,6 +47,11 @@ struct TraversalConfig {
                    // over the rays that enter the tree, sorted by key kind all - 1, 5..8 one ray per
                    // thread over the rays that enter the tree (6..8 sorted by key kind all - 5), 9..12
                    // the same with persistent warps and lane refill (10..12 sorted by key all - 9)
+  int tile;        // warp-cooperative raycastFirst without a queue: 0 consecutive rays per warp; a
+                   // multiple of 8 takes 4 x 8 tiles of the rays read as rows of `tile` rays
+  int block;       // warp-cooperative raycastFirst threads per block: 64, 256, else 128
+  int stack;       // raycastFirst traversal stack entries (warp-cooperative and persistent forms): 32
+                   // when the tree allows it, else 64
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -92,8 +98,8 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
 // queue, the same pre-pass (and sort) as the persistent form runs first.
 // wide = 1 with m.quads set runs over the four-child records.
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
-                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out, int order,
-                                        int occupancy, int wide, cudaStream_t stream, uint32_t* queue = nullptr,
+                                        const SideTable& sides, float near_d, float far_d, bvhc_hit* out,
+                                        const TraversalConfig& cfg, cudaStream_t stream, uint32_t* queue = nullptr,
                                         unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
 // closestPointToPoint.  variant 0: one query per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the queries sorted by a Morton key of the point (queue, qcount and sort

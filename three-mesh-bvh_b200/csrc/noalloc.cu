@@ -18,7 +18,11 @@
 //     so no stale value is read -- but two calls that overlap on the GPU (different streams, or
 //     different host threads) race on the array and must not be issued;
 //   * the first call on each device looks up the array's device address (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture.
+//     that device current; make that first call before any stream capture.  The address belongs to
+//     the device's context: a cudaDeviceReset ends it (and every mesh made on that device before),
+//     so each call compares the current context's id with the one the address was looked up in and
+//     looks it up again in a new context.  The first call after a reset is then a set-up call too.
+#include <cuda.h>  // driver types only: the two context queries are fetched at run time
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -40,17 +44,48 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // id of the context the address belongs to
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the current context (unique within the process; a device reset makes a new context and
+// so a new id); 0 when there is no current context yet or the driver cannot tell.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 // Device address of g_noalloc_scratch on `device` (which must be current).  In host code the
-// array's name is only a stand-in for the symbol, so the address is looked up once per device.
+// array's name is only a stand-in for the symbol, so the address is looked up once per device and
+// context, and again after the device's context was replaced (cudaDeviceReset).
 cudaError_t scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[device]) {
+  unsigned long long ctx = current_context_id();
+  if (!g_scratch_addr[device] || (ctx != 0 && ctx != g_scratch_ctx[device])) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_addr[device] = static_cast<unsigned char*>(p);
+    g_scratch_ctx[device] = current_context_id();   // the look-up made the context current if it was not
   }
   *out = g_scratch_addr[device];
   return cudaSuccess;
