@@ -239,7 +239,14 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 // minThreshold > 0 the reference stops at the first triangle below it in its own order, which a
 // shared order would not reproduce; those calls use the per-query kernel.)
 // ---------------------------------------------------------------------------------------------
-template <int MINB>
+//
+// SEED: before the shared walk, every lane descends on its own from each root to one leaf, always
+// into the nearer child whose score is under maxThreshold^2, and offers that leaf's triangles.  The
+// leaf's box score is under maxThreshold^2, so the reference reaches a leaf there and those
+// triangles are among the candidates it compares; the answer, a minimum under an order that does
+// not depend on the visiting order, is unchanged, while each lane starts the shared walk with a
+// real best distance and so wants far fewer nodes.
+template <int MINB, bool SEED>
 __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
     MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
     const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
@@ -257,6 +264,30 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   const ff max2 = two_prod(max_t, max_t);
   const float kNo = __int_as_float(0x7FFFFFFF);  // NaN: "this lane does not want the entry"
   CPBest b = cp_none();
+  if (SEED && valid) {
+    for (int root = 0; root < m.n_roots; ++root) {
+      uint32_t link = m.roots[root];
+      while (!(link & kLeafBit)) {
+        Pair pr = load_pair(m.nodes, link);
+        float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
+        bool w0 = under_max(s0, pr.l, p, max2), w1 = under_max(s1, pr.r, p, max2);
+        if (!w0 && !w1) break;
+        link = w0 && (!w1 || s0 <= s1) ? pr.ll : pr.lr;
+      }
+      if ((link & kLeafBit) && link != kEmptyLeaf) {
+        uint32_t k = link & ~kLeafBit;
+        for (;;) {
+          Tri t = load_tri(m.tris, k);
+          float d2, err;
+          bool have_ff;
+          ff cand_ff;
+          cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff, true);
+          if (t.flags & kTriLast) break;
+          ++k;
+        }
+      }
+    }
+  }
   float lane_s[kMaxStack];
   bool overflow = false;
   for (int root = 0; root < m.n_roots && !overflow; ++root) {
@@ -1140,13 +1171,15 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
                                  unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  // the warp-cooperative form needs minThreshold 0 (see closest_point_packet_kernel)
-  if (variant == 0 || !(min_t <= 0.0f) || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
+  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 1 and 2 run
+  // the shared walk, 3 and 4 seed it with each lane's own greedy leaf; 2 and 4 over sorted queries
+  const bool sorted = variant == 2 || variant == 4, seed = variant >= 3;
+  if (variant == 0 || !(min_t <= 0.0f) || (sorted && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
     dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
     return cudaGetLastError();
   }
   cudaError_t e;
-  if (variant == 2) {
+  if (sorted) {
     uint32_t *ids, *keys;
     ray_sort_input(2, sort->scratch, queue, &ids, &keys);
     dev::SceneBox box{};
@@ -1161,9 +1194,12 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
     queue = nullptr;
     qcount = nullptr;
   }
-  auto kernel = occupancy == 0   ? dev::closest_point_packet_kernel<1>
-                : occupancy == 1 ? dev::closest_point_packet_kernel<6>
-                                 : dev::closest_point_packet_kernel<8>;
+  auto kernel = seed ? (occupancy == 0   ? dev::closest_point_packet_kernel<1, true>
+                        : occupancy == 1 ? dev::closest_point_packet_kernel<6, true>
+                                         : dev::closest_point_packet_kernel<8, true>)
+                     : (occupancy == 0   ? dev::closest_point_packet_kernel<1, false>
+                        : occupancy == 1 ? dev::closest_point_packet_kernel<6, false>
+                                         : dev::closest_point_packet_kernel<8, false>);
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
   return cudaGetLastError();
 }
