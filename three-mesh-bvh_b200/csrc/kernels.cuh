@@ -146,6 +146,7 @@ struct SceneDev {
   uint32_t root;
   const InstanceDev* inst;
   const uint32_t* mesh_root_off;
+  int n_instances = 1 << 30;   // bounds the instance tree's depth (a median split)
 };
 // World-space raycastFirst over the instances: hits[i] in world space (distance, point; local
 // barycoord and faceIndex), instance[i] the hit instance (0xFFFFFFFF: none).  With `sort` (kind

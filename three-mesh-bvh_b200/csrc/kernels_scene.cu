@@ -42,10 +42,11 @@ __device__ __forceinline__ ff row_apply(const float* hi, const float* lo, int ro
 // The per-thread raycastFirst walk of one geometry's roots, nearest child first, in "while-while"
 // form (each lane descends internal nodes until it holds a leaf, then the lanes holding one test
 // their triangles together).  Returns false on a stack overflow.
+template <int STACK>
 __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const RayF& r, float dlen, int side,
                            const SideTable& sides, float near_d, float far_d, Best& best) {
-  uint32_t stack_link[kMaxStack];
-  float stack_t[kMaxStack];
+  uint32_t stack_link[STACK];
+  float stack_t[STACK];
   for (uint32_t root = r0; root < r1; ++root) {
     uint32_t link = m.roots[root];
     int sp = 0;
@@ -62,7 +63,7 @@ __device__ bool blas_first(const MeshDev& m, uint32_t r0, uint32_t r1, const Ray
         const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
         if (h1st) {
           if (h2nd) {
-            if (sp >= kMaxStack) return false;
+            if (sp >= STACK) return false;
             stack_link[sp] = c2;
             stack_t[sp] = lf ? e1 : e0;
             ++sp;
@@ -189,13 +190,15 @@ __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, 
 // thread i takes ray queue[i] (rays ordered by a Morton key, so that a warp's rays share paths)
 // and writes that ray's row.
 // Instance-tree stack: the tree is a median split (bvhc_scene_set_instances), so its depth is at most
-// log2 of the instance count, below 32 for any instance count the ABI takes; half the geometry
-// trees' kMaxStack keeps the per-thread frame (and its spill traffic at high occupancy) smaller.
+// ceil(log2) of the instance count: TSTACK = 16 serves up to 2^16 instances, 32 any count the ABI
+// takes.  BSTACK (the geometry trees' walk) is 32 when every geometry tree is at most 30 deep, else
+// 64.  Smaller stacks keep the per-thread frame (and its spill traffic at high occupancy) smaller.
 constexpr int kTlasStack = 32;
 
 // 14 resident blocks per SM (36 registers, some spilled): the kernel stalls on fetching its own
 // large body and on its scattered loads, and more resident warps hide both; the instanced bench
 // measured 35.6 / 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks.
+template <int TSTACK, int BSTACK>
 __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
                                                                         const float* __restrict__ rays, uint64_t n,
                                                                         const uint32_t* __restrict__ queue, int side,
@@ -211,8 +214,8 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
   bvhc_hit best_hit;
   ff best_dist = ff_from(kInf);
   uint32_t best_inst = 0xFFFFFFFFu;
-  uint32_t stack_link[kTlasStack];
-  float stack_t[kTlasStack];
+  uint32_t stack_link[TSTACK];
+  float stack_t[TSTACK];
   int sp = 0;
   uint32_t link = sc.root;
   bool go = link != kEmptyLeaf;
@@ -231,7 +234,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
       const bool h1st = lf ? h0 : h1, h2nd = lf ? h1 : h0;
       if (h1st) {
         if (h2nd) {
-          if (sp >= kTlasStack) {
+          if (sp >= TSTACK) {
             atomicOr(m.err, kErrStackOverflow);
             go = false;
             break;
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
         const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * L.vlen / wlen * (1.0f + 0x1p-16f);
         Best b{kInf, 0.0f, 0xFFFFFFFFu};
         const uint32_t g = I.geometry;
-        if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
+        if (!blas_first<BSTACK>(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
                         fminf(L.far_d, tlim), b)) {
           atomicOr(m.err, kErrStackOverflow);
           break;
@@ -498,8 +501,11 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
     if (e != cudaSuccess) return e;
     if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
   }
-  dev::scene_raycast_first_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(
-      blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d, hits, instance);
+  const bool t16 = scene.n_instances <= (1 << 16), b32 = stack_entries(blas, 32) == 32;
+  auto kernel = t16 ? (b32 ? dev::scene_raycast_first_kernel<16, 32> : dev::scene_raycast_first_kernel<16, 64>)
+                    : (b32 ? dev::scene_raycast_first_kernel<32, 32> : dev::scene_raycast_first_kernel<32, 64>);
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d,
+                                                  hits, instance);
   return cudaGetLastError();
 }
 
