@@ -244,6 +244,17 @@ def kernel_launches(cfg):
     return n
 
 
+def all_hits_launches(variant):
+    """Kernels one raycast (all hits) call launches: the traversal, plus for the queue variants the
+    root-box pre-pass and, when the queue is sorted, 3 kernels per radix pass (4 passes for the
+    direction key, 3 for the others)."""
+    if variant in (0, 1, "1t"):
+        return 1
+    v = int(variant)
+    kind = {2: 1, 3: 2, 4: 3, 6: 1, 7: 2, 8: 3, 10: 1, 11: 2, 12: 3}.get(v, 0)
+    return 2 + (3 * (4 if kind == 1 else 3) if kind else 0)
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -764,9 +775,12 @@ def run_all_hits(args, ws, rank, local):
                                        counts.data_ptr(), hits.data_ptr(), 1, stream.cuda_stream), "bvhc_raycast")
 
             # the all-hits kernel variant for this set (one call each, on the same buffers)
-            t_var = {}
-            for v in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12):
-                bvh.set_traversal(**{**cur, "all": v})
+            # the all-hits kernels, and the warp-cooperative one in tiled order with the camera's
+            # row pitch ("1t")
+            t_var, settings = {}, {v: {"all": v} for v in range(13)}
+            settings["1t"] = {"all": 1, "tile": args.camera}
+            for v, kw in settings.items():
+                bvh.set_traversal(**{**cur, **kw})
                 call()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
@@ -775,7 +789,7 @@ def run_all_hits(args, ws, rank, local):
                 e1.synchronize()
                 t_var[v] = e0.elapsed_time(e1)
             best = min(t_var, key=t_var.get)
-            bvh.set_traversal(**{**cur, "all": best})
+            bvh.set_traversal(**{**cur, **settings[best]})
             variants[name] = {"best": best, "timings_ms": {str(k): x for k, x in t_var.items()}}
             for _ in range(args.warmup):
                 call()
@@ -815,7 +829,12 @@ def run_all_hits(args, ws, rank, local):
         achieved = bytes_per_set[k] / (per_set_ms[k] / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "peak_source": how, "ray_set": sets[k][0],
-                "kernel": "raycast_all_kernel" if variants[sets[k][0]]["best"] == 0 else "raycast_all_packet_kernel",
+                "kernel": {0: "raycast_all_kernel", 1: "raycast_all_packet_kernel", "1t": "raycast_all_packet_kernel",
+                           2: "raycast_all_packet_kernel", 3: "raycast_all_packet_kernel",
+                           4: "raycast_all_packet_kernel"}.get(variants[sets[k][0]]["best"],
+                                                              "raycast_all_persistent_kernel"
+                                                              if str(variants[sets[k][0]]["best"]) in
+                                                              ("9", "10", "11", "12") else "raycast_all_kernel"),
                 "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], bytes_per_set))}
     if rank == 0:
         line = {"metric": "Mrays/s raycast all hits (2M tri, cap 64)", "value": weak_scaling_rate(ws, n_step, 1, ms),
@@ -826,7 +845,7 @@ def run_all_hits(args, ws, rank, local):
                            "rays_per_step": n_step, "stored_hits": dict(zip([n for n, _ in sets], stored))},
                 "per_set_ms": dict(zip([n for n, _ in sets], per_set_ms)),
                 "all_hits_variant": variants, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "gpu_launches": args.steps * sum(15 if v["best"] == 2 else 1 for v in variants.values()),
+                "gpu_launches": args.steps * sum(all_hits_launches(v["best"]) for v in variants.values()),
                 "e2e": None, "e2e_note": "not measured: the hit rows (2^24 rays x 64 hits x 32 B per set) are "
                                          "34 GB, more than page-locked host memory should hold"}
         print(json.dumps(line), flush=True)

@@ -174,7 +174,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * sorted by key all - 9).  tile (warp-cooperative raycastFirst without compaction or ordering):
  * 0 gives each warp 32 consecutive rays; a multiple of 8 (at most 2^24) reads the rays as rows of
  * `tile` rays and gives each warp a tile of 4 rows x 8 rays, for rays generated per pixel of a
- * row-major image of that width (the ray-sort granularity without a sort).  block: threads per
+ * row-major image of that width (the ray-sort granularity without a sort); it applies to raycast's
+ * warp-cooperative kernel (all = 1) too.  block: threads per
  * block of the warp-cooperative raycastFirst (64, 128 or 256; 0 = 128).  stack: traversal stack
  * entries of the warp-cooperative and persistent raycastFirst (32 or 64; 0 = 64); 32 applies to
  * trees of depth 30 or less and 64 runs otherwise.  Results are the same for every variant (up to

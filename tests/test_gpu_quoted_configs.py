@@ -162,7 +162,7 @@ def knot2m_all_rows(knot2m):
     return rows
 
 
-@pytest.mark.parametrize("variant", list(range(13)))
+@pytest.mark.parametrize("variant", list(range(13)) + ["1t"])
 def test_knot2m_all_hits_every_variant(knot2m, knot2m_all_rows, cuda, variant):
     """Cap 64 (no ray of these sets has more front-face hits) and cap 2 (rays with more hits than
     the cap keep the first two of the reference's order)."""
@@ -170,7 +170,10 @@ def test_knot2m_all_hits_every_variant(knot2m, knot2m_all_rows, cuda, variant):
 
     geo, bvh, ref, sets, dev, samples, stride = knot2m
     bvh.set_leaf_size(0)
-    bvh.set_traversal(1, 1, 16, 2, 0, 0, 0, 0, variant)
+    if variant == "1t":   # the warp-cooperative kernel in tiled order (the camera's row pitch)
+        bvh.set_traversal(1, 1, 16, 2, 0, 0, 0, 0, 1, 4096)
+    else:
+        bvh.set_traversal(1, 1, 16, 2, 0, 0, 0, 0, variant)
     for name, d in dev.items():
         ec, eh = knot2m_all_rows[name]
         idx = torch.arange(0, d.shape[0], 64, device=cuda)

@@ -1355,14 +1355,16 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   }
   if (mem == BVHC_MEM_DEVICE)
     return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s, variant,
-                                        m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all));
+                                        m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all,
+                                        (uint32_t)m->cfg.tile));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
   BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
                                    static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s, variant,
-                                   m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all));
+                                   m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all,
+                                   (uint32_t)m->cfg.tile));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));

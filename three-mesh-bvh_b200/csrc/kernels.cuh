@@ -114,12 +114,13 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
 // warp-cooperative over the rays sorted by the key sort->kind (queue, qcount and sort scratch for
 // n rays required, else variant 0 runs); 5: one ray per thread over the rays the root-box pre-pass
 // queues (queue and qcount for n rays required; sorted by sort->kind when given); 9: the same
-// queue walked by persistent warps with lane refill (also a zeroed-per-call work counter).
+// queue walked by persistent warps with lane refill (also a zeroed-per-call work counter).  `tile`
+// (variant 1): the warp-cooperative walk takes 4 x 8 tiles of rays read as rows of `tile` rays.
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream, int variant = 0, int occupancy = 0, uint32_t* queue = nullptr,
                                unsigned int* qcount = nullptr, const RaySort* sort = nullptr,
-                               unsigned long long* work = nullptr);
+                               unsigned long long* work = nullptr, uint32_t tile = 0);
 
 // intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
 // sphere i.

@@ -246,6 +246,19 @@ __device__ __forceinline__ bool left_first(const Pair& p, const RayF& r, float e
 }
 
 
+// Tiled ray order: the ray index space read as rows of `pitch` rays (pitch a multiple of 8), cut
+// into bands of 4 rows; work item i of a band is the ray at row (i mod 32) / 8, column
+// 8 (i / 32) + i mod 8 of that band, so each warp takes a 4 x 8 tile.  For rays generated per pixel
+// in row-major order with pitch = the image width, that is a 4 x 8 pixel block.  Items past the
+// last whole band keep their own index.  A bijection of [0, n): for i below the last whole band
+// the row is at most 3 and the column at most pitch - 1, so the ray stays in i's band.
+__device__ __forceinline__ uint64_t tiled_index(uint64_t i, uint64_t pitch, uint64_t n) {
+  const uint64_t band = 4 * pitch;
+  if (i >= n - n % band) return i;
+  const uint64_t b = i / band, r = i - b * band;
+  return b * band + ((r & 31u) >> 3) * pitch + ((r >> 5) << 3) + (r & 7u);
+}
+
 // Pre-pass tiles (classify_kernel, kernels_first.cu).
 constexpr int kClsThreads = 256;
 constexpr int kClsItems = 8;
