@@ -263,13 +263,18 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profile_traffic(name):
-    """dram bytes per launch recorded from an ncu capture in profiles/<name> (None if absent)."""
+def profile_value(name, key):
+    """A `key: value` figure recorded from an ncu capture in profiles/<name> (None if absent)."""
     p = ROOT / "profiles" / name
     if not p.exists():
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    m = re.search(key + r":\s*([0-9.eE+-]+)", p.read_text())
     return float(m.group(1)) if m else None
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture in profiles/<name> (None if absent)."""
+    return profile_value(name, "traffic_bytes_per_launch")
 
 
 def parity_module():
@@ -496,6 +501,13 @@ def run_engine(args, ws, rank, local):
                 "algorithmic_bytes_per_launch": dict(zip([n for n, _ in sets], map(float, bytes_per_launch))),
                 "reference_node_reads_per_ray": [s[0] for s in stats],
                 "reference_triangle_tests_per_ray": [s[1] for s in stats]}
+        # the scene is L2-resident, so the HBM fraction saturates; the kernel is issue-bound, and
+        # the ncu capture of the same kernel gives the figures that bound it
+        prof = f"raycast_first_k2_{sets[k][0]}.md"
+        roof["issue"] = {"source": f"profiles/{prof}",
+                         "warp_instructions_per_ray": profile_value(prof, "warp_instructions_per_ray"),
+                         "issue_slots_active": profile_value(prof, "issue_slots_active"),
+                         "threads_per_instruction": profile_value(prof, "threads_per_instruction")}
         del ref
     del got
     line = None

@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
   const RayF w = make_ray(rays, i);
   const float wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
   const SideTable no_sides{};
-  bvhc_hit best_hit;
+  // the best world record so far lives in the ray's output row (rewritten when a closer instance
+  // hit is found, a few times per ray at most), not in the thread's frame
   ff best_dist = ff_from(kInf);
   uint32_t best_inst = 0xFFFFFFFFu;
   uint32_t stack_link[TSTACK];
@@ -280,7 +281,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
           if (ff_lt(dist, best_dist) || (!ff_lt(best_dist, dist) && j < best_inst)) {
             best_dist = dist;
             best_inst = j;
-            best_hit = h;
+            store_hit(out + i, h);
           }
         }
       }
@@ -296,11 +297,7 @@ __global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev
       }
     }
   }
-  if (best_inst == 0xFFFFFFFFu) {
-    store_miss(out + i);
-  } else {
-    store_hit(out + i, best_hit);
-  }
+  if (best_inst == 0xFFFFFFFFu) store_miss(out + i);
   inst_out[i] = best_inst;
 }
 
