@@ -50,6 +50,8 @@ def parse():
                          "(all hits); build: the device SAH build; scene: instanced BatchedMesh raycastFirst; "
                          "shapecast: triangles within spheres, intersectsSphere, intersectsBox")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
+    ap.add_argument("--closest-variant", type=int, default=None,
+                    help="closest workload: force closestPointToPoint's kernel (0..4) instead of tuning")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
     ap.add_argument("--radial", type=int, default=500)
@@ -691,7 +693,11 @@ def run_closest(args, ws, rank, local):
     from three_mesh_bvh_b200 import autotune
 
     bvh.set_traversal(1, 1, 16, 2)   # register budget shared with the warp-cooperative kernels
-    tuned = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
+    if args.closest_variant is not None:
+        bvh.set_traversal(1, 1, 16, 2, closest=args.closest_variant)
+        tuned = {"best": args.closest_variant, "forced": True}
+    else:
+        tuned = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
 
     def step():
         lib.bvhc_closest_point_to_point(bvh._device_mesh(), pts.data_ptr(), n, 0.0, 5.0, out.data_ptr(), 1, s)
@@ -739,6 +745,11 @@ def run_closest(args, ws, rank, local):
                 "reference_node_reads_per_query": float(nn.mean()),
                 "reference_triangle_tests_per_query": float(nt.mean()),
                 "kernel": "closest_point_kernel" if tuned["best"] == 0 else "closest_point_packet_kernel"}
+        prof = "closest_point_k3.md"
+        roof["issue"] = {"source": f"profiles/{prof}",
+                         "warp_instructions_per_query": profile_value(prof, "warp_instructions_per_query"),
+                         "issue_slots_active": profile_value(prof, "issue_slots_active"),
+                         "threads_per_instruction": profile_value(prof, "threads_per_instruction")}
     if rank == 0:
         line = {"metric": "Mqueries/s closestPointToPoint (80k tri, 256^3 grid)",
                 "value": weak_scaling_rate(ws, n, 1, ms), "unit": "Mqueries/s", "n_gpus": ws, "steps": args.steps,
@@ -749,7 +760,7 @@ def run_closest(args, ws, rank, local):
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
                         "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
-                "gpu_launches": args.steps * (14 if tuned["best"] == 2 else 1)}
+                "gpu_launches": args.steps * (11 if tuned["best"] in (2, 4) else 1)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 
