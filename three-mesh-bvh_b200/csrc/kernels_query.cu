@@ -26,6 +26,19 @@ __device__ __forceinline__ float box_score(const float* b, float3 p) {
   return dx * dx + dy * dy + dz * dz;
 }
 
+// Squared distance from p to the box's centre: the visiting order's tie-break when both child
+// boxes hold p (both scores 0), which the scores alone cannot order.
+__device__ __forceinline__ float centre_d2(const float* b, float3 p) {
+  const float dx = 0.5f * (b[0] + b[3]) - p.x, dy = 0.5f * (b[1] + b[4]) - p.y, dz = 0.5f * (b[2] + b[5]) - p.z;
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// Whether the right child should be visited first: the smaller score, equal scores by the nearer
+// centre (the warp-cooperative and seeded forms; the per-query kernel keeps the reference's order).
+__device__ __forceinline__ bool right_nearer(const Pair& pr, float s0, float s1, float3 p) {
+  return s1 < s0 || (s1 == s0 && centre_d2(pr.r, p) < centre_d2(pr.l, p));
+}
+
 __device__ __noinline__ ff box_score_ff(const float* b, float3 p) {
   ff dx = two_diff(fmaxf(b[0], fminf(b[3], p.x)), p.x);
   ff dy = two_diff(fmaxf(b[1], fminf(b[4], p.y)), p.y);
@@ -272,7 +285,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
         bool w0 = under_max(s0, pr.l, p, max2), w1 = under_max(s1, pr.r, p, max2);
         if (!w0 && !w1) break;
-        link = w0 && (!w1 || s0 <= s1) ? pr.ll : pr.lr;
+        link = w0 && (!w1 || !right_nearer(pr, s0, s1, p)) ? pr.ll : pr.lr;
       }
       if ((link & kLeafBit) && link != kEmptyLeaf) {
         uint32_t k = link & ~kLeafBit;
@@ -319,7 +332,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         unsigned b0 = __ballot_sync(full, w0), b1 = __ballot_sync(full, w1);
         if (b0 && b1) {
           // nearer child first by majority of the lanes that want both (a lane wanting one prefers it)
-          bool pref_right = (w0 && w1) ? s1 < s0 : w1;
+          bool pref_right = (w0 && w1) ? right_nearer(pr, s0, s1, p) : w1;
           unsigned voters = __ballot_sync(full, w0 || w1);
           bool right_first = 2 * __popc(__ballot_sync(full, (w0 || w1) && pref_right)) > __popc(voters);
           if (sp >= kMaxStack) {
