@@ -335,7 +335,9 @@ bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const u
  * back to world space with its distance from the ray origin (convertRaycastIntersect,
  * src/utils/GeometryRayIntersectUtilities.js:3-17), and the closest of them (equal distances
  * keep the lower instance).  hits: world distance and point, the geometry's faceIndex and local
- * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none. */
+ * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none.
+ * The batch's traversal `occupancy` (bvhc_mesh_set_traversal on the batch) sets the kernel's
+ * resident blocks per SM: 0 fourteen, 1 ten, 2 eight. */
 bvhc_status bvhc_scene_raycast_first(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
                                      float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream);
 /* The same without firstHitOnly (the BatchedMesh raycast, then the raycaster's sort): every hit of

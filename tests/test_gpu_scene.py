@@ -71,13 +71,19 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
     bad = _compare(got, ginst, exp, einst)
     assert not bad, bad[:10]
     assert (einst >= 0).mean() > 0.2
-    # device buffers, and every ray order, give the same records
-    for order in (0, 1, 2, 3, 4):
-        scene.set_order(order)
-        dh, di = scene.raycast_first(torch.from_numpy(rays).to(cuda))
-        torch.cuda.synchronize()
-        assert np.array_equal(di.cpu().numpy().view(np.uint32), ginst), order
-        assert np.array_equal(dh.cpu().numpy().view(np.uint8).reshape(-1), got.view(np.uint8).reshape(-1)), order
+    # device buffers, every ray order and every register budget (resident blocks per SM) give the
+    # same records
+    for occ in (0, 1, 2):
+        batch.set_traversal(1, 1, 16, occ)
+        for order in (0, 1, 2, 3, 4):
+            scene.set_order(order)
+            dh, di = scene.raycast_first(torch.from_numpy(rays).to(cuda))
+            torch.cuda.synchronize()
+            assert np.array_equal(di.cpu().numpy().view(np.uint32), ginst), (occ, order)
+            assert np.array_equal(dh.cpu().numpy().view(np.uint8).reshape(-1), got.view(np.uint8).reshape(-1)), (
+                occ, order)
+    batch.set_traversal(1, 1, 16, 0)
+    scene.set_order(0)
     scene.dispose()
 
 

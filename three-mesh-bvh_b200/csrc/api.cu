@@ -2034,6 +2034,7 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
   sd.n_instances = sc->n_instances;
+  sd.occupancy = m->cfg.occupancy;
   if (mem == BVHC_MEM_HOST && n > kPipeChunk) {
     // Large host batches: chunks of kPipeChunk rays rotate over the batch mesh's three pipeline
     // streams and staging slots (instance ids in a slot of the scene's own), so the copies of some
@@ -2117,6 +2118,7 @@ bvhc_status bvhc_scene_raycast(bvhc_scene* sc, const float* rays, uint64_t n, in
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
   sd.n_instances = sc->n_instances;
+  sd.occupancy = m->cfg.occupancy;
   const uint32_t c = cap > 0 ? cap : 1;  // cap 0: counts only (one scratch slot per ray)
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && (!aligned(hits, 16) || !aligned(instance, 4))))

@@ -84,7 +84,7 @@ __device__ __forceinline__ CPBest cp_none() {
 // With `cull`, a triangle whose bounding box is already farther than the best candidate is
 // passed over without its closest point: its distance exceeds the best one, so it cannot win
 // (callers that test minThreshold on every triangle pass false).
-__device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
+__device__ __noinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
                                          float& err, bool& have_ff, ff& cand_ff, bool cull = false) {
   if (cull && b.rec != 0xFFFFFFFFu) {
     // squared distance to the triangle's box: at most 4 roundings above the exact value's

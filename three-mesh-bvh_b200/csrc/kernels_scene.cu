@@ -195,11 +195,12 @@ __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, 
 // 64.  Smaller stacks keep the per-thread frame (and its spill traffic at high occupancy) smaller.
 constexpr int kTlasStack = 32;
 
-// 14 resident blocks per SM (36 registers, some spilled): the kernel stalls on fetching its own
-// large body and on its scattered loads, and more resident warps hide both; the instanced bench
-// measured 35.6 / 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks.
-template <int TSTACK, int BSTACK>
-__global__ void __launch_bounds__(kBlock, 14) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
+// MINB resident blocks per SM (14: 32 registers, some spilled): the kernel stalls on fetching its
+// own large body and on its scattered loads, and more resident warps hide both, while fewer
+// registers spill more to local memory; the instanced bench tunes 14 / 10 / 8 (it measured 35.6 /
+// 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks with 64-entry stacks).
+template <int TSTACK, int BSTACK, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
                                                                         const float* __restrict__ rays, uint64_t n,
                                                                         const uint32_t* __restrict__ queue, int side,
                                                                         float near_d, float far_d,
@@ -498,9 +499,16 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
     if (e != cudaSuccess) return e;
     if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
   }
-  const bool t16 = scene.n_instances <= (1 << 16), b32 = stack_entries(blas, 32) == 32;
-  auto kernel = t16 ? (b32 ? dev::scene_raycast_first_kernel<16, 32> : dev::scene_raycast_first_kernel<16, 64>)
-                    : (b32 ? dev::scene_raycast_first_kernel<32, 32> : dev::scene_raycast_first_kernel<32, 64>);
+  // the small stacks when both trees allow them, else the large ones; resident blocks per SM by
+  // the batch's occupancy setting (0: 14, 1: 10, 2: 8)
+  const bool small = scene.n_instances <= (1 << 16) && stack_entries(blas, 32) == 32;
+  const int occ = scene.occupancy;
+  auto kernel = small ? (occ == 1   ? dev::scene_raycast_first_kernel<16, 32, 10>
+                         : occ == 2 ? dev::scene_raycast_first_kernel<16, 32, 8>
+                                    : dev::scene_raycast_first_kernel<16, 32, 14>)
+                      : (occ == 1   ? dev::scene_raycast_first_kernel<32, 64, 10>
+                         : occ == 2 ? dev::scene_raycast_first_kernel<32, 64, 8>
+                                    : dev::scene_raycast_first_kernel<32, 64, 14>);
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d,
                                                   hits, instance);
   return cudaGetLastError();
