@@ -34,7 +34,7 @@ __device__ __forceinline__ float centre_d2(const float* b, float3 p) {
 }
 
 // Whether the right child should be visited first: the smaller score, equal scores by the nearer
-// centre (the warp-cooperative and seeded forms; the per-query kernel keeps the reference's order).
+// centre (the warp-cooperative forms; the per-query kernel keeps the reference's order).
 __device__ __forceinline__ bool right_nearer(const Pair& pr, float s0, float s1, float3 p) {
   return s1 < s0 || (s1 == s0 && centre_d2(pr.r, p) < centre_d2(pr.l, p));
 }
@@ -84,7 +84,7 @@ __device__ __forceinline__ CPBest cp_none() {
 // With `cull`, a triangle whose bounding box is already farther than the best candidate is
 // passed over without its closest point: its distance exceeds the best one, so it cannot win
 // (callers that test minThreshold on every triangle pass false).
-__device__ __noinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
+__device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& t, uint32_t k, CPBest& b, float& d2,
                                          float& err, bool& have_ff, ff& cand_ff, bool cull = false) {
   if (cull && b.rec != 0xFFFFFFFFu) {
     // squared distance to the triangle's box: at most 4 roundings above the exact value's
@@ -253,13 +253,16 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 // shared order would not reproduce; those calls use the per-query kernel.)
 // ---------------------------------------------------------------------------------------------
 //
-// SEED: before the shared walk, every lane descends on its own from each root to one leaf, always
-// into the nearer child whose score is under maxThreshold^2, and offers that leaf's triangles.  The
-// leaf's box score is under maxThreshold^2, so the reference reaches a leaf there and those
-// triangles are among the candidates it compares; the answer, a minimum under an order that does
-// not depend on the visiting order, is unchanged, while each lane starts the shared walk with a
-// real best distance and so wants far fewer nodes.
-template <int MINB, bool SEED>
+// SHARE: the lanes also prune with a bound taken from the warp's best candidates.  With p0 the
+// first lane's point, any lane j's candidate c_j gives lane i the bound
+// |p_i - c_j| <= d_j + |p_i - p0| + |p0 - p_j|, so lane i's distance is at most
+// B_i = min_j d_j + r_i + max_j r_j (r = |p - p0|, each term rounded up).  A box whose score is
+// above B_i^2 cannot hold lane i's answer, so skipping it changes nothing; and when B_i is below
+// maxThreshold the lane still reaches the leaf of its nearest triangle (its score is at most
+// B_i^2 and under maxThreshold^2), so "null iff no leaf is reached" is kept.  For grid queries
+// (a warp's points a few cells apart) lanes that have not found a candidate yet stop wanting far
+// nodes once any lane has one.
+template <int MINB, bool SHARE>
 __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
     MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
     const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
@@ -277,29 +280,13 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   const ff max2 = two_prod(max_t, max_t);
   const float kNo = __int_as_float(0x7FFFFFFF);  // NaN: "this lane does not want the entry"
   CPBest b = cp_none();
-  if (SEED && valid) {
-    for (int root = 0; root < m.n_roots; ++root) {
-      uint32_t link = m.roots[root];
-      while (!(link & kLeafBit)) {
-        Pair pr = load_pair(m.nodes, link);
-        float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
-        bool w0 = under_max(s0, pr.l, p, max2), w1 = under_max(s1, pr.r, p, max2);
-        if (!w0 && !w1) break;
-        link = w0 && (!w1 || !right_nearer(pr, s0, s1, p)) ? pr.ll : pr.lr;
-      }
-      if ((link & kLeafBit) && link != kEmptyLeaf) {
-        uint32_t k = link & ~kLeafBit;
-        for (;;) {
-          Tri t = load_tri(m.tris, k);
-          float d2, err;
-          bool have_ff;
-          ff cand_ff;
-          cp_offer(m, p, t, k, b, d2, err, have_ff, cand_ff, true);
-          if (t.flags & kTriLast) break;
-          ++k;
-        }
-      }
-    }
+  // SHARE: r = |p - p0| and R = max_j r_j, rounded up (float32 evaluation error < 2^-21 relative)
+  float r_up = 0.0f, big_r = 0.0f, share2 = kInf;
+  if (SHARE) {
+    const float x0 = __shfl_sync(full, p.x, 0), y0 = __shfl_sync(full, p.y, 0), z0 = __shfl_sync(full, p.z, 0);
+    const float dx = p.x - x0, dy = p.y - y0, dz = p.z - z0;
+    r_up = valid ? sqrtf(dx * dx + dy * dy + dz * dz) * (1.0f + 0x1p-20f) : 0.0f;
+    big_r = __uint_as_float(__reduce_max_sync(full, __float_as_uint(r_up)));
   }
   float lane_s[kMaxStack];
   bool overflow = false;
@@ -322,11 +309,17 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
             ++k;
           }
         }
+        if (SHARE) {
+          // the warp's smallest candidate bound (non-negative floats order as their bits)
+          const float wmin2 = __uint_as_float(__reduce_min_sync(full, __float_as_uint(valid ? b.d2 + b.err : kInf)));
+          const float bnd = (sqrtf(wmin2) * (1.0f + 0x1p-20f) + r_up + big_r) * (1.0f + 0x1p-20f);
+          share2 = bnd * bnd * (1.0f + 0x1p-20f);
+        }
         pop = true;
       } else {
         Pair pr = load_pair(m.nodes, link);
         float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
-        float best_hi = b.d2 + b.err;
+        float best_hi = SHARE ? fminf(b.d2 + b.err, share2) : b.d2 + b.err;
         bool w0 = act && s0 * (1.0f - kSlabMargin) <= best_hi && under_max(s0, pr.l, p, max2);
         bool w1 = act && s1 * (1.0f - kSlabMargin) <= best_hi && under_max(s1, pr.r, p, max2);
         unsigned b0 = __ballot_sync(full, w0), b1 = __ballot_sync(full, w1);
@@ -361,7 +354,8 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         bool found = false;
         while (sp > 0) {
           --sp;
-          bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= b.d2 + b.err;  // false for NaN
+          const float lim = SHARE ? fminf(b.d2 + b.err, share2) : b.d2 + b.err;
+          bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= lim;  // false for NaN
           if (__ballot_sync(full, ok)) {
             link = s_link[w][sp];
             act = ok;
@@ -1184,9 +1178,9 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
                                  unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 1 and 2 run
-  // the shared walk, 3 and 4 seed it with each lane's own greedy leaf; 2 and 4 over sorted queries
-  const bool sorted = variant == 2 || variant == 4, seed = variant >= 3;
+  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 3 and 4 add
+  // the warp-shared pruning bound; 2 and 4 run over sorted queries
+  const bool sorted = variant == 2 || variant == 4, share = variant >= 3;
   if (variant == 0 || !(min_t <= 0.0f) || (sorted && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
     dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
     return cudaGetLastError();
@@ -1207,10 +1201,10 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
     queue = nullptr;
     qcount = nullptr;
   }
-  auto kernel = seed ? (occupancy == 0   ? dev::closest_point_packet_kernel<1, true>
+  auto kernel = share ? (occupancy == 0   ? dev::closest_point_packet_kernel<1, true>
                         : occupancy == 1 ? dev::closest_point_packet_kernel<6, true>
                                          : dev::closest_point_packet_kernel<8, true>)
-                     : (occupancy == 0   ? dev::closest_point_packet_kernel<1, false>
+                      : (occupancy == 0   ? dev::closest_point_packet_kernel<1, false>
                         : occupancy == 1 ? dev::closest_point_packet_kernel<6, false>
                                          : dev::closest_point_packet_kernel<8, false>);
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
