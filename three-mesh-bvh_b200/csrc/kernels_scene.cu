@@ -33,18 +33,6 @@ __device__ __forceinline__ RayF ray_from(float3 o, float3 d) {
   return r;
 }
 
-// The world ray of row i, loaded again (a volatile load the compiler cannot merge with the first
-// one), so that the ray's registers are free during the geometry-tree walk instead of spilled;
-// the same values as make_ray's.
-__device__ __forceinline__ RayF reload_ray(const float* __restrict__ rays, uint64_t i) {
-  const float* q = rays + 6 * i;
-  float ox, oy, oz, dx, dy, dz;
-  asm volatile("ld.global.v2.f32 {%0, %1}, [%2];" : "=f"(ox), "=f"(oy) : "l"(q));
-  asm volatile("ld.global.v2.f32 {%0, %1}, [%2];" : "=f"(oz), "=f"(dx) : "l"(q + 2));
-  asm volatile("ld.global.v2.f32 {%0, %1}, [%2];" : "=f"(dy), "=f"(dz) : "l"(q + 4));
-  return ray_from(make_float3(ox, oy, oz), make_float3(dx, dy, dz));
-}
-
 __device__ __forceinline__ ff row_apply(const float* hi, const float* lo, int row, ff x, ff y, ff z, bool affine_t) {
   const int k = row * 4;
   ff s = ff_add(ff_add(ff_mul({hi[k], lo[k]}, x), ff_mul({hi[k + 1], lo[k + 1]}, y)), ff_mul({hi[k + 2], lo[k + 2]}, z));
@@ -221,8 +209,8 @@ __global__ void __launch_bounds__(kBlock, MINB) scene_raycast_first_kernel(MeshD
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const uint64_t i = queue ? queue[t] : t;
-  RayF w = make_ray(rays, i);
-  float wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
+  const RayF w = make_ray(rays, i);
+  const float wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
   const SideTable no_sides{};
   // the best world record so far lives in the ray's output row (rewritten when a closer instance
   // hit is found, a few times per ray at most), not in the thread's frame
@@ -288,8 +276,6 @@ __global__ void __launch_bounds__(kBlock, MINB) scene_raycast_first_kernel(MeshD
           atomicOr(m.err, kErrStackOverflow);
           break;
         }
-        w = reload_ray(rays, i);
-        wlen = sqrtf(w.d.x * w.d.x + w.d.y * w.d.y + w.d.z * w.d.z);
         if (b.rec != 0xFFFFFFFFu) {
           bvhc_hit h;
           const ff dist = world_record(m, I, b.rec, w, L.r, h);
