@@ -51,7 +51,7 @@ def parse():
                          "shapecast: triangles within spheres, intersectsSphere, intersectsBox")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--closest-variant", type=int, default=None,
-                    help="closest workload: force closestPointToPoint's kernel (0..4) instead of tuning")
+                    help="closest workload: force closestPointToPoint's kernel (0..2) instead of tuning")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
     ap.add_argument("--radial", type=int, default=500)
@@ -760,7 +760,7 @@ def run_closest(args, ws, rank, local):
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
                         "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
-                "gpu_launches": args.steps * (11 if tuned["best"] in (2, 4) else 1)}
+                "gpu_launches": args.steps * (11 if tuned["best"] == 2 else 1)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 

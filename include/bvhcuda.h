@@ -162,10 +162,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * warp-cooperative form walk four-child records (collapsed from raycastFirst's child pairs, same
  * leaves).  closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32
  * queries of a warp through one shared traversal (for spatially coherent queries such as grids),
- * 2 the same over the queries sorted by a Morton key of the point, 3 and 4 as 1 and 2 with the
- * lanes also pruning by a bound shared across the warp (the nearest candidate any lane has found
- * plus the points' spread); 1 to 4 apply with minThreshold 0 (otherwise 0 runs), and use the
- * occupancy setting too.  all selects raycast's
+ * 2 the same over the queries sorted by a Morton key of the point; 1 and 2 apply with
+ * minThreshold 0 (otherwise 0 runs), and use the occupancy setting too.  all selects raycast's
  * (all hits) kernel: 0 one ray per thread, 1 the rays of a warp through one shared left-first
  * traversal (each ray's hits stay in the reference's DFS order), 2, 3 and 4 the same over the rays
  * that enter the tree (the others get a zero count), sorted by the key sort = all - 1 names above

@@ -248,14 +248,14 @@ def test_knot80k_closest_point_grid256(knot80k_full, orc, cuda):
     assert pts.shape[0] == 1 << 24
     d = torch.from_numpy(pts).to(cuda)
     results = {}
-    for closest in (0, 1, 2, 3, 4):
+    for closest in (0, 1, 2):
         bvh.set_traversal(1, 1, 16, 2, 0, 0, closest)
         results[closest] = bvh.closest_point_batch(d, 0.0, 5.0).contiguous().view(torch.int32).clone()
         bvh.synchronize()
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
     # every kernel gives the same bytes on every query (exact distance ties go to the earlier
     # triangle in leaf order, whatever the traversal order)
-    for closest in (1, 2, 3, 4):
+    for closest in (1, 2):
         assert torch.equal(results[closest], results[0]), closest
     stride = 16
     idx = np.arange(0, pts.shape[0], stride)

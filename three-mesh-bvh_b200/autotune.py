@@ -128,10 +128,9 @@ def tune_raycast_all(bvh, rays, cap: int = 64, reps: int = 3, candidates=tuple(r
 
 
 def tune_closest_point(bvh, points, min_t: float = 0.0, max_t: float = math.inf, reps: int = 3,
-                       candidates=(0, 1, 2, 3, 4)) -> dict:
+                       candidates=(0, 1, 2)) -> dict:
     """Time closestPointToPoint's kernels (the `closest` field: per query, warp-cooperative,
-    warp-cooperative over Morton-sorted queries, and the two warp-cooperative forms with a
-    warp-shared pruning bound) on `points` (torch CUDA tensor, n x 3), keeping the mesh's other
+    warp-cooperative over Morton-sorted queries) on `points` (torch CUDA tensor, n x 3), keeping the mesh's other
     traversal fields, and install the fastest."""
     import torch
 

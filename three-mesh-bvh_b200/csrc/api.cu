@@ -1102,7 +1102,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 4 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
+         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
          (cfg->tile == 0 || (cfg->tile >= 8 && cfg->tile <= (1 << 24) && cfg->tile % 8 == 0)) &&
          (cfg->block == 0 || cfg->block == 64 || cfg->block == 128 || cfg->block == 256) &&
          (cfg->stack == 0 || cfg->stack == 32 || cfg->stack == 64);
@@ -1620,14 +1620,13 @@ bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n
   return read_and_clear_error(m, s);
 }
 
-// The warp-cooperative closest-point variants over Morton-sorted queries (closest = 2 or 4,
-// minThreshold 0): queue slot `slot` with its sort scratch sized for n queries; nulls for the others.
+// The warp-cooperative closest-point variant over Morton-sorted queries (closest = 2, minThreshold
+// 0): queue slot `slot` with its sort scratch sized for n queries; nulls for the other variants.
 static cudaError_t closest_sort(bvhc_mesh* m, int slot, uint64_t n, float min_threshold, uint32_t** q,
                                 unsigned int** qc, RaySort* sort) {
   *q = nullptr;
   *qc = nullptr;
-  if ((m->cfg.closest != 2 && m->cfg.closest != 4) || n >= (1ull << 32) || !(min_threshold <= 0.0f))
-    return cudaSuccess;
+  if (m->cfg.closest != 2 || n >= (1ull << 32) || !(min_threshold <= 0.0f)) return cudaSuccess;
   cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
   if (e == cudaSuccess && !m->d_qcount[slot])
     e = cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int));

@@ -41,8 +41,7 @@ struct TraversalConfig {
   int sort;        // 0: queue in ray order; 1..3: queue sorted by a Morton key (raysort.cu), implies
                    // the pre-pass
   int closest;     // closestPointToPoint: 0 one query per thread, 1 warp-cooperative, 2 warp-cooperative
-                   // over Morton-sorted queries, 3 / 4 as 1 / 2 with a warp-shared pruning bound
-                   // (1..4 only with minThreshold 0)
+                   // over Morton-sorted queries (1 and 2 only with minThreshold 0)
   int wide;        // warp-cooperative raycastFirst: 1 walks the four-child records
   int all;         // raycast (all hits): 0 one ray per thread, 1 warp-cooperative, 2..4 warp-cooperative
                    // over the rays that enter the tree, sorted by key kind all - 1, 5..8 one ray per

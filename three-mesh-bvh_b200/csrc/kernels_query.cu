@@ -253,16 +253,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 // shared order would not reproduce; those calls use the per-query kernel.)
 // ---------------------------------------------------------------------------------------------
 //
-// SHARE: the lanes also prune with a bound taken from the warp's best candidates.  With p0 the
-// first lane's point, any lane j's candidate c_j gives lane i the bound
-// |p_i - c_j| <= d_j + |p_i - p0| + |p0 - p_j|, so lane i's distance is at most
-// B_i = min_j d_j + r_i + max_j r_j (r = |p - p0|, each term rounded up).  A box whose score is
-// above B_i^2 cannot hold lane i's answer, so skipping it changes nothing; and when B_i is below
-// maxThreshold the lane still reaches the leaf of its nearest triangle (its score is at most
-// B_i^2 and under maxThreshold^2), so "null iff no leaf is reached" is kept.  For grid queries
-// (a warp's points a few cells apart) lanes that have not found a candidate yet stop wanting far
-// nodes once any lane has one.
-template <int MINB, bool SHARE>
+template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
     MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
     const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
@@ -280,14 +271,6 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   const ff max2 = two_prod(max_t, max_t);
   const float kNo = __int_as_float(0x7FFFFFFF);  // NaN: "this lane does not want the entry"
   CPBest b = cp_none();
-  // SHARE: r = |p - p0| and R = max_j r_j, rounded up (float32 evaluation error < 2^-21 relative)
-  float r_up = 0.0f, big_r = 0.0f, share2 = kInf;
-  if (SHARE) {
-    const float x0 = __shfl_sync(full, p.x, 0), y0 = __shfl_sync(full, p.y, 0), z0 = __shfl_sync(full, p.z, 0);
-    const float dx = p.x - x0, dy = p.y - y0, dz = p.z - z0;
-    r_up = valid ? sqrtf(dx * dx + dy * dy + dz * dz) * (1.0f + 0x1p-20f) : 0.0f;
-    big_r = __uint_as_float(__reduce_max_sync(full, __float_as_uint(r_up)));
-  }
   float lane_s[kMaxStack];
   bool overflow = false;
   for (int root = 0; root < m.n_roots && !overflow; ++root) {
@@ -309,17 +292,11 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
             ++k;
           }
         }
-        if (SHARE) {
-          // the warp's smallest candidate bound (non-negative floats order as their bits)
-          const float wmin2 = __uint_as_float(__reduce_min_sync(full, __float_as_uint(valid ? b.d2 + b.err : kInf)));
-          const float bnd = (sqrtf(wmin2) * (1.0f + 0x1p-20f) + r_up + big_r) * (1.0f + 0x1p-20f);
-          share2 = bnd * bnd * (1.0f + 0x1p-20f);
-        }
         pop = true;
       } else {
         Pair pr = load_pair(m.nodes, link);
         float s0 = box_score(pr.l, p), s1 = box_score(pr.r, p);
-        float best_hi = SHARE ? fminf(b.d2 + b.err, share2) : b.d2 + b.err;
+        float best_hi = b.d2 + b.err;
         bool w0 = act && s0 * (1.0f - kSlabMargin) <= best_hi && under_max(s0, pr.l, p, max2);
         bool w1 = act && s1 * (1.0f - kSlabMargin) <= best_hi && under_max(s1, pr.r, p, max2);
         unsigned b0 = __ballot_sync(full, w0), b1 = __ballot_sync(full, w1);
@@ -354,8 +331,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         bool found = false;
         while (sp > 0) {
           --sp;
-          const float lim = SHARE ? fminf(b.d2 + b.err, share2) : b.d2 + b.err;
-          bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= lim;  // false for NaN
+          bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= b.d2 + b.err;  // false for NaN
           if (__ballot_sync(full, ok)) {
             link = s_link[w][sp];
             act = ok;
@@ -1178,9 +1154,9 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
                                  unsigned int* qcount, const RaySort* sort) {
   if (n == 0) return cudaSuccess;
-  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 3 and 4 add
-  // the warp-shared pruning bound; 2 and 4 run over sorted queries
-  const bool sorted = variant == 2 || variant == 4, share = variant >= 3;
+  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 2 runs over
+  // Morton-sorted queries
+  const bool sorted = variant == 2;
   if (variant == 0 || !(min_t <= 0.0f) || (sorted && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
     dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
     return cudaGetLastError();
@@ -1201,12 +1177,9 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
     queue = nullptr;
     qcount = nullptr;
   }
-  auto kernel = share ? (occupancy == 0   ? dev::closest_point_packet_kernel<1, true>
-                        : occupancy == 1 ? dev::closest_point_packet_kernel<6, true>
-                                         : dev::closest_point_packet_kernel<8, true>)
-                      : (occupancy == 0   ? dev::closest_point_packet_kernel<1, false>
-                        : occupancy == 1 ? dev::closest_point_packet_kernel<6, false>
-                                         : dev::closest_point_packet_kernel<8, false>);
+  auto kernel = occupancy == 0   ? dev::closest_point_packet_kernel<1>
+                : occupancy == 1 ? dev::closest_point_packet_kernel<6>
+                                 : dev::closest_point_packet_kernel<8>;
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
   return cudaGetLastError();
 }

@@ -262,17 +262,13 @@ __device__ __forceinline__ bool tri_hit_t(float3 a, float3 b, float3 c, float3 o
 // rather than with the absolute coordinates.
 // ---------------------------------------------------------------------------------------------
 
-// Float32 version: returns |p - q|^2 and the closest point q (world frame).  The Voronoi region
-// is decided first with the same tests, in the same order, as the branching form (vertex a, vertex
-// b, edge ab, vertex c, edge ac, edge bc, interior), and the point is then assembled with selects
-// and at most two divisions, so that lanes of a warp whose points fall in different regions of the
-// same triangle do not take seven paths one after another.  Vertex regions return the vertex
-// itself (bit-exact), as the callers' tie test expects.
+// Float32 version: returns |p - q|^2 and the closest point q (world frame).
 __device__ __forceinline__ float closest_sq_f(float3 p, float3 a, float3 b, float3 c, float3& q, float& scale) {
   float abx = b.x - a.x, aby = b.y - a.y, abz = b.z - a.z;
   float acx = c.x - a.x, acy = c.y - a.y, acz = c.z - a.z;
   float apx = p.x - a.x, apy = p.y - a.y, apz = p.z - a.z;
   scale = max3abs(abx, aby, abz) + max3abs(acx, acy, acz) + max3abs(apx, apy, apz);
+  float lx, ly, lz;  // closest point relative to a
   float d1 = abx * apx + aby * apy + abz * apz;
   float d2 = acx * apx + acy * apy + acz * apz;
   float bpx = apx - abx, bpy = apy - aby, bpz = apz - abz;
@@ -284,37 +280,33 @@ __device__ __forceinline__ float closest_sq_f(float3 p, float3 a, float3 b, floa
   float vc = d1 * d4 - d3 * d2;
   float vb = d5 * d2 - d1 * d6;
   float va = d3 * d6 - d5 * d4;
-  float d43 = d4 - d3, d56 = d5 - d6;
-  // region: 0 vertex a, 1 vertex b, 2 edge ab, 3 vertex c, 4 edge ac, 5 edge bc, 6 interior
-  const int region = (d1 <= 0.0f && d2 <= 0.0f)                  ? 0
-                     : (d3 >= 0.0f && d4 <= d3)                  ? 1
-                     : (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f)  ? 2
-                     : (d6 >= 0.0f && d5 <= d6)                  ? 3
-                     : (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f)  ? 4
-                     : (va <= 0.0f && d43 >= 0.0f && d56 >= 0.0f) ? 5
-                                                                 : 6;
-  // edge parameter (regions 2, 4, 5) and the interior's 1 / (va + vb + vc)
-  const float num = region == 2 ? d1 : (region == 4 ? d2 : d43);
-  const float den = region == 2 ? d1 - d3 : (region == 4 ? d2 - d6 : d43 + d56);
-  const float t = (region == 2 || region == 4 || region == 5) ? num / den : 0.0f;
-  const float inv = region == 6 ? 1.0f / (va + vb + vc) : 0.0f;
-  const float v = vb * inv, w = vc * inv;
-  // l = q - a per region
-  const float ux = region == 5 ? acx - abx : 0.0f, uy = region == 5 ? acy - aby : 0.0f,
-              uz = region == 5 ? acz - abz : 0.0f;
-  float lx, ly, lz;
-  if (region == 6) {
-    lx = abx * v + acx * w; ly = aby * v + acy * w; lz = abz * v + acz * w;
+  if (d1 <= 0.0f && d2 <= 0.0f) {
+    lx = 0.0f; ly = 0.0f; lz = 0.0f;
+    q = a;
+  } else if (d3 >= 0.0f && d4 <= d3) {
+    lx = abx; ly = aby; lz = abz;
+    q = b;
+  } else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+    float v = d1 / (d1 - d3);
+    lx = abx * v; ly = aby * v; lz = abz * v;
+    q = make_float3(a.x + lx, a.y + ly, a.z + lz);
+  } else if (d6 >= 0.0f && d5 <= d6) {
+    lx = acx; ly = acy; lz = acz;
+    q = c;
+  } else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+    float w = d2 / (d2 - d6);
+    lx = acx * w; ly = acy * w; lz = acz * w;
+    q = make_float3(a.x + lx, a.y + ly, a.z + lz);
+  } else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    lx = abx + (acx - abx) * w; ly = aby + (acy - aby) * w; lz = abz + (acz - abz) * w;
+    q = make_float3(a.x + lx, a.y + ly, a.z + lz);
   } else {
-    const bool use_ab = region == 1 || region == 2 || region == 5, use_ac = region == 3 || region == 4;
-    const float sx = use_ab ? abx : (use_ac ? acx : 0.0f), sy = use_ab ? aby : (use_ac ? acy : 0.0f),
-                sz = use_ab ? abz : (use_ac ? acz : 0.0f);
-    const float k = (region == 2 || region == 4) ? t : 1.0f;
-    lx = region == 5 ? abx + ux * t : sx * k;
-    ly = region == 5 ? aby + uy * t : sy * k;
-    lz = region == 5 ? abz + uz * t : sz * k;
+    float den = 1.0f / (va + vb + vc);
+    float v = vb * den, w = vc * den;
+    lx = abx * v + acx * w; ly = aby * v + acy * w; lz = abz * v + acz * w;
+    q = make_float3(a.x + lx, a.y + ly, a.z + lz);
   }
-  q = region == 0 ? a : region == 1 ? b : region == 3 ? c : make_float3(a.x + lx, a.y + ly, a.z + lz);
   float rx = apx - lx, ry = apy - ly, rz = apz - lz;
   return rx * rx + ry * ry + rz * rz;
 }
