@@ -1027,11 +1027,12 @@ def run_scene(args, ws, rank, local):
         lib.bvhc_scene_raycast_first(scene.h, rays.data_ptr(), n_rays, 0, 0.0, math.inf, hits.data_ptr(),
                                      inst.data_ptr(), 1, s)
 
-    # ray order (input order, a Morton key, or the first instance reached) and resident blocks per
-    # SM (the batch's occupancy: 14, 10, 8), whichever is fastest here
+    # ray order (input order, a Morton key, or the first instance reached) and kernel variant
+    # (resident blocks per SM 14 / 10 / 8, or 14 with the stack top in shared memory), whichever is
+    # fastest here
     order_ms = {}
-    for occ in (0, 1, 2):
-        batch.set_traversal(1, 1, 16, occ)
+    for occ in (0, 1, 2, 3):
+        scene.set_variant(occ)
         for order in (0, 1, 2, 3, 4):
             scene.set_order(order)
             step()
@@ -1042,7 +1043,7 @@ def run_scene(args, ws, rank, local):
             e1.synchronize()
             order_ms[(occ, order)] = e0.elapsed_time(e1)
     best_occ, best_order = min(order_ms, key=order_ms.get)
-    batch.set_traversal(1, 1, 16, best_occ)
+    scene.set_variant(best_occ)
     scene.set_order(best_order)
     for _ in range(args.warmup):
         step()
@@ -1117,7 +1118,7 @@ def run_scene(args, ws, rank, local):
                                        "the instance cube), firstHitOnly",
                            "geometry_triangles": int(sum(g.triangle_count for g in geoms)),
                            "hit_fraction": hit_frac, "l2": "inputs (100 MB rays + 134 MB hits) exceed L2",
-                           "ray_order": best_order, "occupancy": best_occ,
+                           "ray_order": best_order, "kernel_variant": best_occ,
                            "order_ms": {str(k): v for k, v in order_ms.items()},
                            "all_hits": {"ms": ms_all, "Mrays_per_s": weak_scaling_rate(ws, n_rays, 1, ms_all),
                                         "cap": cap_all, "mean_hits_per_ray": mean_hits}},

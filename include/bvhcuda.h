@@ -334,9 +334,7 @@ bvhc_status bvhc_scene_set_instances(bvhc_scene* scene, int n_instances, const u
  * back to world space with its distance from the ray origin (convertRaycastIntersect,
  * src/utils/GeometryRayIntersectUtilities.js:3-17), and the closest of them (equal distances
  * keep the lower instance).  hits: world distance and point, the geometry's faceIndex and local
- * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none.
- * The batch's traversal `occupancy` (bvhc_mesh_set_traversal on the batch) sets the kernel's
- * resident blocks per SM: 0 fourteen, 1 ten, 2 eight. */
+ * barycoord; instance[i]: the hit's instance (the Intersection's batchId), BVHC_NO_HIT if none. */
 bvhc_status bvhc_scene_raycast_first(bvhc_scene* scene, const float* rays, uint64_t n, int side, float near_dist,
                                      float far_dist, bvhc_hit* hits, uint32_t* instance, int mem, void* stream);
 /* The same without firstHitOnly (the BatchedMesh raycast, then the raycaster's sort): every hit of
@@ -348,6 +346,11 @@ bvhc_status bvhc_scene_raycast(bvhc_scene* scene, const float* rays, uint64_t n,
                                float far_dist, uint32_t cap, uint32_t* counts, bvhc_hit* hits, uint32_t* instance,
                                int mem, void* stream);
 void bvhc_scene_destroy(bvhc_scene* scene);
+/* Kernel variant of bvhc_scene_raycast_first (no reference counterpart; results are the same for
+ * every variant): resident blocks per SM 14 (0), 10 (1) or 8 (2) -- more blocks hide more latency
+ * and leave fewer registers per thread -- or 14 with the top 8 entries of each geometry-tree
+ * walk's stack in shared memory (3). */
+bvhc_status bvhc_scene_set_variant(bvhc_scene* scene, int variant);
 /* Ray order of bvhc_scene_raycast_first: 0 input order; 1, 2, 3 the rays sorted by a Morton key
  * (direction; entry point into the instances' world box; that point and the direction); 4 sorted
  * by the first instance the ray reaches in the instance tree, so that the rays of a warp walk the

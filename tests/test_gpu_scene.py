@@ -71,18 +71,19 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
     bad = _compare(got, ginst, exp, einst)
     assert not bad, bad[:10]
     assert (einst >= 0).mean() > 0.2
-    # device buffers, every ray order and every register budget (resident blocks per SM) give the
-    # same records
-    for occ in (0, 1, 2):
-        batch.set_traversal(1, 1, 16, occ)
+    # device buffers, every ray order and every kernel variant give the same records
+    for variant in (0, 1, 2, 3):
+        scene.set_variant(variant)
         for order in (0, 1, 2, 3, 4):
             scene.set_order(order)
             dh, di = scene.raycast_first(torch.from_numpy(rays).to(cuda))
             torch.cuda.synchronize()
-            assert np.array_equal(di.cpu().numpy().view(np.uint32), ginst), (occ, order)
+            assert np.array_equal(di.cpu().numpy().view(np.uint32), ginst), (variant, order)
             assert np.array_equal(dh.cpu().numpy().view(np.uint8).reshape(-1), got.view(np.uint8).reshape(-1)), (
-                occ, order)
-    batch.set_traversal(1, 1, 16, 0)
+                variant, order)
+    with pytest.raises(pkg.BVHCError):
+        scene.set_variant(4)
+    scene.set_variant(0)
     scene.set_order(0)
     scene.dispose()
 

@@ -88,6 +88,7 @@ SIGNATURES = [
     ("bvhc_scene_raycast_first", _I, [_P, _P, _U64, _I, _F, _F, _P, _P, _I, _P]),
     ("bvhc_scene_destroy", None, [_P]),
     ("bvhc_scene_set_order", _I, [_P, _I]),
+    ("bvhc_scene_set_variant", _I, [_P, _I]),
     ("bvhc_scene_raycast", _I, [_P, _P, _U64, _I, _F, _F, C.c_uint32, _P, _P, _P, _I, _P]),
     ("bvhc_hit_interpolate", _I, [_P, _P, _U64, _P, _U64, _I, _I, _P, _P, _I, _P]),
     ("bvhc_triangle_hit_point_info", _I, [_P, _P, _P, _U64, _P, _I, _P, _I, _U64, _P, _I, _P, _I, _P]),

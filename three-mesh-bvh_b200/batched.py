@@ -197,6 +197,10 @@ class InstancedScene:
         (4).  Results do not change."""
         N.check(N.lib().bvhc_scene_set_order(self.h, int(kind)), "bvhc_scene_set_order")
 
+    def set_variant(self, variant: int):
+        """raycastFirst kernel variant (bvhc_scene_set_variant): 0..3."""
+        N.check(N.lib().bvhc_scene_set_variant(self.h, int(variant)), "bvhc_scene_set_variant")
+
     def raycast_first(self, rays, side=FrontSide, near=0.0, far=float("inf"), stream=None):
         """World rays (n x 6 float32): numpy -> (hits structured array, instance ids); torch CUDA
         tensor -> ((n, 8) float32 hit tensor, int32 instance tensor), enqueued on `stream`."""

@@ -1827,6 +1827,7 @@ struct bvhc_scene {
   size_t ids_cap = 0;
   // ray ordering (bvhc_scene_set_order): key kind, the instances' world box, sort scratch, queue
   int order = 0;
+  int variant = 0;  // instanced raycastFirst kernel variant (bvhc_scene_set_variant)
   float box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
   RaySortScratch sort_s = {};
   uint64_t sort_cap = 0;
@@ -2033,7 +2034,7 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
   sd.n_instances = sc->n_instances;
-  sd.occupancy = m->cfg.occupancy;
+  sd.occupancy = sc->variant;
   if (mem == BVHC_MEM_HOST && n > kPipeChunk) {
     // Large host batches: chunks of kPipeChunk rays rotate over the batch mesh's three pipeline
     // streams and staging slots (instance ids in a slot of the scene's own), so the copies of some
@@ -2117,7 +2118,7 @@ bvhc_status bvhc_scene_raycast(bvhc_scene* sc, const float* rays, uint64_t n, in
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   SceneDev sd{sc->d_tlas, sc->root, sc->d_inst, m->d_mesh_root_off};
   sd.n_instances = sc->n_instances;
-  sd.occupancy = m->cfg.occupancy;
+  sd.occupancy = sc->variant;
   const uint32_t c = cap > 0 ? cap : 1;  // cap 0: counts only (one scratch slot per ray)
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(counts, 4) || (cap > 0 && (!aligned(hits, 16) || !aligned(instance, 4))))
@@ -2159,6 +2160,12 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
   for (void* p : sc->inst_slot) cudaFree(p);
   free_sort_scratch(sc->sort_s);
   delete sc;
+}
+
+bvhc_status bvhc_scene_set_variant(bvhc_scene* sc, int variant) {
+  if (!sc || variant < 0 || variant > 3) return BVHC_ERR_INVALID_ARGUMENT;
+  sc->variant = variant;
+  return BVHC_OK;
 }
 
 bvhc_status bvhc_scene_set_order(bvhc_scene* scene, int kind) {

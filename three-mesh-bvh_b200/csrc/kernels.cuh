@@ -147,7 +147,7 @@ struct SceneDev {
   const InstanceDev* inst;
   const uint32_t* mesh_root_off;
   int n_instances = 1 << 30;   // bounds the instance tree's depth (a median split)
-  int occupancy = 0;           // raycastFirst resident blocks per SM: 0 fourteen, 1 ten, 2 eight
+  int occupancy = 0;           // raycastFirst kernel variant (bvhc_scene_set_variant)
 };
 // World-space raycastFirst over the instances: hits[i] in world space (distance, point; local
 // barycoord and faceIndex), instance[i] the hit instance (0xFFFFFFFF: none).  With `sort` (kind
