@@ -1028,10 +1028,9 @@ def run_scene(args, ws, rank, local):
                                      inst.data_ptr(), 1, s)
 
     # ray order (input order, a Morton key, or the first instance reached) and kernel variant
-    # (resident blocks per SM 14 / 10 / 8, or 14 with the stack top in shared memory), whichever is
-    # fastest here
+    # (resident blocks per SM 14 / 10 / 8), whichever is fastest here
     order_ms = {}
-    for occ in (0, 1, 2, 3):
+    for occ in (0, 1, 2):
         scene.set_variant(occ)
         for order in (0, 1, 2, 3, 4):
             scene.set_order(order)

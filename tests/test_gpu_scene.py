@@ -72,7 +72,7 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
     assert not bad, bad[:10]
     assert (einst >= 0).mean() > 0.2
     # device buffers, every ray order and every kernel variant give the same records
-    for variant in (0, 1, 2, 3):
+    for variant in (0, 1, 2):
         scene.set_variant(variant)
         for order in (0, 1, 2, 3, 4):
             scene.set_order(order)
@@ -82,7 +82,7 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
             assert np.array_equal(dh.cpu().numpy().view(np.uint8).reshape(-1), got.view(np.uint8).reshape(-1)), (
                 variant, order)
     with pytest.raises(pkg.BVHCError):
-        scene.set_variant(4)
+        scene.set_variant(3)
     scene.set_variant(0)
     scene.set_order(0)
     scene.dispose()

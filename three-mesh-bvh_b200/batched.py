@@ -198,7 +198,7 @@ class InstancedScene:
         N.check(N.lib().bvhc_scene_set_order(self.h, int(kind)), "bvhc_scene_set_order")
 
     def set_variant(self, variant: int):
-        """raycastFirst kernel variant (bvhc_scene_set_variant): 0..3."""
+        """raycastFirst kernel variant (bvhc_scene_set_variant): 0..2."""
         N.check(N.lib().bvhc_scene_set_variant(self.h, int(variant)), "bvhc_scene_set_variant")
 
     def raycast_first(self, rays, side=FrontSide, near=0.0, far=float("inf"), stream=None):

@@ -2163,7 +2163,7 @@ void bvhc_scene_destroy(bvhc_scene* sc) {
 }
 
 bvhc_status bvhc_scene_set_variant(bvhc_scene* sc, int variant) {
-  if (!sc || variant < 0 || variant > 3) return BVHC_ERR_INVALID_ARGUMENT;
+  if (!sc || variant < 0 || variant > 2) return BVHC_ERR_INVALID_ARGUMENT;
   sc->variant = variant;
   return BVHC_OK;
 }

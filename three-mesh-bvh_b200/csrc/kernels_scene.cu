@@ -39,10 +39,9 @@ __device__ __forceinline__ ff row_apply(const float* hi, const float* lo, int ro
   return affine_t ? ff_add(s, ff{hi[k + 3], lo[k + 3]}) : s;
 }
 
-// Traversal stacks of the geometry-tree walk.  LocalStack keeps every entry in thread-local
-// memory.  RingStack keeps the top kRing entries in shared memory (the entry at depth d in slot
-// d mod kRing of the thread's column) and moves an entry to local memory only when a push would
-// overwrite it, so pushes and pops near the top (almost all of them) stay on chip.
+// Traversal stack of the geometry-tree walk, in thread-local memory.  (A form that kept the top 8
+// entries in shared memory measured 22.5 ms against 20.3 ms on the instanced bench: the shared
+// memory it takes is L1 capacity the node reads need.)
 template <int STACK>
 struct LocalStack {
   uint32_t link[STACK];
@@ -61,46 +60,6 @@ struct LocalStack {
     --sp;
     l = link[sp];
     e = t[sp];
-    return true;
-  }
-};
-
-constexpr int kRing = 8;
-__shared__ uint32_t g_ring_link[kRing][kBlock];
-__shared__ float g_ring_t[kRing][kBlock];
-
-template <int STACK>
-struct RingStack {
-  uint32_t link[STACK];  // entries moved out of the ring (depths below lo)
-  float t[STACK];
-  int sp, lo;            // depth of the next push; lowest depth still in the ring
-  __device__ __forceinline__ void reset() { sp = lo = 0; }
-  __device__ __forceinline__ bool push(uint32_t l, float e) {
-    if (sp >= STACK) return false;
-    if (sp - lo == kRing) {  // the ring is full: its deepest entry goes to local memory
-      const int slot = lo % kRing;
-      link[lo] = g_ring_link[slot][threadIdx.x];
-      t[lo] = g_ring_t[slot][threadIdx.x];
-      ++lo;
-    }
-    const int slot = sp % kRing;
-    g_ring_link[slot][threadIdx.x] = l;
-    g_ring_t[slot][threadIdx.x] = e;
-    ++sp;
-    return true;
-  }
-  __device__ __forceinline__ bool pop(uint32_t& l, float& e) {
-    if (sp == 0) return false;
-    --sp;
-    if (sp >= lo) {
-      const int slot = sp % kRing;
-      l = g_ring_link[slot][threadIdx.x];
-      e = g_ring_t[slot][threadIdx.x];
-    } else {  // below the ring: every entry of depth < lo is in local memory
-      l = link[sp];
-      e = t[sp];
-      lo = sp;
-    }
     return true;
   }
 };
@@ -260,7 +219,7 @@ constexpr int kTlasStack = 32;
 // own large body and on its scattered loads, and more resident warps hide both, while fewer
 // registers spill more to local memory; the instanced bench tunes 14 / 10 / 8 (it measured 35.6 /
 // 28.4 / 22.7 / 20.4 / 20.4 ms at 5 / 8 / 12 / 14 / 16 blocks with 64-entry stacks).
-template <int TSTACK, int BSTACK, int MINB, bool RING>
+template <int TSTACK, int BSTACK, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) scene_raycast_first_kernel(MeshDev m, SceneDev sc,
                                                                         const float* __restrict__ rays, uint64_t n,
                                                                         const uint32_t* __restrict__ queue, int side,
@@ -332,17 +291,9 @@ __global__ void __launch_bounds__(kBlock, MINB) scene_raycast_first_kernel(MeshD
         const float tlim = best_dist.hi == kInf ? kInf : best_dist.hi * L.vlen / wlen * (1.0f + 0x1p-16f);
         Best b{kInf, 0.0f, 0xFFFFFFFFu};
         const uint32_t g = I.geometry;
-        bool ok;
-        if (RING) {
-          RingStack<BSTACK> st;
-          ok = blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
-                          fminf(L.far_d, tlim), b, st);
-        } else {
-          LocalStack<BSTACK> st;
-          ok = blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
-                          fminf(L.far_d, tlim), b, st);
-        }
-        if (!ok) {
+        LocalStack<BSTACK> st;
+        if (!blas_first(m, sc.mesh_root_off[g], sc.mesh_root_off[g + 1], L.r, L.len, side, no_sides, L.near_d,
+                        fminf(L.far_d, tlim), b, st)) {
           atomicOr(m.err, kErrStackOverflow);
           break;
         }
@@ -570,18 +521,15 @@ cudaError_t launch_scene_raycast_first(const MeshDev& blas, const SceneDev& scen
     if ((e = launch_ray_sort(sort->kind, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
   }
   // the small stacks when both trees allow them, else the large ones; resident blocks per SM by
-  // the batch's occupancy setting (0: 14, 1: 10, 2: 8; 3: 14 with the geometry walk's stack top in
-  // shared memory)
+  // the scene's variant (0: 14, 1: 10, 2: 8)
   const bool small = scene.n_instances <= (1 << 16) && stack_entries(blas, 32) == 32;
   const int occ = scene.occupancy;
-  auto kernel = small ? (occ == 1   ? dev::scene_raycast_first_kernel<16, 32, 10, false>
-                         : occ == 2 ? dev::scene_raycast_first_kernel<16, 32, 8, false>
-                         : occ == 3 ? dev::scene_raycast_first_kernel<16, 32, 14, true>
-                                    : dev::scene_raycast_first_kernel<16, 32, 14, false>)
-                      : (occ == 1   ? dev::scene_raycast_first_kernel<32, 64, 10, false>
-                         : occ == 2 ? dev::scene_raycast_first_kernel<32, 64, 8, false>
-                         : occ == 3 ? dev::scene_raycast_first_kernel<32, 64, 14, true>
-                                    : dev::scene_raycast_first_kernel<32, 64, 14, false>);
+  auto kernel = small ? (occ == 1   ? dev::scene_raycast_first_kernel<16, 32, 10>
+                         : occ == 2 ? dev::scene_raycast_first_kernel<16, 32, 8>
+                                    : dev::scene_raycast_first_kernel<16, 32, 14>)
+                      : (occ == 1   ? dev::scene_raycast_first_kernel<32, 64, 10>
+                         : occ == 2 ? dev::scene_raycast_first_kernel<32, 64, 8>
+                                    : dev::scene_raycast_first_kernel<32, 64, 14>);
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(blas, scene, rays, n, sorted ? queue : nullptr, side, near_d, far_d,
                                                   hits, instance);
   return cudaGetLastError();
