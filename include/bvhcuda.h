@@ -174,7 +174,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * 0 gives each warp 32 consecutive rays; a multiple of 8 (at most 2^24) reads the rays as rows of
  * `tile` rays and gives each warp a tile of 4 rows x 8 rays, for rays generated per pixel of a
  * row-major image of that width (the ray-sort granularity without a sort); it applies to raycast's
- * warp-cooperative kernel (all = 1) too.  block: threads per
+ * warp-cooperative kernel (all = 1) too.  tile_rows (2, 4 or 8; 0 = 4) is the tile's height R, its
+ * width 32 / R (tile must then be a multiple of 32 / R).  block: threads per
  * block of the warp-cooperative raycastFirst (64, 128 or 256; 0 = 128).  stack: traversal stack
  * entries of the warp-cooperative and persistent raycastFirst (32 or 64; 0 = 64); 32 applies to
  * trees of depth 30 or less and 64 runs otherwise.  Results are the same for every variant (up to
@@ -192,6 +193,7 @@ typedef struct bvhc_traversal_config {
   int32_t tile;
   int32_t block;
   int32_t stack;
+  int32_t tile_rows;
 } bvhc_traversal_config;
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* mesh, const bvhc_traversal_config* cfg);
 bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config* cfg);
@@ -205,7 +207,8 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config
  * without the root-box compaction and each ordering key; register budgets; the tiled ray order for
  * each row pitch in tile_pitches, e.g. an image width) for every device leaf layout in leaf_sizes
  * (NULL / 0: the current one); the layout with the smallest sum of the sets' best times wins.
- * Stage 2: threads per block and the 32-entry stack around each set's best.  Each variant is run
+ * Stage 2: threads per block, the tiled order's tile height and the 32-entry stack around each
+ * set's best.  Each variant is run
  * once untimed, then `reps` times.  Outputs: best[k] and best_ms[k] per set (best_ms nullable),
  * the chosen layout (nullable) and each layout's total (leaf_total_ms[n_leaf_sizes], nullable).
  * The mesh is left with the chosen layout and set 0's variant; callers switch variants per set

@@ -127,7 +127,7 @@ def test_autotune_candidates_and_argument_checks(pkg):
     assert len(base) == 87 and len({tuple(c) for c in base}) == 87
     fields = autotune.FIELDS
     assert fields[:6] == ["persistent", "order", "refill", "occupancy", "compact", "sort"]
-    assert fields[9:] == ["tile", "block", "stack"]
+    assert fields[9:] == ["tile", "block", "stack", "tile_rows"]
     forms = {c[0] for c in base}
     assert forms == {0, 1, 2}
     assert any(c[7] == 1 for c in base)                                    # four-child records

@@ -224,7 +224,7 @@ def test_traversal_variants_agree(pkg, orc, cuda, persistent, order, refill, occ
     bvh.set_traversal(persistent, order, refill, occupancy, compact, sort)
     assert bvh.get_traversal() == dict(persistent=persistent, order=order, refill=refill, occupancy=occupancy,
                                        compact=compact, sort=sort, closest=0, wide=0, all=0, tile=0,
-                                       block=0, stack=0)
+                                       block=0, stack=0, tile_rows=0)
     rays = np.concatenate([pkg.rays_incoherent(100_000, seed=4), pkg.rays_camera(256, 256),
                            pkg.rays_sphere_to_box(50_000, seed=6)])
     for side in (0, 2):
@@ -398,14 +398,16 @@ def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
 
 
 def test_traversal_config_rejects_bad_fields(pkg, cuda):
-    """Tile pitches that are not a positive multiple of 8, block sizes other than 64 / 128 / 256 and
-    stacks other than 32 / 64 are rejected."""
+    """Tile pitches that are not a positive multiple of 8 (of 16 for 2-row tiles), tile heights other
+    than 2 / 4 / 8, block sizes other than 64 / 128 / 256 and stacks other than 32 / 64 are
+    rejected."""
     geo = pkg.torus_knot(10, 3, 32, 8)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
-    for bad in (dict(tile=12), dict(tile=-8), dict(block=96), dict(stack=48), dict(stack=16)):
+    for bad in (dict(tile=12), dict(tile=-8), dict(block=96), dict(stack=48), dict(stack=16), dict(tile_rows=3),
+                dict(tile=24, tile_rows=2)):
         with pytest.raises(pkg.BVHCError):
             bvh.set_traversal(2, 1, 16, 0, **bad)
-    bvh.set_traversal(2, 1, 16, 2, tile=4096, block=256, stack=32)
+    bvh.set_traversal(2, 1, 16, 2, tile=4096, block=256, stack=32, tile_rows=8)
     assert bvh.get_traversal() == dict(persistent=2, order=1, refill=16, occupancy=2, compact=0, sort=0, closest=0,
-                                       wide=0, all=0, tile=4096, block=256, stack=32)
+                                       wide=0, all=0, tile=4096, block=256, stack=32, tile_rows=8)
     bvh.dispose()

@@ -95,13 +95,16 @@ def _first_sample(bvh, d, stride):
 
 def _stage2(cands):
     """The autotuner's stage-2 forms of its stage-1 candidates: threads per block 64 / 256 for the
-    warp-cooperative form over child pairs, and the 32-entry stack for it and the persistent form."""
+    warp-cooperative form over child pairs, its tiled order's other tile heights (2, 8 rows), and
+    the 32-entry stack for it and the persistent form."""
     out = []
     for c in cands:
         if c[0] == 2 and not c[7]:
-            out += [c[:10] + [64, 0], c[:10] + [256, 32], c[:10] + [0, 32]]
+            out += [c[:10] + [64, 0, 0], c[:10] + [256, 32, 0], c[:10] + [0, 32, 0]]
+            if c[9] and c[9] % 16 == 0:
+                out += [c[:10] + [0, 32, 2], c[:10] + [0, 0, 8]]
         elif c[0] == 1:
-            out.append(c[:10] + [0, 32])
+            out.append(c[:10] + [0, 32, 0])
     return out
 
 

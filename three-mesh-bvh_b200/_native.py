@@ -34,7 +34,7 @@ class BvhcTraversalConfig(C.Structure):
     _fields_ = [("persistent", C.c_int32), ("order", C.c_int32), ("refill", C.c_int32), ("occupancy", C.c_int32),
                 ("compact", C.c_int32), ("sort", C.c_int32), ("closest", C.c_int32),
                 ("wide", C.c_int32), ("all", C.c_int32), ("tile", C.c_int32),
-                ("block", C.c_int32), ("stack", C.c_int32)]
+                ("block", C.c_int32), ("stack", C.c_int32), ("tile_rows", C.c_int32)]
 
 
 class BvhcMeshInfo(C.Structure):

@@ -77,9 +77,9 @@ class BatchedMeshBVH:
         return self._mesh
 
     def set_traversal(self, persistent=1, order=1, refill=16, occupancy=0, compact=0, sort=0, closest=0, wide=0,
-                      all=0, tile=0, block=0, stack=0):
+                      all=0, tile=0, block=0, stack=0, tile_rows=0):
         cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide, all, tile,
-                                    block, stack)
+                                    block, stack, tile_rows)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     @staticmethod

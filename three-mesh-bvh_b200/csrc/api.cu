@@ -28,7 +28,7 @@ struct bvhc_mesh {
   unsigned int* d_err = nullptr;
   unsigned long long* d_work = nullptr;  // work counter of the persistent raycastFirst kernel
   unsigned long long* d_work_all = nullptr;  // work counter of the persistent raycast (all hits) kernel
-  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  TraversalConfig cfg{1, 1, 16, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   float scene_lo[3] = {0.0f, 0.0f, 0.0f}, scene_hi[3] = {0.0f, 0.0f, 0.0f};  // box of every triangle
   uint64_t n_nodes = 0, n_tris = 0;
   int n_roots = 0;
@@ -1104,14 +1104,17 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
          cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
          (cfg->tile == 0 || (cfg->tile >= 8 && cfg->tile <= (1 << 24) && cfg->tile % 8 == 0)) &&
+         (cfg->tile_rows == 0 || cfg->tile_rows == 2 || cfg->tile_rows == 4 || cfg->tile_rows == 8) &&
+         (cfg->tile == 0 || cfg->tile % (32 >> tile_rows_log2(cfg->tile_rows)) == 0) &&
          (cfg->block == 0 || cfg->block == 64 || cfg->block == 128 || cfg->block == 256) &&
          (cfg->stack == 0 || cfg->stack == 32 || cfg->stack == 64);
 }
 
 bvhc_status bvhc_mesh_set_traversal(bvhc_mesh* m, const bvhc_traversal_config* cfg) {
   if (!m || !valid_config(cfg)) return BVHC_ERR_INVALID_ARGUMENT;
-  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact, cfg->sort,
-                           cfg->closest,    cfg->wide,  cfg->all,    cfg->tile,      cfg->block,   cfg->stack};
+  m->cfg = TraversalConfig{cfg->persistent, cfg->order, cfg->refill, cfg->occupancy, cfg->compact,
+                           cfg->sort,       cfg->closest, cfg->wide, cfg->all,       cfg->tile,
+                           cfg->block,      cfg->stack,   cfg->tile_rows};
   return BVHC_OK;
 }
 
@@ -1252,6 +1255,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* m, bvhc_traversal_config* c
   cfg->tile = m->cfg.tile;
   cfg->block = m->cfg.block;
   cfg->stack = m->cfg.stack;
+  cfg->tile_rows = m->cfg.tile_rows;
   return BVHC_OK;
 }
 
@@ -1356,7 +1360,7 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   if (mem == BVHC_MEM_DEVICE)
     return from_cuda(launch_raycast_all(m->view(), rays, n, side, tab, near_d, far_d, cap, counts, hits, s, variant,
                                         m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all,
-                                        (uint32_t)m->cfg.tile));
+                                        (uint32_t)m->cfg.tile, m->cfg.tile_rows));
   BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, std::max<uint64_t>(n * cap * sizeof(bvhc_hit), 16)));
   BVHC_CUDA_TRY(ensure(&m->d_out2, &m->out2_cap, n * 4));
@@ -1364,7 +1368,7 @@ static bvhc_status raycast_all_impl(bvhc_mesh* m, const float* rays, uint64_t n,
   BVHC_CUDA_TRY(launch_raycast_all(m->view(), static_cast<const float*>(m->d_in), n, side, tab, near_d, far_d, cap,
                                    static_cast<uint32_t*>(m->d_out2), static_cast<bvhc_hit*>(m->d_out), s, variant,
                                    m->cfg.occupancy, q, qc, sort.kind ? &sort : nullptr, m->d_work_all,
-                                   (uint32_t)m->cfg.tile));
+                                   (uint32_t)m->cfg.tile, m->cfg.tile_rows));
   BVHC_CUDA_TRY(cudaMemcpyAsync(counts, m->d_out2, n * 4, cudaMemcpyDeviceToHost, s));
   if (cap > 0)
     BVHC_CUDA_TRY(cudaMemcpyAsync(hits, m->d_out, n * cap * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));

@@ -5,8 +5,8 @@
 // Stage 1 times every candidate of the list below on each ray set, for each device leaf layout
 // asked for; the layout with the smallest sum of the sets' best times is kept.  Stage 2 refines
 // each set's best warp-cooperative or persistent candidate on that layout: threads per block (64,
-// 128, 256; warp-cooperative form) and the 32-entry traversal stack (when the tree is shallow
-// enough).  Every variant returns the same hits (up to exact ties), so tuning changes speed only.
+// 128, 256; warp-cooperative form), the tile height of a tiled order (2, 4, 8 rows), and the
+// 32-entry traversal stack (when the tree is shallow enough).  Every variant returns the same hits (up to exact ties), so tuning changes speed only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -159,12 +159,20 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
     const bvhc_traversal_config base = chosen[k];
     if (base.persistent == 0 || (base.persistent == 2 && base.wide)) continue;
     std::vector<bvhc_traversal_config> more{base};
-    if (base.persistent == 2)
+    if (base.persistent == 2) {
       for (int block : {64, 256}) {
         bvhc_traversal_config c = base;
         c.block = block;
         more.push_back(c);
       }
+      // a tiled order's other tile heights (2 x 16, 8 x 4) where the row pitch allows them
+      for (int rows : {2, 8})
+        if (base.tile && base.tile % (32 / rows) == 0) {
+          bvhc_traversal_config c = base;
+          c.tile_rows = rows;
+          more.push_back(c);
+        }
+    }
     float ref_ms = 0.0f;
     for (size_t j = 0; j < more.size() && st == BVHC_OK; ++j) {
       float ms = 0.0f;

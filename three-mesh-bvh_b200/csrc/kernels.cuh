@@ -31,6 +31,9 @@ cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n
                                  float near_d, float far_d, bvhc_hit* out, int order, cudaStream_t stream);
 // Traversal variant chosen per call (autotuned): persistent vs one-ray-per-thread grid, child
 // order, and the number of idle lanes that triggers a warp refill.
+// log2 of a tiled order's rows per tile (tile_rows 2, 4 or 8; 0 means 4).
+inline int tile_rows_log2(int rows) { return rows == 2 ? 1 : rows == 8 ? 3 : 2; }
+
 struct TraversalConfig {
   int persistent;  // 1: persistent warps with lane refill; 0: one ray per thread; 2: warp-cooperative
   int order;       // 0: split-axis direction sign (reference order); 1: nearest entry first
@@ -48,10 +51,11 @@ struct TraversalConfig {
                    // thread over the rays that enter the tree (6..8 sorted by key kind all - 5), 9..12
                    // the same with persistent warps and lane refill (10..12 sorted by key all - 9)
   int tile;        // warp-cooperative raycastFirst without a queue: 0 consecutive rays per warp; a
-                   // multiple of 8 takes 4 x 8 tiles of the rays read as rows of `tile` rays
+                   // multiple of 8 takes R x 32/R tiles of the rays read as rows of `tile` rays
   int block;       // warp-cooperative raycastFirst threads per block: 64, 256, else 128
   int stack;       // raycastFirst traversal stack entries (warp-cooperative and persistent forms): 32
                    // when the tree allows it, else 64
+  int tile_rows;   // R of the tiled order: 2, 4 or 8 (0: 4)
 };
 
 // Scratch of the ray-ordering sort for up to n queued rays (raysort.cu).
@@ -114,12 +118,13 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
 // n rays required, else variant 0 runs); 5: one ray per thread over the rays the root-box pre-pass
 // queues (queue and qcount for n rays required; sorted by sort->kind when given); 9: the same
 // queue walked by persistent warps with lane refill (also a zeroed-per-call work counter).  `tile`
-// (variant 1): the warp-cooperative walk takes 4 x 8 tiles of rays read as rows of `tile` rays.
+// (variant 1): the warp-cooperative walk takes tile_rows x 32/tile_rows tiles of rays read as rows
+// of `tile` rays.
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream, int variant = 0, int occupancy = 0, uint32_t* queue = nullptr,
                                unsigned int* qcount = nullptr, const RaySort* sort = nullptr,
-                               unsigned long long* work = nullptr, uint32_t tile = 0);
+                               unsigned long long* work = nullptr, uint32_t tile = 0, int tile_rows = 0);
 
 // intersectsSphere: spheres n x 4 (centre, radius), 16-byte aligned; out[i] = 1 if the mesh meets
 // sphere i.

@@ -209,7 +209,7 @@ template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
     MeshDev m, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides, float near_d,
     float far_d, uint32_t cap, uint32_t* __restrict__ counts, bvhc_hit* __restrict__ hits,
-    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount, uint64_t pitch) {
+    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount, uint64_t pitch, int rows_log2) {
   __shared__ uint32_t s_link[kWarps][kMaxStack];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n_work;
   if (valid && queue) i = __ldg(queue + i);
-  else if (valid && pitch) i = tiled_index(i, pitch, n);  // 4 x 8 tiles of per-pixel rays
+  else if (valid && pitch) i = tiled_index(i, pitch, rows_log2, n);  // tiles of per-pixel rays
   RayF r;
   if (valid) {
     r = make_ray(rays, i);
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
 cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                float near_d, float far_d, uint32_t cap, uint32_t* counts, bvhc_hit* hits,
                                cudaStream_t stream, int variant, int occupancy, uint32_t* queue, unsigned int* qcount,
-                               const RaySort* sort, unsigned long long* work, uint32_t tile) {
+                               const RaySort* sort, unsigned long long* work, uint32_t tile, int tile_rows) {
   if (n == 0) return cudaSuccess;
   if (variant == 0 || (variant == 2 && (!queue || !qcount || !sort || n >= (1ull << 32))) ||
       ((variant == 5 || variant == 9) && (!queue || !qcount || n >= (1ull << 32)))) {
@@ -363,9 +363,10 @@ cudaError_t launch_raycast_all(const MeshDev& m, const float* rays, uint64_t n, 
   auto kernel = occupancy == 0   ? dev::raycast_all_packet_kernel<1>
                 : occupancy == 1 ? dev::raycast_all_packet_kernel<6>
                                  : dev::raycast_all_packet_kernel<8>;
-  const uint64_t pitch = (!queue && tile >= 8 && tile % 8 == 0) ? (uint64_t)tile : 0;
+  const int rl = tile_rows_log2(tile_rows);
+  const uint64_t pitch = (!queue && tile >= 8 && tile % (32u >> rl) == 0) ? (uint64_t)tile : 0;
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, cap, counts, hits, queue,
-                                                  qcount, pitch);
+                                                  qcount, pitch, rl);
   return cudaGetLastError();
 }
 

@@ -27,19 +27,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) raycast_first_packet_kernel(MeshD
                                                                      bvhc_hit* __restrict__ out,
                                                                      const uint32_t* __restrict__ queue,
                                                                      const unsigned int* __restrict__ qcount,
-                                                                     uint64_t pitch) {
+                                                                     uint64_t pitch, int rows_log2) {
   __shared__ uint32_t s_link[BLOCK / 32][STACK];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
   // with a queue (root-box pre-pass, optionally sorted) a warp takes 32 consecutive queue entries;
-  // without one, 32 consecutive rays or (pitch > 0) a 4 x 8 tile of them
+  // without one, 32 consecutive rays or (pitch > 0) a tile of them
   const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
   const bool valid = i < n_work;
   if (valid && queue) i = __ldg(queue + i);
-  else if (valid && pitch) i = tiled_index(i, pitch, n);
+  else if (valid && pitch) i = tiled_index(i, pitch, rows_log2, n);
   RayF r;
   float dlen = 1.0f;
   if (valid) {
@@ -246,7 +246,7 @@ template <int BLOCK, int STACK>
 static void launch_packet_kernel(const MeshDev& m, const float* rays, uint64_t n, int side, const SideTable& sides,
                                  float near_d, float far_d, bvhc_hit* out, int order, int occupancy,
                                  cudaStream_t stream, const uint32_t* queue, const unsigned int* qcount,
-                                 uint64_t pitch) {
+                                 uint64_t pitch, int rows_log2) {
   // occupancy 1 / 2 ask for 768 / 1024 resident threads per SM whatever the block size
   constexpr int k6 = 6 * 128 / BLOCK, k8 = 8 * 128 / BLOCK;
   auto kernel = order == 0 ? (occupancy == 0   ? dev::raycast_first_packet_kernel<0, 1, BLOCK, STACK>
@@ -256,7 +256,7 @@ static void launch_packet_kernel(const MeshDev& m, const float* rays, uint64_t n
                               : occupancy == 1 ? dev::raycast_first_packet_kernel<1, k6, BLOCK, STACK>
                                                : dev::raycast_first_packet_kernel<1, k8, BLOCK, STACK>);
   const unsigned int grid = (unsigned int)((n + BLOCK - 1) / BLOCK);
-  kernel<<<grid, BLOCK, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount, pitch);
+  kernel<<<grid, BLOCK, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount, pitch, rows_log2);
 }
 
 cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uint64_t n, int side,
@@ -280,12 +280,13 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
     return cudaGetLastError();
   }
   // the tiled order applies to the whole ray range (a queue is already in its own order)
-  const uint64_t pitch = (!queue && cfg.tile >= 8 && cfg.tile % 8 == 0) ? (uint64_t)cfg.tile : 0;
+  const int rl = tile_rows_log2(cfg.tile_rows);
+  const uint64_t pitch = (!queue && cfg.tile >= 8 && cfg.tile % (32 >> rl) == 0) ? (uint64_t)cfg.tile : 0;
   const bool s32 = stack_entries(m, cfg.stack) == 32;
   const int block = cfg.block == 64 || cfg.block == 256 ? cfg.block : 128;
 #define BVHC_PACKET(B, S) \
   launch_packet_kernel<B, S>(m, rays, n, side, sides, near_d, far_d, out, cfg.order, cfg.occupancy, stream, queue, \
-                             qcount, pitch)
+                             qcount, pitch, rl)
   if (block == 64) {
     if (s32) BVHC_PACKET(64, 32);
     else BVHC_PACKET(64, 64);

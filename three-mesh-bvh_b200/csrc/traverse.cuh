@@ -246,17 +246,18 @@ __device__ __forceinline__ bool left_first(const Pair& p, const RayF& r, float e
 }
 
 
-// Tiled ray order: the ray index space read as rows of `pitch` rays (pitch a multiple of 8), cut
-// into bands of 4 rows; work item i of a band is the ray at row (i mod 32) / 8, column
-// 8 (i / 32) + i mod 8 of that band, so each warp takes a 4 x 8 tile.  For rays generated per pixel
-// in row-major order with pitch = the image width, that is a 4 x 8 pixel block.  Items past the
-// last whole band keep their own index.  A bijection of [0, n): for i below the last whole band
-// the row is at most 3 and the column at most pitch - 1, so the ray stays in i's band.
-__device__ __forceinline__ uint64_t tiled_index(uint64_t i, uint64_t pitch, uint64_t n) {
-  const uint64_t band = 4 * pitch;
+// Tiled ray order: the ray index space read as rows of `pitch` rays, cut into bands of R = 2^rl
+// rows; work item i of a band is the ray at row (i mod 32) / C, column C (i / 32) + i mod C of that
+// band with C = 32 / R (pitch a multiple of C), so each warp takes an R x C tile.  For rays
+// generated per pixel in row-major order with pitch = the image width, that is an R x C pixel
+// block.  Items past the last whole band keep their own index.  A bijection of [0, n): for i below
+// the last whole band the row is below R and the column below pitch, so the ray stays in i's band.
+__device__ __forceinline__ uint64_t tiled_index(uint64_t i, uint64_t pitch, int rl, uint64_t n) {
+  const int cl = 5 - rl;
+  const uint64_t band = pitch << rl;
   if (i >= n - n % band) return i;
   const uint64_t b = i / band, r = i - b * band;
-  return b * band + ((r & 31u) >> 3) * pitch + ((r >> 5) << 3) + (r & 7u);
+  return b * band + ((r & 31u) >> cl) * pitch + ((r >> 5) << cl) + (r & ((1u << cl) - 1u));
 }
 
 // Pre-pass tiles (classify_kernel, kernels_first.cu).

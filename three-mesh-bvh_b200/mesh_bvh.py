@@ -218,10 +218,10 @@ class MeshBVH:
 
     def set_traversal(self, persistent: int = 1, order: int = 1, refill: int = 16, occupancy: int = 0,
                       compact: int = 0, sort: int = 0, closest: int = 0, wide: int = 0, all: int = 0,
-                      tile: int = 0, block: int = 0, stack: int = 0) -> None:
+                      tile: int = 0, block: int = 0, stack: int = 0, tile_rows: int = 0) -> None:
         """Select the traversal variants (see bvhc_mesh_set_traversal)."""
         cfg = N.BvhcTraversalConfig(persistent, order, refill, occupancy, compact, sort, closest, wide, all, tile,
-                                    block, stack)
+                                    block, stack, tile_rows)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
     def get_traversal(self) -> dict:
