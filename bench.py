@@ -250,7 +250,7 @@ def all_hits_launches(variant):
     """Kernels one raycast (all hits) call launches: the traversal, plus for the queue variants the
     root-box pre-pass and, when the queue is sorted, 3 kernels per radix pass (4 passes for the
     direction key, 3 for the others)."""
-    if variant in (0, 1, "1t"):
+    if variant in (0, 1, "1t", "1t2", "1t8"):
         return 1
     v = int(variant)
     kind = {2: 1, 3: 2, 4: 3, 6: 1, 7: 2, 8: 3, 10: 1, 11: 2, 12: 3}.get(v, 0)
@@ -799,9 +799,11 @@ def run_all_hits(args, ws, rank, local):
 
             # the all-hits kernel variant for this set (one call each, on the same buffers)
             # the all-hits kernels, and the warp-cooperative one in tiled order with the camera's
-            # row pitch ("1t")
+            # row pitch ("1t": 4-row tiles, "1t2" / "1t8": 2 / 8 rows)
             t_var, settings = {}, {v: {"all": v} for v in range(13)}
             settings["1t"] = {"all": 1, "tile": args.camera}
+            settings["1t2"] = {"all": 1, "tile": args.camera, "tile_rows": 2}
+            settings["1t8"] = {"all": 1, "tile": args.camera, "tile_rows": 8}
             for v, kw in settings.items():
                 bvh.set_traversal(**{**cur, **kw})
                 call()
@@ -853,6 +855,7 @@ def run_all_hits(args, ws, rank, local):
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "peak_source": how, "ray_set": sets[k][0],
                 "kernel": {0: "raycast_all_kernel", 1: "raycast_all_packet_kernel", "1t": "raycast_all_packet_kernel",
+                           "1t2": "raycast_all_packet_kernel", "1t8": "raycast_all_packet_kernel",
                            2: "raycast_all_packet_kernel", 3: "raycast_all_packet_kernel",
                            4: "raycast_all_packet_kernel"}.get(variants[sets[k][0]]["best"],
                                                               "raycast_all_persistent_kernel"
