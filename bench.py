@@ -695,9 +695,11 @@ def run_closest(args, ws, rank, local):
     bvh.set_traversal(1, 1, 16, 2)   # register budget shared with the warp-cooperative kernels
     if args.closest_variant is not None:
         bvh.set_traversal(1, 1, 16, 2, closest=args.closest_variant)
-        tuned = {"best": args.closest_variant, "forced": True}
+        tuned = {"best": str(args.closest_variant), "setting": {"closest": args.closest_variant}, "forced": True}
     else:
-        tuned = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
+        # the grid's points come row by row (its last axis fastest): its row length is the tiled
+        # order's pitch, as the caller that made the grid would pass it
+        tuned = autotune.tune_closest_point(bvh, pts, 0.0, 5.0, tile_pitches=(args.grid,))
 
     def step():
         lib.bvhc_closest_point_to_point(bvh._device_mesh(), pts.data_ptr(), n, 0.0, 5.0, out.data_ptr(), 1, s)
@@ -744,7 +746,7 @@ def run_closest(args, ws, rank, local):
                 "traffic": None, "peak_source": how, "algorithmic_bytes_per_launch": n * per_query,
                 "reference_node_reads_per_query": float(nn.mean()),
                 "reference_triangle_tests_per_query": float(nt.mean()),
-                "kernel": "closest_point_kernel" if tuned["best"] == 0 else "closest_point_packet_kernel"}
+                "kernel": "closest_point_kernel" if tuned["setting"]["closest"] == 0 else "closest_point_packet_kernel"}
         prof = "closest_point_k3.md"
         roof["issue"] = {"source": f"profiles/{prof}",
                          "warp_instructions_per_query": profile_value(prof, "warp_instructions_per_query"),
@@ -760,7 +762,7 @@ def run_closest(args, ws, rank, local):
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
                         "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
-                "gpu_launches": args.steps * (11 if tuned["best"] == 2 else 1)}
+                "gpu_launches": args.steps * (11 if tuned["setting"]["closest"] == 2 else 1)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 
@@ -911,7 +913,7 @@ def measure_adjoint(args, ws, rank, local):
     tuned_ray = autotune.tune_raycast_first_sets(bvh, [("camera1024", rays)], leaf_sizes=(0, 2, 4), tag="adjoint",
                                                  tile_pitches=(1024,))
     bvh.set_traversal(*tuned_ray["sets"]["camera1024"]["best"])
-    tuned_cp = autotune.tune_closest_point(bvh, pts, 0.0, 5.0)
+    tuned_cp = autotune.tune_closest_point(bvh, pts, 0.0, 5.0, tile_pitches=(128,))
 
     def fwd():
         return bvh.raycast_first_batch(rays, stream=s)

@@ -12,8 +12,8 @@
   variant traces the whole set, a strided quarter is checked per variant and the whole set for
   the default variant and the host-memory path.
 * closestPointToPoint on the 256^3 grid over that knot's box padded by 10%, maxThreshold 5: every
-  kernel on the whole grid, byte-identical across kernels, a strided 2^20-query sample against the
-  oracle.
+  kernel (and the tiled query orders) on the whole grid, byte-identical across them, a strided
+  2^20-query sample against the oracle.
 
 Tolerances are tests/parity.py's (faceIndex / hit-miss identical except 1e-6 t ties; distance,
 point, barycentrics within 1e-5 relative; closest-point distance within 1e-5 relative).
@@ -251,15 +251,17 @@ def test_knot80k_closest_point_grid256(knot80k_full, orc, cuda):
     assert pts.shape[0] == 1 << 24
     d = torch.from_numpy(pts).to(cuda)
     results = {}
-    for closest in (0, 1, 2):
-        bvh.set_traversal(1, 1, 16, 2, 0, 0, closest)
-        results[closest] = bvh.closest_point_batch(d, 0.0, 5.0).contiguous().view(torch.int32).clone()
+    forms = {0: {}, 1: {}, 2: {}, "1t2": dict(tile=256, tile_rows=2), "1t4": dict(tile=256),
+             "1t8": dict(tile=256, tile_rows=8)}
+    for name, kw in forms.items():
+        bvh.set_traversal(1, 1, 16, 2, 0, 0, 1 if isinstance(name, str) else name, **kw)
+        results[name] = bvh.closest_point_batch(d, 0.0, 5.0).contiguous().view(torch.int32).clone()
         bvh.synchronize()
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
-    # every kernel gives the same bytes on every query (exact distance ties go to the earlier
-    # triangle in leaf order, whatever the traversal order)
-    for closest in (1, 2):
-        assert torch.equal(results[closest], results[0]), closest
+    # every kernel and query order gives the same bytes on every query (exact distance ties go to
+    # the earlier triangle in leaf order, whatever the traversal order)
+    for name in forms:
+        assert torch.equal(results[name], results[0]), name
     stride = 16
     idx = np.arange(0, pts.shape[0], stride)
     got = _rows(results[2][::stride], CLOSEST)

@@ -1664,13 +1664,15 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
     BVHC_CUDA_TRY(closest_sort(m, 3, n, min_threshold, &q, &qc, &sort));
     if (mem == BVHC_MEM_DEVICE)
       return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s, variant,
-                                            m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+                                            m->cfg.occupancy, q, qc, q ? &sort : nullptr, (uint32_t)m->cfg.tile,
+                                            m->cfg.tile_rows));
     BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
     BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
     BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold,
                                        max_threshold, static_cast<bvhc_closest*>(m->d_out), s, variant,
-                                       m->cfg.occupancy, q, qc, q ? &sort : nullptr));
+                                       m->cfg.occupancy, q, qc, q ? &sort : nullptr, (uint32_t)m->cfg.tile,
+                                       m->cfg.tile_rows));
     BVHC_CUDA_TRY(cudaMemcpyAsync(out, m->d_out, n * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, s));
     return read_and_clear_error(m, s);
   }
@@ -1697,7 +1699,8 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], points + 3 * off, cnt * 12, cudaMemcpyHostToDevice, st));
     BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->slot_in[k]), cnt, min_threshold,
                                        max_threshold, static_cast<bvhc_closest*>(m->slot_out[k]), st, variant,
-                                       m->cfg.occupancy, qs[k], qcs[k], qs[k] ? &sorts[k] : nullptr));
+                                       m->cfg.occupancy, qs[k], qcs[k], qs[k] ? &sorts[k] : nullptr,
+                                       (uint32_t)m->cfg.tile, m->cfg.tile_rows));
     BVHC_CUDA_TRY(
         cudaMemcpyAsync(out + off, m->slot_out[k], cnt * sizeof(bvhc_closest), cudaMemcpyDeviceToHost, st));
   }

@@ -108,10 +108,11 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
 // closestPointToPoint.  variant 0: one query per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the queries sorted by a Morton key of the point (queue, qcount and sort
 // scratch for n queries required).  Variants 1 and 2 apply only with min_t <= 0 (else variant 0).
+// Variant 1 reads the queries in tiled order when `tile` is a row length (see tiled_index).
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream, int variant = 0, int occupancy = 0,
                                  uint32_t* queue = nullptr, unsigned int* qcount = nullptr,
-                                 const RaySort* sort = nullptr);
+                                 const RaySort* sort = nullptr, uint32_t tile = 0, int tile_rows = 0);
 
 // raycast (all hits).  variant 0: one ray per thread; 1: warp-cooperative in input order; 2:
 // warp-cooperative over the rays sorted by the key sort->kind (queue, qcount and sort scratch for

@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
     MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
-    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount) {
+    const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount, uint64_t pitch, int rows_log2) {
   __shared__ uint32_t s_link[kBlock / 32][kMaxStack];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
@@ -266,6 +266,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n_work;
   if (valid && queue) i = __ldg(queue + i);
+  else if (valid && pitch) i = tiled_index(i, pitch, rows_log2, n);  // tiles of grid points
   float3 p = make_float3(0.f, 0.f, 0.f);
   if (valid) p = make_float3(__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2));
   const ff max2 = two_prod(max_t, max_t);
@@ -1152,7 +1153,7 @@ __global__ void __launch_bounds__(kBlock) shape_key_kernel(const float* __restri
 
 cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n, float min_t, float max_t,
                                  bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
-                                 unsigned int* qcount, const RaySort* sort) {
+                                 unsigned int* qcount, const RaySort* sort, uint32_t tile, int tile_rows) {
   if (n == 0) return cudaSuccess;
   // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 2 runs over
   // Morton-sorted queries
@@ -1180,7 +1181,10 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
   auto kernel = occupancy == 0   ? dev::closest_point_packet_kernel<1>
                 : occupancy == 1 ? dev::closest_point_packet_kernel<6>
                                  : dev::closest_point_packet_kernel<8>;
-  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount);
+  // input order (variant 1) may be read in tiles: rows of `tile` points (a grid's row), 2-D blocks
+  const int rl = tile_rows_log2(tile_rows);
+  const uint64_t pitch = (!queue && tile >= 8 && tile % (32u >> rl) == 0) ? (uint64_t)tile : 0;
+  kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount, pitch, rl);
   return cudaGetLastError();
 }
 
