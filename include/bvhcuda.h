@@ -208,8 +208,8 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config
  * without the root-box compaction and each ordering key; register budgets; the tiled ray order for
  * each row pitch in tile_pitches, e.g. an image width) for every device leaf layout in leaf_sizes
  * (NULL / 0: the current one); the layout with the smallest sum of the sets' best times wins.
- * Stage 2: threads per block, the tiled order's tile height and the 32-entry stack around each
- * set's best.  Each variant is run
+ * Stage 2: threads per block, the tiled order's tile height, the persistent form's refill
+ * threshold and the 32-entry stack around each set's best.  Each variant is run
  * once untimed, then `reps` times.  Outputs: best[k] and best_ms[k] per set (best_ms nullable),
  * the chosen layout (nullable) and each layout's total (leaf_total_ms[n_leaf_sizes], nullable).
  * The mesh is left with the chosen layout and set 0's variant; callers switch variants per set

@@ -95,8 +95,8 @@ def _first_sample(bvh, d, stride):
 
 def _stage2(cands):
     """The autotuner's stage-2 forms of its stage-1 candidates: threads per block 64 / 256 for the
-    warp-cooperative form over child pairs, its tiled order's other tile heights (2, 8 rows), and
-    the 32-entry stack for it and the persistent form."""
+    warp-cooperative form over child pairs, its tiled order's other tile heights (2, 8 rows), the
+    persistent form's refill thresholds 8 / 24, and the 32-entry stack for both forms."""
     out = []
     for c in cands:
         if c[0] == 2 and not c[7]:
@@ -104,7 +104,7 @@ def _stage2(cands):
             if c[9] and c[9] % 16 == 0:
                 out += [c[:10] + [0, 32, 2], c[:10] + [0, 0, 8]]
         elif c[0] == 1:
-            out.append(c[:10] + [0, 32, 0])
+            out += [c[:10] + [0, 32, 0], [c[0], c[1], 8] + c[3:10] + [0, 0, 0], [c[0], c[1], 24] + c[3:10] + [0, 32, 0]]
     return out
 
 

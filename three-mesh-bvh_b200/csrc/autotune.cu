@@ -5,8 +5,9 @@
 // Stage 1 times every candidate of the list below on each ray set, for each device leaf layout
 // asked for; the layout with the smallest sum of the sets' best times is kept.  Stage 2 refines
 // each set's best warp-cooperative or persistent candidate on that layout: threads per block (64,
-// 128, 256; warp-cooperative form), the tile height of a tiled order (2, 4, 8 rows), and the
-// 32-entry traversal stack (when the tree is shallow enough).  Every variant returns the same hits (up to exact ties), so tuning changes speed only.
+// 128, 256; warp-cooperative form), the tile height of a tiled order (2, 4, 8 rows), the refill
+// threshold (8, 24; persistent form), and the 32-entry traversal stack (when the tree is shallow
+// enough).  Every variant returns the same hits (up to exact ties), so tuning changes speed only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -159,6 +160,13 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
     const bvhc_traversal_config base = chosen[k];
     if (base.persistent == 0 || (base.persistent == 2 && base.wide)) continue;
     std::vector<bvhc_traversal_config> more{base};
+    if (base.persistent == 1)
+      for (int refill : {8, 24})  // the refill thresholds between and below stage 1's 16 and 32
+        if (refill != base.refill) {
+          bvhc_traversal_config c = base;
+          c.refill = refill;
+          more.push_back(c);
+        }
     if (base.persistent == 2) {
       for (int block : {64, 256}) {
         bvhc_traversal_config c = base;
