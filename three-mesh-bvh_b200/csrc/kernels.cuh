@@ -63,7 +63,8 @@ struct RaySortScratch {
   uint32_t* keys[2];  // n entries each
   uint32_t* vals;     // n entries: the queue's ping-pong partner
   uint32_t* hist;     // 256 * ray_sort_tiles(n) entries
-  uint32_t* totals;   // 4 * 256 entries (one row per pass)
+  uint32_t* totals;   // 4 * 256 entries (one row per pass; the closest-point sort, three passes,
+                      // keeps its query box in the last row)
 };
 
 // A sort request: key kind (1..3, raykey.cuh) and the scene box used by the entry-point keys.

@@ -1098,14 +1098,58 @@ __global__ void __launch_bounds__(kBlock) intersects_box_kernel(MeshDev m, const
   out[i] = hit ? 1 : 0;
 }
 
-// Morton key of each query point over the scene box (8 bits per axis), ids in input order, and the
-// queue length; the queue is then sorted by key so that a warp takes 32 nearby points.
-__global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n, SceneBox box,
+// Float bits mapped to unsigned integers that order as the floats do (negatives reversed below the
+// positives), so that atomicMin / atomicMax on them give the float minimum / maximum.
+__device__ __forceinline__ unsigned ordered_bits(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered_bits(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+constexpr int kBoxThreads = 256;
+
+// Bounding box of the query points (finite coordinates only) into qbox[0..2] (minimum) and
+// qbox[3..5] (maximum) as ordered bits; qbox starts as 0xFFFFFFFF (minimum) and 0 (maximum).
+__global__ void __launch_bounds__(kBoxThreads) points_box_kernel(const float* __restrict__ pts, uint64_t n,
+                                                                 unsigned* __restrict__ qbox) {
+  unsigned lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    for (int a = 0; a < 3; ++a) {
+      const float v = __ldg(pts + 3 * i + a);
+      if (!isfinite(v)) continue;
+      const unsigned u = ordered_bits(v);
+      lo[a] = min(lo[a], u);
+      hi[a] = max(hi[a], u);
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    const unsigned l = __reduce_min_sync(0xFFFFFFFFu, lo[a]), h = __reduce_max_sync(0xFFFFFFFFu, hi[a]);
+    if ((threadIdx.x & 31u) == 0) {
+      atomicMin(qbox + a, l);
+      atomicMax(qbox + 3 + a, h);
+    }
+  }
+}
+
+// Morton key of each query point over the query points' own box (8 bits per axis), ids in input
+// order, and the queue length; the queue is then sorted by key so that a warp takes 32 nearby
+// points.  (Over the mesh's box instead, the queries outside it -- a quarter of a grid padded by
+// 10% -- would share clamped keys along every face and keep their input order.)
+__global__ void __launch_bounds__(kBlock) point_key_kernel(const float* __restrict__ pts, uint64_t n,
+                                                          const unsigned* __restrict__ qbox,
                                                           uint32_t* __restrict__ ids, uint32_t* __restrict__ keys,
                                                           unsigned int* __restrict__ qcount) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *qcount = (unsigned int)n;
   if (i >= n) return;
+  SceneBox box;
+  for (int a = 0; a < 3; ++a) {
+    const unsigned l = __ldg(qbox + a), h = __ldg(qbox + 3 + a);
+    box.lo[a] = l <= h ? from_ordered_bits(l) : 0.0f;
+    box.hi[a] = l <= h ? from_ordered_bits(h) : 0.0f;
+  }
   float sx = box.hi[0] > box.lo[0] ? 1.0f / (box.hi[0] - box.lo[0]) : 0.0f;
   float sy = box.hi[1] > box.lo[1] ? 1.0f / (box.hi[1] - box.lo[1]) : 0.0f;
   float sz = box.hi[2] > box.lo[2] ? 1.0f / (box.hi[2] - box.lo[2]) : 0.0f;
@@ -1166,12 +1210,15 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
   if (sorted) {
     uint32_t *ids, *keys;
     ray_sort_input(2, sort->scratch, queue, &ids, &keys);
-    dev::SceneBox box{};
-    for (int a = 0; a < 3; ++a) {
-      box.lo[a] = sort->lo[a];
-      box.hi[a] = sort->hi[a];
-    }
-    dev::point_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(pts, n, box, ids, keys, qcount);
+    // the query points' box, in the last row of the sort's digit totals (a three-pass sort leaves
+    // it unused), then the keys over it
+    unsigned* qbox = sort->scratch.totals + 3 * 256;
+    if ((e = cudaMemsetAsync(qbox, 0xFF, 3 * sizeof(unsigned), stream)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(qbox + 3, 0, 3 * sizeof(unsigned), stream)) != cudaSuccess) return e;
+    const unsigned int gb = (unsigned int)std::min<uint64_t>((n + dev::kBoxThreads - 1) / dev::kBoxThreads, 2048);
+    dev::points_box_kernel<<<gb, dev::kBoxThreads, 0, stream>>>(pts, n, qbox);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    dev::point_key_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(pts, n, qbox, ids, keys, qcount);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = launch_ray_sort(2, n, qcount, sort->scratch, queue, stream)) != cudaSuccess) return e;
   } else {
