@@ -51,7 +51,11 @@ def parse():
                          "shapecast: triangles within spheres, intersectsSphere, intersectsBox")
     ap.add_argument("--grid", type=int, default=256, help="closest workload: grid resolution per axis")
     ap.add_argument("--closest-variant", type=int, default=None,
-                    help="closest workload: force closestPointToPoint's kernel (0..2) instead of tuning")
+                    help="closest workload: force closestPointToPoint's kernel instead of tuning "
+                         "(with --closest-tile-rows: tiled order)")
+    ap.add_argument("--closest-tile-rows", type=int, default=0,
+                    help="closest workload, with --closest-variant 1: read the grid in tiles of this many "
+                         "rows (2, 4, 8) of --grid points")
     ap.add_argument("--batch-meshes", type=int, default=1024)
     ap.add_argument("--tubular", type=int, default=2000)
     ap.add_argument("--radial", type=int, default=500)
@@ -694,8 +698,11 @@ def run_closest(args, ws, rank, local):
 
     bvh.set_traversal(1, 1, 16, 2)   # register budget shared with the warp-cooperative kernels
     if args.closest_variant is not None:
-        bvh.set_traversal(1, 1, 16, 2, closest=args.closest_variant)
-        tuned = {"best": str(args.closest_variant), "setting": {"closest": args.closest_variant}, "forced": True}
+        kw = {"closest": args.closest_variant}
+        if args.closest_tile_rows:
+            kw.update(tile=args.grid, tile_rows=args.closest_tile_rows)
+        bvh.set_traversal(1, 1, 16, 2, **kw)
+        tuned = {"best": str(args.closest_variant), "setting": kw, "forced": True}
     else:
         # the grid's points come row by row (its last axis fastest): its row length is the tiled
         # order's pitch, as the caller that made the grid would pass it
@@ -762,7 +769,7 @@ def run_closest(args, ws, rank, local):
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
                         "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
-                "gpu_launches": args.steps * (11 if tuned["setting"]["closest"] == 2 else 1)}
+                "gpu_launches": args.steps * (11 if tuned["setting"]["closest"] in (2, 4, 6) else 1)}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 

@@ -305,12 +305,17 @@ def test_split_leaf_layouts_agree(pkg, orc, cuda, leaf):
     bvh.dispose()
 
 
-@pytest.mark.parametrize("closest,occupancy", [(1, 0), (1, 2), (2, 0), (2, 2)])
-def test_closest_point_warp_cooperative(pkg, orc, knot80k, closest, occupancy):
-    """The warp-cooperative closest-point kernels (input order and Morton-sorted queries) against the
-    oracle: grid queries with maxThreshold 5 (nulls beyond it), unbounded, and a sparse random set;
-    minThreshold > 0 falls back to the per-query kernel and must match too."""
+@pytest.mark.parametrize("closest,occupancy,leaf", [(1, 0, 0), (1, 2, 0), (2, 0, 0), (2, 2, 0), (1, 0, 4), (3, 0, 0),
+                                                    (4, 2, 2), (5, 1, 0), (6, 0, 0), (6, 2, 3)])
+def test_closest_point_warp_cooperative(pkg, orc, knot80k, closest, occupancy, leaf):
+    """The warp-cooperative closest-point kernels (input order and Morton-sorted queries, whole warps
+    and 16- or 8-lane groups; with and without raycastFirst's split-leaf copy present, which closest
+    point does not read) against the
+    oracle: grid queries with maxThreshold 5 (nulls beyond it, and results beyond it from leaves
+    whose box is within it), unbounded, and a sparse random set; minThreshold > 0 falls back to the
+    per-query kernel and must match too."""
     geo, bvh, ref = knot80k
+    bvh.set_leaf_size(leaf)
     bvh.set_traversal(1, 1, 16, occupancy, 0, 0, closest)
     rng = np.random.default_rng(21)
     lo, hi = geo.position.min(0), geo.position.max(0)
@@ -333,6 +338,7 @@ def test_closest_point_warp_cooperative(pkg, orc, knot80k, closest, occupancy):
             if lo_t == 0.0:
                 assert rep["distance"] == 0, (lo_t, hi_t, rep)
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
+    bvh.set_leaf_size(0)
 
 
 @pytest.mark.parametrize("leaf,occupancy,compact,sort", [(0, 0, 0, 0), (0, 2, 1, 1), (4, 1, 1, 2), (2, 2, 0, 0),
@@ -362,14 +368,15 @@ def test_wide_warp_cooperative_raycast_first(pkg, orc, cuda, leaf, occupancy, co
     bvh.dispose()
 
 
-@pytest.mark.parametrize("closest", [0, 1, 2])
-def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
+@pytest.mark.parametrize("closest,leaf", [(0, 0), (1, 0), (2, 0), (2, 4), (3, 0), (4, 0), (6, 0)])
+def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest, leaf):
     """closestPointToPoint through host memory for more than one pipeline chunk (2.5M points: three
     1M-point chunks on three streams, the last one partial) gives the device-memory call's results,
     and a strided sample of them matches the oracle."""
     import torch
 
     geo, bvh, ref = knot80k
+    bvh.set_leaf_size(leaf)
     bvh.set_traversal(1, 1, 16, 0, 0, 0, closest)
     rng = np.random.default_rng(23)
     lo, hi = geo.position.min(0), geo.position.max(0)
@@ -379,8 +386,8 @@ def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
     torch.cuda.synchronize()
     dev = d.cpu().numpy().view(np.uint8).reshape(-1)
     dev = np.frombuffer(dev.tobytes(), dtype=host.dtype)
-    # byte-identical: exact distance ties go to the earlier triangle in leaf order whatever the
-    # grouping of the queries (chunks, Morton sort per chunk or over the whole call)
+    # byte-identical: exact distance ties go to the smaller faceIndex whatever the grouping of the
+    # queries (chunks, Morton sort per chunk or over the whole call)
     assert np.array_equal(host.view(np.uint8), dev.view(np.uint8))
 
     def tri_distance(p):
@@ -395,19 +402,20 @@ def test_closest_point_host_pipeline(pkg, orc, knot80k, cuda, closest):
     rep = check_closest(host[idx], exp, tri_distance(pts[idx]))
     assert rep["null"] == 0 and rep["face"] == 0 and rep["distance"] == 0, rep
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
+    bvh.set_leaf_size(0)
 
 
 def test_traversal_config_rejects_bad_fields(pkg, cuda):
     """Tile pitches that are not a positive multiple of 8 (of 16 for 2-row tiles), tile heights other
-    than 2 / 4 / 8, block sizes other than 64 / 128 / 256 and stacks other than 32 / 64 are
-    rejected."""
+    than 2 / 4 / 8, block sizes other than 64 / 128 / 256, stacks other than 32 / 64 and
+    closest-point kernels outside 0..6 are rejected."""
     geo = pkg.torus_knot(10, 3, 32, 8)
     bvh = pkg.MeshBVH(geo, {"strategy": pkg.SAH})
     for bad in (dict(tile=12), dict(tile=-8), dict(block=96), dict(stack=48), dict(stack=16), dict(tile_rows=3),
-                dict(tile=24, tile_rows=2)):
+                dict(tile=24, tile_rows=2), dict(closest=7), dict(closest=-1)):
         with pytest.raises(pkg.BVHCError):
             bvh.set_traversal(2, 1, 16, 0, **bad)
-    bvh.set_traversal(2, 1, 16, 2, tile=4096, block=256, stack=32, tile_rows=8)
-    assert bvh.get_traversal() == dict(persistent=2, order=1, refill=16, occupancy=2, compact=0, sort=0, closest=0,
+    bvh.set_traversal(2, 1, 16, 2, tile=4096, block=256, stack=32, tile_rows=8, closest=6)
+    assert bvh.get_traversal() == dict(persistent=2, order=1, refill=16, occupancy=2, compact=0, sort=0, closest=6,
                                        wide=0, all=0, tile=4096, block=256, stack=32, tile_rows=8)
     bvh.dispose()

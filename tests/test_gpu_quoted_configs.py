@@ -251,17 +251,29 @@ def test_knot80k_closest_point_grid256(knot80k_full, orc, cuda):
     assert pts.shape[0] == 1 << 24
     d = torch.from_numpy(pts).to(cuda)
     results = {}
-    forms = {0: {}, 1: {}, 2: {}, "1t2": dict(tile=256, tile_rows=2), "1t4": dict(tile=256),
-             "1t8": dict(tile=256, tile_rows=8)}
+    forms = {0: {}, 1: {}, 2: {}, 3: {}, 4: {}, 5: {}, 6: {}, "1t2": dict(tile=256, tile_rows=2), "1t4": dict(tile=256),
+             "1t8": dict(tile=256, tile_rows=8), "3t4": dict(tile=256), "3t8": dict(tile=256, tile_rows=8),
+             "5t4": dict(tile=256)}
     for name, kw in forms.items():
-        bvh.set_traversal(1, 1, 16, 2, 0, 0, 1 if isinstance(name, str) else name, **kw)
+        bvh.set_traversal(1, 1, 16, 2, 0, 0, int(str(name)[0]), **kw)
         results[name] = bvh.closest_point_batch(d, 0.0, 5.0).contiguous().view(torch.int32).clone()
         bvh.synchronize()
+    # raycastFirst's split-leaf layouts leave closest point on the reference's leaves
+    for leaf in (2, 4):
+        bvh.set_leaf_size(leaf)
+        for name in (2, "1t4"):
+            bvh.set_traversal(1, 1, 16, 2, 0, 0, int(str(name)[0]), **forms[name])
+            results[f"{name}@leaf{leaf}"] = bvh.closest_point_batch(d, 0.0, 5.0).contiguous().view(torch.int32).clone()
+            bvh.synchronize()
+    bvh.set_leaf_size(0)
     bvh.set_traversal(1, 1, 16, 0, 0, 0, 0)
     # every kernel and query order gives the same bytes on every query (exact distance ties go to
-    # the earlier triangle in leaf order, whatever the traversal order)
-    for name in forms:
+    # the smaller faceIndex, whatever the traversal order)
+    for name in results:
         assert torch.equal(results[name], results[0]), name
+    # results beyond maxThreshold: leaves whose box is within it but whose triangles are not
+    dist = results[0].view(torch.float32)[:, 1]
+    assert int(((dist > 5.0) & torch.isfinite(dist)).sum()) > 1000
     stride = 16
     idx = np.arange(0, pts.shape[0], stride)
     got = _rows(results[2][::stride], CLOSEST)

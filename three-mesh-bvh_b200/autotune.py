@@ -128,20 +128,22 @@ def tune_raycast_all(bvh, rays, cap: int = 64, reps: int = 3, candidates=tuple(r
 
 
 def tune_closest_point(bvh, points, min_t: float = 0.0, max_t: float = math.inf, reps: int = 3,
-                       candidates=(0, 1, 2), tile_pitches=()) -> dict:
-    """Time closestPointToPoint's kernels (the `closest` field: per query, warp-cooperative,
-    warp-cooperative over Morton-sorted queries; and the warp-cooperative kernel reading the
-    queries in tiled order for each row length in `tile_pitches`, e.g. a grid's, with 2-, 4- and
-    8-row tiles) on `points` (torch CUDA tensor, n x 3), keeping the mesh's other traversal fields,
-    and install the fastest.  Returns {"best": name, "setting": fields, "timings_ms": ...}."""
+                       candidates=(0, 1, 2, 3, 4, 5, 6), tile_pitches=()) -> dict:
+    """Time closestPointToPoint's kernels (the `closest` field: per query; warp-cooperative in
+    input order and over Morton-sorted queries, with whole warps (1, 2), 16-lane (3, 4) or 8-lane
+    (5, 6) groups; and each input-order form reading the queries in tiled order for each row length
+    in `tile_pitches`, e.g. a grid's, with 2-, 4- and 8-row tiles) on `points` (torch CUDA tensor,
+    n x 3), keeping the mesh's other traversal fields, and install the fastest.
+    Returns {"best": name, "setting": fields, "timings_ms": ...}."""
     import torch
 
     cur = bvh.get_traversal()
     settings = {str(c): {"closest": c, "tile": 0, "tile_rows": 0} for c in candidates}
     for pitch in tile_pitches:
-        for rows in (2, 4, 8):
-            if pitch % (32 // rows) == 0:
-                settings[f"1t{rows}@{pitch}"] = {"closest": 1, "tile": pitch, "tile_rows": rows}
+        for c in (c for c in candidates if c % 2 == 1):
+            for rows in (2, 4, 8):
+                if pitch % (32 // rows) == 0:
+                    settings[f"{c}t{rows}@{pitch}"] = {"closest": c, "tile": pitch, "tile_rows": rows}
     stream = torch.cuda.current_stream(points.device)
     out = torch.empty((points.shape[0], 5), dtype=torch.float32, device=points.device)
     timings = {}

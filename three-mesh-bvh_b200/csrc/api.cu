@@ -76,7 +76,9 @@ struct bvhc_mesh {
   // raycastFirst's own copy of the tree with split leaves (bvhc_mesh_set_leaf_size > 0).  Only
   // raycastFirst uses it: its result does not depend on the grouping of triangles into leaves,
   // while closestPointToPoint's maxThreshold / minThreshold rules and raycast's hit order follow
-  // the reference's leaves, so those queries keep the records above.
+  // the reference's leaves, so those queries keep the records above (closest point on split
+  // leaves, with maxThreshold tested at the reference leaf's level, measured slower on every
+  // kernel form: per-triangle box culling already prunes inside a leaf).
   int leaf_size = 0;
   PairNode* d_nodes_f = nullptr;
   TriRecord* d_tris_f = nullptr;
@@ -248,7 +250,7 @@ struct Converter {
     p.link[0] = ll;
     p.link[1] = lr;
     p.axis = axis;
-    p.pad = 0;
+    p.flags = 0;
     return idx;
   }
 };
@@ -417,7 +419,7 @@ struct LeafSplitter {
     p.link[0] = ll;
     p.link[1] = lr;
     p.axis = (uint32_t)axis;
-    p.pad = 0;
+    p.flags = 0;
     return idx;
   }
 
@@ -1102,7 +1104,7 @@ static bool valid_config(const bvhc_traversal_config* cfg) {
   return cfg && cfg->persistent >= 0 && cfg->persistent <= 2 && (cfg->order == 0 || cfg->order == 1) &&
          cfg->refill >= 1 && cfg->refill <= 32 && cfg->occupancy >= 0 && cfg->occupancy <= 2 &&
          (cfg->compact == 0 || cfg->compact == 1) && cfg->sort >= 0 && cfg->sort <= 3 && cfg->closest >= 0 &&
-         cfg->closest <= 2 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
+         cfg->closest <= 6 && (cfg->wide == 0 || cfg->wide == 1) && cfg->all >= 0 && cfg->all <= 12 &&
          (cfg->tile == 0 || (cfg->tile >= 8 && cfg->tile <= (1 << 24) && cfg->tile % 8 == 0)) &&
          (cfg->tile_rows == 0 || cfg->tile_rows == 2 || cfg->tile_rows == 4 || cfg->tile_rows == 8) &&
          (cfg->tile == 0 || cfg->tile % (32 >> tile_rows_log2(cfg->tile_rows)) == 0) &&
@@ -1624,13 +1626,15 @@ bvhc_status bvhc_sphere_triangles(bvhc_mesh* m, const float* spheres, uint64_t n
   return read_and_clear_error(m, s);
 }
 
-// The warp-cooperative closest-point variant over Morton-sorted queries (closest = 2, minThreshold
-// 0): queue slot `slot` with its sort scratch sized for n queries; nulls for the other variants.
+// The warp-cooperative closest-point variants over Morton-sorted queries (closest = 2, 4 or 6,
+// minThreshold 0): queue slot `slot` with its sort scratch sized for n queries; nulls for the
+// other variants.
 static cudaError_t closest_sort(bvhc_mesh* m, int slot, uint64_t n, float min_threshold, uint32_t** q,
                                 unsigned int** qc, RaySort* sort) {
   *q = nullptr;
   *qc = nullptr;
-  if (m->cfg.closest != 2 || n >= (1ull << 32) || !(min_threshold <= 0.0f)) return cudaSuccess;
+  if (m->cfg.closest <= 0 || m->cfg.closest % 2 != 0 || n >= (1ull << 32) || !(min_threshold <= 0.0f))
+    return cudaSuccess;
   cudaError_t e = ensure(reinterpret_cast<void**>(&m->d_queue[slot]), &m->queue_cap[slot], n * sizeof(uint32_t));
   if (e == cudaSuccess && !m->d_qcount[slot])
     e = cudaMalloc(reinterpret_cast<void**>(&m->d_qcount[slot]), sizeof(unsigned int));
@@ -1656,6 +1660,7 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
   BVHC_CUDA_TRY(cudaSetDevice(m->device));
   if (mem == BVHC_MEM_DEVICE && (!aligned(points, 4) || !aligned(out, 4))) return BVHC_ERR_INVALID_ARGUMENT;
   const int variant = m->cfg.closest;
+  const MeshDev v = m->view();
   uint32_t* q;
   unsigned int* qc;
   RaySort sort{};
@@ -1663,13 +1668,13 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
     // one launch; the sorted variant uses queue slot 3
     BVHC_CUDA_TRY(closest_sort(m, 3, n, min_threshold, &q, &qc, &sort));
     if (mem == BVHC_MEM_DEVICE)
-      return from_cuda(launch_closest_point(m->view(), points, n, min_threshold, max_threshold, out, s, variant,
+      return from_cuda(launch_closest_point(v, points, n, min_threshold, max_threshold, out, s, variant,
                                             m->cfg.occupancy, q, qc, q ? &sort : nullptr, (uint32_t)m->cfg.tile,
                                             m->cfg.tile_rows));
     BVHC_CUDA_TRY(ensure(&m->d_in, &m->in_cap, n * 12));
     BVHC_CUDA_TRY(ensure(&m->d_out, &m->out_cap, n * sizeof(bvhc_closest)));
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->d_in, points, n * 12, cudaMemcpyHostToDevice, s));
-    BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->d_in), n, min_threshold,
+    BVHC_CUDA_TRY(launch_closest_point(v, static_cast<const float*>(m->d_in), n, min_threshold,
                                        max_threshold, static_cast<bvhc_closest*>(m->d_out), s, variant,
                                        m->cfg.occupancy, q, qc, q ? &sort : nullptr, (uint32_t)m->cfg.tile,
                                        m->cfg.tile_rows));
@@ -1697,7 +1702,7 @@ bvhc_status bvhc_closest_point_to_point(bvhc_mesh* m, const float* points, uint6
     const uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
     cudaStream_t st = m->pipe[k];
     BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], points + 3 * off, cnt * 12, cudaMemcpyHostToDevice, st));
-    BVHC_CUDA_TRY(launch_closest_point(m->view(), static_cast<const float*>(m->slot_in[k]), cnt, min_threshold,
+    BVHC_CUDA_TRY(launch_closest_point(v, static_cast<const float*>(m->slot_in[k]), cnt, min_threshold,
                                        max_threshold, static_cast<bvhc_closest*>(m->slot_out[k]), st, variant,
                                        m->cfg.occupancy, qs[k], qcs[k], qs[k] ? &sorts[k] : nullptr,
                                        (uint32_t)m->cfg.tile, m->cfg.tile_rows));
@@ -1890,7 +1895,7 @@ uint32_t build_tlas(std::vector<InstBox>& boxes, size_t a, size_t b, std::vector
   n.link[0] = l;
   n.link[1] = r;
   n.axis = (uint32_t)axis;
-  n.pad = 0;
+  n.flags = 0;
   return (uint32_t)me;
 }
 

@@ -58,6 +58,7 @@ __device__ __forceinline__ bool under_max(float s, const float* b, float3 p, ff 
 struct CPBest {
   float d2, err;     // float32 squared distance and its error bound
   uint32_t rec;      // triangle record (0xFFFFFFFF: none yet)
+  uint32_t face;     // its faceIndex
   float3 q;          // float32 closest point
   bool vertex;       // q is an input vertex, bit-exact
   bool ff_ok;        // ffv holds the float-float squared distance
@@ -69,6 +70,7 @@ __device__ __forceinline__ CPBest cp_none() {
   b.d2 = kInf;
   b.err = 0.0f;
   b.rec = 0xFFFFFFFFu;
+  b.face = 0xFFFFFFFFu;
   b.q = make_float3(0.f, 0.f, 0.f);
   b.vertex = false;
   b.ff_ok = false;
@@ -77,10 +79,11 @@ __device__ __forceinline__ CPBest cp_none() {
 }
 
 // Offers triangle record k to the query at p: a strictly smaller squared distance replaces the
-// best (the reference's strict `<` on distSq), and an exact tie goes to the earlier record in
-// leaf order (the reference keeps whichever its own traversal reached first; a fixed rule keeps
-// the answer independent of how queries are grouped).  Returns the candidate's float32 squared
-// distance and bound, and its float-float value when one was needed.
+// best (the reference's strict `<` on distSq), and an exact tie goes to the smaller faceIndex
+// (the reference keeps whichever its own traversal reached first; a fixed rule on the triangle
+// itself keeps the answer independent of how queries are grouped and of how the triangles of a
+// leaf are laid out).  Every record holds a distinct faceIndex.  Returns the candidate's float32
+// squared distance and bound, and its float-float value when one was needed.
 // With `cull`, a triangle whose bounding box is already farther than the best candidate is
 // passed over without its closest point: its distance exceeds the best one, so it cannot win
 // (callers that test minThreshold on every triangle pass false).
@@ -118,10 +121,10 @@ __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& 
   } else if (d2 - err > b.d2 + b.err) {
     take = false;
   } else if (is_vertex && b.vertex && q.x == b.q.x && q.y == b.q.y && q.z == b.q.z) {
-    take = k < b.rec;  // the same vertex: an exact tie, the earlier record in leaf order wins
+    take = t.face < b.face;  // the same vertex: an exact tie, the smaller faceIndex wins
   } else {
     // Undecided in float32: the float-float squared distances decide, and an exact tie goes to
-    // the earlier record in leaf order.  Candidates are thus ranked by a total order that does
+    // the smaller faceIndex.  Candidates are thus ranked by a total order that does
     // not depend on the order they are offered in, and every box that could hold a candidate at
     // the best distance is entered (box tests keep a relative slack), so the answer is the same
     // for any traversal order: per query, warp-shared, sorted or chunked.
@@ -132,12 +135,13 @@ __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& 
     }
     cand_ff = closest_ff(p, t.a, t.b, t.c).d2;
     have_ff = true;
-    take = ff_lt(cand_ff, b.ffv) || (!ff_lt(b.ffv, cand_ff) && k < b.rec);
+    take = ff_lt(cand_ff, b.ffv) || (!ff_lt(b.ffv, cand_ff) && t.face < b.face);
   }
   if (take) {
     b.d2 = d2;
     b.err = err;
     b.rec = k;
+    b.face = t.face;
     b.q = q;
     b.vertex = is_vertex;
     b.ff_ok = have_ff;
@@ -253,14 +257,18 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
 // shared order would not reproduce; those calls use the per-query kernel.)
 // ---------------------------------------------------------------------------------------------
 //
-template <int MINB>
+// GROUP = 32 walks the tree with the whole warp; 16 and 8 split the warp into groups of that many
+// lanes (consecutive queries), each with its own shared stack: a group's node set is the union over
+// fewer, closer queries, and groups at different nodes on the same code path still issue together.
+template <int MINB, int GROUP>
 __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
     MeshDev m, const float* __restrict__ pts, uint64_t n, float max_t, bvhc_closest* __restrict__ out,
     const uint32_t* __restrict__ queue, const unsigned int* __restrict__ qcount, uint64_t pitch, int rows_log2) {
-  __shared__ uint32_t s_link[kBlock / 32][kMaxStack];
-  const unsigned full = 0xFFFFFFFFu;
-  const int w = threadIdx.x >> 5;
-  const unsigned lane = threadIdx.x & 31u;
+  static_assert(GROUP == 32 || GROUP == 16 || GROUP == 8, "group of 8, 16 or 32 lanes");
+  __shared__ uint32_t s_link[kBlock / GROUP][kMaxStack];
+  const int w = threadIdx.x / GROUP;                      // group within the block
+  const unsigned lane = threadIdx.x & (GROUP - 1u);       // lane within the group
+  const unsigned full = GROUP == 32 ? 0xFFFFFFFFu : ((1u << GROUP) - 1u) << ((threadIdx.x & 31u) & ~(GROUP - 1u));
   const uint64_t n_work = queue ? (uint64_t)__ldg(qcount) : n;
   if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -300,12 +308,12 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         float best_hi = b.d2 + b.err;
         bool w0 = act && s0 * (1.0f - kSlabMargin) <= best_hi && under_max(s0, pr.l, p, max2);
         bool w1 = act && s1 * (1.0f - kSlabMargin) <= best_hi && under_max(s1, pr.r, p, max2);
-        unsigned b0 = __ballot_sync(full, w0), b1 = __ballot_sync(full, w1);
+        unsigned b0 = __ballot_sync(full, w0) & full, b1 = __ballot_sync(full, w1) & full;
         if (b0 && b1) {
           // nearer child first by majority of the lanes that want both (a lane wanting one prefers it)
           bool pref_right = (w0 && w1) ? right_nearer(pr, s0, s1, p) : w1;
-          unsigned voters = __ballot_sync(full, w0 || w1);
-          bool right_first = 2 * __popc(__ballot_sync(full, (w0 || w1) && pref_right)) > __popc(voters);
+          unsigned voters = __ballot_sync(full, w0 || w1) & full;
+          bool right_first = 2 * __popc(__ballot_sync(full, (w0 || w1) && pref_right) & full) > __popc(voters);
           if (sp >= kMaxStack) {
             if (lane == 0) atomicOr(m.err, kErrStackOverflow);
             b = cp_none();
@@ -317,7 +325,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
           ++sp;
           link = right_first ? pr.lr : pr.ll;
           act = right_first ? w1 : w0;
-          __syncwarp();
+          __syncwarp(full);
         } else if (b0) {
           link = pr.ll;
           act = w0;
@@ -333,7 +341,7 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
         while (sp > 0) {
           --sp;
           bool ok = lane_s[sp] * (1.0f - kSlabMargin) <= b.d2 + b.err;  // false for NaN
-          if (__ballot_sync(full, ok)) {
+          if (__ballot_sync(full, ok) & full) {
             link = s_link[w][sp];
             act = ok;
             found = true;
@@ -1199,9 +1207,10 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
                                  bvhc_closest* out, cudaStream_t stream, int variant, int occupancy, uint32_t* queue,
                                  unsigned int* qcount, const RaySort* sort, uint32_t tile, int tile_rows) {
   if (n == 0) return cudaSuccess;
-  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel); 2 runs over
+  // the warp-cooperative forms need minThreshold 0 (see closest_point_packet_kernel): 1 / 2 with
+  // whole warps, 3 / 4 with 16-lane groups, 5 / 6 with 8-lane groups; the even ones run over
   // Morton-sorted queries
-  const bool sorted = variant == 2;
+  const bool sorted = variant > 0 && variant % 2 == 0;
   if (variant == 0 || !(min_t <= 0.0f) || (sorted && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
     dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
     return cudaGetLastError();
@@ -1225,10 +1234,17 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
     queue = nullptr;
     qcount = nullptr;
   }
-  auto kernel = occupancy == 0   ? dev::closest_point_packet_kernel<1>
-                : occupancy == 1 ? dev::closest_point_packet_kernel<6>
-                                 : dev::closest_point_packet_kernel<8>;
-  // input order (variant 1) may be read in tiles: rows of `tile` points (a grid's row), 2-D blocks
+  using K = void (*)(MeshDev, const float*, uint64_t, float, bvhc_closest*, const uint32_t*, const unsigned int*,
+                     uint64_t, int);
+  static const K kernels[3][3] = {
+      {dev::closest_point_packet_kernel<1, 32>, dev::closest_point_packet_kernel<6, 32>,
+       dev::closest_point_packet_kernel<8, 32>},
+      {dev::closest_point_packet_kernel<1, 16>, dev::closest_point_packet_kernel<6, 16>,
+       dev::closest_point_packet_kernel<8, 16>},
+      {dev::closest_point_packet_kernel<1, 8>, dev::closest_point_packet_kernel<6, 8>,
+       dev::closest_point_packet_kernel<8, 8>}};
+  const K kernel = kernels[std::min((variant - 1) / 2, 2)][occupancy < 0 ? 0 : occupancy > 2 ? 2 : occupancy];
+  // input order (odd variants) may be read in tiles: rows of `tile` points (a grid's row), 2-D blocks
   const int rl = tile_rows_log2(tile_rows);
   const uint64_t pitch = (!queue && tile >= 8 && tile % (32u >> rl) == 0) ? (uint64_t)tile : 0;
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount, pitch, rl);

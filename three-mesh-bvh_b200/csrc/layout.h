@@ -22,13 +22,13 @@ constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kEmptyLeaf = 0xFFFFFFFFu;
 constexpr int kMaxStack = 64;  // deepest supported tree (the reference's default maxDepth is 40)
 
-struct alignas(16) PairNode {
+struct alignas(64) PairNode {
   // f[0..5]  left child  box (min xyz, max xyz)
   // f[6..11] right child box
   float f[12];
   uint32_t link[2];   // left, right child links
   uint32_t axis;      // split axis of this node (0, 1, 2)
-  uint32_t pad;
+  uint32_t flags;     // 0 (reserved)
 };
 static_assert(sizeof(PairNode) == 64, "PairNode must be 64 bytes");
 

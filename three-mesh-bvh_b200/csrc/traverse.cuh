@@ -31,6 +31,13 @@ constexpr float kSlabMargin = 9.5367431640625e-07f;  // 2^-20, relative slack on
 constexpr float kTiny = 1e-30f;                      // stand-in for a zero direction component
 
 __device__ __forceinline__ float4 ld4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// 32 bytes in one load instruction (the 256-bit global load of sm_100) through the read-only path;
+// p must be 32-byte aligned.
+__device__ __forceinline__ void ld8(const void* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
 
 struct RayF {
   float3 o, d, inv;
@@ -101,18 +108,22 @@ __device__ __forceinline__ int tri_side(const Tri& t, int side, const SideTable&
 
 struct Pair {
   float l[6], r[6];
-  uint32_t ll, lr, axis;
+  uint32_t ll, lr, axis, flags;
 };
 
 __device__ __forceinline__ Pair load_pair(const PairNode* __restrict__ nodes, uint32_t k) {
   const PairNode* n = nodes + k;
-  float4 q0 = ld4(&n->f[0]), q1 = ld4(&n->f[4]), q2 = ld4(&n->f[8]), q3 = ld4(&n->link[0]);
+  // two 256-bit loads per record (every pair array is its own allocation of 64-byte records)
+  float4 q0, q1, q2, q3;
+  ld8(&n->f[0], q0, q1);
+  ld8(&n->f[8], q2, q3);
   Pair p;
   p.l[0] = q0.x; p.l[1] = q0.y; p.l[2] = q0.z; p.l[3] = q0.w; p.l[4] = q1.x; p.l[5] = q1.y;
   p.r[0] = q1.z; p.r[1] = q1.w; p.r[2] = q2.x; p.r[3] = q2.y; p.r[4] = q2.z; p.r[5] = q2.w;
   p.ll = __float_as_uint(q3.x);
   p.lr = __float_as_uint(q3.y);
   p.axis = __float_as_uint(q3.z);
+  p.flags = __float_as_uint(q3.w);
   return p;
 }
 
