@@ -675,6 +675,15 @@ def run_batched(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def closest_launches(variant: int) -> int:
+    """Kernels one closestPointToPoint call launches: the per-query kernel alone; the
+    warp-cooperative forms' traversal and finalize, after the query box, the Morton keys and a
+    three-pass radix sort (three kernels a pass) for the sorted forms."""
+    if variant == 0:
+        return 1
+    return 2 + (11 if variant % 2 == 0 else 0)
+
+
 def run_closest(args, ws, rank, local):
     """Closest point / unsigned SDF: the 80,000-triangle knot, a 256^3 grid over its bounding box
     padded by 10%, closestPointToPoint with maxThreshold 5 and minThreshold 0."""
@@ -769,7 +778,7 @@ def run_closest(args, ws, rank, local):
                 "closest_variant": tuned, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "e2e": {"value": weak_scaling_rate(ws, n, 1, e2e_ms), "unit": "Mqueries/s",
                         "h2d_bytes_per_step": int(n * 12), "d2h_bytes_per_step": int(n * 20)},
-                "gpu_launches": args.steps * (11 if tuned["setting"]["closest"] in (2, 4, 6) else 1)}
+                "gpu_launches": args.steps * closest_launches(tuned["setting"]["closest"])}
         print(json.dumps(line), flush=True)
     bvh.dispose()
 

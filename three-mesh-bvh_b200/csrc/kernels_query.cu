@@ -34,9 +34,12 @@ __device__ __forceinline__ float centre_d2(const float* b, float3 p) {
 }
 
 // Whether the right child should be visited first: the smaller score, equal scores by the nearer
-// centre (the warp-cooperative forms; the per-query kernel keeps the reference's order).
+// centre (the warp-cooperative forms; the per-query kernel keeps the reference's order).  The
+// centre distances are computed only on equal scores (written as a branch: as one expression they
+// were evaluated on every node, 4% of the grid's time).
 __device__ __forceinline__ bool right_nearer(const Pair& pr, float s0, float s1, float3 p) {
-  return s1 < s0 || (s1 == s0 && centre_d2(pr.r, p) < centre_d2(pr.l, p));
+  if (s1 != s0) return s1 < s0;
+  return centre_d2(pr.r, p) < centre_d2(pr.l, p);
 }
 
 __device__ __noinline__ ff box_score_ff(const float* b, float3 p) {
@@ -149,15 +152,16 @@ __device__ __forceinline__ void cp_offer(const MeshDev& m, float3 p, const Tri& 
   }
 }
 
-// The reported record: distance and closest point in float-float, rounded once.
-__device__ __forceinline__ void cp_store(const MeshDev& m, float3 p, const CPBest& b, bvhc_closest* o) {
-  if (b.rec == 0xFFFFFFFFu) {
+// The reported record of triangle record `rec` (0xFFFFFFFF: none): distance and closest point in
+// float-float, rounded once.
+__device__ __forceinline__ void cp_store(const MeshDev& m, float3 p, uint32_t rec, bvhc_closest* o) {
+  if (rec == 0xFFFFFFFFu) {
     o->face_index = BVHC_NO_HIT;
     o->distance = kInf;
     o->point[0] = o->point[1] = o->point[2] = 0.0f;
     return;
   }
-  Tri t = load_tri(m.tris, b.rec);
+  Tri t = load_tri(m.tris, rec);
   CPFF c = closest_ff(p, t.a, t.b, t.c);
   o->face_index = t.face;
   o->distance = ff_to_f(ff_sqrt(c.d2));
@@ -240,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
       if (!found) break;
     }
   }
-  cp_store(m, p, b, out + i);
+  cp_store(m, p, b.rec, out + i);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -352,7 +356,19 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
       }
     }
   }
-  if (valid) cp_store(m, p, b, out + i);
+  // pending: the record index in face_index; closest_point_finalize_kernel completes the record,
+  // which keeps the float-float code out of this kernel
+  if (valid) out[i].face_index = b.rec;
+}
+
+// Completes the records closest_point_packet_kernel left pending, one query per thread in input
+// order.
+__global__ void __launch_bounds__(kBlock) closest_point_finalize_kernel(MeshDev m, const float* __restrict__ pts,
+                                                                        uint64_t n, bvhc_closest* __restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float3 p = make_float3(__ldg(pts + 3 * i), __ldg(pts + 3 * i + 1), __ldg(pts + 3 * i + 2));
+  cp_store(m, p, out[i].face_index, out + i);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1248,6 +1264,8 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
   const int rl = tile_rows_log2(tile_rows);
   const uint64_t pitch = (!queue && tile >= 8 && tile % (32u >> rl) == 0) ? (uint64_t)tile : 0;
   kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, max_t, out, queue, qcount, pitch, rl);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  dev::closest_point_finalize_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, out);
   return cudaGetLastError();
 }
 
