@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--closest-variant", type=int, default=None,
                     help="closest workload: force closestPointToPoint's kernel instead of tuning "
                          "(with --closest-tile-rows: tiled order)")
+    ap.add_argument("--scene-variant", type=int, default=None,
+                    help="scene workload: force the instanced kernel variant (0..2, with ray order 0) instead of "
+                         "tuning")
     ap.add_argument("--closest-tile-rows", type=int, default=0,
                     help="closest workload, with --closest-variant 1: read the grid in tiles of this many "
                          "rows (2, 4, 8) of --grid points")
@@ -1051,9 +1054,10 @@ def run_scene(args, ws, rank, local):
     # ray order (input order, a Morton key, or the first instance reached) and kernel variant
     # (resident blocks per SM 14 / 10 / 8), whichever is fastest here
     order_ms = {}
-    for occ in (0, 1, 2):
+    variants = (0, 1, 2) if args.scene_variant is None else (args.scene_variant,)
+    for occ in variants:
         scene.set_variant(occ)
-        for order in (0, 1, 2, 3, 4):
+        for order in ((0, 1, 2, 3, 4) if args.scene_variant is None else (0,)):
             scene.set_order(order)
             step()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
