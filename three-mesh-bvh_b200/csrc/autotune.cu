@@ -34,8 +34,9 @@ bvhc_traversal_config make(int persistent, int order, int refill, int occupancy,
 
 // Stage-1 candidates: one ray per thread (both child orders); warp-cooperative over child pairs
 // (child order x register budget x queue) and over four-child records; persistent warps (child
-// order x refill threshold x register budget x queue); warp-cooperative in tiled ray order, one
-// per row pitch given.  Queue: none, compaction, compaction + ordering key 1, 2, 3.
+// order x refill threshold x register budget x queue); warp-cooperative in tiled ray order over
+// child pairs (child order x register budget) and over four-child records (register budget), for
+// each row pitch given.  Queue: none, compaction, compaction + ordering key 1, 2, 3.
 std::vector<bvhc_traversal_config> stage1(const int32_t* tiles, int n_tiles) {
   static const int kQueue[5][2] = {{0, 0}, {1, 0}, {1, 1}, {1, 2}, {1, 3}};
   std::vector<bvhc_traversal_config> c;
@@ -50,9 +51,11 @@ std::vector<bvhc_traversal_config> stage1(const int32_t* tiles, int n_tiles) {
     for (int refill : {16, 32})
       for (int occ = 1; occ < 3; ++occ)
         for (const auto& q : kQueue) c.push_back(make(1, order, refill, occ, q[0], q[1], 0, 0));
-  for (int k = 0; k < n_tiles; ++k)
+  for (int k = 0; k < n_tiles; ++k) {
     for (int order = 0; order < 2; ++order)
       for (int occ = 0; occ < 3; ++occ) c.push_back(make(2, order, 16, occ, 0, 0, 0, tiles[k]));
+    for (int occ = 0; occ < 3; ++occ) c.push_back(make(2, 1, 16, occ, 0, 0, 1, tiles[k]));  // four-child records
+  }
   return c;
 }
 
@@ -158,7 +161,7 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
   // stage 2: block size and stack depth around each set's best
   for (int k = 0; k < n_sets && st == BVHC_OK; ++k) {
     const bvhc_traversal_config base = chosen[k];
-    if (base.persistent == 0 || (base.persistent == 2 && base.wide)) continue;
+    if (base.persistent == 0 || (base.persistent == 2 && base.wide && !base.tile)) continue;
     std::vector<bvhc_traversal_config> more{base};
     if (base.persistent == 1)
       for (int refill : {8, 24})  // the refill thresholds between and below stage 1's 16 and 32
@@ -169,6 +172,7 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
         }
     if (base.persistent == 2) {
       for (int block : {64, 256}) {
+        if (base.wide) break;  // the four-child kernel has one block size
         bvhc_traversal_config c = base;
         c.block = block;
         more.push_back(c);
@@ -192,13 +196,15 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
       }
     }
     if (st != BVHC_OK) break;
-    bvhc_traversal_config shallow = chosen[k];
-    shallow.stack = 32;
-    float ms = 0.0f;
-    st = time_variant(mesh, shallow, rays[k], counts[k], side, near_dist, far_dist, out, reps, s, t, &ms);
-    if (st == BVHC_OK && ms < ref_ms) {
-      ref_ms = ms;
-      chosen[k] = shallow;
+    if (!(chosen[k].persistent == 2 && chosen[k].wide)) {  // the four-child kernel has one stack size
+      bvhc_traversal_config shallow = chosen[k];
+      shallow.stack = 32;
+      float ms = 0.0f;
+      st = time_variant(mesh, shallow, rays[k], counts[k], side, near_dist, far_dist, out, reps, s, t, &ms);
+      if (st == BVHC_OK && ms < ref_ms) {
+        ref_ms = ms;
+        chosen[k] = shallow;
+      }
     }
     chosen_ms[k] = ref_ms;
   }

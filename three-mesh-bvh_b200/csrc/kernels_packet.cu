@@ -120,7 +120,7 @@ template <int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
     MeshDev m, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides, float near_d,
     float far_d, bvhc_hit* __restrict__ out, const uint32_t* __restrict__ queue,
-    const unsigned int* __restrict__ qcount) {
+    const unsigned int* __restrict__ qcount, uint64_t pitch, int rows_log2) {
   __shared__ uint32_t s_link[kWarps][kMaxStack];
   const unsigned full = 0xFFFFFFFFu;
   const int w = threadIdx.x >> 5;
@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
   if ((uint64_t)blockIdx.x * blockDim.x >= n_work) return;  // block-uniform
   const bool valid = i < n_work;
   if (valid && queue) i = __ldg(queue + i);
+  else if (valid && pitch) i = tiled_index(i, pitch, rows_log2, n);
   RayF r;
   float dlen = 1.0f;
   if (valid) {
@@ -152,9 +153,13 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
         if (link != kEmptyLeaf && valid) leaf_first(m, link & ~kLeafBit, r, dlen, side, sides, near_d, far_d, best);
         pop = true;
       } else {
+        // 112 of the record's 128 bytes: three 256-bit loads and one 128-bit load (the quad array is
+        // one allocation of 128-byte records)
         const QuadNode* qn = m.quads + link;
-        const float4 lx = ld4(qn->lo[0]), ly = ld4(qn->lo[1]), lz = ld4(qn->lo[2]);
-        const float4 hx = ld4(qn->hi[0]), hy = ld4(qn->hi[1]), hz = ld4(qn->hi[2]);
+        float4 lx, ly, lz, hx, hy, hz;
+        ld8(qn->lo[0], lx, ly);
+        ld8(qn->lo[2], lz, hx);
+        ld8(qn->hi[1], hy, hz);
         const float4 lk = ld4(qn->link);
         const uint32_t ck[4] = {__float_as_uint(lk.x), __float_as_uint(lk.y), __float_as_uint(lk.z),
                                 __float_as_uint(lk.w)};
@@ -272,16 +277,17 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
     queue = nullptr;
     qcount = nullptr;
   }
+  // the tiled order applies to the whole ray range (a queue is already in its own order)
+  const int rl = tile_rows_log2(cfg.tile_rows);
+  const uint64_t pitch = (!queue && cfg.tile >= 8 && cfg.tile % (32 >> rl) == 0) ? (uint64_t)cfg.tile : 0;
   if (cfg.wide && m.quads && m.quad_roots) {
     auto k4 = cfg.occupancy == 0   ? dev::raycast_first_packet4_kernel<1>
               : cfg.occupancy == 1 ? dev::raycast_first_packet4_kernel<6>
                                    : dev::raycast_first_packet4_kernel<8>;
-    k4<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount);
+    k4<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount, pitch,
+                                                rl);
     return cudaGetLastError();
   }
-  // the tiled order applies to the whole ray range (a queue is already in its own order)
-  const int rl = tile_rows_log2(cfg.tile_rows);
-  const uint64_t pitch = (!queue && cfg.tile >= 8 && cfg.tile % (32 >> rl) == 0) ? (uint64_t)cfg.tile : 0;
   const bool s32 = stack_entries(m, cfg.stack) == 32;
   const int block = cfg.block == 64 || cfg.block == 256 ? cfg.block : 128;
 #define BVHC_PACKET(B, S) \
