@@ -238,14 +238,14 @@ def traversal_kernel(cfg):
 
 def kernel_launches(cfg):
     """Kernels one raycastFirst call launches with a variant (persistent, order, refill, occupancy,
-    compact, sort): the traversal, the persistent form's finalize pass, the root-box pre-pass and
-    the ray-ordering sort (key pass(es) + 4 radix passes of 3 kernels)."""
+    compact, sort): the traversal, the finalize pass of the persistent and warp-cooperative forms,
+    the root-box pre-pass and the ray-ordering sort (key pass(es) + 4 radix passes of 3 kernels)."""
     cfg = list(cfg) if cfg is not None else [1, 1, 16, 0, 0, 0]
     cfg += [0] * (6 - len(cfg))
     persistent, compact, sort = cfg[0], cfg[4], cfg[5]
     if persistent == 0:
         return 1
-    n = 1 + (1 if persistent == 1 else 0)
+    n = 2
     if compact or sort:
         n += 1
     if sort:
@@ -254,14 +254,14 @@ def kernel_launches(cfg):
 
 
 def all_hits_launches(variant):
-    """Kernels one raycast (all hits) call launches: the traversal, plus for the queue variants the
-    root-box pre-pass and, when the queue is sorted, 3 kernels per radix pass (4 passes for the
-    direction key, 3 for the others)."""
+    """Kernels one raycast (all hits) call launches: the traversal and the finalize kernel that
+    completes the stored hits, plus for the queue variants the root-box pre-pass and, when the
+    queue is sorted, 3 kernels per radix pass (4 passes for the direction key, 3 for the others)."""
     if variant in (0, 1, "1t", "1t2", "1t8"):
-        return 1
+        return 2
     v = int(variant)
     kind = {2: 1, 3: 2, 4: 3, 6: 1, 7: 2, 8: 3, 10: 1, 11: 2, 12: 3}.get(v, 0)
-    return 2 + (3 * (4 if kind == 1 else 3) if kind else 0)
+    return 3 + (3 * (4 if kind == 1 else 3) if kind else 0)
 
 
 def measured_peak():

@@ -99,6 +99,10 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
                                             bvhc_hit* out, unsigned long long* work, const TraversalConfig& cfg,
                                             cudaStream_t stream, uint32_t* queue = nullptr,
                                             unsigned int* qcount = nullptr, const RaySort* sort = nullptr);
+// Completes the pending records a traversal left in `out` (record index in face_index), for the
+// queued rays (queue / qcount) or all n.
+cudaError_t launch_finalize_first(const MeshDev& m, const float* rays, uint64_t n, bvhc_hit* out,
+                                  const uint32_t* queue, const unsigned int* qcount, cudaStream_t stream);
 // Warp-cooperative raycastFirst: the 32 rays of a warp share one traversal (coherent rays).  With a
 // queue, the same pre-pass (and sort) as the persistent form runs first.
 // wide = 1 with m.quads set runs over the four-child records.

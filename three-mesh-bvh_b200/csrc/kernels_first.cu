@@ -140,12 +140,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
       link = m.roots[root];
       return;
     }
-    if (best.rec == 0xFFFFFFFFu) {
-      store_miss(out + rid);
-    } else {
-      // pending: the record index in face_index, finalize_first_kernel completes it
-      __stcs(reinterpret_cast<float4*>(out + rid), make_float4(__uint_as_float(best.rec), best.t, 0.0f, 0.0f));
-    }
+    store_first_pending(out + rid, best);  // finalize_first_kernel completes a hit
     active = false;
   };
 
@@ -449,8 +444,14 @@ cudaError_t launch_raycast_first_persistent(const MeshDev& m, const BatchDev* ba
   else launch_persistent_cfg<false>(a, cfg, stream);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  return launch_finalize_first(m, rays, n, out, a.queue, a.qcount, stream);
+}
+
+cudaError_t launch_finalize_first(const MeshDev& m, const float* rays, uint64_t n, bvhc_hit* out,
+                                  const uint32_t* queue, const unsigned int* qcount, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
   unsigned int fg = (unsigned int)std::min<uint64_t>(grid_for(n), 8192);
-  dev::finalize_first_kernel<<<fg, dev::kBlock, 0, stream>>>(m, rays, n, out, a.queue, a.qcount);
+  dev::finalize_first_kernel<<<fg, dev::kBlock, 0, stream>>>(m, rays, n, out, queue, qcount);
   return cudaGetLastError();
 }
 

@@ -15,7 +15,9 @@ namespace dev {
 // lanes at once, so the triangle tests run at full SIMD width.  Each lane keeps its own entry
 // distance for every stacked child; a stacked child is skipped when no lane still needs it.
 // Visiting a node a lane's ray does not enter costs that lane nothing but idle time, and testing
-// a triangle it would not have reached cannot change its closest hit.
+// a triangle it would not have reached cannot change its closest hit.  The kernel leaves each hit
+// pending (its triangle record); finalize_first_kernel computes the reported records, which keeps
+// the float-float record code out of the traversal kernel.
 // ---------------------------------------------------------------------------------------------
 
 // BLOCK threads per block (64, 128 or 256), STACK shared-stack entries (32 or 64; the launch picks 32
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) raycast_first_packet_kernel(MeshD
       }
     }
   }
-  if (valid) finish_first(m, best.rec, r, out + i);
+  if (valid) store_first_pending(out + i, best);  // finalize_first_kernel completes a hit
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_packet4_kernel(
       }
     }
   }
-  if (valid) finish_first(m, best.rec, r, out + i);
+  if (valid) store_first_pending(out + i, best);  // finalize_first_kernel completes a hit
 }
 
 }  // namespace dev
@@ -286,7 +288,9 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
                                    : dev::raycast_first_packet4_kernel<8>;
     k4<<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out, queue, qcount, pitch,
                                                 rl);
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_finalize_first(m, rays, n, out, queue, qcount, stream);
   }
   const bool s32 = stack_entries(m, cfg.stack) == 32;
   const int block = cfg.block == 64 || cfg.block == 256 ? cfg.block : 128;
@@ -304,7 +308,9 @@ cudaError_t launch_raycast_first_packet(const MeshDev& m, const float* rays, uin
     else BVHC_PACKET(128, 64);
   }
 #undef BVHC_PACKET
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_finalize_first(m, rays, n, out, queue, qcount, stream);
 }
 
 }  // namespace bvhc

@@ -227,6 +227,13 @@ __device__ __forceinline__ void leaf_first(const MeshDev& m, uint32_t k, const R
   }
 }
 
+// A traversal's result left for finalize_first_kernel: a miss record, or pending (the triangle
+// record index in face_index, t in distance).
+__device__ __forceinline__ void store_first_pending(bvhc_hit* o, const Best& b) {
+  if (b.rec == 0xFFFFFFFFu) store_miss(o);
+  else __stcs(reinterpret_cast<float4*>(o), make_float4(__uint_as_float(b.rec), b.t, 0.0f, 0.0f));
+}
+
 // The reported record of the best hit: t, distance, point and barycentrics in float-float.
 __device__ __forceinline__ void finish_first(const MeshDev& m, uint32_t rec, const RayF& r, bvhc_hit* o) {
   if (rec == 0xFFFFFFFFu) {
