@@ -16,9 +16,6 @@ namespace dev {
 // (t, distance, point, barycentrics in float-float) one ray per thread, which keeps that code out
 // of the traversal loops (the camera set: 11.2 -> 6.9 ms of traversal).
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ void store_pending(bvhc_hit* p, uint32_t rec) {
-  __stcs(reinterpret_cast<float4*>(p), make_float4(__uint_as_float(rec), 0.0f, 0.0f, 0.0f));
-}
 
 // One ray per thread: all n rays, or with a queue the queued ones (the rays that enter the tree, so
 // that a warp's lanes mostly have hits to complete).
@@ -79,7 +76,7 @@ __global__ void __launch_bounds__(kBlock) raycast_all_kernel(MeshDev m, const fl
             float th, te;
             if (ts >= 0 && tri_hit_t(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts, th, te) &&
                 in_range(th, te, t, r, dlen, near_d, far_d)) {
-              if (cnt < cap) store_pending(out + cnt, k);
+              if (cnt < cap) store_pending_record(out + cnt, k, 0.0f);
               ++cnt;
             }
             if (t.flags & kTriLast) break;
@@ -175,7 +172,7 @@ __global__ void __launch_bounds__(kBlock, kAllBlocksPerSm) raycast_all_persisten
               float th, te;
               if (ts >= 0 && tri_hit_t(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts, th, te) &&
                   in_range(th, te, t, r, dlen, near_d, far_d)) {
-                if (cnt < cap) store_pending(out + cnt, k);
+                if (cnt < cap) store_pending_record(out + cnt, k, 0.0f);
                 ++cnt;
               }
               if (t.flags & kTriLast) break;
@@ -271,7 +268,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_all_packet_kernel(
             float th, te;
             if (ts >= 0 && tri_hit_t(t.a, t.b, t.c, r.o, r.d, r.d_l1, ts, th, te) &&
                 in_range(th, te, t, r, dlen, near_d, far_d)) {
-              if (cnt < cap) store_pending(out + cnt, k);
+              if (cnt < cap) store_pending_record(out + cnt, k, 0.0f);
               ++cnt;
             }
             if (t.flags & kTriLast) break;

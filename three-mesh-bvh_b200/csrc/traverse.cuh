@@ -227,11 +227,19 @@ __device__ __forceinline__ void leaf_first(const MeshDev& m, uint32_t k, const R
   }
 }
 
-// A traversal's result left for finalize_first_kernel: a miss record, or pending (the triangle
-// record index in face_index, t in distance).
+// A pending record: the triangle record index in face_index, `t` in distance.  All 32 bytes are
+// written, so that the record's DRAM sector is written whole (a half-sector store makes L2 fetch
+// the other half first).
+__device__ __forceinline__ void store_pending_record(bvhc_hit* o, uint32_t rec, float t) {
+  float4* p = reinterpret_cast<float4*>(o);
+  __stcs(p, make_float4(__uint_as_float(rec), t, 0.0f, 0.0f));
+  __stcs(p + 1, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+}
+
+// A traversal's result left for finalize_first_kernel: a miss record, or pending.
 __device__ __forceinline__ void store_first_pending(bvhc_hit* o, const Best& b) {
   if (b.rec == 0xFFFFFFFFu) store_miss(o);
-  else __stcs(reinterpret_cast<float4*>(o), make_float4(__uint_as_float(b.rec), b.t, 0.0f, 0.0f));
+  else store_pending_record(o, b.rec, b.t);
 }
 
 // The reported record of the best hit: t, distance, point and barycentrics in float-float.
