@@ -133,16 +133,32 @@ struct TriFF {
   ff N, U, V, W, T;
 };
 
-static __device__ __noinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
+// The float-float determinants of a ray / triangle pair, together with what a hit record's
+// barycentrics need from the same edge vectors and normal: g = |n|^2 and l12 = |e1|^2 |e2|^2 (the
+// degenerate-triangle test), so that a record takes one evaluation.  One out-of-line body serves
+// every float-float triangle evaluation (tri_eval_ff below), which keeps kernels that call it from
+// several places fetching one copy of the code.
+struct TriFFHit {
+  TriFF e;
+  ff g, l12;
+};
+
+static __device__ __noinline__ TriFFHit tri_eval_ff_hit(float3 a, float3 b, float3 c, float3 o, float3 d) {
   ff3 e1 = ff3_diff(b, a), e2 = ff3_diff(c, a), q = ff3_diff(o, a);
   ff3 n = ff3_cross(e1, e2);
-  TriFF r;
-  r.N = ff3_dot_f(d, n);
-  r.U = ff3_dot_f(d, ff3_cross(q, e2));
-  r.V = ff3_dot_f(d, ff3_cross(e1, q));
-  r.W = ff_sub(ff_sub(r.N, r.U), r.V);
-  r.T = ff3_dot(q, n);
+  TriFFHit r;
+  r.e.N = ff3_dot_f(d, n);
+  r.e.U = ff3_dot_f(d, ff3_cross(q, e2));
+  r.e.V = ff3_dot_f(d, ff3_cross(e1, q));
+  r.e.W = ff_sub(ff_sub(r.e.N, r.e.U), r.e.V);
+  r.e.T = ff3_dot(q, n);
+  r.g = ff3_dot(n, n);
+  r.l12 = ff_mul(ff3_dot(e1, e1), ff3_dot(e2, e2));
   return r;
+}
+
+__device__ __forceinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
+  return tri_eval_ff_hit(a, b, c, o, d).e;
 }
 
 __device__ __forceinline__ bool tri_decide_ff(const TriFF& r, int side) {

@@ -136,8 +136,8 @@ __device__ __forceinline__ ff dir_length(float3 d) {
 // Full intersection record for a triangle known to be hit, in float-float, rounded once.
 // barycoord follows Triangle.getBarycoord: (0, 0, 0) when the triangle's Gram determinant
 // |e1 x e2|^2 vanishes at float64 resolution (the reference's `denom === 0` case).
-static __device__ void make_hit(const Tri& t, const RayF& r, ff tt, ff dist, bvhc_hit& h) {
-  TriFF e = tri_eval_ff(t.a, t.b, t.c, r.o, r.d);
+// x = tri_eval_ff_hit of the triangle and ray, tt = its t, dist = the hit's distance.
+static __device__ void make_hit(const Tri& t, const RayF& r, const TriFFHit& x, ff tt, ff dist, bvhc_hit& h) {
   ff3 px = {ff_add(ff_from(r.o.x), ff_mul_f(tt, r.d.x)), ff_add(ff_from(r.o.y), ff_mul_f(tt, r.d.y)),
             ff_add(ff_from(r.o.z), ff_mul_f(tt, r.d.z))};
   h.face_index = t.face;
@@ -145,16 +145,12 @@ static __device__ void make_hit(const Tri& t, const RayF& r, ff tt, ff dist, bvh
   h.point[0] = ff_to_f(px.x);
   h.point[1] = ff_to_f(px.y);
   h.point[2] = ff_to_f(px.z);
-  ff3 e1 = ff3_diff(t.b, t.a), e2 = ff3_diff(t.c, t.a);
-  ff3 n = ff3_cross(e1, e2);
-  ff g = ff3_dot(n, n);
-  ff l12 = ff_mul(ff3_dot(e1, e1), ff3_dot(e2, e2));
-  if (g.hi <= 8.8817841970012523e-16f * l12.hi) {  // 2^-50
+  if (x.g.hi <= 8.8817841970012523e-16f * x.l12.hi) {  // 2^-50
     h.barycoord[0] = h.barycoord[1] = h.barycoord[2] = 0.0f;
   } else {
-    h.barycoord[0] = ff_to_f(ff_div(e.W, e.N));
-    h.barycoord[1] = ff_to_f(ff_div(e.U, e.N));
-    h.barycoord[2] = ff_to_f(ff_div(e.V, e.N));
+    h.barycoord[0] = ff_to_f(ff_div(x.e.W, x.e.N));
+    h.barycoord[1] = ff_to_f(ff_div(x.e.U, x.e.N));
+    h.barycoord[2] = ff_to_f(ff_div(x.e.V, x.e.N));
   }
 }
 
@@ -249,9 +245,10 @@ __device__ __forceinline__ void finish_first(const MeshDev& m, uint32_t rec, con
     return;
   }
   Tri t = load_tri(m.tris, rec);
-  ff tt = tri_t_ff(tri_eval_ff(t.a, t.b, t.c, r.o, r.d));
+  const TriFFHit x = tri_eval_ff_hit(t.a, t.b, t.c, r.o, r.d);
+  const ff tt = tri_t_ff(x.e);
   bvhc_hit h;
-  make_hit(t, r, tt, ff_mul(tt, dir_length(r.d)), h);
+  make_hit(t, r, x, tt, ff_mul(tt, dir_length(r.d)), h);
   store_hit(o, h);
 }
 
