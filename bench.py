@@ -679,11 +679,11 @@ def run_batched(args, ws, rank, local):
 
 
 def closest_launches(variant: int) -> int:
-    """Kernels one closestPointToPoint call launches: the per-query kernel alone; the
-    warp-cooperative forms' traversal and finalize, after the query box, the Morton keys and a
-    three-pass radix sort (three kernels a pass) for the sorted forms."""
+    """Kernels one closestPointToPoint call launches: the traversal (per query or warp-cooperative)
+    and the finalize kernel, after the query box, the Morton keys and a three-pass radix sort
+    (three kernels a pass) for the sorted forms."""
     if variant == 0:
-        return 1
+        return 2
     return 2 + (11 if variant % 2 == 0 else 0)
 
 

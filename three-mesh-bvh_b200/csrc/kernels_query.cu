@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) closest_point_kernel(MeshDev m, const 
       if (!found) break;
     }
   }
-  cp_store(m, p, b.rec, out + i);
+  out[i].face_index = b.rec;  // pending, as in the warp-cooperative kernel
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -361,8 +361,8 @@ __global__ void __launch_bounds__(kBlock, MINB) closest_point_packet_kernel(
   if (valid) out[i].face_index = b.rec;
 }
 
-// Completes the records closest_point_packet_kernel left pending, one query per thread in input
-// order.
+// Completes the records closest_point_kernel / closest_point_packet_kernel left pending, one query
+// per thread in input order.
 __global__ void __launch_bounds__(kBlock) closest_point_finalize_kernel(MeshDev m, const float* __restrict__ pts,
                                                                         uint64_t n, bvhc_closest* __restrict__ out) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1227,11 +1227,13 @@ cudaError_t launch_closest_point(const MeshDev& m, const float* pts, uint64_t n,
   // whole warps, 3 / 4 with 16-lane groups, 5 / 6 with 8-lane groups; the even ones run over
   // Morton-sorted queries
   const bool sorted = variant > 0 && variant % 2 == 0;
+  cudaError_t e;
   if (variant == 0 || !(min_t <= 0.0f) || (sorted && (!queue || !qcount || !sort || n >= (1ull << 32)))) {
     dev::closest_point_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, min_t, max_t, out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    dev::closest_point_finalize_kernel<<<grid_for(n), dev::kBlock, 0, stream>>>(m, pts, n, out);
     return cudaGetLastError();
   }
-  cudaError_t e;
   if (sorted) {
     uint32_t *ids, *keys;
     ray_sort_input(2, sort->scratch, queue, &ids, &keys);
