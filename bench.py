@@ -238,13 +238,13 @@ def traversal_kernel(cfg):
 
 def kernel_launches(cfg):
     """Kernels one raycastFirst call launches with a variant (persistent, order, refill, occupancy,
-    compact, sort): the traversal, the finalize pass of the persistent and warp-cooperative forms,
-    the root-box pre-pass and the ray-ordering sort (key pass(es) + 4 radix passes of 3 kernels)."""
+    compact, sort): the traversal, the finalize pass that completes the records, the root-box
+    pre-pass and the ray-ordering sort (key pass(es) + 4 radix passes of 3 kernels)."""
     cfg = list(cfg) if cfg is not None else [1, 1, 16, 0, 0, 0]
     cfg += [0] * (6 - len(cfg))
     persistent, compact, sort = cfg[0], cfg[4], cfg[5]
     if persistent == 0:
-        return 1
+        return 2
     n = 2
     if compact or sort:
         n += 1

@@ -124,19 +124,20 @@ def test_autotune_candidates_and_argument_checks(pkg):
 
     lib = pkg.lib()
     base = autotune.candidates()
-    assert len(base) == 87 and len({tuple(c) for c in base}) == 87
+    assert len(base) == 95 and len({tuple(c) for c in base}) == 95
     fields = autotune.FIELDS
     assert fields[:6] == ["persistent", "order", "refill", "occupancy", "compact", "sort"]
     assert fields[9:] == ["tile", "block", "stack", "tile_rows"]
     forms = {c[0] for c in base}
     assert forms == {0, 1, 2}
     assert any(c[7] == 1 for c in base)                                    # four-child records
+    assert sum(1 for c in base if c[0] == 1 and c[7] == 1) == 8           # persistent over them
     assert {(c[4], c[5]) for c in base if c[0] == 1} == {(0, 0), (1, 0), (1, 1), (1, 2), (1, 3)}
     tiled = autotune.candidates((4096, 1920))
     # per pitch: child pairs (2 child orders x 3 register budgets), then four-child records (3 budgets)
-    assert tiled[:87] == base and len(tiled) == 87 + 18
-    assert {c[9] for c in tiled[87:]} == {4096, 1920} and all(c[0] == 2 and c[4] == 0 for c in tiled[87:])
-    assert [c[7] for c in tiled[87:96]] == [0] * 6 + [1] * 3
+    assert tiled[:95] == base and len(tiled) == 95 + 18
+    assert {c[9] for c in tiled[95:]} == {4096, 1920} and all(c[0] == 2 and c[4] == 0 for c in tiled[95:])
+    assert [c[7] for c in tiled[95:104]] == [0] * 6 + [1] * 3
     with pytest.raises(ValueError):
         autotune.candidates((-8,))
     assert lib.bvhc_autotune_candidates(None, 1, None, 0) == -1

@@ -34,7 +34,8 @@ bvhc_traversal_config make(int persistent, int order, int refill, int occupancy,
 
 // Stage-1 candidates: one ray per thread (both child orders); warp-cooperative over child pairs
 // (child order x register budget x queue) and over four-child records; persistent warps (child
-// order x refill threshold x register budget x queue); warp-cooperative in tiled ray order over
+// order x refill threshold x register budget x queue) and over four-child records (refill
+// threshold x register budget x compaction); warp-cooperative in tiled ray order over
 // child pairs (child order x register budget) and over four-child records (register budget), for
 // each row pitch given.  Queue: none, compaction, compaction + ordering key 1, 2, 3.
 std::vector<bvhc_traversal_config> stage1(const int32_t* tiles, int n_tiles) {
@@ -51,6 +52,10 @@ std::vector<bvhc_traversal_config> stage1(const int32_t* tiles, int n_tiles) {
     for (int refill : {16, 32})
       for (int occ = 1; occ < 3; ++occ)
         for (const auto& q : kQueue) c.push_back(make(1, order, refill, occ, q[0], q[1], 0, 0));
+  // persistent over four-child records (nearest child first), without a queue or with compaction
+  for (int refill : {16, 32})
+    for (int occ = 1; occ < 3; ++occ)
+      for (int compact = 0; compact < 2; ++compact) c.push_back(make(1, 1, refill, occ, compact, 0, 1, 0));
   for (int k = 0; k < n_tiles; ++k) {
     for (int order = 0; order < 2; ++order)
       for (int occ = 0; occ < 3; ++occ) c.push_back(make(2, order, 16, occ, 0, 0, 0, tiles[k]));
@@ -196,7 +201,7 @@ extern "C" bvhc_status bvhc_mesh_autotune(bvhc_mesh* mesh, int n_sets, const flo
       }
     }
     if (st != BVHC_OK) break;
-    if (!(chosen[k].persistent == 2 && chosen[k].wide)) {  // the four-child kernel has one stack size
+    if (!chosen[k].wide) {  // the four-child kernels have one stack size
       bvhc_traversal_config shallow = chosen[k];
       shallow.stack = 32;
       float ms = 0.0f;

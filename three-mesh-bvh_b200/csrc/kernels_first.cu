@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kBlock) raycast_first_kernel(MeshDev m, const 
       if (!found) break;
     }
   }
-  finish_first(m, best.rec, r, out + i);
+  store_first_pending(out + i, best);  // finalize_first_kernel completes a hit
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -99,7 +99,10 @@ __device__ __forceinline__ int mesh_of_ray(const BatchDev& bd, uint64_t rid) {
 // meshes of a BatchedMesh, ExtensionUtilities.js:87-161); a lane looks up its ray's mesh when it
 // takes the ray and traverses that mesh's roots.  Otherwise the mesh's roots are m.roots[0..n).
 // MINB: minimum resident blocks per SM requested from the register allocator (1 = no limit).
-template <int ORDER, bool BATCHED, int MINB, int STACK>
+// WIDE: walk the four-child records (m.quads, m.quad_roots; same leaves and triangle records):
+// half the levels, so half as many dependent node loads per ray; at a record the children the ray
+// enters are taken nearest first (ORDER does not apply) and the others stacked farthest first.
+template <int ORDER, bool BATCHED, int MINB, int STACK, bool WIDE = false>
 __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
     MeshDev m, const BatchDev bd, const float* __restrict__ rays, uint64_t n, int side, const SideTable sides,
     float near_d, float far_d, bvhc_hit* __restrict__ out, unsigned long long* __restrict__ work, int refill,
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
       }
     }
     if (++root < root_end) {
-      link = m.roots[root];
+      link = WIDE ? m.quad_roots[root] : m.roots[root];
       return;
     }
     store_first_pending(out + rid, best);  // finalize_first_kernel completes a hit
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
             root_end = m.n_roots;
           }
           sp = 0;
-          link = m.roots[root];
+          link = WIDE ? m.quad_roots[root] : m.roots[root];
         }
       }
       if (need <= avail) {
@@ -195,8 +198,68 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
       if (idle == 0xFFFFFFFFu && __ballot_sync(0xFFFFFFFFu, active) == 0u) break;
     }
     if (!active) continue;
-    // phase 1: child pairs, until this lane holds a leaf or has finished its ray
-    while (active && !(link & kLeafBit)) {
+    // phase 1: child pairs (or four-child records), until this lane holds a leaf or has finished
+    // its ray
+    while (WIDE && active && !(link & kLeafBit)) {
+      const QuadNode* qn = m.quads + link;
+      float4 lx, ly, lz, hx, hy, hz;
+      ld8(qn->lo[0], lx, ly);
+      ld8(qn->lo[2], lz, hx);
+      ld8(qn->hi[1], hy, hz);
+      const float4 lk = ld4(qn->link);
+      const uint32_t ck[4] = {__float_as_uint(lk.x), __float_as_uint(lk.y), __float_as_uint(lk.z),
+                              __float_as_uint(lk.w)};
+      const float blo[3][4] = {{lx.x, lx.y, lx.z, lx.w}, {ly.x, ly.y, ly.z, ly.w}, {lz.x, lz.y, lz.z, lz.w}};
+      const float bhi[3][4] = {{hx.x, hx.y, hx.z, hx.w}, {hy.x, hy.y, hy.z, hy.w}, {hz.x, hz.y, hz.z, hz.w}};
+      const float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
+      float key[4];
+      uint32_t cl[4];
+      int nh = 0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        float e;
+        const bool h = ck[c] != kEmptyLeaf &&
+                       box_hit(blo[0][c], blo[1][c], blo[2][c], bhi[0][c], bhi[1][c], bhi[2][c], r, near_d, lim, e);
+        key[c] = h ? e : kInf;
+        cl[c] = ck[c];
+        nh += h ? 1 : 0;
+      }
+      // the four (entry, child) pairs nearest first; children the ray misses sort last
+      auto cas = [&](int a, int c) {
+        if (key[c] < key[a]) {
+          const float tk = key[a];
+          key[a] = key[c];
+          key[c] = tk;
+          const uint32_t tl = cl[a];
+          cl[a] = cl[c];
+          cl[c] = tl;
+        }
+      };
+      cas(0, 1);
+      cas(2, 3);
+      cas(0, 2);
+      cas(1, 3);
+      cas(1, 2);
+      if (nh == 0) {
+        pop_next();
+      } else if (sp + nh - 1 > STACK) {
+        atomicOr(m.err, kErrStackOverflow);
+        best.rec = 0xFFFFFFFFu;
+        sp = 0;
+        root = root_end;
+        pop_next();
+      } else {
+#pragma unroll
+        for (int j = 3; j >= 1; --j)
+          if (j < nh) {
+            stack_link[sp] = cl[j];
+            stack_t[sp] = key[j];
+            ++sp;
+          }
+        link = cl[0];
+      }
+    }
+    while (!WIDE && active && !(link & kLeafBit)) {
       Pair p = load_pair(m.nodes, link);
       float lim = fminf(far_d, (best.t + best.err) * (1.0f + kSlabMargin));
       float e0, e1;
@@ -336,7 +399,7 @@ __global__ void __launch_bounds__(kClsThreads) classify_kernel(
 // (device, kernel variant).
 template <class K>
 static unsigned int persistent_grid(K kernel, int variant) {
-  constexpr int kDevs = 64, kVariants = 24;
+  constexpr int kDevs = 64, kVariants = 27;
   static unsigned int cache[kDevs][kVariants] = {};
   int dev_id = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev_id);
@@ -363,10 +426,11 @@ struct PersistentArgs {
   const unsigned int* qcount;
 };
 
-template <int ORDER, bool BATCHED, int MINB, int STACK>
+template <int ORDER, bool BATCHED, int MINB, int STACK, bool WIDE = false>
 static void launch_persistent(const PersistentArgs& a, cudaStream_t stream) {
-  auto kernel = dev::raycast_first_persistent_kernel<ORDER, BATCHED, MINB, STACK>;
-  int variant = (STACK == 32 ? 12 : 0) + ORDER * 6 + (BATCHED ? 3 : 0) + (MINB == 1 ? 0 : (MINB == 6 ? 1 : 2));
+  auto kernel = dev::raycast_first_persistent_kernel<ORDER, BATCHED, MINB, STACK, WIDE>;
+  const int occ_id = MINB == 1 ? 0 : (MINB == 6 ? 1 : 2);
+  int variant = WIDE ? 24 + occ_id : (STACK == 32 ? 12 : 0) + ORDER * 6 + (BATCHED ? 3 : 0) + occ_id;
   unsigned int g = persistent_grid(kernel, variant);
   g = (unsigned int)std::min<uint64_t>(g, (a.n + dev::kBlock - 1) / dev::kBlock);
   kernel<<<g, dev::kBlock, 0, stream>>>(a.m, a.bd, a.rays, a.n, a.side, a.sides, a.near_d, a.far_d, a.out, a.work,
@@ -382,6 +446,13 @@ static void launch_persistent_occ(const PersistentArgs& a, int occupancy, cudaSt
 
 template <bool BATCHED>
 static void launch_persistent_cfg(const PersistentArgs& a, const TraversalConfig& cfg, cudaStream_t stream) {
+  if (!BATCHED && cfg.wide && a.m.quads && a.m.quad_roots) {
+    // four-child records: nearest child first, the 64-entry stack (a record stacks up to three)
+    if (cfg.occupancy == 0) launch_persistent<1, false, 1, 64, true>(a, stream);
+    else if (cfg.occupancy == 1) launch_persistent<1, false, 6, 64, true>(a, stream);
+    else launch_persistent<1, false, 8, 64, true>(a, stream);
+    return;
+  }
   const bool s32 = stack_entries(a.m, cfg.stack) == 32;
   if (cfg.order == 0) {
     if (s32) launch_persistent_occ<0, BATCHED, 32>(a, cfg.occupancy, stream);
@@ -462,7 +533,9 @@ cudaError_t launch_raycast_first(const MeshDev& m, const float* rays, uint64_t n
     dev::raycast_first_kernel<0><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
   else
     dev::raycast_first_kernel<1><<<grid_for(n), dev::kBlock, 0, stream>>>(m, rays, n, side, sides, near_d, far_d, out);
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_finalize_first(m, rays, n, out, nullptr, nullptr, stream);
 }
 
 // The pre-pass over a single mesh's rays for the all-hits raycast: rays that miss get a hit count of
