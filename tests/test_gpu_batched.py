@@ -32,8 +32,11 @@ def _hits(t):
         np.dtype([("face_index", "<u4"), ("distance", "<f4"), ("point", "<f4", 3), ("barycoord", "<f4", 3)]))
 
 
-@pytest.mark.parametrize("cfg", [(1, 1, 16, 0, 0), (1, 0, 32, 1, 1), (0, 1, 16, 0, 0), (1, 1, 8, 2, 1)])
+@pytest.mark.parametrize("cfg", [(1, 1, 16, 0, 0), (1, 0, 32, 1, 1), (0, 1, 16, 0, 0), (1, 1, 8, 2, 1),
+                                 (1, 1, 32, 2, 1, 0, 0, 1), (1, 1, 16, 1, 0, 0, 0, 1)])
 def test_batched_matches_oracle_per_geometry(orc, scene, cfg):
+    """Each geometry's rays against its own oracle, for the persistent launch over child pairs and
+    over four-child records (the 8th field, wide), with and without compaction, and per ray."""
     batch, rays, off, d_rays = scene
     batch.set_traversal(*cfg)
     got = _hits(batch.raycast_first(d_rays, off))

@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(kClsThreads) classify_kernel(
 // (device, kernel variant).
 template <class K>
 static unsigned int persistent_grid(K kernel, int variant) {
-  constexpr int kDevs = 64, kVariants = 27;
+  constexpr int kDevs = 64, kVariants = 30;
   static unsigned int cache[kDevs][kVariants] = {};
   int dev_id = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev_id);
@@ -430,7 +430,7 @@ template <int ORDER, bool BATCHED, int MINB, int STACK, bool WIDE = false>
 static void launch_persistent(const PersistentArgs& a, cudaStream_t stream) {
   auto kernel = dev::raycast_first_persistent_kernel<ORDER, BATCHED, MINB, STACK, WIDE>;
   const int occ_id = MINB == 1 ? 0 : (MINB == 6 ? 1 : 2);
-  int variant = WIDE ? 24 + occ_id : (STACK == 32 ? 12 : 0) + ORDER * 6 + (BATCHED ? 3 : 0) + occ_id;
+  int variant = WIDE ? 24 + (BATCHED ? 3 : 0) + occ_id : (STACK == 32 ? 12 : 0) + ORDER * 6 + (BATCHED ? 3 : 0) + occ_id;
   unsigned int g = persistent_grid(kernel, variant);
   g = (unsigned int)std::min<uint64_t>(g, (a.n + dev::kBlock - 1) / dev::kBlock);
   kernel<<<g, dev::kBlock, 0, stream>>>(a.m, a.bd, a.rays, a.n, a.side, a.sides, a.near_d, a.far_d, a.out, a.work,
@@ -446,11 +446,12 @@ static void launch_persistent_occ(const PersistentArgs& a, int occupancy, cudaSt
 
 template <bool BATCHED>
 static void launch_persistent_cfg(const PersistentArgs& a, const TraversalConfig& cfg, cudaStream_t stream) {
-  if (!BATCHED && cfg.wide && a.m.quads && a.m.quad_roots) {
-    // four-child records: nearest child first, the 64-entry stack (a record stacks up to three)
-    if (cfg.occupancy == 0) launch_persistent<1, false, 1, 64, true>(a, stream);
-    else if (cfg.occupancy == 1) launch_persistent<1, false, 6, 64, true>(a, stream);
-    else launch_persistent<1, false, 8, 64, true>(a, stream);
+  if (cfg.wide && a.m.quads && a.m.quad_roots) {
+    // four-child records: nearest child first, the 64-entry stack (a record stacks up to three);
+    // a batch's meshes index their quad roots as their child-pair roots
+    if (cfg.occupancy == 0) launch_persistent<1, BATCHED, 1, 64, true>(a, stream);
+    else if (cfg.occupancy == 1) launch_persistent<1, BATCHED, 6, 64, true>(a, stream);
+    else launch_persistent<1, BATCHED, 8, 64, true>(a, stream);
     return;
   }
   const bool s32 = stack_entries(a.m, cfg.stack) == 32;
