@@ -354,7 +354,8 @@ bvhc_status bvhc_scene_raycast(bvhc_scene* scene, const float* rays, uint64_t n,
 void bvhc_scene_destroy(bvhc_scene* scene);
 /* Kernel variant of bvhc_scene_raycast_first (no reference counterpart; results are the same for
  * every variant): resident blocks per SM 14 (0), 10 (1) or 8 (2) -- more blocks hide more latency
- * and leave fewer registers per thread. */
+ * and leave fewer registers per thread.  The first-hit query walks raycastFirst's records
+ * (bvhc_mesh_set_leaf_size applies); the all-hits query the reference's. */
 bvhc_status bvhc_scene_set_variant(bvhc_scene* scene, int variant);
 /* Ray order of bvhc_scene_raycast_first: 0 input order; 1, 2, 3 the rays sorted by a Morton key
  * (direction; entry point into the instances' world box; that point and the direction); 4 sorted

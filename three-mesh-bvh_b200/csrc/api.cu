@@ -2065,7 +2065,7 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
       const uint64_t cnt = std::min<uint64_t>(kPipeChunk, n - off);
       cudaStream_t st = m->pipe[k];
       BVHC_CUDA_TRY(cudaMemcpyAsync(m->slot_in[k], rays + 6 * off, cnt * 24, cudaMemcpyHostToDevice, st));
-      BVHC_CUDA_TRY(launch_scene_raycast_first(m->view(), sd, static_cast<const float*>(m->slot_in[k]), cnt, side,
+      BVHC_CUDA_TRY(launch_scene_raycast_first(m->view_first(), sd, static_cast<const float*>(m->slot_in[k]), cnt, side,
                                                near_dist, far_dist, static_cast<bvhc_hit*>(m->slot_out[k]),
                                                static_cast<uint32_t*>(sc->inst_slot[k]), st));
       BVHC_CUDA_TRY(cudaMemcpyAsync(hits + off, m->slot_out[k], cnt * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, st));
@@ -2103,14 +2103,14 @@ bvhc_status bvhc_scene_raycast_first(bvhc_scene* sc, const float* rays, uint64_t
   const RaySort* sp = sort.kind ? &sort : nullptr;
   if (mem == BVHC_MEM_DEVICE) {
     if (!aligned(rays, 8) || !aligned(hits, 16) || !aligned(instance, 4)) return BVHC_ERR_INVALID_ARGUMENT;
-    return from_cuda(launch_scene_raycast_first(m->view(), sd, rays, n, side, near_dist, far_dist, hits, instance, s,
+    return from_cuda(launch_scene_raycast_first(m->view_first(), sd, rays, n, side, near_dist, far_dist, hits, instance, s,
                                                 sp, sc->d_queue, sc->d_qcount));
   }
   BVHC_CUDA_TRY(ensure(&sc->d_in, &sc->in_cap, n * 24));
   BVHC_CUDA_TRY(ensure(&sc->d_out, &sc->out_cap, n * sizeof(bvhc_hit)));
   BVHC_CUDA_TRY(ensure(&sc->d_ids, &sc->ids_cap, n * 4));
   BVHC_CUDA_TRY(cudaMemcpyAsync(sc->d_in, rays, n * 24, cudaMemcpyHostToDevice, s));
-  BVHC_CUDA_TRY(launch_scene_raycast_first(m->view(), sd, static_cast<const float*>(sc->d_in), n, side, near_dist,
+  BVHC_CUDA_TRY(launch_scene_raycast_first(m->view_first(), sd, static_cast<const float*>(sc->d_in), n, side, near_dist,
                                            far_dist, static_cast<bvhc_hit*>(sc->d_out),
                                            static_cast<uint32_t*>(sc->d_ids), s, sp, sc->d_queue, sc->d_qcount));
   BVHC_CUDA_TRY(cudaMemcpyAsync(hits, sc->d_out, n * sizeof(bvhc_hit), cudaMemcpyDeviceToHost, s));
