@@ -616,13 +616,20 @@ def measure_batched(args, ws, rank, local):
     # autotune the batched launch over the traversal variants
     from three_mesh_bvh_b200 import autotune
 
-    # (the batched launch always runs the persistent form; ray ordering applies to single meshes)
+    # (the batched launch always runs the persistent form; ray ordering applies to single meshes),
+    # on each device leaf layout
     cands = [c for c in autotune.candidates() if c[0] == 1 and c[5] == 0]
     timings = {}
-    for cand in cands:
-        batch.set_traversal(*cand)
-        timings[str(list(cand))] = timed(lambda: batch.raycast_first(d_rays, off, out=out, stream=s), 1, 1)
-    best = min(cands, key=lambda c: timings[str(list(c))])
+    for leaf in (0, 2, 4):
+        batch.set_leaf_size(leaf)
+        for cand in cands:
+            batch.set_traversal(*cand)
+            timings[f"{list(cand)}/leaf{leaf}"] = timed(lambda: batch.raycast_first(d_rays, off, out=out, stream=s),
+                                                        1, 1)
+    best_key = min(timings, key=timings.get)
+    best_leaf = int(best_key.split("/leaf")[1])
+    best = next(c for c in cands if f"{list(c)}/leaf{best_leaf}" == best_key)
+    batch.set_leaf_size(best_leaf)
     batch.set_traversal(*best)
     graph = batch.capture(d_rays, off, out)
     with ClockSampler(local) as clk:
@@ -660,7 +667,7 @@ def measure_batched(args, ws, rank, local):
                                            "same_face_indices": same_plain},
                "per_mesh_persistent_launches": {"ms": ms_pers, "mrays_s": n / (ms_pers / 1e3) / 1e6},
                "speedup_vs_per_mesh_plain": ms_plain / ms_graph, "same_face_indices": same_plain,
-               "parity": par, "traversal": list(best), "autotune_ms": timings, "clocks": clk.summary(),
+               "parity": par, "traversal": list(best), "leaf_size": best_leaf, "autotune_ms": timings, "clocks": clk.summary(),
                "setup_s": t_setup, "gpu_launches": args.steps * kernel_launches(best)}
     graph.destroy()
     batch.dispose()

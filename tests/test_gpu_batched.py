@@ -32,12 +32,16 @@ def _hits(t):
         np.dtype([("face_index", "<u4"), ("distance", "<f4"), ("point", "<f4", 3), ("barycoord", "<f4", 3)]))
 
 
-@pytest.mark.parametrize("cfg", [(1, 1, 16, 0, 0), (1, 0, 32, 1, 1), (0, 1, 16, 0, 0), (1, 1, 8, 2, 1),
-                                 (1, 1, 32, 2, 1, 0, 0, 1), (1, 1, 16, 1, 0, 0, 0, 1)])
-def test_batched_matches_oracle_per_geometry(orc, scene, cfg):
+@pytest.mark.parametrize("cfg,leaf", [((1, 1, 16, 0, 0), 0), ((1, 0, 32, 1, 1), 0), ((0, 1, 16, 0, 0), 0),
+                                      ((1, 1, 8, 2, 1), 0), ((1, 1, 32, 2, 1, 0, 0, 1), 0),
+                                      ((1, 1, 16, 1, 0, 0, 0, 1), 0), ((1, 1, 16, 2, 1, 0, 0, 1), 4),
+                                      ((1, 1, 16, 2, 1), 2)])
+def test_batched_matches_oracle_per_geometry(orc, scene, cfg, leaf):
     """Each geometry's rays against its own oracle, for the persistent launch over child pairs and
-    over four-child records (the 8th field, wide), with and without compaction, and per ray."""
+    over four-child records (the 8th field, wide), with and without compaction, per ray, and on
+    split-leaf layouts."""
     batch, rays, off, d_rays = scene
+    batch.set_leaf_size(leaf)
     batch.set_traversal(*cfg)
     got = _hits(batch.raycast_first(d_rays, off))
     batch.synchronize()
@@ -49,6 +53,7 @@ def test_batched_matches_oracle_per_geometry(orc, scene, cfg):
         rep = check_first(got[a:b], exp, tie_exempt(ac, ah))
         bad = {x: rep[x] for x in ("hitmiss", "face", "distance", "point", "barycoord") if rep[x]}
         assert not bad, (k, rep)
+    batch.set_leaf_size(0)
 
 
 def test_per_mesh_launches_and_graph_agree(scene, cuda):

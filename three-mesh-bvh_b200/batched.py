@@ -82,6 +82,14 @@ class BatchedMeshBVH:
                                     block, stack, tile_rows)
         N.check(N.lib().bvhc_mesh_set_traversal(self._device_mesh(), C.byref(cfg)), "bvhc_mesh_set_traversal")
 
+    def set_leaf_size(self, max_leaf: int):
+        """raycastFirst's device leaf layout for every geometry (bvhc_mesh_set_leaf_size): 0 keeps the
+        reference's leaves, max_leaf > 0 splits larger leaves into exact-bounds subtrees."""
+        N.check(N.lib().bvhc_mesh_set_leaf_size(self._device_mesh(), int(max_leaf)), "bvhc_mesh_set_leaf_size")
+
+    def get_leaf_size(self) -> int:
+        return int(N.lib().bvhc_mesh_get_leaf_size(self._device_mesh()))
+
     @staticmethod
     def _offsets(ray_offsets) -> np.ndarray:
         return np.ascontiguousarray(ray_offsets, dtype=np.uint64)
