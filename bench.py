@@ -1058,11 +1058,13 @@ def run_scene(args, ws, rank, local):
         lib.bvhc_scene_raycast_first(scene.h, rays.data_ptr(), n_rays, 0, 0.0, math.inf, hits.data_ptr(),
                                      inst.data_ptr(), 1, s)
 
-    # ray order (input order, a Morton key, or the first instance reached) and kernel variant
-    # (resident blocks per SM 14 / 10 / 8), whichever is fastest here
+    # ray order (input order, a Morton key, or the first instance reached), kernel variant
+    # (resident blocks per SM 14 / 10 / 8) and the geometries' leaf layout, whichever is fastest here
     order_ms = {}
     variants = (0, 1, 2) if args.scene_variant is None else (args.scene_variant,)
-    for occ in variants:
+    leaves = (0, 4) if args.scene_variant is None else (0,)
+    for leaf, occ in ((lf, v) for lf in leaves for v in variants):
+        batch.set_leaf_size(leaf)
         scene.set_variant(occ)
         for order in ((0, 1, 2, 3, 4) if args.scene_variant is None else (0,)):
             scene.set_order(order)
@@ -1072,8 +1074,9 @@ def run_scene(args, ws, rank, local):
             step()
             e1.record(stream)
             e1.synchronize()
-            order_ms[(occ, order)] = e0.elapsed_time(e1)
-    best_occ, best_order = min(order_ms, key=order_ms.get)
+            order_ms[(leaf, occ, order)] = e0.elapsed_time(e1)
+    best_leaf, best_occ, best_order = min(order_ms, key=order_ms.get)
+    batch.set_leaf_size(best_leaf)
     scene.set_variant(best_occ)
     scene.set_order(best_order)
     for _ in range(args.warmup):
@@ -1149,7 +1152,7 @@ def run_scene(args, ws, rank, local):
                                        "the instance cube), firstHitOnly",
                            "geometry_triangles": int(sum(g.triangle_count for g in geoms)),
                            "hit_fraction": hit_frac, "l2": "inputs (100 MB rays + 134 MB hits) exceed L2",
-                           "ray_order": best_order, "kernel_variant": best_occ,
+                           "ray_order": best_order, "kernel_variant": best_occ, "leaf_size": best_leaf,
                            "order_ms": {str(k): v for k, v in order_ms.items()},
                            "all_hits": {"ms": ms_all, "Mrays_per_s": weak_scaling_rate(ws, n_rays, 1, ms_all),
                                         "cap": cap_all, "mean_hits_per_ray": mean_hits}},

@@ -85,6 +85,13 @@ def test_scene_matches_oracle(pkg, orc, batch, cuda, n_inst, scaled):
         scene.set_variant(3)
     scene.set_variant(0)
     scene.set_order(0)
+    # the geometries on split leaves of at most 4 triangles (the first-hit query walks
+    # raycastFirst's records): the oracle's records again
+    batch.set_leaf_size(4)
+    got4, ginst4 = scene.raycast_first(rays)
+    batch.set_leaf_size(0)
+    bad = _compare(got4, ginst4, exp, einst)
+    assert not bad, bad[:10]
     scene.dispose()
 
 

@@ -297,8 +297,9 @@ __global__ void __launch_bounds__(kBlock, MINB) raycast_first_persistent_kernel(
   }
 }
 
-// Completes the pending hits of raycast_first_persistent_kernel, one ray per thread (grid-stride).
-// With a queue only its entries can be pending; the other rays were finished by classify_kernel.
+// Completes the pending hits every raycastFirst traversal kernel leaves (per ray, persistent,
+// warp-cooperative), one ray per thread (grid-stride).  With a queue only its entries can be
+// pending; the other rays were finished by classify_kernel.
 __global__ void __launch_bounds__(kBlock) finalize_first_kernel(MeshDev m, const float* __restrict__ rays, uint64_t n,
                                                                 bvhc_hit* __restrict__ out,
                                                                 const uint32_t* __restrict__ queue,
