@@ -38,10 +38,10 @@ __global__ void __launch_bounds__(kBlock) raycast_all_finalize_kernel(MeshDev m,
   bvhc_hit* out = hits + i * (uint64_t)cap;
   for (uint32_t k = 0; k < c; ++k) {
     const Tri t = load_tri(m.tris, out[k].face_index);
-    const TriFFHit x = tri_eval_ff_hit(t.a, t.b, t.c, r.o, r.d);
-    const ff tt = tri_t_ff(x.e);
+    const TriFF e = tri_eval_ff(t.a, t.b, t.c, r.o, r.d);
+    const ff tt = tri_t_ff(e);
     bvhc_hit h;
-    make_hit(t, r, x, tt, ff_mul(tt, dlen), h);
+    make_hit(t, r, e, tt, ff_mul(tt, dlen), h);
     store_hit(out + k, h);
   }
 }

@@ -160,9 +160,9 @@ __device__ __noinline__ bool local_ray(const InstanceDev& I, const RayF& w, floa
 __device__ __noinline__ ff world_record(const MeshDev& m, const InstanceDev& I, uint32_t rec, const RayF& w,
                                         const RayF& lr, bvhc_hit& h) {
   const Tri t = load_tri(m.tris, rec);
-  const TriFFHit x = tri_eval_ff_hit(t.a, t.b, t.c, lr.o, lr.d);
-  const ff tt = tri_t_ff(x.e);
-  make_hit(t, lr, x, tt, ff_mul(tt, dir_length(lr.d)), h);
+  const TriFF e = tri_eval_ff(t.a, t.b, t.c, lr.o, lr.d);
+  const ff tt = tri_t_ff(e);
+  make_hit(t, lr, e, tt, ff_mul(tt, dir_length(lr.d)), h);
   const ff ox = ff_from(w.o.x), oy = ff_from(w.o.y), oz = ff_from(w.o.z);
   const ff dx = ff_from(w.d.x), dy = ff_from(w.d.y), dz = ff_from(w.d.z);
   ff3 P[3];

@@ -133,32 +133,44 @@ struct TriFF {
   ff N, U, V, W, T;
 };
 
-// The float-float determinants of a ray / triangle pair, together with what a hit record's
-// barycentrics need from the same edge vectors and normal: g = |n|^2 and l12 = |e1|^2 |e2|^2 (the
-// degenerate-triangle test), so that a record takes one evaluation.  One out-of-line body serves
-// every float-float triangle evaluation (tri_eval_ff below), which keeps kernels that call it from
-// several places fetching one copy of the code.
-struct TriFFHit {
-  TriFF e;
-  ff g, l12;
-};
-
-static __device__ __noinline__ TriFFHit tri_eval_ff_hit(float3 a, float3 b, float3 c, float3 o, float3 d) {
+// The float-float determinants of a ray / triangle pair.  One out-of-line body serves every
+// float-float triangle evaluation, which keeps kernels that call it from several places fetching
+// one copy of the code.
+static __device__ __noinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
   ff3 e1 = ff3_diff(b, a), e2 = ff3_diff(c, a), q = ff3_diff(o, a);
   ff3 n = ff3_cross(e1, e2);
-  TriFFHit r;
-  r.e.N = ff3_dot_f(d, n);
-  r.e.U = ff3_dot_f(d, ff3_cross(q, e2));
-  r.e.V = ff3_dot_f(d, ff3_cross(e1, q));
-  r.e.W = ff_sub(ff_sub(r.e.N, r.e.U), r.e.V);
-  r.e.T = ff3_dot(q, n);
-  r.g = ff3_dot(n, n);
-  r.l12 = ff_mul(ff3_dot(e1, e1), ff3_dot(e2, e2));
+  TriFF r;
+  r.N = ff3_dot_f(d, n);
+  r.U = ff3_dot_f(d, ff3_cross(q, e2));
+  r.V = ff3_dot_f(d, ff3_cross(e1, q));
+  r.W = ff_sub(ff_sub(r.N, r.U), r.V);
+  r.T = ff3_dot(q, n);
   return r;
 }
 
-__device__ __forceinline__ TriFF tri_eval_ff(float3 a, float3 b, float3 c, float3 o, float3 d) {
-  return tri_eval_ff_hit(a, b, c, o, d).e;
+// A triangle whose barycentrics the hit record leaves at zero: |n|^2 <= 2^-50 |e1|^2 |e2|^2 in
+// float-float (n = e1 x e2).
+static __device__ __noinline__ bool tri_degenerate_ff(float3 a, float3 b, float3 c) {
+  const ff3 e1 = ff3_diff(b, a), e2 = ff3_diff(c, a);
+  const ff3 n = ff3_cross(e1, e2);
+  const ff g = ff3_dot(n, n);
+  const ff l12 = ff_mul(ff3_dot(e1, e1), ff3_dot(e2, e2));
+  return g.hi <= 8.8817841970012523e-16f * l12.hi;  // 2^-50
+}
+
+// The same decision, settled in float32 when it is clear.  The float32 normal differs from the
+// exact one by at most about 9u |e1| |e2| (u = 2^-24: the edge differences, products and sums), so a
+// float32 normal of at least 2^-16 |e1| |e2| (squared: 2^-32, with |e1|^2 |e2|^2 kept inside the
+// normal float range) puts the exact |n|^2 above 2^-33 |e1|^2 |e2|^2, far from 2^-50: not
+// degenerate.  Anything else takes the float-float test.
+__device__ __forceinline__ bool tri_degenerate(float3 a, float3 b, float3 c) {
+  const float e1x = b.x - a.x, e1y = b.y - a.y, e1z = b.z - a.z;
+  const float e2x = c.x - a.x, e2y = c.y - a.y, e2z = c.z - a.z;
+  const float nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+  const float gf = nx * nx + ny * ny + nz * nz;
+  const float lf = (e1x * e1x + e1y * e1y + e1z * e1z) * (e2x * e2x + e2y * e2y + e2z * e2z);
+  if (lf >= 0x1p-60f && lf <= 0x1p100f && gf >= 0x1p-32f * lf) return false;
+  return tri_degenerate_ff(a, b, c);
 }
 
 __device__ __forceinline__ bool tri_decide_ff(const TriFF& r, int side) {

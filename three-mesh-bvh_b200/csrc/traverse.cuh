@@ -136,8 +136,8 @@ __device__ __forceinline__ ff dir_length(float3 d) {
 // Full intersection record for a triangle known to be hit, in float-float, rounded once.
 // barycoord follows Triangle.getBarycoord: (0, 0, 0) when the triangle's Gram determinant
 // |e1 x e2|^2 vanishes at float64 resolution (the reference's `denom === 0` case).
-// x = tri_eval_ff_hit of the triangle and ray, tt = its t, dist = the hit's distance.
-static __device__ void make_hit(const Tri& t, const RayF& r, const TriFFHit& x, ff tt, ff dist, bvhc_hit& h) {
+// e = tri_eval_ff of the triangle and ray, tt = its t, dist = the hit's distance.
+static __device__ void make_hit(const Tri& t, const RayF& r, const TriFF& e, ff tt, ff dist, bvhc_hit& h) {
   ff3 px = {ff_add(ff_from(r.o.x), ff_mul_f(tt, r.d.x)), ff_add(ff_from(r.o.y), ff_mul_f(tt, r.d.y)),
             ff_add(ff_from(r.o.z), ff_mul_f(tt, r.d.z))};
   h.face_index = t.face;
@@ -145,12 +145,12 @@ static __device__ void make_hit(const Tri& t, const RayF& r, const TriFFHit& x, 
   h.point[0] = ff_to_f(px.x);
   h.point[1] = ff_to_f(px.y);
   h.point[2] = ff_to_f(px.z);
-  if (x.g.hi <= 8.8817841970012523e-16f * x.l12.hi) {  // 2^-50
+  if (tri_degenerate(t.a, t.b, t.c)) {
     h.barycoord[0] = h.barycoord[1] = h.barycoord[2] = 0.0f;
   } else {
-    h.barycoord[0] = ff_to_f(ff_div(x.e.W, x.e.N));
-    h.barycoord[1] = ff_to_f(ff_div(x.e.U, x.e.N));
-    h.barycoord[2] = ff_to_f(ff_div(x.e.V, x.e.N));
+    h.barycoord[0] = ff_to_f(ff_div(e.W, e.N));
+    h.barycoord[1] = ff_to_f(ff_div(e.U, e.N));
+    h.barycoord[2] = ff_to_f(ff_div(e.V, e.N));
   }
 }
 
@@ -245,10 +245,10 @@ __device__ __forceinline__ void finish_first(const MeshDev& m, uint32_t rec, con
     return;
   }
   Tri t = load_tri(m.tris, rec);
-  const TriFFHit x = tri_eval_ff_hit(t.a, t.b, t.c, r.o, r.d);
-  const ff tt = tri_t_ff(x.e);
+  const TriFF e = tri_eval_ff(t.a, t.b, t.c, r.o, r.d);
+  const ff tt = tri_t_ff(e);
   bvhc_hit h;
-  make_hit(t, r, x, tt, ff_mul(tt, dir_length(r.d)), h);
+  make_hit(t, r, e, tt, ff_mul(tt, dir_length(r.d)), h);
   store_hit(o, h);
 }
 
