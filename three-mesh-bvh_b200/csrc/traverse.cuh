@@ -148,9 +148,12 @@ static __device__ void make_hit(const Tri& t, const RayF& r, const TriFF& e, ff 
   if (tri_degenerate(t.a, t.b, t.c)) {
     h.barycoord[0] = h.barycoord[1] = h.barycoord[2] = 0.0f;
   } else {
-    h.barycoord[0] = ff_to_f(ff_div(e.W, e.N));
-    h.barycoord[1] = ff_to_f(ff_div(e.U, e.N));
-    h.barycoord[2] = ff_to_f(ff_div(e.V, e.N));
+    // W / N, U / N, V / N through one float-float reciprocal (relative error ~2^-44, rounded once
+    // to float32)
+    const ff rn = ff_div(ff{1.0f, 0.0f}, e.N);
+    h.barycoord[0] = ff_to_f(ff_mul(e.W, rn));
+    h.barycoord[1] = ff_to_f(ff_mul(e.U, rn));
+    h.barycoord[2] = ff_to_f(ff_mul(e.V, rn));
   }
 }
 
