@@ -159,8 +159,8 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * the compaction pass) orders the remaining rays by a Morton key before the traversal: 1 the ray
  * direction (cube-map coordinates), 2 the point where the ray enters the mesh's bounding box, 3
  * that point (coarser) followed by the direction; 0 keeps the input order.  wide = 1 makes the
- * warp-cooperative form walk four-child records (collapsed from raycastFirst's child pairs, same
- * leaves).  closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32
+ * warp-cooperative and persistent forms (and batched launches) walk four-child records (collapsed
+ * from raycastFirst's child pairs, same leaves; children taken nearest first, 64-entry stack).  closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32
  * queries of a warp through one shared traversal (for spatially coherent queries such as grids),
  * 2 the same over the queries sorted by a Morton key of the point, 3 and 4 as 1 and 2 with groups
  * of 16 consecutive queries (two shared traversals per warp), 5 and 6 with groups of 8; 1 to 6
@@ -206,7 +206,7 @@ bvhc_status bvhc_mesh_get_traversal(const bvhc_mesh* mesh, bvhc_traversal_config
  * and the shader stack depth, src/webgl/glsl/bvh_ray_functions.glsl.js:14-16).  Times the
  * traversal variants with CUDA events on `stream` over the caller's ray sets (device memory,
  * n_sets sets of counts[k] rays) and installs the fastest.  Stage 1: every candidate (one ray per
- * thread; warp-cooperative over child pairs or four-child records; persistent warps; with and
+ * thread; warp-cooperative over child pairs or four-child records; persistent warps over either; with and
  * without the root-box compaction and each ordering key; register budgets; the tiled ray order for
  * each row pitch in tile_pitches, e.g. an image width) for every device leaf layout in leaf_sizes
  * (NULL / 0: the current one); the layout with the smallest sum of the sets' best times wins.
