@@ -162,10 +162,11 @@ bvhc_status bvhc_mesh_get_info(const bvhc_mesh* mesh, bvhc_mesh_info* info);
  * warp-cooperative and persistent forms (and batched launches) walk four-child records (collapsed
  * from raycastFirst's child pairs, same leaves; children taken nearest first, 64-entry stack).
  * closest selects closestPointToPoint's kernel: 0 one query per thread, 1 the 32 queries of a warp
- * through one shared traversal (for spatially coherent queries such as grids), 2 the same over the queries sorted by a Morton key of the point, 3 and 4 as 1 and 2 with groups
- * of 16 consecutive queries (two shared traversals per warp), 5 and 6 with groups of 8; 1 to 6
- * apply with minThreshold 0 (otherwise 0 runs), and use the occupancy setting too; 1, 3 and 5 also
- * read the queries in tiled order when `tile` is set (rows of `tile` points, e.g. a grid's row).
+ * through one shared traversal (for spatially coherent queries such as grids), 2 the same over the
+ * queries sorted by a Morton key of the point, 3 and 4 as 1 and 2 with groups of 16 consecutive
+ * queries (two shared traversals per warp), 5 and 6 with groups of 8; 1 to 6 apply with
+ * minThreshold 0 (otherwise 0 runs), and use the occupancy setting too; 1, 3 and 5 also read the
+ * queries in tiled order when `tile` is set (rows of `tile` points, e.g. a grid's row).
  * All forms return the same bytes.  all selects raycast's
  * (all hits) kernel: 0 one ray per thread, 1 the rays of a warp through one shared left-first
  * traversal (each ray's hits stay in the reference's DFS order), 2, 3 and 4 the same over the rays
