@@ -119,6 +119,33 @@ def test_degenerate_triangle_gpu(pkg, cuda):
     assert bvh.raycastFirst(((0, 0, 1), (0, 0, -1)), pkg.FrontSide) is None
 
 
+def test_sliver_triangles_barycoords(pkg, orc, cuda):
+    """Hit records on sliver triangles (apex 2^-30 .. 2^-12 of the base length off the base line):
+    the degenerate-triangle test is settled in float32 only when the triangle is clearly not
+    degenerate (apex at 2^-16 and wider here) and in float-float otherwise, and the records (the
+    zero barycentrics of the degenerate ones included) match the oracle's."""
+    heights = [2.0 ** -30, 2.0 ** -28, 2.0 ** -20, 2.0 ** -18, 2.0 ** -17, 2.0 ** -16, 2.0 ** -15, 2.0 ** -12]
+    pos, rays = [], []
+    for k, h in enumerate(heights):
+        x = 10.0 * k
+        pos += [[x, 0.0, 0.0], [x + 2.0, 0.0, 0.0], [x + 1.0, h, 0.0]]
+        for fx, fy in ((1.0, 0.5), (0.75, 0.25), (1.25, 0.25), (1.0, 0.875)):
+            rays.append([x + fx, h * fy, 5.0, 0.0, 0.0, -1.0])
+    geo = pkg.Geometry(np.array(pos, dtype=np.float32), None)
+    bvh = pkg.MeshBVH(geo)
+    ref = _oracle_for(orc, bvh, geo)
+    rays = np.array(rays, dtype=np.float32)
+    got = bvh.raycast_first_batch(rays, pkg.DoubleSide)
+    exp = ref.raycast_first(rays, pkg.DoubleSide)
+    ac, ah = ref.raycast_all(rays, pkg.DoubleSide)
+    _assert_first_ok(check_first(got, exp, tie_exempt(ac, ah)))
+    hit = exp["face_index"] != 0xFFFFFFFF
+    assert hit.sum() >= 20
+    zero = (exp["barycoord"] == 0).all(1)
+    assert zero[hit].any() and (~zero[hit]).any()   # both degenerate and ordinary slivers are hit
+    bvh.dispose()
+
+
 def test_sphere_distance_gpu(pkg, cuda):
     geo = pkg.sphere(1, 200, 200)
     bvh = pkg.MeshBVH(geo, {"verbose": False})
